@@ -1,0 +1,161 @@
+#ifndef PHY_FLUID_H
+#define PHY_FLUID_H
+
+/*
+ * SPH fluid entry points added by the B200 build (ABI version 3).
+ *
+ * They expose the reference's Rust API of crates/phy-fluid to C callers:
+ * SphParams<T> (src/sph/params.rs:12-86), FluidWorld<T> (src/sph/world.rs:
+ * 21-197) and FluidSubsystem<T> (src/subsystem.rs:26-164).  A world handle is
+ * the PhyWorldHandle of phy_ffi.h; `sub` selects a fluid subsystem by its index
+ * among the world's fluid subsystems (0 for the first).
+ *
+ * Particle fields are read and written in insertion order, exactly like the
+ * reference's `FluidWorld::particles` Vec, whatever order the device keeps
+ * them in.  Vector fields are xyz-interleaved (3 doubles per particle).
+ *
+ * Precision forms of the step:
+ *   PHY_PRECISION_F64_PLAIN  f64 everywhere, the reference's operation order,
+ *                            no FMA contraction: bit-identical to
+ *                            FluidWorld<f64>::step and run-to-run.
+ *   PHY_PRECISION_F32_COMP   pairwise kernel math in f32 on cell-relative
+ *                            coordinates with compensated (Kahan) sums of
+ *                            density and force; positions, velocities,
+ *                            cell keys, integration and diagnostics stay f64.
+ *
+ * Return codes are those of phy_ffi.h.
+ */
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "phy_ffi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PHY_MAX_MATERIALS 16
+
+enum {
+  PHY_PRECISION_F64_PLAIN = 0,
+  PHY_PRECISION_F32_COMP = 1
+};
+
+/* Particle fields (crates/phy-fluid/src/particle.rs:17-46). */
+enum {
+  PHY_FIELD_POS = 0,      /* 3 per particle */
+  PHY_FIELD_VEL = 1,      /* 3 */
+  PHY_FIELD_ACC = 2,      /* 3, written by the step */
+  PHY_FIELD_BODY_ACC = 3, /* 3, coupling input, zeroed by the step */
+  PHY_FIELD_RHO = 4,      /* 1, written by the step */
+  PHY_FIELD_P = 5,        /* 1, written by the step */
+  PHY_FIELD_MASS = 6,     /* 1 */
+  PHY_FIELD_MU_EFF = 7,   /* 1, written by the step */
+  PHY_FIELD_XSPH = 8,     /* 3, written by the step */
+  PHY_FIELD_MATERIAL = 9  /* 1, integer value carried in a double */
+};
+
+/* SphParams<f64> (crates/phy-fluid/src/sph/params.rs:12-86).  The two
+ * per-material tables are Rust Vecs there; here they hold n_visc_k and
+ * n_visc_n entries (1..PHY_MAX_MATERIALS).  `viscosity` is carried but, as in
+ * the reference, the step reads visc_k/visc_n only. */
+typedef struct PhySphParams {
+  double rest_density;
+  double stiffness;
+  double viscosity;
+  double shear_min;
+  double mass;
+  double h;
+  double gravity[3];
+  double bounds_min[3];
+  double bounds_max[3];
+  double boundary_damp;
+  double xsph_eps;
+  uint32_t n_visc_k;
+  uint32_t n_visc_n;
+  double visc_k[PHY_MAX_MATERIALS];
+  double visc_n[PHY_MAX_MATERIALS];
+} PhySphParams;
+
+/* SphParams::defaults() (params.rs:55-85). */
+void phy_sph_params_defaults(PhySphParams *out);
+
+/* World holding one empty FluidSubsystem::new(FluidWorld::new(params))
+ * (world.rs:94-102, subsystem.rs:44-55).  The smoothing length used by the
+ * kernel coefficients and the grid cell is captured here, as in the
+ * reference; later changes of params->h move only the cutoff tests. */
+PhyWorldHandle *phy_fluid_world_create(const PhySphParams *params, int32_t precision);
+
+/* Appends another fluid subsystem; returns its `sub` index or -1. */
+int32_t phy_fluid_add_subsystem(PhyWorldHandle *w, const PhySphParams *params, int32_t precision);
+
+/* FluidWorld::fill_box (world.rs:124-144). */
+int32_t phy_fluid_fill_box(PhyWorldHandle *w, uint32_t sub, const double *min3, const double *max3,
+                           double spacing, double margin);
+
+/* FluidWorld::lattice_mass (world.rs:148-169); NaN on error. */
+double phy_fluid_lattice_mass(PhyWorldHandle *w, uint32_t sub, double spacing);
+
+/* Appends n particles like Particle::with_material (particle.rs:50-71) with
+ * the given velocity.  vel and material may be NULL (zero / material 0). */
+int32_t phy_fluid_add_particles(PhyWorldHandle *w, uint32_t sub, uint64_t n, const double *pos,
+                                const double *vel, const double *mass, const uint32_t *material);
+
+/* FluidWorld::len (world.rs:105-107); -1 on error. */
+int64_t phy_fluid_len(PhyWorldHandle *w, uint32_t sub);
+
+/* Reads / writes one particle field for all particles, insertion order.
+ * len is in doubles and must be at least len(sub) * components. */
+int32_t phy_fluid_get_field(PhyWorldHandle *w, uint32_t sub, int32_t field, double *out, uint64_t len);
+int32_t phy_fluid_set_field(PhyWorldHandle *w, uint32_t sub, int32_t field, const double *in,
+                            uint64_t len);
+
+/* The public `params` field: live read and write. */
+int32_t phy_fluid_get_params(PhyWorldHandle *w, uint32_t sub, PhySphParams *out);
+int32_t phy_fluid_set_params(PhyWorldHandle *w, uint32_t sub, const PhySphParams *in);
+
+/* FluidWorld::step (world.rs:183-192) on one subsystem, `n` times, without
+ * the World's coupling stage or time accumulation. */
+int32_t phy_fluid_step(PhyWorldHandle *w, uint32_t sub, double dt, uint32_t n);
+
+/* FluidSubsystem::total_momentum and kinetic_energy (subsystem.rs:149-163):
+ * out4 = {Px, Py, Pz, KE}, summed in insertion order in f64. */
+int32_t phy_fluid_diagnostics(PhyWorldHandle *w, uint32_t sub, double *out4);
+
+/* FluidSubsystem coupling coefficients (subsystem.rs:26-55):
+ * {thermal_expansion, heat_gain, t_ref, drag, friction}. */
+int32_t phy_fluid_get_coupling(PhyWorldHandle *w, uint32_t sub, double *out5);
+int32_t phy_fluid_set_coupling(PhyWorldHandle *w, uint32_t sub, const double *in5);
+
+/* Runs all of the world's device work on the given cudaStream_t (NULL = the
+ * handle's own stream).  The caller keeps the stream alive. */
+int32_t phy_fluid_set_stream(PhyWorldHandle *w, void *cuda_stream);
+
+/* Blocks until the world's device work has finished. */
+int32_t phy_fluid_synchronize(PhyWorldHandle *w);
+
+/* Enables (on != 0) or disables counting of neighbour candidates and pairs
+ * in the density pass of `sub` (one atomic per warp; off by default). */
+int32_t phy_fluid_set_counting(PhyWorldHandle *w, uint32_t sub, int32_t on);
+
+/* Counters of the last counted step of `sub`: out4 = {candidates visited,
+ * pairs with r < h, particles, grid cells}.  Used for roofline accounting. */
+int32_t phy_fluid_step_counters(PhyWorldHandle *w, uint32_t sub, uint64_t *out4);
+
+/* Per-phase device timing of `sub` with CUDA events on its stream.  While on,
+ * every step waits for its own events (so leave it off on the hot path);
+ * phy_fluid_phase_times returns the accumulated milliseconds
+ * out5 = {sort, per-particle prep, density pass, force pass, steps timed}
+ * and resets them when reset != 0. */
+int32_t phy_fluid_set_timing(PhyWorldHandle *w, uint32_t sub, int32_t on);
+int32_t phy_fluid_phase_times(PhyWorldHandle *w, uint32_t sub, double *out5, int32_t reset);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *phy_fluid_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHY_FLUID_H */

@@ -1,0 +1,186 @@
+"""TEST INFRASTRUCTURE ONLY — ctypes wrapper of the CPU oracle (liboracle.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, always as the checker or the timed CPU baseline, never on the product
+path.  Parity against reference-generated outputs is unpinned (the Rust
+reference cannot be built here; see sph_oracle.cpp).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "liboracle.so"
+
+F_POS, F_VEL, F_ACC, F_BODY_ACC, F_RHO, F_P, F_MASS, F_MU_EFF, F_XSPH, F_MATERIAL = range(10)
+_VEC = {F_POS, F_VEL, F_ACC, F_BODY_ACC, F_XSPH}
+
+
+class OrcParams(C.Structure):
+    _fields_ = [
+        ("rest_density", C.c_double), ("stiffness", C.c_double), ("viscosity", C.c_double),
+        ("shear_min", C.c_double), ("mass", C.c_double), ("h", C.c_double),
+        ("gravity", C.c_double * 3), ("bounds_min", C.c_double * 3), ("bounds_max", C.c_double * 3),
+        ("boundary_damp", C.c_double), ("xsph_eps", C.c_double),
+        ("n_visc_k", C.c_uint32), ("n_visc_n", C.c_uint32),
+        ("visc_k", C.c_double * 16), ("visc_n", C.c_double * 16),
+    ]
+
+
+_lib = None
+DP = C.POINTER(C.c_double)
+SRC = Path(__file__).resolve().parent / "sph_oracle.cpp"
+
+
+def build(force: bool = False) -> Path:
+    """Compiles liboracle.so with the flags of oracle/Makefile (no FMA contraction)."""
+    if not force and LIB_PATH.exists() and LIB_PATH.stat().st_mtime >= SRC.stat().st_mtime:
+        return LIB_PATH
+    import subprocess
+    r = subprocess.run(["make", "-C", os.fspath(LIB_PATH.parent), "liboracle.so"], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
+    return LIB_PATH
+
+
+def load():
+    global _lib
+    if _lib is None:
+        build()
+        lib = C.CDLL(os.fspath(LIB_PATH))
+        sig = {
+            "orc_new": (C.c_void_p, [C.POINTER(OrcParams)]),
+            "orc_free": (None, [C.c_void_p]),
+            "orc_len": (C.c_uint64, [C.c_void_p]),
+            "orc_set_threads": (None, [C.c_void_p, C.c_int]),
+            "orc_max_threads": (C.c_int, []),
+            "orc_set_params": (None, [C.c_void_p, C.POINTER(OrcParams)]),
+            "orc_get_params": (None, [C.c_void_p, C.POINTER(OrcParams)]),
+            "orc_fill_box": (None, [C.c_void_p, DP, DP, C.c_double, C.c_double]),
+            "orc_lattice_mass": (C.c_double, [C.c_void_p, C.c_double]),
+            "orc_add": (None, [C.c_void_p, C.c_uint64, DP, DP, DP, C.POINTER(C.c_uint64)]),
+            "orc_get": (C.c_int, [C.c_void_p, C.c_int, DP]),
+            "orc_set": (C.c_int, [C.c_void_p, C.c_int, DP]),
+            "orc_step": (None, [C.c_void_p, C.c_double]),
+            "orc_step_n": (None, [C.c_void_p, C.c_double, C.c_int]),
+            "orc_cell_keys": (None, [C.c_void_p, C.POINTER(C.c_int64)]),
+            "orc_neighbors": (C.c_uint64, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64), C.c_uint64]),
+            "orc_diagnostics": (None, [C.c_void_p, DP]),
+            "orc_counters": (None, [C.c_void_p, C.POINTER(C.c_uint64), C.c_int]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def params_struct(p) -> OrcParams:
+    """OrcParams from any object with SphParams' attribute names."""
+    c = OrcParams()
+    for name in ("rest_density", "stiffness", "viscosity", "shear_min", "mass", "h", "boundary_damp",
+                 "xsph_eps"):
+        setattr(c, name, float(getattr(p, name)))
+    for name in ("gravity", "bounds_min", "bounds_max"):
+        arr = getattr(c, name)
+        v = getattr(p, name)
+        for k in range(3):
+            arr[k] = float(v[k])
+    c.n_visc_k = len(p.visc_k)
+    c.n_visc_n = len(p.visc_n)
+    for k, v in enumerate(p.visc_k):
+        c.visc_k[k] = float(v)
+    for k, v in enumerate(p.visc_n):
+        c.visc_n[k] = float(v)
+    return c
+
+
+class OracleWorld:
+    """CPU restatement of FluidWorld<f64> (crates/phy-fluid/src/sph/world.rs)."""
+
+    def __init__(self, params, threads: int = 1):
+        self._lib = load()
+        c = params_struct(params)
+        self._w = self._lib.orc_new(C.byref(c))
+        self._lib.orc_set_threads(self._w, threads)
+
+    def __del__(self):
+        try:
+            self._lib.orc_free(self._w)
+        except Exception:
+            pass
+
+    def set_threads(self, n: int) -> None:
+        self._lib.orc_set_threads(self._w, n)
+
+    def set_params(self, params) -> None:
+        c = params_struct(params)
+        self._lib.orc_set_params(self._w, C.byref(c))
+
+    def __len__(self) -> int:
+        return int(self._lib.orc_len(self._w))
+
+    def fill_box(self, mn, mx, spacing, margin) -> None:
+        a = np.asarray(mn, np.float64)
+        b = np.asarray(mx, np.float64)
+        self._lib.orc_fill_box(self._w, a.ctypes.data_as(DP), b.ctypes.data_as(DP), spacing, margin)
+
+    def lattice_mass(self, s: float) -> float:
+        return float(self._lib.orc_lattice_mass(self._w, s))
+
+    def add_particles(self, pos, mass, vel=None, material=None) -> None:
+        pos = np.ascontiguousarray(pos, np.float64).reshape(-1)
+        n = pos.size // 3
+        mass = np.ascontiguousarray(np.broadcast_to(np.asarray(mass, np.float64), (n,)))
+        vp = None
+        if vel is not None:
+            vel = np.ascontiguousarray(vel, np.float64).reshape(-1)
+            vp = vel.ctypes.data_as(DP)
+        mp = None
+        if material is not None:
+            material = np.ascontiguousarray(np.broadcast_to(np.asarray(material, np.uint64), (n,)))
+            mp = material.ctypes.data_as(C.POINTER(C.c_uint64))
+        self._lib.orc_add(self._w, n, pos.ctypes.data_as(DP), vp, mass.ctypes.data_as(DP), mp)
+
+    def get(self, field: int) -> np.ndarray:
+        n = len(self)
+        out = np.empty(3 * n if field in _VEC else n, np.float64)
+        if self._lib.orc_get(self._w, field, out.ctypes.data_as(DP)) != 0:
+            raise ValueError(field)
+        return out.reshape(n, 3) if field in _VEC else out
+
+    def set(self, field: int, values) -> None:
+        a = np.ascontiguousarray(values, np.float64).reshape(-1)
+        if self._lib.orc_set(self._w, field, a.ctypes.data_as(DP)) != 0:
+            raise ValueError(field)
+
+    def step(self, dt: float, n: int = 1) -> None:
+        self._lib.orc_step_n(self._w, dt, n)
+
+    def cell_keys(self) -> np.ndarray:
+        out = np.empty(3 * len(self), np.int64)
+        self._lib.orc_cell_keys(self._w, out.ctypes.data_as(C.POINTER(C.c_int64)))
+        return out.reshape(-1, 3)
+
+    def neighbors(self, i: int, cap: int = 4096) -> np.ndarray:
+        out = np.empty(cap, np.uint64)
+        n = self._lib.orc_neighbors(self._w, i, out.ctypes.data_as(C.POINTER(C.c_uint64)), cap)
+        return out[: min(n, cap)].copy()
+
+    def diagnostics(self) -> np.ndarray:
+        out = np.empty(4, np.float64)
+        self._lib.orc_diagnostics(self._w, out.ctypes.data_as(DP))
+        return out
+
+    def counters(self, reset: bool = True) -> tuple:
+        out = (C.c_uint64 * 2)()
+        self._lib.orc_counters(self._w, out, 1 if reset else 0)
+        return int(out[0]), int(out[1])
+
+
+def max_threads() -> int:
+    return int(load().orc_max_threads())

@@ -1,0 +1,521 @@
+// TEST INFRASTRUCTURE ONLY — the CPU oracle for the SPH fluid step.
+//
+// This file restates, in plain C++17, the reference's weakly-compressible SPH
+// step `FluidWorld<T>::step` (jojo240607/physics, crate phy-fluid) so that the
+// CUDA product can be checked against it.  It is never linked into the
+// product library and nothing in `physics_b200/` loads it; only the tests,
+// `__graft_entry__.smoke()` and the CPU-baseline leg of `bench.py` do.
+//
+// Parity status: the reference is Rust and cannot be compiled here (no
+// cargo/rustc, crates not vendored), and its own tests hold no golden vectors
+// for this path.  The restatement is therefore pinned only against the
+// reference's property tests and the analytic known answers derivable from
+// its definitions (see tests/test_oracle.py) — parity against
+// reference-generated outputs is UNPINNED.
+//
+// Arithmetic contract (follows the reference expression by expression):
+//   * no FMA contraction (build with -ffp-contract=off), IEEE division/sqrt;
+//   * evaluation order left-to-right exactly as the Rust source groups it;
+//   * |v| = sqrt((x*x + y*y) + z*z): nalgebra 0.33.3 `Matrix::norm` =
+//     `norm_squared().sqrt()`, and its `dotx` special-cases 3-vectors as
+//     `a + b + c` of the component products (nalgebra is a crates.io
+//     dependency, absent here; this is its published algorithm);
+//   * neighbour visit order: 27 cells with di outermost, dk innermost, and the
+//     particles of a cell in ascending insertion index (HashMap of Vec pushed
+//     in index order).
+//
+// The density and force passes optionally run on OpenMP threads, mirroring the
+// reference's rayon per-particle maps; results do not depend on the thread
+// count because every particle's reduction is sequential and write-disjoint.
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;  // std::f64::consts::PI
+
+struct V3 {
+  double x, y, z;
+};
+inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 operator*(V3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline V3 operator/(V3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+inline V3& operator+=(V3& a, V3 b) {
+  a.x = a.x + b.x;
+  a.y = a.y + b.y;
+  a.z = a.z + b.z;
+  return a;
+}
+// nalgebra Vector3::norm (see header).
+inline double norm(V3 a) { return std::sqrt((a.x * a.x + a.y * a.y) + a.z * a.z); }
+inline double norm_squared(V3 a) { return (a.x * a.x + a.y * a.y) + a.z * a.z; }
+
+}  // namespace
+
+extern "C" {
+
+// Same field layout as `PhySphParams` in include/phy_fluid.h.
+// Mirrors SphParams<T> (crates/phy-fluid/src/sph/params.rs:12-86).
+struct OrcParams {
+  double rest_density, stiffness, viscosity, shear_min, mass, h;
+  double gravity[3], bounds_min[3], bounds_max[3];
+  double boundary_damp, xsph_eps;
+  uint32_t n_visc_k, n_visc_n;
+  double visc_k[16], visc_n[16];
+};
+
+}  // extern "C"
+
+namespace {
+
+// Particle<T> (crates/phy-fluid/src/particle.rs:17-46).
+struct Particle {
+  V3 pos{0, 0, 0}, vel{0, 0, 0}, acc{0, 0, 0}, body_acc{0, 0, 0};
+  double rho = 0, p = 0, mass = 0;
+  uint64_t material = 0;
+  double mu_eff = 0;
+  V3 xsph{0, 0, 0};
+};
+
+// Kernels<T> (crates/phy-fluid/src/kernels.rs:20-66): coefficients captured from h.
+struct Kernels {
+  double h, h2, poly6_coeff, spiky_grad_coeff, visc_lap_coeff;
+  explicit Kernels(double hh) {
+    h = hh;
+    h2 = hh * hh;
+    double h3 = h2 * hh;
+    double h6 = h3 * h3;
+    double h9 = h6 * h3;
+    poly6_coeff = 315.0 / (64.0 * kPi * h9);       // kernels.rs:31
+    spiky_grad_coeff = (-45.0) / (kPi * h6);       // kernels.rs:32
+    visc_lap_coeff = 45.0 / (kPi * h6);            // kernels.rs:33
+  }
+  double poly6(double r) const {  // kernels.rs:39-45
+    if (r >= h) return 0.0;
+    double diff = h2 - r * r;
+    return poly6_coeff * diff * diff * diff;
+  }
+  double spiky_grad_mag(double r) const {  // kernels.rs:50-56
+    if (r >= h || r <= 0.0) return 0.0;
+    double diff = h - r;
+    return spiky_grad_coeff * diff * diff;
+  }
+  double visc_lap(double r) const {  // kernels.rs:60-65
+    if (r >= h) return 0.0;
+    return visc_lap_coeff * (h - r);
+  }
+};
+
+// num-traits `ToPrimitive::to_i64` for f64: Some only inside (-2^63, 2^63).
+inline int64_t to_i64_or_zero(double v) {
+  if (v > -9223372036854775808.0 && v < 9223372036854775808.0) return (int64_t)v;
+  return 0;
+}
+
+struct Key {
+  int64_t i, j, k;
+  bool operator==(const Key& o) const { return i == o.i && j == o.j && k == o.k; }
+};
+struct KeyHash {
+  size_t operator()(const Key& a) const {
+    uint64_t h = (uint64_t)a.i * 0x9E3779B97F4A7C15ull;
+    h ^= (uint64_t)a.j * 0xC2B2AE3D27D4EB4Full + (h << 6) + (h >> 2);
+    h ^= (uint64_t)a.k * 0x165667B19E3779F9ull + (h << 6) + (h >> 2);
+    return (size_t)h;
+  }
+};
+
+// Grid<T> (crates/phy-fluid/src/sph/grid.rs:10-56).
+struct Grid {
+  double cell;
+  std::unordered_map<Key, std::vector<uint32_t>, KeyHash> map;
+  explicit Grid(double c) : cell(c) {}
+  Key key_of(V3 p) const {  // grid.rs:25-33
+    double inv = 1.0 / cell;
+    return {to_i64_or_zero(std::floor(p.x * inv)), to_i64_or_zero(std::floor(p.y * inv)),
+            to_i64_or_zero(std::floor(p.z * inv))};
+  }
+  void build(const std::vector<Particle>& ps) {  // grid.rs:35-40
+    map.clear();
+    for (size_t i = 0; i < ps.size(); ++i) map[key_of(ps[i].pos)].push_back((uint32_t)i);
+  }
+  template <class F>
+  void for_each_neighbor(V3 p, F&& f) const {  // grid.rs:43-56
+    Key c = key_of(p);
+    for (int64_t di = -1; di <= 1; ++di)
+      for (int64_t dj = -1; dj <= 1; ++dj)
+        for (int64_t dk = -1; dk <= 1; ++dk) {
+          auto it = map.find(Key{c.i + di, c.j + dj, c.k + dk});
+          if (it == map.end()) continue;
+          for (uint32_t id : it->second) f((size_t)id);
+        }
+  }
+};
+
+// Per-pass counters used by the roofline accounting (candidates visited and
+// pairs inside the support radius).
+struct Counters {
+  uint64_t candidates = 0, pairs = 0;
+};
+
+// FluidWorld<f64> (crates/phy-fluid/src/sph/world.rs:21-397).
+struct World {
+  OrcParams params;
+  std::vector<Particle> particles;
+  Kernels kernels;
+  Grid grid;
+  int nthreads = 1;
+  Counters counters;
+
+  explicit World(const OrcParams& p) : params(p), kernels(p.h), grid(p.h) {}  // world.rs:94-102
+
+  // world.rs:148-169
+  double lattice_mass(double s) const {
+    double h = params.h;
+    double hs = h / s;
+    int n_shell = (int)std::ceil(hs) + 1;
+    double sum_w = 0.0;
+    for (int i = -n_shell; i <= n_shell; ++i)
+      for (int j = -n_shell; j <= n_shell; ++j)
+        for (int l = -n_shell; l <= n_shell; ++l) {
+          double rr = std::sqrt((double)(i * i + j * j + l * l));
+          double r = s * rr;
+          if (r < h) sum_w = sum_w + kernels.poly6(r);
+        }
+    if (sum_w > 0.0) return params.rest_density / sum_w;
+    return params.mass;
+  }
+
+  // world.rs:124-144 (float-accumulated loops, z innermost).
+  void fill_box(V3 mn, V3 mx, double spacing, double margin) {
+    V3 lo = mn + V3{margin, margin, margin};
+    V3 hi = mx - V3{margin, margin, margin};
+    double d = spacing;
+    double mass = lattice_mass(d);
+    double x = lo.x;
+    while (x <= hi.x) {
+      double y = lo.y;
+      while (y <= hi.y) {
+        double z = lo.z;
+        while (z <= hi.z) {
+          Particle pt;
+          pt.pos = {x, y, z};
+          pt.mass = mass;
+          particles.push_back(pt);
+          z = z + d;
+        }
+        y = y + d;
+      }
+      x = x + d;
+    }
+  }
+
+  void step(double dt) {  // world.rs:183-192
+    if (particles.empty()) return;
+    grid.build(particles);
+    compute_density_pressure();
+    compute_forces();
+    integrate(dt);
+    enforce_bounds();
+  }
+
+  void compute_density_pressure() {  // world.rs:204-246
+    const double h = params.h;
+    const size_t n = particles.size();
+    const double rest = params.rest_density, stiff = params.stiffness;
+    std::vector<V3> pos(n);
+    std::vector<double> mass(n);
+    for (size_t i = 0; i < n; ++i) {
+      pos[i] = particles[i].pos;
+      mass[i] = particles[i].mass;
+    }
+    std::vector<double> rho_out(n), p_out(n);
+    uint64_t cand = 0, pairs = 0;
+#pragma omp parallel for schedule(static) num_threads(nthreads) reduction(+ : cand, pairs)
+    for (long long ii = 0; ii < (long long)n; ++ii) {
+      size_t i = (size_t)ii;
+      V3 p_i = pos[i];
+      double rho = 0.0;
+      grid.for_each_neighbor(p_i, [&](size_t j) {
+        double r = norm(p_i - pos[j]);  // na_distance, world.rs:777-779
+        ++cand;
+        if (r < h) {
+          rho = rho + mass[j] * kernels.poly6(r);
+          ++pairs;
+        }
+      });
+      double over = rho - rest;
+      double p = over > 0.0 ? stiff * over : 0.0;
+      rho_out[i] = rho;
+      p_out[i] = p;
+    }
+    for (size_t i = 0; i < n; ++i) {
+      particles[i].rho = rho_out[i];
+      particles[i].p = p_out[i];
+    }
+    counters.candidates += cand;
+    counters.pairs += pairs;
+  }
+
+  void compute_forces() {  // world.rs:252-347
+    const size_t n = particles.size();
+    const double h = params.h;
+    const double r_eps = 1e-4;
+    const double shear_min = params.shear_min;
+    std::vector<V3> pos(n), vel(n);
+    std::vector<double> rho(n), pr(n), mass(n);
+    std::vector<uint64_t> mat(n);
+    for (size_t i = 0; i < n; ++i) {
+      pos[i] = particles[i].pos;
+      vel[i] = particles[i].vel;
+      rho[i] = particles[i].rho;
+      pr[i] = particles[i].p;
+      mass[i] = particles[i].mass;
+      mat[i] = particles[i].material;
+    }
+    std::vector<V3> acc_out(n), xsph_out(n);
+    std::vector<double> mu_out(n);
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (long long ii = 0; ii < (long long)n; ++ii) {
+      size_t i = (size_t)ii;
+      V3 p_i = pos[i], v_i = vel[i];
+      double rho_i = rho[i], p_i_p = pr[i], m_i = mass[i];
+      V3 f_press{0, 0, 0}, f_visc_raw{0, 0, 0}, xsph{0, 0, 0};
+      double shear = 0.0;
+      grid.for_each_neighbor(p_i, [&](size_t j) {
+        if (j == i) return;
+        V3 d = pos[j] - p_i;
+        double r = norm(d);
+        if (r >= h || r <= 0.0) return;
+        double rho_j = rho[j];
+        double p_j = pr[j];
+        double grad = kernels.spiky_grad_mag(r);
+        V3 dir = d / r;
+        double coef = m_i * mass[j] * (p_i_p / (rho_i * rho_i) + p_j / (rho_j * rho_j));
+        f_press += dir * (coef * grad);
+        double lap = kernels.visc_lap(r);
+        f_visc_raw += (vel[j] - v_i) * (m_i * mass[j] / rho_j * lap);
+        double w = kernels.poly6(r);
+        xsph += (vel[j] - v_i) * (mass[j] / rho_j * w);
+        double dv = norm(vel[j] - v_i);
+        shear = shear + dv / (r + r_eps) * (mass[j] / rho_j);
+      });
+      // world.rs:319-327; visc_k/visc_n are indexed like Rust slices.
+      uint64_t m_idx = mat[i] < params.n_visc_k ? mat[i] : 0;
+      double kc = params.visc_k[m_idx];
+      double nn = params.visc_n[m_idx];
+      double sreg = shear > shear_min ? shear : shear_min;
+      double mu_eff = kc * std::pow(sreg, nn - 1.0);
+      V3 f_visc = f_visc_raw * mu_eff;
+      V3 acc = rho_i > 0.0 ? (f_press + f_visc) / rho_i : V3{0, 0, 0};
+      acc_out[i] = acc;
+      mu_out[i] = mu_eff;
+      xsph_out[i] = xsph;
+    }
+    for (size_t i = 0; i < n; ++i) {
+      particles[i].acc = acc_out[i];
+      particles[i].mu_eff = mu_out[i];
+      particles[i].xsph = xsph_out[i];
+    }
+  }
+
+  void integrate(double dt) {  // world.rs:352-363
+    V3 g{params.gravity[0], params.gravity[1], params.gravity[2]};
+    double eps = params.xsph_eps;
+    for (auto& pt : particles) {
+      V3 a = pt.acc + g + pt.body_acc;
+      pt.vel += a * dt;
+      pt.vel += pt.xsph * eps;
+      pt.pos += pt.vel * dt;
+      pt.body_acc = {0, 0, 0};
+    }
+  }
+
+  void enforce_bounds() {  // world.rs:366-397
+    const double* lo = params.bounds_min;
+    const double* hi = params.bounds_max;
+    double damp = params.boundary_damp;
+    for (auto& pt : particles) {
+      double p[3] = {pt.pos.x, pt.pos.y, pt.pos.z};
+      double v[3] = {pt.vel.x, pt.vel.y, pt.vel.z};
+      for (int a = 0; a < 3; ++a) {
+        if (p[a] < lo[a]) {
+          p[a] = lo[a];
+          v[a] = -v[a] * damp;
+        } else if (p[a] > hi[a]) {
+          p[a] = hi[a];
+          v[a] = -v[a] * damp;
+        }
+      }
+      pt.pos = {p[0], p[1], p[2]};
+      pt.vel = {v[0], v[1], v[2]};
+    }
+  }
+};
+
+enum Field : int {
+  F_POS = 0, F_VEL = 1, F_ACC = 2, F_BODY_ACC = 3, F_RHO = 4, F_P = 5,
+  F_MASS = 6, F_MU_EFF = 7, F_XSPH = 8, F_MATERIAL = 9
+};
+
+V3* vec_field(Particle& p, int f) {
+  switch (f) {
+    case F_POS: return &p.pos;
+    case F_VEL: return &p.vel;
+    case F_ACC: return &p.acc;
+    case F_BODY_ACC: return &p.body_acc;
+    case F_XSPH: return &p.xsph;
+    default: return nullptr;
+  }
+}
+double* scalar_field(Particle& p, int f) {
+  switch (f) {
+    case F_RHO: return &p.rho;
+    case F_P: return &p.p;
+    case F_MASS: return &p.mass;
+    case F_MU_EFF: return &p.mu_eff;
+    default: return nullptr;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void* orc_new(const OrcParams* p) { return new World(*p); }
+void orc_free(void* w) { delete static_cast<World*>(w); }
+uint64_t orc_len(void* w) { return static_cast<World*>(w)->particles.size(); }
+void orc_set_threads(void* w, int n) { static_cast<World*>(w)->nthreads = n < 1 ? 1 : n; }
+int orc_max_threads() {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+// Live parameter update: kernels and grid keep the h captured at construction
+// (world.rs:94-102), exactly like mutating `FluidWorld::params` in Rust.
+void orc_set_params(void* w, const OrcParams* p) { static_cast<World*>(w)->params = *p; }
+void orc_get_params(void* w, OrcParams* p) { *p = static_cast<World*>(w)->params; }
+
+void orc_fill_box(void* w, const double* mn, const double* mx, double spacing, double margin) {
+  static_cast<World*>(w)->fill_box({mn[0], mn[1], mn[2]}, {mx[0], mx[1], mx[2]}, spacing, margin);
+}
+double orc_lattice_mass(void* w, double s) { return static_cast<World*>(w)->lattice_mass(s); }
+
+// Appends n particles built like Particle::with_material (particle.rs:50-71);
+// vel may be null (zero velocity).
+void orc_add(void* w, uint64_t n, const double* pos, const double* vel, const double* mass,
+             const uint64_t* material) {
+  World* W = static_cast<World*>(w);
+  for (uint64_t i = 0; i < n; ++i) {
+    Particle pt;
+    pt.pos = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    if (vel) pt.vel = {vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]};
+    pt.mass = mass[i];
+    pt.material = material ? material[i] : 0;
+    W->particles.push_back(pt);
+  }
+}
+
+// Field access in insertion order: vector fields are xyz-interleaved.
+int orc_get(void* w, int field, double* out) {
+  World* W = static_cast<World*>(w);
+  size_t n = W->particles.size();
+  for (size_t i = 0; i < n; ++i) {
+    Particle& p = W->particles[i];
+    if (field == F_MATERIAL) {
+      out[i] = (double)p.material;
+    } else if (V3* v = vec_field(p, field)) {
+      out[3 * i] = v->x;
+      out[3 * i + 1] = v->y;
+      out[3 * i + 2] = v->z;
+    } else if (double* s = scalar_field(p, field)) {
+      out[i] = *s;
+    } else {
+      return -1;
+    }
+  }
+  return 0;
+}
+int orc_set(void* w, int field, const double* in) {
+  World* W = static_cast<World*>(w);
+  size_t n = W->particles.size();
+  for (size_t i = 0; i < n; ++i) {
+    Particle& p = W->particles[i];
+    if (field == F_MATERIAL) {
+      p.material = (uint64_t)in[i];
+    } else if (V3* v = vec_field(p, field)) {
+      *v = {in[3 * i], in[3 * i + 1], in[3 * i + 2]};
+    } else if (double* s = scalar_field(p, field)) {
+      *s = in[i];
+    } else {
+      return -1;
+    }
+  }
+  return 0;
+}
+
+void orc_step(void* w, double dt) { static_cast<World*>(w)->step(dt); }
+void orc_step_n(void* w, double dt, int n) {
+  for (int i = 0; i < n; ++i) static_cast<World*>(w)->step(dt);
+}
+
+// Grid::key_of for every particle (int64 xyz-interleaved), used to pin the
+// device cell keys bit-exactly.
+void orc_cell_keys(void* w, int64_t* out) {
+  World* W = static_cast<World*>(w);
+  for (size_t i = 0; i < W->particles.size(); ++i) {
+    Key k = W->grid.key_of(W->particles[i].pos);
+    out[3 * i] = k.i;
+    out[3 * i + 1] = k.j;
+    out[3 * i + 2] = k.k;
+  }
+}
+
+// Neighbour list of particle i in the reference's visit order
+// (for_each_neighbor over a grid built from the current positions).
+// Returns the number of candidates; writes up to cap indices.
+uint64_t orc_neighbors(void* w, uint64_t i, uint64_t* out, uint64_t cap) {
+  World* W = static_cast<World*>(w);
+  W->grid.build(W->particles);
+  uint64_t cnt = 0;
+  W->grid.for_each_neighbor(W->particles[i].pos, [&](size_t j) {
+    if (cnt < cap) out[cnt] = j;
+    ++cnt;
+  });
+  return cnt;
+}
+
+// Diagnostics of FluidSubsystem (subsystem.rs:149-163): momentum xyz, KE.
+void orc_diagnostics(void* w, double* out4) {
+  World* W = static_cast<World*>(w);
+  V3 p{0, 0, 0};
+  for (auto& pt : W->particles) p += pt.vel * pt.mass;
+  double e = 0.0;
+  for (auto& pt : W->particles) e = e + (norm_squared(pt.vel) * pt.mass) / (1.0 + 1.0);
+  out4[0] = p.x;
+  out4[1] = p.y;
+  out4[2] = p.z;
+  out4[3] = e;
+}
+
+// Candidates visited and in-range pairs counted by the density passes since
+// the last reset (roofline accounting).
+void orc_counters(void* w, uint64_t* out2, int reset) {
+  World* W = static_cast<World*>(w);
+  out2[0] = W->counters.candidates;
+  out2[1] = W->counters.pairs;
+  if (reset) W->counters = Counters{};
+}
+
+}  // extern "C"

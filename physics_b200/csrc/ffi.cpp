@@ -1,0 +1,386 @@
+// extern "C" boundary of libphysph.so: the reference's phy-ffi symbols
+// (crates/phy-ffi/src/lib.rs) and the phy_fluid_* additions of ABI 3.
+//
+// Every entry catches all C++ exceptions (the counterpart of the reference's
+// catch_unwind guard, lib.rs:71-75) and maps them to its failure value, with
+// the message kept for phy_fluid_last_error().
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "../../include/phy_ffi.h"
+#include "../../include/phy_fluid.h"
+#include "checkpoint.h"
+#include "fluid_world.h"
+
+using phy::FluidSubsystem;
+using phy::FluidWorld;
+using phy::Precision;
+using phy::SphParams;
+using phy::World;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class R, class F>
+R guard(R fail, F&& f) {
+  try {
+    g_last_error.clear();
+    return f();
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+  } catch (...) {
+    g_last_error = "unknown error";
+  }
+  return fail;
+}
+
+World* as_world(PhyWorldHandle* w) { return reinterpret_cast<World*>(w); }
+PhyWorldHandle* box_world(World* w) { return reinterpret_cast<PhyWorldHandle*>(w); }
+
+FluidSubsystem& sub_of(PhyWorldHandle* w, uint32_t sub) {
+  World* W = as_world(w);
+  if (!W) throw std::invalid_argument("null world handle");
+  if (sub >= W->subs.size()) throw std::invalid_argument("fluid subsystem index out of range");
+  return *W->subs[sub];
+}
+
+Precision precision_of(int32_t p) {
+  if (p == PHY_PRECISION_F64_PLAIN) return Precision::F64Plain;
+  if (p == PHY_PRECISION_F32_COMP) return Precision::F32Comp;
+  throw std::invalid_argument("unknown precision form");
+}
+
+// build_fluid_world (phy-ffi/src/lib.rs:113-126).
+World* build_fluid_world() {
+  auto* W = new World();
+  try {
+    auto fw = std::make_unique<FluidWorld>(SphParams::defaults(), Precision::F64Plain);
+    fw->fill_box({-4.0, -4.0, -1.0}, {0.0, 4.0, 1.0}, 0.18, 0.05);
+    W->subs.push_back(std::make_unique<FluidSubsystem>(std::move(fw)));
+  } catch (...) {
+    delete W;
+    throw;
+  }
+  return W;
+}
+
+// Interleaved xyz readback over every fluid subsystem, truncating at len/3
+// particles (phy-ffi/src/lib.rs:399-460).
+template <class T>
+uintptr_t read_vec(PhyWorldHandle* w, T* buf, uintptr_t len, int field) {
+  World* W = as_world(w);
+  if (!W || !buf) return 0;
+  uintptr_t written = 0;  // particles
+  std::vector<double> tmp;
+  for (auto& s : W->subs) {
+    size_t n = s->world->len();
+    if (n == 0) continue;
+    uintptr_t room = len / 3 - written;
+    if (room == 0) break;
+    size_t take = n < room ? n : (size_t)room;
+    tmp.resize(3 * n);
+    s->world->get_field(field, tmp.data());
+    for (size_t i = 0; i < 3 * take; ++i) buf[3 * written + i] = (T)tmp[i];
+    written += take;
+    if (take < n) break;
+  }
+  return written;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t phy_ffi_abi_version(void) { return PHY_FFI_ABI_VERSION; }
+
+PhyWorldHandle* phy_world_create_fluid(void) {
+  return guard<PhyWorldHandle*>(nullptr, [] { return box_world(build_fluid_world()); });
+}
+
+static PhyWorldHandle* not_in_build(const char* what) {
+  g_last_error = std::string(what) + ": this build holds fluid subsystems only";
+  return nullptr;
+}
+PhyWorldHandle* phy_world_create_rigid(void) { return not_in_build("rigid world"); }
+PhyWorldHandle* phy_world_create_rigid_empty(void) { return not_in_build("rigid world"); }
+PhyWorldHandle* phy_world_create_granular(void) { return not_in_build("granular world"); }
+PhyWorldHandle* phy_world_create_coupled(void) { return not_in_build("coupled fluid+rigid world"); }
+PhyWorldHandle* phy_world_create_soft_empty(void) { return not_in_build("soft world"); }
+PhyWorldHandle* phy_world_create_field_empty(void) { return not_in_build("field world"); }
+PhyWorldHandle* phy_world_create_optics_empty(void) { return not_in_build("optics world"); }
+PhyWorldHandle* phy_world_create_solid_empty(void) { return not_in_build("solid world"); }
+
+int32_t phy_world_step(PhyWorldHandle* w, double dt) {
+  World* W = as_world(w);
+  if (!W) return -1;
+  return guard<int32_t>(-1, [&] {
+    W->step(dt);
+    return 0;
+  });
+}
+
+int32_t phy_world_step_checked(PhyWorldHandle* w, double dt) {
+  World* W = as_world(w);
+  if (!W) return -1;
+  return guard<int32_t>(-1, [&] { return (int32_t)W->step_checked(dt); });
+}
+
+double phy_world_time(PhyWorldHandle* w) {
+  World* W = as_world(w);
+  return W ? W->t : std::numeric_limits<double>::quiet_NaN();
+}
+
+uintptr_t phy_world_sub_count(PhyWorldHandle* w) {
+  World* W = as_world(w);
+  return W ? (uintptr_t)W->subs.size() : 0;
+}
+
+uintptr_t phy_world_fluid_count(PhyWorldHandle* w) {
+  World* W = as_world(w);
+  return W ? (uintptr_t)W->fluid_count() : 0;
+}
+
+uintptr_t phy_world_get_fluid_positions(PhyWorldHandle* w, double* buf, uintptr_t len) {
+  return guard<uintptr_t>(0, [&] { return read_vec<double>(w, buf, len, PHY_FIELD_POS); });
+}
+uintptr_t phy_world_get_fluid_velocities(PhyWorldHandle* w, double* buf, uintptr_t len) {
+  return guard<uintptr_t>(0, [&] { return read_vec<double>(w, buf, len, PHY_FIELD_VEL); });
+}
+uintptr_t phy_world_get_fluid_positions_f32(PhyWorldHandle* w, float* buf, uintptr_t len) {
+  return guard<uintptr_t>(0, [&] { return read_vec<float>(w, buf, len, PHY_FIELD_POS); });
+}
+uintptr_t phy_world_get_fluid_velocities_f32(PhyWorldHandle* w, float* buf, uintptr_t len) {
+  return guard<uintptr_t>(0, [&] { return read_vec<float>(w, buf, len, PHY_FIELD_VEL); });
+}
+
+uintptr_t phy_world_rigid_count(PhyWorldHandle*) { return 0; }
+uintptr_t phy_world_get_rigid_transforms(PhyWorldHandle*, double*, uintptr_t) { return 0; }
+uintptr_t phy_world_get_rigid_transforms_f32(PhyWorldHandle*, float*, uintptr_t) { return 0; }
+
+int32_t phy_world_step_f32(PhyWorldHandle* w, float dt) { return phy_world_step(w, (double)dt); }
+
+int32_t phy_world_save(PhyWorldHandle* w, const char* path) {
+  World* W = as_world(w);
+  if (!W || !path) return -1;
+  return guard<int32_t>(-1, [&] {
+    phy::save_world(*W, path);
+    return 0;
+  });
+}
+
+PhyWorldHandle* phy_world_load(const char* path) {
+  if (!path) return nullptr;
+  return guard<PhyWorldHandle*>(nullptr, [&] { return box_world(phy::load_world(path).release()); });
+}
+
+void phy_world_destroy(PhyWorldHandle* w) {
+  World* W = as_world(w);
+  if (!W) return;
+  guard<int>(0, [&] {
+    delete W;
+    return 0;
+  });
+}
+
+int64_t phy_world_rigid_add_body(PhyWorldHandle*, int32_t, double, const double*, const double*) {
+  g_last_error = "rigid bodies: this build holds fluid subsystems only";
+  return -1;
+}
+int32_t phy_world_rigid_apply_force(PhyWorldHandle*, int64_t, const double*, double, int32_t) { return -1; }
+int32_t phy_world_rigid_apply_torque(PhyWorldHandle*, int64_t, const double*, double, int32_t) { return -1; }
+int32_t phy_world_rigid_get_velocity(PhyWorldHandle*, int64_t, double*) { return -1; }
+int32_t phy_world_rigid_get_angular_velocity(PhyWorldHandle*, int64_t, double*) { return -1; }
+
+// ---- phy_fluid_* -------------------------------------------------------------
+
+void phy_sph_params_defaults(PhySphParams* out) {
+  if (out) *out = SphParams::defaults().to_c();
+}
+
+PhyWorldHandle* phy_fluid_world_create(const PhySphParams* params, int32_t precision) {
+  if (!params) return nullptr;
+  return guard<PhyWorldHandle*>(nullptr, [&] {
+    auto fw = std::make_unique<FluidWorld>(SphParams::from_c(*params), precision_of(precision));
+    auto* W = new World();
+    W->subs.push_back(std::make_unique<FluidSubsystem>(std::move(fw)));
+    return box_world(W);
+  });
+}
+
+int32_t phy_fluid_add_subsystem(PhyWorldHandle* w, const PhySphParams* params, int32_t precision) {
+  World* W = as_world(w);
+  if (!W || !params) return -1;
+  return guard<int32_t>(-1, [&] {
+    auto fw = std::make_unique<FluidWorld>(SphParams::from_c(*params), precision_of(precision));
+    W->subs.push_back(std::make_unique<FluidSubsystem>(std::move(fw)));
+    return (int32_t)(W->subs.size() - 1);
+  });
+}
+
+int32_t phy_fluid_fill_box(PhyWorldHandle* w, uint32_t sub, const double* mn, const double* mx, double spacing,
+                           double margin) {
+  if (!mn || !mx) return -1;
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->fill_box({mn[0], mn[1], mn[2]}, {mx[0], mx[1], mx[2]}, spacing, margin);
+    return 0;
+  });
+}
+
+double phy_fluid_lattice_mass(PhyWorldHandle* w, uint32_t sub, double spacing) {
+  return guard<double>(std::numeric_limits<double>::quiet_NaN(),
+                       [&] { return sub_of(w, sub).world->lattice_mass(spacing); });
+}
+
+int32_t phy_fluid_add_particles(PhyWorldHandle* w, uint32_t sub, uint64_t n, const double* pos, const double* vel,
+                                const double* mass, const uint32_t* material) {
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->add_particles((size_t)n, pos, vel, mass, material);
+    return 0;
+  });
+}
+
+int64_t phy_fluid_len(PhyWorldHandle* w, uint32_t sub) {
+  return guard<int64_t>(-1, [&] { return (int64_t)sub_of(w, sub).world->len(); });
+}
+
+int32_t phy_fluid_get_field(PhyWorldHandle* w, uint32_t sub, int32_t field, double* out, uint64_t len) {
+  if (!out) return -1;
+  return guard<int32_t>(-1, [&] {
+    FluidWorld& fw = *sub_of(w, sub).world;
+    int nc = FluidWorld::components(field);
+    if (nc == 0) throw std::invalid_argument("unknown field");
+    if (len < (uint64_t)nc * fw.len()) throw std::invalid_argument("output buffer too small");
+    fw.get_field(field, out);
+    return 0;
+  });
+}
+
+int32_t phy_fluid_set_field(PhyWorldHandle* w, uint32_t sub, int32_t field, const double* in, uint64_t len) {
+  if (!in) return -1;
+  return guard<int32_t>(-1, [&] {
+    FluidWorld& fw = *sub_of(w, sub).world;
+    int nc = FluidWorld::components(field);
+    if (nc == 0) throw std::invalid_argument("unknown field");
+    if (len < (uint64_t)nc * fw.len()) throw std::invalid_argument("input buffer too small");
+    fw.set_field(field, in);
+    return 0;
+  });
+}
+
+int32_t phy_fluid_get_params(PhyWorldHandle* w, uint32_t sub, PhySphParams* out) {
+  if (!out) return -1;
+  return guard<int32_t>(-1, [&] {
+    *out = sub_of(w, sub).world->params.to_c();
+    return 0;
+  });
+}
+
+int32_t phy_fluid_set_params(PhyWorldHandle* w, uint32_t sub, const PhySphParams* in) {
+  if (!in) return -1;
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->params = SphParams::from_c(*in);
+    return 0;
+  });
+}
+
+int32_t phy_fluid_step(PhyWorldHandle* w, uint32_t sub, double dt, uint32_t n) {
+  return guard<int32_t>(-1, [&] {
+    FluidWorld& fw = *sub_of(w, sub).world;
+    for (uint32_t k = 0; k < n; ++k) fw.step(dt);
+    return 0;
+  });
+}
+
+int32_t phy_fluid_diagnostics(PhyWorldHandle* w, uint32_t sub, double* out4) {
+  if (!out4) return -1;
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->diagnostics(out4);
+    return 0;
+  });
+}
+
+int32_t phy_fluid_get_coupling(PhyWorldHandle* w, uint32_t sub, double* out5) {
+  if (!out5) return -1;
+  return guard<int32_t>(-1, [&] {
+    FluidSubsystem& s = sub_of(w, sub);
+    out5[0] = s.thermal_expansion;
+    out5[1] = s.heat_gain;
+    out5[2] = s.t_ref;
+    out5[3] = s.drag;
+    out5[4] = s.friction;
+    return 0;
+  });
+}
+
+int32_t phy_fluid_set_coupling(PhyWorldHandle* w, uint32_t sub, const double* in5) {
+  if (!in5) return -1;
+  return guard<int32_t>(-1, [&] {
+    FluidSubsystem& s = sub_of(w, sub);
+    s.thermal_expansion = in5[0];
+    s.heat_gain = in5[1];
+    s.t_ref = in5[2];
+    s.drag = in5[3];
+    s.friction = in5[4];
+    return 0;
+  });
+}
+
+int32_t phy_fluid_set_stream(PhyWorldHandle* w, void* cuda_stream) {
+  World* W = as_world(w);
+  if (!W) return -1;
+  return guard<int32_t>(-1, [&] {
+    for (auto& s : W->subs) s->world->set_stream((cudaStream_t)cuda_stream);
+    return 0;
+  });
+}
+
+int32_t phy_fluid_synchronize(PhyWorldHandle* w) {
+  World* W = as_world(w);
+  if (!W) return -1;
+  return guard<int32_t>(-1, [&] {
+    for (auto& s : W->subs) s->world->synchronize();
+    return 0;
+  });
+}
+
+int32_t phy_fluid_step_counters(PhyWorldHandle* w, uint32_t sub, uint64_t* out4) {
+  if (!out4) return -1;
+  return guard<int32_t>(-1, [&] {
+    FluidWorld& fw = *sub_of(w, sub).world;
+    fw.last_step_counters(out4);
+    out4[2] = fw.len();
+    out4[3] = (uint64_t)fw.grid_cells();
+    return 0;
+  });
+}
+
+int32_t phy_fluid_set_counting(PhyWorldHandle* w, uint32_t sub, int32_t on) {
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->set_counting(on != 0);
+    return 0;
+  });
+}
+
+int32_t phy_fluid_set_timing(PhyWorldHandle* w, uint32_t sub, int32_t on) {
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->set_timing(on != 0);
+    return 0;
+  });
+}
+
+int32_t phy_fluid_phase_times(PhyWorldHandle* w, uint32_t sub, double* out5, int32_t reset) {
+  if (!out5) return -1;
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->phase_times(out5, reset != 0);
+    return 0;
+  });
+}
+
+const char* phy_fluid_last_error(void) { return g_last_error.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,818 @@
+// Host-side FluidWorld / FluidSubsystem / World of the B200 build.
+#include "fluid_world.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <climits>
+#include <limits>
+
+namespace phy {
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;  // std::f64::consts::PI
+constexpr long long kMaxCells = 1ll << 27;       // grid box cap (512 MiB of cell starts)
+constexpr int kThreads = 256;
+
+int grid_for(size_t n) { return (int)std::max<size_t>(1, (n + kThreads - 1) / kThreads); }
+
+__global__ void k_set_scalar_by_id(int n, const uint32_t* __restrict__ id, const double* __restrict__ src,
+                                   double* __restrict__ dst) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) dst[s] = src[id[s]];
+}
+__global__ void k_set_u32_by_id(int n, const uint32_t* __restrict__ id, const double* __restrict__ src,
+                                uint32_t* __restrict__ dst) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) {
+    double v = src[id[s]];
+    dst[s] = v >= 4294967295.0 ? 0xffffffffu : (v > 0.0 ? (uint32_t)v : 0u);
+  }
+}
+__global__ void k_set_vec_by_id(int n, const uint32_t* __restrict__ id, const double* __restrict__ src,
+                                double* __restrict__ x, double* __restrict__ y, double* __restrict__ z) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) {
+    size_t o = 3 * (size_t)id[s];
+    x[s] = src[o];
+    y[s] = src[o + 1];
+    z[s] = src[o + 2];
+  }
+}
+__global__ void k_get_scalar_by_id(int n, const uint32_t* __restrict__ id, const double* __restrict__ src,
+                                   double* __restrict__ dst) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) dst[id[s]] = src[s];
+}
+__global__ void k_get_vec_by_id(int n, const uint32_t* __restrict__ id, const double* __restrict__ x,
+                                const double* __restrict__ y, const double* __restrict__ z,
+                                double* __restrict__ dst) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) {
+    size_t o = 3 * (size_t)id[s];
+    dst[o] = x[s];
+    dst[o + 1] = y[s];
+    dst[o + 2] = z[s];
+  }
+}
+// Appends m particles (insertion-order staging: pos 3m, vel 3m, mass m,
+// material m) at slots [n0, n0+m).
+__global__ void k_append(int n0, int m, const double* __restrict__ st, double* px, double* py, double* pz,
+                         double* vx, double* vy, double* vz, double* mass, uint32_t* mat, uint32_t* id) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  const double* pos = st;
+  const double* vel = st + 3 * (size_t)m;
+  const double* ms = st + 6 * (size_t)m;
+  const double* mt = st + 7 * (size_t)m;
+  int s = n0 + k;
+  px[s] = pos[3 * (size_t)k];
+  py[s] = pos[3 * (size_t)k + 1];
+  pz[s] = pos[3 * (size_t)k + 2];
+  vx[s] = vel[3 * (size_t)k];
+  vy[s] = vel[3 * (size_t)k + 1];
+  vz[s] = vel[3 * (size_t)k + 2];
+  mass[s] = ms[k];
+  double v = mt[k];
+  mat[s] = v >= 4294967295.0 ? 0xffffffffu : (v > 0.0 ? (uint32_t)v : 0u);
+  id[s] = (uint32_t)s;
+}
+
+// Cell-key bounding box of n interleaved positions: out[0..2] min, out[3..5]
+// max over finite coordinates, out[6] = 1 when a coordinate is not finite.
+// out must be preset to (LLONG_MAX x3, LLONG_MIN x3, 0).
+__global__ void k_key_bbox(int n, const double* __restrict__ pos3, double inv, long long* out) {
+  long long mn[3] = {LLONG_MAX, LLONG_MAX, LLONG_MAX}, mx[3] = {LLONG_MIN, LLONG_MIN, LLONG_MIN};
+  int bad = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      double x = pos3[3 * (size_t)i + a];
+      if (!isfinite(x)) {
+        bad = 1;
+        continue;
+      }
+      long long k = key_axis(x, inv);
+      mn[a] = k < mn[a] ? k : mn[a];
+      mx[a] = k > mx[a] ? k : mx[a];
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    for (int o = 16; o > 0; o >>= 1) {
+      long long y = __shfl_xor_sync(0xffffffffu, mn[a], o);
+      long long z = __shfl_xor_sync(0xffffffffu, mx[a], o);
+      mn[a] = y < mn[a] ? y : mn[a];
+      mx[a] = z > mx[a] ? z : mx[a];
+    }
+  }
+  bad = __any_sync(0xffffffffu, bad);
+  if ((threadIdx.x & 31) == 0) {
+    for (int a = 0; a < 3; ++a) {
+      if (mn[a] != LLONG_MAX) atomicMin(&out[a], mn[a]);
+      if (mx[a] != LLONG_MIN) atomicMax(&out[3 + a], mx[a]);
+    }
+    if (bad) atomicMax(&out[6], 1ll);
+  }
+}
+
+// num-traits ToPrimitive::to_i64 on f64 with None -> 0 (grid.rs:25-33).
+long long key_axis_host(double x, double inv) {
+  double f = std::floor(x * inv);
+  if (f > -9223372036854775808.0 && f < 9223372036854775808.0) return (long long)f;
+  return 0;
+}
+
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+template <class T>
+void dalloc(T*& p, size_t count) {
+  dfree(p);
+  if (count == 0) count = 1;
+  cuda_check(cudaMalloc((void**)&p, count * sizeof(T)), "cudaMalloc");
+}
+
+// Grows a device array to `cap` elements, keeping the first `keep`.
+template <class T>
+void dgrow(T*& p, size_t keep, size_t cap, cudaStream_t s) {
+  T* q = nullptr;
+  cuda_check(cudaMalloc((void**)&q, std::max<size_t>(cap, 1) * sizeof(T)), "cudaMalloc");
+  if (p && keep) cuda_check(cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, s), "grow copy");
+  if (p) {
+    cuda_check(cudaStreamSynchronize(s), "grow sync");
+    cudaFree(p);
+  }
+  p = q;
+}
+
+}  // namespace
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---- SphParams -------------------------------------------------------------
+
+SphParams SphParams::defaults() {
+  SphParams p;
+  p.rest_density = 1000.0;
+  p.stiffness = 250.0;
+  p.viscosity = 3.5;
+  p.visc_k = {3.5};
+  p.visc_n = {1.0};
+  p.shear_min = 0.01;
+  p.mass = 0.02;
+  p.h = 0.2;
+  p.gravity = {0.0, -9.81, 0.0};
+  p.bounds_min = {-5.0, -5.0, -5.0};
+  p.bounds_max = {5.0, 5.0, 5.0};
+  p.boundary_damp = 0.4;
+  p.xsph_eps = 0.5;
+  return p;
+}
+
+PhySphParams SphParams::to_c() const {
+  PhySphParams c;
+  std::memset(&c, 0, sizeof(c));
+  c.rest_density = rest_density;
+  c.stiffness = stiffness;
+  c.viscosity = viscosity;
+  c.shear_min = shear_min;
+  c.mass = mass;
+  c.h = h;
+  const Vec3* v[3] = {&gravity, &bounds_min, &bounds_max};
+  double* d[3] = {c.gravity, c.bounds_min, c.bounds_max};
+  for (int k = 0; k < 3; ++k) {
+    d[k][0] = v[k]->x;
+    d[k][1] = v[k]->y;
+    d[k][2] = v[k]->z;
+  }
+  c.boundary_damp = boundary_damp;
+  c.xsph_eps = xsph_eps;
+  c.n_visc_k = (uint32_t)std::min<size_t>(visc_k.size(), PHY_MAX_MATERIALS);
+  c.n_visc_n = (uint32_t)std::min<size_t>(visc_n.size(), PHY_MAX_MATERIALS);
+  for (uint32_t k = 0; k < c.n_visc_k; ++k) c.visc_k[k] = visc_k[k];
+  for (uint32_t k = 0; k < c.n_visc_n; ++k) c.visc_n[k] = visc_n[k];
+  return c;
+}
+
+SphParams SphParams::from_c(const PhySphParams& c) {
+  if (c.n_visc_k < 1 || c.n_visc_k > PHY_MAX_MATERIALS || c.n_visc_n > PHY_MAX_MATERIALS)
+    throw std::invalid_argument("SphParams: n_visc_k must be 1..16 and n_visc_n at most 16");
+  SphParams p;
+  p.rest_density = c.rest_density;
+  p.stiffness = c.stiffness;
+  p.viscosity = c.viscosity;
+  p.shear_min = c.shear_min;
+  p.mass = c.mass;
+  p.h = c.h;
+  p.gravity = {c.gravity[0], c.gravity[1], c.gravity[2]};
+  p.bounds_min = {c.bounds_min[0], c.bounds_min[1], c.bounds_min[2]};
+  p.bounds_max = {c.bounds_max[0], c.bounds_max[1], c.bounds_max[2]};
+  p.boundary_damp = c.boundary_damp;
+  p.xsph_eps = c.xsph_eps;
+  p.visc_k.assign(c.visc_k, c.visc_k + c.n_visc_k);
+  p.visc_n.assign(c.visc_n, c.visc_n + c.n_visc_n);
+  return p;
+}
+
+// ---- FluidWorld --------------------------------------------------------------
+
+FluidWorld::FluidWorld(const SphParams& p, Precision prec) : params(p), prec_(prec), h0_(p.h) {
+  cuda_check(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  stream_ = own_stream_;
+  dalloc(b_.flags, 1);
+  dalloc(b_.counters, 2);
+  cuda_check(cudaMemsetAsync(b_.flags, 0, sizeof(uint32_t), stream_), "memset");
+  cuda_check(cudaMemsetAsync(b_.counters, 0, 2 * sizeof(unsigned long long), stream_), "memset");
+}
+
+FluidWorld::~FluidWorld() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  free_all();
+  dfree(d_bbox_);
+  for (auto& e : ev_)
+    if (e) cudaEventDestroy(e);
+  if (own_stream_) cudaStreamDestroy(own_stream_);
+}
+
+void FluidWorld::free_all() {
+  for (int k = 0; k < 6; ++k) {
+    dfree(b_.pv0[k]);
+    dfree(b_.pv1[k]);
+  }
+  for (int q = 0; q < 2; ++q) {
+    dfree(b_.pc[q].mass);
+    dfree(b_.pc[q].mat);
+    dfree(b_.pc[q].id);
+    for (int k = 0; k < 3; ++k) dfree(b_.pc[q].ba[k]);
+  }
+  dfree(b_.rho);
+  dfree(b_.p);
+  dfree(b_.pr2);
+  dfree(b_.mr);
+  for (int k = 0; k < 3; ++k) {
+    dfree(b_.acc[k]);
+    dfree(b_.xsph[k]);
+  }
+  dfree(b_.mu);
+  dfree(b_.cpos);
+  dfree(b_.cvel);
+  dfree(b_.cmr);
+  dfree(b_.cell_of);
+  dfree(b_.rank);
+  dfree(b_.tmp);
+  dfree(b_.perm);
+  dfree(b_.cell_start);
+  dfree(b_.block_sums);
+  dfree(b_.stage);
+  dfree(b_.flags);
+  dfree(b_.counters);
+}
+
+void FluidWorld::set_stream(cudaStream_t s) {
+  cuda_check(cudaStreamSynchronize(stream_), "stream switch");
+  stream_ = s ? s : own_stream_;
+}
+
+void FluidWorld::synchronize() { cuda_check(cudaStreamSynchronize(stream_), "synchronize"); }
+
+// Grows every per-particle array to hold n particles (geometric growth),
+// keeping the current n_ particles.
+void FluidWorld::ensure_capacity(size_t n) {
+  if (n > 0x7fffffffull) throw std::invalid_argument("FluidWorld: more than 2^31-1 particles");
+  if ((int)n <= b_.capacity) return;
+  size_t cap = std::max<size_t>(n, (size_t)b_.capacity + b_.capacity / 2);
+  cudaStream_t s = stream_;
+  for (int k = 0; k < 6; ++k) {
+    dgrow(b_.pv0[k], 0, cap, s);
+    dgrow(b_.pv1[k], n_, cap, s);
+  }
+  // The current per-particle constants live in pc[cur]; the other set is
+  // scratch for the next sort.
+  for (int q = 0; q < 2; ++q) {
+    size_t keep = q == b_.cur ? n_ : 0;
+    dgrow(b_.pc[q].mass, keep, cap, s);
+    dgrow(b_.pc[q].mat, keep, cap, s);
+    dgrow(b_.pc[q].id, keep, cap, s);
+    if (b_.has_ba)
+      for (int k = 0; k < 3; ++k) dgrow(b_.pc[q].ba[k], keep, cap, s);
+  }
+  dgrow(b_.rho, n_, cap, s);
+  dgrow(b_.p, n_, cap, s);
+  dgrow(b_.pr2, 0, cap, s);
+  dgrow(b_.mr, 0, cap, s);
+  for (int k = 0; k < 3; ++k) {
+    dgrow(b_.acc[k], n_, cap, s);
+    dgrow(b_.xsph[k], n_, cap, s);
+  }
+  dgrow(b_.mu, n_, cap, s);
+  if (prec_ == Precision::F32Comp) {
+    dgrow(b_.cpos, 0, cap, s);
+    dgrow(b_.cvel, 0, cap, s);
+    dgrow(b_.cmr, 0, cap, s);
+  }
+  dgrow(b_.cell_of, 0, cap, s);
+  dgrow(b_.rank, 0, cap, s);
+  dgrow(b_.tmp, 0, cap, s);
+  dgrow(b_.perm, 0, cap, s);
+  dgrow(b_.stage, 0, 8 * cap, s);
+  b_.capacity = (int)cap;
+}
+
+void FluidWorld::grow_box_with_bounds() {
+  const double inv = 1.0 / h0_;  // grid.rs:27, cell = h captured at construction
+  const double lo[3] = {params.bounds_min.x, params.bounds_min.y, params.bounds_min.z};
+  const double hi[3] = {params.bounds_max.x, params.bounds_max.y, params.bounds_max.z};
+  for (int a = 0; a < 3; ++a) {
+    long long k0 = key_axis_host(lo[a], inv), k1 = key_axis_host(hi[a], inv);
+    long long mn = std::min(k0, k1), mx = std::max(k0, k1);
+    if (!box_valid_) {
+      kmin_[a] = mn;
+      kmax_[a] = mx;
+    } else {
+      kmin_[a] = std::min(kmin_[a], mn);
+      kmax_[a] = std::max(kmax_[a], mx);
+    }
+  }
+  box_valid_ = true;
+}
+
+// Widens the box with the keys of host positions.  Keys of non-finite
+// coordinates (0 on that axis, as in the reference) are included only when
+// the box stays within the cell cap; otherwise such particles are reported
+// through the out-of-box flag at run time.
+void FluidWorld::grow_box_with_positions(size_t n, const double* pos3) {
+  const double inv = 1.0 / h0_;
+  long long mn[3] = {LLONG_MAX, LLONG_MAX, LLONG_MAX}, mx[3] = {LLONG_MIN, LLONG_MIN, LLONG_MIN};
+  bool any_nonfinite = false;
+  for (size_t i = 0; i < n; ++i) {
+    for (int a = 0; a < 3; ++a) {
+      double x = pos3[3 * i + a];
+      if (!std::isfinite(x)) {
+        any_nonfinite = true;
+        continue;
+      }
+      long long k = key_axis_host(x, inv);
+      mn[a] = std::min(mn[a], k);
+      mx[a] = std::max(mx[a], k);
+    }
+  }
+  merge_box(mn, mx, any_nonfinite);
+}
+
+// Same as grow_box_with_positions for positions already on the device
+// (interleaved xyz), through a reduction kernel and one small readback.
+void FluidWorld::grow_box_with_device_positions(size_t n, const double* d_pos3) {
+  if (n == 0) return;
+  if (!d_bbox_) dalloc(d_bbox_, 7);
+  long long init[7] = {LLONG_MAX, LLONG_MAX, LLONG_MAX, LLONG_MIN, LLONG_MIN, LLONG_MIN, 0};
+  long long res[7];
+  cuda_check(cudaMemcpyAsync(d_bbox_, init, sizeof(init), cudaMemcpyHostToDevice, stream_), "bbox init");
+  int blocks = (int)std::min<size_t>(148 * 8, (n + kThreads - 1) / kThreads);
+  k_key_bbox<<<std::max(blocks, 1), kThreads, 0, stream_>>>((int)n, d_pos3, 1.0 / h0_, d_bbox_);
+  cuda_check(cudaGetLastError(), "bbox kernel");
+  cuda_check(cudaMemcpyAsync(res, d_bbox_, sizeof(res), cudaMemcpyDeviceToHost, stream_), "bbox read");
+  cuda_check(cudaStreamSynchronize(stream_), "bbox sync");
+  merge_box(res, res + 3, res[6] != 0);
+}
+
+// Merges a key range into the box (throws, leaving the box unchanged, when
+// the result would exceed the cell cap).
+void FluidWorld::merge_box(const long long* pmn, const long long* pmx, bool any_nonfinite) {
+  if (!box_valid_) grow_box_with_bounds();
+  long long mn[3], mx[3];
+  for (int a = 0; a < 3; ++a) {
+    mn[a] = std::min(kmin_[a], pmn[a]);
+    mx[a] = std::max(kmax_[a], pmx[a]);
+  }
+  auto cells = [](const long long* a, const long long* b) {
+    long double c = 1;
+    for (int q = 0; q < 3; ++q) c *= (long double)(b[q] - a[q] + 3);
+    return c;
+  };
+  if (cells(mn, mx) > (long double)kMaxCells)
+    throw std::invalid_argument("FluidWorld: particle positions span more grid cells than the 2^27-cell box");
+  if (any_nonfinite) {
+    long long mn0[3], mx0[3];
+    for (int a = 0; a < 3; ++a) {
+      mn0[a] = std::min(mn[a], 0ll);
+      mx0[a] = std::max(mx[a], 0ll);
+    }
+    if (cells(mn0, mx0) <= (long double)kMaxCells)
+      for (int a = 0; a < 3; ++a) {
+        mn[a] = mn0[a];
+        mx[a] = mx0[a];
+      }
+  }
+  for (int a = 0; a < 3; ++a) {
+    kmin_[a] = mn[a];
+    kmax_[a] = mx[a];
+  }
+}
+
+// (Re)builds the dense box: keys [kmin-1, kmax+1] per axis, so that every
+// cell inside [kmin, kmax] has its 26 neighbours in the box.
+void FluidWorld::ensure_cells() {
+  grow_box_with_bounds();
+  long long total = 1;
+  int nc[3];
+  for (int a = 0; a < 3; ++a) {
+    long long d = kmax_[a] - kmin_[a] + 3;
+    if (d > kMaxCells) throw std::invalid_argument("FluidWorld: grid box exceeds 2^27 cells");
+    nc[a] = (int)d;
+    total *= d;
+    if (total > kMaxCells)
+      throw std::invalid_argument("FluidWorld: bounds span more than 2^27 grid cells of size h");
+  }
+  for (int a = 0; a < 3; ++a) {
+    nc_[a] = nc[a];
+    bx0_[a] = kmin_[a] - 1;
+  }
+  ncells_ = (int)total;
+  if (ncells_ > b_.cell_capacity) {
+    int cap = (int)std::min<long long>(kMaxCells, std::max<long long>(ncells_, (long long)b_.cell_capacity * 3 / 2));
+    size_t scan_len = scan_block_sums_needed(cap) * 4096;
+    cuda_check(cudaStreamSynchronize(stream_), "cells sync");
+    dalloc(b_.cell_start, scan_len);
+    dalloc(b_.block_sums, scan_block_sums_needed(cap));
+    b_.cell_capacity = cap;
+  }
+}
+
+StepConsts FluidWorld::make_consts(double dt) const {
+  StepConsts c;
+  std::memset(&c, 0, sizeof(c));
+  // Kernels::new(h0) (kernels.rs:22-35), evaluated in the same order.
+  const double h = h0_;
+  const double h2 = h * h, h3 = h2 * h, h6 = h3 * h3, h9 = h6 * h3;
+  c.h0 = h;
+  c.h0sq = h2;
+  c.poly6_c = 315.0 / (64.0 * kPi * h9);
+  c.spiky_c = (-45.0) / (kPi * h6);
+  c.lap_c = 45.0 / (kPi * h6);
+  c.inv_cell = 1.0 / h;
+  c.h = params.h;
+  c.r2_guard = std::nextafter(params.h * params.h, std::numeric_limits<double>::infinity());
+  if (std::isnan(c.r2_guard)) c.r2_guard = std::numeric_limits<double>::quiet_NaN();
+  c.rest = params.rest_density;
+  c.stiff = params.stiffness;
+  c.shear_min = params.shear_min;
+  c.damp = params.boundary_damp;
+  c.xsph_eps = params.xsph_eps;
+  c.dt = dt;
+  const Vec3* v[3] = {&params.gravity, &params.bounds_min, &params.bounds_max};
+  double* d[3] = {c.g, c.lo, c.hi};
+  for (int k = 0; k < 3; ++k) {
+    d[k][0] = v[k]->x;
+    d[k][1] = v[k]->y;
+    d[k][2] = v[k]->z;
+  }
+  c.n_visc_k = (int)params.visc_k.size();
+  for (size_t k = 0; k < params.visc_k.size() && k < (size_t)kMaxMaterials; ++k) c.visc_k[k] = params.visc_k[k];
+  for (size_t k = 0; k < params.visc_n.size() && k < (size_t)kMaxMaterials; ++k) c.visc_n[k] = params.visc_n[k];
+  c.n = (int)n_;
+  c.bx0 = bx0_[0];
+  c.by0 = bx0_[1];
+  c.bz0 = bx0_[2];
+  c.ncx = nc_[0];
+  c.ncy = nc_[1];
+  c.ncz = nc_[2];
+  c.ncells = ncells_;
+  c.h0f = (float)h;
+  c.h0sqf = (float)h2;
+  c.poly6_cf = (float)c.poly6_c;
+  c.spiky_cf = (float)c.spiky_c;
+  c.lap_cf = (float)c.lap_c;
+  c.hf = (float)params.h;
+  c.h2f = (float)(params.h * params.h);
+  return c;
+}
+
+double FluidWorld::lattice_mass(double s) const {
+  // world.rs:148-169: uses the live params.h and the captured kernels.
+  const double h = params.h;
+  const double hh = h0_;
+  const double h2 = hh * hh, h3 = h2 * hh, h6 = h3 * h3, h9 = h6 * h3;
+  const double poly6_c = 315.0 / (64.0 * kPi * h9);
+  auto poly6 = [&](double r) {
+    if (r >= hh) return 0.0;
+    double diff = h2 - r * r;
+    return poly6_c * diff * diff * diff;
+  };
+  int n_shell = (int)std::ceil(h / s) + 1;
+  double sum_w = 0.0;
+  for (int i = -n_shell; i <= n_shell; ++i)
+    for (int j = -n_shell; j <= n_shell; ++j)
+      for (int l = -n_shell; l <= n_shell; ++l) {
+        double rr = std::sqrt((double)(i * i + j * j + l * l));
+        double r = s * rr;
+        if (r < h) sum_w = sum_w + poly6(r);
+      }
+  return sum_w > 0.0 ? params.rest_density / sum_w : params.mass;
+}
+
+void FluidWorld::fill_box(Vec3 mn, Vec3 mx, double spacing, double margin) {
+  // world.rs:124-144: float-accumulated lattice, z innermost.
+  const double lo[3] = {mn.x + margin, mn.y + margin, mn.z + margin};
+  const double hi[3] = {mx.x - margin, mx.y - margin, mx.z - margin};
+  const double d = spacing;
+  const double mass = lattice_mass(d);
+  std::vector<double> pos;
+  for (double x = lo[0]; x <= hi[0]; x = x + d)
+    for (double y = lo[1]; y <= hi[1]; y = y + d)
+      for (double z = lo[2]; z <= hi[2]; z = z + d) {
+        pos.push_back(x);
+        pos.push_back(y);
+        pos.push_back(z);
+      }
+  size_t m = pos.size() / 3;
+  std::vector<double> ms(m, mass);
+  add_particles(m, pos.data(), nullptr, ms.data(), nullptr);
+}
+
+void FluidWorld::add_particles(size_t m, const double* pos, const double* vel, const double* mass,
+                               const uint32_t* material) {
+  if (m == 0) return;
+  if (!pos || !mass) throw std::invalid_argument("add_particles: pos and mass are required");
+  ensure_capacity(n_ + m);
+  // Staging layout: pos 3m | vel 3m | mass m | material m (as doubles).
+  std::vector<double> st(8 * m, 0.0);
+  std::memcpy(st.data(), pos, 3 * m * sizeof(double));
+  if (vel) std::memcpy(st.data() + 3 * m, vel, 3 * m * sizeof(double));
+  std::memcpy(st.data() + 6 * m, mass, m * sizeof(double));
+  if (material)
+    for (size_t k = 0; k < m; ++k) st[7 * m + k] = (double)material[k];
+  // stage holds 8 * capacity doubles.
+  cuda_check(cudaMemcpyAsync(b_.stage, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice, stream_),
+             "append upload");
+  grow_box_with_device_positions(m, b_.stage);
+  ParticleConsts& pc = b_.pc[b_.cur];
+  k_append<<<grid_for(m), kThreads, 0, stream_>>>((int)n_, (int)m, b_.stage, b_.pv1[0], b_.pv1[1], b_.pv1[2],
+                                                  b_.pv1[3], b_.pv1[4], b_.pv1[5], pc.mass, pc.mat, pc.id);
+  // Particle::new: acc, rho, p, mu_eff, xsph start at zero (particle.rs:50-63).
+  size_t bytes = m * sizeof(double);
+  cuda_check(cudaMemsetAsync(b_.rho + n_, 0, bytes, stream_), "memset");
+  cuda_check(cudaMemsetAsync(b_.p + n_, 0, bytes, stream_), "memset");
+  cuda_check(cudaMemsetAsync(b_.mu + n_, 0, bytes, stream_), "memset");
+  for (int k = 0; k < 3; ++k) {
+    cuda_check(cudaMemsetAsync(b_.acc[k] + n_, 0, bytes, stream_), "memset");
+    cuda_check(cudaMemsetAsync(b_.xsph[k] + n_, 0, bytes, stream_), "memset");
+    if (b_.has_ba) cuda_check(cudaMemsetAsync(pc.ba[k] + n_, 0, bytes, stream_), "memset");
+  }
+  cuda_check(cudaGetLastError(), "append kernel");
+  n_ += m;
+  // The staging vector must outlive the copy.
+  cuda_check(cudaStreamSynchronize(stream_), "append sync");
+}
+
+int FluidWorld::components(int field) {
+  switch (field) {
+    case PHY_FIELD_POS:
+    case PHY_FIELD_VEL:
+    case PHY_FIELD_ACC:
+    case PHY_FIELD_BODY_ACC:
+    case PHY_FIELD_XSPH:
+      return 3;
+    case PHY_FIELD_RHO:
+    case PHY_FIELD_P:
+    case PHY_FIELD_MASS:
+    case PHY_FIELD_MU_EFF:
+    case PHY_FIELD_MATERIAL:
+      return 1;
+    default:
+      return 0;
+  }
+}
+
+void FluidWorld::get_field(int field, double* out) {
+  int nc = components(field);
+  if (nc == 0) throw std::invalid_argument("get_field: unknown field");
+  if (n_ == 0) return;
+  const int n = (int)n_;
+  const ParticleConsts& pc = b_.pc[b_.cur];
+  double* st = b_.stage;
+  switch (field) {
+    case PHY_FIELD_POS:
+      k_get_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, b_.pv1[0], b_.pv1[1], b_.pv1[2], st);
+      break;
+    case PHY_FIELD_VEL:
+      k_get_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, b_.pv1[3], b_.pv1[4], b_.pv1[5], st);
+      break;
+    case PHY_FIELD_ACC:
+      k_get_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, b_.acc[0], b_.acc[1], b_.acc[2], st);
+      break;
+    case PHY_FIELD_XSPH:
+      k_get_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, b_.xsph[0], b_.xsph[1], b_.xsph[2], st);
+      break;
+    case PHY_FIELD_BODY_ACC:
+      if (b_.has_ba)
+        k_get_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, pc.ba[0], pc.ba[1], pc.ba[2], st);
+      else
+        cuda_check(cudaMemsetAsync(st, 0, 3 * n_ * sizeof(double), stream_), "memset");
+      break;
+    case PHY_FIELD_RHO:
+      k_get_scalar_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, b_.rho, st);
+      break;
+    case PHY_FIELD_P:
+      k_get_scalar_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, b_.p, st);
+      break;
+    case PHY_FIELD_MASS:
+      k_get_scalar_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, pc.mass, st);
+      break;
+    case PHY_FIELD_MU_EFF:
+      k_get_scalar_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, b_.mu, st);
+      break;
+    case PHY_FIELD_MATERIAL:
+      launch_unsort_u32(b_, n, pc.mat, st, stream_);
+      break;
+  }
+  cuda_check(cudaGetLastError(), "get_field kernel");
+  cuda_check(cudaMemcpyAsync(out, st, (size_t)nc * n_ * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+             "get_field copy");
+  cuda_check(cudaStreamSynchronize(stream_), "get_field sync");
+}
+
+void FluidWorld::set_field(int field, const double* in) {
+  int nc = components(field);
+  if (nc == 0) throw std::invalid_argument("set_field: unknown field");
+  if (n_ == 0) return;
+  const int n = (int)n_;
+  ParticleConsts& pc = b_.pc[b_.cur];
+  double* st = b_.stage;
+  cuda_check(cudaMemcpyAsync(st, in, (size_t)nc * n_ * sizeof(double), cudaMemcpyHostToDevice, stream_),
+             "set_field copy");
+  // New positions may widen the grid box; checked before the state changes.
+  if (field == PHY_FIELD_POS) grow_box_with_device_positions(n_, st);
+  if (field == PHY_FIELD_BODY_ACC && !b_.has_ba) {
+    for (int q = 0; q < 2; ++q)
+      for (int k = 0; k < 3; ++k) dgrow(b_.pc[q].ba[k], 0, (size_t)b_.capacity, stream_);
+    b_.has_ba = true;
+  }
+  switch (field) {
+    case PHY_FIELD_POS:
+      k_set_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, st, b_.pv1[0], b_.pv1[1], b_.pv1[2]);
+      break;
+    case PHY_FIELD_VEL:
+      k_set_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, st, b_.pv1[3], b_.pv1[4], b_.pv1[5]);
+      break;
+    case PHY_FIELD_ACC:
+      k_set_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, st, b_.acc[0], b_.acc[1], b_.acc[2]);
+      break;
+    case PHY_FIELD_XSPH:
+      k_set_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, st, b_.xsph[0], b_.xsph[1], b_.xsph[2]);
+      break;
+    case PHY_FIELD_BODY_ACC:
+      k_set_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, st, pc.ba[0], pc.ba[1], pc.ba[2]);
+      break;
+    case PHY_FIELD_RHO:
+      k_set_scalar_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, st, b_.rho);
+      break;
+    case PHY_FIELD_P:
+      k_set_scalar_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, st, b_.p);
+      break;
+    case PHY_FIELD_MASS:
+      k_set_scalar_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, st, pc.mass);
+      break;
+    case PHY_FIELD_MU_EFF:
+      k_set_scalar_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, st, b_.mu);
+      break;
+    case PHY_FIELD_MATERIAL:
+      k_set_u32_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, st, pc.mat);
+      break;
+  }
+  cuda_check(cudaGetLastError(), "set_field kernel");
+  // The caller's buffer may be reused as soon as we return.
+  cuda_check(cudaStreamSynchronize(stream_), "set_field sync");
+}
+
+void FluidWorld::step(double dt) {
+  if (n_ == 0) return;  // world.rs:184-186
+  if (params.visc_k.empty() || params.visc_k.size() > (size_t)kMaxMaterials)
+    throw std::invalid_argument("step: visc_k must hold 1..16 entries");
+  if (params.visc_n.size() < params.visc_k.size())
+    throw std::invalid_argument("step: visc_n shorter than visc_k (the reference would index out of bounds)");
+  ensure_cells();
+  StepConsts c = make_consts(dt);
+  cuda_check(cudaMemsetAsync(b_.flags, 0, sizeof(uint32_t), stream_), "flags reset");
+  if (counting_) cuda_check(cudaMemsetAsync(b_.counters, 0, 2 * sizeof(unsigned long long), stream_), "memset");
+  unsigned long long* saved = b_.counters;
+  if (!counting_) b_.counters = nullptr;
+  PassEvents pe;
+  if (timing_) {
+    cuda_check(cudaEventRecord(ev_[0], stream_), "event");
+    pe.after_prep = ev_[2];
+    pe.after_density = ev_[3];
+  }
+  launch_sort(c, b_, stream_);
+  if (timing_) cuda_check(cudaEventRecord(ev_[1], stream_), "event");
+  if (prec_ == Precision::F64Plain)
+    launch_plain_passes(c, b_, stream_, pe);
+  else
+    launch_comp_passes(c, b_, stream_, pe);
+  b_.counters = saved;
+  cuda_check(cudaGetLastError(), "step launch");
+  if (timing_) {
+    cuda_check(cudaEventRecord(ev_[4], stream_), "event");
+    cuda_check(cudaEventSynchronize(ev_[4]), "event sync");
+    for (int k = 0; k < 4; ++k) {
+      float ms = 0.f;
+      cuda_check(cudaEventElapsedTime(&ms, ev_[k], ev_[k + 1]), "elapsed");
+      phase_ms_[k] += ms;
+    }
+    timed_steps_ += 1;
+  }
+}
+
+void FluidWorld::set_timing(bool on) {
+  if (on && !ev_[0])
+    for (auto& e : ev_) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+  timing_ = on;
+}
+
+void FluidWorld::phase_times(double* out5, bool reset) {
+  for (int k = 0; k < 4; ++k) out5[k] = phase_ms_[k];
+  out5[4] = timed_steps_;
+  if (reset) {
+    for (auto& v : phase_ms_) v = 0;
+    timed_steps_ = 0;
+  }
+}
+
+uint32_t FluidWorld::last_step_flags() {
+  uint32_t f = 0;
+  cuda_check(cudaMemcpyAsync(&f, b_.flags, sizeof(f), cudaMemcpyDeviceToHost, stream_), "flags");
+  cuda_check(cudaStreamSynchronize(stream_), "flags sync");
+  return f;
+}
+
+void FluidWorld::last_step_counters(uint64_t* out2) {
+  unsigned long long v[2];
+  cuda_check(cudaMemcpyAsync(v, b_.counters, sizeof(v), cudaMemcpyDeviceToHost, stream_), "counters");
+  cuda_check(cudaStreamSynchronize(stream_), "counters sync");
+  out2[0] = v[0];
+  out2[1] = v[1];
+}
+
+void FluidWorld::diagnostics(double* out4) {
+  // Serial f64 sums in insertion order, like the reference's loops.
+  std::vector<double> vel(3 * n_), mass(n_);
+  get_field(PHY_FIELD_VEL, vel.data());
+  get_field(PHY_FIELD_MASS, mass.data());
+  double px = 0, py = 0, pz = 0, e = 0;
+  for (size_t i = 0; i < n_; ++i) {
+    double vx = vel[3 * i], vy = vel[3 * i + 1], vz = vel[3 * i + 2], m = mass[i];
+    px = px + vx * m;
+    py = py + vy * m;
+    pz = pz + vz * m;
+  }
+  for (size_t i = 0; i < n_; ++i) {
+    double vx = vel[3 * i], vy = vel[3 * i + 1], vz = vel[3 * i + 2];
+    double n2 = (vx * vx + vy * vy) + vz * vz;
+    e = e + (n2 * mass[i]) / (1.0 + 1.0);
+  }
+  out4[0] = px;
+  out4[1] = py;
+  out4[2] = pz;
+  out4[3] = e;
+}
+
+// ---- FluidSubsystem / World ------------------------------------------------
+
+int FluidSubsystem::validate() {
+  if (world->is_empty()) return 0;
+  uint32_t f = world->last_step_flags();
+  if (f & kFlagNonFinite) return 2;
+  if (f & kFlagOutOfBox) return 5;
+  return 0;
+}
+
+void World::step(double dt) {
+  for (auto& s : subs) s->world->step(dt);
+  // Coupling stage (subsystem.rs:92-143) needs a HeatField or a
+  // RigidSubsystem; worlds of this build hold fluid subsystems only, so it
+  // has nothing to couple.
+  t += dt;
+}
+
+int World::step_checked(double dt) {
+  step(dt);
+  for (auto& s : subs) {
+    int rc = s->validate();
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+size_t World::fluid_count() const {
+  size_t n = 0;
+  for (auto& s : subs) n += s->world->len();
+  return n;
+}
+
+}  // namespace phy

@@ -1,0 +1,151 @@
+// Host-side mirror of the reference's fluid API (crates/phy-fluid):
+//   SphParams<T>      src/sph/params.rs:12-86
+//   FluidWorld<T>     src/sph/world.rs:21-197
+//   FluidSubsystem<T> src/subsystem.rs:26-164
+//   World<T>          crates/phy-core/src/world.rs:78-294 (fluid subsystems only)
+//
+// The device holds the particle state; nothing is mirrored on the host.  Host
+// reads and writes of a particle field go through permutation kernels so that
+// callers always see insertion order, as with the reference's `particles` Vec.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/phy_fluid.h"
+#include "sph_buffers.h"
+
+namespace phy {
+
+struct Vec3 {
+  double x, y, z;
+};
+
+struct SphParams {
+  double rest_density, stiffness, viscosity;
+  std::vector<double> visc_k, visc_n;
+  double shear_min, mass, h;
+  Vec3 gravity, bounds_min, bounds_max;
+  double boundary_damp, xsph_eps;
+
+  static SphParams defaults();  // params.rs:55-85
+  PhySphParams to_c() const;
+  static SphParams from_c(const PhySphParams& c);
+};
+
+enum class Precision : int { F64Plain = 0, F32Comp = 1 };
+
+class CudaError : public std::runtime_error {
+ public:
+  using std::runtime_error::runtime_error;
+};
+
+void cuda_check(cudaError_t e, const char* what);
+
+class FluidWorld {
+ public:
+  FluidWorld(const SphParams& params, Precision prec);
+  ~FluidWorld();
+  FluidWorld(const FluidWorld&) = delete;
+  FluidWorld& operator=(const FluidWorld&) = delete;
+
+  // Public, live parameters (the reference's `pub params`).  The smoothing
+  // length of the kernel coefficients and of the grid cell was captured at
+  // construction (world.rs:94-102).
+  SphParams params;
+
+  size_t len() const { return n_; }
+  bool is_empty() const { return n_ == 0; }
+  Precision precision() const { return prec_; }
+  double captured_h() const { return h0_; }
+
+  double lattice_mass(double s) const;                                  // world.rs:148-169
+  void fill_box(Vec3 mn, Vec3 mx, double spacing, double margin);       // world.rs:124-144
+  void add_particles(size_t n, const double* pos, const double* vel, const double* mass,
+                     const uint32_t* material);                         // world.rs:171-174
+  void step(double dt);                                                 // world.rs:183-192
+
+  // Insertion-order field access (particle.rs:17-46).
+  static int components(int field);
+  void get_field(int field, double* out);
+  void set_field(int field, const double* in);
+
+  void set_stream(cudaStream_t s);
+  cudaStream_t stream() const { return stream_; }
+  void synchronize();
+  // Error bits of the last step (synchronises).
+  uint32_t last_step_flags();
+  // Candidates / pairs of the last step (synchronises); counting is enabled
+  // by set_counting(true) and costs one atomic per warp.
+  void set_counting(bool on) { counting_ = on; }
+  void last_step_counters(uint64_t* out2);
+  int grid_cells() const { return ncells_; }
+
+  // Total momentum and kinetic energy (subsystem.rs:149-163), f64, insertion order.
+  void diagnostics(double* out4);
+
+  // Per-phase device timing with CUDA events on the world's stream: while
+  // enabled, every step records events around the sort, the per-particle
+  // preparation, the density pass and the force pass, and waits for them to
+  // accumulate the durations (ms).  out = {sort, prep, density, force, steps}.
+  void set_timing(bool on);
+  void phase_times(double* out5, bool reset);
+
+  // Device state access for in-library consumers (sorted order).
+  DevBuffers& buffers() { return b_; }
+  StepConsts make_consts(double dt) const;
+
+ private:
+  void ensure_capacity(size_t n);
+  void ensure_cells();
+  void grow_box_with_bounds();
+  void grow_box_with_positions(size_t n, const double* pos3);
+  void merge_box(const long long* mn, const long long* mx, bool any_nonfinite);
+  void grow_box_with_device_positions(size_t n, const double* d_pos3);
+  void free_all();
+
+  Precision prec_;
+  double h0_;
+  size_t n_ = 0;
+  DevBuffers b_;
+  cudaStream_t stream_ = nullptr;
+  cudaStream_t own_stream_ = nullptr;
+  // Grid box: inclusive key range of occupied-or-possible cells (unpadded).
+  bool box_valid_ = false;
+  long long kmin_[3] = {0, 0, 0}, kmax_[3] = {0, 0, 0};
+  int ncells_ = 0;
+  long long bx0_[3] = {0, 0, 0};
+  int nc_[3] = {0, 0, 0};
+  bool counting_ = false;
+  bool timing_ = false;
+  cudaEvent_t ev_[5] = {};
+  double phase_ms_[4] = {0, 0, 0, 0};
+  double timed_steps_ = 0;
+  long long* d_bbox_ = nullptr;  // 7 values: min xyz, max xyz, non-finite flag
+};
+
+// FluidSubsystem<T> (subsystem.rs:26-55): the world plus coupling coefficients.
+struct FluidSubsystem {
+  std::unique_ptr<FluidWorld> world;
+  double thermal_expansion = 0.0, heat_gain = 0.0, t_ref = 0.0, drag = 1.0, friction = 0.1;
+  explicit FluidSubsystem(std::unique_ptr<FluidWorld> w) : world(std::move(w)) {}
+  // Subsystem::validate (subsystem.rs:74-90): 0 ok, 2 non-finite, 5 grid box.
+  int validate();
+};
+
+// World<T> restricted to fluid subsystems (phy-core/src/world.rs:224-293).
+class World {
+ public:
+  std::vector<std::unique_ptr<FluidSubsystem>> subs;
+  double t = 0.0;
+  void step(double dt);            // world.rs:265-267
+  int step_checked(double dt);     // world.rs:282-293
+  size_t fluid_count() const;
+};
+
+}  // namespace phy

@@ -1,0 +1,305 @@
+// Spatial hash of the SPH step on the device: integer cell keys, a counting
+// sort by cell, a stable within-cell order by insertion index, and the gather
+// that moves every per-particle array into the new order.
+//
+// Reference behaviour reproduced (crates/phy-fluid/src/sph/grid.rs):
+//   * key_of: floor(x * (1/cell)) per axis, f64 -> i64, None -> 0 (25-33);
+//   * build: a cell's particles in ascending insertion index (35-40).
+// The sort is deterministic even though the histogram uses atomics: ranks
+// inside a cell are recomputed from the insertion indices, so the final order
+// is the total order (cell, insertion index) whatever the atomic order was.
+//
+// All kernels here are integer/byte work bound by HBM bandwidth; launches use
+// 256-thread blocks and grid-stride loops sized to a multiple of the SM count.
+#include <cuda_runtime.h>
+
+#include "sph_buffers.h"
+
+namespace phy {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kThreads * kScanItems;  // 4096 cells per scan block
+
+int grid_for(int n, int threads = kThreads) {
+  int b = (n + threads - 1) / threads;
+  return b < 1 ? 1 : b;
+}
+
+// Cell of every particle plus its arrival rank inside the cell.  Lanes of a
+// warp that share a cell (the common case: the previous order is already
+// sorted by cell) are aggregated into one atomic.
+__global__ void __launch_bounds__(kThreads) k_cell_hist(StepConsts c, const double* __restrict__ px,
+                                                        const double* __restrict__ py,
+                                                        const double* __restrict__ pz,
+                                                        uint32_t* __restrict__ cell_of,
+                                                        uint32_t* __restrict__ rank,
+                                                        uint32_t* __restrict__ count,
+                                                        uint32_t* __restrict__ flags) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool active = i < c.n;
+  uint32_t cell = 0;
+  if (active) {
+    long long kx = key_axis(px[i], c.inv_cell);
+    long long ky = key_axis(py[i], c.inv_cell);
+    long long kz = key_axis(pz[i], c.inv_cell);
+    if (cell_interior(c, kx, ky, kz)) {
+      cell = (uint32_t)cell_linear(c, kx, ky, kz);
+    } else {
+      cell = (uint32_t)c.ncells;  // overflow cell: never visited as a neighbour
+      atomicOr(flags, kFlagOutOfBox);
+    }
+    cell_of[i] = cell;
+  }
+  unsigned mask = __ballot_sync(0xffffffffu, active);
+  if (!active) return;
+  unsigned peers = __match_any_sync(mask, cell);
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(peers) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(&count[cell], (uint32_t)__popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  rank[i] = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+}
+
+// Sum of each 4096-cell tile.
+__global__ void __launch_bounds__(kThreads) k_scan_reduce(const uint32_t* __restrict__ v,
+                                                          uint32_t* __restrict__ block_sums) {
+  const uint4* t = reinterpret_cast<const uint4*>(v + (size_t)blockIdx.x * kScanTile) + threadIdx.x * 4;
+  uint32_t s = 0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint4 a = t[q];
+    s += a.x + a.y + a.z + a.w;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ uint32_t ws[kThreads / 32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t tot = 0;
+    for (int w = 0; w < kThreads / 32; ++w) tot += ws[w];
+    block_sums[blockIdx.x] = tot;
+  }
+}
+
+// Block-wide exclusive scan of one value per thread; returns the block total.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t& total) {
+  __shared__ uint32_t ws[32];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[warp] = x;
+  __syncthreads();
+  int nw = blockDim.x >> 5;
+  if (warp == 0) {
+    uint32_t w = lane < nw ? ws[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < nw) ws[lane] = w;
+  }
+  __syncthreads();
+  uint32_t warp_off = warp > 0 ? ws[warp - 1] : 0;
+  total = ws[nw - 1];
+  __syncthreads();
+  return warp_off + x - v;
+}
+
+// Exclusive scan of the tile sums, one block of 1024 threads, in chunks.
+__global__ void __launch_bounds__(1024) k_scan_top(uint32_t* __restrict__ block_sums, int nb) {
+  uint32_t carry = 0;
+  for (int base = 0; base < nb; base += blockDim.x) {
+    int k = base + threadIdx.x;
+    uint32_t v = k < nb ? block_sums[k] : 0;
+    uint32_t total;
+    uint32_t ex = block_exclusive_scan(v, total);
+    if (k < nb) block_sums[k] = carry + ex;
+    carry += total;
+  }
+}
+
+// In-place exclusive scan of each tile plus its tile offset.
+__global__ void __launch_bounds__(kThreads) k_scan_apply(uint32_t* __restrict__ v,
+                                                         const uint32_t* __restrict__ block_sums) {
+  uint4* t = reinterpret_cast<uint4*>(v + (size_t)blockIdx.x * kScanTile) + threadIdx.x * 4;
+  uint32_t a[kScanItems];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint4 u = t[q];
+    a[4 * q] = u.x;
+    a[4 * q + 1] = u.y;
+    a[4 * q + 2] = u.z;
+    a[4 * q + 3] = u.w;
+  }
+  uint32_t s = 0;
+#pragma unroll
+  for (int q = 0; q < kScanItems; ++q) {
+    uint32_t x = a[q];
+    a[q] = s;
+    s += x;
+  }
+  uint32_t total;
+  uint32_t off = block_exclusive_scan(s, total) + block_sums[blockIdx.x];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    t[q] = make_uint4(a[4 * q] + off, a[4 * q + 1] + off, a[4 * q + 2] + off, a[4 * q + 3] + off);
+}
+
+__global__ void __launch_bounds__(kThreads) k_scatter(int n, const uint32_t* __restrict__ cell_of,
+                                                      const uint32_t* __restrict__ rank,
+                                                      const uint32_t* __restrict__ cell_start,
+                                                      uint32_t* __restrict__ tmp) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  tmp[cell_start[cell_of[i]] + rank[i]] = (uint32_t)i;
+}
+
+// Final slot of every particle: its rank by insertion index among the
+// particles of its cell.  The overflow cell keeps arrival order (its
+// particles never interact).
+__global__ void __launch_bounds__(kThreads) k_order(int n, int ncells, const uint32_t* __restrict__ cell_of,
+                                                    const uint32_t* __restrict__ cell_start,
+                                                    const uint32_t* __restrict__ tmp,
+                                                    const uint32_t* __restrict__ id,
+                                                    uint32_t* __restrict__ perm) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  uint32_t i = tmp[s];
+  uint32_t cell = cell_of[i];
+  if ((int)cell == ncells) {
+    perm[s] = i;
+    return;
+  }
+  uint32_t cs = cell_start[cell], ce = cell_start[cell + 1];
+  uint32_t mine = id[i];
+  uint32_t r = 0;
+  for (uint32_t k = cs; k < ce; ++k) r += id[tmp[k]] < mine ? 1u : 0u;
+  perm[cs + r] = i;
+}
+
+struct GatherArgs {
+  const double* src_pv[6];
+  double* dst_pv[6];
+  ParticleConsts src, dst;
+  int has_ba;
+};
+
+__global__ void __launch_bounds__(kThreads) k_gather(int n, const uint32_t* __restrict__ perm, GatherArgs g) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  uint32_t i = perm[s];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) g.dst_pv[k][s] = g.src_pv[k][i];
+  g.dst.mass[s] = g.src.mass[i];
+  g.dst.mat[s] = g.src.mat[i];
+  g.dst.id[s] = g.src.id[i];
+  if (g.has_ba) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) g.dst.ba[k][s] = g.src.ba[k][i];
+  }
+}
+
+__global__ void k_unsort_f64(int n, const uint32_t* __restrict__ id, const double* __restrict__ src,
+                             double* __restrict__ dst) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) dst[id[s]] = src[s];
+}
+__global__ void k_unsort_u32(int n, const uint32_t* __restrict__ id, const uint32_t* __restrict__ src,
+                             double* __restrict__ dst) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) dst[id[s]] = (double)src[s];
+}
+__global__ void k_iota(uint32_t* dst, int n) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) dst[s] = (uint32_t)s;
+}
+__global__ void k_fill(double* dst, double v, int n) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) dst[s] = v;
+}
+__global__ void k_interleave3(const double* x, const double* y, const double* z, double* d, int n) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) {
+    d[3 * (size_t)s] = x[s];
+    d[3 * (size_t)s + 1] = y[s];
+    d[3 * (size_t)s + 2] = z[s];
+  }
+}
+__global__ void k_deinterleave3(const double* d, double* x, double* y, double* z, int n) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) {
+    x[s] = d[3 * (size_t)s];
+    y[s] = d[3 * (size_t)s + 1];
+    z[s] = d[3 * (size_t)s + 2];
+  }
+}
+__global__ void k_u32_from_f64(const double* src, uint32_t* dst, int n) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) dst[s] = (uint32_t)src[s];
+}
+
+}  // namespace
+
+// Cells scanned per step: the box plus the overflow cell, rounded up to whole
+// scan tiles (the padding stays zero, so the prefix at index ncells+1 is n).
+static int scan_length(int ncells) { return ((ncells + 2 + kScanTile - 1) / kScanTile) * kScanTile; }
+
+size_t scan_block_sums_needed(int ncells) { return (size_t)scan_length(ncells) / kScanTile; }
+
+void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s) {
+  const int n = c.n;
+  const int len = scan_length(c.ncells);
+  const int nb = len / kScanTile;
+  cudaMemsetAsync(b.cell_start, 0, (size_t)len * sizeof(uint32_t), s);
+  k_cell_hist<<<grid_for(n), kThreads, 0, s>>>(c, b.pv1[0], b.pv1[1], b.pv1[2], b.cell_of, b.rank,
+                                               b.cell_start, b.flags);
+  k_scan_reduce<<<nb, kThreads, 0, s>>>(b.cell_start, b.block_sums);
+  k_scan_top<<<1, 1024, 0, s>>>(b.block_sums, nb);
+  k_scan_apply<<<nb, kThreads, 0, s>>>(b.cell_start, b.block_sums);
+  k_scatter<<<grid_for(n), kThreads, 0, s>>>(n, b.cell_of, b.rank, b.cell_start, b.tmp);
+  const ParticleConsts& src = b.pc[b.cur];
+  const ParticleConsts& dst = b.pc[b.cur ^ 1];
+  k_order<<<grid_for(n), kThreads, 0, s>>>(n, c.ncells, b.cell_of, b.cell_start, b.tmp, src.id, b.perm);
+  GatherArgs g;
+  for (int k = 0; k < 6; ++k) {
+    g.src_pv[k] = b.pv1[k];
+    g.dst_pv[k] = b.pv0[k];
+  }
+  g.src = src;
+  g.dst = dst;
+  g.has_ba = b.has_ba ? 1 : 0;
+  k_gather<<<grid_for(n), kThreads, 0, s>>>(n, b.perm, g);
+  b.cur ^= 1;
+}
+
+void launch_unsort_f64(const DevBuffers& b, int n, const double* src_sorted, double* dst_orig,
+                       cudaStream_t s) {
+  k_unsort_f64<<<grid_for(n), kThreads, 0, s>>>(n, b.pc[b.cur].id, src_sorted, dst_orig);
+}
+void launch_unsort_u32(const DevBuffers& b, int n, const uint32_t* src_sorted, double* dst_orig,
+                       cudaStream_t s) {
+  k_unsort_u32<<<grid_for(n), kThreads, 0, s>>>(n, b.pc[b.cur].id, src_sorted, dst_orig);
+}
+void launch_iota(uint32_t* dst, int n, cudaStream_t s) { k_iota<<<grid_for(n), kThreads, 0, s>>>(dst, n); }
+void launch_fill_f64(double* dst, double v, int n, cudaStream_t s) {
+  k_fill<<<grid_for(n), kThreads, 0, s>>>(dst, v, n);
+}
+void launch_interleave3(const double* x, const double* y, const double* z, double* dst, int n,
+                        cudaStream_t s) {
+  k_interleave3<<<grid_for(n), kThreads, 0, s>>>(x, y, z, dst, n);
+}
+void launch_deinterleave3(const double* src, double* x, double* y, double* z, int n, cudaStream_t s) {
+  k_deinterleave3<<<grid_for(n), kThreads, 0, s>>>(src, x, y, z, n);
+}
+void launch_u32_from_f64(const double* src, uint32_t* dst, int n, cudaStream_t s) {
+  k_u32_from_f64<<<grid_for(n), kThreads, 0, s>>>(src, dst, n);
+}
+
+}  // namespace phy

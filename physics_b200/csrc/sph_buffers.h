@@ -1,0 +1,85 @@
+// Device buffers of one fluid subsystem and the host-side launchers.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sph_common.cuh"
+
+namespace phy {
+
+// Per-particle constants carried through the sort (double-buffered: the sort
+// gathers set `cur` into set `cur ^ 1`).
+struct ParticleConsts {
+  double* mass = nullptr;
+  uint32_t* mat = nullptr;
+  uint32_t* id = nullptr;   // insertion index
+  double* ba[3] = {nullptr, nullptr, nullptr};  // body_acc, optional
+};
+
+struct DevBuffers {
+  int capacity = 0;        // particles
+  int cell_capacity = 0;   // grid cells (excluding the overflow cell)
+  // Positions/velocities.  pv0: sorted state read by the passes.
+  // pv1: output of the force pass (same order as pv0) and upload target.
+  double* pv0[6] = {};
+  double* pv1[6] = {};
+  ParticleConsts pc[2];
+  int cur = 0;
+  bool has_ba = false;
+  // Step outputs, sorted order.
+  double* rho = nullptr;
+  double* p = nullptr;
+  double* pr2 = nullptr;   // p / (rho*rho)
+  double* mr = nullptr;    // mass / rho
+  double* acc[3] = {};
+  double* xsph[3] = {};
+  double* mu = nullptr;
+  // f32-compensated form: per-particle packed operands.
+  float4* cpos = nullptr;  // cell-local x, y, z (f32) and mass
+  float4* cvel = nullptr;  // vx, vy, vz (f32) and p/rho^2 (f32)
+  float* cmr = nullptr;    // mass/rho (f32)
+  // Sort scratch.
+  uint32_t* cell_of = nullptr;
+  uint32_t* rank = nullptr;
+  uint32_t* tmp = nullptr;
+  uint32_t* perm = nullptr;
+  uint32_t* cell_start = nullptr;  // cell_capacity + 2 entries
+  uint32_t* block_sums = nullptr;
+  int block_sums_capacity = 0;
+  // Insertion-order staging for uploads and downloads (f64 and u32 views).
+  double* stage = nullptr;   // 3 * capacity doubles
+  uint32_t* flags = nullptr; // error bits, device
+  unsigned long long* counters = nullptr;  // candidates, pairs (device)
+};
+
+// grid.cu
+void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s);
+void launch_unsort_f64(const DevBuffers& b, int n, const double* src_sorted, double* dst_orig,
+                       cudaStream_t s);
+void launch_unsort_u32(const DevBuffers& b, int n, const uint32_t* src_sorted, double* dst_orig,
+                       cudaStream_t s);
+void launch_iota(uint32_t* dst, int n, cudaStream_t s);
+void launch_fill_f64(double* dst, double v, int n, cudaStream_t s);
+void launch_interleave3(const double* x, const double* y, const double* z, double* dst, int n,
+                        cudaStream_t s);
+void launch_deinterleave3(const double* src, double* x, double* y, double* z, int n,
+                          cudaStream_t s);
+void launch_u32_from_f64(const double* src, uint32_t* dst, int n, cudaStream_t s);
+
+// Optional events recorded between the passes (phase timing); any may be null.
+struct PassEvents {
+  cudaEvent_t after_prep = nullptr;
+  cudaEvent_t after_density = nullptr;
+};
+
+// step_plain.cu
+void launch_plain_passes(const StepConsts& c, DevBuffers& b, cudaStream_t s, const PassEvents& ev);
+
+// step_comp.cu
+void launch_comp_passes(const StepConsts& c, DevBuffers& b, cudaStream_t s, const PassEvents& ev);
+
+size_t scan_block_sums_needed(int count);
+
+}  // namespace phy

@@ -1,0 +1,318 @@
+"""CPU oracle checks: golden fixtures, the reference's own SPH property tests
+(crates/phy-fluid/src/sph/tests.rs, crates/phy-demo/tests/*.rs) and analytic
+known answers.  No GPU involved."""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import assert_bits_equal, ref_test_params
+from physics_b200 import SphParams, scenes
+
+
+def world(oracle_mod, params=None, threads=1):
+    return oracle_mod.OracleWorld(params or SphParams.defaults(), threads=threads)
+
+
+# ---- golden fixtures (second restatement, tests/golden/gen_golden.py) -------------
+
+def test_golden_quickstart(oracle_mod, golden):
+    g = golden("quickstart")
+    O = oracle_mod
+    w = world(O)
+    w.fill_box((-1, 1, -1), (1, 3, 1), 0.3, 0.1)
+    assert len(w) == 343
+    w.step(0.01)
+    for k, f in (("pos", O.F_POS), ("vel", O.F_VEL), ("acc", O.F_ACC), ("rho", O.F_RHO), ("p", O.F_P),
+                 ("mu_eff", O.F_MU_EFF), ("xsph", O.F_XSPH), ("mass", O.F_MASS)):
+        assert_bits_equal(w.get(f), g[f"step1_{k}"], f"step1 {k}")
+    done = 1
+    for n in (50, 100, 200):
+        w.step(0.01, n - done)
+        done = n
+        assert_bits_equal(w.get(O.F_POS), g[f"step{n}_pos"], f"step{n} pos")
+        assert_bits_equal(w.get(O.F_VEL), g[f"step{n}_vel"], f"step{n} vel")
+    assert_bits_equal(w.get(O.F_RHO), g["step200_rho"], "step200 rho")
+    assert_bits_equal(w.get(O.F_ACC), g["step200_acc"], "step200 acc")
+
+
+def test_golden_dam216(oracle_mod, golden):
+    g = golden("dam216")
+    O = oracle_mod
+    p = SphParams.defaults()
+    p.bounds_min, p.bounds_max = (0.0, 0.0, 0.0), (1.2, 1.2, 1.2)
+    w = world(O, p)
+    assert w.lattice_mass(0.1) == float(g["mass"])
+    pos = scenes.dam_break_positions(6, 6, 6)
+    assert_bits_equal(pos, g["init_pos"], "generator")
+    w.add_particles(pos, float(g["mass"]))
+    w.step(0.005)
+    for k, f in (("pos", O.F_POS), ("vel", O.F_VEL), ("acc", O.F_ACC), ("rho", O.F_RHO), ("p", O.F_P),
+                 ("mu_eff", O.F_MU_EFF), ("xsph", O.F_XSPH)):
+        assert_bits_equal(w.get(f), g[f"step1_{k}"], f"step1 {k}")
+    w.step(0.005, 29)
+    for k, f in (("pos", O.F_POS), ("vel", O.F_VEL), ("acc", O.F_ACC), ("rho", O.F_RHO), ("p", O.F_P),
+                 ("mu_eff", O.F_MU_EFF), ("xsph", O.F_XSPH)):
+        assert_bits_equal(w.get(f), g[f"step30_{k}"], f"step30 {k}")
+
+
+def test_golden_materials(oracle_mod, golden):
+    g = golden("materials")
+    O = oracle_mod
+    p = ref_test_params(gravity=(0.0, 0.0, 0.0))
+    p.visc_k, p.visc_n = [3.5, 10.0], [1.0, 1.0]
+    w = world(O, p)
+    w.add_particles([[0, 0, 0], [0, 0.06, 0]], 0.05, vel=[[-300, 0, 0], [300, 0, 0]], material=[0, 1])
+    w.step(0.001)
+    for k, f in (("pos", O.F_POS), ("vel", O.F_VEL), ("mu_eff", O.F_MU_EFF), ("acc", O.F_ACC), ("rho", O.F_RHO)):
+        assert_bits_equal(w.get(f), g[f"twomat_{k}"], f"twomat {k}")
+    for n in (0.5, 1.0, 1.5):
+        p = ref_test_params(gravity=(0.0, 0.0, 0.0))
+        p.visc_k, p.visc_n = [3.5], [n]
+        w = world(O, p)
+        pos = [((ix - 2.0) * 0.08, iy * 0.06, 0.0) for iy in range(2) for ix in range(5)]
+        vel = [((-300.0 if iy == 0 else 300.0), 0.0, 0.0) for iy in range(2) for ix in range(5)]
+        w.add_particles(pos, 0.05, vel=vel)
+        w.step(0.001)
+        tag = str(n).replace(".", "p")
+        assert_bits_equal(w.get(O.F_MU_EFF), g[f"shear{tag}_mu_eff"], f"shear {n} mu")
+        assert_bits_equal(w.get(O.F_POS), g[f"shear{tag}_pos"], f"shear {n} pos")
+
+
+# ---- analytic known answers ------------------------------------------------------------
+
+def test_kat_quickstart_mass_and_self_density(oracle_mod):
+    """Spacing 0.3 > h: lattice_mass sums only the self term, so the first-step
+    density of every particle is mass * poly6(0) = rest density (world.rs:148-169)."""
+    O = oracle_mod
+    w = world(O)
+    w.fill_box((-1, 1, -1), (1, 3, 1), 0.3, 0.1)
+    m = w.get(O.F_MASS)
+    assert m[0] == 5.10633472583484
+    h = 0.2
+    poly6_0 = 315.0 / (64.0 * math.pi * h ** 9) * (h * h) ** 3
+    w.step(0.01)
+    rho = w.get(O.F_RHO)
+    np.testing.assert_allclose(rho, 1000.0, rtol=1e-14)
+    np.testing.assert_allclose(rho, m * poly6_0, rtol=1e-15)
+    # no neighbours: acc = 0, so v = g dt and x = x0 + v dt exactly.
+    v = w.get(O.F_VEL)
+    assert np.all(v[:, 1] == -9.81 * 0.01) and np.all(v[:, [0, 2]] == 0.0)
+
+
+def test_kat_two_particle_force(oracle_mod):
+    """Two particles at r < h: symmetric pressure and viscosity evaluated by hand."""
+    O = oracle_mod
+    p = ref_test_params(gravity=(0.0, 0.0, 0.0))
+    w = world(O, p)
+    w.add_particles([[0.0, 0.0, 0.0], [0.05, 0.0, 0.0]], 2.0, vel=[[0.0, 0.0, 0.0], [1.0, 0.0, 0.0]])
+    w.step(1e-3)
+    h = 0.2
+    r = 0.05
+    c6 = 315.0 / (64.0 * math.pi * h ** 9)
+    w0 = c6 * (h * h) ** 3
+    wr = c6 * (h * h - r * r) ** 3
+    rho = 2.0 * w0 + 2.0 * wr
+    prs = 250.0 * (rho - 1000.0) if rho > 1000.0 else 0.0
+    rho_o = w.get(O.F_RHO)
+    np.testing.assert_allclose(rho_o, rho, rtol=1e-14)
+    np.testing.assert_allclose(w.get(O.F_P), prs, rtol=1e-12, atol=1e-9)
+    spiky = -45.0 / (math.pi * h ** 6) * (h - r) ** 2
+    lap = 45.0 / (math.pi * h ** 6) * (h - r)
+    coef = 4.0 * (2 * prs / rho ** 2)
+    f_press0 = 1.0 * coef * spiky            # on particle 0, direction +x
+    f_visc0 = 1.0 * (4.0 / rho * lap) * 3.5  # dv = +1
+    acc0 = (f_press0 + f_visc0) / rho
+    acc = w.get(O.F_ACC)
+    np.testing.assert_allclose(acc[0, 0], acc0, rtol=1e-12)
+    np.testing.assert_allclose(acc[1, 0], -acc0, rtol=1e-12)
+    assert np.all(acc[:, 1:] == 0.0)
+
+
+def test_kat_interior_lattice_density(oracle_mod):
+    """An interior particle of an unjittered lattice has rho = rest density (world.rs:146-169)."""
+    O = oracle_mod
+    p = SphParams.defaults()
+    p.gravity = (0.0, 0.0, 0.0)
+    w = world(O, p)
+    w.fill_box((-0.55, -0.55, -0.55), (0.55, 0.55, 0.55), 0.1, 0.0)
+    w.step(1e-6)
+    pos0 = w.get(O.F_POS)
+    rho = w.get(O.F_RHO)
+    centre = np.argmin(np.linalg.norm(pos0, axis=1))
+    np.testing.assert_allclose(rho[centre], 1000.0, rtol=1e-12)
+
+
+def test_cell_keys_floor_semantics(oracle_mod):
+    """Grid::key_of is floor(x * (1/h)) per axis (grid.rs:25-33), negative included."""
+    O = oracle_mod
+    w = world(O)
+    pts = np.array([[0.0, -0.0, 0.2], [-1e-12, 0.19999999999999998, -0.2], [4.99, -4.99, 0.3999999999]], np.float64)
+    w.add_particles(pts, 1.0)
+    keys = w.cell_keys()
+    inv = 1.0 / 0.2
+    expect = np.floor(pts * inv).astype(np.int64)
+    assert np.array_equal(keys, expect)
+
+
+def test_neighbor_visit_order(oracle_mod):
+    """27 cells with di outer and dk inner, ascending insertion index in a cell (grid.rs:43-56)."""
+    O = oracle_mod
+    w = world(O)
+    rng = np.random.default_rng(3)
+    pts = rng.uniform(-0.5, 0.5, size=(300, 3))
+    w.add_particles(pts, 1.0)
+    keys = w.cell_keys()
+    nb = w.neighbors(0)
+    k0 = keys[0]
+    expect = []
+    for di in (-1, 0, 1):
+        for dj in (-1, 0, 1):
+            for dk in (-1, 0, 1):
+                cell = k0 + np.array([di, dj, dk])
+                expect.extend(np.flatnonzero(np.all(keys == cell, axis=1)).tolist())
+    assert nb.tolist() == expect
+
+
+# ---- the reference's property tests, on the oracle ------------------------------------
+
+def test_fill_box_count_matches_grid(oracle_mod):
+    """sph/tests.rs:18-29."""
+    w = world(oracle_mod, ref_test_params())
+    w.fill_box((-1, -1, -1), (1, 1, 1), 0.2, 0.05)
+    assert 500 < len(w) < 2000
+
+
+def test_density_converges_near_rest(oracle_mod):
+    """sph/tests.rs:31-56."""
+    w = world(oracle_mod, ref_test_params(gravity=(0.0, 0.0, 0.0)))
+    w.fill_box((-0.5, -0.5, -0.5), (0.5, 0.5, 0.5), 0.1, 0.05)
+    w.step(0.002, 15)
+    avg = w.get(oracle_mod.F_RHO).mean()
+    assert abs(avg - 1000.0) / 1000.0 < 0.25
+
+
+def test_particle_count_conserved(oracle_mod):
+    """sph/tests.rs:58-72."""
+    w = world(oracle_mod, ref_test_params())
+    w.fill_box((-1, -1, -1), (1, 1, 1), 0.1, 0.05)
+    n0 = len(w)
+    w.step(0.003, 50)
+    assert len(w) == n0
+
+
+def test_dam_break_stays_in_bounds(oracle_mod):
+    """sph/tests.rs:74-95."""
+    O = oracle_mod
+    w = world(O, ref_test_params())
+    w.fill_box((-1.5, -1.5, -0.5), (-0.5, 1.5, 0.5), 0.1, 0.05)
+    for _ in range(12):
+        w.step(0.0025, 10)
+        pos = w.get(O.F_POS)
+        assert np.isfinite(pos).all()
+        assert (pos >= -3.0 - 1e-6).all() and (pos <= 3.0 + 1e-6).all()
+
+
+def test_material_tag_distinguishes_viscosity(oracle_mod):
+    """sph/tests.rs:406-427."""
+    O = oracle_mod
+    p = ref_test_params(gravity=(0.0, 0.0, 0.0))
+    p.visc_k, p.visc_n = [3.5, 10.0], [1.0, 1.0]
+    w = world(O, p)
+    w.add_particles([[0, 0, 0], [0, 0.06, 0]], 0.05, vel=[[-300, 0, 0], [300, 0, 0]], material=[0, 1])
+    w.step(0.001)
+    mu = w.get(O.F_MU_EFF)
+    assert abs(mu[0] - 3.5) < 1e-6 and abs(mu[1] - 10.0) < 1e-6
+
+
+def test_non_newtonian_ordering(oracle_mod):
+    """sph/tests.rs:392-404."""
+    O = oracle_mod
+    mus = []
+    for n in (0.5, 1.0, 1.5):
+        p = ref_test_params(gravity=(0.0, 0.0, 0.0))
+        p.visc_k, p.visc_n = [3.5], [n]
+        w = world(O, p)
+        pos = [((ix - 2.0) * 0.08, iy * 0.06, 0.0) for iy in range(2) for ix in range(5)]
+        vel = [((-300.0 if iy == 0 else 300.0), 0.0, 0.0) for iy in range(2) for ix in range(5)]
+        w.add_particles(pos, 0.05, vel=vel)
+        w.step(0.001)
+        mus.append(w.get(O.F_MU_EFF)[0])
+    assert mus[0] < mus[1] < mus[2]
+
+
+def test_closed_system_invariants(oracle_mod):
+    """phy-demo/tests/stability.rs:55-108 (800 particles, h = 2 spacing, no gravity),
+    shortened from 1000 to 300 steps to keep the CPU suite fast."""
+    O = oracle_mod
+    half = 5.0
+    spacing = (8.0 * half ** 3 / 800) ** (1.0 / 3.0)
+    p = SphParams.defaults()
+    p.h = spacing * 2.0
+    p.gravity = (0.0, 0.0, 0.0)
+    p.bounds_min, p.bounds_max = (-7.0, -1.0, -7.0), (7.0, 13.0, 7.0)
+    w = world(O, p, threads=4)
+    w.fill_box((-half, 1.0, -half), (half, 1.0 + 2 * half, half), spacing, 0.1)
+    e0 = w.diagnostics()[3]
+    w.step(0.01, 300)
+    d = w.diagnostics()
+    assert np.isfinite(w.get(O.F_POS)).all()
+    assert abs(d[3] - e0) <= 1e-2
+    assert np.linalg.norm(d[:3]) <= 1e-3
+
+
+def test_thread_count_does_not_change_results(oracle_mod):
+    """Write-disjoint per-particle maps (world.rs:201-203): rayon/OpenMP thread count is irrelevant."""
+    O = oracle_mod
+    pos = scenes.dam_break_positions(8, 10, 8)
+    p = SphParams.defaults()
+    p.bounds_min, p.bounds_max = (0.0, 0.0, 0.0), (1.6, 1.6, 1.6)
+    outs = []
+    for t in (1, 4):
+        w = world(O, p, threads=t)
+        w.add_particles(pos, scenes.lattice_mass(0.1))
+        w.step(0.005, 10)
+        outs.append(w.get(O.F_POS))
+    assert_bits_equal(outs[0], outs[1], "threads 1 vs 4")
+
+
+def test_live_h_change_keeps_captured_kernels(oracle_mod):
+    """F7: kernels and grid keep the h of FluidWorld::new; the cutoff uses the live h."""
+    O = oracle_mod
+    pos = scenes.dam_break_positions(4, 4, 4)
+    p = SphParams.defaults()
+    p.bounds_min, p.bounds_max = (0.0, 0.0, 0.0), (0.8, 0.8, 0.8)
+    a = world(O, p)
+    a.add_particles(pos, 1.0)
+    p2 = SphParams.defaults()
+    p2.bounds_min, p2.bounds_max = p.bounds_min, p.bounds_max
+    p2.h = 0.15
+    a.set_params(p2)
+    a.step(0.001)
+    b = world(O, p2)  # constructed with h = 0.15: different kernels and cells
+    b.add_particles(pos, 1.0)
+    b.step(0.001)
+    assert not np.array_equal(a.get(O.F_RHO), b.get(O.F_RHO))
+
+
+def test_scene_generator_sizes():
+    assert scenes.config("quickstart").n == 343
+    assert scenes.dam_break_positions(80, 160, 80).shape == (1024000, 3)
+    assert scenes.config("grad_64k").n == 65536
+    assert scenes.lattice_mass(0.1) == 0.99031946198009
+    u = scenes.uniform01(0xC0FFEE, 0, 1000)
+    assert u.min() >= 0.0 and u.max() < 1.0
+
+
+def test_splitmix_matches_sequential_definition():
+    """Vectorised SplitMix64 equals the sequential Rng::next_u64 (replay.rs:40-46)."""
+    mask = (1 << 64) - 1
+    state = 12345
+    ref = []
+    for _ in range(8):
+        state = (state + 0x9E3779B97F4A7C15) & mask
+        z = state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & mask
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
+        ref.append(z ^ (z >> 31))
+    assert scenes.splitmix64(12345, 0, 8).tolist() == ref

@@ -1,0 +1,112 @@
+"""FP32-compensated CUDA step vs the f64 oracle.
+
+Gate (teacher-forced, one step from the same state): max relative density
+error <= 1e-5.  Pressure error is normalised by stiffness * rest density
+(p is ~0 near rest, so a relative p error is meaningless); acceleration,
+XSPH and position errors are reported and bounded loosely."""
+import numpy as np
+import pytest
+
+from helpers import assert_bits_equal, ref_test_params
+from physics_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+RHO_TOL = 1e-5
+
+
+def _params(sc):
+    from physics_b200 import SphParams
+    p = SphParams.defaults()
+    p.bounds_min, p.bounds_max = sc.bounds_min, sc.bounds_max
+    return p
+
+
+def errors(w, O, ow, p):
+    rho_g, rho_o = w.rho, ow.get(O.F_RHO)
+    e = {"rho_rel": float(np.max(np.abs(rho_g - rho_o) / np.abs(rho_o))),
+         "p_norm": float(np.max(np.abs(w.p - ow.get(O.F_P))) / (p.stiffness * p.rest_density))}
+    acc_o = ow.get(O.F_ACC)
+    scale = np.max(np.linalg.norm(acc_o, axis=1)) + 1e-30
+    e["acc_rel_to_max"] = float(np.max(np.linalg.norm(w.acc - acc_o, axis=1)) / scale)
+    e["pos_abs"] = float(np.max(np.abs(w.pos - ow.get(O.F_POS))))
+    return e
+
+
+@pytest.mark.parametrize("dims,presteps", [((16, 24, 16), 0), ((16, 24, 16), 200), ((10, 10, 10), 60)])
+def test_density_error_gate_teacher_forced(gpu, oracle_mod, dims, presteps):
+    O = oracle_mod
+    sc = scenes.dam_break(*dims, box=2.0 * max(dims) * 0.1, dt=0.005, steps=0)
+    p = _params(sc)
+    ow = O.OracleWorld(p, threads=O.max_threads())
+    ow.add_particles(sc.pos, sc.mass)
+    if presteps:
+        ow.step(0.005, presteps)  # a developed, splashing state
+    w = gpu.FluidWorld(p, "comp")
+    w.add_particles(ow.get(O.F_POS), ow.get(O.F_MASS), vel=ow.get(O.F_VEL))
+    ow.step(0.005)
+    w.step(0.005)
+    e = errors(w, O, ow, p)
+    print("comp errors", dims, presteps, e)
+    assert e["rho_rel"] <= RHO_TOL, e
+    assert e["p_norm"] <= 1e-5, e
+    assert e["acc_rel_to_max"] <= 1e-3, e
+    assert e["pos_abs"] <= 1e-9, e
+
+
+def test_comp_run_to_run_deterministic(gpu):
+    sc = scenes.dam_break(20, 30, 20, box=6.0, dt=0.005, steps=0)
+    p = _params(sc)
+    outs = []
+    for _ in range(2):
+        w = gpu.FluidWorld(p, "comp")
+        w.add_particles(sc.pos, sc.mass)
+        w.step(0.005, 30)
+        outs.append((w.pos.copy(), w.vel.copy(), w.rho.copy()))
+    for a, b in zip(*outs):
+        assert_bits_equal(a, b, "comp run-to-run")
+
+
+def test_comp_property_tests(gpu):
+    """The reference's property tests (sph/tests.rs:31-95) on the compensated form."""
+    w = gpu.FluidWorld(ref_test_params(gravity=(0.0, 0.0, 0.0)), "comp")
+    w.fill_box((-0.5, -0.5, -0.5), (0.5, 0.5, 0.5), 0.1, 0.05)
+    w.step(0.002, 15)
+    assert abs(w.rho.mean() - 1000.0) / 1000.0 < 0.25
+    w = gpu.FluidWorld(ref_test_params(), "comp")
+    w.fill_box((-1.5, -1.5, -0.5), (-0.5, 1.5, 0.5), 0.1, 0.05)
+    n0 = w.len()
+    for _ in range(12):
+        w.step(0.0025, 10)
+        pos = w.pos
+        assert np.isfinite(pos).all()
+        assert (pos >= -3.0 - 1e-6).all() and (pos <= 3.0 + 1e-6).all()
+    assert w.len() == n0
+
+
+def test_comp_materials(gpu):
+    """material_tag_distinguishes_viscosity (sph/tests.rs:406-427) in the compensated form."""
+    p = ref_test_params(gravity=(0.0, 0.0, 0.0))
+    p.visc_k, p.visc_n = [3.5, 10.0], [1.0, 1.0]
+    w = gpu.FluidWorld(p, "comp")
+    w.add_particles([[0, 0, 0], [0, 0.06, 0]], 0.05, vel=[[-300, 0, 0], [300, 0, 0]], material=[0, 1])
+    w.step(0.001)
+    assert abs(w.effective_viscosity(0) - 3.5) < 1e-6 and abs(w.effective_viscosity(1) - 10.0) < 1e-6
+
+
+def test_comp_free_running_stays_close(gpu, oracle_mod):
+    """Over 100 free-running steps the compensated trajectory stays near the f64 one
+    (the dynamics are chaotic, so this bounds drift rather than pinning bits)."""
+    O = oracle_mod
+    sc = scenes.dam_break(12, 16, 12, box=3.2, dt=0.005, steps=0)
+    p = _params(sc)
+    ow = O.OracleWorld(p, threads=O.max_threads())
+    ow.add_particles(sc.pos, sc.mass)
+    w = gpu.FluidWorld(p, "comp")
+    w.add_particles(sc.pos, sc.mass)
+    ow.step(0.005, 100)
+    w.step(0.005, 100)
+    dpos = np.abs(w.pos - ow.get(O.F_POS)).max()
+    drho = np.abs(w.rho - ow.get(O.F_RHO)).max() / 1000.0
+    print("comp free-running drift: pos", dpos, "rho", drho)
+    assert dpos < 1e-3 and drho < 1e-2
