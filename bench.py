@@ -144,7 +144,8 @@ def run_ours(args):
         return float(t.item())
 
     K, W = args.steps, args.warmup
-    pos = scenes.dam_break_positions(*DIMS)
+    dims = tuple(args.dims)
+    pos = scenes.dam_break_positions(*dims)
     n = pos.shape[0]
     params = make_params(pb)
     stream = torch.cuda.Stream()
@@ -259,7 +260,7 @@ def run_ours(args):
             "dtype": "f32c/f64",
             "data": "synthetic (seeded jittered dam-break lattice)",
             "config": {
-                "workload": f"dam_break_{DIMS[0]}x{DIMS[1]}x{DIMS[2]}: {n} particles, spacing 0.1 = h/2, "
+                "workload": f"dam_break_{dims[0]}x{dims[1]}x{dims[2]}: {n} particles, spacing 0.1 = h/2, "
                             f"bounds [0,{BOX}]^3, dt={DT}, FP32-compensated step",
                 "particles": n,
                 "parallelism": f"replicas x{world_size}",
@@ -378,6 +379,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--dims", type=int, nargs=3, default=list(DIMS),
+                    help="lattice of the dam block (default 128 256 128 = 4,194,304 particles); smaller blocks "
+                         "are for profiling captures only")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -151,6 +151,15 @@ int32_t phy_fluid_step_counters(PhyWorldHandle *w, uint32_t sub, uint64_t *out4)
 int32_t phy_fluid_set_timing(PhyWorldHandle *w, uint32_t sub, int32_t on);
 int32_t phy_fluid_phase_times(PhyWorldHandle *w, uint32_t sub, double *out5, int32_t reset);
 
+/* Kernel configuration of `sub` (no effect on the f64 plain form's results):
+ *   PHY_TUNE_COMP_TILE  0 = x-major cell runs, 4 = staged 4x4x4-cell tiles
+ *                       (default) for the FP32-compensated passes;
+ *   PHY_TUNE_HALO_CAP   staged particles per tile halo before a tile is
+ *                       computed from global memory (default: the kernels'
+ *                       capacity). */
+enum { PHY_TUNE_COMP_TILE = 0, PHY_TUNE_HALO_CAP = 1 };
+int32_t phy_fluid_set_tuning(PhyWorldHandle *w, uint32_t sub, int32_t param, int64_t value);
+
 /* Message of the last failing call on this thread ("" if none). */
 const char *phy_fluid_last_error(void);
 

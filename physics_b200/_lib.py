@@ -16,6 +16,9 @@ MAX_MATERIALS = 16
 PRECISION_F64_PLAIN = 0
 PRECISION_F32_COMP = 1
 
+TUNE_COMP_TILE = 0
+TUNE_HALO_CAP = 1
+
 FIELD_POS = 0
 FIELD_VEL = 1
 FIELD_ACC = 2
@@ -108,6 +111,7 @@ SIGNATURES = {
     "phy_fluid_step_counters": (C.c_int32, [H, C.c_uint32, C.POINTER(C.c_uint64)]),
     "phy_fluid_set_timing": (C.c_int32, [H, C.c_uint32, C.c_int32]),
     "phy_fluid_phase_times": (C.c_int32, [H, C.c_uint32, DP, C.c_int32]),
+    "phy_fluid_set_tuning": (C.c_int32, [H, C.c_uint32, C.c_int32, C.c_int64]),
     "phy_fluid_last_error": (C.c_char_p, []),
 }
 

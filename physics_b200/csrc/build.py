@@ -33,7 +33,8 @@ PER_FILE = {
     "grid.cu": ["-fmad=false"],
     "fluid_world.cu": ["-fmad=false"],
 }
-SOURCES = ["grid.cu", "step_plain.cu", "step_comp.cu", "fluid_world.cu", "ffi.cpp", "checkpoint.cpp"]
+SOURCES = ["grid.cu", "step_plain.cu", "step_comp.cu", "step_tiled.cu", "fluid_world.cu", "ffi.cpp",
+           "checkpoint.cpp"]
 
 
 def _nvcc() -> str:

@@ -381,6 +381,19 @@ int32_t phy_fluid_phase_times(PhyWorldHandle* w, uint32_t sub, double* out5, int
   });
 }
 
+int32_t phy_fluid_set_tuning(PhyWorldHandle* w, uint32_t sub, int32_t param, int64_t value) {
+  return guard<int32_t>(-1, [&] {
+    FluidWorld& fw = *sub_of(w, sub).world;
+    if (param == PHY_TUNE_COMP_TILE)
+      fw.set_comp_tile((int)value);
+    else if (param == PHY_TUNE_HALO_CAP)
+      fw.set_halo_cap(value > (1 << 30) ? (1 << 30) : (int)value);
+    else
+      throw std::invalid_argument("unknown tuning parameter");
+    return 0;
+  });
+}
+
 const char* phy_fluid_last_error(void) { return g_last_error.c_str(); }
 
 }  // extern "C"

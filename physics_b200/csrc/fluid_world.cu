@@ -264,6 +264,13 @@ void FluidWorld::free_all() {
   dfree(b_.cpos);
   dfree(b_.cvel);
   dfree(b_.cmr);
+  dfree(b_.nbr);
+  dfree(b_.nbr_count);
+  dfree(b_.nbr16);
+  dfree(b_.sorted_cell);
+  dfree(b_.tile_head);
+  dfree(b_.tile_slot);
+  dfree(b_.num_tiles);
   dfree(b_.cell_of);
   dfree(b_.rank);
   dfree(b_.tmp);
@@ -285,7 +292,8 @@ void FluidWorld::synchronize() { cuda_check(cudaStreamSynchronize(stream_), "syn
 // Grows every per-particle array to hold n particles (geometric growth),
 // keeping the current n_ particles.
 void FluidWorld::ensure_capacity(size_t n) {
-  if (n > 0x7fffffffull) throw std::invalid_argument("FluidWorld: more than 2^31-1 particles");
+  if (n >= (1ull << (32 - kCodeBits)))
+    throw std::invalid_argument("FluidWorld: more than 2^27 particles in one subsystem");
   if ((int)n <= b_.capacity) return;
   size_t cap = std::max<size_t>(n, (size_t)b_.capacity + b_.capacity / 2);
   cudaStream_t s = stream_;
@@ -317,12 +325,41 @@ void FluidWorld::ensure_capacity(size_t n) {
     dgrow(b_.cvel, 0, cap, s);
     dgrow(b_.cmr, 0, cap, s);
   }
+  dgrow(b_.nbr_count, 0, cap, s);
+  dfree(b_.nbr);
+  dfree(b_.nbr16);
+  dfree(b_.sorted_cell);
+  dfree(b_.tile_head);
+  dfree(b_.tile_slot);
   dgrow(b_.cell_of, 0, cap, s);
   dgrow(b_.rank, 0, cap, s);
   dgrow(b_.tmp, 0, cap, s);
   dgrow(b_.perm, 0, cap, s);
   dgrow(b_.stage, 0, 8 * cap, s);
   b_.capacity = (int)cap;
+  ensure_mode_buffers();
+}
+
+// Buffers that depend on the kernel form: 32-bit neighbour lists for the
+// x-major passes, 16-bit staged-slot lists and the tile list for tiles.
+void FluidWorld::ensure_mode_buffers() {
+  const size_t cap = (size_t)b_.capacity;
+  if (cap == 0) return;
+  const bool tiled = prec_ == Precision::F32Comp && comp_tile_ > 0;
+  if (!tiled && !b_.nbr) dalloc(b_.nbr, (size_t)kMaxNeighbors * cap);
+  if (tiled) {
+    if (!b_.nbr16) dalloc(b_.nbr16, (size_t)kMaxNeighbors * cap);
+    if (!b_.sorted_cell) dalloc(b_.sorted_cell, cap);
+    if (!b_.tile_head) dalloc(b_.tile_head, tile_head_length((int)cap));
+    if (!b_.tile_slot) dalloc(b_.tile_slot, cap + 1);
+    if (!b_.num_tiles) dalloc(b_.num_tiles, 1);
+  }
+}
+
+void FluidWorld::set_comp_tile(int t) {
+  if (t != 0 && t != 4) throw std::invalid_argument("comp tile must be 0 (x-major runs) or 4");
+  comp_tile_ = t;
+  ensure_mode_buffers();
 }
 
 void FluidWorld::grow_box_with_bounds() {
@@ -420,10 +457,12 @@ void FluidWorld::merge_box(const long long* pmn, const long long* pmx, bool any_
 // cell inside [kmin, kmax] has its 26 neighbours in the box.
 void FluidWorld::ensure_cells() {
   grow_box_with_bounds();
+  tile_ = (prec_ == Precision::F32Comp) ? comp_tile_ : 0;
   long long total = 1;
   int nc[3];
   for (int a = 0; a < 3; ++a) {
     long long d = kmax_[a] - kmin_[a] + 3;
+    if (tile_) d = (d + tile_ - 1) / tile_ * tile_;
     if (d > kMaxCells) throw std::invalid_argument("FluidWorld: grid box exceeds 2^27 cells");
     nc[a] = (int)d;
     total *= d;
@@ -440,8 +479,16 @@ void FluidWorld::ensure_cells() {
     size_t scan_len = scan_block_sums_needed(cap) * 4096;
     cuda_check(cudaStreamSynchronize(stream_), "cells sync");
     dalloc(b_.cell_start, scan_len);
-    dalloc(b_.block_sums, scan_block_sums_needed(cap));
     b_.cell_capacity = cap;
+  }
+  // The scan's tile sums serve the cell scan and the tile-head scan (n + 1
+  // entries) alike.
+  const int sums = (int)std::max(scan_block_sums_needed(b_.cell_capacity),
+                                 tile_head_length(std::max(b_.capacity, 1)) / 4096);
+  if (sums > b_.block_sums_capacity) {
+    cuda_check(cudaStreamSynchronize(stream_), "sums sync");
+    dalloc(b_.block_sums, (size_t)sums);
+    b_.block_sums_capacity = sums;
   }
 }
 
@@ -484,6 +531,14 @@ StepConsts FluidWorld::make_consts(double dt) const {
   c.ncy = nc_[1];
   c.ncz = nc_[2];
   c.ncells = ncells_;
+  c.tile = tile_;
+  c.tile_log2 = tile_ == 4 ? 2 : 0;
+  c.halo_cap = halo_cap_;
+  if (tile_) {
+    c.ntx = nc_[0] / tile_;
+    c.nty = nc_[1] / tile_;
+    c.ntz = nc_[2] / tile_;
+  }
   c.h0f = (float)h;
   c.h0sqf = (float)h2;
   c.poly6_cf = (float)c.poly6_c;
@@ -713,6 +768,8 @@ void FluidWorld::step(double dt) {
   if (timing_) cuda_check(cudaEventRecord(ev_[1], stream_), "event");
   if (prec_ == Precision::F64Plain)
     launch_plain_passes(c, b_, stream_, pe);
+  else if (tile_)
+    launch_comp_tiled(c, b_, stream_, pe);
   else
     launch_comp_passes(c, b_, stream_, pe);
   b_.counters = saved;

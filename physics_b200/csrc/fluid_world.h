@@ -96,12 +96,21 @@ class FluidWorld {
   void set_timing(bool on);
   void phase_times(double* out5, bool reset);
 
+  // Kernel configuration of the compensated form: tile edge in cells
+  // (0 = x-major runs, 4 = staged 4x4x4 tiles, the default).
+  void set_comp_tile(int t);
+  int comp_tile() const { return comp_tile_; }
+  // Staging capacity (particles per tile halo) below the kernels' maximum;
+  // smaller values route more tiles through the global-memory path.
+  void set_halo_cap(int v) { halo_cap_ = v < 0 ? 0 : v; }
+
   // Device state access for in-library consumers (sorted order).
   DevBuffers& buffers() { return b_; }
   StepConsts make_consts(double dt) const;
 
  private:
   void ensure_capacity(size_t n);
+  void ensure_mode_buffers();
   void ensure_cells();
   void grow_box_with_bounds();
   void grow_box_with_positions(size_t n, const double* pos3);
@@ -122,6 +131,9 @@ class FluidWorld {
   long long bx0_[3] = {0, 0, 0};
   int nc_[3] = {0, 0, 0};
   bool counting_ = false;
+  int comp_tile_ = 4;
+  int halo_cap_ = 1 << 30;
+  int tile_ = 0;  // linearisation of the current box (0 = x-major)
   bool timing_ = false;
   cudaEvent_t ev_[5] = {};
   double phase_ms_[4] = {0, 0, 0, 0};

@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(kThreads) k_cell_hist(StepConsts c, const doub
     long long ky = key_axis(py[i], c.inv_cell);
     long long kz = key_axis(pz[i], c.inv_cell);
     if (cell_interior(c, kx, ky, kz)) {
-      cell = (uint32_t)cell_linear(c, kx, ky, kz);
+      cell = (uint32_t)cell_index(c, kx, ky, kz);
     } else {
       cell = (uint32_t)c.ncells;  // overflow cell: never visited as a neighbour
       atomicOr(flags, kFlagOutOfBox);
@@ -189,6 +189,8 @@ struct GatherArgs {
   double* dst_pv[6];
   ParticleConsts src, dst;
   int has_ba;
+  const uint32_t* cell_of;
+  uint32_t* sorted_cell;  // nullable: cell of every sorted slot
 };
 
 __global__ void __launch_bounds__(kThreads) k_gather(int n, const uint32_t* __restrict__ perm, GatherArgs g) {
@@ -204,6 +206,45 @@ __global__ void __launch_bounds__(kThreads) k_gather(int n, const uint32_t* __re
 #pragma unroll
     for (int k = 0; k < 3; ++k) g.dst.ba[k][s] = g.src.ba[k][i];
   }
+  if (g.sorted_cell) g.sorted_cell[s] = g.cell_of[i];
+}
+
+// Tile list of a tiled sort: head[s] = 1 where slot s starts a new tile
+// (slots of the overflow cell excluded); head[n] = 0.
+__global__ void __launch_bounds__(kThreads) k_tile_heads(int n, int ncells, int tile_log2,
+                                                        const uint32_t* __restrict__ sorted_cell,
+                                                        uint32_t* __restrict__ head) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s > n) return;
+  uint32_t h = 0;
+  if (s < n) {
+    const uint32_t c = sorted_cell[s];
+    if ((int)c != ncells) {
+      const uint32_t t = c >> (3 * tile_log2);
+      h = (s == 0 || (sorted_cell[s - 1] >> (3 * tile_log2)) != t) ? 1u : 0u;
+    }
+  }
+  head[s] = h;
+}
+
+// After the exclusive scan of head: tile_slot[k] = first slot of tile k;
+// tile_slot[count] = first overflow slot (end of the last tile);
+// *num_tiles = count.
+__global__ void __launch_bounds__(kThreads) k_tile_emit(int n, int ncells, const uint32_t* __restrict__ sorted_cell,
+                                                       const uint32_t* __restrict__ scanned,
+                                                       const uint32_t* __restrict__ cell_start,
+                                                       uint32_t* __restrict__ tile_slot,
+                                                       uint32_t* __restrict__ num_tiles) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) {
+    if (s == n) {
+      const uint32_t count = scanned[n];
+      *num_tiles = count;
+      tile_slot[count] = cell_start[ncells];
+    }
+    return;
+  }
+  if (scanned[s + 1] != scanned[s]) tile_slot[scanned[s]] = (uint32_t)s;
 }
 
 __global__ void k_unsort_f64(int n, const uint32_t* __restrict__ id, const double* __restrict__ src,
@@ -252,6 +293,7 @@ __global__ void k_u32_from_f64(const double* src, uint32_t* dst, int n) {
 static int scan_length(int ncells) { return ((ncells + 2 + kScanTile - 1) / kScanTile) * kScanTile; }
 
 size_t scan_block_sums_needed(int ncells) { return (size_t)scan_length(ncells) / kScanTile; }
+size_t tile_head_length(int n) { return (size_t)((n + 1 + kScanTile - 1) / kScanTile) * kScanTile; }
 
 void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s) {
   const int n = c.n;
@@ -275,8 +317,22 @@ void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s) {
   g.src = src;
   g.dst = dst;
   g.has_ba = b.has_ba ? 1 : 0;
+  g.cell_of = b.cell_of;
+  g.sorted_cell = c.tile ? b.sorted_cell : nullptr;
   k_gather<<<grid_for(n), kThreads, 0, s>>>(n, b.perm, g);
   b.cur ^= 1;
+  if (c.tile) {
+    // head flags in `rank` (free after the scatter), scanned in place.
+    const int hlen = ((n + 1 + kScanTile - 1) / kScanTile) * kScanTile;
+    cudaMemsetAsync(b.tile_head, 0, (size_t)hlen * sizeof(uint32_t), s);
+    k_tile_heads<<<grid_for(n + 1), kThreads, 0, s>>>(n, c.ncells, c.tile_log2, b.sorted_cell, b.tile_head);
+    const int hb = hlen / kScanTile;
+    k_scan_reduce<<<hb, kThreads, 0, s>>>(b.tile_head, b.block_sums);
+    k_scan_top<<<1, 1024, 0, s>>>(b.block_sums, hb);
+    k_scan_apply<<<hb, kThreads, 0, s>>>(b.tile_head, b.block_sums);
+    k_tile_emit<<<grid_for(n + 1), kThreads, 0, s>>>(n, c.ncells, b.sorted_cell, b.tile_head, b.cell_start,
+                                                   b.tile_slot, b.num_tiles);
+  }
 }
 
 void launch_unsort_f64(const DevBuffers& b, int n, const double* src_sorted, double* dst_orig,

@@ -40,6 +40,21 @@ struct DevBuffers {
   float4* cpos = nullptr;  // cell-local x, y, z (f32) and mass
   float4* cvel = nullptr;  // vx, vy, vz (f32) and p/rho^2 (f32)
   float* cmr = nullptr;    // mass/rho (f32)
+  // Neighbour lists written by the density pass and read by the force pass:
+  // entry k of particle i at nbr[k * capacity + i] (column-major, so a warp's
+  // k-th entries are contiguous); nbr_count[i] may exceed kMaxNeighbors, in
+  // which case the force pass rescans the 27 cells for that particle.
+  uint32_t* nbr = nullptr;
+  uint32_t* nbr_count = nullptr;
+  // Tiled form: 16-bit neighbour slots (shared-memory staging order of the
+  // tile's halo), column-major like nbr.
+  uint16_t* nbr16 = nullptr;
+  // Tiled sort: cell of each sorted slot, tile heads (scan scratch), first
+  // slot of every occupied tile (+ end), and the device-side tile count.
+  uint32_t* sorted_cell = nullptr;
+  uint32_t* tile_head = nullptr;
+  uint32_t* tile_slot = nullptr;
+  uint32_t* num_tiles = nullptr;
   // Sort scratch.
   uint32_t* cell_of = nullptr;
   uint32_t* rank = nullptr;
@@ -81,5 +96,9 @@ void launch_plain_passes(const StepConsts& c, DevBuffers& b, cudaStream_t s, con
 void launch_comp_passes(const StepConsts& c, DevBuffers& b, cudaStream_t s, const PassEvents& ev);
 
 size_t scan_block_sums_needed(int count);
+size_t tile_head_length(int n);
+
+// step_tiled.cu: the FP32-compensated passes over staged 4x4x4-cell tiles.
+void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const PassEvents& ev);
 
 }  // namespace phy

@@ -18,6 +18,14 @@
 namespace phy {
 
 constexpr int kMaxMaterials = 16;
+// Neighbour-list capacity per particle (in-range pairs; ~31 at rest density
+// with spacing h/2, ~40 under strong compression).
+constexpr int kMaxNeighbors = 64;
+// f32-compensated lists pack the 27-cell offset code under the index.
+constexpr int kCodeBits = 5;
+// The first kStagedNeighbors entries of a list are staged in shared memory
+// and written out coalesced; further entries go straight to global memory.
+constexpr int kStagedNeighbors = 40;
 
 // Error bits written by device code into the per-world flag word.
 enum : uint32_t {
@@ -39,6 +47,16 @@ struct StepConsts {
   long long bx0, by0, bz0;
   int ncx, ncy, ncz;
   int ncells;
+  // Cell linearisation: tile == 0 is x-major / z-minor over the box (the
+  // reference's 27-cell order becomes 9 runs of 3 cells); tile == B (a power
+  // of two) orders B^3-cell tiles x-major and the cells inside a tile
+  // x-major, so a tile's particles are contiguous (ncx, ncy, ncz are then
+  // multiples of B and ntx, nty, ntz count tiles).
+  int tile, tile_log2;
+  int ntx, nty, ntz;
+  // Tiles whose halo holds more particles than this are computed from
+  // global memory instead of shared memory (<= the kernels' capacity).
+  int halo_cap;
   // f32 copies for the compensated form.
   float h0f, h0sqf, poly6_cf, spiky_cf, lap_cf, hf, h2f;
 };
@@ -58,6 +76,22 @@ __device__ __forceinline__ int cell_linear(const StepConsts& c, long long i, lon
   long long a = i - c.bx0, b = j - c.by0, d = k - c.bz0;
   if (a < 0 || b < 0 || d < 0 || a >= c.ncx || b >= c.ncy || d >= c.ncz) return -1;
   return (int)((a * c.ncy + b) * c.ncz + d);
+}
+
+// Tiled linear index of box coordinates (a, b, d), all inside the box.
+__device__ __forceinline__ int tiled_index(const StepConsts& c, int a, int b, int d) {
+  const int L = c.tile_log2, m = c.tile - 1;
+  const int tile = ((a >> L) * c.nty + (b >> L)) * c.ntz + (d >> L);
+  return (tile << (3 * L)) + ((((a & m) << L) + (b & m)) << L) + (d & m);
+}
+
+// Sort cell of integer key (i,j,k) under the configured linearisation, or -1
+// when outside the box.
+__device__ __forceinline__ int cell_index(const StepConsts& c, long long i, long long j, long long k) {
+  if (c.tile == 0) return cell_linear(c, i, j, k);
+  long long a = i - c.bx0, b = j - c.by0, d = k - c.bz0;
+  if (a < 0 || b < 0 || d < 0 || a >= c.ncx || b >= c.ncy || d >= c.ncz) return -1;
+  return tiled_index(c, (int)a, (int)b, (int)d);
 }
 
 // A particle's own cell is an "interior" cell when its 27 neighbours are all
@@ -80,6 +114,19 @@ __device__ __forceinline__ void material_coeffs(const StepConsts& c, int m, doub
       n = c.visc_n[q];
     }
   }
+}
+
+// Writes the staged part of each thread's neighbour list (column-major in
+// shared memory, bank = thread) to its global column-major list: at step k
+// the 32 lanes of a warp store 32 consecutive words.
+template <int kBlock>
+__device__ __forceinline__ void flush_staged_list(const uint32_t (*s_list)[kBlock], uint32_t* lst, int stride,
+                                                  uint32_t cnt, bool active) {
+  const unsigned am = __activemask();
+  const uint32_t mine = active ? (cnt < (uint32_t)kStagedNeighbors ? cnt : (uint32_t)kStagedNeighbors) : 0u;
+  const uint32_t kmax = __reduce_max_sync(am, mine);
+  for (uint32_t k = 0; k < kmax; ++k)
+    if (k < mine) lst[(size_t)k * stride] = s_list[k][threadIdx.x];
 }
 
 #endif  // __CUDACC__

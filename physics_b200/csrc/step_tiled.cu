@@ -1,0 +1,574 @@
+// FP32-compensated SPH passes over staged cell tiles.
+//
+// The sort orders cells in 4x4x4 tiles (tiled_index), so the particles of a
+// tile are one contiguous slot range.  A persistent grid walks the list of
+// occupied tiles; for each tile a CTA stages the particles of the tile's
+// 6x6x6-cell halo into shared memory once (about 3.4 stagings per particle
+// per pass instead of ~219 per-candidate gathers through L1/L2) and every
+// query particle of the tile reads its 27 neighbour cells from there.
+//
+// Arithmetic is the compensated form of step_comp.cu: f32 pair math on
+// tile-relative coordinates (cell offset + cell-local f32 coordinate, so the
+// absolute rounding error is about (B+1) h0 2^-24 whatever the scene's
+// extent), Kahan-compensated density and force sums, f64 integration.
+//
+// The density pass records each particle's in-range neighbours as 16-bit
+// shared-memory slot indices; the force pass re-stages the same halo in the
+// same order and walks the list without re-filtering candidates, so its
+// lanes stay converged.  Tiles whose halo exceeds the staging capacity, and
+// lists longer than kMaxNeighbors, fall back to reading global memory.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "sph_buffers.h"
+
+namespace phy {
+
+namespace {
+
+constexpr int kTB = 4;                          // tile edge (cells)
+constexpr int kTL = 2;                          // log2(kTB)
+constexpr int kH = kTB + 2;                     // halo edge (cells)
+constexpr int kNH = kH * kH * kH;               // halo cells
+constexpr int kTT = 256;                        // threads per CTA
+constexpr int kHaloCap = 2048;                  // staged particles per tile
+constexpr int kListRows = kMaxNeighbors + 1;    // smem list rows (+1 row absorbs overflow writes)
+static_assert(kNH <= kTT, "one halo cell per thread");
+static_assert(kHaloCap <= 65536, "16-bit slots");
+
+__device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
+  float y = x - c;
+  float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+struct TiledArgs {
+  const double* __restrict__ px;
+  const double* __restrict__ py;
+  const double* __restrict__ pz;
+  const double* __restrict__ vx;
+  const double* __restrict__ vy;
+  const double* __restrict__ vz;
+  const double* __restrict__ mass;
+  const uint32_t* __restrict__ mat;
+  const uint32_t* __restrict__ cell_start;
+  const uint32_t* __restrict__ sorted_cell;
+  const uint32_t* __restrict__ tile_slot;
+  const uint32_t* __restrict__ num_tiles;
+  float4* cpos;  // cell-local x, y, z and mass
+  float4* cvel;  // vx, vy, vz and p/rho^2
+  float* cmr;    // mass/rho
+  double* bax;
+  double* bay;
+  double* baz;
+  double* rho;
+  double* p;
+  double* acc[3];
+  double* xsph[3];
+  double* mu;
+  double* out_pv[6];
+  uint16_t* nbr16;
+  uint32_t* nbr_count;
+  int stride;
+  uint32_t* flags;
+  unsigned long long* counters;
+};
+
+// nbr_count value of a particle whose tile was not staged (force rescans).
+constexpr uint32_t kNoList = 0xffffffffu;
+
+// Block-wide exclusive scan (kTT threads, one value each).
+__device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* ws, uint32_t& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < kTT / 32 ? ws[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < kTT / 32) ws[lane] = w;
+  }
+  __syncthreads();
+  total = ws[kTT / 32 - 1];
+  const uint32_t off = warp > 0 ? ws[warp - 1] : 0u;
+  __syncthreads();
+  return off + x - v;
+}
+
+struct TileGeom {
+  int tx, ty, tz;  // tile coordinates
+  uint32_t first, last;
+};
+
+__device__ __forceinline__ TileGeom tile_geom(const StepConsts& c, const TiledArgs& a, uint32_t k) {
+  TileGeom g;
+  g.first = a.tile_slot[k];
+  g.last = a.tile_slot[k + 1];
+  const int t = (int)(a.sorted_cell[g.first] >> (3 * kTL));
+  g.tz = t % c.ntz;
+  g.ty = (t / c.ntz) % c.nty;
+  g.tx = t / (c.ntz * c.nty);
+  return g;
+}
+
+// Slot ranges of the tile's halo cells: s_src[h] = first global slot,
+// s_off[h] = first staged slot (exclusive scan), s_off[kNH] = total.
+__device__ __forceinline__ uint32_t halo_table(const StepConsts& c, const TiledArgs& a, const TileGeom& g,
+                                               uint32_t* s_src, uint32_t* s_off, uint32_t* ws) {
+  const int h = threadIdx.x;
+  uint32_t cnt = 0, src = 0;
+  if (h < kNH) {
+    const int ax = g.tx * kTB - 1 + h / (kH * kH);
+    const int ay = g.ty * kTB - 1 + (h / kH) % kH;
+    const int az = g.tz * kTB - 1 + h % kH;
+    if (ax >= 0 && ay >= 0 && az >= 0 && ax < c.ncx && ay < c.ncy && az < c.ncz) {
+      const int lin = tiled_index(c, ax, ay, az);
+      src = a.cell_start[lin];
+      cnt = a.cell_start[lin + 1] - src;
+    }
+  }
+  uint32_t total;
+  const uint32_t off = block_scan(cnt, ws, total);
+  if (h < kNH) {
+    s_src[h] = src;
+    s_off[h] = off;
+  }
+  if (h == 0) s_off[kNH] = total;
+  __syncthreads();
+  return total;
+}
+
+// Tile-relative f32 position of a particle staged from halo cell h.
+__device__ __forceinline__ float4 tile_rel(const StepConsts& c, float4 q, int h) {
+  const float ox = (float)(h / (kH * kH) - 1) * c.h0f;
+  const float oy = (float)((h / kH) % kH - 1) * c.h0f;
+  const float oz = (float)(h % kH - 1) * c.h0f;
+  return make_float4(ox + q.x, oy + q.y, oz + q.z, q.w);
+}
+
+// Halo cell of a particle of the tile itself.
+__device__ __forceinline__ int own_halo_cell(uint32_t cell) {
+  const int u = (int)(cell & ((1u << (3 * kTL)) - 1u));
+  const int ux = u >> (2 * kTL), uy = (u >> kTL) & (kTB - 1), uz = u & (kTB - 1);
+  return ((ux + 1) * kH + (uy + 1)) * kH + (uz + 1);
+}
+
+// Warp-cooperative staging: warp w copies halo z-runs w, w+8, ... (6 cells
+// with fixed hx, hy; their staged slots are contiguous), lanes taking
+// consecutive slots so global reads coalesce.  `emit(slot, h, src)` stores
+// one particle read from global slot `src` of halo cell h.
+template <class Emit>
+__device__ __forceinline__ void stage_halo(const uint32_t* s_src, const uint32_t* s_off, Emit emit) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int run = warp; run < kH * kH; run += kTT / 32) {
+    const int h0 = run * kH;
+    const uint32_t b0 = s_off[h0], b6 = s_off[h0 + kH];
+    for (uint32_t k = b0 + lane; k < b6; k += 32) {
+      int hz = 0;
+#pragma unroll
+      for (int z = 1; z < kH; ++z) hz += k >= s_off[h0 + z] ? 1 : 0;
+      const int h = h0 + hz;
+      emit(k, h, s_src[h] + (k - s_off[h]));
+    }
+  }
+}
+
+__device__ __forceinline__ void write_density(const StepConsts& c, const TiledArgs& a, int qi, double rho) {
+  const double over = rho - c.rest;
+  const double pr = over > 0.0 ? c.stiff * over : 0.0;
+  a.rho[qi] = rho;
+  a.p[qi] = pr;
+  a.cvel[qi].w = (float)(pr / (rho * rho));
+  a.cmr[qi] = (float)(a.mass[qi] / rho);
+}
+
+// Density of particle qi from global memory (tiles that do not fit the
+// staging buffer): 27 cells by tiled index, cell-local offsets.
+__device__ void density_global(const StepConsts& c, const TiledArgs& a, int qi) {
+  const double xi = a.px[qi], yi = a.py[qi], zi = a.pz[qi];
+  const long long kx = key_axis(xi, c.inv_cell), ky = key_axis(yi, c.inv_cell), kz = key_axis(zi, c.inv_cell);
+  const float4 pi = a.cpos[qi];
+  const float hc2 = fminf(c.h2f, c.h0sqf);
+  float s = 0.f, comp = 0.f;
+  const int bx = (int)(kx - c.bx0), by = (int)(ky - c.by0), bz = (int)(kz - c.bz0);
+  for (int di = -1; di <= 1; ++di)
+    for (int dj = -1; dj <= 1; ++dj)
+      for (int dk = -1; dk <= 1; ++dk) {
+        const int lin = tiled_index(c, bx + di, by + dj, bz + dk);
+        const int s0 = (int)a.cell_start[lin], e0 = (int)a.cell_start[lin + 1];
+        const float ox = (float)di * c.h0f - pi.x, oy = (float)dj * c.h0f - pi.y, oz = (float)dk * c.h0f - pi.z;
+        float part = 0.f;
+        for (int j = s0; j < e0; ++j) {
+          const float4 q = a.cpos[j];
+          const float dx = ox + q.x, dy = oy + q.y, dz = oz + q.z;
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          const float t = r2 < hc2 ? c.h0sqf - r2 : 0.f;
+          part = fmaf(t * t, t * q.w, part);
+        }
+        kahan_add(s, comp, c.poly6_cf * part);
+      }
+  write_density(c, a, qi, (double)s - (double)comp);
+  a.nbr_count[qi] = kNoList;
+}
+
+template <bool kCount>
+__global__ void __launch_bounds__(kTT) k_density_tiled(StepConsts c, TiledArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float4* s_pos = reinterpret_cast<float4*>(smem);
+  uint16_t (*s_list)[kTT] = reinterpret_cast<uint16_t (*)[kTT]>(smem + kHaloCap * sizeof(float4));
+  uint32_t* s_src = reinterpret_cast<uint32_t*>(smem + kHaloCap * sizeof(float4) + kListRows * kTT * 2);
+  uint32_t* s_off = s_src + kNH;
+  uint32_t* ws = s_off + kNH + 1;
+  const float hc2 = fminf(c.h2f, c.h0sqf);
+  const uint32_t ntiles = *a.num_tiles;
+  unsigned cand = 0, pairs = 0;
+  for (uint32_t k = blockIdx.x; k < ntiles; k += gridDim.x) {
+    const TileGeom g = tile_geom(c, a, k);
+    const uint32_t total = halo_table(c, a, g, s_src, s_off, ws);
+    if (total > (uint32_t)min(c.halo_cap, kHaloCap)) {
+      for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT) density_global(c, a, (int)qi);
+      continue;  // uniform across the CTA
+    }
+    stage_halo(s_src, s_off, [&](uint32_t slot, int h, uint32_t src) { s_pos[slot] = tile_rel(c, a.cpos[src], h); });
+    __syncthreads();
+    for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT) {
+      const int hq = own_halo_cell(a.sorted_cell[qi]);
+      const uint32_t si = s_off[hq] + (qi - s_src[hq]);
+      const float4 pi = s_pos[si];
+      float s = 0.f, comp = 0.f;
+      uint32_t cnt = 0;
+#pragma unroll
+      for (int di = -1; di <= 1; ++di) {
+#pragma unroll
+        for (int dj = -1; dj <= 1; ++dj) {
+          const int h0 = hq + di * kH * kH + dj * kH - 1;  // cells h0 .. h0+2 (dk = -1, 0, 1)
+          const uint32_t s0 = s_off[h0], e0 = s_off[h0 + 3];
+          if (kCount) cand += e0 - s0;
+          float part = 0.f;
+#pragma unroll 4
+          for (uint32_t j = s0; j < e0; ++j) {
+            const float4 q = s_pos[j];
+            const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            const float t = r2 < hc2 ? c.h0sqf - r2 : 0.f;
+            part = fmaf(t * t, t * q.w, part);
+            if (kCount) pairs += r2 < hc2 ? 1u : 0u;
+            // Branchless append: the row index saturates at the spare row.
+            s_list[min(cnt, (uint32_t)kMaxNeighbors)][threadIdx.x] = (uint16_t)j;
+            cnt += r2 >= hc2 ? 0u : 1u;
+          }
+          kahan_add(s, comp, c.poly6_cf * part);
+        }
+      }
+      // Coalesced write-out: at step e the warp stores 32 consecutive entries.
+      {
+        uint16_t* lst = a.nbr16 + qi;
+        const unsigned am = __activemask();
+        const uint32_t mine = min(cnt, (uint32_t)kMaxNeighbors);
+        const uint32_t kmax = __reduce_max_sync(am, mine);
+        for (uint32_t e = 0; e < kmax; ++e)
+          if (e < mine) lst[(size_t)e * a.stride] = s_list[e][threadIdx.x];
+      }
+      a.nbr_count[qi] = cnt;
+      write_density(c, a, (int)qi, (double)s - (double)comp);
+    }
+    __syncthreads();
+  }
+  // Particles of the overflow cell (outside the grid box): no neighbours.
+  const uint32_t end = a.tile_slot[ntiles];
+  for (uint32_t qi = end + blockIdx.x * kTT + threadIdx.x; qi < (uint32_t)c.n; qi += gridDim.x * kTT) {
+    write_density(c, a, (int)qi, 0.0);
+    a.nbr_count[qi] = 0;
+  }
+  if (kCount) {
+    const unsigned wc = __reduce_add_sync(0xffffffffu, cand);
+    const unsigned wp = __reduce_add_sync(0xffffffffu, pairs);
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(&a.counters[0], (unsigned long long)wc);
+      atomicAdd(&a.counters[1], (unsigned long long)wp);
+    }
+  }
+}
+
+struct CompAcc {
+  float fpx = 0.f, fpy = 0.f, fpz = 0.f, cpx = 0.f, cpy = 0.f, cpz = 0.f;
+  float fvx = 0.f, fvy = 0.f, fvz = 0.f, cvx = 0.f, cvy = 0.f, cvz = 0.f;
+  float xsx = 0.f, xsy = 0.f, xsz = 0.f, shear = 0.f;
+};
+
+// One neighbour pair (compute_forces' loop body, world.rs:291-316) in f32.
+__device__ __forceinline__ void pair_f32(const StepConsts& c, float dx, float dy, float dz, float m_j, float4 vj,
+                                         float mr_j, float4 vi, float m_i, float pr2_i, CompAcc& q) {
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  if (!(r2 < fminf(c.h2f, c.h0sqf)) || r2 <= 0.0f) return;
+  const float inv_r = rsqrtf(r2);
+  const float r = r2 * inv_r;
+  const float hr = c.h0f - r;
+  const float fp = (m_i * m_j) * (pr2_i + vj.w) * (c.spiky_cf * hr * hr) * inv_r;
+  kahan_add(q.fpx, q.cpx, dx * fp);
+  kahan_add(q.fpy, q.cpy, dy * fp);
+  kahan_add(q.fpz, q.cpz, dz * fp);
+  const float dvx = vj.x - vi.x, dvy = vj.y - vi.y, dvz = vj.z - vi.z;
+  const float vf = m_i * mr_j * (c.lap_cf * hr);
+  kahan_add(q.fvx, q.cvx, dvx * vf);
+  kahan_add(q.fvy, q.cvy, dvy * vf);
+  kahan_add(q.fvz, q.cvz, dvz * vf);
+  const float t = c.h0sqf - r2;
+  const float xw = mr_j * (c.poly6_cf * t * t * t);
+  q.xsx = fmaf(dvx, xw, q.xsx);
+  q.xsy = fmaf(dvy, xw, q.xsy);
+  q.xsz = fmaf(dvz, xw, q.xsz);
+  const float dvn = sqrtf(dvx * dvx + dvy * dvy + dvz * dvz);
+  q.shear = fmaf(__fdividef(dvn, r + 1e-4f), mr_j, q.shear);
+}
+
+// mu_eff, acc, integrate and bounds in f64 (world.rs:319-397).
+__device__ __forceinline__ void finish_particle(const StepConsts& c, const TiledArgs& a, int i, const CompAcc& q) {
+  const double rho_i = a.rho[i];
+  const uint32_t m = a.mat[i];
+  const int midx = (int)m < c.n_visc_k ? (int)m : 0;
+  double kc, nn;
+  material_coeffs(c, midx, kc, nn);
+  const double ex = nn - 1.0;
+  const double sh = (double)q.shear;
+  const double sreg = sh > c.shear_min ? sh : c.shear_min;
+  const double mu = kc * (ex == 0.0 ? 1.0 : pow(sreg, ex));
+  double ax = 0.0, ay = 0.0, az = 0.0;
+  if (rho_i > 0.0) {
+    ax = (((double)q.fpx - (double)q.cpx) + ((double)q.fvx - (double)q.cvx) * mu) / rho_i;
+    ay = (((double)q.fpy - (double)q.cpy) + ((double)q.fvy - (double)q.cvy) * mu) / rho_i;
+    az = (((double)q.fpz - (double)q.cpz) + ((double)q.fvz - (double)q.cvz) * mu) / rho_i;
+  }
+  a.acc[0][i] = ax;
+  a.acc[1][i] = ay;
+  a.acc[2][i] = az;
+  a.xsph[0][i] = q.xsx;
+  a.xsph[1][i] = q.xsy;
+  a.xsph[2][i] = q.xsz;
+  a.mu[i] = mu;
+  double b3[3] = {0.0, 0.0, 0.0};
+  if (a.bax) {
+    b3[0] = a.bax[i];
+    b3[1] = a.bay[i];
+    b3[2] = a.baz[i];
+    a.bax[i] = 0.0;
+    a.bay[i] = 0.0;
+    a.baz[i] = 0.0;
+  }
+  double p3[3] = {a.px[i], a.py[i], a.pz[i]};
+  double v3[3] = {a.vx[i], a.vy[i], a.vz[i]};
+  const double acc3[3] = {ax, ay, az};
+  const double xs3[3] = {(double)q.xsx, (double)q.xsy, (double)q.xsz};
+  bool finite = true;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    double v = v3[k] + ((acc3[k] + c.g[k]) + b3[k]) * c.dt;
+    v = v + xs3[k] * c.xsph_eps;
+    double x = p3[k] + v * c.dt;
+    if (x < c.lo[k]) {
+      x = c.lo[k];
+      v = -v * c.damp;
+    } else if (x > c.hi[k]) {
+      x = c.hi[k];
+      v = -v * c.damp;
+    }
+    finite = finite && isfinite(x) && isfinite(v);
+    a.out_pv[k][i] = x;
+    a.out_pv[3 + k][i] = v;
+  }
+  if (!finite) atomicOr(a.flags, kFlagNonFinite);
+}
+
+// Forces of particle qi from global memory (tiles that were not staged).
+__device__ void force_global(const StepConsts& c, const TiledArgs& a, int qi) {
+  const double xi = a.px[qi], yi = a.py[qi], zi = a.pz[qi];
+  const long long kx = key_axis(xi, c.inv_cell), ky = key_axis(yi, c.inv_cell), kz = key_axis(zi, c.inv_cell);
+  const float4 pi = a.cpos[qi];
+  const float4 vi = a.cvel[qi];
+  CompAcc q;
+  const int bx = (int)(kx - c.bx0), by = (int)(ky - c.by0), bz = (int)(kz - c.bz0);
+  for (int di = -1; di <= 1; ++di)
+    for (int dj = -1; dj <= 1; ++dj)
+      for (int dk = -1; dk <= 1; ++dk) {
+        const int lin = tiled_index(c, bx + di, by + dj, bz + dk);
+        const int s0 = (int)a.cell_start[lin], e0 = (int)a.cell_start[lin + 1];
+        const float ox = (float)di * c.h0f - pi.x, oy = (float)dj * c.h0f - pi.y, oz = (float)dk * c.h0f - pi.z;
+        for (int j = s0; j < e0; ++j) {
+          if (j == qi) continue;
+          const float4 pj = a.cpos[j];
+          pair_f32(c, ox + pj.x, oy + pj.y, oz + pj.z, pj.w, a.cvel[j], a.cmr[j], vi, pi.w, vi.w, q);
+        }
+      }
+  finish_particle(c, a, qi, q);
+}
+
+__global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float4* s_pos = reinterpret_cast<float4*>(smem);
+  float4* s_vel = s_pos + kHaloCap;
+  float* s_mr = reinterpret_cast<float*>(s_vel + kHaloCap);
+  uint32_t* s_src = reinterpret_cast<uint32_t*>(s_mr + kHaloCap);
+  uint32_t* s_off = s_src + kNH;
+  uint32_t* ws = s_off + kNH + 1;
+  const uint32_t ntiles = *a.num_tiles;
+  for (uint32_t k = blockIdx.x; k < ntiles; k += gridDim.x) {
+    const TileGeom g = tile_geom(c, a, k);
+    const uint32_t total = halo_table(c, a, g, s_src, s_off, ws);
+    if (total > (uint32_t)min(c.halo_cap, kHaloCap)) {
+      for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT) force_global(c, a, (int)qi);
+      continue;
+    }
+    stage_halo(s_src, s_off, [&](uint32_t slot, int h, uint32_t src) {
+      s_pos[slot] = tile_rel(c, a.cpos[src], h);
+      s_vel[slot] = a.cvel[src];
+      s_mr[slot] = a.cmr[src];
+    });
+    __syncthreads();
+    for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT) {
+      const int hq = own_halo_cell(a.sorted_cell[qi]);
+      const uint32_t si = s_off[hq] + (qi - s_src[hq]);
+      const float4 pi = s_pos[si];
+      const float4 vi = s_vel[si];
+      CompAcc q;
+      const uint32_t cnt = a.nbr_count[qi];
+      if (cnt <= (uint32_t)kMaxNeighbors) {
+        const uint16_t* lst = a.nbr16 + qi;
+        const size_t st = (size_t)a.stride;
+        uint32_t e = 0;
+        // Four list entries per batch: their loads are independent.
+        for (; e + 4 <= cnt; e += 4) {
+          const uint32_t j0 = lst[e * st], j1 = lst[(e + 1) * st], j2 = lst[(e + 2) * st], j3 = lst[(e + 3) * st];
+          const uint32_t js[4] = {j0, j1, j2, j3};
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float4 pj = s_pos[js[u]];
+            pair_f32(c, pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, pj.w, s_vel[js[u]], s_mr[js[u]], vi, pi.w, vi.w, q);
+          }
+        }
+        for (; e < cnt; ++e) {
+          const uint32_t j = lst[e * st];
+          const float4 pj = s_pos[j];
+          pair_f32(c, pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, pj.w, s_vel[j], s_mr[j], vi, pi.w, vi.w, q);
+        }
+      } else {
+        // List overflow: rescan the 27 staged cells.
+        for (int di = -1; di <= 1; ++di)
+          for (int dj = -1; dj <= 1; ++dj) {
+            const int h0 = hq + di * kH * kH + dj * kH - 1;
+            for (uint32_t j = s_off[h0]; j < s_off[h0 + 3]; ++j) {
+              if (j == si) continue;
+              const float4 pj = s_pos[j];
+              pair_f32(c, pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, pj.w, s_vel[j], s_mr[j], vi, pi.w, vi.w, q);
+            }
+          }
+      }
+      finish_particle(c, a, (int)qi, q);
+    }
+    __syncthreads();
+  }
+  const uint32_t end = a.tile_slot[ntiles];
+  for (uint32_t qi = end + blockIdx.x * kTT + threadIdx.x; qi < (uint32_t)c.n; qi += gridDim.x * kTT) {
+    CompAcc q;
+    finish_particle(c, a, (int)qi, q);
+  }
+}
+
+// Cell-local f32 operands of every particle (as in step_comp.cu).
+__global__ void __launch_bounds__(256) k_prep_tiled(StepConsts c, TiledArgs a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c.n) return;
+  const double x = a.px[i], y = a.py[i], z = a.pz[i];
+  const long long kx = key_axis(x, c.inv_cell);
+  const long long ky = key_axis(y, c.inv_cell);
+  const long long kz = key_axis(z, c.inv_cell);
+  a.cpos[i] = make_float4((float)(x - (double)kx * c.h0), (float)(y - (double)ky * c.h0),
+                          (float)(z - (double)kz * c.h0), (float)a.mass[i]);
+  a.cvel[i] = make_float4((float)a.vx[i], (float)a.vy[i], (float)a.vz[i], 0.0f);
+}
+
+constexpr size_t kDensitySmem = kHaloCap * sizeof(float4) + kListRows * kTT * 2 + (2 * kNH + 1 + 32) * 4;
+constexpr size_t kForceSmem = kHaloCap * (2 * sizeof(float4) + sizeof(float)) + (2 * kNH + 1 + 32) * 4;
+
+struct Persistent {
+  int density_blocks = 0, force_blocks = 0;
+};
+
+Persistent persistent_grid() {
+  static Persistent p;
+  static bool done = false;
+  if (!done) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(k_density_tiled<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDensitySmem);
+    cudaFuncSetAttribute(k_density_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDensitySmem);
+    cudaFuncSetAttribute(k_force_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kForceSmem);
+    int bd = 0, bf = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bd, k_density_tiled<false>, kTT, kDensitySmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force_tiled, kTT, kForceSmem);
+    p.density_blocks = sms * std::max(bd, 1);
+    p.force_blocks = sms * std::max(bf, 1);
+    done = true;
+  }
+  return p;
+}
+
+}  // namespace
+
+void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const PassEvents& ev) {
+  const ParticleConsts& pc = b.pc[b.cur];
+  TiledArgs a;
+  a.px = b.pv0[0];
+  a.py = b.pv0[1];
+  a.pz = b.pv0[2];
+  a.vx = b.pv0[3];
+  a.vy = b.pv0[4];
+  a.vz = b.pv0[5];
+  a.mass = pc.mass;
+  a.mat = pc.mat;
+  a.cell_start = b.cell_start;
+  a.sorted_cell = b.sorted_cell;
+  a.tile_slot = b.tile_slot;
+  a.num_tiles = b.num_tiles;
+  a.cpos = b.cpos;
+  a.cvel = b.cvel;
+  a.cmr = b.cmr;
+  a.bax = b.has_ba ? pc.ba[0] : nullptr;
+  a.bay = b.has_ba ? pc.ba[1] : nullptr;
+  a.baz = b.has_ba ? pc.ba[2] : nullptr;
+  a.rho = b.rho;
+  a.p = b.p;
+  for (int k = 0; k < 3; ++k) {
+    a.acc[k] = b.acc[k];
+    a.xsph[k] = b.xsph[k];
+  }
+  a.mu = b.mu;
+  for (int k = 0; k < 6; ++k) a.out_pv[k] = b.pv1[k];
+  a.nbr16 = b.nbr16;
+  a.nbr_count = b.nbr_count;
+  a.stride = b.capacity;
+  a.flags = b.flags;
+  a.counters = b.counters;
+  const Persistent pg = persistent_grid();
+  k_prep_tiled<<<(c.n + 255) / 256, 256, 0, s>>>(c, a);
+  if (ev.after_prep) cudaEventRecord(ev.after_prep, s);
+  if (a.counters)
+    k_density_tiled<true><<<pg.density_blocks, kTT, kDensitySmem, s>>>(c, a);
+  else
+    k_density_tiled<false><<<pg.density_blocks, kTT, kDensitySmem, s>>>(c, a);
+  if (ev.after_density) cudaEventRecord(ev.after_density, s);
+  k_force_tiled<<<pg.force_blocks, kTT, kForceSmem, s>>>(c, a);
+}
+
+}  // namespace phy

@@ -312,6 +312,15 @@ class FluidWorld:
         L.check(self._lib.phy_fluid_step_counters(self._h, self._sub, out), "phy_fluid_step_counters")
         return {"candidates": out[0], "pairs": out[1], "particles": out[2], "cells": out[3]}
 
+    def set_tuning(self, comp_tile: Optional[int] = None, halo_cap: Optional[int] = None) -> None:
+        """Kernel configuration (phy_fluid_set_tuning); results of the f64 form never change."""
+        if comp_tile is not None:
+            L.check(self._lib.phy_fluid_set_tuning(self._h, self._sub, L.TUNE_COMP_TILE, comp_tile),
+                    "phy_fluid_set_tuning")
+        if halo_cap is not None:
+            L.check(self._lib.phy_fluid_set_tuning(self._h, self._sub, L.TUNE_HALO_CAP, halo_cap),
+                    "phy_fluid_set_tuning")
+
     def set_timing(self, on: bool) -> None:
         L.check(self._lib.phy_fluid_set_timing(self._h, self._sub, 1 if on else 0), "phy_fluid_set_timing")
 
