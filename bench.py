@@ -197,6 +197,15 @@ def run_ours(args):
     p_err = float(np.max(np.abs(probe.p - plain.p)) / (params.stiffness * params.rest_density))
     del probe
 
+    # ---- the full configured trajectory (1000 steps from the initial dam) ---------------
+    full = None
+    traj = None
+    if args.full_steps > 0:
+        traj = new_world("comp")
+        ms_full, _ = timed(traj, args.full_steps, 0)
+        full = {"steps": args.full_steps, "value": world_size * n * args.full_steps / (ms_full / 1e3),
+                "ms_per_step": ms_full / args.full_steps}
+
     # ---- per-kernel device times (CUDA events on the launch stream) ----------------
     def phases(w, steps):
         w.set_timing(True)
@@ -209,6 +218,14 @@ def run_ours(args):
 
     ph_comp = phases(comp, min(K, 50))
     ph_plain = phases(plain, min(k_plain, 10))
+    if traj is not None:
+        full["phase_ms_at_end"] = phases(traj, 20)
+        traj.set_counting(True)
+        traj.step(DT)
+        tc = traj.step_counters()
+        full["pairs_per_particle_at_end"] = tc["pairs"] / n
+        traj.set_counting(False)
+        del traj
     comp.set_counting(True)
     comp.step(DT)
     cnt = comp.step_counters()
@@ -267,6 +284,7 @@ def run_ours(args):
                 "l2": "inputs larger than L2 (state ~1.4 GB per replica)",
             },
             "plain_f64": {"value": plain_value, "ms_per_step": ms_plain / k_plain, "steps": k_plain},
+            "full_trajectory": full,
             "ratio_comp_vs_plain": value / plain_value,
             "density_err_max_rel": dens_err,
             "pressure_err_norm": p_err,
@@ -379,6 +397,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--full-steps", type=int, default=1000,
+                    help="also time this many steps from the initial dam (the configured 1000-step run; "
+                         "the column compresses and splashes, so per-step cost changes along it); 0 = skip")
     ap.add_argument("--dims", type=int, nargs=3, default=list(DIMS),
                     help="lattice of the dam block (default 128 256 128 = 4,194,304 particles); smaller blocks "
                          "are for profiling captures only")

@@ -18,9 +18,10 @@
 namespace phy {
 
 constexpr int kMaxMaterials = 16;
-// Neighbour-list capacity per particle (in-range pairs; ~31 at rest density
-// with spacing h/2, ~40 under strong compression).
-constexpr int kMaxNeighbors = 64;
+// Neighbour-list capacity per particle (in-range pairs: ~31 at rest density
+// with spacing h/2, ~60 at twice the rest density, which the bottom of a
+// tall column reaches with the default stiffness).
+constexpr int kMaxNeighbors = 96;
 // f32-compensated lists pack the 27-cell offset code under the index.
 constexpr int kCodeBits = 5;
 // The first kStagedNeighbors entries of a list are staged in shared memory

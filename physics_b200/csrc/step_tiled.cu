@@ -32,8 +32,7 @@ constexpr int kTL = 2;                          // log2(kTB)
 constexpr int kH = kTB + 2;                     // halo edge (cells)
 constexpr int kNH = kH * kH * kH;               // halo cells
 constexpr int kTT = 256;                        // threads per CTA
-constexpr int kHaloCap = 2048;                  // staged particles per tile
-constexpr int kListRows = kMaxNeighbors + 1;    // smem list rows (+1 row absorbs overflow writes)
+constexpr int kHaloCap = 2000;                  // staged slots per tile (3 force CTAs fit an SM)
 static_assert(kNH <= kTT, "one halo cell per thread");
 static_assert(kHaloCap <= 65536, "16-bit slots");
 
@@ -75,6 +74,35 @@ struct TiledArgs {
   uint32_t* flags;
   unsigned long long* counters;
 };
+
+// Packed f32x2 arithmetic (sm_100): two lanes of a 64-bit register pair per
+// instruction.
+struct f2 {
+  unsigned long long v;
+};
+__device__ __forceinline__ f2 f2_pack(float a, float b) {
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(f2 r, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r.v));
+}
+__device__ __forceinline__ f2 f2_sub(f2 a, f2 b) {
+  f2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ f2 f2_mul(f2 a, f2 b) {
+  f2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c) {
+  f2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return r;
+}
 
 // nbr_count value of a particle whose tile was not staged (force rescans).
 constexpr uint32_t kNoList = 0xffffffffu;
@@ -122,10 +150,12 @@ __device__ __forceinline__ TileGeom tile_geom(const StepConsts& c, const TiledAr
   return g;
 }
 
-// Slot ranges of the tile's halo cells: s_src[h] = first global slot,
-// s_off[h] = first staged slot (exclusive scan), s_off[kNH] = total.
+// Slot ranges of the tile's halo cells: s_src[h] / s_end[h] = global slot
+// range, s_off[h] = first staged slot; every cell's staged range is padded to
+// an even length (one far-away dummy particle), so all runs are pair-aligned.
+// s_off[kNH] = total staged slots.
 __device__ __forceinline__ uint32_t halo_table(const StepConsts& c, const TiledArgs& a, const TileGeom& g,
-                                               uint32_t* s_src, uint32_t* s_off, uint32_t* ws) {
+                                               uint32_t* s_src, uint32_t* s_end, uint32_t* s_off, uint32_t* ws) {
   const int h = threadIdx.x;
   uint32_t cnt = 0, src = 0;
   if (h < kNH) {
@@ -139,9 +169,10 @@ __device__ __forceinline__ uint32_t halo_table(const StepConsts& c, const TiledA
     }
   }
   uint32_t total;
-  const uint32_t off = block_scan(cnt, ws, total);
+  const uint32_t off = block_scan((cnt + 1u) & ~1u, ws, total);
   if (h < kNH) {
     s_src[h] = src;
+    s_end[h] = src + cnt;
     s_off[h] = off;
   }
   if (h == 0) s_off[kNH] = total;
@@ -168,29 +199,49 @@ __device__ __forceinline__ int own_halo_cell(uint32_t cell) {
 // with fixed hx, hy; their staged slots are contiguous), lanes taking
 // consecutive slots so global reads coalesce.  `emit(slot, h, src)` stores
 // one particle read from global slot `src` of halo cell h.
-template <class Emit>
-__device__ __forceinline__ void stage_halo(const uint32_t* s_src, const uint32_t* s_off, Emit emit) {
+template <class Emit, class Dummy>
+__device__ __forceinline__ void stage_halo(const uint32_t* s_src, const uint32_t* s_end, const uint32_t* s_off,
+                                           int run_lo, int run_hi, uint32_t base, Emit emit, Dummy dummy) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int run = warp; run < kH * kH; run += kTT / 32) {
+  for (int run = run_lo + warp; run < run_hi; run += kTT / 32) {
     const int h0 = run * kH;
     const uint32_t b0 = s_off[h0], b6 = s_off[h0 + kH];
+#pragma unroll 2
     for (uint32_t k = b0 + lane; k < b6; k += 32) {
       int hz = 0;
 #pragma unroll
       for (int z = 1; z < kH; ++z) hz += k >= s_off[h0 + z] ? 1 : 0;
       const int h = h0 + hz;
-      emit(k, h, s_src[h] + (k - s_off[h]));
+      const uint32_t src = s_src[h] + (k - s_off[h]);
+      if (src < s_end[h])
+        emit(k - base, h, src);
+      else
+        dummy(k - base);
     }
   }
+}
+
+// Slab decomposition of a tile whose whole halo does not fit the staging
+// buffer: the core is processed in x-slabs of `slab` cell layers, each with
+// the (slab+2) x 6 x 6-cell halo (a contiguous halo-index range).  Returns
+// the thickest slab (4, 2 or 1) whose halos all fit, or 0 (none fits).
+__device__ __forceinline__ int pick_slab(const uint32_t* s_off, uint32_t cap) {
+  constexpr int L = kH * kH;  // halo cells per x-layer
+  if (s_off[kNH] <= cap) return kTB;
+  if (s_off[4 * L] - s_off[0] <= cap && s_off[6 * L] - s_off[2 * L] <= cap) return 2;
+  for (int x0 = 0; x0 < kTB; ++x0)
+    if (s_off[(x0 + 3) * L] - s_off[x0 * L] > cap) return 0;
+  return 1;
 }
 
 __device__ __forceinline__ void write_density(const StepConsts& c, const TiledArgs& a, int qi, double rho) {
   const double over = rho - c.rest;
   const double pr = over > 0.0 ? c.stiff * over : 0.0;
+  const double inv = 1.0 / rho;
   a.rho[qi] = rho;
   a.p[qi] = pr;
-  a.cvel[qi].w = (float)(pr / (rho * rho));
-  a.cmr[qi] = (float)(a.mass[qi] / rho);
+  a.cvel[qi].w = (float)(pr * inv * inv);
+  a.cmr[qi] = (float)(a.mass[qi] * inv);
 }
 
 // Density of particle qi from global memory (tiles that do not fit the
@@ -222,68 +273,124 @@ __device__ void density_global(const StepConsts& c, const TiledArgs& a, int qi) 
   a.nbr_count[qi] = kNoList;
 }
 
+// Staged density operands: slots 2p and 2p+1 share two float4s,
+// (x0, x1, y0, y1) and (z0, z1, m0, m1), so a pair of candidates loads into
+// 64-bit register pairs ready for f32x2 arithmetic.
+__device__ __forceinline__ void put_pair_slot(float* sp, uint32_t k, float4 v) {
+  float* base = sp + (k >> 1) * 8 + (k & 1);
+  base[0] = v.x;
+  base[2] = v.y;
+  base[4] = v.z;
+  base[6] = v.w;
+}
+
+constexpr float kFar = 1.0e18f;  // dummy particle coordinate (never in range)
+
+// Appends 16-bit neighbour slots to a particle's row-major list (row of
+// kMaxNeighbors entries) through a 64-bit register accumulator flushed with
+// 8-byte stores; entries past kMaxNeighbors are dropped (the count still
+// grows and the force pass then rescans).
+struct ListWriter {
+  uint16_t* row;
+  unsigned long long acc = 0;
+  uint32_t n = 0;
+  __device__ __forceinline__ void push(uint32_t slot) {
+    acc |= (unsigned long long)slot << (16 * (n & 3));
+    ++n;
+    if ((n & 3) == 0) {
+      if (n <= (uint32_t)kMaxNeighbors) *reinterpret_cast<unsigned long long*>(row + n - 4) = acc;
+      acc = 0;
+    }
+  }
+  __device__ __forceinline__ void finish() {
+    if ((n & 3) && n < (uint32_t)kMaxNeighbors) *reinterpret_cast<unsigned long long*>(row + (n & ~3u)) = acc;
+  }
+};
+
 template <bool kCount>
 __global__ void __launch_bounds__(kTT) k_density_tiled(StepConsts c, TiledArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
-  float4* s_pos = reinterpret_cast<float4*>(smem);
-  uint16_t (*s_list)[kTT] = reinterpret_cast<uint16_t (*)[kTT]>(smem + kHaloCap * sizeof(float4));
-  uint32_t* s_src = reinterpret_cast<uint32_t*>(smem + kHaloCap * sizeof(float4) + kListRows * kTT * 2);
-  uint32_t* s_off = s_src + kNH;
+  float* s_pp = reinterpret_cast<float*>(smem);  // kHaloCap slots, pair-interleaved
+  uint32_t* s_src = reinterpret_cast<uint32_t*>(smem + kHaloCap * sizeof(float4));
+  uint32_t* s_end = s_src + kNH;
+  uint32_t* s_off = s_end + kNH;
   uint32_t* ws = s_off + kNH + 1;
   const float hc2 = fminf(c.h2f, c.h0sqf);
+  const f2 H0SQ = f2_pack(c.h0sqf, c.h0sqf);
   const uint32_t ntiles = *a.num_tiles;
   unsigned cand = 0, pairs = 0;
   for (uint32_t k = blockIdx.x; k < ntiles; k += gridDim.x) {
     const TileGeom g = tile_geom(c, a, k);
-    const uint32_t total = halo_table(c, a, g, s_src, s_off, ws);
-    if (total > (uint32_t)min(c.halo_cap, kHaloCap)) {
+    halo_table(c, a, g, s_src, s_end, s_off, ws);
+    const int slab = pick_slab(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
+    if (slab == 0) {
       for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT) density_global(c, a, (int)qi);
       continue;  // uniform across the CTA
     }
-    stage_halo(s_src, s_off, [&](uint32_t slot, int h, uint32_t src) { s_pos[slot] = tile_rel(c, a.cpos[src], h); });
+    for (int x0 = 0; x0 < kTB; x0 += slab) {
+    const uint32_t base = s_off[x0 * kH * kH];
+    stage_halo(
+        s_src, s_end, s_off, x0 * kH, (x0 + slab + 2) * kH, base,
+        [&](uint32_t slot, int h, uint32_t src) { put_pair_slot(s_pp, slot, tile_rel(c, a.cpos[src], h)); },
+        [&](uint32_t slot) { put_pair_slot(s_pp, slot, make_float4(kFar, kFar, kFar, 0.f)); });
     __syncthreads();
-    for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT) {
+    const float4* s_pp4 = reinterpret_cast<const float4*>(s_pp);
+    const uint32_t qfirst = s_src[((x0 + 1) * kH + 1) * kH + 1];
+    const uint32_t qlast = s_end[((x0 + slab) * kH + kTB) * kH + kTB];
+    for (uint32_t qi = qfirst + threadIdx.x; qi < qlast; qi += kTT) {
       const int hq = own_halo_cell(a.sorted_cell[qi]);
-      const uint32_t si = s_off[hq] + (qi - s_src[hq]);
-      const float4 pi = s_pos[si];
+      const uint32_t si = s_off[hq] - base + (qi - s_src[hq]);
+      const float* own = s_pp + (si >> 1) * 8 + (si & 1);
+      const f2 PX = f2_pack(own[0], own[0]), PY = f2_pack(own[2], own[2]), PZ = f2_pack(own[4], own[4]);
       float s = 0.f, comp = 0.f;
-      uint32_t cnt = 0;
+      ListWriter lw;
+      lw.row = a.nbr16 + (size_t)qi * kMaxNeighbors;
 #pragma unroll
       for (int di = -1; di <= 1; ++di) {
 #pragma unroll
         for (int dj = -1; dj <= 1; ++dj) {
           const int h0 = hq + di * kH * kH + dj * kH - 1;  // cells h0 .. h0+2 (dk = -1, 0, 1)
-          const uint32_t s0 = s_off[h0], e0 = s_off[h0 + 3];
-          if (kCount) cand += e0 - s0;
-          float part = 0.f;
-#pragma unroll 4
-          for (uint32_t j = s0; j < e0; ++j) {
-            const float4 q = s_pos[j];
-            const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            const float t = r2 < hc2 ? c.h0sqf - r2 : 0.f;
-            part = fmaf(t * t, t * q.w, part);
-            if (kCount) pairs += r2 < hc2 ? 1u : 0u;
-            // Branchless append: the row index saturates at the spare row.
-            s_list[min(cnt, (uint32_t)kMaxNeighbors)][threadIdx.x] = (uint16_t)j;
-            cnt += r2 >= hc2 ? 0u : 1u;
+          const uint32_t s0 = s_off[h0] - base, e0 = s_off[h0 + 3] - base;  // both even
+          if (kCount) cand += (s_end[h0] - s_src[h0]) + (s_end[h0 + 1] - s_src[h0 + 1]) + (s_end[h0 + 2] - s_src[h0 + 2]);
+          f2 PART = f2_pack(0.f, 0.f);
+          for (uint32_t cb = s0; cb < e0; cb += 32) {
+            const uint32_t ce = min(cb + 32u, e0);
+            uint32_t mask = 0;
+#pragma unroll 2
+            for (uint32_t j = cb; j < ce; j += 2) {
+              const float4 A = s_pp4[j];      // x0 x1 y0 y1
+              const float4 B = s_pp4[j + 1];  // z0 z1 m0 m1
+              const f2 DX = f2_sub(f2_pack(A.x, A.y), PX);
+              const f2 DY = f2_sub(f2_pack(A.z, A.w), PY);
+              const f2 DZ = f2_sub(f2_pack(B.x, B.y), PZ);
+              const f2 R2 = f2_fma(DZ, DZ, f2_fma(DY, DY, f2_mul(DX, DX)));
+              float r0, r1;
+              f2_unpack(R2, r0, r1);
+              const bool in0 = r0 < hc2, in1 = r1 < hc2;
+              float t0, t1;
+              f2_unpack(f2_sub(H0SQ, R2), t0, t1);
+              const f2 T = f2_pack(in0 ? t0 : 0.f, in1 ? t1 : 0.f);
+              PART = f2_fma(f2_mul(T, T), f2_mul(T, f2_pack(B.z, B.w)), PART);
+              mask |= ((in0 ? 1u : 0u) | (in1 ? 2u : 0u)) << (j - cb);
+            }
+            if (kCount) pairs += __popc(mask);
+            while (mask) {
+              const uint32_t b = __ffs(mask) - 1;
+              mask &= mask - 1;
+              lw.push(cb + b);
+            }
           }
-          kahan_add(s, comp, c.poly6_cf * part);
+          float p0, p1;
+          f2_unpack(PART, p0, p1);
+          kahan_add(s, comp, c.poly6_cf * (p0 + p1));
         }
       }
-      // Coalesced write-out: at step e the warp stores 32 consecutive entries.
-      {
-        uint16_t* lst = a.nbr16 + qi;
-        const unsigned am = __activemask();
-        const uint32_t mine = min(cnt, (uint32_t)kMaxNeighbors);
-        const uint32_t kmax = __reduce_max_sync(am, mine);
-        for (uint32_t e = 0; e < kmax; ++e)
-          if (e < mine) lst[(size_t)e * a.stride] = s_list[e][threadIdx.x];
-      }
-      a.nbr_count[qi] = cnt;
+      lw.finish();
+      a.nbr_count[qi] = lw.n;
       write_density(c, a, (int)qi, (double)s - (double)comp);
     }
     __syncthreads();
+    }  // slabs
   }
   // Particles of the overflow cell (outside the grid box): no neighbours.
   const uint32_t end = a.tile_slot[ntiles];
@@ -346,9 +453,10 @@ __device__ __forceinline__ void finish_particle(const StepConsts& c, const Tiled
   const double mu = kc * (ex == 0.0 ? 1.0 : pow(sreg, ex));
   double ax = 0.0, ay = 0.0, az = 0.0;
   if (rho_i > 0.0) {
-    ax = (((double)q.fpx - (double)q.cpx) + ((double)q.fvx - (double)q.cvx) * mu) / rho_i;
-    ay = (((double)q.fpy - (double)q.cpy) + ((double)q.fvy - (double)q.cvy) * mu) / rho_i;
-    az = (((double)q.fpz - (double)q.cpz) + ((double)q.fvz - (double)q.cvz) * mu) / rho_i;
+    const double inv = 1.0 / rho_i;
+    ax = (((double)q.fpx - (double)q.cpx) + ((double)q.fvx - (double)q.cvx) * mu) * inv;
+    ay = (((double)q.fpy - (double)q.cpy) + ((double)q.fvy - (double)q.cvy) * mu) * inv;
+    az = (((double)q.fpz - (double)q.cpz) + ((double)q.fvz - (double)q.cvz) * mu) * inv;
   }
   a.acc[0][i] = ax;
   a.acc[1][i] = ay;
@@ -413,69 +521,137 @@ __device__ void force_global(const StepConsts& c, const TiledArgs& a, int qi) {
   finish_particle(c, a, qi, q);
 }
 
+// Batch partial sums of the pressure and raw viscous forces; folded into the
+// Kahan-compensated totals every four pairs.
+struct ForcePart {
+  float fx = 0.f, fy = 0.f, fz = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+};
+
+__device__ __forceinline__ void fold(CompAcc& q, ForcePart& b) {
+  kahan_add(q.fpx, q.cpx, b.fx);
+  kahan_add(q.fpy, q.cpy, b.fy);
+  kahan_add(q.fpz, q.cpz, b.fz);
+  kahan_add(q.fvx, q.cvx, b.vx);
+  kahan_add(q.fvy, q.cvy, b.vy);
+  kahan_add(q.fvz, q.cvz, b.vz);
+  b = ForcePart();
+}
+
+// One listed neighbour (r < min(h, h0) by construction; r == 0, i.e. i
+// itself or a coincident particle, contributes nothing, as the reference
+// skips r <= 0).  Branchless.
+__device__ __forceinline__ void pair_listed(const StepConsts& c, float4 pj, float4 vj, float mr_j, float4 pi,
+                                            float4 vi, float lapm_i, ForcePart& b, CompAcc& q) {
+  const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  const bool pos = r2 > 0.f;
+  const float inv_r = pos ? rsqrtf(r2) : 0.f;
+  const float mr = pos ? mr_j : 0.f;
+  const float r = r2 * inv_r;
+  const float hr = c.h0f - r;
+  // (d/r) * m_i m_j (p_i/rho_i^2 + p_j/rho_j^2) * spiky(r)
+  const float fp = (pi.w * pj.w) * (vi.w + vj.w) * (c.spiky_cf * hr) * (hr * inv_r);
+  b.fx = fmaf(dx, fp, b.fx);
+  b.fy = fmaf(dy, fp, b.fy);
+  b.fz = fmaf(dz, fp, b.fz);
+  // dv * (m_i m_j / rho_j * lap(r))
+  const float dvx = vj.x - vi.x, dvy = vj.y - vi.y, dvz = vj.z - vi.z;
+  const float vf = lapm_i * mr * hr;
+  b.vx = fmaf(dvx, vf, b.vx);
+  b.vy = fmaf(dvy, vf, b.vy);
+  b.vz = fmaf(dvz, vf, b.vz);
+  // XSPH: dv * (m_j / rho_j * poly6(r))
+  const float t = c.h0sqf - r2;
+  const float xw = (mr * c.poly6_cf) * (t * t * t);
+  q.xsx = fmaf(dvx, xw, q.xsx);
+  q.xsy = fmaf(dvy, xw, q.xsy);
+  q.xsz = fmaf(dvz, xw, q.xsz);
+  // strain-rate proxy: |dv| / (r + 1e-4) * m_j / rho_j
+  const float dv2 = dvx * dvx + dvy * dvy + dvz * dvz;
+  const float dvn = dv2 > 0.f ? dv2 * rsqrtf(dv2) : 0.f;
+  q.shear = fmaf(__fdividef(dvn, r + 1e-4f), mr, q.shear);
+}
+
 __global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
-  float4* s_pos = reinterpret_cast<float4*>(smem);
-  float4* s_vel = s_pos + kHaloCap;
-  float* s_mr = reinterpret_cast<float*>(s_vel + kHaloCap);
+  float4* s_rec = reinterpret_cast<float4*>(smem);  // slot k: [2k] = position, [2k+1] = velocity
+  float* s_mr = reinterpret_cast<float*>(s_rec + 2 * kHaloCap);
   uint32_t* s_src = reinterpret_cast<uint32_t*>(s_mr + kHaloCap);
-  uint32_t* s_off = s_src + kNH;
+  uint32_t* s_end = s_src + kNH;
+  uint32_t* s_off = s_end + kNH;
   uint32_t* ws = s_off + kNH + 1;
+  const float hc2 = fminf(c.h2f, c.h0sqf);
   const uint32_t ntiles = *a.num_tiles;
   for (uint32_t k = blockIdx.x; k < ntiles; k += gridDim.x) {
     const TileGeom g = tile_geom(c, a, k);
-    const uint32_t total = halo_table(c, a, g, s_src, s_off, ws);
-    if (total > (uint32_t)min(c.halo_cap, kHaloCap)) {
+    halo_table(c, a, g, s_src, s_end, s_off, ws);
+    const int slab = pick_slab(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
+    if (slab == 0) {
       for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT) force_global(c, a, (int)qi);
       continue;
     }
-    stage_halo(s_src, s_off, [&](uint32_t slot, int h, uint32_t src) {
-      s_pos[slot] = tile_rel(c, a.cpos[src], h);
-      s_vel[slot] = a.cvel[src];
-      s_mr[slot] = a.cmr[src];
-    });
+    for (int x0 = 0; x0 < kTB; x0 += slab) {
+    const uint32_t base = s_off[x0 * kH * kH];
+    stage_halo(
+        s_src, s_end, s_off, x0 * kH, (x0 + slab + 2) * kH, base,
+        [&](uint32_t slot, int h, uint32_t src) {
+          s_rec[2 * slot] = tile_rel(c, a.cpos[src], h);
+          s_rec[2 * slot + 1] = a.cvel[src];
+          s_mr[slot] = a.cmr[src];
+        },
+        [&](uint32_t slot) {
+          s_rec[2 * slot] = make_float4(kFar, kFar, kFar, 0.f);
+          s_rec[2 * slot + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+          s_mr[slot] = 0.f;
+        });
     __syncthreads();
-    for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT) {
+    const uint32_t qfirst = s_src[((x0 + 1) * kH + 1) * kH + 1];
+    const uint32_t qlast = s_end[((x0 + slab) * kH + kTB) * kH + kTB];
+    for (uint32_t qi = qfirst + threadIdx.x; qi < qlast; qi += kTT) {
       const int hq = own_halo_cell(a.sorted_cell[qi]);
-      const uint32_t si = s_off[hq] + (qi - s_src[hq]);
-      const float4 pi = s_pos[si];
-      const float4 vi = s_vel[si];
+      const uint32_t si = s_off[hq] - base + (qi - s_src[hq]);
+      const float4 pi = s_rec[2 * si];
+      const float4 vi = s_rec[2 * si + 1];
+      const float lapm_i = pi.w * c.lap_cf;
       CompAcc q;
+      ForcePart b;
       const uint32_t cnt = a.nbr_count[qi];
       if (cnt <= (uint32_t)kMaxNeighbors) {
-        const uint16_t* lst = a.nbr16 + qi;
-        const size_t st = (size_t)a.stride;
-        uint32_t e = 0;
-        // Four list entries per batch: their loads are independent.
-        for (; e + 4 <= cnt; e += 4) {
-          const uint32_t j0 = lst[e * st], j1 = lst[(e + 1) * st], j2 = lst[(e + 2) * st], j3 = lst[(e + 3) * st];
-          const uint32_t js[4] = {j0, j1, j2, j3};
+        // Row-major list: 8 entries per 16-byte load, the next load issued
+        // before the current eight pairs are computed.
+        const uint4* row = reinterpret_cast<const uint4*>(a.nbr16 + (size_t)qi * kMaxNeighbors);
+        uint4 cur = cnt > 0 ? row[0] : make_uint4(0, 0, 0, 0);
+        for (uint32_t e0 = 0; e0 < cnt; e0 += 8) {
+          const uint4 nxt = e0 + 8 < cnt ? row[(e0 >> 3) + 1] : cur;
+          const uint32_t w[4] = {cur.x, cur.y, cur.z, cur.w};
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const float4 pj = s_pos[js[u]];
-            pair_f32(c, pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, pj.w, s_vel[js[u]], s_mr[js[u]], vi, pi.w, vi.w, q);
+          for (int u = 0; u < 8; ++u) {
+            if (e0 + u < cnt) {
+              const uint32_t j = (w[u >> 1] >> (16 * (u & 1))) & 0xffffu;
+              pair_listed(c, s_rec[2 * j], s_rec[2 * j + 1], s_mr[j], pi, vi, lapm_i, b, q);
+            }
+            if (u == 3 || u == 7) fold(q, b);
           }
-        }
-        for (; e < cnt; ++e) {
-          const uint32_t j = lst[e * st];
-          const float4 pj = s_pos[j];
-          pair_f32(c, pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, pj.w, s_vel[j], s_mr[j], vi, pi.w, vi.w, q);
+          cur = nxt;
         }
       } else {
-        // List overflow: rescan the 27 staged cells.
+        // List overflow: rescan the 27 staged cells with the cutoff test.
         for (int di = -1; di <= 1; ++di)
           for (int dj = -1; dj <= 1; ++dj) {
             const int h0 = hq + di * kH * kH + dj * kH - 1;
-            for (uint32_t j = s_off[h0]; j < s_off[h0 + 3]; ++j) {
-              if (j == si) continue;
-              const float4 pj = s_pos[j];
-              pair_f32(c, pj.x - pi.x, pj.y - pi.y, pj.z - pi.z, pj.w, s_vel[j], s_mr[j], vi, pi.w, vi.w, q);
+            for (uint32_t j = s_off[h0] - base; j < s_off[h0 + 3] - base; ++j) {
+              const float4 pj = s_rec[2 * j];
+              const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+              if (!(dx * dx + dy * dy + dz * dz < hc2)) continue;
+              pair_listed(c, pj, s_rec[2 * j + 1], s_mr[j], pi, vi, lapm_i, b, q);
+              fold(q, b);
             }
           }
       }
       finish_particle(c, a, (int)qi, q);
     }
     __syncthreads();
+    }  // slabs
   }
   const uint32_t end = a.tile_slot[ntiles];
   for (uint32_t qi = end + blockIdx.x * kTT + threadIdx.x; qi < (uint32_t)c.n; qi += gridDim.x * kTT) {
@@ -497,8 +673,8 @@ __global__ void __launch_bounds__(256) k_prep_tiled(StepConsts c, TiledArgs a) {
   a.cvel[i] = make_float4((float)a.vx[i], (float)a.vy[i], (float)a.vz[i], 0.0f);
 }
 
-constexpr size_t kDensitySmem = kHaloCap * sizeof(float4) + kListRows * kTT * 2 + (2 * kNH + 1 + 32) * 4;
-constexpr size_t kForceSmem = kHaloCap * (2 * sizeof(float4) + sizeof(float)) + (2 * kNH + 1 + 32) * 4;
+constexpr size_t kDensitySmem = kHaloCap * sizeof(float4) + (3 * kNH + 1 + 32) * 4;
+constexpr size_t kForceSmem = kHaloCap * (2 * sizeof(float4) + sizeof(float)) + (3 * kNH + 1 + 32) * 4;
 
 struct Persistent {
   int density_blocks = 0, force_blocks = 0;

@@ -51,7 +51,7 @@ def test_density_error_gate_teacher_forced(gpu, oracle_mod, dims, presteps):
     assert e["rho_rel"] <= RHO_TOL, e
     assert e["p_norm"] <= 1e-5, e
     assert e["acc_rel_to_max"] <= 1e-3, e
-    assert e["pos_abs"] <= 1e-9, e
+    assert e["pos_abs"] <= 1e-8, e  # 1e-7 of the particle spacing
 
 
 def test_comp_run_to_run_deterministic(gpu):
@@ -156,3 +156,31 @@ def test_tiled_sparse_and_out_of_bounds_particles(gpu, oracle_mod):
     ok = fin & (ro > 0)
     assert np.max(np.abs(rg[ok] - ro[ok]) / ro[ok]) <= RHO_TOL
     assert np.isfinite(w.pos[fin]).all()
+
+
+@pytest.mark.parametrize("spacing,halo_cap", [(0.08, None), (0.08, 2500), (0.068, None)])
+def test_compressed_regimes(gpu, oracle_mod, spacing, halo_cap):
+    """Compressed fluid, as at the bottom of a tall column: ~16 particles per cell
+    (spacing 0.08) makes a tile's halo too large to stage whole, so the tile is processed
+    in x-slabs of 1 or 2 cell layers; at spacing 0.068 lists exceed their capacity and the
+    force pass rescans.  Density gate and force agreement against the oracle."""
+    O = oracle_mod
+    p = ref_test_params(gravity=(0.0, 0.0, 0.0))
+    rng = np.random.default_rng(4)
+    n = int(1.2 / spacing)
+    g = (np.arange(n) + 0.5) * spacing - 0.6
+    pos = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    pos += rng.uniform(-0.05, 0.05, pos.shape) * spacing
+    vel = rng.normal(0, 0.2, pos.shape)
+    ow = O.OracleWorld(p, threads=O.max_threads())
+    ow.add_particles(pos, 0.9, vel=vel)
+    w = gpu.FluidWorld(p, "comp")
+    w.set_tuning(halo_cap=halo_cap)
+    w.add_particles(pos, 0.9, vel=vel)
+    w.set_counting(True)
+    ow.step(0.001)
+    w.step(0.001)
+    e = errors(w, O, ow, p)
+    cnt = w.step_counters()
+    print("compressed", spacing, halo_cap, e, cnt["pairs"] / len(pos))
+    assert e["rho_rel"] <= RHO_TOL and e["acc_rel_to_max"] <= 1e-3, e
