@@ -160,6 +160,35 @@ int32_t phy_fluid_phase_times(PhyWorldHandle *w, uint32_t sub, double *out5, int
 enum { PHY_TUNE_COMP_TILE = 0, PHY_TUNE_HALO_CAP = 1 };
 int32_t phy_fluid_set_tuning(PhyWorldHandle *w, uint32_t sub, int32_t param, int64_t value);
 
+/* Scratch capacity of phy_fluid_density_noalloc. */
+#define PHY_NOALLOC_MAX_PARTICLES 65536
+#define PHY_NOALLOC_MAX_CELLS 262144
+
+/* Density and pressure of n particles in caller-owned device buffers,
+ * computed without allocating any device memory.  This entry point has no
+ * counterpart in the reference: it is for callers that cannot allocate on
+ * the device at that moment (an engine that owns all device memory and gives
+ * plugins only its own buffers, a process whose allocator policy forbids
+ * foreign cudaMalloc/cudaFree, a latency-critical loop that must not enter the
+ * driver's allocator).  Inputs: pos (3n doubles, xyz interleaved) and mass
+ * (n); outputs: rho and p (n doubles each); all device pointers, caller
+ * order.  The values are bit-identical to the density pass of the f64 plain
+ * step (FluidWorld<f64>::compute_density_pressure, world.rs:204-246) with
+ * kernel coefficients and grid cell taken from params->h.
+ *   Limits: n <= PHY_NOALLOC_MAX_PARTICLES and a cell-key bounding box (plus
+ * one cell on each side) of at most PHY_NOALLOC_MAX_CELLS cells; larger
+ * inputs return -1 and phy_fluid_last_error() says why.
+ *   Scratch: one fixed 4 MiB array in device memory that every GPU which
+ * loads the library holds until the process exits.  All calls share it and
+ * it keeps the last call's contents, so calls that overlap on the GPU (other
+ * threads or streams on the same device) race; serialise them.  The first
+ * call on a device looks up the array's address with that device current;
+ * make that first call before any stream capture.  The call works on the
+ * given cudaStream_t (NULL: the legacy default stream) and returns after that
+ * stream has finished.  Returns 0 or -1. */
+int32_t phy_fluid_density_noalloc(const PhySphParams *params, uint64_t n, const double *pos,
+                                  const double *mass, double *rho, double *p, void *cuda_stream);
+
 /* Message of the last failing call on this thread ("" if none). */
 const char *phy_fluid_last_error(void);
 

@@ -19,6 +19,9 @@ PRECISION_F32_COMP = 1
 TUNE_COMP_TILE = 0
 TUNE_HALO_CAP = 1
 
+NOALLOC_MAX_PARTICLES = 65536
+NOALLOC_MAX_CELLS = 262144
+
 FIELD_POS = 0
 FIELD_VEL = 1
 FIELD_ACC = 2
@@ -112,6 +115,8 @@ SIGNATURES = {
     "phy_fluid_set_timing": (C.c_int32, [H, C.c_uint32, C.c_int32]),
     "phy_fluid_phase_times": (C.c_int32, [H, C.c_uint32, DP, C.c_int32]),
     "phy_fluid_set_tuning": (C.c_int32, [H, C.c_uint32, C.c_int32, C.c_int64]),
+    "phy_fluid_density_noalloc": (C.c_int32, [C.POINTER(PhySphParams), C.c_uint64, C.c_void_p, C.c_void_p,
+                                              C.c_void_p, C.c_void_p, C.c_void_p]),
     "phy_fluid_last_error": (C.c_char_p, []),
 }
 

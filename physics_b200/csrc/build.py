@@ -30,11 +30,12 @@ NVCC_COMMON = ARCH + [
 # Per-file flags: the f64 plain passes must not contract a*b+c into an FMA.
 PER_FILE = {
     "step_plain.cu": ["-fmad=false"],
+    "noalloc.cu": ["-fmad=false"],
     "grid.cu": ["-fmad=false"],
     "fluid_world.cu": ["-fmad=false"],
 }
 SOURCES = ["grid.cu", "step_plain.cu", "step_comp.cu", "step_tiled.cu", "fluid_world.cu", "ffi.cpp",
-           "checkpoint.cpp"]
+           "checkpoint.cpp", "noalloc.cu"]
 
 
 def _nvcc() -> str:

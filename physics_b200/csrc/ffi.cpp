@@ -94,6 +94,10 @@ uintptr_t read_vec(PhyWorldHandle* w, T* buf, uintptr_t len, int field) {
 
 }  // namespace
 
+namespace phy {
+void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+}  // namespace phy
+
 extern "C" {
 
 uint32_t phy_ffi_abi_version(void) { return PHY_FFI_ABI_VERSION; }
