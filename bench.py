@@ -117,6 +117,90 @@ def make_params(pb):
     return p
 
 
+BATCH_DT = 0.005
+BATCH_CHUNK = 10  # steps per captured CUDA graph
+
+
+def run_batched(pb, scenes, stream, n_scenes: int, steps: int, warmup: int) -> dict:
+    """The batched form: n_scenes independent dam breaks (log-uniform 2k..200k particles,
+    aspect U[0.5,2], fill U[0.2,0.5]) in one world, one sort and one persistent launch per
+    pass, steps captured in CUDA graphs, launch knobs from the library's autotuner; against
+    looping the single-scene step over the same scenes (each scene its own world and
+    phy_fluid_step call)."""
+    import torch
+    batch = scenes.batch_scenes(n_scenes)
+    counts = [b.n for b in batch]
+    total = int(sum(counts))
+    mass = scenes.lattice_mass(scenes.SPACING)
+    p = pb.SphParams.defaults()
+    w = pb.FluidWorld(p, "comp")
+    w.set_stream(stream.cuda_stream)
+    w.add_particles(np.concatenate([b.pos for b in batch]), np.full(total, mass))
+    w.set_scenes(counts, [b.bounds_min for b in batch], [b.bounds_max for b in batch])
+    w.set_tuning(graph_chunk=BATCH_CHUNK)
+    t0 = time.time()
+    trials = w.autotune(BATCH_DT, BATCH_CHUNK)
+    tune_s = time.time() - t0
+    chosen = w.tuning()
+
+    def timed(fn, k):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn(k)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    w.step(BATCH_DT, max(warmup, BATCH_CHUNK))
+    ms = timed(lambda k: w.step(BATCH_DT, k), steps)
+    # The same batch without graph capture.
+    w.set_tuning(graph_chunk=0)
+    k_eager = max(BATCH_CHUNK, steps // 4)
+    ms_eager = timed(lambda k: w.step(BATCH_DT, k), k_eager)
+    del w
+    # Looping the single-scene step: one world per scene, default configuration.
+    worlds = []
+    for b in batch:
+        q = pb.SphParams.defaults()
+        q.bounds_min, q.bounds_max = b.bounds_min, b.bounds_max
+        ws = pb.FluidWorld(q, "comp")
+        ws.set_stream(stream.cuda_stream)
+        ws.add_particles(b.pos, np.full(b.n, mass))
+        worlds.append(ws)
+    for ws in worlds:
+        ws.step(BATCH_DT, warmup)
+
+    def loop(k):
+        for ws in worlds:
+            ws.step(BATCH_DT, k)
+
+    ms_loop = timed(loop, steps)
+    del worlds
+    value = total * steps / (ms / 1e3)
+    loop_value = total * steps / (ms_loop / 1e3)
+    return {
+        "workload": f"{n_scenes} dam-break scenes, {total} particles (log-uniform 2000..200000 per scene, "
+                    f"aspect U[0.5,2], fill U[0.2,0.5]), dt={BATCH_DT}, FP32-compensated",
+        "scenes": n_scenes,
+        "particles": total,
+        "steps": steps,
+        "value": value,
+        "unit": UNIT,
+        "ms_per_step": ms / steps,
+        "graph_chunk": BATCH_CHUNK,
+        "eager_value": total * k_eager / (ms_eager / 1e3),
+        "loop_single_scene_value": loop_value,
+        "loop_single_scene_ms_per_step": ms_loop / steps,
+        "speedup_vs_loop": value / loop_value,
+        "tuning": {k: chosen[k] for k in ("ctas_per_sm", "queue", "sort_block", "graph_chunk")},
+        "autotune": {"trials": len(trials), "seconds": tune_s,
+                     "best_ms_per_step": min(t["ms_per_step"] for t in trials),
+                     "worst_ms_per_step": max(t["ms_per_step"] for t in trials)},
+    }
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -231,6 +315,10 @@ def run_ours(args):
     cnt = comp.step_counters()
     comp.set_counting(False)
 
+    batched = None
+    if args.batch_scenes > 0 and args.batch_steps > 0:
+        batched = run_batched(pb, scenes, stream, args.batch_scenes, args.batch_steps, W)
+
     # ---- end to end through the C ABI with host buffers ------------------------------
     pin_pos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
     pin_vel = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
@@ -315,6 +403,7 @@ def run_ours(args):
             "gpu_launches": launches_per_step * K,
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if world_size > 1:
@@ -397,6 +486,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--batch-scenes", type=int, default=256, help="scenes of the batched form (0: skip)")
+    ap.add_argument("--batch-steps", type=int, default=200, help="timed steps of the batched form")
     ap.add_argument("--full-steps", type=int, default=1000,
                     help="also time this many steps from the initial dam (the configured 1000-step run; "
                          "the column compresses and splashes, so per-step cost changes along it); 0 = skip")

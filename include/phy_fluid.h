@@ -152,13 +152,67 @@ int32_t phy_fluid_set_timing(PhyWorldHandle *w, uint32_t sub, int32_t on);
 int32_t phy_fluid_phase_times(PhyWorldHandle *w, uint32_t sub, double *out5, int32_t reset);
 
 /* Kernel configuration of `sub` (no effect on the f64 plain form's results):
- *   PHY_TUNE_COMP_TILE  0 = x-major cell runs, 4 = staged 4x4x4-cell tiles
- *                       (default) for the FP32-compensated passes;
- *   PHY_TUNE_HALO_CAP   staged particles per tile halo before a tile is
- *                       computed from global memory (default: the kernels'
- *                       capacity). */
-enum { PHY_TUNE_COMP_TILE = 0, PHY_TUNE_HALO_CAP = 1 };
+ *   PHY_TUNE_COMP_TILE    0 = x-major cell runs, 4 = staged 4x4x4-cell tiles
+ *                         (default) for the FP32-compensated passes;
+ *   PHY_TUNE_HALO_CAP     staged particles per tile halo before a tile is
+ *                         computed from global memory (default: the kernels'
+ *                         capacity).
+ * Launch knobs (results never depend on them):
+ *   PHY_TUNE_CTAS_PER_SM  resident CTAs per SM of the tiled passes'
+ *                         persistent grids (0 = occupancy limit, default);
+ *   PHY_TUNE_QUEUE        0 = static tile stride, 1 = device work queue;
+ *   PHY_TUNE_SORT_BLOCK   threads per block of the sort's per-particle
+ *                         kernels (32..256, default 256);
+ *   PHY_TUNE_GRAPH_CHUNK  0 = launch every step (default); k > 0 = capture
+ *                         runs of k steps of phy_fluid_step into a CUDA graph
+ *                         once and replay it (re-captured when parameters,
+ *                         dt, the particle set or a buffer change).
+ * phy_fluid_get_tuning reads the same parameters. */
+enum {
+  PHY_TUNE_COMP_TILE = 0,
+  PHY_TUNE_HALO_CAP = 1,
+  PHY_TUNE_CTAS_PER_SM = 2,
+  PHY_TUNE_QUEUE = 3,
+  PHY_TUNE_SORT_BLOCK = 4,
+  PHY_TUNE_GRAPH_CHUNK = 5
+};
 int32_t phy_fluid_set_tuning(PhyWorldHandle *w, uint32_t sub, int32_t param, int64_t value);
+int32_t phy_fluid_get_tuning(PhyWorldHandle *w, uint32_t sub, int32_t param, int64_t *out);
+
+/* Batched scenes (no counterpart in the reference, which steps one scene per
+ * FluidWorld).  Partitions the subsystem's particles, in insertion order,
+ * into n_scenes consecutive scenes of counts[s] particles with their own wall
+ * bounds (bounds_min / bounds_max: 3 doubles per scene, replacing
+ * SphParams::bounds_* for that scene) and their own grid box.  Every
+ * phy_fluid_step then advances all scenes with one sort and one persistent
+ * launch per pass; scenes never interact and share every other parameter.
+ * Each scene's result is bit-identical to the same scene stepped alone in a
+ * world of the same form and kernel configuration.  FP32-compensated tiled
+ * form only; afterwards phy_fluid_add_particles fails until
+ * phy_fluid_clear_scenes.  1 <= n_scenes <= 65535; the counts must add up to
+ * the particle count.  Returns 0, -1 (bad arguments) or 5 (the boxes exceed
+ * 2^27 cells). */
+int32_t phy_fluid_set_scenes(PhyWorldHandle *w, uint32_t sub, uint32_t n_scenes, const uint64_t *counts,
+                             const double *bounds_min, const double *bounds_max);
+int32_t phy_fluid_clear_scenes(PhyWorldHandle *w, uint32_t sub);
+uint32_t phy_fluid_scene_count(PhyWorldHandle *w, uint32_t sub);
+
+/* One autotuner candidate: launch knobs and the measured device time. */
+typedef struct PhyTuneTrial {
+  int32_t ctas_per_sm;
+  int32_t queue;
+  int32_t sort_block;
+  int32_t reserved;
+  double ms_per_step;
+} PhyTuneTrial;
+
+/* Autotuner (no reference counterpart): times `steps` steps of dt for every
+ * combination of the launch knobs (sort block 128/256, static stride or work
+ * queue, 1..occupancy-limit CTAs per SM), each from the same saved state,
+ * restores that state, and keeps the fastest configuration.  Writes up to
+ * `cap` trials to out (may be NULL) and their number to *n_out. */
+int32_t phy_fluid_autotune(PhyWorldHandle *w, uint32_t sub, double dt, uint32_t steps, PhyTuneTrial *out,
+                           uint32_t cap, uint32_t *n_out);
 
 /* Scratch capacity of phy_fluid_density_noalloc. */
 #define PHY_NOALLOC_MAX_PARTICLES 65536

@@ -18,6 +18,12 @@ PRECISION_F32_COMP = 1
 
 TUNE_COMP_TILE = 0
 TUNE_HALO_CAP = 1
+TUNE_CTAS_PER_SM = 2
+TUNE_QUEUE = 3
+TUNE_SORT_BLOCK = 4
+TUNE_GRAPH_CHUNK = 5
+TUNE_PARAMS = {"comp_tile": TUNE_COMP_TILE, "halo_cap": TUNE_HALO_CAP, "ctas_per_sm": TUNE_CTAS_PER_SM,
+               "queue": TUNE_QUEUE, "sort_block": TUNE_SORT_BLOCK, "graph_chunk": TUNE_GRAPH_CHUNK}
 
 NOALLOC_MAX_PARTICLES = 65536
 NOALLOC_MAX_CELLS = 262144
@@ -34,6 +40,11 @@ FIELD_XSPH = 8
 FIELD_MATERIAL = 9
 FIELD_COMPONENTS = {FIELD_POS: 3, FIELD_VEL: 3, FIELD_ACC: 3, FIELD_BODY_ACC: 3, FIELD_RHO: 1, FIELD_P: 1,
                     FIELD_MASS: 1, FIELD_MU_EFF: 1, FIELD_XSPH: 3, FIELD_MATERIAL: 1}
+
+
+class PhyTuneTrial(C.Structure):
+    _fields_ = [("ctas_per_sm", C.c_int32), ("queue", C.c_int32), ("sort_block", C.c_int32),
+                ("reserved", C.c_int32), ("ms_per_step", C.c_double)]
 
 
 class PhySphParams(C.Structure):
@@ -115,6 +126,12 @@ SIGNATURES = {
     "phy_fluid_set_timing": (C.c_int32, [H, C.c_uint32, C.c_int32]),
     "phy_fluid_phase_times": (C.c_int32, [H, C.c_uint32, DP, C.c_int32]),
     "phy_fluid_set_tuning": (C.c_int32, [H, C.c_uint32, C.c_int32, C.c_int64]),
+    "phy_fluid_get_tuning": (C.c_int32, [H, C.c_uint32, C.c_int32, C.POINTER(C.c_int64)]),
+    "phy_fluid_set_scenes": (C.c_int32, [H, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64), DP, DP]),
+    "phy_fluid_clear_scenes": (C.c_int32, [H, C.c_uint32]),
+    "phy_fluid_scene_count": (C.c_uint32, [H, C.c_uint32]),
+    "phy_fluid_autotune": (C.c_int32, [H, C.c_uint32, C.c_double, C.c_uint32, C.POINTER(PhyTuneTrial),
+                                       C.c_uint32, C.POINTER(C.c_uint32)]),
     "phy_fluid_density_noalloc": (C.c_int32, [C.POINTER(PhySphParams), C.c_uint64, C.c_void_p, C.c_void_p,
                                               C.c_void_p, C.c_void_p, C.c_void_p]),
     "phy_fluid_last_error": (C.c_char_p, []),

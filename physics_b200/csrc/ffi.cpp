@@ -20,6 +20,9 @@ using phy::FluidSubsystem;
 using phy::FluidWorld;
 using phy::Precision;
 using phy::SphParams;
+using phy::LaunchTuning;
+using phy::TuneTrial;
+using phy::Vec3;
 using phy::World;
 
 namespace {
@@ -294,8 +297,7 @@ int32_t phy_fluid_set_params(PhyWorldHandle* w, uint32_t sub, const PhySphParams
 
 int32_t phy_fluid_step(PhyWorldHandle* w, uint32_t sub, double dt, uint32_t n) {
   return guard<int32_t>(-1, [&] {
-    FluidWorld& fw = *sub_of(w, sub).world;
-    for (uint32_t k = 0; k < n; ++k) fw.step(dt);
+    sub_of(w, sub).world->step_n(dt, (int)n);
     return 0;
   });
 }
@@ -388,12 +390,105 @@ int32_t phy_fluid_phase_times(PhyWorldHandle* w, uint32_t sub, double* out5, int
 int32_t phy_fluid_set_tuning(PhyWorldHandle* w, uint32_t sub, int32_t param, int64_t value) {
   return guard<int32_t>(-1, [&] {
     FluidWorld& fw = *sub_of(w, sub).world;
-    if (param == PHY_TUNE_COMP_TILE)
-      fw.set_comp_tile((int)value);
-    else if (param == PHY_TUNE_HALO_CAP)
-      fw.set_halo_cap(value > (1 << 30) ? (1 << 30) : (int)value);
-    else
-      throw std::invalid_argument("unknown tuning parameter");
+    LaunchTuning t = fw.launch_tuning();
+    auto in_range = [&](int64_t lo, int64_t hi) {
+      if (value < lo || value > hi) throw std::invalid_argument("tuning value out of range");
+      return (int)value;
+    };
+    switch (param) {
+      case PHY_TUNE_COMP_TILE:
+        fw.set_comp_tile((int)value);
+        break;
+      case PHY_TUNE_HALO_CAP:
+        fw.set_halo_cap(value > (1 << 30) ? (1 << 30) : (int)value);
+        break;
+      case PHY_TUNE_CTAS_PER_SM:
+        t.ctas_per_sm = in_range(0, 64);
+        fw.set_launch_tuning(t);
+        break;
+      case PHY_TUNE_QUEUE:
+        t.queue = in_range(0, 1);
+        fw.set_launch_tuning(t);
+        break;
+      case PHY_TUNE_SORT_BLOCK:
+        t.sort_block = in_range(32, 256) / 32 * 32;
+        fw.set_launch_tuning(t);
+        break;
+      case PHY_TUNE_GRAPH_CHUNK:
+        fw.set_graph_chunk(in_range(0, 1 << 20));
+        break;
+      default:
+        throw std::invalid_argument("unknown tuning parameter");
+    }
+    return 0;
+  });
+}
+
+int32_t phy_fluid_get_tuning(PhyWorldHandle* w, uint32_t sub, int32_t param, int64_t* out) {
+  if (!out) return -1;
+  return guard<int32_t>(-1, [&] {
+    FluidWorld& fw = *sub_of(w, sub).world;
+    const LaunchTuning t = fw.launch_tuning();
+    switch (param) {
+      case PHY_TUNE_COMP_TILE: *out = fw.comp_tile(); break;
+      case PHY_TUNE_HALO_CAP: *out = fw.halo_cap(); break;
+      case PHY_TUNE_CTAS_PER_SM: *out = t.ctas_per_sm; break;
+      case PHY_TUNE_QUEUE: *out = t.queue; break;
+      case PHY_TUNE_SORT_BLOCK: *out = t.sort_block; break;
+      case PHY_TUNE_GRAPH_CHUNK: *out = fw.graph_chunk(); break;
+      default: throw std::invalid_argument("unknown tuning parameter");
+    }
+    return 0;
+  });
+}
+
+int32_t phy_fluid_set_scenes(PhyWorldHandle* w, uint32_t sub, uint32_t n_scenes, const uint64_t* counts,
+                             const double* bounds_min, const double* bounds_max) {
+  if (!counts || !bounds_min || !bounds_max) return -1;
+  return guard<int32_t>(-1, [&] {
+    FluidWorld& fw = *sub_of(w, sub).world;
+    std::vector<uint64_t> c(counts, counts + n_scenes);
+    std::vector<Vec3> lo(n_scenes), hi(n_scenes);
+    for (uint32_t s = 0; s < n_scenes; ++s) {
+      lo[s] = {bounds_min[3 * s], bounds_min[3 * s + 1], bounds_min[3 * s + 2]};
+      hi[s] = {bounds_max[3 * s], bounds_max[3 * s + 1], bounds_max[3 * s + 2]};
+    }
+    try {
+      fw.set_scenes(c, lo, hi);
+    } catch (const std::invalid_argument& e) {
+      if (std::string(e.what()).find("2^27") != std::string::npos) {
+        g_last_error = e.what();
+        return 5;
+      }
+      throw;
+    }
+    return 0;
+  });
+}
+
+int32_t phy_fluid_clear_scenes(PhyWorldHandle* w, uint32_t sub) {
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->clear_scenes();
+    return 0;
+  });
+}
+
+uint32_t phy_fluid_scene_count(PhyWorldHandle* w, uint32_t sub) {
+  return guard<uint32_t>(0u, [&] { return (uint32_t)sub_of(w, sub).world->scene_count(); });
+}
+
+int32_t phy_fluid_autotune(PhyWorldHandle* w, uint32_t sub, double dt, uint32_t steps, PhyTuneTrial* out,
+                           uint32_t cap, uint32_t* n_out) {
+  return guard<int32_t>(-1, [&] {
+    const std::vector<TuneTrial> trials = sub_of(w, sub).world->autotune(dt, (int)steps);
+    for (size_t k = 0; out && k < trials.size() && k < cap; ++k) {
+      out[k].ctas_per_sm = trials[k].tuning.ctas_per_sm;
+      out[k].queue = trials[k].tuning.queue;
+      out[k].sort_block = trials[k].tuning.sort_block;
+      out[k].reserved = 0;
+      out[k].ms_per_step = trials[k].ms_per_step;
+    }
+    if (n_out) *n_out = (uint32_t)trials.size();
     return 0;
   });
 }

@@ -117,6 +117,75 @@ __global__ void k_key_bbox(int n, const double* __restrict__ pos3, double inv, l
   }
 }
 
+// Scene of every slot from its insertion index: the scene whose insertion
+// range [pbase[s], pbase[s+1]) holds it.
+__global__ void k_scene_of_id(int n, const uint32_t* __restrict__ id, const uint32_t* __restrict__ pbase,
+                              int n_scenes, uint16_t* __restrict__ scene) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const uint32_t i = id[s];
+  int lo = 0, hi = n_scenes - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pbase[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  scene[s] = (uint16_t)lo;
+}
+
+// Cell-key bounding box of each scene's finite positions (interleaved xyz,
+// insertion order): one block per scene, out[7 s ..] = min xyz, max xyz,
+// non-finite flag.
+__global__ void __launch_bounds__(kThreads) k_scene_bbox(const double* __restrict__ pos3,
+                                                         const uint32_t* __restrict__ pbase, double inv,
+                                                         long long* __restrict__ out) {
+  const int sc = blockIdx.x;
+  long long mn[3] = {LLONG_MAX, LLONG_MAX, LLONG_MAX}, mx[3] = {LLONG_MIN, LLONG_MIN, LLONG_MIN};
+  int bad = 0;
+  for (uint32_t i = pbase[sc] + threadIdx.x; i < pbase[sc + 1]; i += kThreads) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double x = pos3[3 * (size_t)i + a];
+      if (!isfinite(x)) {
+        bad = 1;
+        continue;
+      }
+      const long long k = key_axis(x, inv);
+      mn[a] = k < mn[a] ? k : mn[a];
+      mx[a] = k > mx[a] ? k : mx[a];
+    }
+  }
+  __shared__ long long s_mn[3][kThreads / 32], s_mx[3][kThreads / 32];
+  __shared__ int s_bad[kThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const long long y = __shfl_xor_sync(0xffffffffu, mn[a], o);
+      const long long z = __shfl_xor_sync(0xffffffffu, mx[a], o);
+      mn[a] = y < mn[a] ? y : mn[a];
+      mx[a] = z > mx[a] ? z : mx[a];
+    }
+    if (lane == 0) {
+      s_mn[a][warp] = mn[a];
+      s_mx[a][warp] = mx[a];
+    }
+  }
+  bad = __any_sync(0xffffffffu, bad);
+  if (lane == 0) s_bad[warp] = bad;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long r[7] = {LLONG_MAX, LLONG_MAX, LLONG_MAX, LLONG_MIN, LLONG_MIN, LLONG_MIN, 0};
+    for (int w = 0; w < kThreads / 32; ++w) {
+      for (int a = 0; a < 3; ++a) {
+        r[a] = s_mn[a][w] < r[a] ? s_mn[a][w] : r[a];
+        r[3 + a] = s_mx[a][w] > r[3 + a] ? s_mx[a][w] : r[3 + a];
+      }
+      r[6] |= s_bad[w];
+    }
+    for (int k = 0; k < 7; ++k) out[7 * sc + k] = r[k];
+  }
+}
+
 // num-traits ToPrimitive::to_i64 on f64 with None -> 0 (grid.rs:25-33).
 long long key_axis_host(double x, double inv) {
   double f = std::floor(x * inv);
@@ -234,8 +303,12 @@ FluidWorld::FluidWorld(const SphParams& p, Precision prec) : params(p), prec_(pr
 
 FluidWorld::~FluidWorld() {
   if (stream_) cudaStreamSynchronize(stream_);
+  drop_graphs();
   free_all();
   dfree(d_bbox_);
+  dfree(d_pbase_);
+  dfree(d_scene_bbox_);
+  release_snapshot();
   for (auto& e : ev_)
     if (e) cudaEventDestroy(e);
   if (own_stream_) cudaStreamDestroy(own_stream_);
@@ -250,6 +323,7 @@ void FluidWorld::free_all() {
     dfree(b_.pc[q].mass);
     dfree(b_.pc[q].mat);
     dfree(b_.pc[q].id);
+    dfree(b_.pc[q].scene);
     for (int k = 0; k < 3; ++k) dfree(b_.pc[q].ba[k]);
   }
   dfree(b_.rho);
@@ -271,6 +345,8 @@ void FluidWorld::free_all() {
   dfree(b_.tile_head);
   dfree(b_.tile_slot);
   dfree(b_.num_tiles);
+  dfree(b_.boxes);
+  dfree(b_.queue);
   dfree(b_.cell_of);
   dfree(b_.rank);
   dfree(b_.tmp);
@@ -310,6 +386,7 @@ void FluidWorld::ensure_capacity(size_t n) {
     dgrow(b_.pc[q].id, keep, cap, s);
     if (b_.has_ba)
       for (int k = 0; k < 3; ++k) dgrow(b_.pc[q].ba[k], keep, cap, s);
+    if (b_.pc[q].scene) dgrow(b_.pc[q].scene, keep, cap, s);
   }
   dgrow(b_.rho, n_, cap, s);
   dgrow(b_.p, n_, cap, s);
@@ -337,6 +414,7 @@ void FluidWorld::ensure_capacity(size_t n) {
   dgrow(b_.perm, 0, cap, s);
   dgrow(b_.stage, 0, 8 * cap, s);
   b_.capacity = (int)cap;
+  ++alloc_gen_;
   ensure_mode_buffers();
 }
 
@@ -353,11 +431,14 @@ void FluidWorld::ensure_mode_buffers() {
     if (!b_.tile_head) dalloc(b_.tile_head, tile_head_length((int)cap));
     if (!b_.tile_slot) dalloc(b_.tile_slot, cap + 1);
     if (!b_.num_tiles) dalloc(b_.num_tiles, 1);
+    if (!b_.queue) dalloc(b_.queue, 2);
   }
+  ++alloc_gen_;
 }
 
 void FluidWorld::set_comp_tile(int t) {
   if (t != 0 && t != 4) throw std::invalid_argument("comp tile must be 0 (x-major runs) or 4");
+  if (t == 0 && !scenes_.empty()) throw std::invalid_argument("batched scenes need the tiled form (comp tile 4)");
   comp_tile_ = t;
   ensure_mode_buffers();
 }
@@ -454,32 +535,92 @@ void FluidWorld::merge_box(const long long* pmn, const long long* pmx, bool any_
 }
 
 // (Re)builds the dense box: keys [kmin-1, kmax+1] per axis, so that every
-// cell inside [kmin, kmax] has its 26 neighbours in the box.
+// cell inside [kmin, kmax] has its 26 neighbours in the box.  The tiled form
+// rounds each axis up to whole tiles and keeps a device table of scene boxes
+// (one box for a single world, one per scene of a batch, numbered
+// consecutively).
 void FluidWorld::ensure_cells() {
-  grow_box_with_bounds();
   tile_ = (prec_ == Precision::F32Comp) ? comp_tile_ : 0;
-  long long total = 1;
-  int nc[3];
-  for (int a = 0; a < 3; ++a) {
-    long long d = kmax_[a] - kmin_[a] + 3;
-    if (tile_) d = (d + tile_ - 1) / tile_ * tile_;
-    if (d > kMaxCells) throw std::invalid_argument("FluidWorld: grid box exceeds 2^27 cells");
-    nc[a] = (int)d;
-    total *= d;
-    if (total > kMaxCells)
-      throw std::invalid_argument("FluidWorld: bounds span more than 2^27 grid cells of size h");
-  }
-  for (int a = 0; a < 3; ++a) {
-    nc_[a] = nc[a];
-    bx0_[a] = kmin_[a] - 1;
+  auto box_dims = [&](const long long* kmin, const long long* kmax, int* nc) {
+    long long total = 1;
+    for (int a = 0; a < 3; ++a) {
+      long long d = kmax[a] - kmin[a] + 3;
+      if (tile_) d = (d + tile_ - 1) / tile_ * tile_;
+      if (d > kMaxCells) throw std::invalid_argument("FluidWorld: grid box exceeds 2^27 cells");
+      nc[a] = (int)d;
+      total *= d;
+      if (total > kMaxCells)
+        throw std::invalid_argument("FluidWorld: bounds span more than 2^27 grid cells of size h");
+    }
+    return total;
+  };
+  std::vector<SceneBox> boxes;
+  long long total = 0;
+  if (scenes_.empty()) {
+    grow_box_with_bounds();
+    int nc[3];
+    total = box_dims(kmin_, kmax_, nc);
+    for (int a = 0; a < 3; ++a) {
+      nc_[a] = nc[a];
+      bx0_[a] = kmin_[a] - 1;
+    }
+    if (tile_) {
+      SceneBox bx;
+      std::memset(&bx, 0, sizeof(bx));
+      const double lo[3] = {params.bounds_min.x, params.bounds_min.y, params.bounds_min.z};
+      const double hi[3] = {params.bounds_max.x, params.bounds_max.y, params.bounds_max.z};
+      for (int a = 0; a < 3; ++a) {
+        bx.b0[a] = bx0_[a];
+        bx.nc[a] = nc[a];
+        bx.nt[a] = nc[a] / tile_;
+        bx.lo[a] = lo[a];
+        bx.hi[a] = hi[a];
+      }
+      boxes.push_back(bx);
+    }
+  } else {
+    for (const Scene& sc : scenes_) {
+      SceneBox bx;
+      std::memset(&bx, 0, sizeof(bx));
+      int nc[3];
+      const long long cells = box_dims(sc.kmin, sc.kmax, nc);
+      const double lo[3] = {sc.lo.x, sc.lo.y, sc.lo.z}, hi[3] = {sc.hi.x, sc.hi.y, sc.hi.z};
+      for (int a = 0; a < 3; ++a) {
+        bx.b0[a] = sc.kmin[a] - 1;
+        bx.nc[a] = nc[a];
+        bx.nt[a] = nc[a] / tile_;
+        bx.lo[a] = lo[a];
+        bx.hi[a] = hi[a];
+      }
+      bx.cell_base = (int)total;
+      total += cells;
+      if (total > kMaxCells) throw std::invalid_argument("FluidWorld: the scenes' boxes exceed 2^27 cells");
+      boxes.push_back(bx);
+    }
   }
   ncells_ = (int)total;
+  if (!boxes.empty() &&
+      (boxes.size() != host_boxes_.size() ||
+       std::memcmp(boxes.data(), host_boxes_.data(), boxes.size() * sizeof(SceneBox)) != 0)) {
+    if ((int)boxes.size() > boxes_capacity_) {
+      cuda_check(cudaStreamSynchronize(stream_), "boxes sync");
+      dalloc(b_.boxes, boxes.size());
+      boxes_capacity_ = (int)boxes.size();
+      ++alloc_gen_;
+    }
+    host_boxes_ = boxes;
+    cuda_check(cudaMemcpyAsync(b_.boxes, host_boxes_.data(), host_boxes_.size() * sizeof(SceneBox),
+                               cudaMemcpyHostToDevice, stream_),
+               "boxes upload");
+    cuda_check(cudaStreamSynchronize(stream_), "boxes upload sync");
+  }
   if (ncells_ > b_.cell_capacity) {
     int cap = (int)std::min<long long>(kMaxCells, std::max<long long>(ncells_, (long long)b_.cell_capacity * 3 / 2));
     size_t scan_len = scan_block_sums_needed(cap) * 4096;
     cuda_check(cudaStreamSynchronize(stream_), "cells sync");
     dalloc(b_.cell_start, scan_len);
     b_.cell_capacity = cap;
+    ++alloc_gen_;
   }
   // The scan's tile sums serve the cell scan and the tile-head scan (n + 1
   // entries) alike.
@@ -489,6 +630,7 @@ void FluidWorld::ensure_cells() {
     cuda_check(cudaStreamSynchronize(stream_), "sums sync");
     dalloc(b_.block_sums, (size_t)sums);
     b_.block_sums_capacity = sums;
+    ++alloc_gen_;
   }
 }
 
@@ -534,6 +676,8 @@ StepConsts FluidWorld::make_consts(double dt) const {
   c.tile = tile_;
   c.tile_log2 = tile_ == 4 ? 2 : 0;
   c.halo_cap = halo_cap_;
+  c.boxes = tile_ ? b_.boxes : nullptr;
+  c.n_scenes = scenes_.empty() ? 1 : (int)scenes_.size();
   if (tile_) {
     c.ntx = nc_[0] / tile_;
     c.nty = nc_[1] / tile_;
@@ -595,6 +739,7 @@ void FluidWorld::add_particles(size_t m, const double* pos, const double* vel, c
                                const uint32_t* material) {
   if (m == 0) return;
   if (!pos || !mass) throw std::invalid_argument("add_particles: pos and mass are required");
+  if (!scenes_.empty()) throw std::invalid_argument("add_particles: the world holds batched scenes (clear_scenes first)");
   ensure_capacity(n_ + m);
   // Staging layout: pos 3m | vel 3m | mass m | material m (as doubles).
   std::vector<double> st(8 * m, 0.0);
@@ -703,11 +848,17 @@ void FluidWorld::set_field(int field, const double* in) {
   cuda_check(cudaMemcpyAsync(st, in, (size_t)nc * n_ * sizeof(double), cudaMemcpyHostToDevice, stream_),
              "set_field copy");
   // New positions may widen the grid box; checked before the state changes.
-  if (field == PHY_FIELD_POS) grow_box_with_device_positions(n_, st);
+  if (field == PHY_FIELD_POS) {
+    if (scenes_.empty())
+      grow_box_with_device_positions(n_, st);
+    else
+      grow_scene_boxes(st);
+  }
   if (field == PHY_FIELD_BODY_ACC && !b_.has_ba) {
     for (int q = 0; q < 2; ++q)
       for (int k = 0; k < 3; ++k) dgrow(b_.pc[q].ba[k], 0, (size_t)b_.capacity, stream_);
     b_.has_ba = true;
+    ++alloc_gen_;
   }
   switch (field) {
     case PHY_FIELD_POS:
@@ -746,34 +897,47 @@ void FluidWorld::set_field(int field, const double* in) {
   cuda_check(cudaStreamSynchronize(stream_), "set_field sync");
 }
 
-void FluidWorld::step(double dt) {
-  if (n_ == 0) return;  // world.rs:184-186
+// Validation, grid box and launch constants of a step (host work only, no
+// device synchronisation unless a buffer grows).
+StepConsts FluidWorld::prepare_step(double dt) {
   if (params.visc_k.empty() || params.visc_k.size() > (size_t)kMaxMaterials)
     throw std::invalid_argument("step: visc_k must hold 1..16 entries");
   if (params.visc_n.size() < params.visc_k.size())
     throw std::invalid_argument("step: visc_n shorter than visc_k (the reference would index out of bounds)");
+  if (!scenes_.empty() && !(prec_ == Precision::F32Comp && comp_tile_ > 0))
+    throw std::invalid_argument("step: batched scenes need the tiled compensated form");
   ensure_cells();
-  StepConsts c = make_consts(dt);
+  return make_consts(dt);
+}
+
+// The device work of one step on the world's stream.
+void FluidWorld::enqueue_step(const StepConsts& c, const PassEvents& pe) {
   cuda_check(cudaMemsetAsync(b_.flags, 0, sizeof(uint32_t), stream_), "flags reset");
   if (counting_) cuda_check(cudaMemsetAsync(b_.counters, 0, 2 * sizeof(unsigned long long), stream_), "memset");
   unsigned long long* saved = b_.counters;
   if (!counting_) b_.counters = nullptr;
-  PassEvents pe;
-  if (timing_) {
-    cuda_check(cudaEventRecord(ev_[0], stream_), "event");
-    pe.after_prep = ev_[2];
-    pe.after_density = ev_[3];
-  }
-  launch_sort(c, b_, stream_);
+  if (timing_) cuda_check(cudaEventRecord(ev_[0], stream_), "event");
+  launch_sort(c, b_, stream_, tuning_.sort_block);
   if (timing_) cuda_check(cudaEventRecord(ev_[1], stream_), "event");
   if (prec_ == Precision::F64Plain)
     launch_plain_passes(c, b_, stream_, pe);
   else if (tile_)
-    launch_comp_tiled(c, b_, stream_, pe);
+    launch_comp_tiled(c, b_, stream_, pe, tuning_);
   else
     launch_comp_passes(c, b_, stream_, pe);
   b_.counters = saved;
   cuda_check(cudaGetLastError(), "step launch");
+}
+
+void FluidWorld::step(double dt) {
+  if (n_ == 0) return;  // world.rs:184-186
+  StepConsts c = prepare_step(dt);
+  PassEvents pe;
+  if (timing_) {
+    pe.after_prep = ev_[2];
+    pe.after_density = ev_[3];
+  }
+  enqueue_step(c, pe);
   if (timing_) {
     cuda_check(cudaEventRecord(ev_[4], stream_), "event");
     cuda_check(cudaEventSynchronize(ev_[4]), "event sync");
@@ -784,6 +948,251 @@ void FluidWorld::step(double dt) {
     }
     timed_steps_ += 1;
   }
+}
+
+void FluidWorld::step_n(double dt, int n) {
+  if (n_ == 0 || n <= 0) return;
+  if (graph_chunk_ > 0 && !timing_)
+    for (; n >= graph_chunk_; n -= graph_chunk_) run_graph(dt, graph_chunk_);
+  for (; n > 0; --n) step(dt);
+}
+
+void FluidWorld::drop_graphs() {
+  for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
+  graphs_.clear();
+}
+
+// k steps as one CUDA graph.  The key holds every value a captured launch
+// bakes in: the launch constants (parameters, dt, box, particle count), the
+// buffer generation, the double-buffer parity, counting, body_acc, the
+// launch knobs and the stream.
+void FluidWorld::run_graph(double dt, int k) {
+  const StepConsts c = prepare_step(dt);
+  if (tile_) (void)tiled_max_ctas_per_sm();  // one-time attribute setup, outside the capture
+  std::vector<unsigned char> key(sizeof(StepConsts) + 64, 0);
+  std::memcpy(key.data(), &c, sizeof(StepConsts));
+  long long extra[8] = {k, (long long)alloc_gen_, b_.cur, counting_ ? 1 : 0, b_.has_ba ? 1 : 0,
+                        tuning_.ctas_per_sm + 1000ll * tuning_.queue, tuning_.sort_block,
+                        (long long)(uintptr_t)stream_};
+  std::memcpy(key.data() + sizeof(StepConsts), extra, sizeof(extra));
+  const int cur0 = b_.cur;
+  cudaGraphExec_t exec = nullptr;
+  for (auto& g : graphs_)
+    if (g.key == key) exec = g.exec;
+  if (!exec) {
+    cudaGraph_t graph = nullptr;
+    cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "graph capture");
+    try {
+      PassEvents none;
+      for (int q = 0; q < k; ++q) enqueue_step(c, none);
+    } catch (...) {
+      cudaStreamEndCapture(stream_, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      b_.cur = cur0;
+      throw;
+    }
+    cuda_check(cudaStreamEndCapture(stream_, &graph), "graph capture end");
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    cuda_check(e, "graph instantiate");
+    if (graphs_.size() >= 4) {
+      cudaGraphExecDestroy(graphs_.front().exec);
+      graphs_.erase(graphs_.begin());
+    }
+    graphs_.push_back({key, exec});
+  }
+  b_.cur = cur0;
+  cuda_check(cudaGraphLaunch(exec, stream_), "graph launch");
+  b_.cur = cur0 ^ (k & 1);
+}
+
+// ---- Batched scenes ---------------------------------------------------------
+
+void FluidWorld::set_scenes(const std::vector<uint64_t>& counts, const std::vector<Vec3>& lo,
+                            const std::vector<Vec3>& hi) {
+  if (prec_ != Precision::F32Comp || comp_tile_ == 0)
+    throw std::invalid_argument("set_scenes: batched scenes need the tiled compensated form");
+  if (counts.empty() || counts.size() > 65535 || lo.size() != counts.size() || hi.size() != counts.size())
+    throw std::invalid_argument("set_scenes: 1..65535 scenes, one bounds pair each");
+  uint64_t sum = 0;
+  for (uint64_t c : counts) sum += c;
+  if (sum != n_) throw std::invalid_argument("set_scenes: scene counts must add up to the particle count");
+  const double inv = 1.0 / h0_;
+  std::vector<Scene> sc(counts.size());
+  std::vector<uint32_t> pbase(counts.size() + 1, 0);
+  uint64_t first = 0;
+  for (size_t s = 0; s < counts.size(); ++s) {
+    sc[s].first = first;
+    sc[s].count = counts[s];
+    sc[s].lo = lo[s];
+    sc[s].hi = hi[s];
+    const double l[3] = {lo[s].x, lo[s].y, lo[s].z}, h[3] = {hi[s].x, hi[s].y, hi[s].z};
+    for (int a = 0; a < 3; ++a) {
+      const long long k0 = key_axis_host(l[a], inv), k1 = key_axis_host(h[a], inv);
+      sc[s].kmin[a] = std::min(k0, k1);
+      sc[s].kmax[a] = std::max(k0, k1);
+    }
+    pbase[s] = (uint32_t)first;
+    first += counts[s];
+  }
+  pbase[counts.size()] = (uint32_t)first;
+  cuda_check(cudaStreamSynchronize(stream_), "scenes sync");
+  dalloc(d_pbase_, pbase.size());
+  cuda_check(cudaMemcpy(d_pbase_, pbase.data(), pbase.size() * sizeof(uint32_t), cudaMemcpyHostToDevice),
+             "pbase upload");
+  for (int q = 0; q < 2; ++q)
+    if (!b_.pc[q].scene) dalloc(b_.pc[q].scene, (size_t)std::max(b_.capacity, 1));
+  ++alloc_gen_;
+  if (n_ > 0)
+    k_scene_of_id<<<grid_for(n_), kThreads, 0, stream_>>>((int)n_, b_.pc[b_.cur].id, d_pbase_, (int)counts.size(),
+                                                           b_.pc[b_.cur].scene);
+  cuda_check(cudaGetLastError(), "scene ids");
+  scenes_ = sc;
+  // Positions (insertion order) widen each scene's box.
+  if (n_ > 0) {
+    k_get_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>((int)n_, b_.pc[b_.cur].id, b_.pv1[0], b_.pv1[1],
+                                                             b_.pv1[2], b_.stage);
+    grow_scene_boxes(b_.stage);
+  }
+  ensure_cells();
+}
+
+// Widens each scene's key range with its finite positions (interleaved xyz
+// in insertion order on the device); throws, leaving the ranges unchanged,
+// when the boxes would exceed the cell cap.
+void FluidWorld::grow_scene_boxes(const double* d_pos3) {
+  const int ns = (int)scenes_.size();
+  dalloc(d_scene_bbox_, 7 * (size_t)ns);
+  k_scene_bbox<<<ns, kThreads, 0, stream_>>>(d_pos3, d_pbase_, 1.0 / h0_, d_scene_bbox_);
+  cuda_check(cudaGetLastError(), "scene bbox");
+  std::vector<long long> r(7 * (size_t)ns);
+  cuda_check(cudaMemcpyAsync(r.data(), d_scene_bbox_, r.size() * sizeof(long long), cudaMemcpyDeviceToHost, stream_),
+             "scene bbox read");
+  cuda_check(cudaStreamSynchronize(stream_), "scene bbox sync");
+  std::vector<Scene> sc = scenes_;
+  long double total = 0;
+  for (int s = 0; s < ns; ++s) {
+    long double cells = 1;
+    for (int a = 0; a < 3; ++a) {
+      if (sc[s].count > 0 && r[7 * s + a] != LLONG_MAX) {
+        sc[s].kmin[a] = std::min(sc[s].kmin[a], r[7 * s + a]);
+        sc[s].kmax[a] = std::max(sc[s].kmax[a], r[7 * s + 3 + a]);
+      }
+      cells *= (long double)(sc[s].kmax[a] - sc[s].kmin[a] + 3 + 3);
+    }
+    total += cells;
+  }
+  if (total > (long double)kMaxCells)
+    throw std::invalid_argument("FluidWorld: the scenes' positions span more than 2^27 grid cells");
+  scenes_ = sc;
+}
+
+void FluidWorld::clear_scenes() {
+  scenes_.clear();
+  host_boxes_.clear();
+  for (int q = 0; q < 2; ++q) dfree(b_.pc[q].scene);
+  ++alloc_gen_;
+}
+
+// ---- Autotuner ----------------------------------------------------------------
+
+// Saves (restore = false) or restores (restore = true) the particle state a
+// step reads and the outputs it leaves: pv1, the current per-particle
+// constants, rho, p, acc, xsph and mu.  The saved copy is kept until
+// release_snapshot().
+void FluidWorld::snapshot(bool restore) {
+  const size_t n = n_;
+  if (restore) b_.cur = snap_cur_;
+  ParticleConsts& pc = b_.pc[b_.cur];
+  std::vector<std::pair<void*, size_t>> arrays;
+  for (int k = 0; k < 6; ++k) arrays.push_back({b_.pv1[k], n * 8});
+  arrays.push_back({pc.mass, n * 8});
+  arrays.push_back({pc.mat, n * 4});
+  arrays.push_back({pc.id, n * 4});
+  if (pc.scene) arrays.push_back({pc.scene, n * 2});
+  if (b_.has_ba)
+    for (int k = 0; k < 3; ++k) arrays.push_back({pc.ba[k], n * 8});
+  arrays.push_back({b_.rho, n * 8});
+  arrays.push_back({b_.p, n * 8});
+  arrays.push_back({b_.mu, n * 8});
+  for (int k = 0; k < 3; ++k) {
+    arrays.push_back({b_.acc[k], n * 8});
+    arrays.push_back({b_.xsph[k], n * 8});
+  }
+  if (!restore) {
+    release_snapshot();
+    snap_.assign(arrays.size(), nullptr);
+    for (size_t q = 0; q < arrays.size(); ++q) {
+      dalloc(snap_[q], (arrays[q].second + 7) / 8);
+      cuda_check(cudaMemcpyAsync(snap_[q], arrays[q].first, arrays[q].second, cudaMemcpyDeviceToDevice, stream_),
+                 "snapshot");
+    }
+    snap_cur_ = b_.cur;
+  } else {
+    if (snap_.size() != arrays.size()) throw std::logic_error("snapshot: no saved state of this layout");
+    for (size_t q = 0; q < arrays.size(); ++q)
+      cuda_check(cudaMemcpyAsync(arrays[q].first, snap_[q], arrays[q].second, cudaMemcpyDeviceToDevice, stream_),
+                 "restore");
+  }
+  cuda_check(cudaStreamSynchronize(stream_), "snapshot sync");
+}
+
+void FluidWorld::release_snapshot() {
+  for (auto& p : snap_) dfree(p);
+  snap_.clear();
+}
+
+std::vector<TuneTrial> FluidWorld::autotune(double dt, int steps) {
+  std::vector<TuneTrial> trials;
+  if (n_ == 0 || steps <= 0) return trials;
+  if (timing_) throw std::invalid_argument("autotune: phase timing is on");
+  std::vector<LaunchTuning> cands;
+  const bool tiled = prec_ == Precision::F32Comp && comp_tile_ > 0;
+  const int max_per_sm = tiled ? tiled_max_ctas_per_sm() : 1;
+  for (int sort_block : {128, 256})
+    for (int queue = 0; queue <= (tiled ? 1 : 0); ++queue)
+      for (int per = 1; per <= max_per_sm; ++per) {
+        LaunchTuning t;
+        t.ctas_per_sm = tiled ? per : 0;
+        t.queue = queue;
+        t.sort_block = sort_block;
+        cands.push_back(t);
+      }
+  const LaunchTuning saved = tuning_;
+  snapshot(false);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cuda_check(cudaEventCreate(&e0), "event");
+  cuda_check(cudaEventCreate(&e1), "event");
+  try {
+    for (const LaunchTuning& t : cands) {
+      tuning_ = t;
+      step_n(dt, 1);  // warm-up (and graph capture when chunked)
+      if (graph_chunk_ > 0) step_n(dt, graph_chunk_);
+      cuda_check(cudaEventRecord(e0, stream_), "event");
+      step_n(dt, steps);
+      cuda_check(cudaEventRecord(e1, stream_), "event");
+      cuda_check(cudaEventSynchronize(e1), "event sync");
+      float ms = 0.f;
+      cuda_check(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+      trials.push_back({t, (double)ms / steps});
+      snapshot(true);  // every candidate starts from the same state
+    }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    tuning_ = saved;
+    snapshot(true);
+    release_snapshot();
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  release_snapshot();
+  size_t best = 0;
+  for (size_t q = 1; q < trials.size(); ++q)
+    if (trials[q].ms_per_step < trials[best].ms_per_step) best = q;
+  tuning_ = trials[best].tuning;
+  return trials;
 }
 
 void FluidWorld::set_timing(bool on) {

@@ -47,6 +47,12 @@ class CudaError : public std::runtime_error {
 
 void cuda_check(cudaError_t e, const char* what);
 
+// One configuration of the launch knobs and its measured step time.
+struct TuneTrial {
+  LaunchTuning tuning;
+  double ms_per_step;
+};
+
 class FluidWorld {
  public:
   FluidWorld(const SphParams& params, Precision prec);
@@ -69,6 +75,30 @@ class FluidWorld {
   void add_particles(size_t n, const double* pos, const double* vel, const double* mass,
                      const uint32_t* material);                         // world.rs:171-174
   void step(double dt);                                                 // world.rs:183-192
+  // n steps; with a graph chunk set, runs of `chunk` steps are captured once
+  // into a CUDA graph and replayed (re-captured when a parameter, dt, the
+  // particle count or a buffer changes).
+  void step_n(double dt, int n);
+  void set_graph_chunk(int steps) { graph_chunk_ = steps < 0 ? 0 : steps; }
+  int graph_chunk() const { return graph_chunk_; }
+
+  // Batched scenes: partitions the particles (insertion order) into
+  // consecutive scenes of counts[s] particles, each with its own wall bounds
+  // and its own grid box; a step then advances every scene through one sort
+  // and one persistent launch per pass.  The scenes never interact; shared
+  // parameters are the world's.  Tiled compensated form only; the particle
+  // set is then fixed (add_particles throws until clear_scenes()).
+  void set_scenes(const std::vector<uint64_t>& counts, const std::vector<Vec3>& lo, const std::vector<Vec3>& hi);
+  void clear_scenes();
+  int scene_count() const { return (int)scenes_.size(); }
+
+  // Launch knobs of the tiled passes and the sort (results do not depend on
+  // them) and the project's autotuner over them: every candidate runs
+  // `steps` steps from the same saved state (restored afterwards), the
+  // fastest is kept.  Returns the trials in order.
+  void set_launch_tuning(const LaunchTuning& t) { tuning_ = t; }
+  LaunchTuning launch_tuning() const { return tuning_; }
+  std::vector<TuneTrial> autotune(double dt, int steps);
 
   // Insertion-order field access (particle.rs:17-46).
   static int components(int field);
@@ -103,6 +133,7 @@ class FluidWorld {
   // Staging capacity (particles per tile halo) below the kernels' maximum;
   // smaller values route more tiles through the global-memory path.
   void set_halo_cap(int v) { halo_cap_ = v < 0 ? 0 : v; }
+  int halo_cap() const { return halo_cap_; }
 
   // Device state access for in-library consumers (sorted order).
   DevBuffers& buffers() { return b_; }
@@ -116,7 +147,14 @@ class FluidWorld {
   void grow_box_with_positions(size_t n, const double* pos3);
   void merge_box(const long long* mn, const long long* mx, bool any_nonfinite);
   void grow_box_with_device_positions(size_t n, const double* d_pos3);
+  void grow_scene_boxes(const double* d_pos3);
   void free_all();
+  StepConsts prepare_step(double dt);
+  void enqueue_step(const StepConsts& c, const PassEvents& pe);
+  void run_graph(double dt, int k);
+  void drop_graphs();
+  void snapshot(bool restore);
+  void release_snapshot();
 
   Precision prec_;
   double h0_;
@@ -139,6 +177,30 @@ class FluidWorld {
   double phase_ms_[4] = {0, 0, 0, 0};
   double timed_steps_ = 0;
   long long* d_bbox_ = nullptr;  // 7 values: min xyz, max xyz, non-finite flag
+
+  // Batched scenes.
+  struct Scene {
+    uint64_t first, count;
+    Vec3 lo, hi;
+    long long kmin[3], kmax[3];
+  };
+  std::vector<Scene> scenes_;
+  std::vector<SceneBox> host_boxes_;  // last uploaded box table
+  int boxes_capacity_ = 0;
+  uint32_t* d_pbase_ = nullptr;
+  long long* d_scene_bbox_ = nullptr;
+  LaunchTuning tuning_;
+  // CUDA graphs of step chunks, keyed by everything a captured launch bakes in.
+  struct GraphEntry {
+    std::vector<unsigned char> key;
+    cudaGraphExec_t exec;
+  };
+  std::vector<GraphEntry> graphs_;
+  int graph_chunk_ = 0;
+  unsigned long long alloc_gen_ = 0;  // bumped on every (re)allocation
+  // Autotuner state copy.
+  std::vector<double*> snap_;
+  int snap_cur_ = 0;
 };
 
 // FluidSubsystem<T> (subsystem.rs:26-55): the world plus coupling coefficients.

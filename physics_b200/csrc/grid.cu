@@ -37,7 +37,8 @@ __global__ void __launch_bounds__(kThreads) k_cell_hist(StepConsts c, const doub
                                                         uint32_t* __restrict__ cell_of,
                                                         uint32_t* __restrict__ rank,
                                                         uint32_t* __restrict__ count,
-                                                        uint32_t* __restrict__ flags) {
+                                                        uint32_t* __restrict__ flags,
+                                                        const uint16_t* __restrict__ scene) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = i < c.n;
   uint32_t cell = 0;
@@ -45,9 +46,18 @@ __global__ void __launch_bounds__(kThreads) k_cell_hist(StepConsts c, const doub
     long long kx = key_axis(px[i], c.inv_cell);
     long long ky = key_axis(py[i], c.inv_cell);
     long long kz = key_axis(pz[i], c.inv_cell);
-    if (cell_interior(c, kx, ky, kz)) {
-      cell = (uint32_t)cell_index(c, kx, ky, kz);
+    bool inside;
+    if (c.tile) {
+      // Tiled linearisation: the particle's scene box.
+      const SceneBox& bx = c.boxes[scene ? scene[i] : 0];
+      const long long a = kx - bx.b0[0], b = ky - bx.b0[1], d = kz - bx.b0[2];
+      inside = a >= 1 && b >= 1 && d >= 1 && a < bx.nc[0] - 1 && b < bx.nc[1] - 1 && d < bx.nc[2] - 1;
+      if (inside) cell = (uint32_t)box_tiled_index(c, bx, (int)a, (int)b, (int)d);
     } else {
+      inside = cell_interior(c, kx, ky, kz);
+      if (inside) cell = (uint32_t)cell_linear(c, kx, ky, kz);
+    }
+    if (!inside) {
       cell = (uint32_t)c.ncells;  // overflow cell: never visited as a neighbour
       atomicOr(flags, kFlagOutOfBox);
     }
@@ -206,6 +216,7 @@ __global__ void __launch_bounds__(kThreads) k_gather(int n, const uint32_t* __re
 #pragma unroll
     for (int k = 0; k < 3; ++k) g.dst.ba[k][s] = g.src.ba[k][i];
   }
+  if (g.src.scene) g.dst.scene[s] = g.src.scene[i];
   if (g.sorted_cell) g.sorted_cell[s] = g.cell_of[i];
 }
 
@@ -295,20 +306,22 @@ static int scan_length(int ncells) { return ((ncells + 2 + kScanTile - 1) / kSca
 size_t scan_block_sums_needed(int ncells) { return (size_t)scan_length(ncells) / kScanTile; }
 size_t tile_head_length(int n) { return (size_t)((n + 1 + kScanTile - 1) / kScanTile) * kScanTile; }
 
-void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s) {
+void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s, int block) {
+  // Per-particle kernels take any warp multiple up to kThreads.
+  const int bs = block >= 32 && block <= kThreads ? block / 32 * 32 : kThreads;
   const int n = c.n;
   const int len = scan_length(c.ncells);
   const int nb = len / kScanTile;
   cudaMemsetAsync(b.cell_start, 0, (size_t)len * sizeof(uint32_t), s);
-  k_cell_hist<<<grid_for(n), kThreads, 0, s>>>(c, b.pv1[0], b.pv1[1], b.pv1[2], b.cell_of, b.rank,
-                                               b.cell_start, b.flags);
+  k_cell_hist<<<grid_for(n, bs), bs, 0, s>>>(c, b.pv1[0], b.pv1[1], b.pv1[2], b.cell_of, b.rank,
+                                               b.cell_start, b.flags, b.pc[b.cur].scene);
   k_scan_reduce<<<nb, kThreads, 0, s>>>(b.cell_start, b.block_sums);
   k_scan_top<<<1, 1024, 0, s>>>(b.block_sums, nb);
   k_scan_apply<<<nb, kThreads, 0, s>>>(b.cell_start, b.block_sums);
-  k_scatter<<<grid_for(n), kThreads, 0, s>>>(n, b.cell_of, b.rank, b.cell_start, b.tmp);
+  k_scatter<<<grid_for(n, bs), bs, 0, s>>>(n, b.cell_of, b.rank, b.cell_start, b.tmp);
   const ParticleConsts& src = b.pc[b.cur];
   const ParticleConsts& dst = b.pc[b.cur ^ 1];
-  k_order<<<grid_for(n), kThreads, 0, s>>>(n, c.ncells, b.cell_of, b.cell_start, b.tmp, src.id, b.perm);
+  k_order<<<grid_for(n, bs), bs, 0, s>>>(n, c.ncells, b.cell_of, b.cell_start, b.tmp, src.id, b.perm);
   GatherArgs g;
   for (int k = 0; k < 6; ++k) {
     g.src_pv[k] = b.pv1[k];
@@ -319,18 +332,18 @@ void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s) {
   g.has_ba = b.has_ba ? 1 : 0;
   g.cell_of = b.cell_of;
   g.sorted_cell = c.tile ? b.sorted_cell : nullptr;
-  k_gather<<<grid_for(n), kThreads, 0, s>>>(n, b.perm, g);
+  k_gather<<<grid_for(n, bs), bs, 0, s>>>(n, b.perm, g);
   b.cur ^= 1;
   if (c.tile) {
     // head flags in `rank` (free after the scatter), scanned in place.
     const int hlen = ((n + 1 + kScanTile - 1) / kScanTile) * kScanTile;
     cudaMemsetAsync(b.tile_head, 0, (size_t)hlen * sizeof(uint32_t), s);
-    k_tile_heads<<<grid_for(n + 1), kThreads, 0, s>>>(n, c.ncells, c.tile_log2, b.sorted_cell, b.tile_head);
+    k_tile_heads<<<grid_for(n + 1, bs), bs, 0, s>>>(n, c.ncells, c.tile_log2, b.sorted_cell, b.tile_head);
     const int hb = hlen / kScanTile;
     k_scan_reduce<<<hb, kThreads, 0, s>>>(b.tile_head, b.block_sums);
     k_scan_top<<<1, 1024, 0, s>>>(b.block_sums, hb);
     k_scan_apply<<<hb, kThreads, 0, s>>>(b.tile_head, b.block_sums);
-    k_tile_emit<<<grid_for(n + 1), kThreads, 0, s>>>(n, c.ncells, b.sorted_cell, b.tile_head, b.cell_start,
+    k_tile_emit<<<grid_for(n + 1, bs), bs, 0, s>>>(n, c.ncells, b.sorted_cell, b.tile_head, b.cell_start,
                                                    b.tile_slot, b.num_tiles);
   }
 }

@@ -16,6 +16,7 @@ struct ParticleConsts {
   uint32_t* mat = nullptr;
   uint32_t* id = nullptr;   // insertion index
   double* ba[3] = {nullptr, nullptr, nullptr};  // body_acc, optional
+  uint16_t* scene = nullptr;  // scene of a batched world, optional
 };
 
 struct DevBuffers {
@@ -55,6 +56,10 @@ struct DevBuffers {
   uint32_t* tile_head = nullptr;
   uint32_t* tile_slot = nullptr;
   uint32_t* num_tiles = nullptr;
+  // Scene boxes of the tiled linearisation (one entry for a single world) and
+  // the work-queue counters of the persistent passes (density, force).
+  SceneBox* boxes = nullptr;
+  uint32_t* queue = nullptr;
   // Sort scratch.
   uint32_t* cell_of = nullptr;
   uint32_t* rank = nullptr;
@@ -70,7 +75,7 @@ struct DevBuffers {
 };
 
 // grid.cu
-void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s);
+void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s, int block = 256);
 void launch_unsort_f64(const DevBuffers& b, int n, const double* src_sorted, double* dst_orig,
                        cudaStream_t s);
 void launch_unsort_u32(const DevBuffers& b, int n, const uint32_t* src_sorted, double* dst_orig,
@@ -98,7 +103,19 @@ void launch_comp_passes(const StepConsts& c, DevBuffers& b, cudaStream_t s, cons
 size_t scan_block_sums_needed(int count);
 size_t tile_head_length(int n);
 
+// Launch knobs (results do not depend on them): resident CTAs per SM of the
+// tiled passes' persistent grids (0 = the occupancy limit), their tile
+// distribution (static stride or a device work queue) and the block size of
+// the sort's per-particle kernels.
+struct LaunchTuning {
+  int ctas_per_sm = 0;
+  int queue = 0;
+  int sort_block = 256;
+};
+
 // step_tiled.cu: the FP32-compensated passes over staged 4x4x4-cell tiles.
-void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const PassEvents& ev);
+void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const PassEvents& ev,
+                       const LaunchTuning& t);
+int tiled_max_ctas_per_sm();
 
 }  // namespace phy

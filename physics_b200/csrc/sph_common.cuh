@@ -34,6 +34,18 @@ enum : uint32_t {
   kFlagNonFinite = 2u,   // a new position or velocity is NaN/Inf
 };
 
+// The grid box and wall bounds of one scene in the tiled linearisation.  A
+// batch of independent scenes gives every scene its own box; the boxes'
+// cells are numbered consecutively (cell_base, a multiple of the tile size),
+// so one sort and one persistent pass cover all scenes, which never interact.
+struct SceneBox {
+  long long b0[3];   // key of the box's first cell per axis
+  int nc[3];         // cells per axis (multiples of the tile edge)
+  int nt[3];         // tiles per axis
+  int cell_base;     // first global cell index of the box
+  double lo[3], hi[3];  // bounds_min / bounds_max of the scene
+};
+
 // Everything a step kernel needs, passed by value (kernel parameter space).
 struct StepConsts {
   // Captured at construction from the initial h (kernels.rs:22-35, grid.rs:27).
@@ -58,6 +70,11 @@ struct StepConsts {
   // Tiles whose halo holds more particles than this are computed from
   // global memory instead of shared memory (<= the kernels' capacity).
   int halo_cap;
+  // Tiled form: device table of the scene boxes (one entry for a single
+  // world).  A particle's scene is its entry in ParticleConsts::scene (all 0
+  // when that array is absent); ncells counts the cells of all boxes.
+  const SceneBox* boxes;
+  int n_scenes;
   // f32 copies for the compensated form.
   float h0f, h0sqf, poly6_cf, spiky_cf, lap_cf, hf, h2f;
 };
@@ -101,6 +118,13 @@ __device__ __forceinline__ int cell_index(const StepConsts& c, long long i, long
 __device__ __forceinline__ bool cell_interior(const StepConsts& c, long long i, long long j, long long k) {
   long long a = i - c.bx0, b = j - c.by0, d = k - c.bz0;
   return a >= 1 && b >= 1 && d >= 1 && a < c.ncx - 1 && b < c.ncy - 1 && d < c.ncz - 1;
+}
+
+// Global tiled cell index of box coordinates (a, b, d) inside box `bx`.
+__device__ __forceinline__ int box_tiled_index(const StepConsts& c, const SceneBox& bx, int a, int b, int d) {
+  const int L = c.tile_log2, m = c.tile - 1;
+  const int tile = ((a >> L) * bx.nt[1] + (b >> L)) * bx.nt[2] + (d >> L);
+  return bx.cell_base + (tile << (3 * L)) + ((((a & m) << L) + (b & m)) << L) + (d & m);
 }
 
 // visc_k[m], visc_n[m] by unrolled selection: a dynamic index into the

@@ -70,6 +70,8 @@ struct TiledArgs {
   double* out_pv[6];
   uint16_t* nbr16;
   uint32_t* nbr_count;
+  const uint16_t* __restrict__ scene;  // null: one scene
+  uint32_t* queue;                      // null: static tile stride
   int stride;
   uint32_t* flags;
   unsigned long long* counters;
@@ -135,7 +137,8 @@ __device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* ws, uint32_
 }
 
 struct TileGeom {
-  int tx, ty, tz;  // tile coordinates
+  int tx, ty, tz;  // tile coordinates inside the scene box
+  int sc;          // scene
   uint32_t first, last;
 };
 
@@ -143,11 +146,23 @@ __device__ __forceinline__ TileGeom tile_geom(const StepConsts& c, const TiledAr
   TileGeom g;
   g.first = a.tile_slot[k];
   g.last = a.tile_slot[k + 1];
-  const int t = (int)(a.sorted_cell[g.first] >> (3 * kTL));
-  g.tz = t % c.ntz;
-  g.ty = (t / c.ntz) % c.nty;
-  g.tx = t / (c.ntz * c.nty);
+  g.sc = a.scene ? (int)a.scene[g.first] : 0;
+  const SceneBox& bx = c.boxes[g.sc];
+  const int t = (int)((a.sorted_cell[g.first] - (uint32_t)bx.cell_base) >> (3 * kTL));
+  g.tz = t % bx.nt[2];
+  g.ty = (t / bx.nt[2]) % bx.nt[1];
+  g.tx = t / (bx.nt[2] * bx.nt[1]);
   return g;
+}
+
+// Next tile of a persistent CTA: the static stride, or the next entry of the
+// pass's work queue (one atomic per tile, broadcast through shared memory).
+__device__ __forceinline__ uint32_t next_tile(uint32_t* queue, int pass, uint32_t strided, uint32_t* s_next) {
+  if (!queue) return strided;
+  __syncthreads();  // every thread has read the previous entry
+  if (threadIdx.x == 0) *s_next = atomicAdd(queue + pass, 1u);
+  __syncthreads();
+  return *s_next;
 }
 
 // Slot ranges of the tile's halo cells: s_src[h] / s_end[h] = global slot
@@ -159,11 +174,12 @@ __device__ __forceinline__ uint32_t halo_table(const StepConsts& c, const TiledA
   const int h = threadIdx.x;
   uint32_t cnt = 0, src = 0;
   if (h < kNH) {
+    const SceneBox& bx = c.boxes[g.sc];
     const int ax = g.tx * kTB - 1 + h / (kH * kH);
     const int ay = g.ty * kTB - 1 + (h / kH) % kH;
     const int az = g.tz * kTB - 1 + h % kH;
-    if (ax >= 0 && ay >= 0 && az >= 0 && ax < c.ncx && ay < c.ncy && az < c.ncz) {
-      const int lin = tiled_index(c, ax, ay, az);
+    if (ax >= 0 && ay >= 0 && az >= 0 && ax < bx.nc[0] && ay < bx.nc[1] && az < bx.nc[2]) {
+      const int lin = box_tiled_index(c, bx, ax, ay, az);
       src = a.cell_start[lin];
       cnt = a.cell_start[lin + 1] - src;
     }
@@ -246,17 +262,17 @@ __device__ __forceinline__ void write_density(const StepConsts& c, const TiledAr
 
 // Density of particle qi from global memory (tiles that do not fit the
 // staging buffer): 27 cells by tiled index, cell-local offsets.
-__device__ void density_global(const StepConsts& c, const TiledArgs& a, int qi) {
+__device__ void density_global(const StepConsts& c, const TiledArgs& a, int qi, const SceneBox& box) {
   const double xi = a.px[qi], yi = a.py[qi], zi = a.pz[qi];
   const long long kx = key_axis(xi, c.inv_cell), ky = key_axis(yi, c.inv_cell), kz = key_axis(zi, c.inv_cell);
   const float4 pi = a.cpos[qi];
   const float hc2 = fminf(c.h2f, c.h0sqf);
   float s = 0.f, comp = 0.f;
-  const int bx = (int)(kx - c.bx0), by = (int)(ky - c.by0), bz = (int)(kz - c.bz0);
+  const int bx = (int)(kx - box.b0[0]), by = (int)(ky - box.b0[1]), bz = (int)(kz - box.b0[2]);
   for (int di = -1; di <= 1; ++di)
     for (int dj = -1; dj <= 1; ++dj)
       for (int dk = -1; dk <= 1; ++dk) {
-        const int lin = tiled_index(c, bx + di, by + dj, bz + dk);
+        const int lin = box_tiled_index(c, box, bx + di, by + dj, bz + dk);
         const int s0 = (int)a.cell_start[lin], e0 = (int)a.cell_start[lin + 1];
         const float ox = (float)di * c.h0f - pi.x, oy = (float)dj * c.h0f - pi.y, oz = (float)dk * c.h0f - pi.z;
         float part = 0.f;
@@ -317,14 +333,17 @@ __global__ void __launch_bounds__(kTT) k_density_tiled(StepConsts c, TiledArgs a
   uint32_t* ws = s_off + kNH + 1;
   const float hc2 = fminf(c.h2f, c.h0sqf);
   const f2 H0SQ = f2_pack(c.h0sqf, c.h0sqf);
+  __shared__ uint32_t s_next;
   const uint32_t ntiles = *a.num_tiles;
   unsigned cand = 0, pairs = 0;
-  for (uint32_t k = blockIdx.x; k < ntiles; k += gridDim.x) {
+  for (uint32_t k = next_tile(a.queue, 0, blockIdx.x, &s_next); k < ntiles;
+       k = next_tile(a.queue, 0, k + gridDim.x, &s_next)) {
     const TileGeom g = tile_geom(c, a, k);
     halo_table(c, a, g, s_src, s_end, s_off, ws);
     const int slab = pick_slab(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
     if (slab == 0) {
-      for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT) density_global(c, a, (int)qi);
+      for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT)
+        density_global(c, a, (int)qi, c.boxes[g.sc]);
       continue;  // uniform across the CTA
     }
     for (int x0 = 0; x0 < kTB; x0 += slab) {
@@ -441,7 +460,8 @@ __device__ __forceinline__ void pair_f32(const StepConsts& c, float dx, float dy
 }
 
 // mu_eff, acc, integrate and bounds in f64 (world.rs:319-397).
-__device__ __forceinline__ void finish_particle(const StepConsts& c, const TiledArgs& a, int i, const CompAcc& q) {
+__device__ __forceinline__ void finish_particle(const StepConsts& c, const TiledArgs& a, int i, const CompAcc& q,
+                                                const SceneBox& bx) {
   const double rho_i = a.rho[i];
   const uint32_t m = a.mat[i];
   const int midx = (int)m < c.n_visc_k ? (int)m : 0;
@@ -484,11 +504,11 @@ __device__ __forceinline__ void finish_particle(const StepConsts& c, const Tiled
     double v = v3[k] + ((acc3[k] + c.g[k]) + b3[k]) * c.dt;
     v = v + xs3[k] * c.xsph_eps;
     double x = p3[k] + v * c.dt;
-    if (x < c.lo[k]) {
-      x = c.lo[k];
+    if (x < bx.lo[k]) {
+      x = bx.lo[k];
       v = -v * c.damp;
-    } else if (x > c.hi[k]) {
-      x = c.hi[k];
+    } else if (x > bx.hi[k]) {
+      x = bx.hi[k];
       v = -v * c.damp;
     }
     finite = finite && isfinite(x) && isfinite(v);
@@ -499,17 +519,17 @@ __device__ __forceinline__ void finish_particle(const StepConsts& c, const Tiled
 }
 
 // Forces of particle qi from global memory (tiles that were not staged).
-__device__ void force_global(const StepConsts& c, const TiledArgs& a, int qi) {
+__device__ void force_global(const StepConsts& c, const TiledArgs& a, int qi, const SceneBox& box) {
   const double xi = a.px[qi], yi = a.py[qi], zi = a.pz[qi];
   const long long kx = key_axis(xi, c.inv_cell), ky = key_axis(yi, c.inv_cell), kz = key_axis(zi, c.inv_cell);
   const float4 pi = a.cpos[qi];
   const float4 vi = a.cvel[qi];
   CompAcc q;
-  const int bx = (int)(kx - c.bx0), by = (int)(ky - c.by0), bz = (int)(kz - c.bz0);
+  const int bx = (int)(kx - box.b0[0]), by = (int)(ky - box.b0[1]), bz = (int)(kz - box.b0[2]);
   for (int di = -1; di <= 1; ++di)
     for (int dj = -1; dj <= 1; ++dj)
       for (int dk = -1; dk <= 1; ++dk) {
-        const int lin = tiled_index(c, bx + di, by + dj, bz + dk);
+        const int lin = box_tiled_index(c, box, bx + di, by + dj, bz + dk);
         const int s0 = (int)a.cell_start[lin], e0 = (int)a.cell_start[lin + 1];
         const float ox = (float)di * c.h0f - pi.x, oy = (float)dj * c.h0f - pi.y, oz = (float)dk * c.h0f - pi.z;
         for (int j = s0; j < e0; ++j) {
@@ -518,7 +538,7 @@ __device__ void force_global(const StepConsts& c, const TiledArgs& a, int qi) {
           pair_f32(c, ox + pj.x, oy + pj.y, oz + pj.z, pj.w, a.cvel[j], a.cmr[j], vi, pi.w, vi.w, q);
         }
       }
-  finish_particle(c, a, qi, q);
+  finish_particle(c, a, qi, q, box);
 }
 
 // Batch partial sums of the pressure and raw viscous forces; folded into the
@@ -581,13 +601,15 @@ __global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) 
   uint32_t* s_off = s_end + kNH;
   uint32_t* ws = s_off + kNH + 1;
   const float hc2 = fminf(c.h2f, c.h0sqf);
+  __shared__ uint32_t s_next;
   const uint32_t ntiles = *a.num_tiles;
-  for (uint32_t k = blockIdx.x; k < ntiles; k += gridDim.x) {
+  for (uint32_t k = next_tile(a.queue, 1, blockIdx.x, &s_next); k < ntiles;
+       k = next_tile(a.queue, 1, k + gridDim.x, &s_next)) {
     const TileGeom g = tile_geom(c, a, k);
     halo_table(c, a, g, s_src, s_end, s_off, ws);
     const int slab = pick_slab(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
     if (slab == 0) {
-      for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT) force_global(c, a, (int)qi);
+      for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT) force_global(c, a, (int)qi, c.boxes[g.sc]);
       continue;
     }
     for (int x0 = 0; x0 < kTB; x0 += slab) {
@@ -648,7 +670,7 @@ __global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) 
             }
           }
       }
-      finish_particle(c, a, (int)qi, q);
+      finish_particle(c, a, (int)qi, q, c.boxes[g.sc]);
     }
     __syncthreads();
     }  // slabs
@@ -656,13 +678,17 @@ __global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) 
   const uint32_t end = a.tile_slot[ntiles];
   for (uint32_t qi = end + blockIdx.x * kTT + threadIdx.x; qi < (uint32_t)c.n; qi += gridDim.x * kTT) {
     CompAcc q;
-    finish_particle(c, a, (int)qi, q);
+    finish_particle(c, a, (int)qi, q, c.boxes[a.scene ? (int)a.scene[qi] : 0]);
   }
 }
 
 // Cell-local f32 operands of every particle (as in step_comp.cu).
 __global__ void __launch_bounds__(256) k_prep_tiled(StepConsts c, TiledArgs a) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0 && a.queue) {
+    a.queue[0] = 0;  // the density and force passes start their queues here
+    a.queue[1] = 0;
+  }
   if (i >= c.n) return;
   const double x = a.px[i], y = a.py[i], z = a.pz[i];
   const long long kx = key_axis(x, c.inv_cell);
@@ -676,33 +702,41 @@ __global__ void __launch_bounds__(256) k_prep_tiled(StepConsts c, TiledArgs a) {
 constexpr size_t kDensitySmem = kHaloCap * sizeof(float4) + (3 * kNH + 1 + 32) * 4;
 constexpr size_t kForceSmem = kHaloCap * (2 * sizeof(float4) + sizeof(float)) + (3 * kNH + 1 + 32) * 4;
 
-struct Persistent {
-  int density_blocks = 0, force_blocks = 0;
+// Resident CTAs per SM of the persistent passes (occupancy limits, computed
+// once; the shared-memory opt-in is set on the same first call).
+struct Occupancy {
+  int sms = 1, density = 1, force = 1;
 };
 
-Persistent persistent_grid() {
-  static Persistent p;
-  static bool done = false;
-  if (!done) {
-    int dev = 0, sms = 0;
+const Occupancy& occupancy() {
+  static const Occupancy o = [] {
+    Occupancy r;
+    int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&r.sms, cudaDevAttrMultiProcessorCount, dev);
     cudaFuncSetAttribute(k_density_tiled<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDensitySmem);
     cudaFuncSetAttribute(k_density_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDensitySmem);
     cudaFuncSetAttribute(k_force_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kForceSmem);
     int bd = 0, bf = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bd, k_density_tiled<false>, kTT, kDensitySmem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force_tiled, kTT, kForceSmem);
-    p.density_blocks = sms * std::max(bd, 1);
-    p.force_blocks = sms * std::max(bf, 1);
-    done = true;
-  }
-  return p;
+    r.sms = std::max(r.sms, 1);
+    r.density = std::max(bd, 1);
+    r.force = std::max(bf, 1);
+    return r;
+  }();
+  return o;
 }
 
 }  // namespace
 
-void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const PassEvents& ev) {
+int tiled_max_ctas_per_sm() {
+  const Occupancy& o = occupancy();
+  return std::max(o.density, o.force);
+}
+
+void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const PassEvents& ev,
+                       const LaunchTuning& t) {
   const ParticleConsts& pc = b.pc[b.cur];
   TiledArgs a;
   a.px = b.pv0[0];
@@ -733,18 +767,25 @@ void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const
   for (int k = 0; k < 6; ++k) a.out_pv[k] = b.pv1[k];
   a.nbr16 = b.nbr16;
   a.nbr_count = b.nbr_count;
+  a.scene = pc.scene;
+  a.queue = t.queue ? b.queue : nullptr;
   a.stride = b.capacity;
   a.flags = b.flags;
   a.counters = b.counters;
-  const Persistent pg = persistent_grid();
+  // Persistent grids: SM count x resident CTAs per SM (the occupancy limit,
+  // or the tuned count when smaller).
+  const Occupancy& o = occupancy();
+  const int per_sm = t.ctas_per_sm;
+  const int density_blocks = o.sms * (per_sm > 0 ? std::min(per_sm, o.density) : o.density);
+  const int force_blocks = o.sms * (per_sm > 0 ? std::min(per_sm, o.force) : o.force);
   k_prep_tiled<<<(c.n + 255) / 256, 256, 0, s>>>(c, a);
   if (ev.after_prep) cudaEventRecord(ev.after_prep, s);
   if (a.counters)
-    k_density_tiled<true><<<pg.density_blocks, kTT, kDensitySmem, s>>>(c, a);
+    k_density_tiled<true><<<density_blocks, kTT, kDensitySmem, s>>>(c, a);
   else
-    k_density_tiled<false><<<pg.density_blocks, kTT, kDensitySmem, s>>>(c, a);
+    k_density_tiled<false><<<density_blocks, kTT, kDensitySmem, s>>>(c, a);
   if (ev.after_density) cudaEventRecord(ev.after_density, s);
-  k_force_tiled<<<pg.force_blocks, kTT, kForceSmem, s>>>(c, a);
+  k_force_tiled<<<force_blocks, kTT, kForceSmem, s>>>(c, a);
 }
 
 }  // namespace phy

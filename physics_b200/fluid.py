@@ -312,14 +312,58 @@ class FluidWorld:
         L.check(self._lib.phy_fluid_step_counters(self._h, self._sub, out), "phy_fluid_step_counters")
         return {"candidates": out[0], "pairs": out[1], "particles": out[2], "cells": out[3]}
 
-    def set_tuning(self, comp_tile: Optional[int] = None, halo_cap: Optional[int] = None) -> None:
-        """Kernel configuration (phy_fluid_set_tuning); results of the f64 form never change."""
-        if comp_tile is not None:
-            L.check(self._lib.phy_fluid_set_tuning(self._h, self._sub, L.TUNE_COMP_TILE, comp_tile),
+    def set_tuning(self, **knobs: int) -> None:
+        """Kernel configuration (phy_fluid_set_tuning): comp_tile, halo_cap, ctas_per_sm, queue,
+        sort_block, graph_chunk.  Results of the f64 form never change; the launch knobs
+        (ctas_per_sm, queue, sort_block, graph_chunk) change no result of either form."""
+        for name, value in knobs.items():
+            if name not in L.TUNE_PARAMS:
+                raise ValueError(f"unknown tuning parameter {name!r}")
+            if value is None:
+                continue
+            L.check(self._lib.phy_fluid_set_tuning(self._h, self._sub, L.TUNE_PARAMS[name], int(value)),
                     "phy_fluid_set_tuning")
-        if halo_cap is not None:
-            L.check(self._lib.phy_fluid_set_tuning(self._h, self._sub, L.TUNE_HALO_CAP, halo_cap),
-                    "phy_fluid_set_tuning")
+
+    def tuning(self) -> dict:
+        """Current value of every tuning parameter (phy_fluid_get_tuning)."""
+        out = {}
+        v = C.c_int64()
+        for name, code in L.TUNE_PARAMS.items():
+            L.check(self._lib.phy_fluid_get_tuning(self._h, self._sub, code, C.byref(v)), "phy_fluid_get_tuning")
+            out[name] = int(v.value)
+        return out
+
+    def autotune(self, dt: float, steps: int = 10) -> list:
+        """The library's autotuner (phy_fluid_autotune): every launch-knob combination timed over
+        `steps` steps from the same state, the state restored, the fastest kept.  Returns the
+        trials as dicts in the order run."""
+        cap = 256
+        out = (L.PhyTuneTrial * cap)()
+        n = C.c_uint32()
+        L.check(self._lib.phy_fluid_autotune(self._h, self._sub, dt, steps, out, cap, C.byref(n)),
+                "phy_fluid_autotune")
+        return [{"ctas_per_sm": t.ctas_per_sm, "queue": t.queue, "sort_block": t.sort_block,
+                 "ms_per_step": t.ms_per_step} for t in out[:min(n.value, cap)]]
+
+    # ---- batched scenes -----------------------------------------------------------
+    def set_scenes(self, counts, bounds_min, bounds_max) -> None:
+        """Partitions the particles (insertion order) into consecutive scenes with their own
+        bounds (phy_fluid_set_scenes); one step then advances every scene."""
+        counts = np.ascontiguousarray(counts, np.uint64)
+        lo = np.ascontiguousarray(bounds_min, np.float64).reshape(-1, 3)
+        hi = np.ascontiguousarray(bounds_max, np.float64).reshape(-1, 3)
+        if lo.shape[0] != counts.size or hi.shape[0] != counts.size:
+            raise ValueError("one bounds pair per scene")
+        L.check(self._lib.phy_fluid_set_scenes(self._h, self._sub, counts.size,
+                                               counts.ctypes.data_as(C.POINTER(C.c_uint64)), _dp(lo), _dp(hi)),
+                "phy_fluid_set_scenes")
+
+    def clear_scenes(self) -> None:
+        L.check(self._lib.phy_fluid_clear_scenes(self._h, self._sub), "phy_fluid_clear_scenes")
+
+    @property
+    def scene_count(self) -> int:
+        return int(self._lib.phy_fluid_scene_count(self._h, self._sub))
 
     def set_timing(self, on: bool) -> None:
         L.check(self._lib.phy_fluid_set_timing(self._h, self._sub, 1 if on else 0), "phy_fluid_set_timing")

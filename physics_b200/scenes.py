@@ -18,6 +18,14 @@ Scenes (positions as an (N, 3) float64 array, insertion order):
     - 80x160x80  = 1,024,000 particles, box 32,   dt 0.005  (plain f64 at scale)
     - 128x256x128 = 4,194,304 particles, box 51.2, dt 0.0025 (precision form)
     - 32x64x32   = 65,536 particles,    box 12.8, dt 0.005  (differentiation form)
+* ``batch_scenes(n_scenes, nmin, nmax)`` — independent dam breaks of uneven
+  size for the batched form: per scene five draws of the stream seeded with
+  BATCH_SEED (scene-major): target count log-uniform in [nmin, nmax], box
+  aspect per axis uniform in [0.5, 2], fill fraction (block volume / box
+  volume) uniform in [0.2, 0.5].  The block keeps the box's aspect, sits in
+  the low corner and is the dam-break lattice above (jitter seed SEED + 1 +
+  scene index); bounds [0, box extent] per axis.  The standard batch is 256
+  scenes in [2000, 200000] stepped 200 times at dt 0.005.
 """
 from __future__ import annotations
 
@@ -27,6 +35,7 @@ import numpy as np
 
 GOLDEN = np.uint64(0x9E3779B97F4A7C15)
 SEED = 0xC0FFEE
+BATCH_SEED = 0xBA7C4ED
 SPACING = 0.1
 
 
@@ -131,3 +140,32 @@ def config(name: str) -> Scene:
         nx, ny, nz = (int(v) for v in name.split("_")[1:4])
         return dam_break(nx, ny, nz, max(nx, ny, nz) * SPACING * 2.0, 0.005, 100)
     raise KeyError(name)
+
+
+@dataclass
+class BatchScene:
+    pos: np.ndarray
+    bounds_min: tuple
+    bounds_max: tuple
+
+    @property
+    def n(self) -> int:
+        return self.pos.shape[0]
+
+
+def batch_scenes(n_scenes: int = 256, nmin: int = 2000, nmax: int = 200000, seed: int = BATCH_SEED,
+                 spacing: float = SPACING) -> list:
+    """The batched form's scenes (see the module docstring)."""
+    u = uniform01(seed, 0, 5 * n_scenes).reshape(n_scenes, 5)
+    out = []
+    for sc in range(n_scenes):
+        target = np.exp(np.log(nmin) + u[sc, 0] * (np.log(nmax) - np.log(nmin)))
+        aspect = 0.5 + 1.5 * u[sc, 1:4]
+        fill = 0.2 + 0.3 * u[sc, 4]
+        volume = target * spacing ** 3 / fill
+        edge = (volume / float(np.prod(aspect))) ** (1.0 / 3.0)
+        box = edge * aspect
+        counts = np.maximum(1, np.round(box * fill ** (1.0 / 3.0) / spacing)).astype(int)
+        pos = dam_break_positions(int(counts[0]), int(counts[1]), int(counts[2]), spacing, SEED + 1 + sc)
+        out.append(BatchScene(pos, (0.0, 0.0, 0.0), tuple(float(b) for b in box)))
+    return out
