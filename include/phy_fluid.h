@@ -214,6 +214,27 @@ typedef struct PhyTuneTrial {
 int32_t phy_fluid_autotune(PhyWorldHandle *w, uint32_t sub, double dt, uint32_t steps, PhyTuneTrial *out,
                            uint32_t cap, uint32_t *n_out);
 
+/* Adjoint of the f64 plain step (PHY_PRECISION_F64_PLAIN worlds only).
+ * phy_fluid_tape_begin makes the current state checkpoint 0 and records every
+ * following phy_fluid_step of `sub` (its dt), saving a state checkpoint every
+ * `checkpoint_every` steps; parameters must stay unchanged and body
+ * accelerations unset while recording.  phy_fluid_step_backward runs the
+ * reverse sweep over all recorded steps, re-running each segment forward
+ * from its checkpoint (the f64 plain step repeats bit-exactly): given
+ * dL/dpos_T and dL/dvel_T (3n doubles each, insertion order, xyz
+ * interleaved; NULL = zero) it writes dL/dpos_0, dL/dvel_0 (3n each) and
+ * grad_params2 = {dL/d stiffness, dL/d visc_k[0]} (any output may be NULL).
+ * Neighbour sets and branches (walls, max(0, .), shear_min) are held as the
+ * forward took them.  The world is left in its recorded end state and the
+ * tape is kept for further sweeps until phy_fluid_tape_clear or the next
+ * phy_fluid_tape_begin.  The reference has no adjoint; these calls replace
+ * nothing in phy_ffi.h. */
+int32_t phy_fluid_tape_begin(PhyWorldHandle *w, uint32_t sub, uint32_t checkpoint_every);
+int32_t phy_fluid_tape_clear(PhyWorldHandle *w, uint32_t sub);
+uint32_t phy_fluid_tape_steps(PhyWorldHandle *w, uint32_t sub);
+int32_t phy_fluid_step_backward(PhyWorldHandle *w, uint32_t sub, const double *grad_pos, const double *grad_vel,
+                                double *grad_pos0, double *grad_vel0, double *grad_params2);
+
 /* Scratch capacity of phy_fluid_density_noalloc. */
 #define PHY_NOALLOC_MAX_PARTICLES 65536
 #define PHY_NOALLOC_MAX_CELLS 262144

@@ -70,6 +70,7 @@ def load():
             "orc_neighbors": (C.c_uint64, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64), C.c_uint64]),
             "orc_diagnostics": (None, [C.c_void_p, DP]),
             "orc_counters": (None, [C.c_void_p, C.POINTER(C.c_uint64), C.c_int]),
+            "orc_jvp": (None, [C.c_void_p, C.c_double, C.c_int, DP, DP, C.c_double, C.c_double]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -160,6 +161,15 @@ class OracleWorld:
 
     def step(self, dt: float, n: int = 1) -> None:
         self._lib.orc_step_n(self._w, dt, n)
+
+    def jvp(self, dt: float, n: int, tx, tv, dk: float = 0.0, dc: float = 0.0) -> tuple:
+        """n steps with forward-mode tangents (orc_jvp): tx, tv are the (N, 3) tangents of the
+        positions and velocities, dk and dc those of stiffness and visc_k[0].  Advances the world
+        and returns the tangents of the final positions and velocities."""
+        x = np.array(tx, np.float64, copy=True).reshape(-1)
+        v = np.array(tv, np.float64, copy=True).reshape(-1)
+        self._lib.orc_jvp(self._w, dt, n, x.ctypes.data_as(DP), v.ctypes.data_as(DP), dk, dc)
+        return x.reshape(-1, 3), v.reshape(-1, 3)
 
     def cell_keys(self) -> np.ndarray:
         out = np.empty(3 * len(self), np.int64)

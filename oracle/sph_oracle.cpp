@@ -361,6 +361,132 @@ struct World {
   }
 };
 
+// Forward-mode derivative (JVP) of one step, for checking the product's
+// adjoint: the primal is advanced by the very same step() passes (so every
+// branch is the reference's), and the tangents (tx, tv) of positions and
+// velocities plus the tangents dk of stiffness and dc of visc_k[0] are
+// pushed through the differentiated expressions of world.rs:204-397 with the
+// neighbour sets and branches of that step.
+struct Jvp {
+  World& W;
+  explicit Jvp(World& w) : W(w) {}
+
+  static double dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+
+  void step(double dt, std::vector<V3>& tx, std::vector<V3>& tv, double dk, double dc) {
+    auto& P = W.particles;
+    const size_t n = P.size();
+    if (n == 0) return;
+    const Kernels& K = W.kernels;
+    const double h = W.params.h, rest = W.params.rest_density, stiff = W.params.stiffness;
+    const double r_eps = 1e-4, shear_min = W.params.shear_min;
+    auto wp = [&](double r) {  // d poly6 / dr
+      if (r >= K.h) return 0.0;
+      double q = K.h2 - r * r;
+      return -6.0 * K.poly6_coeff * r * q * q;
+    };
+    auto gp = [&](double r) {  // d spiky_grad_mag / dr
+      if (r >= K.h || r <= 0.0) return 0.0;
+      return -2.0 * K.spiky_grad_coeff * (K.h - r);
+    };
+    auto lp = [&](double r) { return r >= K.h ? 0.0 : -K.visc_lap_coeff; };
+    W.grid.build(P);
+    W.compute_density_pressure();
+    // Density, pressure and p / rho^2 tangents.
+    std::vector<double> trho(n), tpr2(n), pr2(n);
+#pragma omp parallel for schedule(static) num_threads(W.nthreads)
+    for (long long ii = 0; ii < (long long)n; ++ii) {
+      size_t i = (size_t)ii;
+      V3 p_i = P[i].pos;
+      double t = 0.0;
+      W.grid.for_each_neighbor(p_i, [&](size_t j) {
+        V3 d = p_i - P[j].pos;
+        double r = norm(d);
+        if (!(r < h) || r <= 0.0) return;
+        double dr = dot(d, tx[i] - tx[j]) / r;
+        t += P[j].mass * wp(r) * dr;
+      });
+      trho[i] = t;
+      double rho = P[i].rho, over = rho - rest;
+      double tp = over > 0.0 ? dk * over + stiff * t : 0.0;
+      pr2[i] = P[i].p / (rho * rho);
+      tpr2[i] = tp / (rho * rho) - 2.0 * P[i].p * t / (rho * rho * rho);
+    }
+    // Force tangents (the primal sums are recomputed alongside).
+    std::vector<V3> tacc(n), txs(n);
+    const std::vector<Particle> snap = P;
+#pragma omp parallel for schedule(static) num_threads(W.nthreads)
+    for (long long ii = 0; ii < (long long)n; ++ii) {
+      size_t i = (size_t)ii;
+      const Particle& a = snap[i];
+      V3 fp{0, 0, 0}, fv{0, 0, 0}, tfp{0, 0, 0}, tfv{0, 0, 0}, txsph{0, 0, 0};
+      double shear = 0.0, tshear = 0.0;
+      double m_i = a.mass, rho_i = a.rho;
+      W.grid.for_each_neighbor(a.pos, [&](size_t j) {
+        if (j == i) return;
+        const Particle& b = snap[j];
+        V3 d = b.pos - a.pos;
+        double r = norm(d);
+        if (r >= h || r <= 0.0) return;
+        V3 u = d / r, dd = tx[j] - tx[i];
+        double dr = dot(u, dd);
+        V3 du = (dd - u * dr) / r;
+        double mm = m_i * b.mass;
+        double G = K.spiky_grad_mag(r), L = K.visc_lap(r), Wv = K.poly6(r);
+        double A = mm * (pr2[i] + pr2[j]), tA = mm * (tpr2[i] + tpr2[j]);
+        fp += u * (A * G);
+        tfp += du * (A * G) + u * (tA * G + A * gp(r) * dr);
+        V3 dv = b.vel - a.vel, tdv = tv[j] - tv[i];
+        double B = mm / b.rho, tB = -mm * trho[j] / (b.rho * b.rho);
+        fv += dv * (B * L);
+        tfv += tdv * (B * L) + dv * (tB * L + B * lp(r) * dr);
+        double mr = b.mass / b.rho, tmr = -b.mass * trho[j] / (b.rho * b.rho);
+        txsph += tdv * (mr * Wv) + dv * (tmr * Wv + mr * wp(r) * dr);
+        double dvn = norm(dv), tdvn = dvn > 0.0 ? dot(dv, tdv) / dvn : 0.0;
+        double re = r + r_eps;
+        shear += dvn / re * mr;
+        tshear += tdvn / re * mr - dvn * dr / (re * re) * mr + dvn / re * tmr;
+      });
+      uint64_t m_idx = a.material < W.params.n_visc_k ? a.material : 0;
+      double kc = W.params.visc_k[m_idx], nn = W.params.visc_n[m_idx];
+      double ex = nn - 1.0;
+      double sreg = shear > shear_min ? shear : shear_min;
+      double fac = std::pow(sreg, ex);
+      double tkc = m_idx == 0 ? dc : 0.0;
+      double tmu = tkc * fac + ((ex != 0.0 && shear > shear_min) ? kc * ex * std::pow(sreg, ex - 1.0) * tshear : 0.0);
+      double mu = kc * fac;
+      V3 acc = (fp + fv * mu) / rho_i;
+      tacc[i] = (tfp + tfv * mu + fv * tmu) / rho_i - acc * (trho[i] / rho_i);
+      txs[i] = txsph;
+    }
+    W.compute_forces();
+    // Integration and walls: the primal's decisions, recomputed in its order.
+    V3 g{W.params.gravity[0], W.params.gravity[1], W.params.gravity[2]};
+    const double eps = W.params.xsph_eps, damp = W.params.boundary_damp;
+    for (size_t i = 0; i < n; ++i) {
+      const Particle& pt = P[i];
+      V3 a = pt.acc + g + pt.body_acc;
+      V3 v = pt.vel + a * dt;
+      v = v + pt.xsph * eps;
+      V3 x = pt.pos + v * dt;
+      V3 tv2 = tv[i] + tacc[i] * dt + txs[i] * eps;
+      V3 tx1 = tx[i] + tv2 * dt;
+      double xs[3] = {x.x, x.y, x.z};
+      double t_x[3] = {tx1.x, tx1.y, tx1.z}, t_v[3] = {tv2.x, tv2.y, tv2.z};
+      for (int k = 0; k < 3; ++k) {
+        if (xs[k] < W.params.bounds_min[k] || xs[k] > W.params.bounds_max[k]) {
+          t_x[k] = 0.0;
+          t_v[k] = -damp * t_v[k];
+        }
+      }
+      tx[i] = {t_x[0], t_x[1], t_x[2]};
+      tv[i] = {t_v[0], t_v[1], t_v[2]};
+    }
+    W.integrate(dt);
+    W.enforce_bounds();
+  }
+};
+
 enum Field : int {
   F_POS = 0, F_VEL = 1, F_ACC = 2, F_BODY_ACC = 3, F_RHO = 4, F_P = 5,
   F_MASS = 6, F_MU_EFF = 7, F_XSPH = 8, F_MATERIAL = 9
@@ -468,6 +594,29 @@ int orc_set(void* w, int field, const double* in) {
 void orc_step(void* w, double dt) { static_cast<World*>(w)->step(dt); }
 void orc_step_n(void* w, double dt, int n) {
   for (int i = 0; i < n; ++i) static_cast<World*>(w)->step(dt);
+}
+
+// n steps with forward-mode tangents: tx, tv (3n doubles, xyz interleaved,
+// insertion order) hold the tangents of positions and velocities on entry
+// and at the end; dk, dc are the tangents of stiffness and visc_k[0].
+void orc_jvp(void* w, double dt, int n, double* tx, double* tv, double dk, double dc) {
+  World* W = static_cast<World*>(w);
+  const size_t m = W->particles.size();
+  std::vector<V3> x(m), v(m);
+  for (size_t i = 0; i < m; ++i) {
+    x[i] = {tx[3 * i], tx[3 * i + 1], tx[3 * i + 2]};
+    v[i] = {tv[3 * i], tv[3 * i + 1], tv[3 * i + 2]};
+  }
+  Jvp J(*W);
+  for (int k = 0; k < n; ++k) J.step(dt, x, v, dk, dc);
+  for (size_t i = 0; i < m; ++i) {
+    tx[3 * i] = x[i].x;
+    tx[3 * i + 1] = x[i].y;
+    tx[3 * i + 2] = x[i].z;
+    tv[3 * i] = v[i].x;
+    tv[3 * i + 1] = v[i].y;
+    tv[3 * i + 2] = v[i].z;
+  }
 }
 
 // Grid::key_of for every particle (int64 xyz-interleaved), used to pin the

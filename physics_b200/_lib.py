@@ -130,6 +130,10 @@ SIGNATURES = {
     "phy_fluid_set_scenes": (C.c_int32, [H, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64), DP, DP]),
     "phy_fluid_clear_scenes": (C.c_int32, [H, C.c_uint32]),
     "phy_fluid_scene_count": (C.c_uint32, [H, C.c_uint32]),
+    "phy_fluid_tape_begin": (C.c_int32, [H, C.c_uint32, C.c_uint32]),
+    "phy_fluid_tape_clear": (C.c_int32, [H, C.c_uint32]),
+    "phy_fluid_tape_steps": (C.c_uint32, [H, C.c_uint32]),
+    "phy_fluid_step_backward": (C.c_int32, [H, C.c_uint32, DP, DP, DP, DP, DP]),
     "phy_fluid_autotune": (C.c_int32, [H, C.c_uint32, C.c_double, C.c_uint32, C.POINTER(PhyTuneTrial),
                                        C.c_uint32, C.POINTER(C.c_uint32)]),
     "phy_fluid_density_noalloc": (C.c_int32, [C.POINTER(PhySphParams), C.c_uint64, C.c_void_p, C.c_void_p,

@@ -35,7 +35,7 @@ PER_FILE = {
     "fluid_world.cu": ["-fmad=false"],
 }
 SOURCES = ["grid.cu", "step_plain.cu", "step_comp.cu", "step_tiled.cu", "fluid_world.cu", "ffi.cpp",
-           "checkpoint.cpp", "noalloc.cu"]
+           "checkpoint.cpp", "noalloc.cu", "adjoint.cu"]
 
 
 def _nvcc() -> str:

@@ -477,6 +477,32 @@ uint32_t phy_fluid_scene_count(PhyWorldHandle* w, uint32_t sub) {
   return guard<uint32_t>(0u, [&] { return (uint32_t)sub_of(w, sub).world->scene_count(); });
 }
 
+int32_t phy_fluid_tape_begin(PhyWorldHandle* w, uint32_t sub, uint32_t checkpoint_every) {
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->tape_begin((int)checkpoint_every);
+    return 0;
+  });
+}
+
+int32_t phy_fluid_tape_clear(PhyWorldHandle* w, uint32_t sub) {
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->tape_clear();
+    return 0;
+  });
+}
+
+uint32_t phy_fluid_tape_steps(PhyWorldHandle* w, uint32_t sub) {
+  return guard<uint32_t>(0u, [&] { return (uint32_t)sub_of(w, sub).world->tape_steps(); });
+}
+
+int32_t phy_fluid_step_backward(PhyWorldHandle* w, uint32_t sub, const double* grad_pos, const double* grad_vel,
+                                double* grad_pos0, double* grad_vel0, double* grad_params2) {
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->step_backward(grad_pos, grad_vel, grad_pos0, grad_vel0, grad_params2);
+    return 0;
+  });
+}
+
 int32_t phy_fluid_autotune(PhyWorldHandle* w, uint32_t sub, double dt, uint32_t steps, PhyTuneTrial* out,
                            uint32_t cap, uint32_t* n_out) {
   return guard<int32_t>(-1, [&] {

@@ -1,6 +1,8 @@
 // Host-side FluidWorld / FluidSubsystem / World of the B200 build.
 #include "fluid_world.h"
 
+#include "adjoint.h"
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -309,6 +311,7 @@ FluidWorld::~FluidWorld() {
   dfree(d_pbase_);
   dfree(d_scene_bbox_);
   release_snapshot();
+  tape_clear();
   for (auto& e : ev_)
     if (e) cudaEventDestroy(e);
   if (own_stream_) cudaStreamDestroy(own_stream_);
@@ -931,6 +934,19 @@ void FluidWorld::enqueue_step(const StepConsts& c, const PassEvents& pe) {
 
 void FluidWorld::step(double dt) {
   if (n_ == 0) return;  // world.rs:184-186
+  step_impl(dt);
+}
+
+// One step; returns the launch constants it ran with.
+StepConsts FluidWorld::step_impl(double dt) {
+  if (tape_.on && !recomputing_) {
+    const PhySphParams now = params.to_c();
+    if (std::memcmp(&now, &tape_.params, sizeof(now)) != 0)
+      throw std::invalid_argument("step: parameters changed while the adjoint tape is recording");
+    if (b_.has_ba) throw std::invalid_argument("step: body accelerations are not recorded by the adjoint tape");
+    if (!tape_.dts.empty() && tape_.dts.size() % (size_t)tape_.every == 0) save_checkpoint();
+    tape_.dts.push_back(dt);
+  }
   StepConsts c = prepare_step(dt);
   PassEvents pe;
   if (timing_) {
@@ -948,11 +964,12 @@ void FluidWorld::step(double dt) {
     }
     timed_steps_ += 1;
   }
+  return c;
 }
 
 void FluidWorld::step_n(double dt, int n) {
   if (n_ == 0 || n <= 0) return;
-  if (graph_chunk_ > 0 && !timing_)
+  if (graph_chunk_ > 0 && !timing_ && !tape_.on)
     for (; n >= graph_chunk_; n -= graph_chunk_) run_graph(dt, graph_chunk_);
   for (; n > 0; --n) step(dt);
 }
@@ -1279,6 +1296,221 @@ size_t World::fluid_count() const {
   size_t n = 0;
   for (auto& s : subs) n += s->world->len();
   return n;
+}
+
+}  // namespace phy
+
+namespace phy {
+
+// ---- Adjoint ---------------------------------------------------------------------
+
+void FluidWorld::save_checkpoint() {
+  double* ck = nullptr;
+  dalloc(ck, 6 * n_);
+  const ParticleConsts& pc = b_.pc[b_.cur];
+  k_get_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>((int)n_, pc.id, b_.pv1[0], b_.pv1[1], b_.pv1[2], ck);
+  k_get_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>((int)n_, pc.id, b_.pv1[3], b_.pv1[4], b_.pv1[5],
+                                                           ck + 3 * n_);
+  cuda_check(cudaGetLastError(), "checkpoint");
+  tape_.ckpt.push_back(ck);
+}
+
+void FluidWorld::tape_clear() {
+  for (auto& p : tape_.ckpt) dfree(p);
+  tape_.ckpt.clear();
+  tape_.dts.clear();
+  tape_.on = false;
+}
+
+void FluidWorld::tape_begin(int every) {
+  if (prec_ != Precision::F64Plain) throw std::invalid_argument("tape_begin: the adjoint is of the f64 plain form");
+  if (!scenes_.empty()) throw std::invalid_argument("tape_begin: batched scenes are not recorded");
+  if (b_.has_ba) throw std::invalid_argument("tape_begin: body accelerations are not recorded");
+  if (every < 1) throw std::invalid_argument("tape_begin: checkpoint interval must be >= 1");
+  if (n_ == 0) throw std::invalid_argument("tape_begin: empty world");
+  tape_clear();
+  tape_.every = every;
+  tape_.params = params.to_c();
+  save_checkpoint();
+  tape_.on = true;
+}
+
+namespace {
+
+// Device arrays of one recorded step (sorted order) plus its launch constants.
+struct TapeSlot {
+  double* f = nullptr;       // 22 arrays of n doubles
+  uint32_t* u = nullptr;     // mat, id (n each) and cell_start
+  StepConsts c;
+  AdjTape view(size_t n) const {
+    AdjTape t;
+    double* q = f;
+    auto take = [&]() {
+      double* r = q;
+      q += n;
+      return r;
+    };
+    for (int k = 0; k < 3; ++k) t.x[k] = take();
+    for (int k = 0; k < 3; ++k) t.v[k] = take();
+    t.mass = take();
+    t.rho = take();
+    t.p = take();
+    t.pr2 = take();
+    t.mr = take();
+    for (int k = 0; k < 3; ++k) t.acc[k] = take();
+    for (int k = 0; k < 3; ++k) t.xsph[k] = take();
+    t.mu = take();
+    for (int k = 0; k < 3; ++k) t.fv[k] = take();
+    t.shear = take();
+    t.mat = u;
+    t.id = u + n;
+    t.cell_start = u + 2 * n;
+    return t;
+  }
+};
+
+}  // namespace
+
+void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, double* gv0, double* gparams) {
+  const size_t n = n_;
+  const int T = (int)tape_.dts.size();
+  if (!tape_.on) throw std::invalid_argument("step_backward: no adjoint tape (call tape_begin before stepping)");
+  if (n == 0) return;
+  cudaStream_t s = stream_;
+  // Work arrays: gx_ins, gv_ins, gx, gv, P, Q, Y (3 each), sig, rbar,
+  // rbar_tot, cc, kk, the tape's fv and shear outputs (4): 30 arrays of n,
+  // then the two parameter accumulators.
+  constexpr size_t kWorkArrays = 30;
+  double* work = nullptr;
+  dalloc(work, kWorkArrays * n + 2);
+  AdjWork w;
+  {
+    double* q = work;
+    size_t taken = 0;
+    auto take = [&]() {
+      if (++taken > kWorkArrays) throw std::logic_error("step_backward: work partition exceeds its allocation");
+      double* r = q;
+      q += n;
+      return r;
+    };
+    for (int k = 0; k < 3; ++k) w.gx_ins[k] = take();
+    for (int k = 0; k < 3; ++k) w.gv_ins[k] = take();
+    for (int k = 0; k < 3; ++k) w.gx[k] = take();
+    for (int k = 0; k < 3; ++k) w.gv[k] = take();
+    for (int k = 0; k < 3; ++k) w.P[k] = take();
+    for (int k = 0; k < 3; ++k) w.Q[k] = take();
+    for (int k = 0; k < 3; ++k) w.Y[k] = take();
+    w.sig = take();
+    w.rbar = take();
+    w.rbar_tot = take();
+    w.cc = take();
+    w.kk = take();
+    for (int k = 0; k < 3; ++k) b_.tape_fv[k] = take();
+    b_.tape_shear = take();
+    w.param_acc = q;
+  }
+  const int nslots = std::min(tape_.every, std::max(T, 1));
+  std::vector<TapeSlot> slots(nslots);
+  auto cleanup = [&]() {
+    for (auto& sl : slots) {
+      dfree(sl.f);
+      dfree(sl.u);
+    }
+    for (int k = 0; k < 3; ++k) b_.tape_fv[k] = nullptr;
+    b_.tape_shear = nullptr;
+    dfree(work);
+    recomputing_ = false;
+  };
+  try {
+    snapshot(false);  // the world returns to x_T, v_T afterwards
+    // Seeds (insertion order): dL/dx_T, dL/dv_T.
+    cuda_check(cudaMemsetAsync(work, 0, (6 * n + 0) * sizeof(double), s), "seed clear");
+    cuda_check(cudaMemsetAsync(w.param_acc, 0, 2 * sizeof(double), s), "param clear");
+    if (gx) {
+      cuda_check(cudaMemcpyAsync(b_.stage, gx, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s), "seed upload");
+      launch_deinterleave3(b_.stage, w.gx_ins[0], w.gx_ins[1], w.gx_ins[2], (int)n, s);
+    }
+    if (gv) {
+      cuda_check(cudaMemcpyAsync(b_.stage + 3 * n, gv, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s),
+                 "seed upload");
+      launch_deinterleave3(b_.stage + 3 * n, w.gv_ins[0], w.gv_ins[1], w.gv_ins[2], (int)n, s);
+    }
+    cuda_check(cudaStreamSynchronize(s), "seed sync");
+    recomputing_ = true;
+    const int every = tape_.every;
+    const int nseg = (T + every - 1) / every;
+    for (int seg = nseg - 1; seg >= 0; --seg) {
+      const int t0 = seg * every, t1 = std::min(T, t0 + every);
+      // Restore checkpoint `seg` and re-run its steps, recording each.
+      const ParticleConsts& pc = b_.pc[b_.cur];
+      const double* ck = tape_.ckpt[seg];
+      k_set_vec_by_id<<<grid_for(n), kThreads, 0, s>>>((int)n, pc.id, ck, b_.pv1[0], b_.pv1[1], b_.pv1[2]);
+      k_set_vec_by_id<<<grid_for(n), kThreads, 0, s>>>((int)n, pc.id, ck + 3 * n, b_.pv1[3], b_.pv1[4],
+                                                       b_.pv1[5]);
+      for (int t = t0; t < t1; ++t) {
+        TapeSlot& sl = slots[t - t0];
+        const StepConsts c = step_impl(tape_.dts[t]);
+        const size_t ncs = (size_t)c.ncells + 2;
+        if (!sl.f) dalloc(sl.f, 22 * n);
+        if (!sl.u || sl.c.ncells != c.ncells) dalloc(sl.u, 2 * n + ncs);
+        sl.c = c;
+        const AdjTape v = sl.view(n);
+        const ParticleConsts& q = b_.pc[b_.cur];
+        const size_t B = n * sizeof(double);
+        auto copy = [&](const void* dst, const void* src, size_t bytes, const char* what) {
+          const cudaError_t e = cudaMemcpyAsync(const_cast<void*>(dst), src, bytes, cudaMemcpyDeviceToDevice, s);
+          if (e != cudaSuccess)
+            throw CudaError(std::string("tape copy of ") + what + ": " + cudaGetErrorString(e) + " (" +
+                            std::to_string(bytes) + " bytes, dst " + std::to_string((uintptr_t)dst) + ", src " +
+                            std::to_string((uintptr_t)src) + ")");
+        };
+        for (int k = 0; k < 3; ++k) {
+          copy(v.x[k], b_.pv0[k], B, "x");
+          copy(v.v[k], b_.pv0[3 + k], B, "v");
+          copy(v.acc[k], b_.acc[k], B, "acc");
+          copy(v.xsph[k], b_.xsph[k], B, "xsph");
+          copy(v.fv[k], b_.tape_fv[k], B, "fv");
+        }
+        copy(v.mass, q.mass, B, "mass");
+        copy(v.rho, b_.rho, B, "rho");
+        copy(v.p, b_.p, B, "p");
+        copy(v.pr2, b_.pr2, B, "pr2");
+        copy(v.mr, b_.mr, B, "mr");
+        copy(v.mu, b_.mu, B, "mu");
+        copy(v.shear, b_.tape_shear, B, "shear");
+        copy(v.mat, q.mat, n * 4, "mat");
+        copy(v.id, q.id, n * 4, "id");
+        copy(v.cell_start, b_.cell_start, ncs * 4, "cell_start");
+      }
+      for (int t = t1 - 1; t >= t0; --t) launch_adjoint_step(slots[t - t0].c, slots[t - t0].view(n), w, s);
+      cuda_check(cudaGetLastError(), "adjoint step");
+    }
+    recomputing_ = false;
+    std::vector<double> host(6 * n);
+    launch_interleave3(w.gx_ins[0], w.gx_ins[1], w.gx_ins[2], b_.stage, (int)n, s);
+    launch_interleave3(w.gv_ins[0], w.gv_ins[1], w.gv_ins[2], b_.stage + 3 * n, (int)n, s);
+    double pa[2] = {0.0, 0.0};
+    cuda_check(cudaMemcpyAsync(host.data(), b_.stage, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, s),
+               "gradient read");
+    cuda_check(cudaMemcpyAsync(pa, w.param_acc, sizeof(pa), cudaMemcpyDeviceToHost, s), "gradient read");
+    cuda_check(cudaStreamSynchronize(s), "gradient sync");
+    if (gx0) std::memcpy(gx0, host.data(), 3 * n * sizeof(double));
+    if (gv0) std::memcpy(gv0, host.data() + 3 * n, 3 * n * sizeof(double));
+    if (gparams) {
+      gparams[0] = pa[0];
+      gparams[1] = pa[1];
+    }
+    snapshot(true);
+    release_snapshot();
+  } catch (...) {
+    cleanup();
+    if (!snap_.empty()) {
+      snapshot(true);
+      release_snapshot();
+    }
+    throw;
+  }
+  cleanup();
 }
 
 }  // namespace phy

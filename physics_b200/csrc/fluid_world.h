@@ -100,6 +100,20 @@ class FluidWorld {
   LaunchTuning launch_tuning() const { return tuning_; }
   std::vector<TuneTrial> autotune(double dt, int steps);
 
+  // Adjoint of the f64 plain step (world.rs:183-397).  tape_begin makes the
+  // current state checkpoint 0 and records every following step's dt, with a
+  // state checkpoint every `every` steps; parameters must not change and
+  // body accelerations must not be set while recording.  step_backward runs
+  // the reverse sweep over the recorded steps, re-running each segment
+  // forward from its checkpoint: given dL/dx_T and dL/dv_T (insertion order,
+  // xyz interleaved; null = zero) it returns dL/dx_0, dL/dv_0 and
+  // {dL/d stiffness, dL/d visc_k[0]} (outputs may be null) and leaves the
+  // world in its state x_T, v_T.  The tape is kept for further sweeps.
+  void tape_begin(int every);
+  void tape_clear();
+  int tape_steps() const { return (int)tape_.dts.size(); }
+  void step_backward(const double* gx, const double* gv, double* gx0, double* gv0, double* gparams);
+
   // Insertion-order field access (particle.rs:17-46).
   static int components(int field);
   void get_field(int field, double* out);
@@ -150,6 +164,8 @@ class FluidWorld {
   void grow_scene_boxes(const double* d_pos3);
   void free_all();
   StepConsts prepare_step(double dt);
+  StepConsts step_impl(double dt);
+  void save_checkpoint();
   void enqueue_step(const StepConsts& c, const PassEvents& pe);
   void run_graph(double dt, int k);
   void drop_graphs();
@@ -198,6 +214,16 @@ class FluidWorld {
   std::vector<GraphEntry> graphs_;
   int graph_chunk_ = 0;
   unsigned long long alloc_gen_ = 0;  // bumped on every (re)allocation
+  // Adjoint tape: per-step dt and device checkpoints (6n doubles each: pos
+  // and vel, xyz interleaved, insertion order) every `every` steps.
+  struct Tape {
+    bool on = false;
+    int every = 1;
+    std::vector<double> dts;
+    std::vector<double*> ckpt;
+    PhySphParams params;
+  } tape_;
+  bool recomputing_ = false;
   // Autotuner state copy.
   std::vector<double*> snap_;
   int snap_cur_ = 0;

@@ -72,6 +72,10 @@ struct DevBuffers {
   double* stage = nullptr;   // 3 * capacity doubles
   uint32_t* flags = nullptr; // error bits, device
   unsigned long long* counters = nullptr;  // candidates, pairs (device)
+  // Optional outputs of the f64 plain force pass for the adjoint's tape: the
+  // raw viscous force and the strain-rate proxy of every sorted slot.
+  double* tape_fv[3] = {nullptr, nullptr, nullptr};
+  double* tape_shear = nullptr;
 };
 
 // grid.cu

@@ -73,6 +73,8 @@ struct PlainArgs {
   int stride;  // column stride of nbr (the buffer capacity)
   uint32_t* flags;
   unsigned long long* counters;
+  double* fv_out[3];  // nullable: raw viscous force (adjoint tape)
+  double* shear_out;  // nullable: strain-rate proxy (adjoint tape)
 };
 
 // compute_density_pressure (world.rs:204-246).  Also records, in visit
@@ -238,6 +240,12 @@ __global__ void __launch_bounds__(kThreads) k_force_plain(StepConsts c, PlainArg
   a.xsph[1][i] = q.xsy;
   a.xsph[2][i] = q.xsz;
   a.mu[i] = mu;
+  if (a.shear_out) {
+    a.fv_out[0][i] = q.fvx;
+    a.fv_out[1][i] = q.fvy;
+    a.fv_out[2][i] = q.fvz;
+    a.shear_out[i] = q.shear;
+  }
   // integrate (352-363): a = (acc + g) + body_acc; v += a dt; v += xsph eps; x += v dt.
   double bx = 0.0, by = 0.0, bz = 0.0;
   if (a.bax) {
@@ -312,6 +320,8 @@ void launch_plain_passes(const StepConsts& c, DevBuffers& b, cudaStream_t s, con
   a.stride = b.capacity;
   a.flags = b.flags;
   a.counters = b.counters;
+  for (int k = 0; k < 3; ++k) a.fv_out[k] = b.tape_fv[k];
+  a.shear_out = b.tape_shear;
   const int grid = (c.n + kThreads - 1) / kThreads;
   if (ev.after_prep) cudaEventRecord(ev.after_prep, s);
   if (a.counters)

@@ -345,6 +345,36 @@ class FluidWorld:
         return [{"ctas_per_sm": t.ctas_per_sm, "queue": t.queue, "sort_block": t.sort_block,
                  "ms_per_step": t.ms_per_step} for t in out[:min(n.value, cap)]]
 
+    # ---- adjoint (f64 plain form) ----------------------------------------------------
+    def tape_begin(self, checkpoint_every: int = 10) -> None:
+        """Starts recording steps for step_backward (phy_fluid_tape_begin)."""
+        L.check(self._lib.phy_fluid_tape_begin(self._h, self._sub, checkpoint_every), "phy_fluid_tape_begin")
+
+    def tape_clear(self) -> None:
+        L.check(self._lib.phy_fluid_tape_clear(self._h, self._sub), "phy_fluid_tape_clear")
+
+    @property
+    def tape_steps(self) -> int:
+        return int(self._lib.phy_fluid_tape_steps(self._h, self._sub))
+
+    def step_backward(self, grad_pos=None, grad_vel=None) -> dict:
+        """Reverse sweep over the recorded steps (phy_fluid_step_backward).  grad_pos, grad_vel:
+        dL/dpos_T, dL/dvel_T as (N, 3) arrays (None = zero).  Returns dL/dpos_0, dL/dvel_0 and the
+        parameter gradients {"stiffness", "visc_k0"}."""
+        n = len(self)
+        gp = None if grad_pos is None else np.ascontiguousarray(grad_pos, np.float64).reshape(-1)
+        gv = None if grad_vel is None else np.ascontiguousarray(grad_vel, np.float64).reshape(-1)
+        for g in (gp, gv):
+            if g is not None and g.size != 3 * n:
+                raise ValueError("gradients must hold 3 values per particle")
+        op = np.empty((n, 3), np.float64)
+        ov = np.empty((n, 3), np.float64)
+        par = np.empty(2, np.float64)
+        L.check(self._lib.phy_fluid_step_backward(self._h, self._sub, None if gp is None else _dp(gp),
+                                                  None if gv is None else _dp(gv), _dp(op), _dp(ov), _dp(par)),
+                "phy_fluid_step_backward")
+        return {"pos": op, "vel": ov, "stiffness": float(par[0]), "visc_k0": float(par[1])}
+
     # ---- batched scenes -----------------------------------------------------------
     def set_scenes(self, counts, bounds_min, bounds_max) -> None:
         """Partitions the particles (insertion order) into consecutive scenes with their own

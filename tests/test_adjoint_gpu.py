@@ -1,0 +1,180 @@
+"""Adjoint of the f64 plain step (phy_fluid_step_backward) against the oracle's
+forward-mode derivative and against central finite differences.
+
+The loss is the differentiation form's: L = mean_i |x_i(T) - target_i|^2 with
+target = initial lattice + (0.5, 0, 0) + N(0, 0.01^2), initial velocities
+f32-drawn N(0, 0.1^2).  The oracle's JVP (oracle/sph_oracle.cpp, Jvp) pushes
+tangents through the same piecewise-smooth map the adjoint reverses, so the
+two agree to rounding; finite differences agree as far as no branch (wall,
+neighbour set, max(0, .)) flips inside the +-eps interval."""
+import numpy as np
+import pytest
+
+from physics_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+DT = 0.005
+
+
+def _problem(dims=(8, 12, 8), box=2.4, seed=5):
+    sc = scenes.dam_break(*dims, box=box, dt=DT, steps=0)
+    rng = np.random.default_rng(seed)
+    v0 = (rng.standard_normal((sc.n, 3), dtype=np.float32) * np.float32(0.1)).astype(np.float64)
+    target = sc.pos + np.array([0.5, 0.0, 0.0]) + rng.normal(0.0, 0.01, (sc.n, 3))
+    return sc, v0, target
+
+
+def _params(sc, stiffness=None, visc=None):
+    from physics_b200 import SphParams
+    p = SphParams.defaults()
+    p.bounds_min, p.bounds_max = sc.bounds_min, sc.bounds_max
+    if stiffness is not None:
+        p.stiffness = stiffness
+    if visc is not None:
+        p.visc_k = [visc]
+    return p
+
+
+def _gpu_world(gpu, sc, v0, **kw):
+    w = gpu.FluidWorld(_params(sc, **kw), "f64")
+    w.add_particles(sc.pos, np.full(sc.n, sc.mass), vel=v0)
+    return w
+
+
+def _loss_grad(x, target):
+    n = x.shape[0]
+    return float(np.mean(np.sum((x - target) ** 2, axis=1))), 2.0 * (x - target) / n
+
+
+def _adjoint(gpu, sc, v0, target, steps, every, **kw):
+    w = _gpu_world(gpu, sc, v0, **kw)
+    w.tape_begin(every)
+    w.step(DT, steps)
+    L, g = _loss_grad(w.pos, target)
+    return w, L, w.step_backward(g, None)
+
+
+def _loss(gpu, sc, v0, target, steps, **kw):
+    w = _gpu_world(gpu, sc, v0, **kw)
+    w.step(DT, steps)
+    return _loss_grad(w.pos, target)[0]
+
+
+def _unit(rng, shape):
+    d = rng.normal(size=shape)
+    return d / np.linalg.norm(d)
+
+
+def test_adjoint_matches_oracle_jvp(gpu, oracle_mod):
+    O = oracle_mod
+    sc, v0, target = _problem()
+    steps = 24
+    w, L, g = _adjoint(gpu, sc, v0, target, steps, every=5)
+    xT = w.pos
+    rng = np.random.default_rng(1)
+    for k in range(3):
+        dv = _unit(rng, v0.shape)
+        dx = _unit(rng, v0.shape) if k == 2 else np.zeros_like(v0)
+        ow = O.OracleWorld(_params(sc), threads=O.max_threads())
+        ow.add_particles(sc.pos, np.full(sc.n, sc.mass), vel=v0)
+        tx, _ = ow.jvp(DT, steps, dx, dv)
+        assert np.array_equal(ow.get(O.F_POS).view(np.uint64), xT.view(np.uint64))  # same primal, bit for bit
+        want = float(np.sum(2.0 * (xT - target) / sc.n * tx))
+        got = float(np.sum(g["vel"] * dv) + np.sum(g["pos"] * dx))
+        assert abs(got - want) <= 1e-9 * abs(want) + 1e-18, (k, got, want)
+    for dk, dc, key in ((1.0, 0.0, "stiffness"), (0.0, 1.0, "visc_k0")):
+        ow = O.OracleWorld(_params(sc), threads=O.max_threads())
+        ow.add_particles(sc.pos, np.full(sc.n, sc.mass), vel=v0)
+        tx, _ = ow.jvp(DT, steps, np.zeros_like(v0), np.zeros_like(v0), dk, dc)
+        want = float(np.sum(2.0 * (xT - target) / sc.n * tx))
+        assert abs(g[key] - want) <= 1e-8 * abs(want) + 1e-18, (key, g[key], want)
+
+
+def test_adjoint_checkpoint_interval_changes_no_bit(gpu):
+    sc, v0, target = _problem()
+    outs = [_adjoint(gpu, sc, v0, target, 17, every)[2] for every in (1, 4, 17, 40)]
+    for o in outs[1:]:
+        assert np.array_equal(o["vel"].view(np.uint64), outs[0]["vel"].view(np.uint64))
+        assert np.array_equal(o["pos"].view(np.uint64), outs[0]["pos"].view(np.uint64))
+        assert o["stiffness"] == outs[0]["stiffness"] and o["visc_k0"] == outs[0]["visc_k0"]
+
+
+def test_adjoint_central_differences(gpu):
+    sc, v0, target = _problem()
+    steps, eps = 24, 1e-4
+    _, _, g = _adjoint(gpu, sc, v0, target, steps, every=6)
+    rng = np.random.default_rng(2)
+    for _ in range(4):
+        d = _unit(rng, v0.shape)
+        fd = (_loss(gpu, sc, v0 + eps * d, target, steps) - _loss(gpu, sc, v0 - eps * d, target, steps)) / (2 * eps)
+        ad = float(np.sum(g["vel"] * d))
+        assert abs(ad - fd) <= 1e-4 * abs(fd), (ad, fd)
+    # visc_k[0] (3.5): eps = 1e-4 absolute.
+    fd = (_loss(gpu, sc, v0, target, steps, visc=3.5 + eps) - _loss(gpu, sc, v0, target, steps, visc=3.5 - eps)) / (
+        2 * eps)
+    assert abs(g["visc_k0"] - fd) <= 1e-4 * abs(fd), (g["visc_k0"], fd)
+    # stiffness (250): its derivative is small, so a relative step of 1e-4 keeps rounding out of the quotient.
+    h = 250.0 * 1e-4
+    fd = (_loss(gpu, sc, v0, target, steps, stiffness=250.0 + h) -
+          _loss(gpu, sc, v0, target, steps, stiffness=250.0 - h)) / (2 * h)
+    assert abs(g["stiffness"] - fd) <= 1e-3 * abs(fd), (g["stiffness"], fd)
+
+
+def test_backward_keeps_state_and_tape(gpu):
+    sc, v0, target = _problem()
+    w = _gpu_world(gpu, sc, v0)
+    w.tape_begin(4)
+    w.step(DT, 9)
+    assert w.tape_steps == 9
+    before = (w.pos, w.vel, w.rho)
+    L, gx = _loss_grad(w.pos, target)
+    g1 = w.step_backward(gx, None)
+    after = (w.pos, w.vel, w.rho)
+    for a, b in zip(before, after):
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    g2 = w.step_backward(gx, None)  # the tape is kept
+    assert np.array_equal(g1["vel"].view(np.uint64), g2["vel"].view(np.uint64))
+    # Stepping on matches a world that never ran a backward sweep.
+    ref = _gpu_world(gpu, sc, v0)
+    ref.step(DT, 9)
+    w.tape_clear()
+    w.step(DT, 5)
+    ref.step(DT, 5)
+    assert np.array_equal(w.pos.view(np.uint64), ref.pos.view(np.uint64))
+
+
+def test_tape_argument_errors(gpu):
+    from physics_b200 import PhyError
+    sc, v0, target = _problem()
+    comp = gpu.FluidWorld(_params(sc), "comp")
+    comp.add_particles(sc.pos, np.full(sc.n, sc.mass))
+    with pytest.raises(PhyError):
+        comp.tape_begin(5)
+    w = _gpu_world(gpu, sc, v0)
+    with pytest.raises(PhyError):
+        w.step_backward(np.zeros((sc.n, 3)))
+    w.tape_begin(5)
+    w.step(DT, 2)
+    p = w.params
+    p.stiffness = 300.0
+    w.params = p
+    with pytest.raises(PhyError):
+        w.step(DT)
+
+
+def test_gradient_64k_form(gpu):
+    """The differentiation form: 64k-particle dam break, 100 steps at dt 0.005, a
+    checkpoint every 10 steps; adjoint vs central differences on 4 directions."""
+    sc, v0, target = _problem((32, 64, 32), 12.8, seed=64)
+    steps, eps = 100, 1e-4
+    _, L, g = _adjoint(gpu, sc, v0, target, steps, every=10)
+    assert np.all(np.isfinite(g["vel"]))
+    rng = np.random.default_rng(3)
+    errs = []
+    for _ in range(4):
+        d = _unit(rng, v0.shape)
+        fd = (_loss(gpu, sc, v0 + eps * d, target, steps) - _loss(gpu, sc, v0 - eps * d, target, steps)) / (2 * eps)
+        errs.append(abs(float(np.sum(g["vel"] * d)) - fd) / abs(fd))
+    print("64k relative errors vs central differences", errs)
+    assert max(errs) <= 1e-4, errs
