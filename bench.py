@@ -201,6 +201,112 @@ def run_batched(pb, scenes, stream, n_scenes: int, steps: int, warmup: int) -> d
     }
 
 
+ADJ_DIMS = (32, 64, 32)
+ADJ_BOX = 12.8
+ADJ_DT = 0.005
+ADJ_STEPS = 100
+ADJ_EVERY = 10
+
+
+def adjoint_problem(scenes, seed: int = 64):
+    """The differentiation form: 64k-particle dam break, initial velocities f32-drawn
+    N(0, 0.1^2), target = initial lattice + (0.5, 0, 0) + N(0, 0.01^2)."""
+    pos = scenes.dam_break_positions(*ADJ_DIMS)
+    rng = np.random.default_rng(seed)
+    v0 = (rng.standard_normal(pos.shape, dtype=np.float32) * np.float32(0.1)).astype(np.float64)
+    target = pos + np.array([0.5, 0.0, 0.0]) + rng.normal(0.0, 0.01, pos.shape)
+    return pos, v0, target
+
+
+def run_adjoint(pb, scenes, stream, directions: int) -> dict:
+    """step_backward on the differentiation form: device time of the 100-step forward, of
+    the recorded forward and of the reverse sweep (checkpoint every 10 steps, segments
+    re-run forward), and the gradient against central finite differences (eps = 1e-4)
+    of the same f64 plain forward on `directions` random unit directions."""
+    import torch
+    pos, v0, target = adjoint_problem(scenes)
+    n = pos.shape[0]
+    mass = scenes.lattice_mass(scenes.SPACING)
+
+    def world(v, stiffness=None, visc=None):
+        p = pb.SphParams.defaults()
+        p.bounds_min, p.bounds_max = (0.0, 0.0, 0.0), (ADJ_BOX, ADJ_BOX, ADJ_BOX)
+        if stiffness is not None:
+            p.stiffness = stiffness
+        if visc is not None:
+            p.visc_k = [visc]
+        w = pb.FluidWorld(p, "f64")
+        w.set_stream(stream.cuda_stream)
+        w.add_particles(pos, mass, vel=v)
+        return w
+
+    def loss(x):
+        return float(np.mean(np.sum((x - target) ** 2, axis=1)))
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    warm = world(v0)
+    warm.step(ADJ_DT, 10)
+    w = world(v0)
+    fwd_ms, _ = timed(lambda: w.step(ADJ_DT, ADJ_STEPS))
+    w = world(v0)
+    w.tape_begin(ADJ_EVERY)
+    taped_ms, _ = timed(lambda: w.step(ADJ_DT, ADJ_STEPS))
+    xT = w.pos
+    L = loss(xT)
+    gx = 2.0 * (xT - target) / n
+    w.step_backward(gx, None)  # warm-up sweep (allocations)
+    t0 = time.perf_counter()
+    bwd_ms, g = timed(lambda: w.step_backward(gx, None))
+    bwd_wall_ms = (time.perf_counter() - t0) * 1e3
+    del w, warm
+
+    def run_loss(v, **kw):
+        q = world(v, **kw)
+        q.step(ADJ_DT, ADJ_STEPS)
+        return loss(q.pos)
+
+    eps = 1e-4
+    rng = np.random.default_rng(7)
+    errs = []
+    for _ in range(directions):
+        d = rng.normal(size=v0.shape)
+        d /= np.linalg.norm(d)
+        fd = (run_loss(v0 + eps * d) - run_loss(v0 - eps * d)) / (2 * eps)
+        errs.append(abs(float(np.sum(g["vel"] * d)) - fd) / abs(fd))
+    fd_visc = (run_loss(v0, visc=3.5 + eps) - run_loss(v0, visc=3.5 - eps)) / (2 * eps)
+    hk = 250.0 * eps
+    fd_stiff = (run_loss(v0, stiffness=250.0 + hk) - run_loss(v0, stiffness=250.0 - hk)) / (2 * hk)
+    return {
+        "workload": f"dam_break_{ADJ_DIMS[0]}x{ADJ_DIMS[1]}x{ADJ_DIMS[2]}: {n} particles, {ADJ_STEPS} steps at "
+                    f"dt={ADJ_DT}, checkpoint every {ADJ_EVERY}; loss = mean |x_T - target|^2",
+        "particles": n,
+        "loss": L,
+        "forward_ms": fwd_ms,
+        "recorded_forward_ms": taped_ms,
+        "backward_ms": bwd_ms,
+        "backward_wall_ms": bwd_wall_ms,
+        "backward_over_forward": bwd_ms / fwd_ms,
+        "fd_directions": directions,
+        "fd_eps": eps,
+        "fd_max_rel_err": max(errs),
+        "fd_median_rel_err": float(np.median(errs)),
+        "grad_visc_k0": g["visc_k0"],
+        "fd_visc_k0_rel_err": abs(g["visc_k0"] - fd_visc) / abs(fd_visc),
+        "grad_stiffness": g["stiffness"],
+        "fd_stiffness_rel_err": abs(g["stiffness"] - fd_stiff) / abs(fd_stiff),
+        "fd_stiffness_step": hk,
+    }
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -315,6 +421,10 @@ def run_ours(args):
     cnt = comp.step_counters()
     comp.set_counting(False)
 
+    adjoint = None
+    if args.adjoint_directions > 0:
+        adjoint = run_adjoint(pb, scenes, stream, args.adjoint_directions)
+
     batched = None
     if args.batch_scenes > 0 and args.batch_steps > 0:
         batched = run_batched(pb, scenes, stream, args.batch_scenes, args.batch_steps, W)
@@ -404,6 +514,7 @@ def run_ours(args):
             "clocks": clocks,
             "cpu_baseline": cpu,
             "batched": batched,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     if world_size > 1:
@@ -487,6 +598,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--batch-scenes", type=int, default=256, help="scenes of the batched form (0: skip)")
+    ap.add_argument("--adjoint-directions", type=int, default=32,
+                    help="finite-difference directions of the adjoint check (0: skip the adjoint)")
     ap.add_argument("--batch-steps", type=int, default=200, help="timed steps of the batched form")
     ap.add_argument("--full-steps", type=int, default=1000,
                     help="also time this many steps from the initial dam (the configured 1000-step run; "

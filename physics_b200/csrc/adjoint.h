@@ -27,6 +27,11 @@ struct AdjTape {
   const double* fv[3];  // raw viscous force (before mu)
   const double* shear;  // strain-rate proxy
   const uint32_t* cell_start;
+  // The density pass's neighbour lists (entry k of slot i at nbr[k * n + i],
+  // every j != i not excluded by r >= h, in visit order); a count above
+  // kMaxNeighbors means the list overflowed and the 27 cells are rescanned.
+  const uint32_t* nbr;
+  const uint32_t* nbr_count;
 };
 
 // Adjoint state: gx_ins / gv_ins hold dL/dx, dL/dv in insertion order

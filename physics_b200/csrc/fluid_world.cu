@@ -188,6 +188,31 @@ __global__ void __launch_bounds__(kThreads) k_scene_bbox(const double* __restric
   }
 }
 
+// One recorded step of the adjoint tape: every per-particle array of the
+// step copied in one launch (22 f64 arrays, 2 u32 arrays).
+struct TapeCopy {
+  const double* src[22];
+  double* dst[22];
+  const uint32_t* usrc[3];  // mat, id, neighbour count
+  uint32_t* udst[3];
+  const uint32_t* nbr;      // column-major, stride nbr_stride
+  uint32_t* nbr_dst;        // column-major, stride n
+  int nbr_stride;
+};
+
+__global__ void k_tape_copy(int n, TapeCopy t) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+#pragma unroll
+  for (int k = 0; k < 22; ++k) t.dst[k][s] = t.src[k][s];
+  t.udst[0][s] = t.usrc[0][s];
+  t.udst[1][s] = t.usrc[1][s];
+  const uint32_t cnt = t.usrc[2][s];
+  t.udst[2][s] = cnt;
+  const uint32_t m = cnt < (uint32_t)kMaxNeighbors ? cnt : (uint32_t)kMaxNeighbors;
+  for (uint32_t k = 0; k < m; ++k) t.nbr_dst[(size_t)k * n + s] = t.nbr[(size_t)k * t.nbr_stride + s];
+}
+
 // num-traits ToPrimitive::to_i64 on f64 with None -> 0 (grid.rs:25-33).
 long long key_axis_host(double x, double inv) {
   double f = std::floor(x * inv);
@@ -1136,27 +1161,39 @@ void FluidWorld::snapshot(bool restore) {
     arrays.push_back({b_.acc[k], n * 8});
     arrays.push_back({b_.xsph[k], n * 8});
   }
+  // One arena, reused while large enough; each array at a 256-byte offset.
+  std::vector<size_t> off(arrays.size());
+  size_t total = 0;
+  for (size_t q = 0; q < arrays.size(); ++q) {
+    off[q] = total;
+    total += (arrays[q].second + 255) / 256 * 256;
+  }
   if (!restore) {
-    release_snapshot();
-    snap_.assign(arrays.size(), nullptr);
-    for (size_t q = 0; q < arrays.size(); ++q) {
-      dalloc(snap_[q], (arrays[q].second + 7) / 8);
-      cuda_check(cudaMemcpyAsync(snap_[q], arrays[q].first, arrays[q].second, cudaMemcpyDeviceToDevice, stream_),
-                 "snapshot");
+    if (total > snap_bytes_) {
+      release_snapshot();
+      dalloc(snap_arena_, total / 8);
+      snap_bytes_ = total;
     }
-    snap_cur_ = b_.cur;
-  } else {
-    if (snap_.size() != arrays.size()) throw std::logic_error("snapshot: no saved state of this layout");
     for (size_t q = 0; q < arrays.size(); ++q)
-      cuda_check(cudaMemcpyAsync(arrays[q].first, snap_[q], arrays[q].second, cudaMemcpyDeviceToDevice, stream_),
+      cuda_check(cudaMemcpyAsync(reinterpret_cast<char*>(snap_arena_) + off[q], arrays[q].first, arrays[q].second,
+                                 cudaMemcpyDeviceToDevice, stream_),
+                 "snapshot");
+    snap_cur_ = b_.cur;
+    snap_count_ = arrays.size();
+  } else {
+    if (snap_count_ != arrays.size() || !snap_arena_) throw std::logic_error("snapshot: no saved state of this layout");
+    for (size_t q = 0; q < arrays.size(); ++q)
+      cuda_check(cudaMemcpyAsync(arrays[q].first, reinterpret_cast<char*>(snap_arena_) + off[q], arrays[q].second,
+                                 cudaMemcpyDeviceToDevice, stream_),
                  "restore");
   }
   cuda_check(cudaStreamSynchronize(stream_), "snapshot sync");
 }
 
 void FluidWorld::release_snapshot() {
-  for (auto& p : snap_) dfree(p);
-  snap_.clear();
+  dfree(snap_arena_);
+  snap_bytes_ = 0;
+  snap_count_ = 0;
 }
 
 std::vector<TuneTrial> FluidWorld::autotune(double dt, int steps) {
@@ -1305,21 +1342,34 @@ namespace phy {
 // ---- Adjoint ---------------------------------------------------------------------
 
 void FluidWorld::save_checkpoint() {
-  double* ck = nullptr;
-  dalloc(ck, 6 * n_);
+  const size_t k = tape_.nckpt;
+  if (k >= tape_.ckpt.size()) {
+    tape_.ckpt.push_back(nullptr);
+    dalloc(tape_.ckpt.back(), 6 * n_);
+  }
+  double* ck = tape_.ckpt[k];
   const ParticleConsts& pc = b_.pc[b_.cur];
   k_get_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>((int)n_, pc.id, b_.pv1[0], b_.pv1[1], b_.pv1[2], ck);
   k_get_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>((int)n_, pc.id, b_.pv1[3], b_.pv1[4], b_.pv1[5],
                                                            ck + 3 * n_);
   cuda_check(cudaGetLastError(), "checkpoint");
-  tape_.ckpt.push_back(ck);
+  ++tape_.nckpt;
 }
 
 void FluidWorld::tape_clear() {
   for (auto& p : tape_.ckpt) dfree(p);
   tape_.ckpt.clear();
+  tape_.nckpt = 0;
   tape_.dts.clear();
   tape_.on = false;
+  tape_.n = 0;
+  dfree(adj_work_);
+  for (auto& p : adj_slot_f_) dfree(p);
+  for (auto& p : adj_slot_u_) dfree(p);
+  adj_slot_f_.clear();
+  adj_slot_u_.clear();
+  adj_slot_ucount_.clear();
+  release_snapshot();
 }
 
 void FluidWorld::tape_begin(int every) {
@@ -1328,7 +1378,11 @@ void FluidWorld::tape_begin(int every) {
   if (b_.has_ba) throw std::invalid_argument("tape_begin: body accelerations are not recorded");
   if (every < 1) throw std::invalid_argument("tape_begin: checkpoint interval must be >= 1");
   if (n_ == 0) throw std::invalid_argument("tape_begin: empty world");
-  tape_clear();
+  // Checkpoint and sweep buffers are kept for the next tape of the same size.
+  if (tape_.n != n_) tape_clear();
+  tape_.n = n_;
+  tape_.nckpt = 0;
+  tape_.dts.clear();
   tape_.every = every;
   tape_.params = params.to_c();
   save_checkpoint();
@@ -1340,7 +1394,7 @@ namespace {
 // Device arrays of one recorded step (sorted order) plus its launch constants.
 struct TapeSlot {
   double* f = nullptr;       // 22 arrays of n doubles
-  uint32_t* u = nullptr;     // mat, id (n each) and cell_start
+  uint32_t* u = nullptr;     // mat, id, nbr_count (n each), nbr (96 n), cell_start
   StepConsts c;
   AdjTape view(size_t n) const {
     AdjTape t;
@@ -1364,7 +1418,9 @@ struct TapeSlot {
     t.shear = take();
     t.mat = u;
     t.id = u + n;
-    t.cell_start = u + 2 * n;
+    t.nbr_count = u + 2 * n;
+    t.nbr = u + 3 * n;
+    t.cell_start = u + (3 + (size_t)kMaxNeighbors) * n;
     return t;
   }
 };
@@ -1381,8 +1437,8 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
   // rbar_tot, cc, kk, the tape's fv and shear outputs (4): 30 arrays of n,
   // then the two parameter accumulators.
   constexpr size_t kWorkArrays = 30;
-  double* work = nullptr;
-  dalloc(work, kWorkArrays * n + 2);
+  if (!adj_work_) dalloc(adj_work_, kWorkArrays * n + 2);
+  double* work = adj_work_;
   AdjWork w;
   {
     double* q = work;
@@ -1411,14 +1467,14 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
   }
   const int nslots = std::min(tape_.every, std::max(T, 1));
   std::vector<TapeSlot> slots(nslots);
+  if ((int)adj_slot_f_.size() < nslots) {
+    adj_slot_f_.resize(nslots, nullptr);
+    adj_slot_u_.resize(nslots, nullptr);
+    adj_slot_ucount_.resize(nslots, 0);
+  }
   auto cleanup = [&]() {
-    for (auto& sl : slots) {
-      dfree(sl.f);
-      dfree(sl.u);
-    }
     for (int k = 0; k < 3; ++k) b_.tape_fv[k] = nullptr;
     b_.tape_shear = nullptr;
-    dfree(work);
     recomputing_ = false;
   };
   try {
@@ -1449,38 +1505,54 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
                                                        b_.pv1[5]);
       for (int t = t0; t < t1; ++t) {
         TapeSlot& sl = slots[t - t0];
+        const int si = t - t0;
         const StepConsts c = step_impl(tape_.dts[t]);
         const size_t ncs = (size_t)c.ncells + 2;
-        if (!sl.f) dalloc(sl.f, 22 * n);
-        if (!sl.u || sl.c.ncells != c.ncells) dalloc(sl.u, 2 * n + ncs);
+        const size_t ucount = (3 + (size_t)kMaxNeighbors) * n + ncs;
+        if (!adj_slot_f_[si]) dalloc(adj_slot_f_[si], 22 * n);
+        if (adj_slot_ucount_[si] < ucount) {
+          dalloc(adj_slot_u_[si], ucount);
+          adj_slot_ucount_[si] = ucount;
+        }
+        sl.f = adj_slot_f_[si];
+        sl.u = adj_slot_u_[si];
         sl.c = c;
         const AdjTape v = sl.view(n);
         const ParticleConsts& q = b_.pc[b_.cur];
         const size_t B = n * sizeof(double);
-        auto copy = [&](const void* dst, const void* src, size_t bytes, const char* what) {
-          const cudaError_t e = cudaMemcpyAsync(const_cast<void*>(dst), src, bytes, cudaMemcpyDeviceToDevice, s);
-          if (e != cudaSuccess)
-            throw CudaError(std::string("tape copy of ") + what + ": " + cudaGetErrorString(e) + " (" +
-                            std::to_string(bytes) + " bytes, dst " + std::to_string((uintptr_t)dst) + ", src " +
-                            std::to_string((uintptr_t)src) + ")");
+        TapeCopy tc;
+        int k = 0;
+        auto add = [&](const double* dst, const double* src) {
+          tc.dst[k] = const_cast<double*>(dst);
+          tc.src[k] = src;
+          ++k;
         };
-        for (int k = 0; k < 3; ++k) {
-          copy(v.x[k], b_.pv0[k], B, "x");
-          copy(v.v[k], b_.pv0[3 + k], B, "v");
-          copy(v.acc[k], b_.acc[k], B, "acc");
-          copy(v.xsph[k], b_.xsph[k], B, "xsph");
-          copy(v.fv[k], b_.tape_fv[k], B, "fv");
-        }
-        copy(v.mass, q.mass, B, "mass");
-        copy(v.rho, b_.rho, B, "rho");
-        copy(v.p, b_.p, B, "p");
-        copy(v.pr2, b_.pr2, B, "pr2");
-        copy(v.mr, b_.mr, B, "mr");
-        copy(v.mu, b_.mu, B, "mu");
-        copy(v.shear, b_.tape_shear, B, "shear");
-        copy(v.mat, q.mat, n * 4, "mat");
-        copy(v.id, q.id, n * 4, "id");
-        copy(v.cell_start, b_.cell_start, ncs * 4, "cell_start");
+        for (int a = 0; a < 3; ++a) add(v.x[a], b_.pv0[a]);
+        for (int a = 0; a < 3; ++a) add(v.v[a], b_.pv0[3 + a]);
+        add(v.mass, q.mass);
+        add(v.rho, b_.rho);
+        add(v.p, b_.p);
+        add(v.pr2, b_.pr2);
+        add(v.mr, b_.mr);
+        for (int a = 0; a < 3; ++a) add(v.acc[a], b_.acc[a]);
+        for (int a = 0; a < 3; ++a) add(v.xsph[a], b_.xsph[a]);
+        add(v.mu, b_.mu);
+        for (int a = 0; a < 3; ++a) add(v.fv[a], b_.tape_fv[a]);
+        add(v.shear, b_.tape_shear);
+        if (k != 22) throw std::logic_error("step_backward: tape layout");
+        tc.usrc[0] = q.mat;
+        tc.udst[0] = const_cast<uint32_t*>(v.mat);
+        tc.usrc[1] = q.id;
+        tc.udst[1] = const_cast<uint32_t*>(v.id);
+        tc.usrc[2] = b_.nbr_count;
+        tc.udst[2] = const_cast<uint32_t*>(v.nbr_count);
+        tc.nbr = b_.nbr;
+        tc.nbr_dst = const_cast<uint32_t*>(v.nbr);
+        tc.nbr_stride = b_.capacity;
+        k_tape_copy<<<grid_for(n), kThreads, 0, s>>>((int)n, tc);
+        cuda_check(cudaMemcpyAsync(const_cast<uint32_t*>(v.cell_start), b_.cell_start, ncs * 4,
+                                   cudaMemcpyDeviceToDevice, s),
+                   "tape copy");
       }
       for (int t = t1 - 1; t >= t0; --t) launch_adjoint_step(slots[t - t0].c, slots[t - t0].view(n), w, s);
       cuda_check(cudaGetLastError(), "adjoint step");
@@ -1501,13 +1573,9 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
       gparams[1] = pa[1];
     }
     snapshot(true);
-    release_snapshot();
   } catch (...) {
     cleanup();
-    if (!snap_.empty()) {
-      snapshot(true);
-      release_snapshot();
-    }
+    if (snap_count_) snapshot(true);
     throw;
   }
   cleanup();

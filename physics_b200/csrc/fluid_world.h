@@ -219,13 +219,22 @@ class FluidWorld {
   struct Tape {
     bool on = false;
     int every = 1;
+    size_t n = 0;        // particle count the buffers are sized for
     std::vector<double> dts;
-    std::vector<double*> ckpt;
+    std::vector<double*> ckpt;  // pool; the first nckpt are this tape's
+    size_t nckpt = 0;
     PhySphParams params;
   } tape_;
+  // Reverse-sweep buffers kept between sweeps (freed by tape_clear).
+  double* adj_work_ = nullptr;
+  std::vector<double*> adj_slot_f_;
+  std::vector<uint32_t*> adj_slot_u_;
+  std::vector<size_t> adj_slot_ucount_;
   bool recomputing_ = false;
-  // Autotuner state copy.
-  std::vector<double*> snap_;
+  // Saved state (autotuner, reverse sweep): one arena reused while large enough.
+  double* snap_arena_ = nullptr;
+  size_t snap_bytes_ = 0;
+  size_t snap_count_ = 0;
   int snap_cur_ = 0;
 };
 

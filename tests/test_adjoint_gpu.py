@@ -178,3 +178,22 @@ def test_gradient_64k_form(gpu):
         errs.append(abs(float(np.sum(g["vel"] * d)) - fd) / abs(fd))
     print("64k relative errors vs central differences", errs)
     assert max(errs) <= 1e-4, errs
+
+
+def test_gradient_64k_form_vs_oracle_jvp(gpu, oracle_mod):
+    """The 64k differentiation form against the oracle's forward-mode derivative
+    along one combined direction (initial velocities, stiffness and visc_k[0])."""
+    O = oracle_mod
+    sc, v0, target = _problem((32, 64, 32), 12.8, seed=64)
+    steps = 100
+    w, L, g = _adjoint(gpu, sc, v0, target, steps, every=10)
+    xT = w.pos
+    d = _unit(np.random.default_rng(4), v0.shape)
+    ow = O.OracleWorld(_params(sc), threads=O.max_threads())
+    ow.add_particles(sc.pos, np.full(sc.n, sc.mass), vel=v0)
+    tx, _ = ow.jvp(DT, steps, np.zeros_like(v0), d, 1.0, 1.0)
+    assert np.array_equal(ow.get(O.F_POS).view(np.uint64), xT.view(np.uint64))
+    want = float(np.sum(2.0 * (xT - target) / sc.n * tx))
+    got = float(np.sum(g["vel"] * d)) + g["stiffness"] + g["visc_k0"]
+    print("64k adjoint vs oracle JVP", got, want, abs(got - want) / abs(want))
+    assert abs(got - want) <= 1e-8 * abs(want), (got, want)
