@@ -201,6 +201,13 @@ struct GatherArgs {
   int has_ba;
   const uint32_t* cell_of;
   uint32_t* sorted_cell;  // nullable: cell of every sorted slot
+  // Tiled compensated form (nullable): the f32 operands of every sorted slot
+  // (cell-local position and mass; velocity), and the persistent passes' work
+  // queues, reset here.
+  float4* cpos;
+  float4* cvel;
+  uint32_t* queue;
+  double inv_cell, h0;
 };
 
 __global__ void __launch_bounds__(kThreads) k_gather(int n, const uint32_t* __restrict__ perm, GatherArgs g) {
@@ -218,6 +225,18 @@ __global__ void __launch_bounds__(kThreads) k_gather(int n, const uint32_t* __re
   }
   if (g.src.scene) g.dst.scene[s] = g.src.scene[i];
   if (g.sorted_cell) g.sorted_cell[s] = g.cell_of[i];
+  if (g.cpos) {
+    // Cell-local f32 coordinates (the cell is that of the f64 cell key).
+    const double x = g.dst_pv[0][s], y = g.dst_pv[1][s], z = g.dst_pv[2][s];
+    const long long kx = key_axis(x, g.inv_cell), ky = key_axis(y, g.inv_cell), kz = key_axis(z, g.inv_cell);
+    g.cpos[s] = make_float4((float)(x - (double)kx * g.h0), (float)(y - (double)ky * g.h0),
+                            (float)(z - (double)kz * g.h0), (float)g.dst.mass[s]);
+    g.cvel[s] = make_float4((float)g.dst_pv[3][s], (float)g.dst_pv[4][s], (float)g.dst_pv[5][s], 0.0f);
+    if (s == 0 && g.queue) {
+      g.queue[0] = 0;
+      g.queue[1] = 0;
+    }
+  }
 }
 
 // Tile list of a tiled sort: head[s] = 1 where slot s starts a new tile
@@ -332,6 +351,11 @@ void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s, int block) 
   g.has_ba = b.has_ba ? 1 : 0;
   g.cell_of = b.cell_of;
   g.sorted_cell = c.tile ? b.sorted_cell : nullptr;
+  g.cpos = c.tile ? b.cpos : nullptr;
+  g.cvel = c.tile ? b.cvel : nullptr;
+  g.queue = c.tile ? b.queue : nullptr;
+  g.inv_cell = c.inv_cell;
+  g.h0 = c.h0;
   k_gather<<<grid_for(n, bs), bs, 0, s>>>(n, b.perm, g);
   b.cur ^= 1;
   if (c.tile) {

@@ -262,7 +262,8 @@ __device__ __forceinline__ void write_density(const StepConsts& c, const TiledAr
 
 // Density of particle qi from global memory (tiles that do not fit the
 // staging buffer): 27 cells by tiled index, cell-local offsets.
-__device__ void density_global(const StepConsts& c, const TiledArgs& a, int qi, const SceneBox& box) {
+__device__ void density_global(const StepConsts& c, const TiledArgs& a, int qi, int sc) {
+  const SceneBox& box = c.boxes[sc];
   const double xi = a.px[qi], yi = a.py[qi], zi = a.pz[qi];
   const long long kx = key_axis(xi, c.inv_cell), ky = key_axis(yi, c.inv_cell), kz = key_axis(zi, c.inv_cell);
   const float4 pi = a.cpos[qi];
@@ -343,7 +344,7 @@ __global__ void __launch_bounds__(kTT) k_density_tiled(StepConsts c, TiledArgs a
     const int slab = pick_slab(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
     if (slab == 0) {
       for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT)
-        density_global(c, a, (int)qi, c.boxes[g.sc]);
+        density_global(c, a, (int)qi, g.sc);
       continue;  // uniform across the CTA
     }
     for (int x0 = 0; x0 < kTB; x0 += slab) {
@@ -519,7 +520,8 @@ __device__ __forceinline__ void finish_particle(const StepConsts& c, const Tiled
 }
 
 // Forces of particle qi from global memory (tiles that were not staged).
-__device__ void force_global(const StepConsts& c, const TiledArgs& a, int qi, const SceneBox& box) {
+__device__ void force_global(const StepConsts& c, const TiledArgs& a, int qi, int sc) {
+  const SceneBox& box = c.boxes[sc];
   const double xi = a.px[qi], yi = a.py[qi], zi = a.pz[qi];
   const long long kx = key_axis(xi, c.inv_cell), ky = key_axis(yi, c.inv_cell), kz = key_axis(zi, c.inv_cell);
   const float4 pi = a.cpos[qi];
@@ -594,8 +596,11 @@ __device__ __forceinline__ void pair_listed(const StepConsts& c, float4 pj, floa
 
 __global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
-  float4* s_rec = reinterpret_cast<float4*>(smem);  // slot k: [2k] = position, [2k+1] = velocity
-  float* s_mr = reinterpret_cast<float*>(s_rec + 2 * kHaloCap);
+  // Staged neighbour records as separate 16-byte arrays (a 32-byte record
+  // stride would map every record onto 4 of the 8 bank quads).
+  float4* s_pos = reinterpret_cast<float4*>(smem);
+  float4* s_vel = s_pos + kHaloCap;
+  float* s_mr = reinterpret_cast<float*>(s_vel + kHaloCap);
   uint32_t* s_src = reinterpret_cast<uint32_t*>(s_mr + kHaloCap);
   uint32_t* s_end = s_src + kNH;
   uint32_t* s_off = s_end + kNH;
@@ -609,7 +614,7 @@ __global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) 
     halo_table(c, a, g, s_src, s_end, s_off, ws);
     const int slab = pick_slab(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
     if (slab == 0) {
-      for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT) force_global(c, a, (int)qi, c.boxes[g.sc]);
+      for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT) force_global(c, a, (int)qi, g.sc);
       continue;
     }
     for (int x0 = 0; x0 < kTB; x0 += slab) {
@@ -617,13 +622,13 @@ __global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) 
     stage_halo(
         s_src, s_end, s_off, x0 * kH, (x0 + slab + 2) * kH, base,
         [&](uint32_t slot, int h, uint32_t src) {
-          s_rec[2 * slot] = tile_rel(c, a.cpos[src], h);
-          s_rec[2 * slot + 1] = a.cvel[src];
+          s_pos[slot] = tile_rel(c, a.cpos[src], h);
+          s_vel[slot] = a.cvel[src];
           s_mr[slot] = a.cmr[src];
         },
         [&](uint32_t slot) {
-          s_rec[2 * slot] = make_float4(kFar, kFar, kFar, 0.f);
-          s_rec[2 * slot + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+          s_pos[slot] = make_float4(kFar, kFar, kFar, 0.f);
+          s_vel[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
           s_mr[slot] = 0.f;
         });
     __syncthreads();
@@ -632,8 +637,8 @@ __global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) 
     for (uint32_t qi = qfirst + threadIdx.x; qi < qlast; qi += kTT) {
       const int hq = own_halo_cell(a.sorted_cell[qi]);
       const uint32_t si = s_off[hq] - base + (qi - s_src[hq]);
-      const float4 pi = s_rec[2 * si];
-      const float4 vi = s_rec[2 * si + 1];
+      const float4 pi = s_pos[si];
+      const float4 vi = s_vel[si];
       const float lapm_i = pi.w * c.lap_cf;
       CompAcc q;
       ForcePart b;
@@ -650,7 +655,7 @@ __global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) 
           for (int u = 0; u < 8; ++u) {
             if (e0 + u < cnt) {
               const uint32_t j = (w[u >> 1] >> (16 * (u & 1))) & 0xffffu;
-              pair_listed(c, s_rec[2 * j], s_rec[2 * j + 1], s_mr[j], pi, vi, lapm_i, b, q);
+              pair_listed(c, s_pos[j], s_vel[j], s_mr[j], pi, vi, lapm_i, b, q);
             }
             if (u == 3 || u == 7) fold(q, b);
           }
@@ -662,10 +667,10 @@ __global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) 
           for (int dj = -1; dj <= 1; ++dj) {
             const int h0 = hq + di * kH * kH + dj * kH - 1;
             for (uint32_t j = s_off[h0] - base; j < s_off[h0 + 3] - base; ++j) {
-              const float4 pj = s_rec[2 * j];
+              const float4 pj = s_pos[j];
               const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
               if (!(dx * dx + dy * dy + dz * dz < hc2)) continue;
-              pair_listed(c, pj, s_rec[2 * j + 1], s_mr[j], pi, vi, lapm_i, b, q);
+              pair_listed(c, pj, s_vel[j], s_mr[j], pi, vi, lapm_i, b, q);
               fold(q, b);
             }
           }
@@ -680,23 +685,6 @@ __global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) 
     CompAcc q;
     finish_particle(c, a, (int)qi, q, c.boxes[a.scene ? (int)a.scene[qi] : 0]);
   }
-}
-
-// Cell-local f32 operands of every particle (as in step_comp.cu).
-__global__ void __launch_bounds__(256) k_prep_tiled(StepConsts c, TiledArgs a) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0 && a.queue) {
-    a.queue[0] = 0;  // the density and force passes start their queues here
-    a.queue[1] = 0;
-  }
-  if (i >= c.n) return;
-  const double x = a.px[i], y = a.py[i], z = a.pz[i];
-  const long long kx = key_axis(x, c.inv_cell);
-  const long long ky = key_axis(y, c.inv_cell);
-  const long long kz = key_axis(z, c.inv_cell);
-  a.cpos[i] = make_float4((float)(x - (double)kx * c.h0), (float)(y - (double)ky * c.h0),
-                          (float)(z - (double)kz * c.h0), (float)a.mass[i]);
-  a.cvel[i] = make_float4((float)a.vx[i], (float)a.vy[i], (float)a.vz[i], 0.0f);
 }
 
 constexpr size_t kDensitySmem = kHaloCap * sizeof(float4) + (3 * kNH + 1 + 32) * 4;
@@ -778,7 +766,8 @@ void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const
   const int per_sm = t.ctas_per_sm;
   const int density_blocks = o.sms * (per_sm > 0 ? std::min(per_sm, o.density) : o.density);
   const int force_blocks = o.sms * (per_sm > 0 ? std::min(per_sm, o.force) : o.force);
-  k_prep_tiled<<<(c.n + 255) / 256, 256, 0, s>>>(c, a);
+  // The f32 operands (cpos, cvel) and the work-queue reset come from the
+  // sort's gather; the "prep" phase of a tiled step is empty.
   if (ev.after_prep) cudaEventRecord(ev.after_prep, s);
   if (a.counters)
     k_density_tiled<true><<<density_blocks, kTT, kDensitySmem, s>>>(c, a);
