@@ -222,7 +222,7 @@ __device__ __forceinline__ void stage_halo(const uint32_t* s_src, const uint32_t
   for (int run = run_lo + warp; run < run_hi; run += kTT / 32) {
     const int h0 = run * kH;
     const uint32_t b0 = s_off[h0], b6 = s_off[h0 + kH];
-#pragma unroll 2
+#pragma unroll 4
     for (uint32_t k = b0 + lane; k < b6; k += 32) {
       int hz = 0;
 #pragma unroll
