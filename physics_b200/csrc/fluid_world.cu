@@ -375,6 +375,7 @@ void FluidWorld::free_all() {
   dfree(b_.num_tiles);
   dfree(b_.boxes);
   dfree(b_.queue);
+  dfree(b_.dense_cells);
   dfree(b_.cell_of);
   dfree(b_.rank);
   dfree(b_.tmp);
@@ -436,6 +437,7 @@ void FluidWorld::ensure_capacity(size_t n) {
   dfree(b_.sorted_cell);
   dfree(b_.tile_head);
   dfree(b_.tile_slot);
+  dfree(b_.dense_cells);
   dgrow(b_.cell_of, 0, cap, s);
   dgrow(b_.rank, 0, cap, s);
   dgrow(b_.tmp, 0, cap, s);
@@ -459,7 +461,8 @@ void FluidWorld::ensure_mode_buffers() {
     if (!b_.tile_head) dalloc(b_.tile_head, tile_head_length((int)cap));
     if (!b_.tile_slot) dalloc(b_.tile_slot, cap + 1);
     if (!b_.num_tiles) dalloc(b_.num_tiles, 1);
-    if (!b_.queue) dalloc(b_.queue, 2);
+    if (!b_.queue) dalloc(b_.queue, 3);
+    if (!b_.dense_cells) dalloc(b_.dense_cells, cap);
   }
   ++alloc_gen_;
 }
@@ -1519,7 +1522,6 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
         sl.c = c;
         const AdjTape v = sl.view(n);
         const ParticleConsts& q = b_.pc[b_.cur];
-        const size_t B = n * sizeof(double);
         TapeCopy tc;
         int k = 0;
         auto add = [&](const double* dst, const double* src) {

@@ -233,8 +233,9 @@ __global__ void __launch_bounds__(kThreads) k_gather(int n, const uint32_t* __re
                             (float)(z - (double)kz * g.h0), (float)g.dst.mass[s]);
     g.cvel[s] = make_float4((float)g.dst_pv[3][s], (float)g.dst_pv[4][s], (float)g.dst_pv[5][s], 0.0f);
     if (s == 0 && g.queue) {
-      g.queue[0] = 0;
+      g.queue[0] = 0;  // density and force work queues
       g.queue[1] = 0;
+      g.queue[2] = 0;  // dense-cell count
     }
   }
 }

@@ -56,10 +56,13 @@ struct DevBuffers {
   uint32_t* tile_head = nullptr;
   uint32_t* tile_slot = nullptr;
   uint32_t* num_tiles = nullptr;
-  // Scene boxes of the tiled linearisation (one entry for a single world) and
-  // the work-queue counters of the persistent passes (density, force).
+  // Scene boxes of the tiled linearisation (one entry for a single world),
+  // the work-queue counters of the persistent passes (density, force) and the
+  // dense-cell count, and the dense-cell list (cells of tiles too dense to
+  // stage).
   SceneBox* boxes = nullptr;
   uint32_t* queue = nullptr;
+  uint32_t* dense_cells = nullptr;
   // Sort scratch.
   uint32_t* cell_of = nullptr;
   uint32_t* rank = nullptr;

@@ -72,6 +72,10 @@ struct TiledArgs {
   uint32_t* nbr_count;
   const uint16_t* __restrict__ scene;  // null: one scene
   uint32_t* queue;                      // null: static tile stride
+  // Cells of tiles too dense to stage (their halo does not fit even one
+  // x-slab), computed by the dense-cell kernels: list and device count.
+  uint32_t* dense_cells;
+  uint32_t* dense_count;
   int stride;
   uint32_t* flags;
   unsigned long long* counters;
@@ -260,36 +264,6 @@ __device__ __forceinline__ void write_density(const StepConsts& c, const TiledAr
   a.cmr[qi] = (float)(a.mass[qi] * inv);
 }
 
-// Density of particle qi from global memory (tiles that do not fit the
-// staging buffer): 27 cells by tiled index, cell-local offsets.
-__device__ void density_global(const StepConsts& c, const TiledArgs& a, int qi, int sc) {
-  const SceneBox& box = c.boxes[sc];
-  const double xi = a.px[qi], yi = a.py[qi], zi = a.pz[qi];
-  const long long kx = key_axis(xi, c.inv_cell), ky = key_axis(yi, c.inv_cell), kz = key_axis(zi, c.inv_cell);
-  const float4 pi = a.cpos[qi];
-  const float hc2 = fminf(c.h2f, c.h0sqf);
-  float s = 0.f, comp = 0.f;
-  const int bx = (int)(kx - box.b0[0]), by = (int)(ky - box.b0[1]), bz = (int)(kz - box.b0[2]);
-  for (int di = -1; di <= 1; ++di)
-    for (int dj = -1; dj <= 1; ++dj)
-      for (int dk = -1; dk <= 1; ++dk) {
-        const int lin = box_tiled_index(c, box, bx + di, by + dj, bz + dk);
-        const int s0 = (int)a.cell_start[lin], e0 = (int)a.cell_start[lin + 1];
-        const float ox = (float)di * c.h0f - pi.x, oy = (float)dj * c.h0f - pi.y, oz = (float)dk * c.h0f - pi.z;
-        float part = 0.f;
-        for (int j = s0; j < e0; ++j) {
-          const float4 q = a.cpos[j];
-          const float dx = ox + q.x, dy = oy + q.y, dz = oz + q.z;
-          const float r2 = dx * dx + dy * dy + dz * dz;
-          const float t = r2 < hc2 ? c.h0sqf - r2 : 0.f;
-          part = fmaf(t * t, t * q.w, part);
-        }
-        kahan_add(s, comp, c.poly6_cf * part);
-      }
-  write_density(c, a, qi, (double)s - (double)comp);
-  a.nbr_count[qi] = kNoList;
-}
-
 // Staged density operands: slots 2p and 2p+1 share two float4s,
 // (x0, x1, y0, y1) and (z0, z1, m0, m1), so a pair of candidates loads into
 // 64-bit register pairs ready for f32x2 arithmetic.
@@ -324,6 +298,23 @@ struct ListWriter {
   }
 };
 
+// Appends the occupied cells of tile g to the dense-cell list (one atomic per
+// tile).  Uniform across the CTA; `s_base` is shared scratch.
+__device__ __forceinline__ void queue_dense_cells(const TiledArgs& a, const TileGeom& g, uint32_t* ws,
+                                                  uint32_t* s_base) {
+  constexpr int kCells = kTB * kTB * kTB;
+  const uint32_t first_cell = (a.sorted_cell[g.first] >> (3 * kTL)) << (3 * kTL);
+  const int t = threadIdx.x;
+  const uint32_t cell = first_cell + (uint32_t)t;
+  const uint32_t occupied = (t < kCells && a.cell_start[cell + 1] > a.cell_start[cell]) ? 1u : 0u;
+  uint32_t total;
+  const uint32_t off = block_scan(occupied, ws, total);
+  if (t == 0) *s_base = atomicAdd(a.dense_count, total);
+  __syncthreads();
+  if (occupied) a.dense_cells[*s_base + off] = cell;
+  __syncthreads();
+}
+
 template <bool kCount>
 __global__ void __launch_bounds__(kTT) k_density_tiled(StepConsts c, TiledArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -343,8 +334,7 @@ __global__ void __launch_bounds__(kTT) k_density_tiled(StepConsts c, TiledArgs a
     halo_table(c, a, g, s_src, s_end, s_off, ws);
     const int slab = pick_slab(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
     if (slab == 0) {
-      for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT)
-        density_global(c, a, (int)qi, g.sc);
+      queue_dense_cells(a, g, ws, &s_next);
       continue;  // uniform across the CTA
     }
     for (int x0 = 0; x0 < kTB; x0 += slab) {
@@ -434,32 +424,6 @@ struct CompAcc {
   float xsx = 0.f, xsy = 0.f, xsz = 0.f, shear = 0.f;
 };
 
-// One neighbour pair (compute_forces' loop body, world.rs:291-316) in f32.
-__device__ __forceinline__ void pair_f32(const StepConsts& c, float dx, float dy, float dz, float m_j, float4 vj,
-                                         float mr_j, float4 vi, float m_i, float pr2_i, CompAcc& q) {
-  const float r2 = dx * dx + dy * dy + dz * dz;
-  if (!(r2 < fminf(c.h2f, c.h0sqf)) || r2 <= 0.0f) return;
-  const float inv_r = rsqrtf(r2);
-  const float r = r2 * inv_r;
-  const float hr = c.h0f - r;
-  const float fp = (m_i * m_j) * (pr2_i + vj.w) * (c.spiky_cf * hr * hr) * inv_r;
-  kahan_add(q.fpx, q.cpx, dx * fp);
-  kahan_add(q.fpy, q.cpy, dy * fp);
-  kahan_add(q.fpz, q.cpz, dz * fp);
-  const float dvx = vj.x - vi.x, dvy = vj.y - vi.y, dvz = vj.z - vi.z;
-  const float vf = m_i * mr_j * (c.lap_cf * hr);
-  kahan_add(q.fvx, q.cvx, dvx * vf);
-  kahan_add(q.fvy, q.cvy, dvy * vf);
-  kahan_add(q.fvz, q.cvz, dvz * vf);
-  const float t = c.h0sqf - r2;
-  const float xw = mr_j * (c.poly6_cf * t * t * t);
-  q.xsx = fmaf(dvx, xw, q.xsx);
-  q.xsy = fmaf(dvy, xw, q.xsy);
-  q.xsz = fmaf(dvz, xw, q.xsz);
-  const float dvn = sqrtf(dvx * dvx + dvy * dvy + dvz * dvz);
-  q.shear = fmaf(__fdividef(dvn, r + 1e-4f), mr_j, q.shear);
-}
-
 // mu_eff, acc, integrate and bounds in f64 (world.rs:319-397).
 __device__ __forceinline__ void finish_particle(const StepConsts& c, const TiledArgs& a, int i, const CompAcc& q,
                                                 const SceneBox& bx) {
@@ -519,30 +483,6 @@ __device__ __forceinline__ void finish_particle(const StepConsts& c, const Tiled
   if (!finite) atomicOr(a.flags, kFlagNonFinite);
 }
 
-// Forces of particle qi from global memory (tiles that were not staged).
-__device__ void force_global(const StepConsts& c, const TiledArgs& a, int qi, int sc) {
-  const SceneBox& box = c.boxes[sc];
-  const double xi = a.px[qi], yi = a.py[qi], zi = a.pz[qi];
-  const long long kx = key_axis(xi, c.inv_cell), ky = key_axis(yi, c.inv_cell), kz = key_axis(zi, c.inv_cell);
-  const float4 pi = a.cpos[qi];
-  const float4 vi = a.cvel[qi];
-  CompAcc q;
-  const int bx = (int)(kx - box.b0[0]), by = (int)(ky - box.b0[1]), bz = (int)(kz - box.b0[2]);
-  for (int di = -1; di <= 1; ++di)
-    for (int dj = -1; dj <= 1; ++dj)
-      for (int dk = -1; dk <= 1; ++dk) {
-        const int lin = box_tiled_index(c, box, bx + di, by + dj, bz + dk);
-        const int s0 = (int)a.cell_start[lin], e0 = (int)a.cell_start[lin + 1];
-        const float ox = (float)di * c.h0f - pi.x, oy = (float)dj * c.h0f - pi.y, oz = (float)dk * c.h0f - pi.z;
-        for (int j = s0; j < e0; ++j) {
-          if (j == qi) continue;
-          const float4 pj = a.cpos[j];
-          pair_f32(c, ox + pj.x, oy + pj.y, oz + pj.z, pj.w, a.cvel[j], a.cmr[j], vi, pi.w, vi.w, q);
-        }
-      }
-  finish_particle(c, a, qi, q, box);
-}
-
 // Batch partial sums of the pressure and raw viscous forces; folded into the
 // Kahan-compensated totals every four pairs.
 struct ForcePart {
@@ -594,7 +534,9 @@ __device__ __forceinline__ void pair_listed(const StepConsts& c, float4 pj, floa
   q.shear = fmaf(__fdividef(dvn, r + 1e-4f), mr, q.shear);
 }
 
-__global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) {
+// Three CTAs per SM is the shared-memory limit (75 KB each), so registers up to
+// 65536 / (3 x 256) cost no occupancy.
+__global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   // Staged neighbour records as separate 16-byte arrays (a 32-byte record
   // stride would map every record onto 4 of the 8 bank quads).
@@ -613,10 +555,7 @@ __global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) 
     const TileGeom g = tile_geom(c, a, k);
     halo_table(c, a, g, s_src, s_end, s_off, ws);
     const int slab = pick_slab(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
-    if (slab == 0) {
-      for (uint32_t qi = g.first + threadIdx.x; qi < g.last; qi += kTT) force_global(c, a, (int)qi, g.sc);
-      continue;
-    }
+    if (slab == 0) continue;  // the dense-cell pass computes this tile
     for (int x0 = 0; x0 < kTB; x0 += slab) {
     const uint32_t base = s_off[x0 * kH * kH];
     stage_halo(
@@ -687,13 +626,189 @@ __global__ void __launch_bounds__(kTT) k_force_tiled(StepConsts c, TiledArgs a) 
   }
 }
 
+// ---- Dense cells ---------------------------------------------------------------
+//
+// Tiles whose halo does not fit the staging buffer even in 1-layer slabs
+// (cells of hundreds to thousands of particles, as when the fluid has
+// collapsed onto the floor) are computed per occupied cell: a CTA holds
+// kDQ queries per thread in registers and streams each of the 27 neighbour
+// cells through shared memory in chunks, every staged candidate serving all
+// the CTA's queries (broadcast reads).  The force pass has no list for these
+// particles; it tests every candidate.
+
+constexpr int kDT = 256;       // threads per dense CTA
+constexpr int kDQ = 2;         // queries per thread
+constexpr int kDChunk = 1024;  // candidates staged per chunk
+
+struct CellGeom {
+  int ax, ay, az;  // box coordinates
+  int sc;
+};
+
+__device__ __forceinline__ CellGeom cell_geom(const StepConsts& c, const TiledArgs& a, uint32_t cell) {
+  CellGeom g;
+  g.sc = a.scene ? (int)a.scene[a.cell_start[cell]] : 0;
+  const SceneBox& bx = c.boxes[g.sc];
+  const uint32_t rel = cell - (uint32_t)bx.cell_base;
+  const int t = (int)(rel >> (3 * kTL));
+  const int u = (int)(rel & ((1u << (3 * kTL)) - 1u));
+  const int tz = t % bx.nt[2], ty = (t / bx.nt[2]) % bx.nt[1], tx = t / (bx.nt[2] * bx.nt[1]);
+  g.ax = tx * kTB + (u >> (2 * kTL));
+  g.ay = ty * kTB + ((u >> kTL) & (kTB - 1));
+  g.az = tz * kTB + (u & (kTB - 1));
+  return g;
+}
+
+template <bool kCount>
+__global__ void __launch_bounds__(kDT) k_density_dense(StepConsts c, TiledArgs a) {
+  __shared__ float4 s_c[kDChunk];
+  const uint32_t ncells = *a.dense_count;
+  const float hc2 = fminf(c.h2f, c.h0sqf);
+  unsigned cand = 0, pairs = 0;
+  for (uint32_t w = blockIdx.x; w < ncells; w += gridDim.x) {
+    const uint32_t cell = a.dense_cells[w];
+    const CellGeom cg = cell_geom(c, a, cell);
+    const SceneBox& bx = c.boxes[cg.sc];
+    const uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
+    for (uint32_t qb = q0; qb < q1; qb += kDT * kDQ) {
+      float4 qp[kDQ];
+      float s[kDQ], comp[kDQ];
+      unsigned nvalid = 0;
+#pragma unroll
+      for (int k = 0; k < kDQ; ++k) {
+        const uint32_t qi = qb + threadIdx.x + k * kDT;
+        qp[k] = qi < q1 ? a.cpos[qi] : make_float4(kFar, kFar, kFar, 0.f);
+        nvalid += qi < q1 ? 1u : 0u;
+        s[k] = 0.f;
+        comp[k] = 0.f;
+      }
+      for (int nb = 0; nb < 27; ++nb) {
+        const int di = nb / 9 - 1, dj = (nb / 3) % 3 - 1, dk = nb % 3 - 1;
+        const int lin = box_tiled_index(c, bx, cg.ax + di, cg.ay + dj, cg.az + dk);
+        const uint32_t s0 = a.cell_start[lin], e0 = a.cell_start[lin + 1];
+        const float ox = (float)di * c.h0f, oy = (float)dj * c.h0f, oz = (float)dk * c.h0f;
+        for (uint32_t cb = s0; cb < e0; cb += kDChunk) {
+          const uint32_t m = min(e0 - cb, (uint32_t)kDChunk);
+          __syncthreads();  // the previous chunk is consumed
+          for (uint32_t j = threadIdx.x; j < m; j += kDT) {
+            const float4 v = a.cpos[cb + j];
+            s_c[j] = make_float4(v.x + ox, v.y + oy, v.z + oz, v.w);
+          }
+          __syncthreads();
+          if (kCount) cand += m * nvalid;
+          for (uint32_t j0 = 0; j0 < m; j0 += 32) {
+            const uint32_t j1 = min(j0 + 32u, m);
+            float part[kDQ];
+#pragma unroll
+            for (int k = 0; k < kDQ; ++k) part[k] = 0.f;
+            for (uint32_t j = j0; j < j1; ++j) {
+              const float4 v = s_c[j];
+#pragma unroll
+              for (int k = 0; k < kDQ; ++k) {
+                const float dx = v.x - qp[k].x, dy = v.y - qp[k].y, dz = v.z - qp[k].z;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                const bool in = r2 < hc2;
+                const float t = in ? c.h0sqf - r2 : 0.f;
+                part[k] = fmaf(t * t, t * v.w, part[k]);
+                if (kCount) pairs += in ? 1u : 0u;
+              }
+            }
+#pragma unroll
+            for (int k = 0; k < kDQ; ++k) kahan_add(s[k], comp[k], c.poly6_cf * part[k]);
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kDQ; ++k) {
+        const uint32_t qi = qb + threadIdx.x + k * kDT;
+        if (qi < q1) {
+          write_density(c, a, (int)qi, (double)s[k] - (double)comp[k]);
+          a.nbr_count[qi] = kNoList;
+        }
+      }
+    }
+  }
+  if (kCount) {
+    // Placeholder queries (kFar) never pair and count no candidates.
+    const unsigned wc = __reduce_add_sync(0xffffffffu, cand);
+    const unsigned wp = __reduce_add_sync(0xffffffffu, pairs);
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(&a.counters[0], (unsigned long long)wc);
+      atomicAdd(&a.counters[1], (unsigned long long)wp);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kDT) k_force_dense(StepConsts c, TiledArgs a) {
+  __shared__ float4 s_pos[kDChunk];
+  __shared__ float4 s_vel[kDChunk];
+  __shared__ float s_mr[kDChunk];
+  const uint32_t ncells = *a.dense_count;
+  const float hc2 = fminf(c.h2f, c.h0sqf);
+  for (uint32_t w = blockIdx.x; w < ncells; w += gridDim.x) {
+    const uint32_t cell = a.dense_cells[w];
+    const CellGeom cg = cell_geom(c, a, cell);
+    const SceneBox& bx = c.boxes[cg.sc];
+    const uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
+    for (uint32_t qb = q0; qb < q1; qb += kDT * kDQ) {
+      float4 qp[kDQ], qv[kDQ];
+      CompAcc acc[kDQ];
+      ForcePart part[kDQ];
+#pragma unroll
+      for (int k = 0; k < kDQ; ++k) {
+        const uint32_t qi = qb + threadIdx.x + k * kDT;
+        qp[k] = qi < q1 ? a.cpos[qi] : make_float4(kFar, kFar, kFar, 0.f);
+        qv[k] = qi < q1 ? a.cvel[qi] : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      for (int nb = 0; nb < 27; ++nb) {
+        const int di = nb / 9 - 1, dj = (nb / 3) % 3 - 1, dk = nb % 3 - 1;
+        const int lin = box_tiled_index(c, bx, cg.ax + di, cg.ay + dj, cg.az + dk);
+        const uint32_t s0 = a.cell_start[lin], e0 = a.cell_start[lin + 1];
+        const float ox = (float)di * c.h0f, oy = (float)dj * c.h0f, oz = (float)dk * c.h0f;
+        for (uint32_t cb = s0; cb < e0; cb += kDChunk) {
+          const uint32_t m = min(e0 - cb, (uint32_t)kDChunk);
+          __syncthreads();
+          for (uint32_t j = threadIdx.x; j < m; j += kDT) {
+            const float4 v = a.cpos[cb + j];
+            s_pos[j] = make_float4(v.x + ox, v.y + oy, v.z + oz, v.w);
+            s_vel[j] = a.cvel[cb + j];
+            s_mr[j] = a.cmr[cb + j];
+          }
+          __syncthreads();
+#pragma unroll
+          for (int k = 0; k < kDQ; ++k) {
+            const float lapm = qp[k].w * c.lap_cf;
+            uint32_t since = 0;
+            for (uint32_t j = 0; j < m; ++j) {
+              const float4 pj = s_pos[j];
+              const float dx = pj.x - qp[k].x, dy = pj.y - qp[k].y, dz = pj.z - qp[k].z;
+              if (!(dx * dx + dy * dy + dz * dz < hc2)) continue;
+              pair_listed(c, pj, s_vel[j], s_mr[j], qp[k], qv[k], lapm, part[k], acc[k]);
+              if (++since == 4) {
+                fold(acc[k], part[k]);
+                since = 0;
+              }
+            }
+            fold(acc[k], part[k]);
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kDQ; ++k) {
+        const uint32_t qi = qb + threadIdx.x + k * kDT;
+        if (qi < q1) finish_particle(c, a, (int)qi, acc[k], bx);
+      }
+    }
+  }
+}
+
 constexpr size_t kDensitySmem = kHaloCap * sizeof(float4) + (3 * kNH + 1 + 32) * 4;
 constexpr size_t kForceSmem = kHaloCap * (2 * sizeof(float4) + sizeof(float)) + (3 * kNH + 1 + 32) * 4;
 
 // Resident CTAs per SM of the persistent passes (occupancy limits, computed
 // once; the shared-memory opt-in is set on the same first call).
 struct Occupancy {
-  int sms = 1, density = 1, force = 1;
+  int sms = 1, density = 1, force = 1, dense_density = 1, dense_force = 1;
 };
 
 const Occupancy& occupancy() {
@@ -708,6 +823,11 @@ const Occupancy& occupancy() {
     int bd = 0, bf = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bd, k_density_tiled<false>, kTT, kDensitySmem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force_tiled, kTT, kForceSmem);
+    int dd = 0, df = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dd, k_density_dense<false>, kDT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&df, k_force_dense, kDT, 0);
+    r.dense_density = std::max(dd, 1);
+    r.dense_force = std::max(df, 1);
     r.sms = std::max(r.sms, 1);
     r.density = std::max(bd, 1);
     r.force = std::max(bf, 1);
@@ -757,6 +877,8 @@ void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const
   a.nbr_count = b.nbr_count;
   a.scene = pc.scene;
   a.queue = t.queue ? b.queue : nullptr;
+  a.dense_count = b.queue + 2;
+  a.dense_cells = b.dense_cells;
   a.stride = b.capacity;
   a.flags = b.flags;
   a.counters = b.counters;
@@ -769,12 +891,17 @@ void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const
   // The f32 operands (cpos, cvel) and the work-queue reset come from the
   // sort's gather; the "prep" phase of a tiled step is empty.
   if (ev.after_prep) cudaEventRecord(ev.after_prep, s);
-  if (a.counters)
+  const int dense_d_blocks = o.sms * o.dense_density, dense_f_blocks = o.sms * o.dense_force;
+  if (a.counters) {
     k_density_tiled<true><<<density_blocks, kTT, kDensitySmem, s>>>(c, a);
-  else
+    k_density_dense<true><<<dense_d_blocks, kDT, 0, s>>>(c, a);
+  } else {
     k_density_tiled<false><<<density_blocks, kTT, kDensitySmem, s>>>(c, a);
+    k_density_dense<false><<<dense_d_blocks, kDT, 0, s>>>(c, a);
+  }
   if (ev.after_density) cudaEventRecord(ev.after_density, s);
   k_force_tiled<<<force_blocks, kTT, kForceSmem, s>>>(c, a);
+  k_force_dense<<<dense_f_blocks, kDT, 0, s>>>(c, a);
 }
 
 }  // namespace phy

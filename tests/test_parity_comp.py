@@ -184,3 +184,34 @@ def test_compressed_regimes(gpu, oracle_mod, spacing, halo_cap):
     cnt = w.step_counters()
     print("compressed", spacing, halo_cap, e, cnt["pairs"] / len(pos))
     assert e["rho_rel"] <= RHO_TOL and e["acc_rel_to_max"] <= 1e-3, e
+
+
+@pytest.mark.parametrize("per_cell", [60, 400])
+def test_dense_cells(gpu, oracle_mod, per_cell):
+    """Cells of tens to hundreds of particles, as when the fluid has collapsed onto the
+    floor: no tile halo fits the staging buffer, so the dense-cell kernels compute those
+    tiles.  A floor sheet of particles at y = 0 (clamped there, like the collapsed
+    trajectory) plus a dense blob; density gate and force agreement against the oracle,
+    teacher-forced."""
+    O = oracle_mod
+    p = ref_test_params(gravity=(0.0, -9.81, 0.0))
+    p.bounds_min, p.bounds_max = (0.0, 0.0, 0.0), (1.6, 1.6, 1.6)
+    rng = np.random.default_rng(per_cell)
+    ncell = 4 * 4  # a 0.8 x 0.8 floor patch of 4 x 4 cells
+    sheet = np.stack([rng.uniform(0.4, 1.2, ncell * per_cell), np.zeros(ncell * per_cell),
+                      rng.uniform(0.4, 1.2, ncell * per_cell)], -1)
+    blob = rng.uniform(0.6, 1.0, (4 * per_cell, 3))
+    pos = np.concatenate([sheet, blob])
+    vel = rng.normal(0, 0.1, pos.shape)
+    mass = 0.02
+    ow = O.OracleWorld(p, threads=O.max_threads())
+    ow.add_particles(pos, mass, vel=vel)
+    w = gpu.FluidWorld(p, "comp")
+    w.add_particles(pos, mass, vel=vel)
+    ow.step(0.001)
+    w.step(0.001)
+    e = errors(w, O, ow, p)
+    print("dense cells", per_cell, e)
+    assert e["rho_rel"] <= RHO_TOL and e["acc_rel_to_max"] <= 1e-3, e
+    # |p| errors scale with rho, which reaches many times rest density here.
+    assert e["p_norm"] <= 1e-5 * max(1.0, float(np.max(ow.get(O.F_RHO))) / p.rest_density), e
