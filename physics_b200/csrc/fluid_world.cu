@@ -376,6 +376,7 @@ void FluidWorld::free_all() {
   dfree(b_.boxes);
   dfree(b_.queue);
   dfree(b_.dense_cells);
+  dfree(b_.okey);
   dfree(b_.cell_of);
   dfree(b_.rank);
   dfree(b_.tmp);
@@ -438,6 +439,7 @@ void FluidWorld::ensure_capacity(size_t n) {
   dfree(b_.tile_head);
   dfree(b_.tile_slot);
   dfree(b_.dense_cells);
+  dfree(b_.okey);
   dgrow(b_.cell_of, 0, cap, s);
   dgrow(b_.rank, 0, cap, s);
   dgrow(b_.tmp, 0, cap, s);
@@ -463,6 +465,7 @@ void FluidWorld::ensure_mode_buffers() {
     if (!b_.num_tiles) dalloc(b_.num_tiles, 1);
     if (!b_.queue) dalloc(b_.queue, 3);
     if (!b_.dense_cells) dalloc(b_.dense_cells, cap);
+    if (!b_.okey) dalloc(b_.okey, cap);
   }
   ++alloc_gen_;
 }

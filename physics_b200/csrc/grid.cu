@@ -28,6 +28,24 @@ int grid_for(int n, int threads = kThreads) {
   return b < 1 ? 1 : b;
 }
 
+// Spreads the low 10 bits of v three bits apart (Morton interleave).
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+// Position inside its cell quantised to 1024 steps per axis (non-finite or
+// out-of-range values clamp).
+__device__ __forceinline__ uint32_t quantise_local(double x, long long k, double h0, double inv) {
+  const double t = (x - (double)k * h0) * inv * 1024.0;
+  if (!(t > 0.0)) return 0u;
+  return t >= 1023.0 ? 1023u : (uint32_t)t;
+}
+
 // Cell of every particle plus its arrival rank inside the cell.  Lanes of a
 // warp that share a cell (the common case: the previous order is already
 // sorted by cell) are aggregated into one atomic.
@@ -38,7 +56,9 @@ __global__ void __launch_bounds__(kThreads) k_cell_hist(StepConsts c, const doub
                                                         uint32_t* __restrict__ rank,
                                                         uint32_t* __restrict__ count,
                                                         uint32_t* __restrict__ flags,
-                                                        const uint16_t* __restrict__ scene) {
+                                                        const uint16_t* __restrict__ scene,
+                                                        const uint32_t* __restrict__ id,
+                                                        unsigned long long* __restrict__ okey) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = i < c.n;
   uint32_t cell = 0;
@@ -62,6 +82,15 @@ __global__ void __launch_bounds__(kThreads) k_cell_hist(StepConsts c, const doub
       atomicOr(flags, kFlagOutOfBox);
     }
     cell_of[i] = cell;
+    if (okey) {
+      // Tiled form: particles of a cell in Morton order of their position in
+      // the cell, so that a warp's queries are spatial neighbours (the
+      // insertion index breaks ties, keeping the order deterministic).
+      const uint32_t m = (spread3(quantise_local(px[i], kx, c.h0, c.inv_cell)) << 2) |
+                         (spread3(quantise_local(py[i], ky, c.h0, c.inv_cell)) << 1) |
+                         spread3(quantise_local(pz[i], kz, c.h0, c.inv_cell));
+      okey[i] = ((unsigned long long)m << 32) | id[i];
+    }
   }
   unsigned mask = __ballot_sync(0xffffffffu, active);
   if (!active) return;
@@ -178,6 +207,7 @@ __global__ void __launch_bounds__(kThreads) k_order(int n, int ncells, const uin
                                                     const uint32_t* __restrict__ cell_start,
                                                     const uint32_t* __restrict__ tmp,
                                                     const uint32_t* __restrict__ id,
+                                                    const unsigned long long* __restrict__ okey,
                                                     uint32_t* __restrict__ perm) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
@@ -188,9 +218,14 @@ __global__ void __launch_bounds__(kThreads) k_order(int n, int ncells, const uin
     return;
   }
   uint32_t cs = cell_start[cell], ce = cell_start[cell + 1];
-  uint32_t mine = id[i];
   uint32_t r = 0;
-  for (uint32_t k = cs; k < ce; ++k) r += id[tmp[k]] < mine ? 1u : 0u;
+  if (okey) {
+    const unsigned long long mine = okey[i];
+    for (uint32_t k = cs; k < ce; ++k) r += okey[tmp[k]] < mine ? 1u : 0u;
+  } else {
+    const uint32_t mine = id[i];
+    for (uint32_t k = cs; k < ce; ++k) r += id[tmp[k]] < mine ? 1u : 0u;
+  }
   perm[cs + r] = i;
 }
 
@@ -334,14 +369,16 @@ void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s, int block) 
   const int nb = len / kScanTile;
   cudaMemsetAsync(b.cell_start, 0, (size_t)len * sizeof(uint32_t), s);
   k_cell_hist<<<grid_for(n, bs), bs, 0, s>>>(c, b.pv1[0], b.pv1[1], b.pv1[2], b.cell_of, b.rank,
-                                               b.cell_start, b.flags, b.pc[b.cur].scene);
+                                               b.cell_start, b.flags, b.pc[b.cur].scene, b.pc[b.cur].id,
+                                               c.tile ? b.okey : nullptr);
   k_scan_reduce<<<nb, kThreads, 0, s>>>(b.cell_start, b.block_sums);
   k_scan_top<<<1, 1024, 0, s>>>(b.block_sums, nb);
   k_scan_apply<<<nb, kThreads, 0, s>>>(b.cell_start, b.block_sums);
   k_scatter<<<grid_for(n, bs), bs, 0, s>>>(n, b.cell_of, b.rank, b.cell_start, b.tmp);
   const ParticleConsts& src = b.pc[b.cur];
   const ParticleConsts& dst = b.pc[b.cur ^ 1];
-  k_order<<<grid_for(n, bs), bs, 0, s>>>(n, c.ncells, b.cell_of, b.cell_start, b.tmp, src.id, b.perm);
+  k_order<<<grid_for(n, bs), bs, 0, s>>>(n, c.ncells, b.cell_of, b.cell_start, b.tmp, src.id,
+                                         c.tile ? b.okey : nullptr, b.perm);
   GatherArgs g;
   for (int k = 0; k < 6; ++k) {
     g.src_pv[k] = b.pv1[k];

@@ -68,6 +68,9 @@ struct DevBuffers {
   uint32_t* rank = nullptr;
   uint32_t* tmp = nullptr;
   uint32_t* perm = nullptr;
+  // Tiled form: in-cell order key of every particle (Morton code of its
+  // quantised position inside the cell, then its insertion index).
+  unsigned long long* okey = nullptr;
   uint32_t* cell_start = nullptr;  // cell_capacity + 2 entries
   uint32_t* block_sums = nullptr;
   int block_sums_capacity = 0;

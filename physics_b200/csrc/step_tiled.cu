@@ -629,15 +629,18 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
 // ---- Dense cells ---------------------------------------------------------------
 //
 // Tiles whose halo does not fit the staging buffer even in 1-layer slabs
-// (cells of hundreds to thousands of particles, as when the fluid has
-// collapsed onto the floor) are computed per occupied cell: a CTA holds
-// kDQ queries per thread in registers and streams each of the 27 neighbour
-// cells through shared memory in chunks, every staged candidate serving all
-// the CTA's queries (broadcast reads).  The force pass has no list for these
+// (cells of tens to thousands of particles, as when the fluid has collapsed
+// onto the floor) are computed per occupied cell.  The CTA streams each of
+// the cell's 27 neighbour cells through shared memory in chunks; every staged
+// candidate serves all the cell's queries (broadcast reads).  Work is sized
+// to the cell: a cell of Q particles gets S = clamp(512 / Q, 1, 32) lanes per
+// query (a power of two, lanes of one warp), each taking every S-th
+// candidate, and the S partial sums are combined by a fixed shuffle tree;
+// each lane group holds two queries.  The force pass has no list for these
 // particles; it tests every candidate.
 
 constexpr int kDT = 256;       // threads per dense CTA
-constexpr int kDQ = 2;         // queries per thread
+constexpr int kDQ = 2;         // queries per lane group
 constexpr int kDChunk = 1024;  // candidates staged per chunk
 
 struct CellGeom {
@@ -659,9 +662,82 @@ __device__ __forceinline__ CellGeom cell_geom(const StepConsts& c, const TiledAr
   return g;
 }
 
+// The cell's 27 neighbour cells as one virtual candidate range: s_src[nb] is
+// neighbour nb's first slot, s_pre[nb] its first virtual index (s_pre[27] =
+// the total).  Uniform across the CTA; ends with a barrier.
+__device__ __forceinline__ void dense_neighbour_table(const StepConsts& c, const TiledArgs& a, const SceneBox& bx,
+                                                      const CellGeom& cg, uint32_t* s_src, uint32_t* s_pre) {
+  if (threadIdx.x < 32) {
+    const int nb = threadIdx.x;
+    uint32_t src = 0, cnt = 0;
+    if (nb < 27) {
+      const int lin = box_tiled_index(c, bx, cg.ax + nb / 9 - 1, cg.ay + (nb / 3) % 3 - 1, cg.az + nb % 3 - 1);
+      src = a.cell_start[lin];
+      cnt = a.cell_start[lin + 1] - src;
+    }
+    uint32_t x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (nb >= o) x += y;
+    }
+    if (nb < 27) {
+      s_src[nb] = src;
+      s_pre[nb] = x - cnt;
+    }
+    if (nb == 26) s_pre[27] = x;
+  }
+  __syncthreads();
+}
+
+// Neighbour (0..26) holding virtual candidate v: the last nb with s_pre[nb] <= v.
+__device__ __forceinline__ int dense_neighbour_of(const uint32_t* s_pre, uint32_t v) {
+  int lo = 0, hi = 26;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (s_pre[mid] <= v) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Stages virtual candidates [cb, cb + m) of the cell's neighbourhood: slot j
+// gets the candidate's position relative to the query cell's origin (its
+// cell-local f32 coordinates plus the neighbour cell's offset).  `emit(j,
+// src, rel)` stores one candidate.
+template <class Emit>
+__device__ __forceinline__ void dense_stage(const StepConsts& c, const TiledArgs& a, const uint32_t* s_src,
+                                            const uint32_t* s_pre, uint32_t cb, uint32_t m, Emit emit) {
+  for (uint32_t j = threadIdx.x; j < m; j += kDT) {
+    const uint32_t v = cb + j;
+    const int nb = dense_neighbour_of(s_pre, v);
+    const uint32_t src = s_src[nb] + (v - s_pre[nb]);
+    const float4 q = a.cpos[src];
+    const float4 rel = make_float4(q.x + (float)(nb / 9 - 1) * c.h0f, q.y + (float)((nb / 3) % 3 - 1) * c.h0f,
+                                   q.z + (float)(nb % 3 - 1) * c.h0f, q.w);
+    emit(j, src, rel);
+  }
+}
+
+// Lanes per query for a cell of q particles (a power of two, 1..32).
+__device__ __forceinline__ int dense_split(uint32_t q) {
+  int sp = 1;
+  while (sp < 32 && (uint32_t)(2 * sp) * q <= (uint32_t)(kDT * kDQ)) sp <<= 1;
+  return sp;
+}
+
+// Sum over the `sp` lanes of a group (sp a power of two dividing 32); every
+// lane of the group receives the total.  All 32 lanes must call it.
+__device__ __forceinline__ float group_sum(float v, int sp) {
+  for (int o = 1; o < sp; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
 template <bool kCount>
-__global__ void __launch_bounds__(kDT) k_density_dense(StepConsts c, TiledArgs a) {
+// (At least 4 resident CTAs leave 64 registers a thread, enough to hold the
+// two queries without spilling.)
+__global__ void __launch_bounds__(kDT, 4) k_density_dense(StepConsts c, TiledArgs a) {
   __shared__ float4 s_c[kDChunk];
+  __shared__ uint32_t s_src[27], s_pre[28];
   const uint32_t ncells = *a.dense_count;
   const float hc2 = fminf(c.h2f, c.h0sqf);
   unsigned cand = 0, pairs = 0;
@@ -670,59 +746,59 @@ __global__ void __launch_bounds__(kDT) k_density_dense(StepConsts c, TiledArgs a
     const CellGeom cg = cell_geom(c, a, cell);
     const SceneBox& bx = c.boxes[cg.sc];
     const uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
-    for (uint32_t qb = q0; qb < q1; qb += kDT * kDQ) {
+    const int sp = dense_split(q1 - q0);          // uniform across the CTA
+    const int groups = kDT / sp;
+    const int grp = threadIdx.x / sp, sub = threadIdx.x % sp;
+    __syncthreads();  // the previous cell's tables are no longer read
+    dense_neighbour_table(c, a, bx, cg, s_src, s_pre);
+    const uint32_t total = s_pre[27];
+    for (uint32_t qb = q0; qb < q1; qb += (uint32_t)(groups * kDQ)) {
       float4 qp[kDQ];
       float s[kDQ], comp[kDQ];
       unsigned nvalid = 0;
 #pragma unroll
       for (int k = 0; k < kDQ; ++k) {
-        const uint32_t qi = qb + threadIdx.x + k * kDT;
+        const uint32_t qi = qb + (uint32_t)(grp + k * groups);
         qp[k] = qi < q1 ? a.cpos[qi] : make_float4(kFar, kFar, kFar, 0.f);
         nvalid += qi < q1 ? 1u : 0u;
         s[k] = 0.f;
         comp[k] = 0.f;
       }
-      for (int nb = 0; nb < 27; ++nb) {
-        const int di = nb / 9 - 1, dj = (nb / 3) % 3 - 1, dk = nb % 3 - 1;
-        const int lin = box_tiled_index(c, bx, cg.ax + di, cg.ay + dj, cg.az + dk);
-        const uint32_t s0 = a.cell_start[lin], e0 = a.cell_start[lin + 1];
-        const float ox = (float)di * c.h0f, oy = (float)dj * c.h0f, oz = (float)dk * c.h0f;
-        for (uint32_t cb = s0; cb < e0; cb += kDChunk) {
-          const uint32_t m = min(e0 - cb, (uint32_t)kDChunk);
-          __syncthreads();  // the previous chunk is consumed
-          for (uint32_t j = threadIdx.x; j < m; j += kDT) {
-            const float4 v = a.cpos[cb + j];
-            s_c[j] = make_float4(v.x + ox, v.y + oy, v.z + oz, v.w);
-          }
-          __syncthreads();
-          if (kCount) cand += m * nvalid;
-          for (uint32_t j0 = 0; j0 < m; j0 += 32) {
-            const uint32_t j1 = min(j0 + 32u, m);
-            float part[kDQ];
+      for (uint32_t cb = 0; cb < total; cb += kDChunk) {
+        const uint32_t m = min(total - cb, (uint32_t)kDChunk);
+        __syncthreads();  // the previous chunk is consumed
+        dense_stage(c, a, s_src, s_pre, cb, m, [&](uint32_t j, uint32_t, float4 rel) { s_c[j] = rel; });
+        __syncthreads();
+        if (kCount && sub == 0) cand += m * nvalid;
+        // This lane's candidates: sub, sub + sp, ...; partial sums of up to
+        // 32 of them folded by Kahan.
+        for (uint32_t j0 = (uint32_t)sub; j0 < m; j0 += 32u * (uint32_t)sp) {
+          const uint32_t j1 = min(j0 + 32u * (uint32_t)sp, m);
+          float part[kDQ];
 #pragma unroll
-            for (int k = 0; k < kDQ; ++k) part[k] = 0.f;
-            for (uint32_t j = j0; j < j1; ++j) {
-              const float4 v = s_c[j];
+          for (int k = 0; k < kDQ; ++k) part[k] = 0.f;
+          for (uint32_t j = j0; j < j1; j += (uint32_t)sp) {
+            const float4 v = s_c[j];
 #pragma unroll
-              for (int k = 0; k < kDQ; ++k) {
-                const float dx = v.x - qp[k].x, dy = v.y - qp[k].y, dz = v.z - qp[k].z;
-                const float r2 = dx * dx + dy * dy + dz * dz;
-                const bool in = r2 < hc2;
-                const float t = in ? c.h0sqf - r2 : 0.f;
-                part[k] = fmaf(t * t, t * v.w, part[k]);
-                if (kCount) pairs += in ? 1u : 0u;
-              }
+            for (int k = 0; k < kDQ; ++k) {
+              const float dx = v.x - qp[k].x, dy = v.y - qp[k].y, dz = v.z - qp[k].z;
+              const float r2 = dx * dx + dy * dy + dz * dz;
+              const bool in = r2 < hc2;
+              const float t = in ? c.h0sqf - r2 : 0.f;
+              part[k] = fmaf(t * t, t * v.w, part[k]);
+              if (kCount) pairs += in ? 1u : 0u;
             }
-#pragma unroll
-            for (int k = 0; k < kDQ; ++k) kahan_add(s[k], comp[k], c.poly6_cf * part[k]);
           }
+#pragma unroll
+          for (int k = 0; k < kDQ; ++k) kahan_add(s[k], comp[k], c.poly6_cf * part[k]);
         }
       }
 #pragma unroll
       for (int k = 0; k < kDQ; ++k) {
-        const uint32_t qi = qb + threadIdx.x + k * kDT;
-        if (qi < q1) {
-          write_density(c, a, (int)qi, (double)s[k] - (double)comp[k]);
+        const float st = group_sum(s[k], sp), ct = group_sum(comp[k], sp);
+        const uint32_t qi = qb + (uint32_t)(grp + k * groups);
+        if (sub == 0 && qi < q1) {
+          write_density(c, a, (int)qi, (double)st - (double)ct);
           a.nbr_count[qi] = kNoList;
         }
       }
@@ -743,6 +819,7 @@ __global__ void __launch_bounds__(kDT) k_force_dense(StepConsts c, TiledArgs a) 
   __shared__ float4 s_pos[kDChunk];
   __shared__ float4 s_vel[kDChunk];
   __shared__ float s_mr[kDChunk];
+  __shared__ uint32_t s_src[27], s_pre[28];
   const uint32_t ncells = *a.dense_count;
   const float hc2 = fminf(c.h2f, c.h0sqf);
   for (uint32_t w = blockIdx.x; w < ncells; w += gridDim.x) {
@@ -750,53 +827,64 @@ __global__ void __launch_bounds__(kDT) k_force_dense(StepConsts c, TiledArgs a) 
     const CellGeom cg = cell_geom(c, a, cell);
     const SceneBox& bx = c.boxes[cg.sc];
     const uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
-    for (uint32_t qb = q0; qb < q1; qb += kDT * kDQ) {
+    const int sp = dense_split(q1 - q0);
+    const int groups = kDT / sp;
+    const int grp = threadIdx.x / sp, sub = threadIdx.x % sp;
+    __syncthreads();  // the previous cell's tables are no longer read
+    dense_neighbour_table(c, a, bx, cg, s_src, s_pre);
+    const uint32_t total = s_pre[27];
+    for (uint32_t qb = q0; qb < q1; qb += (uint32_t)(groups * kDQ)) {
       float4 qp[kDQ], qv[kDQ];
       CompAcc acc[kDQ];
       ForcePart part[kDQ];
 #pragma unroll
       for (int k = 0; k < kDQ; ++k) {
-        const uint32_t qi = qb + threadIdx.x + k * kDT;
+        const uint32_t qi = qb + (uint32_t)(grp + k * groups);
         qp[k] = qi < q1 ? a.cpos[qi] : make_float4(kFar, kFar, kFar, 0.f);
         qv[k] = qi < q1 ? a.cvel[qi] : make_float4(0.f, 0.f, 0.f, 0.f);
       }
-      for (int nb = 0; nb < 27; ++nb) {
-        const int di = nb / 9 - 1, dj = (nb / 3) % 3 - 1, dk = nb % 3 - 1;
-        const int lin = box_tiled_index(c, bx, cg.ax + di, cg.ay + dj, cg.az + dk);
-        const uint32_t s0 = a.cell_start[lin], e0 = a.cell_start[lin + 1];
-        const float ox = (float)di * c.h0f, oy = (float)dj * c.h0f, oz = (float)dk * c.h0f;
-        for (uint32_t cb = s0; cb < e0; cb += kDChunk) {
-          const uint32_t m = min(e0 - cb, (uint32_t)kDChunk);
-          __syncthreads();
-          for (uint32_t j = threadIdx.x; j < m; j += kDT) {
-            const float4 v = a.cpos[cb + j];
-            s_pos[j] = make_float4(v.x + ox, v.y + oy, v.z + oz, v.w);
-            s_vel[j] = a.cvel[cb + j];
-            s_mr[j] = a.cmr[cb + j];
-          }
-          __syncthreads();
+      for (uint32_t cb = 0; cb < total; cb += kDChunk) {
+        const uint32_t m = min(total - cb, (uint32_t)kDChunk);
+        __syncthreads();
+        dense_stage(c, a, s_src, s_pre, cb, m, [&](uint32_t j, uint32_t src, float4 rel) {
+          s_pos[j] = rel;
+          s_vel[j] = a.cvel[src];
+          s_mr[j] = a.cmr[src];
+        });
+        __syncthreads();
 #pragma unroll
-          for (int k = 0; k < kDQ; ++k) {
-            const float lapm = qp[k].w * c.lap_cf;
-            uint32_t since = 0;
-            for (uint32_t j = 0; j < m; ++j) {
-              const float4 pj = s_pos[j];
-              const float dx = pj.x - qp[k].x, dy = pj.y - qp[k].y, dz = pj.z - qp[k].z;
-              if (!(dx * dx + dy * dy + dz * dz < hc2)) continue;
-              pair_listed(c, pj, s_vel[j], s_mr[j], qp[k], qv[k], lapm, part[k], acc[k]);
-              if (++since == 4) {
-                fold(acc[k], part[k]);
-                since = 0;
-              }
+        for (int k = 0; k < kDQ; ++k) {
+          const float lapm = qp[k].w * c.lap_cf;
+          uint32_t since = 0;
+          for (uint32_t j = (uint32_t)sub; j < m; j += (uint32_t)sp) {
+            const float4 pj = s_pos[j];
+            const float dx = pj.x - qp[k].x, dy = pj.y - qp[k].y, dz = pj.z - qp[k].z;
+            if (!(dx * dx + dy * dy + dz * dz < hc2)) continue;
+            pair_listed(c, pj, s_vel[j], s_mr[j], qp[k], qv[k], lapm, part[k], acc[k]);
+            if (++since == 4) {
+              fold(acc[k], part[k]);
+              since = 0;
             }
-            fold(acc[k], part[k]);
           }
+          fold(acc[k], part[k]);
         }
       }
 #pragma unroll
       for (int k = 0; k < kDQ; ++k) {
-        const uint32_t qi = qb + threadIdx.x + k * kDT;
-        if (qi < q1) finish_particle(c, a, (int)qi, acc[k], bx);
+        // Combine the group's partial sums (compensations applied per lane).
+        CompAcc t;
+        t.fpx = group_sum(acc[k].fpx - acc[k].cpx, sp);
+        t.fpy = group_sum(acc[k].fpy - acc[k].cpy, sp);
+        t.fpz = group_sum(acc[k].fpz - acc[k].cpz, sp);
+        t.fvx = group_sum(acc[k].fvx - acc[k].cvx, sp);
+        t.fvy = group_sum(acc[k].fvy - acc[k].cvy, sp);
+        t.fvz = group_sum(acc[k].fvz - acc[k].cvz, sp);
+        t.xsx = group_sum(acc[k].xsx, sp);
+        t.xsy = group_sum(acc[k].xsy, sp);
+        t.xsz = group_sum(acc[k].xsz, sp);
+        t.shear = group_sum(acc[k].shear, sp);
+        const uint32_t qi = qb + (uint32_t)(grp + k * groups);
+        if (sub == 0 && qi < q1) finish_particle(c, a, (int)qi, t, bx);
       }
     }
   }
