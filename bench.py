@@ -47,6 +47,16 @@ DT = 0.0025
 #   f32c form: reads pos+vel (48), rho (8), material (4), packed f32 operands
 #              cpos (16), cvel (16), m/rho (4); writes as above (104)      = 200
 FORCE_BYTES = {"f64": 188, "comp": 200}
+# DRAM traffic of one k_force_tiled launch per particle, dram__bytes_read.sum +
+# dram__bytes_write.sum from an ncu capture of the 80x160x80 dam break (the
+# 4M launch is larger than an ncu capture should be); at constant density the
+# traffic grows with the particle count, so a full launch is scaled by it.
+FORCE_TRAFFIC_PER_PARTICLE = (238.917888e6 + 80.918784e6) / 1024000
+# Kernels one compensated step launches: the sort (cell histogram, 3-kernel
+# cell scan, scatter, in-cell order, gather), the occupied-tile list (heads,
+# 3-kernel scan, emit) and the passes (tiled and dense-cell density, tiled and
+# dense-cell force).
+LAUNCHES_PER_STEP = 7 + 5 + 4
 # Whole-step compulsory state traffic (f64 pos, vel, mass in; pos, vel, rho, p out).
 STEP_BYTES = 120
 
@@ -347,7 +357,10 @@ def run_ours(args):
         w.add_particles(p, mass, vel=v)
         return w
 
-    def timed(w, steps, warmup, sample_clocks=False):
+    def timed(w, steps, warmup, sample_clocks=False, phase=False):
+        """Device time of `steps` steps (CUDA events on the world's stream); with
+        phase=True the world also records per-pass events inside the timed region
+        (non-blocking) and their per-step means are returned."""
         w.step(DT, warmup)
         w.synchronize()
         barrier()
@@ -355,6 +368,9 @@ def run_ours(args):
         sampler = ClockSampler(local_rank) if sample_clocks else None
         if sampler:
             time.sleep(0.3)
+        if phase:
+            w.set_timing(True)
+            w.phase_times(reset=True)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -363,18 +379,23 @@ def run_ours(args):
         e1.synchronize()
         clocks = sampler.stop() if sampler else None
         ms = max_over_ranks(e0.elapsed_time(e1))
+        ph = None
+        if phase:
+            t = w.phase_times(reset=True)
+            w.set_timing(False)
+            ph = {k: t[k] / max(t["steps"], 1) for k in ("sort", "prep", "density", "force")}
         barrier()
-        return ms, clocks
+        return ms, clocks, ph
 
     # ---- headline: FP32-compensated, state resident in HBM ----------------------------
     comp = new_world("comp")
-    ms_comp, clocks = timed(comp, K, W, sample_clocks=(rank == 0))
+    ms_comp, clocks, ph_comp = timed(comp, K, W, sample_clocks=(rank == 0), phase=True)
     value = world_size * n * K / (ms_comp / 1e3)
 
     # ---- the f64 plain step on the same scene ---------------------------------------
     plain = new_world("f64")
     k_plain = max(3, K // 4)
-    ms_plain, _ = timed(plain, k_plain, max(3, W // 2))
+    ms_plain, _, ph_plain = timed(plain, k_plain, max(3, W // 2), phase=True)
     plain_value = world_size * n * k_plain / (ms_plain / 1e3)
 
     # ---- density error of the compensated form vs f64 plain (teacher-forced step) ----
@@ -392,7 +413,7 @@ def run_ours(args):
     traj = None
     if args.full_steps > 0:
         traj = new_world("comp")
-        ms_full, _ = timed(traj, args.full_steps, 0)
+        ms_full, _, _ = timed(traj, args.full_steps, 0)
         full = {"steps": args.full_steps, "value": world_size * n * args.full_steps / (ms_full / 1e3),
                 "ms_per_step": ms_full / args.full_steps}
 
@@ -406,8 +427,6 @@ def run_ours(args):
         s = max(t["steps"], 1)
         return {k: t[k] / s for k in ("sort", "prep", "density", "force")}
 
-    ph_comp = phases(comp, min(K, 50))
-    ph_plain = phases(plain, min(k_plain, 10))
     if traj is not None:
         full["phase_ms_at_end"] = phases(traj, 20)
         traj.set_counting(True)
@@ -456,7 +475,6 @@ def run_ours(args):
     force_ms = ph_comp["force"]
     achieved = FORCE_BYTES["comp"] * n / (force_ms / 1e3) / 1e9
     step_ms = ms_comp / K
-    launches_per_step = 7 + 3  # sort kernels + prep/density/force
 
     line = None
     if rank == 0:
@@ -491,13 +509,15 @@ def run_ours(args):
             "candidates_per_particle": cnt["candidates"] / n,
             "roofline": {
                 "bound": "hbm",
-                "kernel": "k_force_comp (force + integrate + bounds)",
+                "kernel": "k_force_tiled (force + integrate + bounds; the dense-cell force kernel that follows "
+                          "it has no work in this state and is timed with it)",
                 "achieved": achieved,
                 "peak": hbm_peak,
                 "unit": "GB/s",
                 "frac": achieved / hbm_peak,
                 "peak_kind": peak_kind,
-                "traffic": None,
+                "traffic": FORCE_TRAFFIC_PER_PARTICLE * n,
+                "traffic_note": "ncu DRAM bytes per launch at 1,024,000 particles, scaled by particle count",
                 "algorithmic_bytes_per_particle": FORCE_BYTES["comp"],
                 "note": "sparse neighbour gather: FP/issue-bound, not HBM-bound; frac of measured HBM peak",
             },
@@ -510,7 +530,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": 2 * 24 * n, "steps": ke,
                     "path": "phy_fluid_set_field(pos, vel) from pinned host -> phy_fluid_step -> "
                             "phy_fluid_get_field(pos, vel) to pinned host"},
-            "gpu_launches": launches_per_step * K,
+            "gpu_launches": LAUNCHES_PER_STEP * K,
             "clocks": clocks,
             "cpu_baseline": cpu,
             "batched": batched,

@@ -144,8 +144,9 @@ int32_t phy_fluid_set_counting(PhyWorldHandle *w, uint32_t sub, int32_t on);
 int32_t phy_fluid_step_counters(PhyWorldHandle *w, uint32_t sub, uint64_t *out4);
 
 /* Per-phase device timing of `sub` with CUDA events on its stream.  While on,
- * every step waits for its own events (so leave it off on the hot path);
- * phy_fluid_phase_times returns the accumulated milliseconds
+ * every step records five events without waiting for them (steps are then
+ * not captured into CUDA graphs); phy_fluid_phase_times waits for the last
+ * timed step and returns the accumulated milliseconds
  * out5 = {sort, per-particle prep, density pass, force pass, steps timed}
  * and resets them when reset != 0. */
 int32_t phy_fluid_set_timing(PhyWorldHandle *w, uint32_t sub, int32_t on);

@@ -337,8 +337,8 @@ FluidWorld::~FluidWorld() {
   dfree(d_scene_bbox_);
   release_snapshot();
   tape_clear();
-  for (auto& e : ev_)
-    if (e) cudaEventDestroy(e);
+  for (auto& set : ev_pool_)
+    for (auto& e : set) cudaEventDestroy(e);
   if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 
@@ -945,14 +945,14 @@ StepConsts FluidWorld::prepare_step(double dt) {
 }
 
 // The device work of one step on the world's stream.
-void FluidWorld::enqueue_step(const StepConsts& c, const PassEvents& pe) {
+void FluidWorld::enqueue_step(const StepConsts& c, const PassEvents& pe, const cudaEvent_t* ev) {
   cuda_check(cudaMemsetAsync(b_.flags, 0, sizeof(uint32_t), stream_), "flags reset");
   if (counting_) cuda_check(cudaMemsetAsync(b_.counters, 0, 2 * sizeof(unsigned long long), stream_), "memset");
   unsigned long long* saved = b_.counters;
   if (!counting_) b_.counters = nullptr;
-  if (timing_) cuda_check(cudaEventRecord(ev_[0], stream_), "event");
+  if (ev) cuda_check(cudaEventRecord(ev[0], stream_), "event");
   launch_sort(c, b_, stream_, tuning_.sort_block);
-  if (timing_) cuda_check(cudaEventRecord(ev_[1], stream_), "event");
+  if (ev) cuda_check(cudaEventRecord(ev[1], stream_), "event");
   if (prec_ == Precision::F64Plain)
     launch_plain_passes(c, b_, stream_, pe);
   else if (tile_)
@@ -980,21 +980,20 @@ StepConsts FluidWorld::step_impl(double dt) {
   }
   StepConsts c = prepare_step(dt);
   PassEvents pe;
+  cudaEvent_t* ev = nullptr;
   if (timing_) {
-    pe.after_prep = ev_[2];
-    pe.after_density = ev_[3];
-  }
-  enqueue_step(c, pe);
-  if (timing_) {
-    cuda_check(cudaEventRecord(ev_[4], stream_), "event");
-    cuda_check(cudaEventSynchronize(ev_[4]), "event sync");
-    for (int k = 0; k < 4; ++k) {
-      float ms = 0.f;
-      cuda_check(cudaEventElapsedTime(&ms, ev_[k], ev_[k + 1]), "elapsed");
-      phase_ms_[k] += ms;
+    if (ev_used_ == 4096) collect_phase_times();  // bounds the pool
+    if (ev_used_ == ev_pool_.size()) {
+      std::array<cudaEvent_t, 5> set;
+      for (auto& e : set) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+      ev_pool_.push_back(set);
     }
-    timed_steps_ += 1;
+    ev = ev_pool_[ev_used_++].data();
+    pe.after_prep = ev[2];
+    pe.after_density = ev[3];
   }
+  enqueue_step(c, pe, ev);
+  if (ev) cuda_check(cudaEventRecord(ev[4], stream_), "event");
   return c;
 }
 
@@ -1032,7 +1031,7 @@ void FluidWorld::run_graph(double dt, int k) {
     cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "graph capture");
     try {
       PassEvents none;
-      for (int q = 0; q < k; ++q) enqueue_step(c, none);
+      for (int q = 0; q < k; ++q) enqueue_step(c, none, nullptr);
     } catch (...) {
       cudaStreamEndCapture(stream_, &graph);
       if (graph) cudaGraphDestroy(graph);
@@ -1255,13 +1254,24 @@ std::vector<TuneTrial> FluidWorld::autotune(double dt, int steps) {
   return trials;
 }
 
-void FluidWorld::set_timing(bool on) {
-  if (on && !ev_[0])
-    for (auto& e : ev_) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
-  timing_ = on;
+void FluidWorld::set_timing(bool on) { timing_ = on; }
+
+// Waits for the last timed step and adds every recorded step's phases.
+void FluidWorld::collect_phase_times() {
+  if (ev_used_ == 0) return;
+  cuda_check(cudaEventSynchronize(ev_pool_[ev_used_ - 1][4]), "event sync");
+  for (size_t q = 0; q < ev_used_; ++q)
+    for (int k = 0; k < 4; ++k) {
+      float ms = 0.f;
+      cuda_check(cudaEventElapsedTime(&ms, ev_pool_[q][k], ev_pool_[q][k + 1]), "elapsed");
+      phase_ms_[k] += ms;
+    }
+  timed_steps_ += (double)ev_used_;
+  ev_used_ = 0;
 }
 
 void FluidWorld::phase_times(double* out5, bool reset) {
+  collect_phase_times();
   for (int k = 0; k < 4; ++k) out5[k] = phase_ms_[k];
   out5[4] = timed_steps_;
   if (reset) {

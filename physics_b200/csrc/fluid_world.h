@@ -9,6 +9,7 @@
 // callers always see insertion order, as with the reference's `particles` Vec.
 #pragma once
 
+#include <array>
 #include <cstdint>
 #include <memory>
 #include <stdexcept>
@@ -135,8 +136,9 @@ class FluidWorld {
 
   // Per-phase device timing with CUDA events on the world's stream: while
   // enabled, every step records events around the sort, the per-particle
-  // preparation, the density pass and the force pass, and waits for them to
-  // accumulate the durations (ms).  out = {sort, prep, density, force, steps}.
+  // preparation, the density pass and the force pass without waiting for
+  // them; phase_times waits for the last recorded step and accumulates the
+  // durations (ms).  out = {sort, prep, density, force, steps}.
   void set_timing(bool on);
   void phase_times(double* out5, bool reset);
 
@@ -166,7 +168,7 @@ class FluidWorld {
   StepConsts prepare_step(double dt);
   StepConsts step_impl(double dt);
   void save_checkpoint();
-  void enqueue_step(const StepConsts& c, const PassEvents& pe);
+  void enqueue_step(const StepConsts& c, const PassEvents& pe, const cudaEvent_t* ev);
   void run_graph(double dt, int k);
   void drop_graphs();
   void snapshot(bool restore);
@@ -189,7 +191,10 @@ class FluidWorld {
   int halo_cap_ = 1 << 30;
   int tile_ = 0;  // linearisation of the current box (0 = x-major)
   bool timing_ = false;
-  cudaEvent_t ev_[5] = {};
+  // One set of 5 events per timed step, recycled after phase_times reads them.
+  std::vector<std::array<cudaEvent_t, 5>> ev_pool_;
+  size_t ev_used_ = 0;
+  void collect_phase_times();
   double phase_ms_[4] = {0, 0, 0, 0};
   double timed_steps_ = 0;
   long long* d_bbox_ = nullptr;  // 7 values: min xyz, max xyz, non-finite flag
