@@ -640,7 +640,8 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
 // particles; it tests every candidate.
 
 constexpr int kDT = 256;       // threads per dense CTA
-constexpr int kDQ = 2;         // queries per lane group
+constexpr int kDQ = 2;         // queries per lane group (density)
+constexpr int kFQ = 1;         // queries per lane group (force: its accumulators are large)
 constexpr int kDChunk = 1024;  // candidates staged per chunk
 
 struct CellGeom {
@@ -718,10 +719,11 @@ __device__ __forceinline__ void dense_stage(const StepConsts& c, const TiledArgs
   }
 }
 
-// Lanes per query for a cell of q particles (a power of two, 1..32).
-__device__ __forceinline__ int dense_split(uint32_t q) {
+// Lanes per query for a cell of q particles when each lane group holds
+// `per_group` queries (a power of two, 1..32).
+__device__ __forceinline__ int dense_split(uint32_t q, int per_group) {
   int sp = 1;
-  while (sp < 32 && (uint32_t)(2 * sp) * q <= (uint32_t)(kDT * kDQ)) sp <<= 1;
+  while (sp < 32 && (uint32_t)(2 * sp) * q <= (uint32_t)(kDT * per_group)) sp <<= 1;
   return sp;
 }
 
@@ -746,7 +748,7 @@ __global__ void __launch_bounds__(kDT, 4) k_density_dense(StepConsts c, TiledArg
     const CellGeom cg = cell_geom(c, a, cell);
     const SceneBox& bx = c.boxes[cg.sc];
     const uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
-    const int sp = dense_split(q1 - q0);          // uniform across the CTA
+    const int sp = dense_split(q1 - q0, kDQ);     // uniform across the CTA
     const int groups = kDT / sp;
     const int grp = threadIdx.x / sp, sub = threadIdx.x % sp;
     __syncthreads();  // the previous cell's tables are no longer read
@@ -827,18 +829,18 @@ __global__ void __launch_bounds__(kDT) k_force_dense(StepConsts c, TiledArgs a) 
     const CellGeom cg = cell_geom(c, a, cell);
     const SceneBox& bx = c.boxes[cg.sc];
     const uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
-    const int sp = dense_split(q1 - q0);
+    const int sp = dense_split(q1 - q0, kFQ);
     const int groups = kDT / sp;
     const int grp = threadIdx.x / sp, sub = threadIdx.x % sp;
     __syncthreads();  // the previous cell's tables are no longer read
     dense_neighbour_table(c, a, bx, cg, s_src, s_pre);
     const uint32_t total = s_pre[27];
-    for (uint32_t qb = q0; qb < q1; qb += (uint32_t)(groups * kDQ)) {
-      float4 qp[kDQ], qv[kDQ];
-      CompAcc acc[kDQ];
-      ForcePart part[kDQ];
+    for (uint32_t qb = q0; qb < q1; qb += (uint32_t)(groups * kFQ)) {
+      float4 qp[kFQ], qv[kFQ];
+      CompAcc acc[kFQ];
+      ForcePart part[kFQ];
 #pragma unroll
-      for (int k = 0; k < kDQ; ++k) {
+      for (int k = 0; k < kFQ; ++k) {
         const uint32_t qi = qb + (uint32_t)(grp + k * groups);
         qp[k] = qi < q1 ? a.cpos[qi] : make_float4(kFar, kFar, kFar, 0.f);
         qv[k] = qi < q1 ? a.cvel[qi] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -853,7 +855,7 @@ __global__ void __launch_bounds__(kDT) k_force_dense(StepConsts c, TiledArgs a) 
         });
         __syncthreads();
 #pragma unroll
-        for (int k = 0; k < kDQ; ++k) {
+        for (int k = 0; k < kFQ; ++k) {
           const float lapm = qp[k].w * c.lap_cf;
           uint32_t since = 0;
           for (uint32_t j = (uint32_t)sub; j < m; j += (uint32_t)sp) {
@@ -870,7 +872,7 @@ __global__ void __launch_bounds__(kDT) k_force_dense(StepConsts c, TiledArgs a) 
         }
       }
 #pragma unroll
-      for (int k = 0; k < kDQ; ++k) {
+      for (int k = 0; k < kFQ; ++k) {
         // Combine the group's partial sums (compensations applied per lane).
         CompAcc t;
         t.fpx = group_sum(acc[k].fpx - acc[k].cpx, sp);
