@@ -375,6 +375,7 @@ void FluidWorld::free_all() {
   dfree(b_.num_tiles);
   dfree(b_.boxes);
   dfree(b_.queue);
+  dfree(b_.tile_crowd);
   dfree(b_.dense_cells);
   dfree(b_.okey);
   dfree(b_.cell_of);
@@ -438,6 +439,7 @@ void FluidWorld::ensure_capacity(size_t n) {
   dfree(b_.sorted_cell);
   dfree(b_.tile_head);
   dfree(b_.tile_slot);
+  dfree(b_.tile_crowd);
   dfree(b_.dense_cells);
   dfree(b_.okey);
   dgrow(b_.cell_of, 0, cap, s);
@@ -462,6 +464,7 @@ void FluidWorld::ensure_mode_buffers() {
     if (!b_.sorted_cell) dalloc(b_.sorted_cell, cap);
     if (!b_.tile_head) dalloc(b_.tile_head, tile_head_length((int)cap));
     if (!b_.tile_slot) dalloc(b_.tile_slot, cap + 1);
+    if (!b_.tile_crowd) dalloc(b_.tile_crowd, cap + 1);
     if (!b_.num_tiles) dalloc(b_.num_tiles, 1);
     if (!b_.queue) dalloc(b_.queue, 3);
     if (!b_.dense_cells) dalloc(b_.dense_cells, cap);

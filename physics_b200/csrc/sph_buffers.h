@@ -55,6 +55,7 @@ struct DevBuffers {
   uint32_t* sorted_cell = nullptr;
   uint32_t* tile_head = nullptr;
   uint32_t* tile_slot = nullptr;
+  uint8_t* tile_crowd = nullptr;  // 1: tile above kDenseMean per occupied cell
   uint32_t* num_tiles = nullptr;
   // Scene boxes of the tiled linearisation (one entry for a single world),
   // the work-queue counters of the persistent passes (density, force) and the

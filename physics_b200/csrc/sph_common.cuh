@@ -28,6 +28,12 @@ constexpr int kCodeBits = 5;
 // and written out coalesced; further entries go straight to global memory.
 constexpr int kStagedNeighbors = 40;
 
+// Tiled form: a tile whose occupied cells hold more than this many particles
+// on average goes to the dense-cell passes even when its halo could be
+// staged; from about this density on, neighbour lists overflow and a staged
+// tile would rescan its cells for every query.
+constexpr uint32_t kDenseMean = 32;
+
 // Error bits written by device code into the per-world flag word.
 enum : uint32_t {
   kFlagOutOfBox = 1u,    // a cell key fell outside the grid box

@@ -55,6 +55,7 @@ struct TiledArgs {
   const uint32_t* __restrict__ cell_start;
   const uint32_t* __restrict__ sorted_cell;
   const uint32_t* __restrict__ tile_slot;
+  const uint8_t* __restrict__ tile_crowd;  // 1: route the tile to the dense-cell passes
   const uint32_t* __restrict__ num_tiles;
   float4* cpos;  // cell-local x, y, z and mass
   float4* cvel;  // vx, vy, vz and p/rho^2
@@ -332,7 +333,7 @@ __global__ void __launch_bounds__(kTT) k_density_tiled(StepConsts c, TiledArgs a
        k = next_tile(a.queue, 0, k + gridDim.x, &s_next)) {
     const TileGeom g = tile_geom(c, a, k);
     halo_table(c, a, g, s_src, s_end, s_off, ws);
-    const int slab = pick_slab(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
+    const int slab = a.tile_crowd[k] ? 0 : pick_slab(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
     if (slab == 0) {
       queue_dense_cells(a, g, ws, &s_next);
       continue;  // uniform across the CTA
@@ -554,7 +555,7 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
        k = next_tile(a.queue, 1, k + gridDim.x, &s_next)) {
     const TileGeom g = tile_geom(c, a, k);
     halo_table(c, a, g, s_src, s_end, s_off, ws);
-    const int slab = pick_slab(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
+    const int slab = a.tile_crowd[k] ? 0 : pick_slab(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
     if (slab == 0) continue;  // the dense-cell pass computes this tile
     for (int x0 = 0; x0 < kTB; x0 += slab) {
     const uint32_t base = s_off[x0 * kH * kH];
@@ -948,6 +949,7 @@ void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const
   a.cell_start = b.cell_start;
   a.sorted_cell = b.sorted_cell;
   a.tile_slot = b.tile_slot;
+  a.tile_crowd = b.tile_crowd;
   a.num_tiles = b.num_tiles;
   a.cpos = b.cpos;
   a.cvel = b.cvel;
