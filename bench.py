@@ -13,7 +13,10 @@ step is bit-identical to the f64 oracle).
 
 With --gpus N > 1 (under torchrun) every rank steps its own replica of the
 scene: the single-scene step does not shard ("replicas only"), so value is
-N x particles x K / (max over ranks of the timed region).
+N x particles x K / (max over ranks of the timed region).  The batched form's
+scenes are independent and are partitioned across the ranks by particle count
+instead (its "batched" block: the whole batch's particle-steps over the max
+over ranks).
 
 --impl reference times the CPU restatement of the reference's rayon step
 (oracle/, OpenMP over all host threads) on a bounded sub-block of the same
@@ -131,14 +134,22 @@ BATCH_DT = 0.005
 BATCH_CHUNK = 10  # steps per captured CUDA graph
 
 
-def run_batched(pb, scenes, stream, n_scenes: int, steps: int, warmup: int) -> dict:
+def run_batched(pb, scenes, stream, n_scenes: int, steps: int, warmup: int, rank: int = 0, world_size: int = 1,
+                max_over_ranks=lambda x: x, barrier=lambda: None) -> dict:
     """The batched form: n_scenes independent dam breaks (log-uniform 2k..200k particles,
     aspect U[0.5,2], fill U[0.2,0.5]) in one world, one sort and one persistent launch per
     pass, steps captured in CUDA graphs, launch knobs from the library's autotuner; against
     looping the single-scene step over the same scenes (each scene its own world and
-    phy_fluid_step call)."""
+    phy_fluid_step call).  With several ranks the scenes are partitioned across them by
+    particle count (no collective in the step); times are the max over ranks and the
+    values count every rank's particles (strong scaling: the batch is fixed)."""
     import torch
-    batch = scenes.batch_scenes(n_scenes)
+    every = scenes.batch_scenes(n_scenes)
+    total_all = int(sum(b.n for b in every))
+    parts = scenes.partition_scenes([b.n for b in every], world_size)
+    if any(not part for part in parts):
+        raise ValueError("the batched form needs at least one scene per rank")
+    batch = [every[i] for i in parts[rank]]
     counts = [b.n for b in batch]
     total = int(sum(counts))
     mass = scenes.lattice_mass(scenes.SPACING)
@@ -154,6 +165,7 @@ def run_batched(pb, scenes, stream, n_scenes: int, steps: int, warmup: int) -> d
     chosen = w.tuning()
 
     def timed(fn, k):
+        barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -161,7 +173,7 @@ def run_batched(pb, scenes, stream, n_scenes: int, steps: int, warmup: int) -> d
         fn(k)
         e1.record(stream)
         e1.synchronize()
-        return e0.elapsed_time(e1)
+        return max_over_ranks(e0.elapsed_time(e1))
 
     w.step(BATCH_DT, max(warmup, BATCH_CHUNK))
     ms = timed(lambda k: w.step(BATCH_DT, k), steps)
@@ -188,19 +200,22 @@ def run_batched(pb, scenes, stream, n_scenes: int, steps: int, warmup: int) -> d
 
     ms_loop = timed(loop, steps)
     del worlds
-    value = total * steps / (ms / 1e3)
-    loop_value = total * steps / (ms_loop / 1e3)
+    value = total_all * steps / (ms / 1e3)
+    loop_value = total_all * steps / (ms_loop / 1e3)
     return {
-        "workload": f"{n_scenes} dam-break scenes, {total} particles (log-uniform 2000..200000 per scene, "
+        "workload": f"{n_scenes} dam-break scenes, {total_all} particles (log-uniform 2000..200000 per scene, "
                     f"aspect U[0.5,2], fill U[0.2,0.5]), dt={BATCH_DT}, FP32-compensated",
         "scenes": n_scenes,
-        "particles": total,
+        "particles": total_all,
+        "ranks": world_size,
+        "scaling": "strong (the scenes are partitioned across ranks by particle count)",
+        "particles_rank0": total if rank == 0 else None,
         "steps": steps,
         "value": value,
         "unit": UNIT,
         "ms_per_step": ms / steps,
         "graph_chunk": BATCH_CHUNK,
-        "eager_value": total * k_eager / (ms_eager / 1e3),
+        "eager_value": total_all * k_eager / (ms_eager / 1e3),
         "loop_single_scene_value": loop_value,
         "loop_single_scene_ms_per_step": ms_loop / steps,
         "speedup_vs_loop": value / loop_value,
@@ -446,7 +461,8 @@ def run_ours(args):
 
     batched = None
     if args.batch_scenes > 0 and args.batch_steps > 0:
-        batched = run_batched(pb, scenes, stream, args.batch_scenes, args.batch_steps, W)
+        batched = run_batched(pb, scenes, stream, args.batch_scenes, args.batch_steps, W, rank, world_size,
+                              max_over_ranks, barrier)
 
     # ---- end to end through the C ABI with host buffers ------------------------------
     pin_pos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()

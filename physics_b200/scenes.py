@@ -153,6 +153,23 @@ class BatchScene:
         return self.pos.shape[0]
 
 
+def partition_scenes(counts, nparts: int) -> list:
+    """Scenes split over `nparts` GPUs by particle count (greedy bin packing: the
+    largest scene first, each to the part holding the fewest particles, ties to the
+    lowest part).  Returns one ascending list of scene indices per part; every part's
+    load is within the largest scene of the mean."""
+    if nparts < 1:
+        raise ValueError("nparts must be >= 1")
+    order = sorted(range(len(counts)), key=lambda i: (-int(counts[i]), i))
+    load = [0] * nparts
+    parts = [[] for _ in range(nparts)]
+    for i in order:
+        k = min(range(nparts), key=lambda p: (load[p], p))
+        parts[k].append(i)
+        load[k] += int(counts[i])
+    return [sorted(p) for p in parts]
+
+
 def batch_scenes(n_scenes: int = 256, nmin: int = 2000, nmax: int = 200000, seed: int = BATCH_SEED,
                  spacing: float = SPACING) -> list:
     """The batched form's scenes (see the module docstring)."""
