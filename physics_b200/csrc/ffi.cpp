@@ -9,6 +9,7 @@
 #include <cstring>
 #include <limits>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/phy_ffi.h"
@@ -86,9 +87,14 @@ uintptr_t read_vec(PhyWorldHandle* w, T* buf, uintptr_t len, int field) {
     uintptr_t room = len / 3 - written;
     if (room == 0) break;
     size_t take = n < room ? n : (size_t)room;
-    tmp.resize(3 * n);
-    s->world->get_field(field, tmp.data());
-    for (size_t i = 0; i < 3 * take; ++i) buf[3 * written + i] = (T)tmp[i];
+    if constexpr (std::is_same<T, float>::value) {
+      // The f32 channel is cast on the device (lib.rs:595-653: an `as f32` of each value).
+      s->world->get_vec_f32(field, buf + 3 * written, take);
+    } else {
+      tmp.resize(3 * n);
+      s->world->get_field(field, tmp.data());
+      for (size_t i = 0; i < 3 * take; ++i) buf[3 * written + i] = (T)tmp[i];
+    }
     written += take;
     if (take < n) break;
   }

@@ -58,6 +58,17 @@ __global__ void k_get_vec_by_id(int n, const uint32_t* __restrict__ id, const do
     dst[o + 2] = z[s];
   }
 }
+__global__ void k_get_vec_f32_by_id(int n, const uint32_t* __restrict__ id, const double* __restrict__ x,
+                                    const double* __restrict__ y, const double* __restrict__ z,
+                                    float* __restrict__ dst) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) {
+    size_t o = 3 * (size_t)id[s];
+    dst[o] = (float)x[s];
+    dst[o + 1] = (float)y[s];
+    dst[o + 2] = (float)z[s];
+  }
+}
 // Appends m particles (insertion-order staging: pos 3m, vel 3m, mass m,
 // material m) at slots [n0, n0+m).
 __global__ void k_append(int n0, int m, const double* __restrict__ st, double* px, double* py, double* pz,
@@ -873,6 +884,20 @@ void FluidWorld::get_field(int field, double* out) {
   cuda_check(cudaMemcpyAsync(out, st, (size_t)nc * n_ * sizeof(double), cudaMemcpyDeviceToHost, stream_),
              "get_field copy");
   cuda_check(cudaStreamSynchronize(stream_), "get_field sync");
+}
+
+void FluidWorld::get_vec_f32(int field, float* out, size_t count) {
+  if (field != PHY_FIELD_POS && field != PHY_FIELD_VEL) throw std::invalid_argument("get_vec_f32: pos or vel only");
+  if (n_ == 0 || count == 0) return;
+  if (count > n_) count = n_;
+  const int n = (int)n_;
+  const ParticleConsts& pc = b_.pc[b_.cur];
+  float* st = reinterpret_cast<float*>(b_.stage);  // 3n floats fit the 8n-double stage
+  const int o = field == PHY_FIELD_POS ? 0 : 3;
+  k_get_vec_f32_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, b_.pv1[o], b_.pv1[o + 1], b_.pv1[o + 2], st);
+  cuda_check(cudaGetLastError(), "get_vec_f32 kernel");
+  cuda_check(cudaMemcpyAsync(out, st, 3 * count * sizeof(float), cudaMemcpyDeviceToHost, stream_), "get_vec_f32 copy");
+  cuda_check(cudaStreamSynchronize(stream_), "get_vec_f32 sync");
 }
 
 void FluidWorld::set_field(int field, const double* in) {

@@ -118,6 +118,10 @@ class FluidWorld {
   // Insertion-order field access (particle.rs:17-46).
   static int components(int field);
   void get_field(int field, double* out);
+  // Position or velocity as f32 (an exact `as f32` cast of each f64 value,
+  // made on the device so half the bytes cross to the host): the first
+  // `count` particles in insertion order, xyz interleaved.
+  void get_vec_f32(int field, float* out, size_t count);
   void set_field(int field, const double* in);
 
   void set_stream(cudaStream_t s);

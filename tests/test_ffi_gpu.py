@@ -84,6 +84,10 @@ def test_ffi_f32_channel_matches_f64(gpu):
     lib.phy_world_get_fluid_velocities(w, dp(v64), v64.size)
     lib.phy_world_get_fluid_velocities_f32(w, v32.ctypes.data_as(L.FP), v32.size)
     assert np.array_equal(v32, v64.astype(np.float32))
+    # A short buffer takes whole particles only, in insertion order (lib.rs:399-460).
+    half = np.full(3 * (n // 2) + 2, -1.0, np.float32)
+    assert lib.phy_world_get_fluid_positions_f32(w, half.ctypes.data_as(L.FP), half.size) == n // 2
+    assert np.array_equal(half[:3 * (n // 2)], b32[:3 * (n // 2)]) and (half[3 * (n // 2):] == -1.0).all()
     lib.phy_world_destroy(w)
 
 
