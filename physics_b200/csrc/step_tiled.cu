@@ -426,10 +426,30 @@ struct CompAcc {
 };
 
 // mu_eff, acc, integrate and bounds in f64 (world.rs:319-397).
+// The f64 operands of a particle's integration epilogue, loaded before its
+// pair loop so their latency overlaps the pair work.
+struct OwnState {
+  double rho, p3[3], v3[3];
+  uint32_t mat;
+};
+
+__device__ __forceinline__ OwnState load_own(const TiledArgs& a, int i) {
+  OwnState o;
+  o.rho = a.rho[i];
+  o.mat = a.mat[i];
+  o.p3[0] = a.px[i];
+  o.p3[1] = a.py[i];
+  o.p3[2] = a.pz[i];
+  o.v3[0] = a.vx[i];
+  o.v3[1] = a.vy[i];
+  o.v3[2] = a.vz[i];
+  return o;
+}
+
 __device__ __forceinline__ void finish_particle(const StepConsts& c, const TiledArgs& a, int i, const CompAcc& q,
-                                                const SceneBox& bx) {
-  const double rho_i = a.rho[i];
-  const uint32_t m = a.mat[i];
+                                                const SceneBox& bx, const OwnState& own) {
+  const double rho_i = own.rho;
+  const uint32_t m = own.mat;
   const int midx = (int)m < c.n_visc_k ? (int)m : 0;
   double kc, nn;
   material_coeffs(c, midx, kc, nn);
@@ -460,8 +480,8 @@ __device__ __forceinline__ void finish_particle(const StepConsts& c, const Tiled
     a.bay[i] = 0.0;
     a.baz[i] = 0.0;
   }
-  double p3[3] = {a.px[i], a.py[i], a.pz[i]};
-  double v3[3] = {a.vx[i], a.vy[i], a.vz[i]};
+  double p3[3] = {own.p3[0], own.p3[1], own.p3[2]};
+  double v3[3] = {own.v3[0], own.v3[1], own.v3[2]};
   const double acc3[3] = {ax, ay, az};
   const double xs3[3] = {(double)q.xsx, (double)q.xsy, (double)q.xsz};
   bool finite = true;
@@ -482,6 +502,12 @@ __device__ __forceinline__ void finish_particle(const StepConsts& c, const Tiled
     a.out_pv[3 + k][i] = v;
   }
   if (!finite) atomicOr(a.flags, kFlagNonFinite);
+}
+
+// The same with the particle's f64 state loaded at the point of use.
+__device__ __forceinline__ void finish_particle(const StepConsts& c, const TiledArgs& a, int i, const CompAcc& q,
+                                                const SceneBox& bx) {
+  finish_particle(c, a, i, q, bx, load_own(a, i));
 }
 
 // Batch partial sums of the pressure and raw viscous forces; folded into the
@@ -580,6 +606,7 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
       const float4 pi = s_pos[si];
       const float4 vi = s_vel[si];
       const float lapm_i = pi.w * c.lap_cf;
+      const OwnState own = load_own(a, (int)qi);
       CompAcc q;
       ForcePart b;
       const uint32_t cnt = a.nbr_count[qi];
@@ -615,7 +642,7 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
             }
           }
       }
-      finish_particle(c, a, (int)qi, q, c.boxes[g.sc]);
+      finish_particle(c, a, (int)qi, q, c.boxes[g.sc], own);
     }
     __syncthreads();
     }  // slabs
@@ -623,7 +650,7 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
   const uint32_t end = a.tile_slot[ntiles];
   for (uint32_t qi = end + blockIdx.x * kTT + threadIdx.x; qi < (uint32_t)c.n; qi += gridDim.x * kTT) {
     CompAcc q;
-    finish_particle(c, a, (int)qi, q, c.boxes[a.scene ? (int)a.scene[qi] : 0]);
+    finish_particle(c, a, (int)qi, q, c.boxes[a.scene ? (int)a.scene[qi] : 0], load_own(a, (int)qi));
   }
 }
 
@@ -818,7 +845,9 @@ __global__ void __launch_bounds__(kDT, 4) k_density_dense(StepConsts c, TiledArg
   }
 }
 
-__global__ void __launch_bounds__(kDT) k_force_dense(StepConsts c, TiledArgs a) {
+// (Four resident CTAs, the limit of its shared memory, leave 64 registers a
+// thread, which its single query fits without spilling.)
+__global__ void __launch_bounds__(kDT, 4) k_force_dense(StepConsts c, TiledArgs a) {
   __shared__ float4 s_pos[kDChunk];
   __shared__ float4 s_vel[kDChunk];
   __shared__ float s_mr[kDChunk];
