@@ -15,8 +15,12 @@
 // The density pass records each particle's in-range neighbours as 16-bit
 // shared-memory slot indices; the force pass re-stages the same halo in the
 // same order and walks the list without re-filtering candidates, so its
-// lanes stay converged.  Tiles whose halo exceeds the staging capacity, and
-// lists longer than kMaxNeighbors, fall back to reading global memory.
+// lanes stay converged.  A tile whose halo exceeds the staging capacity is
+// processed in x-slabs of 2 or 1 cell layers; a particle whose list exceeds
+// kMaxNeighbors is rescanned from the staged cells.  Tiles where no slab
+// fits, or flagged crowded by the tile-list kernel (more than kDenseMean
+// particles per occupied cell), go to the dense-cell kernels at the end of
+// this file.
 #include <cuda_runtime.h>
 
 #include <algorithm>
