@@ -48,7 +48,8 @@ struct DevBuffers {
   uint32_t* nbr = nullptr;
   uint32_t* nbr_count = nullptr;
   // Tiled form: 16-bit neighbour slots (shared-memory staging order of the
-  // tile's halo), column-major like nbr.
+  // tile's halo), row-major: the kMaxNeighbors entries of sorted slot i at
+  // nbr16[i * kMaxNeighbors ..].
   uint16_t* nbr16 = nullptr;
   // Tiled sort: cell of each sorted slot, tile heads (scan scratch), first
   // slot of every occupied tile (+ end), and the device-side tile count.
@@ -76,7 +77,7 @@ struct DevBuffers {
   uint32_t* block_sums = nullptr;
   int block_sums_capacity = 0;
   // Insertion-order staging for uploads and downloads (f64 and u32 views).
-  double* stage = nullptr;   // 3 * capacity doubles
+  double* stage = nullptr;   // 8 * capacity doubles
   uint32_t* flags = nullptr; // error bits, device
   unsigned long long* counters = nullptr;  // candidates, pairs (device)
   // Optional outputs of the f64 plain force pass for the adjoint's tape: the
