@@ -282,6 +282,45 @@ __device__ __forceinline__ void put_pair_slot(float* sp, uint32_t k, float4 v) {
 
 constexpr float kFar = 1.0e18f;  // dummy particle coordinate (never in range)
 
+// Filters staged candidates [cb, ce) (an even count, at most 32) against a
+// query at (PX, PY, PZ): returns the in-range mask (bit k = candidate cb + k)
+// and adds -m_j (h0^2 - r^2)^3 of the in-range candidates to NPART.  With the
+// cutoff equal to the kernel radius (kExact) d = r^2 - h0^2 gives both: its
+// sign bit is the in-range bit (d is never -0: r^2 >= +0 and h0^2 > 0), and
+// min(d, 0)^3 = -(h0^2 - r^2)^3 rounds exactly as the positive form.  The
+// bits are shifted in from the right, so the chunk's first candidate ends in
+// the highest bit and one bit reversal restores candidate order.
+template <bool kExact>
+__device__ __forceinline__ uint32_t filter_chunk(const float4* s_pp4, uint32_t cb, uint32_t ce, f2 PX, f2 PY,
+                                                 f2 PZ, f2 HC2, f2 H0SQ, f2& NPART) {
+  uint32_t mask = 0;
+#pragma unroll 2
+  for (uint32_t j = cb; j < ce; j += 2) {
+    const float4 A = s_pp4[j];      // x0 x1 y0 y1
+    const float4 B = s_pp4[j + 1];  // z0 z1 m0 m1
+    const f2 DX = f2_sub(f2_pack(A.x, A.y), PX);
+    const f2 DY = f2_sub(f2_pack(A.z, A.w), PY);
+    const f2 DZ = f2_sub(f2_pack(B.x, B.y), PZ);
+    const f2 R2 = f2_fma(DZ, DZ, f2_fma(DY, DY, f2_mul(DX, DX)));
+    float d0, d1, n0, n1;
+    f2_unpack(f2_sub(R2, HC2), d0, d1);
+    mask = __funnelshift_l(__float_as_uint(d0), mask, 1);
+    mask = __funnelshift_l(__float_as_uint(d1), mask, 1);
+    if (kExact) {
+      n0 = fminf(d0, 0.f);
+      n1 = fminf(d1, 0.f);
+    } else {
+      float e0, e1;
+      f2_unpack(f2_sub(R2, H0SQ), e0, e1);
+      n0 = d0 < 0.f ? e0 : 0.f;
+      n1 = d1 < 0.f ? e1 : 0.f;
+    }
+    const f2 N = f2_pack(n0, n1);
+    NPART = f2_fma(f2_mul(N, N), f2_mul(N, f2_pack(B.z, B.w)), NPART);
+  }
+  return __brev(mask) >> (32u - (ce - cb));
+}
+
 // Appends 16-bit neighbour slots to a particle's row-major list (row of
 // kMaxNeighbors entries) through a 64-bit register accumulator flushed with
 // 8-byte stores; entries past kMaxNeighbors are dropped (the count still
@@ -320,8 +359,11 @@ __device__ __forceinline__ void queue_dense_cells(const TiledArgs& a, const Tile
   __syncthreads();
 }
 
-template <bool kCount>
-__global__ void __launch_bounds__(kTT) k_density_tiled(StepConsts c, TiledArgs a) {
+// kExact: the cutoff min(h, h0) equals the kernel radius h0 (the usual case).
+// Six CTAs per SM is the shared-memory limit (35 KB each); the register cap
+// that matches it (40) costs no spill.
+template <bool kCount, bool kExact>
+__global__ void __launch_bounds__(kTT, 6) k_density_tiled(StepConsts c, TiledArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   float* s_pp = reinterpret_cast<float*>(smem);  // kHaloCap slots, pair-interleaved
   uint32_t* s_src = reinterpret_cast<uint32_t*>(smem + kHaloCap * sizeof(float4));
@@ -329,7 +371,7 @@ __global__ void __launch_bounds__(kTT) k_density_tiled(StepConsts c, TiledArgs a
   uint32_t* s_off = s_end + kNH;
   uint32_t* ws = s_off + kNH + 1;
   const float hc2 = fminf(c.h2f, c.h0sqf);
-  const f2 H0SQ = f2_pack(c.h0sqf, c.h0sqf);
+  const f2 HC2 = f2_pack(hc2, hc2), H0SQ = f2_pack(c.h0sqf, c.h0sqf);
   __shared__ uint32_t s_next;
   const uint32_t ntiles = *a.num_tiles;
   unsigned cand = 0, pairs = 0;
@@ -367,27 +409,10 @@ __global__ void __launch_bounds__(kTT) k_density_tiled(StepConsts c, TiledArgs a
           const int h0 = hq + di * kH * kH + dj * kH - 1;  // cells h0 .. h0+2 (dk = -1, 0, 1)
           const uint32_t s0 = s_off[h0] - base, e0 = s_off[h0 + 3] - base;  // both even
           if (kCount) cand += (s_end[h0] - s_src[h0]) + (s_end[h0 + 1] - s_src[h0 + 1]) + (s_end[h0 + 2] - s_src[h0 + 2]);
-          f2 PART = f2_pack(0.f, 0.f);
+          f2 NPART = f2_pack(0.f, 0.f);
           for (uint32_t cb = s0; cb < e0; cb += 32) {
             const uint32_t ce = min(cb + 32u, e0);
-            uint32_t mask = 0;
-#pragma unroll 2
-            for (uint32_t j = cb; j < ce; j += 2) {
-              const float4 A = s_pp4[j];      // x0 x1 y0 y1
-              const float4 B = s_pp4[j + 1];  // z0 z1 m0 m1
-              const f2 DX = f2_sub(f2_pack(A.x, A.y), PX);
-              const f2 DY = f2_sub(f2_pack(A.z, A.w), PY);
-              const f2 DZ = f2_sub(f2_pack(B.x, B.y), PZ);
-              const f2 R2 = f2_fma(DZ, DZ, f2_fma(DY, DY, f2_mul(DX, DX)));
-              float r0, r1;
-              f2_unpack(R2, r0, r1);
-              const bool in0 = r0 < hc2, in1 = r1 < hc2;
-              float t0, t1;
-              f2_unpack(f2_sub(H0SQ, R2), t0, t1);
-              const f2 T = f2_pack(in0 ? t0 : 0.f, in1 ? t1 : 0.f);
-              PART = f2_fma(f2_mul(T, T), f2_mul(T, f2_pack(B.z, B.w)), PART);
-              mask |= ((in0 ? 1u : 0u) | (in1 ? 2u : 0u)) << (j - cb);
-            }
+            uint32_t mask = filter_chunk<kExact>(s_pp4, cb, ce, PX, PY, PZ, HC2, H0SQ, NPART);
             if (kCount) pairs += __popc(mask);
             while (mask) {
               const uint32_t b = __ffs(mask) - 1;
@@ -396,8 +421,8 @@ __global__ void __launch_bounds__(kTT) k_density_tiled(StepConsts c, TiledArgs a
             }
           }
           float p0, p1;
-          f2_unpack(PART, p0, p1);
-          kahan_add(s, comp, c.poly6_cf * (p0 + p1));
+          f2_unpack(NPART, p0, p1);
+          kahan_add(s, comp, c.poly6_cf * -(p0 + p1));
         }
       }
       lw.finish();
@@ -941,11 +966,12 @@ const Occupancy& occupancy() {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&r.sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaFuncSetAttribute(k_density_tiled<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDensitySmem);
-    cudaFuncSetAttribute(k_density_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDensitySmem);
+    for (auto f : {k_density_tiled<false, true>, k_density_tiled<true, true>, k_density_tiled<false, false>,
+                   k_density_tiled<true, false>})
+      cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDensitySmem);
     cudaFuncSetAttribute(k_force_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kForceSmem);
     int bd = 0, bf = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bd, k_density_tiled<false>, kTT, kDensitySmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bd, k_density_tiled<false, true>, kTT, kDensitySmem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force_tiled, kTT, kForceSmem);
     int dd = 0, df = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dd, k_density_dense<false>, kDT, 0);
@@ -1017,13 +1043,14 @@ void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const
   // sort's gather; the "prep" phase of a tiled step is empty.
   if (ev.after_prep) cudaEventRecord(ev.after_prep, s);
   const int dense_d_blocks = o.sms * o.dense_density, dense_f_blocks = o.sms * o.dense_force;
-  if (a.counters) {
-    k_density_tiled<true><<<density_blocks, kTT, kDensitySmem, s>>>(c, a);
+  const bool exact = std::min(c.h2f, c.h0sqf) == c.h0sqf;
+  auto density = a.counters ? (exact ? k_density_tiled<true, true> : k_density_tiled<true, false>)
+                            : (exact ? k_density_tiled<false, true> : k_density_tiled<false, false>);
+  density<<<density_blocks, kTT, kDensitySmem, s>>>(c, a);
+  if (a.counters)
     k_density_dense<true><<<dense_d_blocks, kDT, 0, s>>>(c, a);
-  } else {
-    k_density_tiled<false><<<density_blocks, kTT, kDensitySmem, s>>>(c, a);
+  else
     k_density_dense<false><<<dense_d_blocks, kDT, 0, s>>>(c, a);
-  }
   if (ev.after_density) cudaEventRecord(ev.after_density, s);
   k_force_tiled<<<force_blocks, kTT, kForceSmem, s>>>(c, a);
   k_force_dense<<<dense_f_blocks, kDT, 0, s>>>(c, a);

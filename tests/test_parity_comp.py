@@ -135,6 +135,34 @@ def test_kernel_routes_agree(gpu, oracle_mod, tile, halo_cap):
     assert np.isfinite(w.pos).all() and (w.pos >= 0).all() and (w.pos <= 3.2).all()
 
 
+@pytest.mark.parametrize("tile", [4, 0])
+def test_comp_live_h_change(gpu, oracle_mod, tile):
+    """A live params.h below the construction h (the cutoff trims the kernel support) and
+    above it (the cutoff stays the kernel radius): the compensated routes meet the density
+    gate against the oracle under the same params, teacher-forced from the oracle's state."""
+    O = oracle_mod
+    sc = scenes.dam_break(14, 20, 14, box=3.2, dt=0.005, steps=0)
+    p = _params(sc)
+    ow = O.OracleWorld(p, threads=O.max_threads())
+    ow.add_particles(sc.pos, sc.mass)
+    ow.step(0.005, 60)
+    w = gpu.FluidWorld(p, "comp")
+    w.set_tuning(comp_tile=tile)
+    w.add_particles(ow.get(O.F_POS), ow.get(O.F_MASS), vel=ow.get(O.F_VEL))
+    for h in (0.17, 0.26):
+        p2 = _params(sc)
+        p2.h = h
+        ow.set_params(p2)
+        w.params = p2
+        w.pos = ow.get(O.F_POS)
+        w.vel = ow.get(O.F_VEL)
+        ow.step(0.005)
+        w.step(0.005)
+        e = errors(w, O, ow, p2)
+        print("live h", tile, h, e)
+        assert e["rho_rel"] <= RHO_TOL and e["acc_rel_to_max"] <= 1e-3, e
+
+
 def test_tiled_sparse_and_out_of_bounds_particles(gpu, oracle_mod):
     """Tiles with a single particle, particles starting outside bounds, and a NaN
     particle (its cell key is 0 on the NaN axis): the tiled form still meets the
