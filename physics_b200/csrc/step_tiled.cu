@@ -322,23 +322,28 @@ __device__ __forceinline__ uint32_t filter_chunk(const float4* s_pp4, uint32_t c
 }
 
 // Appends 16-bit neighbour slots to a particle's row-major list (row of
-// kMaxNeighbors entries) through a 64-bit register accumulator flushed with
-// 8-byte stores; entries past kMaxNeighbors are dropped (the count still
-// grows and the force pass then rescans).
+// kMaxNeighbors entries) through a 64-bit register accumulator (hi:lo) that
+// shifts each new slot in from the top, so four pushes leave the oldest slot
+// in the low 16 bits; flushed with 8-byte stores.  Entries past
+// kMaxNeighbors are dropped (the count still grows and the force pass then
+// rescans).
 struct ListWriter {
   uint16_t* row;
-  unsigned long long acc = 0;
+  uint32_t lo = 0, hi = 0;
   uint32_t n = 0;
   __device__ __forceinline__ void push(uint32_t slot) {
-    acc |= (unsigned long long)slot << (16 * (n & 3));
+    lo = __funnelshift_r(lo, hi, 16);    // low word of (hi:lo) >> 16
+    hi = __byte_perm(hi, slot, 0x5432);  // (hi >> 16) | (slot << 16)
     ++n;
-    if ((n & 3) == 0) {
-      if (n <= (uint32_t)kMaxNeighbors) *reinterpret_cast<unsigned long long*>(row + n - 4) = acc;
-      acc = 0;
-    }
+    if ((n & 3) == 0 && n <= (uint32_t)kMaxNeighbors)
+      *reinterpret_cast<uint2*>(row + n - 4) = make_uint2(lo, hi);
   }
   __device__ __forceinline__ void finish() {
-    if ((n & 3) && n < (uint32_t)kMaxNeighbors) *reinterpret_cast<unsigned long long*>(row + (n & ~3u)) = acc;
+    const uint32_t r = n & 3;  // pending slots, in the top r * 16 bits
+    if (r && n < (uint32_t)kMaxNeighbors) {
+      const unsigned long long v = (((unsigned long long)hi << 32) | lo) >> (16 * (4 - r));
+      *reinterpret_cast<unsigned long long*>(row + (n & ~3u)) = v;
+    }
   }
 };
 
