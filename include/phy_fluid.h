@@ -123,6 +123,18 @@ int32_t phy_fluid_step(PhyWorldHandle *w, uint32_t sub, double dt, uint32_t n);
  * out4 = {Px, Py, Pz, KE}, summed in insertion order in f64. */
 int32_t phy_fluid_diagnostics(PhyWorldHandle *w, uint32_t sub, double *out4);
 
+/* FluidWorld::couple_points (crates/phy-fluid/src/sph/world.rs:691-752, with
+ * CouplePoint of sph/couple.rs): two-way coupling of n point masses with the
+ * fluid of subsystem `sub`, computed on the device and bit-identical to the
+ * reference.  pos, vel: 3n doubles (xyz per point, read only); mass: n;
+ * force: 3n doubles, written for the points inside the bounds (the others
+ * keep their values).  Points are taken in order: each samples the
+ * mass-weighted fluid velocity of its 27 grid cells and shares -force*dt
+ * among those particles by mass before the next point.  Fails (-1) on a
+ * world of batched scenes or while the adjoint tape records. */
+int32_t phy_fluid_couple_points(PhyWorldHandle *w, uint32_t sub, uint64_t n, const double *pos, const double *vel,
+                                const double *mass, double *force, double dt, double drag, double soft_density);
+
 /* FluidSubsystem coupling coefficients (subsystem.rs:26-55):
  * {thermal_expansion, heat_gain, t_ref, drag, friction}. */
 int32_t phy_fluid_get_coupling(PhyWorldHandle *w, uint32_t sub, double *out5);

@@ -71,6 +71,9 @@ def load():
             "orc_diagnostics": (None, [C.c_void_p, DP]),
             "orc_counters": (None, [C.c_void_p, C.POINTER(C.c_uint64), C.c_int]),
             "orc_jvp": (None, [C.c_void_p, C.c_double, C.c_int, DP, DP, C.c_double, C.c_double]),
+            "orc_point_neighbors": (C.c_uint64, [C.c_void_p, DP, C.POINTER(C.c_uint64), C.c_uint64]),
+            "orc_couple_points": (None, [C.c_void_p, C.c_uint64, DP, DP, DP, DP, C.c_double, C.c_double,
+                                          C.c_double]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -185,6 +188,25 @@ class OracleWorld:
         out = np.empty(4, np.float64)
         self._lib.orc_diagnostics(self._w, out.ctypes.data_as(DP))
         return out
+
+    def neighbors_of_point(self, p3, cap: int = 65536) -> np.ndarray:
+        """Indices for_each_neighbor visits for point p3 (grid of the current positions)."""
+        q = np.ascontiguousarray(p3, np.float64).reshape(3)
+        out = np.empty(cap, np.uint64)
+        n = self._lib.orc_point_neighbors(self._w, q.ctypes.data_as(DP), out.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                          cap)
+        return out[: min(n, cap)].astype(np.int64)
+
+    def couple_points(self, pos, vel, mass, dt: float, drag: float, soft_density: float, force=None):
+        """FluidWorld::couple_points (world.rs:691-752): returns the (n, 3) forces; rows of
+        points outside the bounds keep the values of `force` (zeros when None)."""
+        pos = np.ascontiguousarray(pos, np.float64).reshape(-1)
+        vel = np.ascontiguousarray(vel, np.float64).reshape(-1)
+        mass = np.ascontiguousarray(mass, np.float64).reshape(-1)
+        out = np.zeros(pos.size, np.float64) if force is None else np.array(force, np.float64).reshape(-1)
+        self._lib.orc_couple_points(self._w, mass.size, pos.ctypes.data_as(DP), vel.ctypes.data_as(DP),
+                                    mass.ctypes.data_as(DP), out.ctypes.data_as(DP), dt, drag, soft_density)
+        return out.reshape(-1, 3)
 
     def counters(self, reset: bool = True) -> tuple:
         out = (C.c_uint64 * 2)()

@@ -359,6 +359,52 @@ struct World {
       pt.vel = {v[0], v[1], v[2]};
     }
   }
+
+  // world.rs:691-752: point masses (pos, vel, mass in; force out) coupled to
+  // the fluid one after another.  A point outside the bounds is skipped and
+  // its force left as it was; each point's reaction -f*dt is shared among the
+  // fluid particles of its 27 cells by mass, and the next point samples the
+  // updated velocities.
+  void couple_points(size_t np, const V3* ppos, const V3* pvel, const double* pmass, V3* pforce, double dt,
+                     double drag, double soft_density) {
+    if (np == 0 || particles.empty()) return;
+    const double rho_f = params.rest_density;
+    const V3 g{params.gravity[0], params.gravity[1], params.gravity[2]};
+    const double* lo = params.bounds_min;
+    const double* hi = params.bounds_max;
+    grid.build(particles);
+    std::vector<size_t> idxs;
+    for (size_t k = 0; k < np; ++k) {
+      const V3 p = ppos[k];
+      if (p.x < lo[0] || p.x > hi[0] || p.y < lo[1] || p.y > hi[1] || p.z < lo[2] || p.z > hi[2]) continue;
+      V3 v_sum{0, 0, 0};
+      double w_sum = 0.0;
+      grid.for_each_neighbor(p, [&](size_t j) {
+        const double w = particles[j].mass;
+        v_sum += particles[j].vel * w;
+        w_sum = w_sum + w;
+      });
+      const V3 v_f = w_sum > 0.0 ? v_sum / w_sum : V3{0, 0, 0};
+      const double vol = soft_density > 0.0 ? pmass[k] / soft_density : 0.0;
+      const V3 f_b = V3{-g.x, -g.y, -g.z} * (rho_f * vol);
+      const V3 f_d = (v_f - pvel[k]) * (drag * pmass[k]);
+      const V3 f = f_b + f_d;
+      pforce[k] = f;
+      double m_sum = 0.0;
+      idxs.clear();
+      grid.for_each_neighbor(p, [&](size_t j) {
+        m_sum = m_sum + particles[j].mass;
+        idxs.push_back(j);
+      });
+      if (m_sum > 0.0) {
+        const V3 reaction = V3{-f.x, -f.y, -f.z} * dt;
+        for (size_t j : idxs) {
+          const double frac = particles[j].mass / m_sum;
+          particles[j].vel += reaction * frac;
+        }
+      }
+    }
+  }
 };
 
 // Forward-mode derivative (JVP) of one step, for checking the product's
@@ -639,6 +685,39 @@ uint64_t orc_neighbors(void* w, uint64_t i, uint64_t* out, uint64_t cap) {
   W->grid.build(W->particles);
   uint64_t cnt = 0;
   W->grid.for_each_neighbor(W->particles[i].pos, [&](size_t j) {
+    if (cnt < cap) out[cnt] = j;
+    ++cnt;
+  });
+  return cnt;
+}
+
+// FluidWorld::couple_points (world.rs:691-752) on np points: pos, vel,
+// force are 3*np doubles (xyz interleaved), mass np doubles; force is written
+// for the points inside the bounds only.
+void orc_couple_points(void* w, uint64_t np, const double* pos, const double* vel, const double* mass,
+                       double* force, double dt, double drag, double soft_density) {
+  World* W = static_cast<World*>(w);
+  std::vector<V3> p(np), v(np), f(np);
+  for (uint64_t k = 0; k < np; ++k) {
+    p[k] = {pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]};
+    v[k] = {vel[3 * k], vel[3 * k + 1], vel[3 * k + 2]};
+    f[k] = {force[3 * k], force[3 * k + 1], force[3 * k + 2]};
+  }
+  W->couple_points((size_t)np, p.data(), v.data(), mass, f.data(), dt, drag, soft_density);
+  for (uint64_t k = 0; k < np; ++k) {
+    force[3 * k] = f[k].x;
+    force[3 * k + 1] = f[k].y;
+    force[3 * k + 2] = f[k].z;
+  }
+}
+
+// for_each_neighbor of an arbitrary point (xyz) over a grid of the current
+// positions: the particles couple_points visits for it, in visit order.
+uint64_t orc_point_neighbors(void* w, const double* p3, uint64_t* out, uint64_t cap) {
+  World* W = static_cast<World*>(w);
+  W->grid.build(W->particles);
+  uint64_t cnt = 0;
+  W->grid.for_each_neighbor(V3{p3[0], p3[1], p3[2]}, [&](size_t j) {
     if (cnt < cap) out[cnt] = j;
     ++cnt;
   });

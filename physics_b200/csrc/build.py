@@ -33,9 +33,10 @@ PER_FILE = {
     "noalloc.cu": ["-fmad=false"],
     "grid.cu": ["-fmad=false"],
     "fluid_world.cu": ["-fmad=false"],
+    "couple.cu": ["-fmad=false"],
 }
 SOURCES = ["grid.cu", "step_plain.cu", "step_comp.cu", "step_tiled.cu", "fluid_world.cu", "ffi.cpp",
-           "checkpoint.cpp", "noalloc.cu", "adjoint.cu"]
+           "checkpoint.cpp", "noalloc.cu", "adjoint.cu", "couple.cu"]
 
 
 def _nvcc() -> str:

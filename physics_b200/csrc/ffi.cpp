@@ -316,6 +316,15 @@ int32_t phy_fluid_diagnostics(PhyWorldHandle* w, uint32_t sub, double* out4) {
   });
 }
 
+int32_t phy_fluid_couple_points(PhyWorldHandle* w, uint32_t sub, uint64_t n, const double* pos, const double* vel,
+                                const double* mass, double* force, double dt, double drag, double soft_density) {
+  if (n > 0 && (!pos || !vel || !mass || !force)) return -1;
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->couple_points((size_t)n, pos, vel, mass, force, dt, drag, soft_density);
+    return 0;
+  });
+}
+
 int32_t phy_fluid_get_coupling(PhyWorldHandle* w, uint32_t sub, double* out5) {
   if (!out5) return -1;
   return guard<int32_t>(-1, [&] {

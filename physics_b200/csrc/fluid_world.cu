@@ -344,6 +344,7 @@ FluidWorld::~FluidWorld() {
   drop_graphs();
   free_all();
   dfree(d_bbox_);
+  dfree(d_couple_);
   dfree(d_pbase_);
   dfree(d_scene_bbox_);
   release_snapshot();
@@ -1344,6 +1345,46 @@ void FluidWorld::diagnostics(double* out4) {
   out4[1] = py;
   out4[2] = pz;
   out4[3] = e;
+}
+
+// world.rs:691-752 (kernel and semantics in couple.cu).  The cell index of the
+// current positions is built without moving the state, so the step's sorted
+// arrays and outputs stay as they were; only fluid velocities change.
+void FluidWorld::couple_points(size_t np, const double* pos, const double* vel, const double* mass, double* force,
+                               double dt, double drag, double soft_density) {
+  if (np == 0 || n_ == 0) return;  // world.rs:692-694
+  if (!pos || !vel || !mass || !force) throw std::invalid_argument("couple_points: null array");
+  if (!scenes_.empty()) throw std::invalid_argument("couple_points: not available for batched scenes");
+  if (tape_.on) throw std::invalid_argument("couple_points: the adjoint tape does not record coupling");
+  if (np > ((size_t)1 << 24)) throw std::invalid_argument("couple_points: more than 2^24 points");
+  ensure_cells();
+  StepConsts c = make_consts(dt);
+  c.tile = 0;  // x-major cells for the index
+  c.tile_log2 = 0;
+  const size_t need = 10 * np + 1;
+  if (couple_cap_ < need) {
+    dalloc(d_couple_, need);
+    couple_cap_ = need;
+  }
+  std::vector<double> h(10 * np);
+  for (size_t k = 0; k < np; ++k) {
+    double* r = h.data() + 10 * k;
+    for (int a = 0; a < 3; ++a) {
+      r[a] = pos[3 * k + a];
+      r[3 + a] = vel[3 * k + a];
+      r[7 + a] = force[3 * k + a];
+    }
+    r[6] = mass[k];
+  }
+  const size_t bytes = h.size() * sizeof(double);
+  cuda_check(cudaMemcpyAsync(d_couple_, h.data(), bytes, cudaMemcpyHostToDevice, stream_), "couple upload");
+  launch_cell_index(c, b_, reinterpret_cast<uint32_t*>(d_couple_ + 10 * np), stream_);
+  launch_couple_points(c, b_, d_couple_, (int)np, dt, drag, soft_density, stream_);
+  cuda_check(cudaGetLastError(), "couple launch");
+  cuda_check(cudaMemcpyAsync(h.data(), d_couple_, bytes, cudaMemcpyDeviceToHost, stream_), "couple download");
+  cuda_check(cudaStreamSynchronize(stream_), "couple sync");
+  for (size_t k = 0; k < np; ++k)
+    for (int a = 0; a < 3; ++a) force[3 * k + a] = h[10 * k + 7 + a];
 }
 
 // ---- FluidSubsystem / World ------------------------------------------------

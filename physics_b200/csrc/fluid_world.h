@@ -135,6 +135,14 @@ class FluidWorld {
   void last_step_counters(uint64_t* out2);
   int grid_cells() const { return ncells_; }
 
+  // FluidWorld::couple_points (world.rs:691-752) on the device, bit-exact:
+  // np point masses (pos, vel: xyz interleaved; mass) coupled one after
+  // another; force (xyz interleaved) is written for the points inside the
+  // bounds and the fluid velocities take the reactions.  Not available for
+  // batched scenes or while the adjoint tape records.
+  void couple_points(size_t np, const double* pos, const double* vel, const double* mass, double* force,
+                     double dt, double drag, double soft_density);
+
   // Total momentum and kinetic energy (subsystem.rs:149-163), f64, insertion order.
   void diagnostics(double* out4);
 
@@ -202,6 +210,9 @@ class FluidWorld {
   double phase_ms_[4] = {0, 0, 0, 0};
   double timed_steps_ = 0;
   long long* d_bbox_ = nullptr;  // 7 values: min xyz, max xyz, non-finite flag
+  // Point records of couple_points (10 doubles each) plus one word of flags.
+  double* d_couple_ = nullptr;
+  size_t couple_cap_ = 0;
 
   // Batched scenes.
   struct Scene {

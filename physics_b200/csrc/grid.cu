@@ -373,24 +373,36 @@ static int scan_length(int ncells) { return ((ncells + 2 + kScanTile - 1) / kSca
 size_t scan_block_sums_needed(int ncells) { return (size_t)scan_length(ncells) / kScanTile; }
 size_t tile_head_length(int n) { return (size_t)((n + 1 + kScanTile - 1) / kScanTile) * kScanTile; }
 
-void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s, int block) {
-  // Per-particle kernels take any warp multiple up to kThreads.
-  const int bs = block >= 32 && block <= kThreads ? block / 32 * 32 : kThreads;
+// Cells of the current positions (pv1): cell_start over the box and perm[s]
+// = the particle (index into the current arrays) at sorted slot s, ordered
+// by (cell, okey) when okey is given, else by (cell, insertion index).
+static void build_cells(const StepConsts& c, DevBuffers& b, cudaStream_t s, int bs, unsigned long long* okey,
+                        uint32_t* flags) {
   const int n = c.n;
   const int len = scan_length(c.ncells);
   const int nb = len / kScanTile;
+  const ParticleConsts& src = b.pc[b.cur];
   cudaMemsetAsync(b.cell_start, 0, (size_t)len * sizeof(uint32_t), s);
   k_cell_hist<<<grid_for(n, bs), bs, 0, s>>>(c, b.pv1[0], b.pv1[1], b.pv1[2], b.cell_of, b.rank,
-                                               b.cell_start, b.flags, b.pc[b.cur].scene, b.pc[b.cur].id,
-                                               c.tile ? b.okey : nullptr);
+                                               b.cell_start, flags, src.scene, src.id, okey);
   k_scan_reduce<<<nb, kThreads, 0, s>>>(b.cell_start, b.block_sums);
   k_scan_top<<<1, 1024, 0, s>>>(b.block_sums, nb);
   k_scan_apply<<<nb, kThreads, 0, s>>>(b.cell_start, b.block_sums);
   k_scatter<<<grid_for(n, bs), bs, 0, s>>>(n, b.cell_of, b.rank, b.cell_start, b.tmp);
+  k_order<<<grid_for(n, bs), bs, 0, s>>>(n, c.ncells, b.cell_of, b.cell_start, b.tmp, src.id, okey, b.perm);
+}
+
+void launch_cell_index(const StepConsts& c, DevBuffers& b, uint32_t* flags, cudaStream_t s) {
+  build_cells(c, b, s, kThreads, nullptr, flags);
+}
+
+void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s, int block) {
+  // Per-particle kernels take any warp multiple up to kThreads.
+  const int bs = block >= 32 && block <= kThreads ? block / 32 * 32 : kThreads;
+  const int n = c.n;
+  build_cells(c, b, s, bs, c.tile ? b.okey : nullptr, b.flags);
   const ParticleConsts& src = b.pc[b.cur];
   const ParticleConsts& dst = b.pc[b.cur ^ 1];
-  k_order<<<grid_for(n, bs), bs, 0, s>>>(n, c.ncells, b.cell_of, b.cell_start, b.tmp, src.id,
-                                         c.tile ? b.okey : nullptr, b.perm);
   GatherArgs g;
   for (int k = 0; k < 6; ++k) {
     g.src_pv[k] = b.pv1[k];

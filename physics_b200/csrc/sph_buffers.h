@@ -88,6 +88,17 @@ struct DevBuffers {
 
 // grid.cu
 void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s, int block = 256);
+// The cells of the current positions without moving the state: cell_start
+// over the box and perm[s] = the particle at sorted slot s in (cell,
+// insertion index) order.  c.tile must be 0 (x-major cells).  The
+// out-of-box bit goes to `flags` (not the step's error bits).
+void launch_cell_index(const StepConsts& c, DevBuffers& b, uint32_t* flags, cudaStream_t s);
+
+// couple.cu: FluidWorld::couple_points over np points (10 doubles each on the
+// device: pos xyz, vel xyz, mass, force xyz) after launch_cell_index; updates
+// the fluid velocities in pv1 and the forces of the points inside the bounds.
+void launch_couple_points(const StepConsts& c, DevBuffers& b, double* d_pts, int np, double dt, double drag,
+                          double soft_density, cudaStream_t s);
 void launch_unsort_f64(const DevBuffers& b, int n, const double* src_sorted, double* dst_orig,
                        cudaStream_t s);
 void launch_unsort_u32(const DevBuffers& b, int n, const uint32_t* src_sorted, double* dst_orig,

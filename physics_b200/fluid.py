@@ -405,6 +405,21 @@ class FluidWorld:
                 "phy_fluid_phase_times")
         return {"sort": out[0], "prep": out[1], "density": out[2], "force": out[3], "steps": int(out[4])}
 
+    # ---- coupling (world.rs:691-752) ------------------------------------------------
+    def couple_points(self, pos, vel, mass, dt: float, drag: float, soft_density: float, force=None) -> np.ndarray:
+        """FluidWorld::couple_points on the device: returns the (n, 3) forces on the points;
+        rows of points outside the bounds keep the values of `force` (zeros when None).
+        The fluid velocities take the reactions."""
+        pos = np.ascontiguousarray(pos, np.float64).reshape(-1)
+        vel = np.ascontiguousarray(vel, np.float64).reshape(-1)
+        mass = np.ascontiguousarray(mass, np.float64).reshape(-1)
+        if pos.size != 3 * mass.size or vel.size != pos.size:
+            raise ValueError("couple_points: pos and vel need 3 values per mass")
+        out = np.zeros(pos.size, np.float64) if force is None else np.array(force, np.float64).reshape(-1)
+        L.check(self._lib.phy_fluid_couple_points(self._h, self._sub, mass.size, _dp(pos), _dp(vel), _dp(mass),
+                                                  _dp(out), dt, drag, soft_density), "phy_fluid_couple_points")
+        return out.reshape(-1, 3)
+
     # ---- diagnostics (FluidSubsystem, subsystem.rs:149-163) ------------------------
     def _diag(self) -> np.ndarray:
         out = np.empty(4, np.float64)

@@ -1,0 +1,111 @@
+"""FluidWorld::couple_points on the device (phy_fluid_couple_points) against the oracle's
+restatement of phy-fluid/src/sph/world.rs:691-752, bit for bit: forces on the points and
+the fluid velocities that take the reactions, points processed in order, skipped points
+left untouched, and the step that follows the coupling."""
+import numpy as np
+import pytest
+
+from helpers import assert_bits_equal, ref_test_params
+
+pytestmark = pytest.mark.gpu
+
+DT = 0.0025
+
+
+def _pair(gpu, O, prec="f64", lo=-0.5, hi=0.5, spacing=0.1, steps=15):
+    """A fluid block (sph/tests.rs:181-192 for the defaults) on the device and in the
+    oracle; a compensated world's state is copied into the oracle (teacher forcing)."""
+    p = ref_test_params(gravity=(0.0, -9.81, 0.0))
+    w = gpu.FluidWorld(p, prec)
+    w.fill_box((lo,) * 3, (hi,) * 3, spacing, spacing / 2)
+    ow = O.OracleWorld(p)
+    ow.fill_box((lo,) * 3, (hi,) * 3, spacing, spacing / 2)
+    w.step(DT, steps)
+    if prec == "f64":
+        ow.step(DT, steps)
+    else:
+        ow.set(O.F_POS, w.pos)
+        ow.set(O.F_VEL, w.vel)
+    return w, ow, p
+
+
+def _points(n_random=0, seed=3):
+    pts = [[0.0, 0.0, 0.0], [0.03, 0.0, 0.0], [2.0, 2.0, 2.0], [3.5, 0.0, 0.0], [0.1, -0.3, 0.2],
+           [-0.45, 0.4, 0.45], [0.0, -3.0 - 1e-9, 0.0]]
+    rng = np.random.default_rng(seed)
+    pts = np.concatenate([np.array(pts), rng.uniform(-0.6, 0.6, (n_random, 3))])
+    vel = rng.normal(0.0, 0.3, pts.shape)
+    mass = rng.uniform(0.005, 0.05, len(pts))
+    prior = rng.normal(0.0, 1.0, pts.shape)
+    return pts, vel, mass, prior
+
+
+def _check(O, w, ow, pts, vel, mass, prior, drag=1.5, soft=900.0):
+    fg = w.couple_points(pts, vel, mass, DT, drag, soft, force=prior)
+    fo = ow.couple_points(pts, vel, mass, DT, drag, soft, force=prior)
+    assert_bits_equal(fg, fo, "forces")
+    assert_bits_equal(fg[[3, 6]], prior[[3, 6]], "points outside the bounds")
+    assert_bits_equal(w.vel, ow.get(O.F_VEL), "fluid velocities")
+    assert_bits_equal(w.pos, ow.get(O.F_POS), "fluid positions unchanged")
+
+
+def test_couple_points_f64_bitwise_and_next_steps(gpu, oracle_mod):
+    O = oracle_mod
+    w, ow, _ = _pair(gpu, O)
+    pts, vel, mass, prior = _points(n_random=120)
+    _check(O, w, ow, pts, vel, mass, prior)
+    w.step(DT, 5)
+    ow.step(DT, 5)
+    assert_bits_equal(w.pos, ow.get(O.F_POS), "positions after coupling and 5 steps")
+    assert_bits_equal(w.vel, ow.get(O.F_VEL), "velocities after coupling and 5 steps")
+    assert_bits_equal(w.rho, ow.get(O.F_RHO), "densities after coupling and 5 steps")
+
+
+def test_couple_points_on_tiled_compensated_world(gpu, oracle_mod):
+    """The coupling is f64 on any kernel form: on the staged-tile compensated world it
+    equals the oracle's coupling of the same state, and the world keeps stepping."""
+    O = oracle_mod
+    w, ow, _ = _pair(gpu, O, prec="comp", steps=20)
+    rho = w.rho.copy()
+    pts, vel, mass, prior = _points(n_random=40, seed=5)
+    _check(O, w, ow, pts, vel, mass, prior, drag=0.7, soft=1000.0)
+    assert_bits_equal(w.rho, rho, "step outputs untouched")
+    w.step(DT, 10)
+    assert np.isfinite(w.pos).all()
+
+
+def test_couple_points_dense_neighbourhood(gpu, oracle_mod):
+    """Points whose 27 cells hold more than the 1024 candidates staged at a time."""
+    O = oracle_mod
+    w, ow, _ = _pair(gpu, O, lo=-0.3, hi=0.3, spacing=0.04, steps=2)
+    assert len(ow.neighbors_of_point([0.0, 0.0, 0.0])) > 1024
+    pts, vel, mass, prior = _points(n_random=10, seed=7)
+    _check(O, w, ow, pts, vel, mass, prior)
+
+
+def test_couple_points_buoyancy_upward(gpu):
+    """couple_points_buoyancy_upward (sph/tests.rs:179-212) on the device."""
+    p = ref_test_params(gravity=(0.0, -9.81, 0.0))
+    w = gpu.FluidWorld(p)
+    w.fill_box((-0.5,) * 3, (0.5,) * 3, 0.1, 0.05)
+    w.step(DT, 15)
+    before = w.total_momentum()
+    f = w.couple_points([[0.0, 0.0, 0.0]], [[0.0, 0.0, 0.0]], [0.02], DT, 1.0, p.rest_density)
+    assert f[0, 1] > 0.0
+    assert (w.total_momentum() - before)[1] < 0.0
+
+
+def test_couple_points_rejected_configurations(gpu):
+    p = ref_test_params()
+    w = gpu.FluidWorld(p)
+    w.fill_box((-0.5,) * 3, (0.5,) * 3, 0.1, 0.05)
+    w.tape_begin(5)
+    with pytest.raises(gpu.PhyError):
+        w.couple_points([[0.0, 0.0, 0.0]], [[0.0, 0.0, 0.0]], [0.02], DT, 1.0, 1000.0)
+    w.tape_clear()
+    w.couple_points(np.zeros((0, 3)), np.zeros((0, 3)), np.zeros(0), DT, 1.0, 1000.0)  # no points: no-op
+    b = gpu.FluidWorld(p, "comp")
+    b.add_particles([[0.1, 0.1, 0.1], [0.2, 0.2, 0.2]], 0.02)
+    b.set_scenes([1, 1], [(0, 0, 0)] * 2, [(1, 1, 1)] * 2)
+    with pytest.raises(gpu.PhyError):
+        b.couple_points([[0.5, 0.5, 0.5]], [[0.0, 0.0, 0.0]], [0.02], DT, 1.0, 1000.0)
