@@ -135,6 +135,23 @@ int32_t phy_fluid_diagnostics(PhyWorldHandle *w, uint32_t sub, double *out4);
 int32_t phy_fluid_couple_points(PhyWorldHandle *w, uint32_t sub, uint64_t n, const double *pos, const double *vel,
                                 const double *mass, double *force, double dt, double drag, double soft_density);
 
+/* FluidWorld::couple_heat (crates/phy-fluid/src/sph/world.rs:555-678; the
+ * HeatFieldLike grid of phy-field heat.rs:15-33, grid.rs:80-82, 125-130,
+ * 203-208): thermal buoyancy and advective heating between the fluid of
+ * subsystem `sub` and a heat grid, computed on the device and bit-identical
+ * to the reference.  The grid has dims3[0] x dims3[1] x dims3[2] cells of
+ * size `cell` from origin3, values x fastest.  Every particle inside the
+ * bounds gets body_acc += -g * beta * (T - t_ref), T its trilinear grid
+ * temperature (t_ref outside the grid); with heat_gain > 0 the sources `src`
+ * (same layout, updated in place; may be NULL otherwise) take
+ * heat_gain * |v| * dt per particle, added in insertion order.  The velocity
+ * sampler the reference installs into the field is left to the caller (it
+ * captures the positions and velocities phy_fluid_get_field returns).  Fails
+ * (-1) on a world of batched scenes or while the adjoint tape records. */
+int32_t phy_fluid_couple_heat(PhyWorldHandle *w, uint32_t sub, const uint64_t *dims3, const double *origin3,
+                              double cell, const double *temp, double *src, double dt, double t_ref, double beta,
+                              double heat_gain);
+
 /* FluidSubsystem coupling coefficients (subsystem.rs:26-55):
  * {thermal_expansion, heat_gain, t_ref, drag, friction}. */
 int32_t phy_fluid_get_coupling(PhyWorldHandle *w, uint32_t sub, double *out5);

@@ -72,6 +72,8 @@ def load():
             "orc_counters": (None, [C.c_void_p, C.POINTER(C.c_uint64), C.c_int]),
             "orc_jvp": (None, [C.c_void_p, C.c_double, C.c_int, DP, DP, C.c_double, C.c_double]),
             "orc_point_neighbors": (C.c_uint64, [C.c_void_p, DP, C.POINTER(C.c_uint64), C.c_uint64]),
+            "orc_couple_heat": (None, [C.c_void_p, C.POINTER(C.c_uint64), DP, C.c_double, DP, DP, C.c_double,
+                                        C.c_double, C.c_double, C.c_double]),
             "orc_couple_points": (None, [C.c_void_p, C.c_uint64, DP, DP, DP, DP, C.c_double, C.c_double,
                                           C.c_double]),
         }
@@ -196,6 +198,19 @@ class OracleWorld:
         n = self._lib.orc_point_neighbors(self._w, q.ctypes.data_as(DP), out.ctypes.data_as(C.POINTER(C.c_uint64)),
                                           cap)
         return out[: min(n, cap)].astype(np.int64)
+
+    def couple_heat(self, temp, src, origin, cell: float, dt: float, t_ref: float, beta: float,
+                    heat_gain: float) -> np.ndarray:
+        """FluidWorld::couple_heat (world.rs:555-678): temp is the (nz, ny, nx) grid of
+        temperatures (x fastest in memory); returns the updated copy of src.  The particles'
+        body accelerations take the buoyancy terms."""
+        temp = np.ascontiguousarray(temp, np.float64)
+        out = np.array(src, np.float64, copy=True, order="C")
+        dims = (C.c_uint64 * 3)(temp.shape[2], temp.shape[1], temp.shape[0])
+        o = np.ascontiguousarray(origin, np.float64).reshape(3)
+        self._lib.orc_couple_heat(self._w, dims, o.ctypes.data_as(DP), cell, temp.ctypes.data_as(DP),
+                                  out.ctypes.data_as(DP), dt, t_ref, beta, heat_gain)
+        return out
 
     def couple_points(self, pos, vel, mass, dt: float, drag: float, soft_density: float, force=None):
         """FluidWorld::couple_points (world.rs:691-752): returns the (n, 3) forces; rows of

@@ -360,6 +360,86 @@ struct World {
     }
   }
 
+  // world.rs:555-678 against a heat grid (HeatFieldLike of phy-field):
+  // trilinear temperature -> body_acc += -g * beta * (T - t_ref) for the
+  // particles inside the bounds, and heat_gain * |v| * dt added to the
+  // source of the particle's cell, particle after particle.  (The reference
+  // also installs a velocity sampler closure into the field; that part
+  // belongs to the field's own step.)
+  struct HeatGrid {
+    uint64_t nx, ny, nz;
+    V3 origin;
+    double dx;
+    const double* u;
+    double* src;
+    uint64_t idx(uint64_t x, uint64_t y, uint64_t z) const { return x + nx * (y + ny * z); }  // grid.rs:80-82
+    double sample(uint64_t x, uint64_t y, uint64_t z) const {  // grid.rs:203-208
+      return u[idx(x < nx - 1 ? x : nx - 1, y < ny - 1 ? y : ny - 1, z < nz - 1 ? z : nz - 1)];
+    }
+    double sample_trilinear(uint64_t cx, uint64_t cy, uint64_t cz, double fx, double fy, double fz) const {
+      // heat.rs:130-171
+      const uint64_t x1 = cx + 1 < nx - 1 ? cx + 1 : nx - 1, y1 = cy + 1 < ny - 1 ? cy + 1 : ny - 1,
+                     z1 = cz + 1 < nz - 1 ? cz + 1 : nz - 1;
+      const double c000 = sample(cx, cy, cz), c100 = sample(x1, cy, cz), c010 = sample(cx, y1, cz),
+                   c110 = sample(x1, y1, cz), c001 = sample(cx, cy, z1), c101 = sample(x1, cy, z1),
+                   c011 = sample(cx, y1, z1), c111 = sample(x1, y1, z1);
+      const double x00 = c000 + (c100 - c000) * fx;
+      const double x10 = c010 + (c110 - c010) * fx;
+      const double x01 = c001 + (c101 - c001) * fx;
+      const double x11 = c011 + (c111 - c011) * fx;
+      const double y0 = x00 + (x10 - x00) * fy;
+      const double y1v = x01 + (x11 - x01) * fy;
+      return y0 + (y1v - y0) * fz;
+    }
+    void add_source(uint64_t x, uint64_t y, uint64_t z, double v) {  // grid.rs:125-130
+      if (x < nx && y < ny && z < nz) src[idx(x, y, z)] = src[idx(x, y, z)] + v;
+    }
+  };
+
+  // num-traits ToPrimitive::to_usize of an f64 with None -> 0.
+  static uint64_t to_usize_or_zero(double f) {
+    return (f > -1.0 && f < 18446744073709551616.0) ? (uint64_t)f : 0;
+  }
+
+  void couple_heat(HeatGrid& heat, double dt, double t_ref, double beta, double heat_gain) {
+    if (particles.empty()) return;
+    const V3 g{params.gravity[0], params.gravity[1], params.gravity[2]};
+    const double* lo = params.bounds_min;
+    const double* hi = params.bounds_max;
+    const V3 hmin = heat.origin;
+    const double dx = heat.dx;
+    // dims.saturating_sub(1) as T
+    const double nxm1 = heat.nx > 0 ? (double)(heat.nx - 1) : 0.0, nym1 = heat.ny > 0 ? (double)(heat.ny - 1) : 0.0,
+                 nzm1 = heat.nz > 0 ? (double)(heat.nz - 1) : 0.0;
+    auto to_idx = [&](V3 p, uint64_t* c, double* t) {  // world.rs:577-598
+      if (p.x < hmin.x || p.x > hmin.x + dx * nxm1 || p.y < hmin.y || p.y > hmin.y + dx * nym1 || p.z < hmin.z ||
+          p.z > hmin.z + dx * nzm1)
+        return false;
+      const double fx = std::floor((p.x - hmin.x) / dx), fy = std::floor((p.y - hmin.y) / dx),
+                   fz = std::floor((p.z - hmin.z) / dx);
+      c[0] = to_usize_or_zero(fx);
+      c[1] = to_usize_or_zero(fy);
+      c[2] = to_usize_or_zero(fz);
+      t[0] = (p.x - hmin.x) / dx - fx;
+      t[1] = (p.y - hmin.y) / dx - fy;
+      t[2] = (p.z - hmin.z) / dx - fz;
+      return true;
+    };
+    for (auto& pt : particles) {
+      const V3 p = pt.pos;
+      if (p.x < lo[0] || p.x > hi[0] || p.y < lo[1] || p.y > hi[1] || p.z < lo[2] || p.z > hi[2]) continue;
+      uint64_t c[3];
+      double t[3];
+      const double temp = to_idx(p, c, t) ? heat.sample_trilinear(c[0], c[1], c[2], t[0], t[1], t[2]) : t_ref;
+      const double dT = temp - t_ref;
+      pt.body_acc += V3{-g.x * beta * dT, -g.y * beta * dT, -g.z * beta * dT};
+      if (heat_gain > 0.0) {
+        const double speed = norm(pt.vel);
+        if (to_idx(p, c, t)) heat.add_source(c[0], c[1], c[2], heat_gain * speed * dt);
+      }
+    }
+  }
+
   // world.rs:691-752: point masses (pos, vel, mass in; force out) coupled to
   // the fluid one after another.  A point outside the bounds is skipped and
   // its force left as it was; each point's reaction -f*dt is shared among the
@@ -709,6 +789,15 @@ void orc_couple_points(void* w, uint64_t np, const double* pos, const double* ve
     force[3 * k + 1] = f[k].y;
     force[3 * k + 2] = f[k].z;
   }
+}
+
+// FluidWorld::couple_heat (world.rs:555-678) against a heat grid of
+// dims3[0..2] cells (x fastest), origin3 and cell size `cell`: u holds the
+// temperatures, src the sources (updated in place).
+void orc_couple_heat(void* w, const uint64_t* dims3, const double* origin3, double cell, const double* u, double* src,
+                     double dt, double t_ref, double beta, double heat_gain) {
+  World::HeatGrid g{dims3[0], dims3[1], dims3[2], V3{origin3[0], origin3[1], origin3[2]}, cell, u, src};
+  static_cast<World*>(w)->couple_heat(g, dt, t_ref, beta, heat_gain);
 }
 
 // for_each_neighbor of an arbitrary point (xyz) over a grid of the current

@@ -117,6 +117,8 @@ SIGNATURES = {
     "phy_fluid_set_params": (C.c_int32, [H, C.c_uint32, C.POINTER(PhySphParams)]),
     "phy_fluid_step": (C.c_int32, [H, C.c_uint32, C.c_double, C.c_uint32]),
     "phy_fluid_diagnostics": (C.c_int32, [H, C.c_uint32, DP]),
+    "phy_fluid_couple_heat": (C.c_int32, [H, C.c_uint32, C.POINTER(C.c_uint64), DP, C.c_double, DP, DP, C.c_double,
+                                          C.c_double, C.c_double, C.c_double]),
     "phy_fluid_couple_points": (C.c_int32, [H, C.c_uint32, C.c_uint64, DP, DP, DP, DP, C.c_double, C.c_double,
                                             C.c_double]),
     "phy_fluid_get_coupling": (C.c_int32, [H, C.c_uint32, DP]),

@@ -144,7 +144,280 @@ __global__ void __launch_bounds__(kCT) k_couple_points(StepConsts c, CoupleArgs 
   }
 }
 
+// ---- couple_heat (world.rs:555-678) ------------------------------------------------
+//
+// Per particle (parallel): the trilinear temperature of the heat grid at its
+// position gives body_acc += -g * beta * (T - t_ref); its source amount
+// heat_gain * |v| * dt and source cell are stored by insertion index.  The
+// reference adds the sources to the grid particle after particle, so a cell's
+// sum is taken in insertion order: a stable radix sort of the (cell,
+// insertion index) pairs by cell, then one sequential sum per cell.
+
+struct HeatArgs {
+  uint64_t nx, ny, nz;  // grid cells per axis (x fastest in memory)
+  double ox, oy, oz, dx;
+  const double* u;  // temperatures
+  double t_ref, beta, gain, dt;
+  const uint32_t* id;  // sorted slot -> insertion index
+  const double* px;
+  const double* py;
+  const double* pz;
+  const double* vx;
+  const double* vy;
+  const double* vz;
+  double* bax;
+  double* bay;
+  double* baz;
+  uint32_t* key;  // by insertion index: source cell, or nx*ny*nz for none
+  double* val;    // by insertion index: source amount
+  int n;
+};
+
+// num-traits ToPrimitive::to_usize of an f64, None -> 0.
+__device__ __forceinline__ uint64_t to_usize_or_zero(double f) {
+  return (f > -1.0 && f < 18446744073709551616.0) ? (uint64_t)f : 0ull;
+}
+
+// ScalarField::sample (phy-field grid.rs:203-208): indices clamped to the grid.
+__device__ __forceinline__ double heat_sample(const HeatArgs& h, uint64_t x, uint64_t y, uint64_t z) {
+  x = x < h.nx - 1 ? x : h.nx - 1;
+  y = y < h.ny - 1 ? y : h.ny - 1;
+  z = z < h.nz - 1 ? z : h.nz - 1;
+  return h.u[x + h.nx * (y + h.ny * z)];
+}
+
+// HeatField::sample_trilinear (phy-field heat.rs:130-171).
+__device__ double heat_trilinear(const HeatArgs& h, uint64_t cx, uint64_t cy, uint64_t cz, double fx, double fy,
+                                 double fz) {
+  const uint64_t x1 = cx + 1 < h.nx - 1 ? cx + 1 : h.nx - 1;
+  const uint64_t y1 = cy + 1 < h.ny - 1 ? cy + 1 : h.ny - 1;
+  const uint64_t z1 = cz + 1 < h.nz - 1 ? cz + 1 : h.nz - 1;
+  const double c000 = heat_sample(h, cx, cy, cz), c100 = heat_sample(h, x1, cy, cz);
+  const double c010 = heat_sample(h, cx, y1, cz), c110 = heat_sample(h, x1, y1, cz);
+  const double c001 = heat_sample(h, cx, cy, z1), c101 = heat_sample(h, x1, cy, z1);
+  const double c011 = heat_sample(h, cx, y1, z1), c111 = heat_sample(h, x1, y1, z1);
+  const double x00 = c000 + (c100 - c000) * fx;
+  const double x10 = c010 + (c110 - c010) * fx;
+  const double x01 = c001 + (c101 - c001) * fx;
+  const double x11 = c011 + (c111 - c011) * fx;
+  const double y0 = x00 + (x10 - x00) * fy;
+  const double y1v = x01 + (x11 - x01) * fy;
+  return y0 + (y1v - y0) * fz;
+}
+
+__global__ void __launch_bounds__(kCT) k_heat_particles(StepConsts c, HeatArgs h) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= h.n) return;
+  const uint32_t none = (uint32_t)(h.nx * h.ny * h.nz);
+  uint32_t key = none;
+  double val = 0.0;
+  const double x = h.px[s], y = h.py[s], z = h.pz[s];
+  // world.rs:635-645: only particles inside the fluid bounds.
+  if (!(x < c.lo[0] || x > c.hi[0] || y < c.lo[1] || y > c.hi[1] || z < c.lo[2] || z > c.hi[2])) {
+    // to_idx (world.rs:577-598); dims.saturating_sub(1), dims >= 1 here.
+    const bool in = !(x < h.ox || x > h.ox + h.dx * (double)(h.nx - 1) || y < h.oy ||
+                      y > h.oy + h.dx * (double)(h.ny - 1) || z < h.oz || z > h.oz + h.dx * (double)(h.nz - 1));
+    uint64_t cx = 0, cy = 0, cz = 0;
+    double temp = h.t_ref;
+    if (in) {
+      const double fx = floor((x - h.ox) / h.dx), fy = floor((y - h.oy) / h.dx), fz = floor((z - h.oz) / h.dx);
+      cx = to_usize_or_zero(fx);
+      cy = to_usize_or_zero(fy);
+      cz = to_usize_or_zero(fz);
+      temp = heat_trilinear(h, cx, cy, cz, (x - h.ox) / h.dx - fx, (y - h.oy) / h.dx - fy, (z - h.oz) / h.dx - fz);
+    }
+    const double dT = temp - h.t_ref;
+    h.bax[s] = h.bax[s] + -c.g[0] * h.beta * dT;
+    h.bay[s] = h.bay[s] + -c.g[1] * h.beta * dT;
+    h.baz[s] = h.baz[s] + -c.g[2] * h.beta * dT;
+    if (h.gain > 0.0 && in && cx < h.nx && cy < h.ny && cz < h.nz) {
+      const double vx = h.vx[s], vy = h.vy[s], vz = h.vz[s];
+      const double speed = sqrt((vx * vx + vy * vy) + vz * vz);
+      key = (uint32_t)(cx + h.nx * (cy + h.ny * cz));
+      val = h.gain * speed * h.dt;
+    }
+  }
+  const uint32_t i = h.id[s];
+  h.key[i] = key;
+  h.val[i] = val;
+}
+
+// Stable LSD radix sort of 32-bit keys with a 32-bit payload, 8 bits a pass.
+// Block b owns keys [b * kRTile, (b + 1) * kRTile); hist[d * nblocks + b]
+// counts digit d in block b, and its exclusive scan (digit-major) is the
+// first output slot of block b's keys of digit d.
+constexpr int kRT = 256;
+constexpr int kRRounds = 8;
+constexpr int kRTile = kRT * kRRounds;
+
+__global__ void __launch_bounds__(kRT) k_radix_hist(const uint32_t* key, int n, int shift, uint32_t* hist,
+                                                     int nblocks) {
+  __shared__ uint32_t s_h[256];
+  const int t = threadIdx.x;
+  s_h[t] = 0;
+  __syncthreads();
+  const int base = blockIdx.x * kRTile;
+  for (int r = 0; r < kRRounds; ++r) {
+    const int e = base + r * kRT + t;
+    if (e < n) atomicAdd(&s_h[(key[e] >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  hist[(size_t)t * nblocks + blockIdx.x] = s_h[t];
+}
+
+// In-place exclusive scan of len values by one block (each thread scans a
+// contiguous run).
+__global__ void __launch_bounds__(1024) k_scan_single(uint32_t* v, int len) {
+  __shared__ uint32_t s_part[1024];
+  const int t = threadIdx.x;
+  const int per = (len + 1023) / 1024;
+  const int lo = min(t * per, len), hi = min(lo + per, len);
+  uint32_t sum = 0;
+  for (int i = lo; i < hi; ++i) sum += v[i];
+  s_part[t] = sum;
+  __syncthreads();
+  if (t == 0) {
+    uint32_t run = 0;
+    for (int k = 0; k < 1024; ++k) {
+      const uint32_t x = s_part[k];
+      s_part[k] = run;
+      run += x;
+    }
+  }
+  __syncthreads();
+  uint32_t run = s_part[t];
+  for (int i = lo; i < hi; ++i) {
+    const uint32_t x = v[i];
+    v[i] = run;
+    run += x;
+  }
+}
+
+// Scatter with ranks stable in key order: round r takes keys base + r*256 ..
+// +255; a key's rank among equal digits is (earlier rounds) + (earlier warps
+// of this round) + (earlier lanes of its warp).
+__global__ void __launch_bounds__(kRT) k_radix_scatter(const uint32_t* key_in, const uint32_t* val_in,
+                                                        uint32_t* key_out, uint32_t* val_out, int n, int shift,
+                                                        const uint32_t* off, int nblocks) {
+  __shared__ uint32_t s_w[kRT / 32][256];
+  __shared__ uint32_t s_run[256];
+  __shared__ uint32_t s_base[256];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  s_run[t] = 0;
+  s_base[t] = off[(size_t)t * nblocks + blockIdx.x];
+  const int base = blockIdx.x * kRTile;
+  for (int r = 0; r < kRRounds; ++r) {
+    for (int w = 0; w < kRT / 32; ++w) s_w[w][t] = 0;
+    __syncthreads();
+    const int e = base + r * kRT + t;
+    const bool valid = e < n;
+    const uint32_t k = valid ? key_in[e] : 0u;
+    const uint32_t d = valid ? (k >> shift) & 255u : 256u;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t lower = __popc(peers & ((1u << lane) - 1u));
+    if (valid && lower == 0) s_w[warp][d] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      uint32_t pre = 0;
+      for (int w = 0; w < warp; ++w) pre += s_w[w][d];
+      const uint32_t dst = s_base[d] + s_run[d] + pre + lower;
+      key_out[dst] = k;
+      val_out[dst] = val_in[e];
+    }
+    __syncthreads();
+    uint32_t tot = 0;
+    for (int w = 0; w < kRT / 32; ++w) tot += s_w[w][t];
+    s_run[t] += tot;
+    __syncthreads();
+  }
+}
+
+// One sequential sum per source cell, in insertion order (the segment of the
+// sorted keys), onto the cell's current source value.
+__global__ void __launch_bounds__(kCT) k_heat_deposit(const uint32_t* key, const uint32_t* idx, const double* val,
+                                                       int n, uint32_t none, double* src) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const uint32_t k = key[e];
+  if (k == none || (e > 0 && key[e - 1] == k)) return;
+  double sum = src[k];
+  for (int j = e; j < n && key[j] == k; ++j) sum = sum + val[idx[j]];
+  src[k] = sum;
+}
+
+__global__ void k_iota_u32(uint32_t* v, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = (uint32_t)i;
+}
+
 }  // namespace
+
+size_t couple_heat_scratch_bytes(int n, uint64_t cells) {
+  const size_t nb = (size_t)((n + kRTile - 1) / kRTile);
+  return 16 * (size_t)cells + 8 * (size_t)n + 16 * (size_t)n + 1024 * nb + 256;
+}
+
+void launch_couple_heat(const StepConsts& c, DevBuffers& b, const HeatGrid& g, unsigned char* scratch,
+                        cudaStream_t s) {
+  const int n = c.n;
+  const uint64_t cells = g.nx * g.ny * g.nz;
+  const size_t nb = (size_t)((n + kRTile - 1) / kRTile);
+  double* u = reinterpret_cast<double*>(scratch);
+  double* src = u + cells;
+  double* val = src + cells;
+  uint32_t* key0 = reinterpret_cast<uint32_t*>(val + n);
+  uint32_t* key1 = key0 + n;
+  uint32_t* id0 = key1 + n;
+  uint32_t* id1 = id0 + n;
+  uint32_t* hist = id1 + n;
+  const ParticleConsts& pc = b.pc[b.cur];
+  HeatArgs h;
+  h.nx = g.nx;
+  h.ny = g.ny;
+  h.nz = g.nz;
+  h.ox = g.origin[0];
+  h.oy = g.origin[1];
+  h.oz = g.origin[2];
+  h.dx = g.cell;
+  h.u = u;
+  h.t_ref = g.t_ref;
+  h.beta = g.beta;
+  h.gain = g.heat_gain;
+  h.dt = c.dt;
+  h.id = pc.id;
+  h.px = b.pv1[0];
+  h.py = b.pv1[1];
+  h.pz = b.pv1[2];
+  h.vx = b.pv1[3];
+  h.vy = b.pv1[4];
+  h.vz = b.pv1[5];
+  h.bax = pc.ba[0];
+  h.bay = pc.ba[1];
+  h.baz = pc.ba[2];
+  h.key = key0;
+  h.val = val;
+  h.n = n;
+  const int blocks = (n + kCT - 1) / kCT;
+  k_heat_particles<<<blocks, kCT, 0, s>>>(c, h);
+  if (!(g.heat_gain > 0.0)) return;
+  const uint32_t none = (uint32_t)cells;
+  int bits = 0;
+  while (bits < 32 && (none >> bits) != 0u) ++bits;  // keys 0 .. none
+  k_iota_u32<<<blocks, kCT, 0, s>>>(id0, n);
+  uint32_t *kin = key0, *kout = key1, *iin = id0, *iout = id1;
+  for (int shift = 0; shift < bits; shift += 8) {
+    k_radix_hist<<<(int)nb, kRT, 0, s>>>(kin, n, shift, hist, (int)nb);
+    k_scan_single<<<1, 1024, 0, s>>>(hist, (int)(256 * nb));
+    k_radix_scatter<<<(int)nb, kRT, 0, s>>>(kin, iin, kout, iout, n, shift, hist, (int)nb);
+    uint32_t* tk = kin;
+    kin = kout;
+    kout = tk;
+    uint32_t* ti = iin;
+    iin = iout;
+    iout = ti;
+  }
+  k_heat_deposit<<<blocks, kCT, 0, s>>>(kin, iin, val, n, none, src);
+}
 
 void launch_couple_points(const StepConsts& c, DevBuffers& b, double* d_pts, int np, double dt, double drag,
                           double soft_density, cudaStream_t s) {

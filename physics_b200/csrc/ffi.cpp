@@ -325,6 +325,16 @@ int32_t phy_fluid_couple_points(PhyWorldHandle* w, uint32_t sub, uint64_t n, con
   });
 }
 
+int32_t phy_fluid_couple_heat(PhyWorldHandle* w, uint32_t sub, const uint64_t* dims3, const double* origin3,
+                              double cell, const double* temp, double* src, double dt, double t_ref, double beta,
+                              double heat_gain) {
+  if (!dims3 || !origin3 || !temp) return -1;
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->couple_heat(dims3, origin3, cell, temp, src, dt, t_ref, beta, heat_gain);
+    return 0;
+  });
+}
+
 int32_t phy_fluid_get_coupling(PhyWorldHandle* w, uint32_t sub, double* out5) {
   if (!out5) return -1;
   return guard<int32_t>(-1, [&] {

@@ -345,6 +345,7 @@ FluidWorld::~FluidWorld() {
   free_all();
   dfree(d_bbox_);
   dfree(d_couple_);
+  dfree(d_heat_);
   dfree(d_pbase_);
   dfree(d_scene_bbox_);
   release_snapshot();
@@ -1385,6 +1386,59 @@ void FluidWorld::couple_points(size_t np, const double* pos, const double* vel, 
   cuda_check(cudaStreamSynchronize(stream_), "couple sync");
   for (size_t k = 0; k < np; ++k)
     for (int a = 0; a < 3; ++a) force[3 * k + a] = h[10 * k + 7 + a];
+}
+
+// world.rs:555-678 (kernels and semantics in couple.cu).  The velocity
+// sampler the reference installs into the field at this point is the field's
+// own business: it captures the particles' positions and velocities, which
+// get_field returns.
+void FluidWorld::couple_heat(const uint64_t* dims3, const double* origin3, double cell, const double* temp,
+                             double* src, double dt, double t_ref, double beta, double heat_gain) {
+  if (n_ == 0) return;  // world.rs:563-565
+  if (!dims3 || !origin3 || !temp) throw std::invalid_argument("couple_heat: null array");
+  const bool deposit = heat_gain > 0.0;
+  if (deposit && !src) throw std::invalid_argument("couple_heat: null source array");
+  if (!scenes_.empty()) throw std::invalid_argument("couple_heat: not available for batched scenes");
+  if (tape_.on) throw std::invalid_argument("couple_heat: the adjoint tape does not record coupling");
+  uint64_t cells = 1;
+  for (int a = 0; a < 3; ++a) {
+    if (dims3[a] == 0 || dims3[a] >= ((uint64_t)1 << 31)) throw std::invalid_argument("couple_heat: bad grid dims");
+    cells *= dims3[a];
+    if (cells >= ((uint64_t)1 << 31)) throw std::invalid_argument("couple_heat: more than 2^31 grid cells");
+  }
+  if (!b_.has_ba) {
+    for (int q = 0; q < 2; ++q)
+      for (int k = 0; k < 3; ++k) dgrow(b_.pc[q].ba[k], 0, (size_t)b_.capacity, stream_);
+    for (int k = 0; k < 3; ++k)
+      cuda_check(cudaMemsetAsync(b_.pc[b_.cur].ba[k], 0, n_ * sizeof(double), stream_), "memset");
+    b_.has_ba = true;
+    ++alloc_gen_;
+  }
+  ensure_cells();
+  const StepConsts c = make_consts(dt);
+  const size_t need = couple_heat_scratch_bytes((int)n_, cells);
+  if (heat_cap_ < need) {
+    dalloc(d_heat_, need);
+    heat_cap_ = need;
+  }
+  const size_t gbytes = cells * sizeof(double);
+  cuda_check(cudaMemcpyAsync(d_heat_, temp, gbytes, cudaMemcpyHostToDevice, stream_), "couple_heat upload");
+  if (deposit)
+    cuda_check(cudaMemcpyAsync(d_heat_ + gbytes, src, gbytes, cudaMemcpyHostToDevice, stream_), "couple_heat upload");
+  HeatGrid g;
+  g.nx = dims3[0];
+  g.ny = dims3[1];
+  g.nz = dims3[2];
+  for (int a = 0; a < 3; ++a) g.origin[a] = origin3[a];
+  g.cell = cell;
+  g.t_ref = t_ref;
+  g.beta = beta;
+  g.heat_gain = heat_gain;
+  launch_couple_heat(c, b_, g, d_heat_, stream_);
+  cuda_check(cudaGetLastError(), "couple_heat launch");
+  if (deposit)
+    cuda_check(cudaMemcpyAsync(src, d_heat_ + gbytes, gbytes, cudaMemcpyDeviceToHost, stream_), "couple_heat download");
+  cuda_check(cudaStreamSynchronize(stream_), "couple_heat sync");
 }
 
 // ---- FluidSubsystem / World ------------------------------------------------

@@ -143,6 +143,16 @@ class FluidWorld {
   void couple_points(size_t np, const double* pos, const double* vel, const double* mass, double* force,
                      double dt, double drag, double soft_density);
 
+  // FluidWorld::couple_heat (world.rs:555-678) on the device, bit-exact:
+  // against a heat grid of dims3 cells (x fastest), origin3 and cell size
+  // `cell` with temperatures `temp`: body_acc += -g beta (T - t_ref) for the
+  // particles inside the bounds, and with heat_gain > 0 the sources `src`
+  // (dims product doubles, updated in place) take heat_gain |v| dt per
+  // particle, added in insertion order.  Not available for batched scenes or
+  // while the adjoint tape records.
+  void couple_heat(const uint64_t* dims3, const double* origin3, double cell, const double* temp, double* src,
+                   double dt, double t_ref, double beta, double heat_gain);
+
   // Total momentum and kinetic energy (subsystem.rs:149-163), f64, insertion order.
   void diagnostics(double* out4);
 
@@ -213,6 +223,9 @@ class FluidWorld {
   // Point records of couple_points (10 doubles each) plus one word of flags.
   double* d_couple_ = nullptr;
   size_t couple_cap_ = 0;
+  // Scratch arena of couple_heat (grid, sources, sort keys).
+  unsigned char* d_heat_ = nullptr;
+  size_t heat_cap_ = 0;
 
   // Batched scenes.
   struct Scene {

@@ -99,6 +99,21 @@ void launch_cell_index(const StepConsts& c, DevBuffers& b, uint32_t* flags, cuda
 // the fluid velocities in pv1 and the forces of the points inside the bounds.
 void launch_couple_points(const StepConsts& c, DevBuffers& b, double* d_pts, int np, double dt, double drag,
                           double soft_density, cudaStream_t s);
+
+// couple.cu: FluidWorld::couple_heat against a heat grid of nx*ny*nz cells
+// (x fastest), origin and cell size.  The scratch arena (size from
+// couple_heat_scratch_bytes) starts with the grid's temperatures (cells
+// doubles, uploaded by the caller) and sources (cells doubles, in/out); the
+// particles' body accelerations (allocated) take the buoyancy terms.
+struct HeatGrid {
+  uint64_t nx, ny, nz;
+  double origin[3];
+  double cell;
+  double t_ref, beta, heat_gain;
+};
+size_t couple_heat_scratch_bytes(int n, uint64_t cells);
+void launch_couple_heat(const StepConsts& c, DevBuffers& b, const HeatGrid& g, unsigned char* scratch,
+                        cudaStream_t s);
 void launch_unsort_f64(const DevBuffers& b, int n, const double* src_sorted, double* dst_orig,
                        cudaStream_t s);
 void launch_unsort_u32(const DevBuffers& b, int n, const uint32_t* src_sorted, double* dst_orig,

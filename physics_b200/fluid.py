@@ -420,6 +420,21 @@ class FluidWorld:
                                                   _dp(out), dt, drag, soft_density), "phy_fluid_couple_points")
         return out.reshape(-1, 3)
 
+    def couple_heat(self, temp, src, origin, cell: float, dt: float, t_ref: float, beta: float,
+                    heat_gain: float) -> np.ndarray:
+        """FluidWorld::couple_heat on the device: temp is the (nz, ny, nx) grid of temperatures
+        (x fastest in memory); returns the updated copy of src.  The particles' body
+        accelerations take the buoyancy terms."""
+        temp = np.ascontiguousarray(temp, np.float64)
+        if temp.ndim != 3:
+            raise ValueError("couple_heat: temp must be a (nz, ny, nx) array")
+        out = np.array(src, np.float64, copy=True, order="C").reshape(temp.shape)
+        dims = (C.c_uint64 * 3)(temp.shape[2], temp.shape[1], temp.shape[0])
+        o = np.ascontiguousarray(origin, np.float64).reshape(3)
+        L.check(self._lib.phy_fluid_couple_heat(self._h, self._sub, dims, _dp(o), cell, _dp(temp), _dp(out), dt, t_ref,
+                                                beta, heat_gain), "phy_fluid_couple_heat")
+        return out
+
     # ---- diagnostics (FluidSubsystem, subsystem.rs:149-163) ------------------------
     def _diag(self) -> np.ndarray:
         out = np.empty(4, np.float64)

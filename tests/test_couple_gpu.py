@@ -1,7 +1,9 @@
-"""FluidWorld::couple_points on the device (phy_fluid_couple_points) against the oracle's
-restatement of phy-fluid/src/sph/world.rs:691-752, bit for bit: forces on the points and
-the fluid velocities that take the reactions, points processed in order, skipped points
-left untouched, and the step that follows the coupling."""
+"""The fluid's coupling on the device against the oracle's restatement, bit for bit:
+FluidWorld::couple_points (phy_fluid_couple_points, phy-fluid/src/sph/world.rs:691-752:
+forces on the points, fluid velocities that take the reactions, points in order, skipped
+points untouched) and FluidWorld::couple_heat (phy_fluid_couple_heat, world.rs:555-678:
+body accelerations from the trilinear temperature, sources added in insertion order), and
+the steps that follow them."""
 import numpy as np
 import pytest
 
@@ -109,3 +111,76 @@ def test_couple_points_rejected_configurations(gpu):
     b.set_scenes([1, 1], [(0, 0, 0)] * 2, [(1, 1, 1)] * 2)
     with pytest.raises(gpu.PhyError):
         b.couple_points([[0.5, 0.5, 0.5]], [[0.0, 0.0, 0.0]], [0.02], DT, 1.0, 1000.0)
+
+
+# ---- couple_heat (world.rs:555-678) -------------------------------------------------------
+
+def _heat_grid(dims, seed):
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = dims
+    return rng.uniform(-1.0, 2.0, (nz, ny, nx)), rng.normal(0.0, 0.1, (nz, ny, nx))
+
+
+def _heat_check(O, w, ow, temp, src0, origin, cell, args):
+    sg = w.couple_heat(temp, src0, origin, cell, *args)
+    so = ow.couple_heat(temp, src0, origin, cell, *args)
+    assert_bits_equal(sg, so, "sources")
+    assert_bits_equal(w.body_acc, ow.get(O.F_BODY_ACC), "body accelerations")
+    return sg
+
+
+def test_couple_heat_f64_bitwise_and_next_steps(gpu, oracle_mod):
+    """A grid that covers part of the fluid (particles outside it sample t_ref), two calls
+    in a row (body accelerations accumulate), then steps that consume them."""
+    O = oracle_mod
+    w, ow, _ = _pair(gpu, O)
+    temp, src0 = _heat_grid((12, 10, 9), 11)
+    args = (0.01, 0.3, 0.2, 0.05)  # dt, t_ref, beta, heat_gain
+    src = _heat_check(O, w, ow, temp, src0, (-0.7, -0.6, -0.4), 0.1, args)
+    assert np.count_nonzero(src != src0) > 10
+    _heat_check(O, w, ow, temp, src, (-0.2, -0.5, -0.3), 0.07, args)
+    w.step(DT, 3)
+    ow.step(DT, 3)
+    assert_bits_equal(w.pos, ow.get(O.F_POS), "positions after coupling and 3 steps")
+    assert_bits_equal(w.vel, ow.get(O.F_VEL), "velocities after coupling and 3 steps")
+    assert not w.body_acc.any(), "integrate consumes the body accelerations"
+
+
+def test_couple_heat_coarse_and_large_grids(gpu, oracle_mod):
+    """Hundreds of particles per source cell (long in-order sums) and a grid of 2^17 cells
+    (three radix passes), over a world of many sort blocks."""
+    O = oracle_mod
+    sc_dims = (24, 32, 24)
+    from physics_b200 import scenes
+    sc = scenes.dam_break(*sc_dims, box=4.0, dt=DT, steps=0)
+    p = ref_test_params(gravity=(0.3, -9.81, -0.2))
+    p.bounds_min, p.bounds_max = sc.bounds_min, sc.bounds_max
+    w = gpu.FluidWorld(p)
+    w.add_particles(sc.pos, sc.mass)
+    ow = O.OracleWorld(p, threads=O.max_threads())
+    ow.add_particles(sc.pos, np.full(sc.n, sc.mass))
+    w.step(DT, 2)
+    ow.step(DT, 2)
+    args = (0.01, 0.0, 0.4, 0.2)
+    temp, src0 = _heat_grid((5, 7, 4), 12)
+    _heat_check(O, w, ow, temp, src0, (0.0, 0.0, 0.0), 0.6, args)
+    temp, src0 = _heat_grid((64, 64, 32), 13)
+    _heat_check(O, w, ow, temp, src0, (0.1, 0.05, 0.2), 0.05, args)
+
+
+def test_couple_heat_reference_tests(gpu):
+    """couple_heat_warmer_fluid_rises and couple_heat_injects_source_into_moving_region
+    (sph/tests.rs:214-290) on the device."""
+    p = ref_test_params(gravity=(0.0, -9.81, 0.0))
+    w = gpu.FluidWorld(p)
+    w.add_particles([[0.0, 1.0, 0.0]], 0.05)
+    temp = np.zeros((16, 16, 16))
+    temp[:, 9:, :] = 1.0
+    src = w.couple_heat(temp, np.zeros_like(temp), (-8.0, -8.0, -8.0), 1.0, 0.01, 0.0, 0.5, 0.0)
+    assert w.body_acc[0, 1] == 9.81 * 0.5 and p.gravity[1] + w.body_acc[0, 1] > -9.81
+    assert not src.any()
+    p = ref_test_params(gravity=(0.0, 0.0, 0.0))
+    w = gpu.FluidWorld(p)
+    w.add_particles([[0.0, 0.0, 0.0]], 0.05, vel=[[2.0, 0.0, 0.0]])
+    src = w.couple_heat(np.zeros((16, 16, 16)), np.zeros((16, 16, 16)), (0.0, 0.0, 0.0), 1.0, 0.01, 0.0, 0.0, 0.1)
+    assert src[0, 0, 0] == 0.1 * 2.0 * 0.01 and np.count_nonzero(src) == 1

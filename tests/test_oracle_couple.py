@@ -1,7 +1,7 @@
-"""The oracle's FluidWorld::couple_points (phy-fluid/src/sph/world.rs:691-752), which the
-device coupling is checked against, pinned on the CPU: the reference's own test
-(sph/tests.rs:179-212), known answers that follow from the definition, and its
-point-after-point semantics."""
+"""The oracle's FluidWorld::couple_points (phy-fluid/src/sph/world.rs:691-752) and
+couple_heat (world.rs:555-678), which the device coupling is checked against, pinned on the
+CPU: the reference's own tests (sph/tests.rs:179-290), known answers that follow from the
+definitions, and their particle-after-particle and point-after-point semantics."""
 import numpy as np
 
 from helpers import assert_bits_equal, ref_test_params
@@ -90,3 +90,77 @@ def test_points_are_coupled_one_after_another(oracle_mod):
     g = np.array(p.gravity)
     assert_bits_equal(fa[2], -g * (p.rest_density * (mass[2] / 900.0)) + (np.zeros(3) - vel[2]) * (2.0 * mass[2]),
                       "empty neighbourhood")
+
+
+# ---- couple_heat (world.rs:555-678) -------------------------------------------------------
+
+def _one_particle(O, pos, vel=(0.0, 0.0, 0.0), gravity=(0.0, -9.81, 0.0)):
+    p = ref_test_params(gravity=gravity)
+    w = O.OracleWorld(p)
+    w.add_particles([pos], [0.05], vel=[vel])
+    return w, p
+
+
+def test_heat_warmer_fluid_rises(oracle_mod):
+    """couple_heat_warmer_fluid_rises (sph/tests.rs:214-259): 16^3 field of unit cells at
+    origin -8, warm (1) where iy - 8 > 0; the particle at y = 1 gets body_acc.y = 9.81 * 0.5."""
+    O = oracle_mod
+    w, p = _one_particle(O, (0.0, 1.0, 0.0))
+    temp = np.zeros((16, 16, 16))
+    temp[:, 9:, :] = 1.0  # (nz, ny, nx): rows iy with iy * 1 - 16 / 2 > 0
+    src = w.couple_heat(temp, np.zeros_like(temp), (-8.0, -8.0, -8.0), 1.0, 0.01, 0.0, 0.5, 0.0)
+    ba = w.get(O.F_BODY_ACC)[0]
+    assert ba[1] == 9.81 * 0.5 and ba[0] == 0.0 and ba[2] == 0.0
+    assert p.gravity[1] + ba[1] > -9.81
+    assert not src.any()
+
+
+def test_heat_injects_source_into_moving_region(oracle_mod):
+    """couple_heat_injects_source_into_moving_region (sph/tests.rs:261-290): the source of
+    the particle's cell grows by heat_gain * |v| * dt."""
+    O = oracle_mod
+    w, _ = _one_particle(O, (0.0, 0.0, 0.0), vel=(2.0, 0.0, 0.0), gravity=(0.0, 0.0, 0.0))
+    temp = np.zeros((16, 16, 16))
+    src = w.couple_heat(temp, np.zeros_like(temp), (0.0, 0.0, 0.0), 1.0, 0.01, 0.0, 0.0, 0.1)
+    assert src[0, 0, 0] == 0.1 * 2.0 * 0.01 and np.count_nonzero(src) == 1
+
+
+def test_heat_trilinear_and_sequential_sources(oracle_mod):
+    """A field linear in the cell coordinates is sampled exactly (up to rounding); sources of
+    particles sharing a cell are added one after another in insertion order; particles
+    outside the bounds are skipped and those outside the field sample t_ref."""
+    O = oracle_mod
+    p = ref_test_params(gravity=(0.5, -9.81, 0.25))
+    w = O.OracleWorld(p)
+    rng = np.random.default_rng(4)
+    pos = np.concatenate([rng.uniform(-0.9, 0.9, (40, 3)), [[0.11, 0.12, 0.13]] * 5, [[3.5, 0.0, 0.0]],
+                          [[-2.5, 2.9, 0.0]]])
+    vel = rng.normal(0.0, 1.0, pos.shape)
+    w.add_particles(pos, np.full(len(pos), 0.02), vel=vel)
+    nx, ny, nz, dx, origin = 7, 6, 5, 0.4, np.array([-1.2, -1.0, -1.1])
+    iz, iy, ix = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    temp = 1.0 + 2.0 * ix + 3.0 * iy - 1.0 * iz
+    src0 = rng.normal(0.0, 0.1, temp.shape)
+    t_ref, beta, gain, dt = 0.5, 0.25, 0.3, 0.01
+    src = w.couple_heat(temp, src0, origin, dx, dt, t_ref, beta, gain)
+    ba = w.get(O.F_BODY_ACC)
+    g = np.array(p.gravity)
+    expect_src = src0.copy()
+    for i in range(len(pos)):
+        x = pos[i]
+        inb = np.all(x >= -3.0) and np.all(x <= 3.0)
+        top = origin + dx * np.array([nx - 1, ny - 1, nz - 1])
+        inf = np.all(x >= origin) and np.all(x <= top)
+        if not inb:
+            assert not ba[i].any()
+            continue
+        if inf:
+            c = (x - origin) / dx
+            cell = np.floor(c).astype(int)
+            lin = 1.0 + 2.0 * c[0] + 3.0 * c[1] - 1.0 * c[2]
+            np.testing.assert_allclose(-ba[i] / (g * beta), lin - t_ref, rtol=1e-12)
+            speed = np.sqrt((vel[i, 0] ** 2 + vel[i, 1] ** 2) + vel[i, 2] ** 2)
+            expect_src[cell[2], cell[1], cell[0]] += gain * speed * dt
+        else:
+            assert not ba[i].any()
+    assert_bits_equal(src, expect_src, "sources in insertion order")
