@@ -152,6 +152,43 @@ int32_t phy_fluid_couple_heat(PhyWorldHandle *w, uint32_t sub, const uint64_t *d
                               double cell, const double *temp, double *src, double dt, double t_ref, double beta,
                               double heat_gain);
 
+/* One rigid body for phy_fluid_couple_bodies: the parts of phy-rigid's Body
+ * (crates/phy-rigid/src/shape.rs:330-372) and Shape (shape.rs:138-176) that
+ * couple_bodies reads.  Shapes: sphere size {r}; capsule {half_height, r}
+ * along local y; box half extents; convex: data_count vertices (xyz triples
+ * from data[data_first]) and face_count index triples (from
+ * faces[3 * face_first], indices into the body's vertices); heightfield
+ * {nx, nz, cell} with data_count = nx * nz heights from data[data_first].
+ * Compound shapes are not supported. */
+#define PHY_SHAPE_SPHERE 0
+#define PHY_SHAPE_CAPSULE 1
+#define PHY_SHAPE_BOX 2
+#define PHY_SHAPE_CONVEX 3
+#define PHY_SHAPE_HEIGHTFIELD 4
+typedef struct PhyCoupleBody {
+  int32_t shape;
+  uint32_t data_first, data_count, face_first, face_count, reserved;
+  double size[3];
+  double pos[3];
+  double rot[4]; /* unit quaternion (i, j, k, w) */
+  double vel[3]; /* linear velocity, updated by the call */
+  double inv_mass; /* 0 = static */
+} PhyCoupleBody;
+
+/* FluidWorld::couple_bodies (crates/phy-fluid/src/sph/world.rs:414-503):
+ * symmetric soft contact and buoyancy between the fluid of subsystem `sub`
+ * and n_bodies rigid bodies, computed on the device and bit-identical to
+ * the reference's loops (particles in insertion order, bodies in order).
+ * Particles inside a body are pushed to its surface and lose their inward
+ * normal velocity; dynamic bodies take the contact impulses and, when any
+ * particle entered them, the buoyancy impulse -g rho0 V dt of their volume.
+ * `friction` is unused, as in the reference.  Fails (-1) on invalid shapes
+ * or ranges, on a world of batched scenes, or while the adjoint tape
+ * records. */
+int32_t phy_fluid_couple_bodies(PhyWorldHandle *w, uint32_t sub, PhyCoupleBody *bodies, uint32_t n_bodies,
+                                const double *data, uint64_t n_data, const uint32_t *faces, uint64_t n_faces,
+                                double dt, double friction);
+
 /* FluidSubsystem coupling coefficients (subsystem.rs:26-55):
  * {thermal_expansion, heat_gain, t_ref, drag, friction}. */
 int32_t phy_fluid_get_coupling(PhyWorldHandle *w, uint32_t sub, double *out5);

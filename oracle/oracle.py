@@ -74,6 +74,7 @@ def load():
             "orc_point_neighbors": (C.c_uint64, [C.c_void_p, DP, C.POINTER(C.c_uint64), C.c_uint64]),
             "orc_couple_heat": (None, [C.c_void_p, C.POINTER(C.c_uint64), DP, C.c_double, DP, DP, C.c_double,
                                         C.c_double, C.c_double, C.c_double]),
+            "orc_couple_bodies": (None, [C.c_void_p, C.c_void_p, C.c_uint32, DP, C.POINTER(C.c_uint32), C.c_double]),
             "orc_couple_points": (None, [C.c_void_p, C.c_uint64, DP, DP, DP, DP, C.c_double, C.c_double,
                                           C.c_double]),
         }
@@ -212,6 +213,14 @@ class OracleWorld:
                                   out.ctypes.data_as(DP), dt, t_ref, beta, heat_gain)
         return out
 
+    def couple_bodies(self, bodies, dt: float) -> np.ndarray:
+        """FluidWorld::couple_bodies (world.rs:414-503) over body dicts (see pack_bodies);
+        returns the bodies' updated velocities (n, 3)."""
+        arr, data, faces = pack_bodies(bodies, OrcBody)
+        self._lib.orc_couple_bodies(self._w, C.cast(arr, C.c_void_p), len(bodies), data.ctypes.data_as(DP),
+                                    faces.ctypes.data_as(C.POINTER(C.c_uint32)), dt)
+        return np.array([list(b.vel) for b in arr], np.float64).reshape(-1, 3)
+
     def couple_points(self, pos, vel, mass, dt: float, drag: float, soft_density: float, force=None):
         """FluidWorld::couple_points (world.rs:691-752): returns the (n, 3) forces; rows of
         points outside the bounds keep the values of `force` (zeros when None)."""
@@ -227,6 +236,47 @@ class OracleWorld:
         out = (C.c_uint64 * 2)()
         self._lib.orc_counters(self._w, out, 1 if reset else 0)
         return int(out[0]), int(out[1])
+
+
+class OrcBody(C.Structure):
+    """Same layout as PhyCoupleBody (include/phy_fluid.h)."""
+    _fields_ = [("shape", C.c_int32), ("data_first", C.c_uint32), ("data_count", C.c_uint32),
+                ("face_first", C.c_uint32), ("face_count", C.c_uint32), ("reserved", C.c_uint32),
+                ("size", C.c_double * 3), ("pos", C.c_double * 3), ("rot", C.c_double * 4), ("vel", C.c_double * 3),
+                ("inv_mass", C.c_double)]
+
+
+SHAPES = {"sphere": 0, "capsule": 1, "box": 2, "convex": 3, "heightfield": 4}
+
+
+def pack_bodies(bodies, struct):
+    """Body dicts -> (struct array, data doubles, face indices).  A dict holds `shape`
+    (a SHAPES name), `size` (sphere (r,), capsule (half_height, r), box half extents,
+    heightfield (nx, nz, cell)), `pos`, `rot` (unit quaternion i, j, k, w; default identity),
+    `vel`, `inv_mass`, and `verts` + `faces` (convex) or `heights` (heightfield)."""
+    arr = (struct * max(len(bodies), 1))()
+    data, faces = [], []
+    for k, b in enumerate(bodies):
+        o = arr[k]
+        o.shape = SHAPES[b["shape"]]
+        size = list(b.get("size", ())) + [0.0] * 3
+        for a in range(3):
+            o.size[a] = size[a]
+            o.pos[a] = b["pos"][a]
+            o.vel[a] = b.get("vel", (0.0, 0.0, 0.0))[a]
+        rot = b.get("rot", (0.0, 0.0, 0.0, 1.0))
+        for a in range(4):
+            o.rot[a] = rot[a]
+        o.inv_mass = b.get("inv_mass", 0.0)
+        if b["shape"] == "convex":
+            o.data_first, o.data_count = len(data), len(b["verts"])
+            data.extend(np.asarray(b["verts"], np.float64).reshape(-1).tolist())
+            o.face_first, o.face_count = len(faces) // 3, len(b["faces"])
+            faces.extend(np.asarray(b["faces"], np.uint32).reshape(-1).tolist())
+        elif b["shape"] == "heightfield":
+            o.data_first, o.data_count = len(data), len(b["heights"])
+            data.extend(list(b["heights"]))
+    return arr, np.array(data + [0.0], np.float64), np.array(faces + [0], np.uint32)
 
 
 def max_threads() -> int:

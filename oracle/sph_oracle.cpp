@@ -440,6 +440,174 @@ struct World {
     }
   }
 
+  // Rigid bodies for couple_bodies (phy-rigid shape.rs:138-372): the pose
+  // (pos, unit quaternion rot = (i, j, k, w) as nalgebra stores it), the
+  // linear velocity, inv_mass, and the shape: 0 sphere {r}, 1 capsule
+  // {half_height, r} along local y, 2 box {half extents}, 3 convex (vertices,
+  // index faces), 4 heightfield {nx, nz, cell} + heights.
+  struct Body {
+    int shape = 0;
+    double size[3] = {0, 0, 0};
+    V3 pos{0, 0, 0};
+    double rot[4] = {0, 0, 0, 1};
+    V3 vel{0, 0, 0};
+    double inv_mass = 0;
+    std::vector<V3> verts;
+    std::vector<uint32_t> faces;  // 3 per face, indices into verts
+    std::vector<double> heights;
+  };
+
+  static double dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+  static V3 cross(V3 a, V3 b) {  // nalgebra Vector3::cross
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+  }
+  static V3 normalize(V3 a) { return a / norm(a); }
+  // nalgebra 0.33.3 UnitQuaternion * Vector3 (its published formula):
+  // t = 2 (q.v x v); q v = (t * q.w + q.v x t) + v.  inverse() is the
+  // conjugate.
+  static V3 qrot(const double* q, V3 v, bool inverse) {
+    const double s = inverse ? -1.0 : 1.0;
+    const V3 u{s * q[0], s * q[1], s * q[2]};
+    const V3 t = cross(u, v) * 2.0;
+    return (t * q[3] + cross(u, t)) + v;
+  }
+  static V3 to_local(const Body& b, V3 p) { return qrot(b.rot, p - b.pos, true); }   // shape.rs:433-436
+  static V3 to_world(const Body& b, V3 p) { return qrot(b.rot, p, false) + b.pos; }  // shape.rs:438-440
+
+  static V3 support_local(const Body& b, V3 dir) {  // shape.rs:198-256
+    switch (b.shape) {
+      case 0:
+        return normalize(dir) * b.size[0];
+      case 1: {
+        const V3 n = normalize(dir);
+        const V3 end = dir.y > 0.0 ? V3{0.0, b.size[0], 0.0} : dir.y < 0.0 ? V3{0.0, -b.size[0], 0.0} : V3{0, 0, 0};
+        return end + n * b.size[1];
+      }
+      case 2:
+        return {dir.x >= 0.0 ? b.size[0] : -b.size[0], dir.y >= 0.0 ? b.size[1] : -b.size[1],
+                dir.z >= 0.0 ? b.size[2] : -b.size[2]};
+      case 3: {
+        V3 best = b.verts[0];
+        double best_dot = dot(b.verts[0], dir);
+        for (size_t k = 1; k < b.verts.size(); ++k) {
+          const double d = dot(b.verts[k], dir);
+          if (d > best_dot) {
+            best_dot = d;
+            best = b.verts[k];
+          }
+        }
+        return best;
+      }
+      default:
+        return {0, 0, 0};
+    }
+  }
+
+  static bool contains_local(const Body& b, V3 p) {  // shape.rs:287-325
+    switch (b.shape) {
+      case 0:
+        return norm(p) <= b.size[0];
+      case 1: {
+        const double h = b.size[0], r = b.size[1];
+        const double y = p.y < -h ? -h : (p.y > h ? h : p.y);
+        const double cx = p.x * p.x + (p.y - y) * (p.y - y) + p.z * p.z;
+        return cx <= r * r;
+      }
+      case 2:
+        return std::fabs(p.x) <= b.size[0] && std::fabs(p.y) <= b.size[1] && std::fabs(p.z) <= b.size[2];
+      case 3:
+        for (size_t f = 0; f + 2 < b.faces.size(); f += 3) {
+          const V3 a = b.verts[b.faces[f]], bb = b.verts[b.faces[f + 1]], c = b.verts[b.faces[f + 2]];
+          const V3 n = cross(bb - a, c - a);
+          if (dot(p - a, n) > 0.0) return false;
+        }
+        return true;
+      default:
+        return false;
+    }
+  }
+
+  static double body_volume(const Body& b) {  // world.rs:506-540
+    switch (b.shape) {
+      case 0:
+        return 4.0 / 3.0 * kPi * b.size[0] * b.size[0] * b.size[0];
+      case 1:
+        return kPi * b.size[1] * b.size[1] * 2.0 * b.size[0] + 4.0 / 3.0 * kPi * b.size[1] * b.size[1] * b.size[1];
+      case 2:
+        return b.size[0] * b.size[1] * b.size[2] * 8.0;
+      case 4: {
+        const double hx = b.size[0] * b.size[2], hz = b.size[1] * b.size[2];
+        double sum = 0.0;
+        for (double h : b.heights) sum = sum + h;
+        const double hy = b.heights.empty() ? 0.0 : sum / (double)b.heights.size();
+        return hx * hz * std::fabs(hy);
+      }
+      default:
+        return 0.0;
+    }
+  }
+
+  static void push_out(Particle& pt, const Body& b) {  // world.rs:755-773
+    const V3 local = to_local(b, pt.pos);
+    const V3 dir = norm(local) > 1e-9 ? normalize(local) : V3{0.0, 1.0, 0.0};
+    const V3 support_dir = support_local(b, dir);
+    pt.pos = to_world(b, support_dir);
+    const V3 v_rel = pt.vel - b.vel;
+    const V3 n = normalize(to_world(b, normalize(support_dir)) - b.pos);
+    const double vn = dot(v_rel, n);
+    if (vn < 0.0) pt.vel = pt.vel - n * vn;
+  }
+
+  // world.rs:414-503: symmetric soft contact and buoyancy with rigid bodies,
+  // particle after particle (each body's velocity takes the impulses of the
+  // particles before).  As in the reference, a dynamic contact's impulse on
+  // the particle is overwritten by push_out's velocity, while the body keeps
+  // its share.
+  void couple_bodies(std::vector<Body>& bodies, double dt) {
+    if (particles.empty() || bodies.empty()) return;
+    const double rho_f = params.rest_density;
+    const V3 g{params.gravity[0], params.gravity[1], params.gravity[2]};
+    const double particle_vol = params.mass / rho_f;
+    const double restitution = 0.0;
+    std::vector<double> displaced(bodies.size(), 0.0);
+    for (auto& pt : particles) {
+      const V3 p_world = pt.pos;
+      V3 v_p = pt.vel;
+      const double m_p = pt.mass;
+      for (size_t bi = 0; bi < bodies.size(); ++bi) {
+        Body& body = bodies[bi];
+        const V3 local = to_local(body, p_world);
+        if (!contains_local(body, local)) continue;
+        const V3 n = norm(local) > 1e-9 ? normalize(local) : V3{0.0, 1.0, 0.0};
+        if (body.inv_mass <= 0.0) {
+          push_out(pt, body);
+          v_p = pt.vel;
+          continue;
+        }
+        const double v_rel_n = dot(v_p - body.vel, n);
+        if (v_rel_n < 0.0) {
+          const double inv_sum = (1.0 / m_p) + body.inv_mass;
+          const double j_mag = -(1.0 + restitution) * v_rel_n / inv_sum;
+          const V3 j = n * j_mag;
+          v_p = v_p + j / m_p;
+          body.vel = body.vel + V3{-j.x, -j.y, -j.z} * body.inv_mass;  // apply_impulse (shape.rs:461-463)
+        }
+        displaced[bi] = displaced[bi] + particle_vol;
+        push_out(pt, body);
+        v_p = pt.vel;
+      }
+      pt.vel = v_p;
+    }
+    for (size_t bi = 0; bi < bodies.size(); ++bi) {
+      Body& body = bodies[bi];
+      if (body.inv_mass <= 0.0) continue;
+      const double vol_b = body_volume(body);
+      const double v_sub = displaced[bi] > 0.0 ? vol_b : 0.0;
+      const V3 buoy = V3{-g.x, -g.y, -g.z} * (rho_f * v_sub);
+      body.vel = body.vel + (buoy * dt) * body.inv_mass;
+    }
+  }
+
   // world.rs:691-752: point masses (pos, vel, mass in; force out) coupled to
   // the fluid one after another.  A point outside the bounds is skipped and
   // its force left as it was; each point's reaction -f*dt is shared among the
@@ -788,6 +956,46 @@ void orc_couple_points(void* w, uint64_t np, const double* pos, const double* ve
     force[3 * k] = f[k].x;
     force[3 * k + 1] = f[k].y;
     force[3 * k + 2] = f[k].z;
+  }
+}
+
+// Same layout as PhyCoupleBody in include/phy_fluid.h.
+struct OrcBody {
+  int32_t shape;
+  uint32_t data_first, data_count, face_first, face_count, reserved;
+  double size[3], pos[3], rot[4], vel[3], inv_mass;
+};
+
+// FluidWorld::couple_bodies (world.rs:414-503); the bodies' velocities are
+// updated in place.  Convex vertices are data_count xyz triples from
+// data[data_first]; faces are face_count index triples from
+// faces[3 * face_first]; heightfield heights are data_count values.
+void orc_couple_bodies(void* w, OrcBody* bodies, uint32_t nb, const double* data, const uint32_t* faces, double dt) {
+  std::vector<World::Body> bs(nb);
+  for (uint32_t k = 0; k < nb; ++k) {
+    const OrcBody& o = bodies[k];
+    World::Body& b = bs[k];
+    b.shape = o.shape;
+    for (int a = 0; a < 3; ++a) b.size[a] = o.size[a];
+    b.pos = {o.pos[0], o.pos[1], o.pos[2]};
+    for (int a = 0; a < 4; ++a) b.rot[a] = o.rot[a];
+    b.vel = {o.vel[0], o.vel[1], o.vel[2]};
+    b.inv_mass = o.inv_mass;
+    if (o.shape == 3) {
+      for (uint32_t v = 0; v < o.data_count; ++v) {
+        const double* d = data + o.data_first + 3 * v;
+        b.verts.push_back({d[0], d[1], d[2]});
+      }
+      b.faces.assign(faces + 3 * (size_t)o.face_first, faces + 3 * ((size_t)o.face_first + o.face_count));
+    } else if (o.shape == 4) {
+      b.heights.assign(data + o.data_first, data + o.data_first + o.data_count);
+    }
+  }
+  static_cast<World*>(w)->couple_bodies(bs, dt);
+  for (uint32_t k = 0; k < nb; ++k) {
+    bodies[k].vel[0] = bs[k].vel.x;
+    bodies[k].vel[1] = bs[k].vel.y;
+    bodies[k].vel[2] = bs[k].vel.z;
   }
 }
 

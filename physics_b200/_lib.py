@@ -47,6 +47,17 @@ class PhyTuneTrial(C.Structure):
                 ("reserved", C.c_int32), ("ms_per_step", C.c_double)]
 
 
+class PhyCoupleBody(C.Structure):
+    """PhyCoupleBody of include/phy_fluid.h (a rigid body for phy_fluid_couple_bodies)."""
+    _fields_ = [("shape", C.c_int32), ("data_first", C.c_uint32), ("data_count", C.c_uint32),
+                ("face_first", C.c_uint32), ("face_count", C.c_uint32), ("reserved", C.c_uint32),
+                ("size", C.c_double * 3), ("pos", C.c_double * 3), ("rot", C.c_double * 4), ("vel", C.c_double * 3),
+                ("inv_mass", C.c_double)]
+
+
+SHAPES = {"sphere": 0, "capsule": 1, "box": 2, "convex": 3, "heightfield": 4}
+
+
 class PhySphParams(C.Structure):
     _fields_ = [
         ("rest_density", C.c_double),
@@ -119,6 +130,8 @@ SIGNATURES = {
     "phy_fluid_diagnostics": (C.c_int32, [H, C.c_uint32, DP]),
     "phy_fluid_couple_heat": (C.c_int32, [H, C.c_uint32, C.POINTER(C.c_uint64), DP, C.c_double, DP, DP, C.c_double,
                                           C.c_double, C.c_double, C.c_double]),
+    "phy_fluid_couple_bodies": (C.c_int32, [H, C.c_uint32, C.c_void_p, C.c_uint32, DP, C.c_uint64,
+                                            C.POINTER(C.c_uint32), C.c_uint64, C.c_double, C.c_double]),
     "phy_fluid_couple_points": (C.c_int32, [H, C.c_uint32, C.c_uint64, DP, DP, DP, DP, C.c_double, C.c_double,
                                             C.c_double]),
     "phy_fluid_get_coupling": (C.c_int32, [H, C.c_uint32, DP]),

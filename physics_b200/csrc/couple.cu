@@ -350,7 +350,287 @@ __global__ void k_iota_u32(uint32_t* v, int n) {
   if (i < n) v[i] = (uint32_t)i;
 }
 
+// ---- couple_bodies (world.rs:414-503) ------------------------------------------------
+//
+// Containment is tested against each particle's position at the start of its
+// turn, so the particles inside some body are found in parallel; the bodies'
+// velocities then change particle after particle, so those particles are
+// processed by one thread in insertion order (a radix sort of the flagged
+// insertion indices), with the reference's loop over the bodies.
+
+struct V3d {
+  double x, y, z;
+};
+__device__ __forceinline__ V3d v3(double x, double y, double z) { return {x, y, z}; }
+__device__ __forceinline__ V3d operator+(V3d a, V3d b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V3d operator-(V3d a, V3d b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V3d operator*(V3d a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ V3d operator/(V3d a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ double vdot(V3d a, V3d b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+__device__ __forceinline__ double vnorm(V3d a) { return sqrt((a.x * a.x + a.y * a.y) + a.z * a.z); }
+__device__ __forceinline__ V3d vnormalize(V3d a) { return a / vnorm(a); }
+__device__ __forceinline__ V3d vcross(V3d a, V3d b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// Unit quaternion (i, j, k, w) times a vector, nalgebra 0.33.3's formula:
+// t = 2 (q.v x v); q v = (t * q.w + q.v x t) + v; the inverse negates q.v.
+__device__ V3d qrot(const double* q, V3d v, bool inverse) {
+  const double s = inverse ? -1.0 : 1.0;
+  const V3d u = v3(s * q[0], s * q[1], s * q[2]);
+  const V3d t = vcross(u, v) * 2.0;
+  return (t * q[3] + vcross(u, t)) + v;
+}
+
+struct BodyArgs {
+  PhyCoupleBody* bodies;
+  int nb;
+  const double* data;
+  const uint32_t* faces;
+  double* displaced;  // nb
+};
+
+__device__ __forceinline__ V3d body_pos(const PhyCoupleBody& b) { return v3(b.pos[0], b.pos[1], b.pos[2]); }
+__device__ __forceinline__ V3d to_local(const PhyCoupleBody& b, V3d p) { return qrot(b.rot, p - body_pos(b), true); }
+__device__ __forceinline__ V3d to_world(const PhyCoupleBody& b, V3d p) { return qrot(b.rot, p, false) + body_pos(b); }
+
+__device__ V3d support_local(const BodyArgs& a, const PhyCoupleBody& b, V3d dir) {  // shape.rs:198-256
+  switch (b.shape) {
+    case PHY_SHAPE_SPHERE:
+      return vnormalize(dir) * b.size[0];
+    case PHY_SHAPE_CAPSULE: {
+      const V3d n = vnormalize(dir);
+      const V3d end = dir.y > 0.0 ? v3(0.0, b.size[0], 0.0) : dir.y < 0.0 ? v3(0.0, -b.size[0], 0.0) : v3(0, 0, 0);
+      return end + n * b.size[1];
+    }
+    case PHY_SHAPE_BOX:
+      return v3(dir.x >= 0.0 ? b.size[0] : -b.size[0], dir.y >= 0.0 ? b.size[1] : -b.size[1],
+                dir.z >= 0.0 ? b.size[2] : -b.size[2]);
+    case PHY_SHAPE_CONVEX: {
+      const double* v = a.data + b.data_first;
+      V3d best = v3(v[0], v[1], v[2]);
+      double best_dot = vdot(best, dir);
+      for (uint32_t k = 1; k < b.data_count; ++k) {
+        const V3d c = v3(v[3 * k], v[3 * k + 1], v[3 * k + 2]);
+        const double d = vdot(c, dir);
+        if (d > best_dot) {
+          best_dot = d;
+          best = c;
+        }
+      }
+      return best;
+    }
+    default:
+      return v3(0, 0, 0);
+  }
+}
+
+__device__ bool contains_local(const BodyArgs& a, const PhyCoupleBody& b, V3d p) {  // shape.rs:287-325
+  switch (b.shape) {
+    case PHY_SHAPE_SPHERE:
+      return vnorm(p) <= b.size[0];
+    case PHY_SHAPE_CAPSULE: {
+      const double h = b.size[0], r = b.size[1];
+      const double y = p.y < -h ? -h : (p.y > h ? h : p.y);
+      const double cx = p.x * p.x + (p.y - y) * (p.y - y) + p.z * p.z;
+      return cx <= r * r;
+    }
+    case PHY_SHAPE_BOX:
+      return fabs(p.x) <= b.size[0] && fabs(p.y) <= b.size[1] && fabs(p.z) <= b.size[2];
+    case PHY_SHAPE_CONVEX: {
+      const double* v = a.data + b.data_first;
+      const uint32_t* f = a.faces + 3 * (size_t)b.face_first;
+      for (uint32_t k = 0; k < b.face_count; ++k) {
+        const uint32_t i0 = f[3 * k], i1 = f[3 * k + 1], i2 = f[3 * k + 2];
+        const V3d pa = v3(v[3 * i0], v[3 * i0 + 1], v[3 * i0 + 2]);
+        const V3d pb = v3(v[3 * i1], v[3 * i1 + 1], v[3 * i1 + 2]);
+        const V3d pc = v3(v[3 * i2], v[3 * i2 + 1], v[3 * i2 + 2]);
+        if (vdot(p - pa, vcross(pb - pa, pc - pa)) > 0.0) return false;
+      }
+      return true;
+    }
+    default:
+      return false;
+  }
+}
+
+__device__ double body_volume(const BodyArgs& a, const PhyCoupleBody& b) {  // world.rs:506-540
+  const double pi = 3.14159265358979323846;
+  switch (b.shape) {
+    case PHY_SHAPE_SPHERE:
+      return 4.0 / 3.0 * pi * b.size[0] * b.size[0] * b.size[0];
+    case PHY_SHAPE_CAPSULE:
+      return pi * b.size[1] * b.size[1] * 2.0 * b.size[0] + 4.0 / 3.0 * pi * b.size[1] * b.size[1] * b.size[1];
+    case PHY_SHAPE_BOX:
+      return b.size[0] * b.size[1] * b.size[2] * 8.0;
+    case PHY_SHAPE_HEIGHTFIELD: {
+      const double hx = b.size[0] * b.size[2], hz = b.size[1] * b.size[2];
+      double sum = 0.0;
+      for (uint32_t k = 0; k < b.data_count; ++k) sum = sum + a.data[b.data_first + k];
+      const double hy = b.data_count == 0 ? 0.0 : sum / (double)b.data_count;
+      return hx * hz * fabs(hy);
+    }
+    default:
+      return 0.0;
+  }
+}
+
+// world.rs:755-773
+__device__ void push_out(const BodyArgs& a, const PhyCoupleBody& b, V3d& pos, V3d& vel) {
+  const V3d local = to_local(b, pos);
+  const V3d dir = vnorm(local) > 1e-9 ? vnormalize(local) : v3(0.0, 1.0, 0.0);
+  const V3d sd = support_local(a, b, dir);
+  pos = to_world(b, sd);
+  const V3d v_rel = vel - v3(b.vel[0], b.vel[1], b.vel[2]);
+  const V3d n = vnormalize(to_world(b, vnormalize(sd)) - body_pos(b));
+  const double vn = vdot(v_rel, n);
+  if (vn < 0.0) vel = vel - n * vn;
+}
+
+// Flags the particles inside any body: their insertion index and slot are
+// appended (in no particular order) to key / val, the count to *count.
+__global__ void __launch_bounds__(kCT) k_body_flags(BodyArgs a, int n, const double* px, const double* py,
+                                                     const double* pz, const uint32_t* id, uint32_t* key,
+                                                     uint32_t* val, uint32_t* count) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const V3d p = v3(px[s], py[s], pz[s]);
+  bool inside = false;
+  for (int bi = 0; bi < a.nb && !inside; ++bi) inside = contains_local(a, a.bodies[bi], to_local(a.bodies[bi], p));
+  if (!inside) return;
+  const uint32_t k = atomicAdd(count, 1u);
+  key[k] = id[s];
+  val[k] = (uint32_t)s;
+}
+
+// The reference's loops over the flagged particles (insertion order) and the
+// bodies, then the buoyancy impulses.  One thread.
+__global__ void k_body_contacts(StepConsts c, BodyArgs a, const uint32_t* slots, int m, const double* mass,
+                                double* px, double* py, double* pz, double* vx, double* vy, double* vz, double dt,
+                                double particle_vol) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const double rho_f = c.rest;
+  const double restitution = 0.0;
+  for (int bi = 0; bi < a.nb; ++bi) a.displaced[bi] = 0.0;
+  for (int k = 0; k < m; ++k) {
+    const uint32_t s = slots[k];
+    const V3d p_world = v3(px[s], py[s], pz[s]);
+    V3d pos = p_world;
+    V3d vel = v3(vx[s], vy[s], vz[s]);
+    V3d v_p = vel;
+    const double m_p = mass[s];
+    for (int bi = 0; bi < a.nb; ++bi) {
+      PhyCoupleBody& body = a.bodies[bi];
+      const V3d local = to_local(body, p_world);
+      if (!contains_local(a, body, local)) continue;
+      const V3d n = vnorm(local) > 1e-9 ? vnormalize(local) : v3(0.0, 1.0, 0.0);
+      if (body.inv_mass <= 0.0) {
+        push_out(a, body, pos, vel);
+        v_p = vel;
+        continue;
+      }
+      const double v_rel_n = vdot(v_p - v3(body.vel[0], body.vel[1], body.vel[2]), n);
+      if (v_rel_n < 0.0) {
+        const double inv_sum = (1.0 / m_p) + body.inv_mass;
+        const double j_mag = -(1.0 + restitution) * v_rel_n / inv_sum;
+        const V3d j = n * j_mag;
+        v_p = v_p + j / m_p;
+        body.vel[0] = body.vel[0] + -j.x * body.inv_mass;  // apply_impulse(-j) (shape.rs:461-463)
+        body.vel[1] = body.vel[1] + -j.y * body.inv_mass;
+        body.vel[2] = body.vel[2] + -j.z * body.inv_mass;
+      }
+      a.displaced[bi] = a.displaced[bi] + particle_vol;
+      push_out(a, body, pos, vel);
+      v_p = vel;
+    }
+    px[s] = pos.x;
+    py[s] = pos.y;
+    pz[s] = pos.z;
+    vx[s] = v_p.x;
+    vy[s] = v_p.y;
+    vz[s] = v_p.z;
+  }
+  for (int bi = 0; bi < a.nb; ++bi) {
+    PhyCoupleBody& body = a.bodies[bi];
+    if (body.inv_mass <= 0.0) continue;
+    const double vol_b = body_volume(a, body);
+    const double v_sub = a.displaced[bi] > 0.0 ? vol_b : 0.0;
+    const double rv = rho_f * v_sub;
+    body.vel[0] = body.vel[0] + -c.g[0] * rv * dt * body.inv_mass;
+    body.vel[1] = body.vel[1] + -c.g[1] * rv * dt * body.inv_mass;
+    body.vel[2] = body.vel[2] + -c.g[2] * rv * dt * body.inv_mass;
+  }
+}
+
 }  // namespace
+
+size_t couple_bodies_scratch_bytes(int n, int nb, uint64_t n_data, uint64_t n_faces) {
+  return (size_t)nb * sizeof(PhyCoupleBody) + 8 * (size_t)nb + 8 * (size_t)n_data + 4 * (size_t)n_faces +
+         16 * (size_t)n + 1024 * (size_t)((n + kRTile - 1) / kRTile) + 512;
+}
+
+int launch_couple_bodies(const StepConsts& c, DevBuffers& b, const CoupleBodiesLaunch& l, cudaStream_t s) {
+  const int n = c.n;
+  if (cudaMemcpyAsync(l.scratch, l.bodies, (size_t)l.nb * sizeof(PhyCoupleBody), cudaMemcpyHostToDevice, s) !=
+      cudaSuccess)
+    return -1;
+  const size_t nbk = (size_t)((n + kRTile - 1) / kRTile);
+  unsigned char* base = l.scratch;
+  PhyCoupleBody* bodies = reinterpret_cast<PhyCoupleBody*>(base);
+  double* displaced = reinterpret_cast<double*>(bodies + l.nb);
+  double* data = displaced + l.nb;
+  uint32_t* faces = reinterpret_cast<uint32_t*>(data + l.n_data);
+  uint32_t* key0 = faces + l.n_faces;
+  uint32_t* key1 = key0 + n;
+  uint32_t* val0 = key1 + n;
+  uint32_t* val1 = val0 + n;
+  uint32_t* hist = val1 + n;
+  uint32_t* count = hist + 256 * nbk;
+  if (l.n_data && cudaMemcpyAsync(data, l.data, l.n_data * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return -1;
+  if (l.n_faces &&
+      cudaMemcpyAsync(faces, l.faces, l.n_faces * sizeof(uint32_t), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return -1;
+  BodyArgs a;
+  a.bodies = bodies;
+  a.nb = l.nb;
+  a.data = data;
+  a.faces = faces;
+  a.displaced = displaced;
+  const ParticleConsts& pc = b.pc[b.cur];
+  cudaMemsetAsync(count, 0, sizeof(uint32_t), s);
+  const int blocks = (n + kCT - 1) / kCT;
+  k_body_flags<<<blocks, kCT, 0, s>>>(a, n, b.pv1[0], b.pv1[1], b.pv1[2], pc.id, key0, val0, count);
+  uint32_t m = 0;
+  if (cudaMemcpyAsync(&m, count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return -1;
+  uint32_t *kin = key0, *kout = key1, *vin = val0, *vout = val1;
+  if (m > 1) {
+    const int mb = (int)((m + kRTile - 1) / kRTile);
+    int bits = 0;
+    while (bits < 32 && ((uint32_t)(n - 1) >> bits) != 0u) ++bits;
+    for (int shift = 0; shift < bits; shift += 8) {
+      k_radix_hist<<<mb, kRT, 0, s>>>(kin, (int)m, shift, hist, mb);
+      k_scan_single<<<1, 1024, 0, s>>>(hist, 256 * mb);
+      k_radix_scatter<<<mb, kRT, 0, s>>>(kin, vin, kout, vout, (int)m, shift, hist, mb);
+      uint32_t* t = kin;
+      kin = kout;
+      kout = t;
+      t = vin;
+      vin = vout;
+      vout = t;
+    }
+  }
+  k_body_contacts<<<1, 32, 0, s>>>(c, a, vin, (int)m, pc.mass, b.pv1[0], b.pv1[1], b.pv1[2], b.pv1[3], b.pv1[4],
+                                    b.pv1[5], c.dt, l.particle_vol);
+  if (cudaGetLastError() != cudaSuccess ||
+      cudaMemcpyAsync(l.bodies, bodies, (size_t)l.nb * sizeof(PhyCoupleBody), cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return -1;
+  return 0;
+}
 
 size_t couple_heat_scratch_bytes(int n, uint64_t cells) {
   const size_t nb = (size_t)((n + kRTile - 1) / kRTile);

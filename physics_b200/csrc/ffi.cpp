@@ -335,6 +335,17 @@ int32_t phy_fluid_couple_heat(PhyWorldHandle* w, uint32_t sub, const uint64_t* d
   });
 }
 
+int32_t phy_fluid_couple_bodies(PhyWorldHandle* w, uint32_t sub, PhyCoupleBody* bodies, uint32_t n_bodies,
+                                const double* data, uint64_t n_data, const uint32_t* faces, uint64_t n_faces,
+                                double dt, double friction) {
+  (void)friction;  // unused by the reference too (world.rs:755)
+  if (n_bodies > 0 && !bodies) return -1;
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->couple_bodies(bodies, n_bodies, data, n_data, faces, n_faces, dt);
+    return 0;
+  });
+}
+
 int32_t phy_fluid_get_coupling(PhyWorldHandle* w, uint32_t sub, double* out5) {
   if (!out5) return -1;
   return guard<int32_t>(-1, [&] {

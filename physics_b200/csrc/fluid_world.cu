@@ -346,6 +346,7 @@ FluidWorld::~FluidWorld() {
   dfree(d_bbox_);
   dfree(d_couple_);
   dfree(d_heat_);
+  dfree(d_bodies_);
   dfree(d_pbase_);
   dfree(d_scene_bbox_);
   release_snapshot();
@@ -1439,6 +1440,52 @@ void FluidWorld::couple_heat(const uint64_t* dims3, const double* origin3, doubl
   if (deposit)
     cuda_check(cudaMemcpyAsync(src, d_heat_ + gbytes, gbytes, cudaMemcpyDeviceToHost, stream_), "couple_heat download");
   cuda_check(cudaStreamSynchronize(stream_), "couple_heat sync");
+}
+
+// world.rs:414-503 (kernels and semantics in couple.cu).
+void FluidWorld::couple_bodies(PhyCoupleBody* bodies, uint32_t nb, const double* data, uint64_t n_data,
+                               const uint32_t* faces, uint64_t n_faces, double dt) {
+  if (n_ == 0 || nb == 0) return;  // world.rs:415-417
+  if (!bodies) throw std::invalid_argument("couple_bodies: null bodies");
+  if (!scenes_.empty()) throw std::invalid_argument("couple_bodies: not available for batched scenes");
+  if (tape_.on) throw std::invalid_argument("couple_bodies: the adjoint tape does not record coupling");
+  if (nb > (1u << 20)) throw std::invalid_argument("couple_bodies: more than 2^20 bodies");
+  for (uint32_t k = 0; k < nb; ++k) {
+    const PhyCoupleBody& b = bodies[k];
+    if (b.shape < PHY_SHAPE_SPHERE || b.shape > PHY_SHAPE_HEIGHTFIELD)
+      throw std::invalid_argument("couple_bodies: unsupported shape");
+    if (b.shape == PHY_SHAPE_CONVEX) {
+      if (b.data_count == 0 || !data || (uint64_t)b.data_first + 3ull * b.data_count > n_data)
+        throw std::invalid_argument("couple_bodies: convex vertices out of range");
+      if ((b.face_count && !faces) || 3ull * ((uint64_t)b.face_first + b.face_count) > n_faces)
+        throw std::invalid_argument("couple_bodies: convex faces out of range");
+      for (uint64_t f = 3ull * b.face_first; f < 3ull * ((uint64_t)b.face_first + b.face_count); ++f)
+        if (faces[f] >= b.data_count) throw std::invalid_argument("couple_bodies: face index out of range");
+    } else if (b.shape == PHY_SHAPE_HEIGHTFIELD) {
+      if ((b.data_count && !data) || (uint64_t)b.data_first + b.data_count > n_data)
+        throw std::invalid_argument("couple_bodies: heights out of range");
+    }
+  }
+  ensure_cells();
+  const StepConsts c = make_consts(dt);
+  const size_t need = couple_bodies_scratch_bytes((int)n_, (int)nb, n_data, n_faces);
+  if (bodies_cap_ < need) {
+    dalloc(d_bodies_, need);
+    bodies_cap_ = need;
+  }
+  CoupleBodiesLaunch l;
+  l.scratch = d_bodies_;
+  l.bodies = bodies;
+  l.nb = (int)nb;
+  l.data = data;
+  l.n_data = data ? n_data : 0;
+  l.faces = faces;
+  l.n_faces = faces ? n_faces : 0;
+  l.particle_vol = params.mass / params.rest_density;
+  if (launch_couple_bodies(c, b_, l, stream_) != 0) {
+    const cudaError_t e = cudaGetLastError();
+    cuda_check(e == cudaSuccess ? cudaErrorUnknown : e, "couple_bodies");
+  }
 }
 
 // ---- FluidSubsystem / World ------------------------------------------------

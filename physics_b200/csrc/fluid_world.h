@@ -153,6 +153,13 @@ class FluidWorld {
   void couple_heat(const uint64_t* dims3, const double* origin3, double cell, const double* temp, double* src,
                    double dt, double t_ref, double beta, double heat_gain);
 
+  // FluidWorld::couple_bodies (world.rs:414-503) on the device, bit-exact:
+  // `bodies` (velocities updated in place) with their vertex / height data
+  // and face indices as described for PhyCoupleBody.  Not available for
+  // batched scenes or while the adjoint tape records.
+  void couple_bodies(PhyCoupleBody* bodies, uint32_t nb, const double* data, uint64_t n_data, const uint32_t* faces,
+                     uint64_t n_faces, double dt);
+
   // Total momentum and kinetic energy (subsystem.rs:149-163), f64, insertion order.
   void diagnostics(double* out4);
 
@@ -226,6 +233,9 @@ class FluidWorld {
   // Scratch arena of couple_heat (grid, sources, sort keys).
   unsigned char* d_heat_ = nullptr;
   size_t heat_cap_ = 0;
+  // Scratch arena of couple_bodies.
+  unsigned char* d_bodies_ = nullptr;
+  size_t bodies_cap_ = 0;
 
   // Batched scenes.
   struct Scene {

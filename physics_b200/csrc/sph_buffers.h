@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "phy_fluid.h"
 #include "sph_common.cuh"
 
 namespace phy {
@@ -112,6 +113,22 @@ struct HeatGrid {
   double t_ref, beta, heat_gain;
 };
 size_t couple_heat_scratch_bytes(int n, uint64_t cells);
+// couple.cu: FluidWorld::couple_bodies over nb host bodies (PhyCoupleBody,
+// include/phy_fluid.h; velocities updated in place) with their vertex /
+// height data and face indices; uses `scratch` of couple_bodies_scratch_bytes
+// and synchronises the stream.  Returns 0, or -1 on a CUDA error.
+struct CoupleBodiesLaunch {
+  unsigned char* scratch;
+  PhyCoupleBody* bodies;
+  int nb;
+  const double* data;
+  uint64_t n_data;
+  const uint32_t* faces;
+  uint64_t n_faces;
+  double particle_vol;  // params.mass / rest_density (world.rs:424)
+};
+size_t couple_bodies_scratch_bytes(int n, int nb, uint64_t n_data, uint64_t n_faces);
+int launch_couple_bodies(const StepConsts& c, DevBuffers& b, const CoupleBodiesLaunch& l, cudaStream_t s);
 void launch_couple_heat(const StepConsts& c, DevBuffers& b, const HeatGrid& g, unsigned char* scratch,
                         cudaStream_t s);
 void launch_unsort_f64(const DevBuffers& b, int n, const double* src_sorted, double* dst_orig,

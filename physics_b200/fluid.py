@@ -435,6 +435,40 @@ class FluidWorld:
                                                 beta, heat_gain), "phy_fluid_couple_heat")
         return out
 
+    def couple_bodies(self, bodies, dt: float, friction: float = 0.0) -> np.ndarray:
+        """FluidWorld::couple_bodies on the device over body dicts: `shape` (sphere, capsule,
+        box, convex, heightfield), `size` (sphere (r,), capsule (half_height, r), box half
+        extents, heightfield (nx, nz, cell)), `pos`, `rot` (unit quaternion i, j, k, w; default
+        identity), `vel`, `inv_mass` (0 = static), and `verts` + `faces` (convex) or `heights`
+        (heightfield).  Returns the bodies' updated velocities (n, 3); the fluid particles
+        inside a body are pushed out."""
+        arr = (L.PhyCoupleBody * max(len(bodies), 1))()
+        data, faces = [], []
+        for k, b in enumerate(bodies):
+            o = arr[k]
+            o.shape = L.SHAPES[b["shape"]]
+            size = list(b.get("size", ())) + [0.0] * 3
+            vel = b.get("vel", (0.0, 0.0, 0.0))
+            for a in range(3):
+                o.size[a], o.pos[a], o.vel[a] = size[a], b["pos"][a], vel[a]
+            for a, q in enumerate(b.get("rot", (0.0, 0.0, 0.0, 1.0))):
+                o.rot[a] = q
+            o.inv_mass = b.get("inv_mass", 0.0)
+            if b["shape"] == "convex":
+                o.data_first, o.data_count = len(data), len(b["verts"])
+                data.extend(np.asarray(b["verts"], np.float64).reshape(-1).tolist())
+                o.face_first, o.face_count = len(faces) // 3, len(b["faces"])
+                faces.extend(np.asarray(b["faces"], np.uint32).reshape(-1).tolist())
+            elif b["shape"] == "heightfield":
+                o.data_first, o.data_count = len(data), len(b["heights"])
+                data.extend(list(b["heights"]))
+        d = np.array(data + [0.0], np.float64)
+        f = np.array(faces + [0], np.uint32)
+        L.check(self._lib.phy_fluid_couple_bodies(self._h, self._sub, C.cast(arr, C.c_void_p), len(bodies), _dp(d),
+                                                  len(data), f.ctypes.data_as(C.POINTER(C.c_uint32)), len(faces), dt,
+                                                  friction), "phy_fluid_couple_bodies")
+        return np.array([list(o.vel) for o in arr[:len(bodies)]], np.float64).reshape(-1, 3)
+
     # ---- diagnostics (FluidSubsystem, subsystem.rs:149-163) ------------------------
     def _diag(self) -> np.ndarray:
         out = np.empty(4, np.float64)

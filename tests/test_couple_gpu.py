@@ -184,3 +184,120 @@ def test_couple_heat_reference_tests(gpu):
     w.add_particles([[0.0, 0.0, 0.0]], 0.05, vel=[[2.0, 0.0, 0.0]])
     src = w.couple_heat(np.zeros((16, 16, 16)), np.zeros((16, 16, 16)), (0.0, 0.0, 0.0), 1.0, 0.01, 0.0, 0.0, 0.1)
     assert src[0, 0, 0] == 0.1 * 2.0 * 0.01 and np.count_nonzero(src) == 1
+
+
+# ---- couple_bodies (world.rs:414-503) -----------------------------------------------------
+
+def _quat(axis, angle):
+    a = np.asarray(axis, np.float64)
+    a = a / np.linalg.norm(a)
+    return tuple(np.sin(angle / 2) * a) + (np.cos(angle / 2),)
+
+
+TETRA = {"verts": (np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]]) - 0.25) * 0.5,
+         "faces": [[0, 2, 1], [0, 1, 3], [0, 3, 2], [1, 2, 3]]}  # outward (b - a) x (c - a)
+
+
+def _bodies(shift=0.0):
+    return [
+        {"shape": "sphere", "size": (0.22,), "pos": (0.15 + shift, 0.0, 0.05), "vel": (0.0, -0.4, 0.1), "inv_mass": 2.0},
+        {"shape": "box", "size": (0.3, 0.12, 0.2), "pos": (-0.25, 0.2, 0.0), "rot": _quat((1, 2, 3), 0.7),
+         "inv_mass": 0.0},
+        {"shape": "capsule", "size": (0.15, 0.1), "pos": (0.0, -0.3, -0.25), "rot": _quat((0, 0, 1), 1.1),
+         "vel": (0.3, 0.0, 0.0), "inv_mass": 5.0},
+        {"shape": "convex", **TETRA, "pos": (0.3, 0.3, 0.3), "rot": _quat((1, -1, 0), 0.4), "inv_mass": 3.0},
+        {"shape": "heightfield", "size": (3, 2, 0.5), "heights": [0.1, 0.3, -0.2, 0.4, 0.0, 0.2], "pos": (0, -0.5, 0),
+         "inv_mass": 1.0},
+        {"shape": "box", "size": (0.1, 0.1, 0.1), "pos": (2.0, 2.0, 2.0), "vel": (0.0, 0.0, -0.0), "inv_mass": 4.0},
+    ]
+
+
+def _bodies_check(O, w, ow, bodies):
+    vg = w.couple_bodies(bodies, DT)
+    vo = ow.couple_bodies(bodies, DT)
+    assert_bits_equal(vg, vo, "body velocities")
+    assert_bits_equal(w.pos, ow.get(O.F_POS), "fluid positions")
+    assert_bits_equal(w.vel, ow.get(O.F_VEL), "fluid velocities")
+    return vg
+
+
+def test_couple_bodies_f64_bitwise_and_next_steps(gpu, oracle_mod):
+    O = oracle_mod
+    w, ow, _ = _pair(gpu, O)
+    x0 = w.pos.copy()
+    vg = _bodies_check(O, w, ow, _bodies())
+    assert np.count_nonzero(np.any(w.pos != x0, axis=1)) > 20, "particles were pushed out"
+    assert not np.array_equal(vg[0], [0.0, -0.4, 0.1])
+    w.step(DT, 5)
+    ow.step(DT, 5)
+    assert_bits_equal(w.pos, ow.get(O.F_POS), "positions after coupling and 5 steps")
+    assert_bits_equal(w.vel, ow.get(O.F_VEL), "velocities after coupling and 5 steps")
+
+
+def test_couple_bodies_repeated_with_moving_bodies(gpu, oracle_mod):
+    """Bodies integrated by the caller between steps (sph/tests.rs:160-169 style): the
+    coupled trajectory stays bit-identical."""
+    O = oracle_mod
+    w, ow, p = _pair(gpu, O, steps=5)
+    bodies = _bodies()
+    g = np.array(p.gravity)
+    for _ in range(25):
+        for b in bodies:
+            if b["inv_mass"] > 0:
+                b["vel"] = tuple(np.asarray(b.get("vel", (0.0, 0.0, 0.0))) + g * DT)
+                b["pos"] = tuple(np.asarray(b["pos"]) + np.asarray(b["vel"]) * DT)
+        w.step(DT)
+        ow.step(DT)
+        v = _bodies_check(O, w, ow, bodies)
+        for b, vb in zip(bodies, v):
+            b["vel"] = tuple(vb)
+
+
+def test_couple_bodies_on_tiled_compensated_world(gpu, oracle_mod):
+    O = oracle_mod
+    w, ow, _ = _pair(gpu, O, prec="comp", steps=20)
+    _bodies_check(O, w, ow, _bodies(shift=0.05))
+    w.step(DT, 10)
+    assert np.isfinite(w.pos).all()
+
+
+def test_couple_bodies_reference_tests(gpu):
+    """static_body_blocks_fluid and dynamic_body_gets_buoyancy_upward (sph/tests.rs:96-175)."""
+    w = gpu.FluidWorld(ref_test_params())
+    w.fill_box((-1.5, -1.5, -0.5), (1.5, -1.0, 0.5), 0.1, 0.05)
+    box = {"shape": "box", "size": (1.0, 0.5, 1.0), "pos": (0.0, 0.0, 0.0), "inv_mass": 0.0}
+    for _ in range(100):
+        w.step(DT)
+        w.couple_bodies([box], DT)
+    x = w.pos
+    assert not np.any((np.abs(x[:, 0]) <= 1.0) & (np.abs(x[:, 1]) <= 0.5) & (np.abs(x[:, 2]) <= 1.0))
+    p = ref_test_params(gravity=(0.0, -9.81, 0.0))
+    w = gpu.FluidWorld(p)
+    w.fill_box((-0.7, -0.7, -0.7), (0.7, 0.7, 0.7), 0.1, 0.05)
+    w.step(DT, 15)
+    mass_b = p.rest_density * (4.0 / 3.0 * np.pi * 0.6 ** 3) * 0.25
+    pos, vel = np.zeros(3), np.zeros(3)
+    for _ in range(120):
+        vel = vel + np.array(p.gravity) * DT
+        pos = pos + vel * DT
+        w.step(DT)
+        vel = w.couple_bodies([{"shape": "sphere", "size": (0.6,), "pos": pos, "vel": vel, "inv_mass": 1.0 / mass_b}],
+                              DT)[0]
+    assert pos[1] > 0.0
+
+
+def test_couple_bodies_rejects_invalid_input(gpu):
+    import ctypes as C
+    from physics_b200 import _lib as L
+    w = gpu.FluidWorld(ref_test_params())
+    w.fill_box((-0.5,) * 3, (0.5,) * 3, 0.1, 0.05)
+    bad_face = {"shape": "convex", "verts": TETRA["verts"], "faces": [[0, 1, 4]], "pos": (0, 0, 0)}
+    with pytest.raises(gpu.PhyError):
+        w.couple_bodies([bad_face], DT)
+    arr = (L.PhyCoupleBody * 1)()
+    arr[0].shape = 5  # compound: not supported
+    d = np.zeros(1)
+    f = np.zeros(1, np.uint32)
+    assert L.load().phy_fluid_couple_bodies(w._h, 0, C.cast(arr, C.c_void_p), 1, d.ctypes.data_as(L.DP), 0,
+                                            f.ctypes.data_as(C.POINTER(C.c_uint32)), 0, DT, 0.0) == -1
+    w.couple_bodies([], DT)  # no bodies: no-op

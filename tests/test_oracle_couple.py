@@ -164,3 +164,84 @@ def test_heat_trilinear_and_sequential_sources(oracle_mod):
         else:
             assert not ba[i].any()
     assert_bits_equal(src, expect_src, "sources in insertion order")
+
+
+# ---- couple_bodies (world.rs:414-503) -----------------------------------------------------
+
+def test_static_body_blocks_fluid(oracle_mod):
+    """static_body_blocks_fluid (sph/tests.rs:96-129)."""
+    O = oracle_mod
+    w = O.OracleWorld(ref_test_params())
+    w.fill_box((-1.5, -1.5, -0.5), (1.5, -1.0, 0.5), 0.1, 0.05)
+    box = {"shape": "box", "size": (1.0, 0.5, 1.0), "pos": (0.0, 0.0, 0.0), "inv_mass": 0.0}
+    for _ in range(100):
+        w.step(DT)
+        w.couple_bodies([box], DT)
+    x = w.get(O.F_POS)
+    assert not np.any((np.abs(x[:, 0]) <= 1.0) & (np.abs(x[:, 1]) <= 0.5) & (np.abs(x[:, 2]) <= 1.0))
+
+
+def test_dynamic_body_gets_buoyancy_upward(oracle_mod):
+    """dynamic_body_gets_buoyancy_upward (sph/tests.rs:131-175): a sphere of a quarter of the
+    fluid's density, submerged, rises."""
+    O = oracle_mod
+    p = ref_test_params(gravity=(0.0, -9.81, 0.0))
+    w = O.OracleWorld(p, threads=O.max_threads())
+    w.fill_box((-0.7, -0.7, -0.7), (0.7, 0.7, 0.7), 0.1, 0.05)
+    w.step(DT, 15)
+    vol = 4.0 / 3.0 * np.pi * 0.6 ** 3
+    mass_b = p.rest_density * vol * 0.25
+    pos, vel = np.zeros(3), np.zeros(3)
+    g = np.array(p.gravity)
+    for _ in range(120):
+        vel = vel + g * DT
+        pos = pos + vel * DT
+        w.step(DT)
+        vel = w.couple_bodies([{"shape": "sphere", "size": (0.6,), "pos": pos, "vel": vel, "inv_mass": 1.0 / mass_b}],
+                              DT)[0]
+    assert pos[1] > 0.0
+
+
+def test_dynamic_contact_known_answer(oracle_mod):
+    """One particle moving into a dynamic box: the body takes -j inv_mass with
+    j = n * (-v_rel_n / (1/m + inv_mass)); the particle's own share is overwritten by the
+    push-out (the reference keeps push_out's velocity); the particle lands on the support
+    point and loses its inward normal velocity; buoyancy adds -g rho0 V_box dt inv_mass."""
+    O = oracle_mod
+    p = ref_test_params(gravity=(0.0, -9.81, 0.0))
+    w = O.OracleWorld(p)
+    m = 0.05
+    w.add_particles([[0.3, 0.1, 0.0]], [m], vel=[[-1.0, 0.5, 0.0]])
+    inv = 0.5
+    box = {"shape": "box", "size": (0.5, 0.4, 0.3), "pos": (0.0, 0.0, 0.0), "vel": (0.2, 0.0, 0.0), "inv_mass": inv}
+    vb = w.couple_bodies([box], DT)[0]
+    local = np.array([0.3, 0.1, 0.0])
+    n = local / np.sqrt((local[0] ** 2 + local[1] ** 2) + local[2] ** 2)
+    v_rel_n = np.dot(np.array([-1.0, 0.5, 0.0]) - np.array([0.2, 0.0, 0.0]), n)
+    j = n * (-(1.0 + 0.0) * v_rel_n / ((1.0 / m) + inv))
+    v_after = np.array([0.2, 0.0, 0.0]) + (-j) * inv
+    vol = 0.5 * 0.4 * 0.3 * 8.0
+    expect_vb = v_after + (-np.array(p.gravity) * (p.rest_density * vol) * DT) * inv
+    np.testing.assert_allclose(vb, expect_vb, rtol=1e-14, atol=1e-15)
+    assert_bits_equal(w.get(O.F_POS)[0], np.array([0.5, 0.4, 0.3]), "support point")  # dir > 0 on x, y; z >= 0
+    sd = np.array([0.5, 0.4, 0.3])
+    nn = sd / np.linalg.norm(sd)
+    v_rel = np.array([-1.0, 0.5, 0.0]) - v_after
+    vn = np.dot(v_rel, nn)
+    expect_v = np.array([-1.0, 0.5, 0.0]) - nn * vn if vn < 0 else np.array([-1.0, 0.5, 0.0])
+    np.testing.assert_allclose(w.get(O.F_VEL)[0], expect_v, rtol=1e-13, atol=1e-15)
+
+
+def test_rotated_static_box_pushes_out(oracle_mod):
+    """A box of half extents (1, 0.2, 0.2) turned 90 degrees about z contains (0.05, 0.8, 0.03)
+    (local (0.8, -0.05, 0.03)) and moves it to the turned support corner (1, -0.2, 0.2), i.e.
+    (0.2, 1, 0.2) in the world."""
+    O = oracle_mod
+    w = O.OracleWorld(ref_test_params(gravity=(0.0, 0.0, 0.0)))
+    w.add_particles([[0.05, 0.8, 0.03], [0.8, 0.0, 0.0]], [0.02, 0.02])
+    s = np.sqrt(0.5)
+    box = {"shape": "box", "size": (1.0, 0.2, 0.2), "pos": (0.0, 0.0, 0.0), "rot": (0.0, 0.0, s, s), "inv_mass": 0.0}
+    w.couple_bodies([box], DT)
+    x = w.get(O.F_POS)
+    np.testing.assert_allclose(x[0], [0.2, 1.0, 0.2], atol=1e-15)
+    assert_bits_equal(x[1], np.array([0.8, 0.0, 0.0]), "outside the turned box")
