@@ -57,6 +57,15 @@ def test_null_pointer_is_safe():
     lib.phy_world_destroy(None)
     assert lib.phy_fluid_len(None, 0) == -1
     assert lib.phy_fluid_step(None, 0, 0.01, 1) == -1
+    one = np.zeros(3)
+    assert lib.phy_fluid_couple_points(None, 0, 1, one.ctypes.data_as(L.DP), one.ctypes.data_as(L.DP),
+                                       one.ctypes.data_as(L.DP), one.ctypes.data_as(L.DP), 0.01, 1.0, 1000.0) == -1
+    assert lib.phy_fluid_couple_points(None, 0, 1, None, None, None, None, 0.01, 1.0, 1000.0) == -1
+    dims = (C.c_uint64 * 3)(1, 1, 1)
+    assert lib.phy_fluid_couple_heat(None, 0, dims, one.ctypes.data_as(L.DP), 1.0, one.ctypes.data_as(L.DP),
+                                     one.ctypes.data_as(L.DP), 0.01, 0.0, 0.0, 0.0) == -1
+    assert lib.phy_fluid_couple_heat(None, 0, None, None, 1.0, None, None, 0.01, 0.0, 0.0, 0.0) == -1
+    assert lib.phy_fluid_couple_bodies(None, 0, None, 1, None, 0, None, 0, 0.01, 0.0) == -1
     assert lib.phy_fluid_last_error()  # a message was recorded
 
 
