@@ -9,7 +9,7 @@
  * crates/phy-ffi/phy_ffi.h).  Signatures, argument meaning, return codes and
  * null-pointer behaviour are kept; the fluid mechanics behind them run as
  * CUDA kernels on the current device.  Worlds hold only fluid subsystems in
- * this build: the rigid / granular / soft / field / optics / solid factories
+ * this library: the rigid / granular / soft / field / optics / solid factories
  * and the rigid-body controls are exported with the reference's failure values
  * (NULL, -1, 0) so that existing binaries still link and fail cleanly.
  *
@@ -51,7 +51,7 @@ uint32_t phy_ffi_abi_version(void);
  * 0.18, 0.05) in one FluidSubsystem (phy-ffi/src/lib.rs:113-126, 209-214). */
 PhyWorldHandle *phy_world_create_fluid(void);
 
-/* Non-fluid factories: not part of this build, return NULL
+/* Non-fluid factories: not part of this library, return NULL
  * (phy-ffi/src/lib.rs:216-248, 299-328). */
 PhyWorldHandle *phy_world_create_rigid(void);
 PhyWorldHandle *phy_world_create_rigid_empty(void);
@@ -84,7 +84,7 @@ uintptr_t phy_world_get_fluid_positions(PhyWorldHandle *w, double *buf, uintptr_
 /* phy-ffi/src/lib.rs:431-460 */
 uintptr_t phy_world_get_fluid_velocities(PhyWorldHandle *w, double *buf, uintptr_t len);
 
-/* No rigid subsystems in this build: 0 (phy-ffi/src/lib.rs:462-515). */
+/* No rigid subsystems in this library: 0 (phy-ffi/src/lib.rs:462-515). */
 uintptr_t phy_world_rigid_count(PhyWorldHandle *w);
 uintptr_t phy_world_get_rigid_transforms(PhyWorldHandle *w, double *buf, uintptr_t len);
 

@@ -339,7 +339,7 @@ std::unique_ptr<World> load_world_json(const std::string& json) {
     const JVal* fl = sv.get("Fluid");
     if (!fl) {
       std::string tag = sv.obj.empty() ? std::string("?") : sv.obj[0].first;
-      throw std::runtime_error("archive: subsystem '" + tag + "' is not part of this build");
+      throw std::runtime_error("archive: subsystem '" + tag + "' is not part of this library");
     }
     const JVal& wv = fl->at("world");
     SphParams params = read_params(wv.at("params"));

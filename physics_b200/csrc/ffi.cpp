@@ -116,7 +116,7 @@ PhyWorldHandle* phy_world_create_fluid(void) {
 }
 
 static PhyWorldHandle* not_in_build(const char* what) {
-  g_last_error = std::string(what) + ": this build holds fluid subsystems only";
+  g_last_error = std::string(what) + ": this library holds fluid subsystems only";
   return nullptr;
 }
 PhyWorldHandle* phy_world_create_rigid(void) { return not_in_build("rigid world"); }
@@ -201,7 +201,7 @@ void phy_world_destroy(PhyWorldHandle* w) {
 }
 
 int64_t phy_world_rigid_add_body(PhyWorldHandle*, int32_t, double, const double*, const double*) {
-  g_last_error = "rigid bodies: this build holds fluid subsystems only";
+  g_last_error = "rigid bodies: this library holds fluid subsystems only";
   return -1;
 }
 int32_t phy_world_rigid_apply_force(PhyWorldHandle*, int64_t, const double*, double, int32_t) { return -1; }

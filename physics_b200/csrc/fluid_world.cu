@@ -1501,7 +1501,7 @@ int FluidSubsystem::validate() {
 void World::step(double dt) {
   for (auto& s : subs) s->world->step(dt);
   // Coupling stage (subsystem.rs:92-143) needs a HeatField or a
-  // RigidSubsystem; worlds of this build hold fluid subsystems only, so it
+  // RigidSubsystem; worlds of this library hold fluid subsystems only, so it
   // has nothing to couple.
   t += dt;
 }
