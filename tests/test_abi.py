@@ -91,3 +91,31 @@ def test_params_defaults_match_reference():
 
 def test_params_struct_layout():
     assert C.sizeof(L.PhySphParams) == 8 * 17 + 8 + 2 * 8 * 16
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors of PhySphParams and PhyCoupleBody have the C header's sizes and
+    field offsets (compiled here with the system C compiler)."""
+    import shutil
+    import subprocess
+    import pytest
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        pytest.skip("no C compiler")
+    checks = {"PhySphParams": L.PhySphParams, "PhyCoupleBody": L.PhyCoupleBody}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "phy_fluid.h"', "int main(void) {"]
+    for name, st in checks.items():
+        lines.append(f'  printf("{name} size %zu\\n", sizeof({name}));')
+        for f, _ in st._fields_:
+            lines.append(f'  printf("{name} {f} %zu\\n", offsetof({name}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", str(INCLUDE), str(src), "-o", str(exe)], check=True)
+    got = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    want = []
+    for name, st in checks.items():
+        want.append(f"{name} size {C.sizeof(st)}")
+        want += [f"{name} {f} {getattr(st, f).offset}" for f, _ in st._fields_]
+    assert [g for g in got if g] == want
