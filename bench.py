@@ -487,6 +487,10 @@ def run_ours(args):
     ms_e2e = max_over_ranks(f0.elapsed_time(f1))
     e2e_value = world_size * n * ke / (ms_e2e / 1e3)
 
+    coupling = None
+    if not args.no_coupling and world_size == 1:
+        coupling = run_coupling(pb, scenes, comp, n)
+
     hbm_peak, peak_kind = peaks()
     force_ms = ph_comp["force"]
     achieved = FORCE_BYTES["comp"] * n / (force_ms / 1e3) / 1e9
@@ -551,12 +555,75 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "batched": batched,
             "adjoint": adjoint,
+            "coupling": coupling,
         }
         print(json.dumps(line), flush=True)
     if world_size > 1:
         dist.barrier()
         dist.destroy_process_group()
     return line
+
+
+def run_coupling(pb, scenes, w, n: int) -> dict:
+    """The fluid's coupling calls on the 4M state (after the timed steps), each timed by the
+    host clock around the call (every call synchronises; the grid / point / body transfers
+    are inside), next to the oracle on the 524,288-particle block of the same recipe."""
+    from oracle import oracle as O
+    O.build()
+    rng = np.random.default_rng(17)
+    dims = (64, 128, 64)  # heat grid: 0.2-cells over the 12.8 x 25.6 x 12.8 block
+    temp = rng.uniform(0.0, 1.0, dims[::-1])
+    src = np.zeros_like(temp)
+    pts = rng.uniform((0.5, 0.5, 0.5), (12.3, 25.1, 12.3), (4096, 3))
+    pvel = rng.normal(0.0, 0.2, pts.shape)
+    pmass = np.full(len(pts), 0.02)
+    centres = rng.uniform((1.0, 1.0, 1.0), (11.8, 24.6, 11.8), (8, 3))
+    bodies = [{"shape": "sphere", "size": (0.5,), "pos": tuple(c), "vel": (0.0, -0.5, 0.0), "inv_mass": 0.01}
+              for c in centres]
+
+    def wall(fn, reps=3):
+        fn()  # allocations
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        return (time.perf_counter() - t0) / reps
+
+    t_heat = wall(lambda: w.couple_heat(temp, src, (0.0, 0.0, 0.0), 0.2, DT, 0.5, 2e-4, 0.1))
+    t_pts = wall(lambda: w.couple_points(pts, pvel, pmass, DT, 1.0, 1000.0))
+    t_bod = wall(lambda: w.couple_bodies(bodies, DT))
+    # The oracle on the 64 x 128 x 64 block (a quarter of each extent's particles, same spacing).
+    sdims = (64, 128, 64)
+    spos = scenes.dam_break_positions(*sdims)
+    p = pb.SphParams.defaults()
+    p.bounds_min, p.bounds_max = (0.0, 0.0, 0.0), (BOX, BOX, BOX)
+    ow = O.OracleWorld(p)
+    ow.add_particles(spos, scenes.lattice_mass(0.1))
+    ns = spos.shape[0]
+    sgrid = (32, 64, 32)
+    stemp = rng.uniform(0.0, 1.0, sgrid[::-1])
+    spts = rng.uniform((0.5, 0.5, 0.5), (5.9, 12.3, 5.9), (1024, 3))
+    sbodies = [dict(b, pos=tuple(np.asarray(b["pos"]) * 0.5)) for b in bodies[:4]]
+    t0 = time.perf_counter()
+    ow.couple_heat(stemp, np.zeros_like(stemp), (0.0, 0.0, 0.0), 0.2, DT, 0.5, 2e-4, 0.1)
+    c_heat = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ow.couple_points(spts, np.zeros_like(spts), np.full(len(spts), 0.02), DT, 1.0, 1000.0)
+    c_pts = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ow.couple_bodies(sbodies, DT)
+    c_bod = time.perf_counter() - t0
+    return {
+        "workload": f"dam_break_128x256x128 state ({n} particles) after the timed steps; heat grid "
+                    f"{dims[0]}x{dims[1]}x{dims[2]} of 0.2 with sources; 4096 points; 8 spheres r=0.5; host-clock "
+                    f"time per call including transfers",
+        "couple_heat": {"ms": t_heat * 1e3, "particles_per_s": n / t_heat,
+                        "cpu_particles_per_s": ns / c_heat},
+        "couple_points": {"ms": t_pts * 1e3, "points_per_s": len(pts) / t_pts,
+                          "cpu_points_per_s": len(spts) / c_pts},
+        "couple_bodies": {"ms": t_bod * 1e3, "particles_per_s": n / t_bod, "cpu_particles_per_s": ns / c_bod},
+        "cpu_sample": f"oracle, one thread: {sdims[0]}x{sdims[1]}x{sdims[2]} block ({ns} particles), heat grid "
+                      f"{sgrid[0]}x{sgrid[1]}x{sgrid[2]}, 1024 points, 4 spheres",
+    }
 
 
 def _oracle_sample(scenes, pb, n_target: int):
@@ -637,6 +704,8 @@ def main():
     ap.add_argument("--adjoint-directions", type=int, default=32,
                     help="finite-difference directions of the adjoint check (0: skip the adjoint)")
     ap.add_argument("--batch-steps", type=int, default=200, help="timed steps of the batched form")
+    ap.add_argument("--no-coupling", action="store_true", help="skip the coupling calls (couple_heat / _points / "
+                    "_bodies)")
     ap.add_argument("--full-steps", type=int, default=1000,
                     help="also time this many steps from the initial dam (the configured 1000-step run; "
                          "the column compresses and splashes, so per-step cost changes along it); 0 = skip")

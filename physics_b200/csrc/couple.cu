@@ -59,26 +59,33 @@ __global__ void __launch_bounds__(kCT) k_couple_points(StepConsts c, CoupleArgs 
   const int t = threadIdx.x;
   for (int k = 0; k < a.np; ++k) {
     double* q = a.pts + 10 * (size_t)k;
-    if (t == 0) {
+    if (t < 32) {
+      // Warp 0: lane u < 27 reads cell u of the visit order (u = 9 (di+1) +
+      // 3 (dj+1) + (dk+1)); a shuffle scan gives the cells' first candidates.
       const double x = q[0], y = q[1], z = q[2];
       // world.rs:704-711 (a NaN coordinate passes, as there).
       const bool in = !(x < c.lo[0] || x > c.hi[0] || y < c.lo[1] || y > c.hi[1] || z < c.lo[2] || z > c.hi[2]);
-      s_in = in ? 1 : 0;
+      if (t == 0) s_in = in ? 1 : 0;
       if (in) {
         const long long kx = key_axis(x, c.inv_cell), ky = key_axis(y, c.inv_cell), kz = key_axis(z, c.inv_cell);
-        uint32_t acc = 0;
-        int u = 0;
-        for (int di = -1; di <= 1; ++di)
-          for (int dj = -1; dj <= 1; ++dj)
-            for (int dk = -1; dk <= 1; ++dk, ++u) {
-              const int lin = cell_linear(c, kx + di, ky + dj, kz + dk);
-              const uint32_t beg = lin >= 0 ? a.cell_start[lin] : 0u;
-              const uint32_t cnt = lin >= 0 ? a.cell_start[lin + 1] - beg : 0u;
-              s_beg[u] = beg;
-              s_pre[u] = acc;
-              acc += cnt;
-            }
-        s_pre[27] = acc;
+        uint32_t beg = 0, cnt = 0;
+        if (t < 27) {
+          const int lin = cell_linear(c, kx + t / 9 - 1, ky + (t / 3) % 3 - 1, kz + t % 3 - 1);
+          if (lin >= 0) {
+            beg = a.cell_start[lin];
+            cnt = a.cell_start[lin + 1] - beg;
+          }
+        }
+        uint32_t incl = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (t >= o) incl += y;
+        }
+        if (t < 27) {
+          s_beg[t] = beg;
+          s_pre[t] = incl - cnt;
+        }
+        if (t == 26) s_pre[27] = incl;
       }
     }
     __syncthreads();
