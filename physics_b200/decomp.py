@@ -1,0 +1,225 @@
+"""Spatial decomposition of one scene into x-slabs of grid cells, bit-identical to stepping
+the whole scene in one world (no counterpart in the reference, which steps one world).
+
+A step of FluidWorld<f64> (phy-fluid/src/sph/world.rs:183-397) gives particle i a density
+from the particles of the 27 cells around its own (grid.rs:43-56) and a force from those
+particles' densities, so its new state depends on particles at most two cells away along
+each axis.  Slab r owns the particles whose cell key x lies in [lo_r, hi_r); its world holds
+them plus every particle with a key in [lo_r - 2, lo_r) or [hi_r, hi_r + 2) (the halo),
+inserted in ascending global insertion index.  Inside a cell the grid visits particles in
+insertion order, so every sum of an owned particle runs over the same terms in the same
+order as in the whole world, and the owned particles' results are the same bits; the halo's
+results are dropped.  Ownership is recomputed from the new positions before every step
+(particles migrate between slabs), with slab edges that balance the particle counts.
+
+`SlabStepper` runs the slabs in one process (each slab's world may live on its own device);
+`RankSlabStepper` gives each rank of a torch.distributed group one slab and exchanges the
+halo and the migrating particles with point-to-point messages (gloo or NCCL).  A world is
+made by a factory returning an adapter with add(pos, vel, mass, material), step(dt) and
+read() -> {field: array in insertion order}; `DeviceWorld` adapts FluidWorld.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+HALO = 2  # cells of halo on each side of a slab
+FIELDS = ("pos", "vel", "rho", "p", "acc", "mu_eff", "xsph")
+
+
+def key_x(pos: np.ndarray, h0: float) -> np.ndarray:
+    """Grid::key_of along x (grid.rs:25-33): floor(x * (1/h0)) as i64, 0 when not
+    representable (non-finite or out of range)."""
+    f = np.floor(pos[:, 0] * (1.0 / h0))
+    ok = np.isfinite(f) & (f > -9.223372036854775808e18) & (f < 9.223372036854775808e18)
+    out = np.zeros(len(f), np.int64)
+    out[ok] = f[ok].astype(np.int64)
+    return out
+
+
+I64_MIN, I64_MAX = -(1 << 63), (1 << 63) - 1
+
+
+def slab_edges_from_counts(uniq: np.ndarray, counts: np.ndarray, nslabs: int) -> list:
+    """nslabs + 1 key edges (Python ints; the first and last span the whole int64 range)
+    splitting keys, given as distinct values with their counts, into slabs of about equal
+    particle counts: edge r is the key at rank r * total / nslabs of the sorted keys.
+    Deterministic and strictly increasing."""
+    order = np.argsort(uniq, kind="stable")
+    uniq, counts = np.asarray(uniq)[order], np.asarray(counts, np.int64)[order]
+    cum = np.cumsum(counts)
+    total = int(cum[-1]) if len(cum) else 0
+    edges = [I64_MIN]
+    for r in range(1, nslabs):
+        e = int(uniq[int(np.searchsorted(cum, (r * total) // nslabs, side="right"))]) if total else 0
+        edges.append(max(e, edges[-1] + 1))
+    edges.append(I64_MAX)
+    return edges
+
+
+def slab_edges(keys: np.ndarray, nslabs: int) -> list:
+    """slab_edges_from_counts of a key array."""
+    uniq, counts = np.unique(keys, return_counts=True)
+    return slab_edges_from_counts(uniq, counts, nslabs)
+
+
+def slab_mask(keys: np.ndarray, lo: int, hi: int, halo: int = 0) -> np.ndarray:
+    """keys in [lo - halo, hi + halo), the bounds clamped to the int64 range."""
+    return (keys >= max(lo - halo, I64_MIN)) & (keys < min(hi + halo, I64_MAX))
+
+
+class DeviceWorld:
+    """Adapter of a device FluidWorld (physics_b200.FluidWorld) for the steppers."""
+
+    def __init__(self, params, precision: str = "f64"):
+        from .fluid import FluidWorld
+        self.w = FluidWorld(params, precision)
+
+    def add(self, pos, vel, mass, material):
+        if len(mass):
+            self.w.add_particles(pos, mass, vel=vel, material=material)
+
+    def step(self, dt: float):
+        self.w.step(dt)
+
+    def read(self) -> dict:
+        return {f: getattr(self.w, f) for f in FIELDS}
+
+
+def _step_slab(make_world, state: dict, local: np.ndarray, own_in_local: np.ndarray, dt: float) -> dict:
+    """Steps the particles `local` (ascending insertion index) in a fresh world and returns
+    the fields of those flagged by own_in_local."""
+    w = make_world()
+    w.add(state["pos"][local], state["vel"][local], state["mass"][local], state["material"][local])
+    w.step(dt)
+    out = w.read()
+    return {f: np.asarray(out[f])[own_in_local] for f in FIELDS}
+
+
+class SlabStepper:
+    """All slabs in one process; the state is kept in insertion order."""
+
+    def __init__(self, make_world, h0: float, nslabs: int, pos, mass, vel=None, material=None):
+        n = len(pos)
+        self.make_world, self.h0, self.nslabs = make_world, h0, nslabs
+        self.state = {
+            "pos": np.array(pos, np.float64).reshape(n, 3),
+            "vel": np.zeros((n, 3)) if vel is None else np.array(vel, np.float64).reshape(n, 3),
+            "mass": np.broadcast_to(np.asarray(mass, np.float64), (n,)).copy(),
+            "material": np.zeros(n, np.uint32) if material is None else np.asarray(material, np.uint32).copy(),
+        }
+        for f in FIELDS[2:]:
+            self.state[f] = np.zeros((n, 3) if f in ("acc", "xsph") else n)
+        self.edges = None
+
+    def step(self, dt: float, n: int = 1):
+        for _ in range(n):
+            s = self.state
+            k = key_x(s["pos"], self.h0)
+            self.edges = e = slab_edges(k, self.nslabs)
+            new = {f: s[f].copy() for f in FIELDS}
+            for r in range(self.nslabs):
+                own = slab_mask(k, e[r], e[r + 1])
+                if not own.any():
+                    continue
+                local = np.flatnonzero(slab_mask(k, e[r], e[r + 1], HALO))
+                res = _step_slab(self.make_world, s, local, own[local], dt)
+                ids = local[own[local]]
+                for f in FIELDS:
+                    new[f][ids] = res[f]
+            s.update(new)
+
+
+class RankSlabStepper:
+    """One slab per rank of the default torch.distributed group.  Each rank keeps the
+    particles it owns (with their insertion indices); before a step the ranks agree on the
+    slab edges from the gathered key counts, then every rank sends each other rank the
+    particles that rank owns or needs as halo."""
+
+    def __init__(self, make_world, h0: float, ids, pos, mass, vel=None, material=None):
+        import torch.distributed as dist
+        self.dist = dist
+        self.rank, self.size = dist.get_rank(), dist.get_world_size()
+        n = len(ids)
+        self.make_world, self.h0 = make_world, h0
+        self.ids = np.asarray(ids, np.int64)
+        self.state = {
+            "pos": np.array(pos, np.float64).reshape(n, 3),
+            "vel": np.zeros((n, 3)) if vel is None else np.array(vel, np.float64).reshape(n, 3),
+            "mass": np.broadcast_to(np.asarray(mass, np.float64), (n,)).copy(),
+            "material": np.zeros(n, np.uint32) if material is None else np.asarray(material, np.uint32).copy(),
+        }
+        for f in FIELDS[2:]:
+            self.state[f] = np.zeros((n, 3) if f in ("acc", "xsph") else n)
+
+    def _gather(self, obj):
+        out = [None] * self.size
+        self.dist.all_gather_object(out, obj)
+        return out
+
+    def step(self, dt: float, n: int = 1):
+        for _ in range(n):
+            s = self.state
+            k = key_x(s["pos"], self.h0)
+            # Slab edges from all ranks' distinct keys and counts (one entry per cell column;
+            # every rank computes the same edges).
+            parts = self._gather(np.unique(k, return_counts=True))
+            uniq, inv = np.unique(np.concatenate([u for u, _ in parts]), return_inverse=True)
+            counts = np.zeros(len(uniq), np.int64)
+            np.add.at(counts, inv, np.concatenate([c for _, c in parts]))
+            e = slab_edges_from_counts(uniq, counts, self.size)
+            # Outgoing: for each rank, the particles it owns or needs as halo.
+            packets = []
+            for r in range(self.size):
+                sel = slab_mask(k, e[r], e[r + 1], HALO)
+                packets.append({"ids": self.ids[sel], "key": k[sel],
+                                **{f: s[f][sel] for f in ("pos", "vel", "mass", "material")}})
+            inbox = self._exchange(packets)
+            ids = np.concatenate([p["ids"] for p in inbox])
+            order = np.argsort(ids, kind="stable")  # ascending insertion index
+            merged = {f: np.concatenate([p[f] for p in inbox])[order]
+                      for f in ("pos", "vel", "mass", "material", "key")}
+            ids = ids[order]
+            own = slab_mask(merged["key"], e[self.rank], e[self.rank + 1])
+            if own.any():
+                res = _step_slab(self.make_world, merged, np.arange(len(ids)), own, dt)
+            else:
+                res = {f: np.zeros((0, 3) if f in ("pos", "vel", "acc", "xsph") else 0) for f in FIELDS}
+            self.ids = ids[own]
+            self.state = {"mass": merged["mass"][own], "material": merged["material"][own], **res}
+
+    def _exchange(self, packets):
+        """packets[r] goes to rank r; returns the packets received from every rank in rank
+        order (this rank's own packet included).  Point to point: a length message, then
+        the pickled packet, to and from every other rank."""
+        import pickle
+
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device()) if self.dist.get_backend() == "nccl" else "cpu"
+        blobs = [torch.frombuffer(bytearray(pickle.dumps(p)), dtype=torch.uint8).to(dev) for p in packets]
+        lens_out = {r: torch.tensor([blobs[r].numel()], dtype=torch.int64, device=dev) for r in range(self.size)}
+        lens_in = {r: torch.zeros(1, dtype=torch.int64, device=dev) for r in range(self.size)}
+        reqs = []
+        for r in range(self.size):
+            if r != self.rank:
+                reqs.append(self.dist.isend(lens_out[r], r))
+                reqs.append(self.dist.irecv(lens_in[r], r))
+        for q in reqs:
+            q.wait()
+        bufs = {r: torch.empty(int(lens_in[r].item()), dtype=torch.uint8, device=dev) for r in range(self.size)
+                if r != self.rank}
+        reqs = []
+        for r in range(self.size):
+            if r != self.rank:
+                reqs.append(self.dist.isend(blobs[r], r))
+                reqs.append(self.dist.irecv(bufs[r], r))
+        for q in reqs:
+            q.wait()
+        return [packets[r] if r == self.rank else pickle.loads(bufs[r].cpu().numpy().tobytes())
+                for r in range(self.size)]
+
+    def gather_state(self):
+        """The whole state in insertion order (on every rank)."""
+        parts = self._gather((self.ids, self.state))
+        ids = np.concatenate([p[0] for p in parts])
+        order = np.argsort(ids, kind="stable")
+        return ids[order], {f: np.concatenate([p[1][f] for p in parts])[order] for f in parts[0][1]}
