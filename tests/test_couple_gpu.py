@@ -200,7 +200,8 @@ TETRA = {"verts": (np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], 
 
 def _bodies(shift=0.0):
     return [
-        {"shape": "sphere", "size": (0.22,), "pos": (0.15 + shift, 0.0, 0.05), "vel": (0.0, -0.4, 0.1), "inv_mass": 2.0},
+        {"shape": "sphere", "size": (0.22,), "pos": (0.15 + shift, 0.0, 0.05), "vel": (0.0, -0.4, 0.1),
+         "inv_mass": 2.0},
         {"shape": "box", "size": (0.3, 0.12, 0.2), "pos": (-0.25, 0.2, 0.0), "rot": _quat((1, 2, 3), 0.7),
          "inv_mass": 0.0},
         {"shape": "capsule", "size": (0.15, 0.1), "pos": (0.0, -0.3, -0.25), "rot": _quat((0, 0, 1), 1.1),
