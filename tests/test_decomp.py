@@ -83,6 +83,22 @@ def test_one_cell_halo_is_not_enough(oracle_mod, monkeypatch):
     assert not np.array_equal(st.state["acc"], ref["acc"])
 
 
+def test_more_slabs_than_columns_and_a_nan_particle(oracle_mod):
+    """Twelve slabs over a block five cell columns wide (most slabs own nothing), and a
+    particle whose x is NaN (its cell key is 0 on that axis, as Grid::key_of gives it):
+    still the whole world's bits."""
+    O = oracle_mod
+    sc, p, vel, mat = _scene(seed=8)
+    pos = sc.pos.copy()
+    pos[17, 0] = np.nan
+    st = decomp.SlabStepper(lambda: OracleSlabWorld(O, p), p.h, 12, pos, sc.mass, vel=vel, material=mat)
+    st.step(DT, 5)
+    from types import SimpleNamespace
+    ref = _whole(lambda: OracleSlabWorld(O, p), SimpleNamespace(n=sc.n, mass=sc.mass, pos=pos), vel, mat, 5)
+    for f in decomp.FIELDS:
+        assert_bits_equal(st.state[f], ref[f], f"{f}, 12 slabs with a NaN particle")
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
