@@ -19,8 +19,13 @@ instead (its "batched" block: the whole batch's particle-steps over the max
 over ranks).
 
 --impl reference times the CPU restatement of the reference's rayon step
-(oracle/, OpenMP over all host threads) on a bounded sub-block of the same
-scene; the Rust reference itself cannot be built here.
+(oracle/, OpenMP over all host threads) on the same 4,194,304-particle scene,
+without loading the product library; the Rust reference itself cannot be
+built here.
+
+Output: auxiliary blocks first, one JSON object per line with a "block" key
+(precision errors along the trajectory, full trajectory, readback, batched,
+adjoint, coupling); the headline object is the last line.
 """
 from __future__ import annotations
 
@@ -56,12 +61,17 @@ FORCE_BYTES = {"f64": 188, "comp": 200}
 # traffic grows with the particle count, so a full launch is scaled by it.
 FORCE_TRAFFIC_PER_PARTICLE = (238.917888e6 + 80.918784e6) / 1024000
 # Kernels one compensated step launches: the sort (cell histogram, 3-kernel
-# cell scan, scatter, in-cell order, gather), the occupied-tile list (heads,
-# 3-kernel scan, emit) and the passes (tiled and dense-cell density, tiled and
-# dense-cell force).
-LAUNCHES_PER_STEP = 7 + 5 + 4
-# Whole-step compulsory state traffic (f64 pos, vel, mass in; pos, vel, rho, p out).
+# cell scan, scatter, in-cell order of small and of large cells, gather), the
+# occupied-tile list (heads, 3-kernel scan, emit) and the passes (tiled and
+# dense-cell density, tiled and dense-cell force).
+LAUNCHES_PER_STEP = 8 + 5 + 4
+# Whole-step compulsory state traffic (f64 pos, vel, mass in; pos, vel, rho, p out):
+# the algorithmic bytes of one particle-step.
 STEP_BYTES = 120
+# Steps of the configured 1000-step trajectory at which the compensated form's
+# per-output errors are probed (teacher-forced from that state), the last one in
+# the collapsed regime.
+PROBE_FRACTIONS = (0.0, 0.25, 0.5, 0.75, 1.0)
 
 
 def env_int(name, default):
@@ -124,6 +134,15 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def bench_config(dims, n: int, world_size: int) -> dict:
+    """The workload both arms run (the precision of each arm is its line's dtype)."""
+    return {"workload": f"dam_break_{dims[0]}x{dims[1]}x{dims[2]}: {n} particles, spacing 0.1 = h/2, "
+                        f"bounds [0,{BOX}]^3, dt={DT}",
+            "particles": n,
+            "parallelism": f"replicas x{world_size}",
+            "l2": "inputs larger than L2 (state ~1.4 GB per replica)"}
+
+
 def make_params(pb):
     p = pb.SphParams.defaults()
     p.bounds_min, p.bounds_max = (0.0, 0.0, 0.0), (BOX, BOX, BOX)
@@ -160,9 +179,11 @@ def run_batched(pb, scenes, stream, n_scenes: int, steps: int, warmup: int, rank
     w.set_scenes(counts, [b.bounds_min for b in batch], [b.bounds_max for b in batch])
     w.set_tuning(graph_chunk=BATCH_CHUNK)
     t0 = time.time()
-    trials = w.autotune(BATCH_DT, BATCH_CHUNK)
+    # Tuned over the run ahead: the states at 0, steps/2 and steps steps.
+    trials = w.autotune(BATCH_DT, BATCH_CHUNK, horizon=steps)
     tune_s = time.time() - t0
     chosen = w.tuning()
+    finalists = [t for t in trials if t["samples"] == max(t["samples"] for t in trials)]
 
     def timed(fn, k):
         barrier()
@@ -219,10 +240,12 @@ def run_batched(pb, scenes, stream, n_scenes: int, steps: int, warmup: int, rank
         "loop_single_scene_value": loop_value,
         "loop_single_scene_ms_per_step": ms_loop / steps,
         "speedup_vs_loop": value / loop_value,
-        "tuning": {k: chosen[k] for k in ("ctas_per_sm", "queue", "sort_block", "graph_chunk")},
-        "autotune": {"trials": len(trials), "seconds": tune_s,
-                     "best_ms_per_step": min(t["ms_per_step"] for t in trials),
-                     "worst_ms_per_step": max(t["ms_per_step"] for t in trials)},
+        "tuning": {k: chosen[k] for k in ("comp_tile", "ctas_per_sm", "queue", "sort_block", "graph_chunk")},
+        "autotune": {"trials": len(trials), "finalists": len(finalists), "horizon_steps": steps,
+                     "seconds": tune_s,
+                     "best_ms_per_step": min(t["ms_per_step"] for t in finalists),
+                     "worst_finalist_ms_per_step": max(t["ms_per_step"] for t in finalists),
+                     "best_over_timed": min(t["ms_per_step"] for t in finalists) / (ms / steps)},
     }
 
 
@@ -332,6 +355,39 @@ def run_adjoint(pb, scenes, stream, directions: int) -> dict:
     }
 
 
+def probe_errors(pb, new_world, w, n: int, params) -> dict:
+    """Per-output error of one FP32-compensated step against one f64 plain step (itself
+    bit-identical to the f64 oracle), both started from the state of world `w`
+    (teacher-forced): density and acceleration (the force per unit density,
+    world.rs:332-336) as max relative / max-normalised errors, pressure normalised by
+    k*rho0 (p is ~0 near rest), position and velocity after the step."""
+    pos, vel = w.pos.copy(), w.vel.copy()
+    plain = new_world("f64", pos, vel)
+    comp = new_world("comp", pos, vel)
+    plain.step(DT)
+    comp.step(DT)
+    rp, rc = plain.rho, comp.rho
+    live = np.abs(rp) > 0
+    ap, ac = plain.acc, comp.acc
+    amag = np.linalg.norm(ap, axis=1)
+    aerr = np.linalg.norm(ac - ap, axis=1)
+    amax = float(amag.max()) if n else 0.0
+    big = amag > 1e-3 * amax
+    xp, xc = plain.pos, comp.pos
+    vp, vc = plain.vel, comp.vel
+    vmax = float(np.linalg.norm(vp, axis=1).max())
+    out = {
+        "density_max_rel": float(np.max(np.abs(rc[live] - rp[live]) / np.abs(rp[live]))),
+        "pressure_max_norm": float(np.max(np.abs(comp.p - plain.p)) / (params.stiffness * params.rest_density)),
+        "acc_max_norm": float(aerr.max() / amax) if amax > 0 else 0.0,
+        "acc_median_rel": float(np.median(aerr[big] / amag[big])) if big.any() else 0.0,
+        "pos_max_abs_m": float(np.max(np.abs(xc - xp))),
+        "vel_max_norm": float(np.max(np.linalg.norm(vc - vp, axis=1)) / vmax) if vmax > 0 else 0.0,
+    }
+    del plain, comp
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -357,6 +413,10 @@ def run_ours(args):
         t = torch.tensor([x], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    def emit(block: str, obj) -> None:
+        if rank == 0 and obj is not None:
+            print(json.dumps({"block": block, **obj}), flush=True)
 
     K, W = args.steps, args.warmup
     dims = tuple(args.dims)
@@ -412,57 +472,62 @@ def run_ours(args):
     k_plain = max(3, K // 4)
     ms_plain, _, ph_plain = timed(plain, k_plain, max(3, W // 2), phase=True)
     plain_value = world_size * n * k_plain / (ms_plain / 1e3)
+    del plain
 
-    # ---- density error of the compensated form vs f64 plain (teacher-forced step) ----
-    state_pos, state_vel = plain.pos.copy(), plain.vel.copy()
-    probe = new_world("comp", state_pos, state_vel)
-    plain.step(DT)
-    probe.step(DT)
-    rho_ref, rho_c = plain.rho, probe.rho
-    dens_err = float(np.max(np.abs(rho_c - rho_ref) / np.abs(rho_ref)))
-    p_err = float(np.max(np.abs(probe.p - plain.p)) / (params.stiffness * params.rest_density))
-    del probe
-
-    # ---- the full configured trajectory (1000 steps from the initial dam) ---------------
-    full = None
-    traj = None
-    if args.full_steps > 0:
-        traj = new_world("comp")
-        ms_full, _, _ = timed(traj, args.full_steps, 0)
-        full = {"steps": args.full_steps, "value": world_size * n * args.full_steps / (ms_full / 1e3),
-                "ms_per_step": ms_full / args.full_steps}
-
-    # ---- per-kernel device times (CUDA events on the launch stream) ----------------
-    def phases(w, steps):
-        w.set_timing(True)
-        w.phase_times(reset=True)
-        w.step(DT, steps)
-        t = w.phase_times(reset=True)
-        w.set_timing(False)
-        s = max(t["steps"], 1)
-        return {k: t[k] / s for k in ("sort", "prep", "density", "force")}
-
-    if traj is not None:
-        full["phase_ms_at_end"] = phases(traj, 20)
-        traj.set_counting(True)
-        traj.step(DT)
-        tc = traj.step_counters()
-        full["pairs_per_particle_at_end"] = tc["pairs"] / n
-        traj.set_counting(False)
-        del traj
     comp.set_counting(True)
     comp.step(DT)
     cnt = comp.step_counters()
     comp.set_counting(False)
 
+    # ---- the configured 1000-step trajectory, with per-output error probes ------------
+    # Timed in segments between probe points (CUDA events around each segment); a
+    # probe reads the state and steps an f64 plain and a compensated world from it
+    # outside the timed segments.
+    full, errors = None, None
+    if args.full_steps > 0:
+        traj = new_world("comp")
+        probes = sorted({min(int(round(f * args.full_steps)), args.full_steps - 1) for f in PROBE_FRACTIONS})
+        errors = {"workload": f"teacher-forced: one f32c step and one f64 plain step from the state of the "
+                              f"{args.full_steps}-step trajectory at each listed step",
+                  "reference": "f64 plain step (bit-identical to the f64 oracle)", "at_step": {}}
+        done, ms_full = 0, 0.0
+        for s_probe in probes + [args.full_steps]:
+            seg = s_probe - done
+            if seg > 0:
+                ms_seg, _, _ = timed(traj, seg, 0)
+                ms_full += ms_seg
+                done = s_probe
+            if s_probe < args.full_steps and rank == 0:
+                errors["at_step"][str(s_probe)] = probe_errors(pb, new_world, traj, n, params)
+        full = {"steps": args.full_steps, "value": world_size * n * args.full_steps / (ms_full / 1e3),
+                "ms_per_step": ms_full / args.full_steps}
+        traj.set_timing(True)
+        traj.phase_times(reset=True)
+        traj.step(DT, 20)
+        t = traj.phase_times(reset=True)
+        traj.set_timing(False)
+        full["phase_ms_at_end"] = {k: t[k] / max(t["steps"], 1) for k in ("sort", "prep", "density", "force")}
+        traj.set_counting(True)
+        traj.step(DT)
+        full["pairs_per_particle_at_end"] = traj.step_counters()["pairs"] / n
+        traj.set_counting(False)
+        del traj
+        if rank == 0:
+            at = errors["at_step"].values()
+            errors["max_over_probes"] = {k: max(e[k] for e in at) for k in next(iter(at))}
+    emit("precision_errors", errors)
+    emit("full_trajectory", full)
+
     adjoint = None
     if args.adjoint_directions > 0:
         adjoint = run_adjoint(pb, scenes, stream, args.adjoint_directions)
+    emit("adjoint", adjoint)
 
     batched = None
     if args.batch_scenes > 0 and args.batch_steps > 0:
         batched = run_batched(pb, scenes, stream, args.batch_scenes, args.batch_steps, W, rank, world_size,
                               max_over_ranks, barrier)
+    emit("batched", batched)
 
     # ---- end to end through the C ABI with host buffers ------------------------------
     pin_pos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
@@ -487,18 +552,25 @@ def run_ours(args):
     ms_e2e = max_over_ranks(f0.elapsed_time(f1))
     e2e_value = world_size * n * ke / (ms_e2e / 1e3)
 
+    emit("readback", run_readback(pb, comp, n))
+
     coupling = None
     if not args.no_coupling and world_size == 1:
         coupling = run_coupling(pb, scenes, comp, n)
+    emit("coupling", coupling)
 
     hbm_peak, peak_kind = peaks()
     force_ms = ph_comp["force"]
-    achieved = FORCE_BYTES["comp"] * n / (force_ms / 1e3) / 1e9
     step_ms = ms_comp / K
+    # Roofline of the dominant kernel against HBM with the whole step's algorithmic
+    # bytes (120 B per particle-step) over the force pass's own event time.
+    achieved = STEP_BYTES * n / (force_ms / 1e3) / 1e9
+    step_gbs = STEP_BYTES * n / (step_ms / 1e3) / 1e9
 
     line = None
     if rank == 0:
-        cpu = None if (args.no_cpu or world_size > 1) else cpu_baseline(scenes, pb)
+        cpu = None if (args.no_cpu or world_size > 1) else cpu_baseline(scenes, pb, n, dims)
+        err_max = errors["max_over_probes"] if errors else None
         line = {
             "metric": METRIC,
             "value": value,
@@ -512,56 +584,68 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "f32c/f64",
             "data": "synthetic (seeded jittered dam-break lattice)",
-            "config": {
-                "workload": f"dam_break_{dims[0]}x{dims[1]}x{dims[2]}: {n} particles, spacing 0.1 = h/2, "
-                            f"bounds [0,{BOX}]^3, dt={DT}, FP32-compensated step",
-                "particles": n,
-                "parallelism": f"replicas x{world_size}",
-                "l2": "inputs larger than L2 (state ~1.4 GB per replica)",
-            },
-            "plain_f64": {"value": plain_value, "ms_per_step": ms_plain / k_plain, "steps": k_plain},
-            "full_trajectory": full,
+            "config": bench_config(dims, n, world_size),
             "ratio_comp_vs_plain": value / plain_value,
-            "density_err_max_rel": dens_err,
-            "pressure_err_norm": p_err,
+            "plain_f64": {"value": plain_value, "ms_per_step": ms_plain / k_plain, "steps": k_plain},
             "phase_ms": {"comp": ph_comp, "plain_f64": ph_plain},
+            "density_err_max_rel": err_max["density_max_rel"] if err_max else None,
+            "errors_max_over_trajectory": err_max,
+            "full_trajectory": {"steps": full["steps"], "ms_per_step": full["ms_per_step"],
+                                "value": full["value"]} if full else None,
             "pairs_per_particle": cnt["pairs"] / n,
-            "candidates_per_particle": cnt["candidates"] / n,
             "roofline": {
-                "bound": "hbm",
-                "kernel": "k_force_tiled (force + integrate + bounds; the dense-cell force kernel that follows "
-                          "it has no work in this state and is timed with it)",
+                "bound": "issue",
+                "axis": "hbm",
+                "kernel": "k_force_tiled",
                 "achieved": achieved,
                 "peak": hbm_peak,
                 "unit": "GB/s",
                 "frac": achieved / hbm_peak,
                 "peak_kind": peak_kind,
                 "traffic": FORCE_TRAFFIC_PER_PARTICLE * n,
-                "traffic_note": "ncu DRAM bytes per launch at 1,024,000 particles, scaled by particle count",
-                "algorithmic_bytes_per_particle": FORCE_BYTES["comp"],
-                "note": "sparse neighbour gather: FP/issue-bound, not HBM-bound; frac of measured HBM peak",
-            },
-            "step_roofline": {
-                "algorithmic_bytes_per_particle_step": STEP_BYTES,
-                "achieved_gbs": STEP_BYTES * n / (step_ms / 1e3) / 1e9,
-                "frac": STEP_BYTES * n / (step_ms / 1e3) / 1e9 / hbm_peak,
+                "bytes_per_particle": STEP_BYTES,
+                "kernel_ms": force_ms,
+                "step_achieved": step_gbs,
+                "step_frac": step_gbs / hbm_peak,
+                "force_own_bytes_frac": FORCE_BYTES["comp"] * n / (force_ms / 1e3) / 1e9 / hbm_peak,
             },
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 24 * n,
-                    "d2h_bytes_per_step": 2 * 24 * n, "steps": ke,
-                    "path": "phy_fluid_set_field(pos, vel) from pinned host -> phy_fluid_step -> "
-                            "phy_fluid_get_field(pos, vel) to pinned host"},
+                    "d2h_bytes_per_step": 2 * 24 * n, "steps": ke},
             "gpu_launches": LAUNCHES_PER_STEP * K,
             "clocks": clocks,
             "cpu_baseline": cpu,
-            "batched": batched,
-            "adjoint": adjoint,
-            "coupling": coupling,
         }
         print(json.dumps(line), flush=True)
     if world_size > 1:
         dist.barrier()
         dist.destroy_process_group()
     return line
+
+
+def run_readback(pb, w, n: int) -> dict:
+    """phy_world_get_fluid_positions (lib.rs:399-429) of the 4M state into a pageable and
+    into a pinned (phy_fluid_pin_host) host buffer: host clock per call, 3 calls each."""
+    import ctypes as C
+    lib = pb._lib.load()
+    h = w._h
+    out = {}
+    for kind in ("pageable", "pinned"):
+        buf = np.empty(3 * n, np.float64)
+        buf[:] = 0.0  # touch the pages
+        if kind == "pinned" and lib.phy_fluid_pin_host(buf.ctypes.data, buf.nbytes) != 0:
+            out[kind] = {"error": pb._lib.last_error()}
+            continue
+        ptr = buf.ctypes.data_as(C.POINTER(C.c_double))
+        lib.phy_world_get_fluid_positions(h, ptr, buf.size)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            got = lib.phy_world_get_fluid_positions(h, ptr, buf.size)
+        t = (time.perf_counter() - t0) / 3
+        if kind == "pinned":
+            lib.phy_fluid_unpin_host(buf.ctypes.data)
+        out[kind] = {"ms": t * 1e3, "gbs": buf.nbytes / t / 1e9, "particles": int(got)}
+    out["workload"] = f"phy_world_get_fluid_positions of {n} particles (f64 xyz, {24 * n} bytes), host clock"
+    return out
 
 
 def run_coupling(pb, scenes, w, n: int) -> dict:
@@ -626,67 +710,74 @@ def run_coupling(pb, scenes, w, n: int) -> dict:
     }
 
 
-def _oracle_sample(scenes, pb, n_target: int):
-    """A sub-block of the same dam-break recipe with about n_target particles."""
-    for dims in ((64, 128, 64), (48, 96, 48), (40, 80, 40), (32, 64, 32), (24, 48, 24), (16, 32, 16)):
-        if dims[0] * dims[1] * dims[2] <= n_target:
-            return dims
-    return (16, 32, 16)
+def _standalone_scenes():
+    """physics_b200/scenes.py loaded as a lone module: the scene generator needs only
+    numpy, and importing it this way keeps the product library (loaded by the package's
+    __init__) out of the process."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("sph_bench_scenes", ROOT / "physics_b200" / "scenes.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod  # dataclasses resolve their module through sys.modules
+    spec.loader.exec_module(mod)
+    return mod
 
 
-def cpu_baseline(scenes, pb, budget_s: float = 15.0):
-    """The oracle (CPU restatement of the reference's rayon step) on all host threads."""
+def _oracle_world(O, pos, threads: int):
+    """The oracle world of the benchmark scene: SphParams::defaults() restated in the
+    oracle module (params.rs:55-85), bounds [0, 51.2]^3, lattice_mass(0.1)."""
+    p = O.RefParams.defaults()
+    p.bounds_min, p.bounds_max = (0.0, 0.0, 0.0), (BOX, BOX, BOX)
+    w = O.OracleWorld(p, threads=threads)
+    w.add_particles(pos, w.lattice_mass(0.1))
+    return w
+
+
+def cpu_baseline(scenes, pb, n: int, dims, budget_s: float = 15.0):
+    """The oracle (CPU restatement of the reference's rayon step) on all host threads, on
+    the same scene as the headline, for about budget_s seconds of steps from the start."""
     from oracle import oracle as O
     O.build()
     threads = O.max_threads()
-    dims = (64, 128, 64)
-    pos = scenes.dam_break_positions(*dims)
-    p = pb.SphParams.defaults()
-    p.bounds_min, p.bounds_max = (0.0, 0.0, 0.0), (BOX, BOX, BOX)
-    w = O.OracleWorld(p, threads=threads)
-    w.add_particles(pos, scenes.lattice_mass(0.1))
-    w.step(DT)  # warm-up (allocations, page faults)
+    w = _oracle_world(O, scenes.dam_break_positions(*dims), threads)
     steps, t = 0, 0.0
-    while t < budget_s and steps < 20:
+    while (t < budget_s and steps < 50) or steps < 2:
         t0 = time.perf_counter()
         w.step(DT)
         t += time.perf_counter() - t0
         steps += 1
-    return {"value": pos.shape[0] * steps / t, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{steps} steps of a {dims[0]}x{dims[1]}x{dims[2]} ({pos.shape[0]} particles) block of the "
-                      f"same dam-break recipe, OpenMP over {threads} threads, f64 oracle (reference op order)"}
+    return {"value": n * steps / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"steps 1-{steps} of the same {n}-particle scene, OpenMP {threads} threads, f64 oracle"}
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference's rayon step (oracle/, the
+    reference op order, OpenMP over all host threads) on the headline's scene, W untimed
+    and K timed steps from the initial state, as the headline.  Loads liboracle.so only."""
     rank = env_int("RANK", 0)
     if rank != 0:
         return None
-    import physics_b200 as pb  # SphParams defaults only; the timed code is the oracle
-    from physics_b200 import scenes
+    scenes = _standalone_scenes()
+    sys.path.insert(0, str(ROOT))
     from oracle import oracle as O
     O.build()
     threads = O.max_threads()
     K, W = args.steps, args.warmup
-    dims = _oracle_sample(scenes, pb, int(4e7 / max(K, 1)))
+    dims = tuple(args.dims)
     pos = scenes.dam_break_positions(*dims)
-    p = pb.SphParams.defaults()
-    p.bounds_min, p.bounds_max = (0.0, 0.0, 0.0), (BOX, BOX, BOX)
-    w = O.OracleWorld(p, threads=threads)
-    w.add_particles(pos, scenes.lattice_mass(0.1))
+    n = pos.shape[0]
+    w = _oracle_world(O, pos, threads)
     w.step(DT, W)
     t0 = time.perf_counter()
     w.step(DT, K)
     t = time.perf_counter() - t0
-    n = pos.shape[0]
     value = n * K / t
-    sample = (f"each step: one f64 step of a {dims[0]}x{dims[1]}x{dims[2]} ({n} particles) block of the "
-              f"4M dam-break recipe; CPU restatement of the reference's rayon step (oracle/), OpenMP "
-              f"{threads} threads; the Rust reference is not buildable here (no cargo, crates not vendored)")
+    sample = (f"every step of the {n}-particle scene (steps {W + 1}-{W + K}); CPU restatement of the reference's "
+              f"rayon step (oracle/), OpenMP {threads} threads; the Rust reference is not buildable here (no cargo, "
+              f"crates not vendored)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": env_int("WORLD_SIZE", 1),
             "steps": K, "warmup": W, "ms_per_step": t / K * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded jittered dam-break lattice)",
-            "config": {"workload": f"dam_break {n} particles (sub-block of the 4,194,304-particle scene), "
-                                   f"dt={DT}", "particles": n},
+            "config": bench_config(dims, n, env_int("WORLD_SIZE", 1)),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

@@ -165,6 +165,12 @@ int32_t phy_fluid_couple_heat(PhyWorldHandle *w, uint32_t sub, const uint64_t *d
 #define PHY_SHAPE_BOX 2
 #define PHY_SHAPE_CONVEX 3
 #define PHY_SHAPE_HEIGHTFIELD 4
+/* Shape::Compound (phy-rigid shape.rs:176-192): data_count sub shapes (at
+ * least one) as 16-double records from data[data_first]: shape (0..4; no
+ * nested compounds), size[3], offset[3] and unit quaternion (i, j, k, w)
+ * relative to the body, then data_first, data_count, face_first, face_count
+ * of the sub shape's own convex / heightfield data, and one unused value. */
+#define PHY_SHAPE_COMPOUND 5
 typedef struct PhyCoupleBody {
   int32_t shape;
   uint32_t data_first, data_count, face_first, face_count, reserved;
@@ -201,6 +207,17 @@ int32_t phy_fluid_set_stream(PhyWorldHandle *w, void *cuda_stream);
 /* Blocks until the world's device work has finished. */
 int32_t phy_fluid_synchronize(PhyWorldHandle *w);
 
+/* Page-locks a caller-owned host buffer of `bytes` bytes (cudaHostRegister)
+ * so that readbacks into it (phy_world_get_fluid_positions/velocities and
+ * their f32 forms, phy_fluid_get_field) are single DMA copies instead of
+ * staged pageable copies: the zero-copy form of the reference's per-frame
+ * readback path (phy-ffi/src/lib.rs:399-460, 595-653).  Optional; the buffer
+ * stays valid for every other use.  Undo with phy_fluid_unpin_host before
+ * freeing it.  0, or -1 (null, zero size, already registered, or refused by
+ * the driver; phy_fluid_last_error() says why). */
+int32_t phy_fluid_pin_host(void *ptr, uint64_t bytes);
+int32_t phy_fluid_unpin_host(void *ptr);
+
 /* Enables (on != 0) or disables counting of neighbour candidates and pairs
  * in the density pass of `sub` (one atomic per warp; off by default). */
 int32_t phy_fluid_set_counting(PhyWorldHandle *w, uint32_t sub, int32_t on);
@@ -220,7 +237,8 @@ int32_t phy_fluid_phase_times(PhyWorldHandle *w, uint32_t sub, double *out5, int
 
 /* Kernel configuration of `sub` (no effect on the f64 plain form's results):
  *   PHY_TUNE_COMP_TILE    0 = x-major cell runs, 4 = staged 4x4x4-cell tiles
- *                         (default) for the FP32-compensated passes;
+ *                         (default), 2 = staged 2x2x2-cell tiles, for the
+ *                         FP32-compensated passes (cells per tile edge);
  *   PHY_TUNE_HALO_CAP     staged particles per tile halo before a tile is
  *                         computed from global memory (default: the kernels'
  *                         capacity).
@@ -269,17 +287,30 @@ typedef struct PhyTuneTrial {
   int32_t ctas_per_sm;
   int32_t queue;
   int32_t sort_block;
+  int32_t comp_tile;   /* cells per tile edge of the trial (0: not a tiled world) */
+  double ms_per_step;  /* mean over the sampled states the trial ran on */
+  int32_t samples;     /* sampled states it ran on */
   int32_t reserved;
-  double ms_per_step;
 } PhyTuneTrial;
 
 /* Autotuner (no reference counterpart): times `steps` steps of dt for every
- * combination of the launch knobs (sort block 128/256, static stride or work
- * queue, 1..occupancy-limit CTAs per SM), each from the same saved state,
- * restores that state, and keeps the fastest configuration.  Writes up to
- * `cap` trials to out (may be NULL) and their number to *n_out. */
+ * combination of the knobs (sort block 128/256, static stride or work
+ * queue, 1..occupancy-limit CTAs per SM, and for tiled worlds 4 or 2 cells
+ * per tile edge), each from the same saved state, restores that state, and
+ * keeps the fastest configuration.  Writes up to `cap` trials to out (may be
+ * NULL) and their number to *n_out.  No knob changes a result bit except the
+ * tile edge, which changes the compensated form's summation order only. */
 int32_t phy_fluid_autotune(PhyWorldHandle *w, uint32_t sub, double dt, uint32_t steps, PhyTuneTrial *out,
                            uint32_t cap, uint32_t *n_out);
+
+/* The same over the run ahead: first steps `horizon` steps with the current
+ * configuration, saving the states after horizon/2 and horizon steps; every
+ * candidate runs from the starting state, the six fastest also from the two
+ * later ones, and the fastest mean over the three wins (a collapsing scene
+ * gets the configuration of the states it will spend its time in).  The
+ * world returns to its starting state.  horizon = 0 is phy_fluid_autotune. */
+int32_t phy_fluid_autotune_horizon(PhyWorldHandle *w, uint32_t sub, double dt, uint32_t steps, uint32_t horizon,
+                                   PhyTuneTrial *out, uint32_t cap, uint32_t *n_out);
 
 /* Adjoint of the f64 plain step (PHY_PRECISION_F64_PLAIN worlds only).
  * phy_fluid_tape_begin makes the current state checkpoint 0 and records every

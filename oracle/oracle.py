@@ -30,6 +30,32 @@ class OrcParams(C.Structure):
     ]
 
 
+class RefParams:
+    """SphParams<f64>::defaults() restated for the oracle alone
+    (crates/phy-fluid/src/sph/params.rs:55-85), so that a CPU-only run of the
+    reference's step (the bench's reference arm) needs nothing from the
+    product library."""
+
+    def __init__(self):
+        self.rest_density = 1000.0
+        self.stiffness = 250.0
+        self.viscosity = 3.5
+        self.visc_k = [3.5]
+        self.visc_n = [1.0]
+        self.shear_min = 0.01
+        self.mass = 0.02
+        self.h = 0.2
+        self.gravity = (0.0, -9.81, 0.0)
+        self.bounds_min = (-5.0, -5.0, -5.0)
+        self.bounds_max = (5.0, 5.0, 5.0)
+        self.boundary_damp = 0.4
+        self.xsph_eps = 0.5
+
+    @staticmethod
+    def defaults() -> "RefParams":
+        return RefParams()
+
+
 _lib = None
 DP = C.POINTER(C.c_double)
 SRC = Path(__file__).resolve().parent / "sph_oracle.cpp"
@@ -246,14 +272,15 @@ class OrcBody(C.Structure):
                 ("inv_mass", C.c_double)]
 
 
-SHAPES = {"sphere": 0, "capsule": 1, "box": 2, "convex": 3, "heightfield": 4}
+SHAPES = {"sphere": 0, "capsule": 1, "box": 2, "convex": 3, "heightfield": 4, "compound": 5}
 
 
 def pack_bodies(bodies, struct):
     """Body dicts -> (struct array, data doubles, face indices).  A dict holds `shape`
     (a SHAPES name), `size` (sphere (r,), capsule (half_height, r), box half extents,
     heightfield (nx, nz, cell)), `pos`, `rot` (unit quaternion i, j, k, w; default identity),
-    `vel`, `inv_mass`, and `verts` + `faces` (convex) or `heights` (heightfield)."""
+    `vel`, `inv_mass`, and `verts` + `faces` (convex), `heights` (heightfield) or `subs`
+    (compound: shape dicts with `offset` and `rot` relative to the body)."""
     arr = (struct * max(len(bodies), 1))()
     data, faces = [], []
     for k, b in enumerate(bodies):
@@ -268,15 +295,37 @@ def pack_bodies(bodies, struct):
         for a in range(4):
             o.rot[a] = rot[a]
         o.inv_mass = b.get("inv_mass", 0.0)
-        if b["shape"] == "convex":
-            o.data_first, o.data_count = len(data), len(b["verts"])
-            data.extend(np.asarray(b["verts"], np.float64).reshape(-1).tolist())
-            o.face_first, o.face_count = len(faces) // 3, len(b["faces"])
-            faces.extend(np.asarray(b["faces"], np.uint32).reshape(-1).tolist())
-        elif b["shape"] == "heightfield":
-            o.data_first, o.data_count = len(data), len(b["heights"])
-            data.extend(list(b["heights"]))
+        o.data_first, o.data_count, o.face_first, o.face_count = _shape_data(b, data, faces)
     return arr, np.array(data + [0.0], np.float64), np.array(faces + [0], np.uint32)
+
+
+def _shape_data(b, data, faces):
+    """Appends a shape's convex vertices and faces, heightfield heights, or compound
+    sub-shape records (16 doubles each: shape, size[3], offset[3], quaternion, data_first,
+    data_count, face_first, face_count, 0) to data / faces; returns (data_first,
+    data_count, face_first, face_count)."""
+    kind = b["shape"]
+    if kind == "convex":
+        d0, f0 = len(data), len(faces) // 3
+        data.extend(np.asarray(b["verts"], np.float64).reshape(-1).tolist())
+        faces.extend(np.asarray(b["faces"], np.uint32).reshape(-1).tolist())
+        return d0, len(b["verts"]), f0, len(b["faces"])
+    if kind == "heightfield":
+        d0 = len(data)
+        data.extend(float(h) for h in b["heights"])
+        return d0, len(b["heights"]), 0, 0
+    if kind == "compound":
+        d0 = len(data)
+        data.extend([0.0] * (16 * len(b["subs"])))
+        for q, sub in enumerate(b["subs"]):
+            size = list(sub.get("size", ())) + [0.0] * 3
+            rec = [float(SHAPES[sub["shape"]])] + [float(v) for v in size[:3]]
+            rec += [float(v) for v in sub.get("offset", (0.0, 0.0, 0.0))]
+            rec += [float(v) for v in sub.get("rot", (0.0, 0.0, 0.0, 1.0))]
+            rec += [float(v) for v in _shape_data(sub, data, faces)] + [0.0]
+            data[d0 + 16 * q: d0 + 16 * (q + 1)] = rec
+        return d0, len(b["subs"]), 0, 0
+    return 0, 0, 0, 0
 
 
 def max_threads() -> int:

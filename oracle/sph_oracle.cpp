@@ -444,7 +444,9 @@ struct World {
   // (pos, unit quaternion rot = (i, j, k, w) as nalgebra stores it), the
   // linear velocity, inv_mass, and the shape: 0 sphere {r}, 1 capsule
   // {half_height, r} along local y, 2 box {half extents}, 3 convex (vertices,
-  // index faces), 4 heightfield {nx, nz, cell} + heights.
+  // index faces), 4 heightfield {nx, nz, cell} + heights, 5 compound: sub
+  // shapes (shape.rs:176-192), each with its own offset and rotation
+  // relative to the body (the sub shapes' own pose fields).
   struct Body {
     int shape = 0;
     double size[3] = {0, 0, 0};
@@ -455,6 +457,7 @@ struct World {
     std::vector<V3> verts;
     std::vector<uint32_t> faces;  // 3 per face, indices into verts
     std::vector<double> heights;
+    std::vector<Body> subs;  // compound: sub shapes, pos = offset, rot = quat
   };
 
   static double dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
@@ -498,6 +501,23 @@ struct World {
         }
         return best;
       }
+      case 5: {
+        // The sub shape farthest along dir, in body coordinates; the search
+        // starts from the first sub shape's offset at dot 0 (shape.rs:238-254).
+        V3 best = b.subs[0].pos;
+        double best_dot = 0.0;
+        for (const Body& sub : b.subs) {
+          const V3 d_local = qrot(sub.rot, dir, true);
+          const V3 sp = support_local(sub, d_local);
+          const V3 ws = sub.pos + qrot(sub.rot, sp, false);
+          const double d = dot(ws, dir);
+          if (d > best_dot) {
+            best_dot = d;
+            best = ws;
+          }
+        }
+        return best;
+      }
       default:
         return {0, 0, 0};
     }
@@ -522,6 +542,10 @@ struct World {
           if (dot(p - a, n) > 0.0) return false;
         }
         return true;
+      case 5:  // any sub shape contains p in its own coordinates (shape.rs:319-322)
+        for (const Body& sub : b.subs)
+          if (contains_local(sub, qrot(sub.rot, p - sub.pos, true))) return true;
+        return false;
       default:
         return false;
     }
@@ -541,6 +565,11 @@ struct World {
         for (double h : b.heights) sum = sum + h;
         const double hy = b.heights.empty() ? 0.0 : sum / (double)b.heights.size();
         return hx * hz * std::fabs(hy);
+      }
+      case 5: {  // sum of the sub shapes' volumes, folded from 0 in order (world.rs:531-534)
+        double v = 0.0;
+        for (const Body& sub : b.subs) v = v + body_volume(sub);
+        return v;
       }
       default:
         return 0.0;
@@ -966,10 +995,27 @@ struct OrcBody {
   double size[3], pos[3], rot[4], vel[3], inv_mass;
 };
 
+// Convex vertices / heightfield heights of a shape from the shared arrays.
+static void shape_data(World::Body& b, uint32_t data_first, uint32_t data_count, uint32_t face_first,
+                       uint32_t face_count, const double* data, const uint32_t* faces) {
+  if (b.shape == 3) {
+    for (uint32_t v = 0; v < data_count; ++v) {
+      const double* d = data + data_first + 3 * v;
+      b.verts.push_back({d[0], d[1], d[2]});
+    }
+    b.faces.assign(faces + 3 * (size_t)face_first, faces + 3 * ((size_t)face_first + face_count));
+  } else if (b.shape == 4) {
+    b.heights.assign(data + data_first, data + data_first + data_count);
+  }
+}
+
 // FluidWorld::couple_bodies (world.rs:414-503); the bodies' velocities are
 // updated in place.  Convex vertices are data_count xyz triples from
 // data[data_first]; faces are face_count index triples from
-// faces[3 * face_first]; heightfield heights are data_count values.
+// faces[3 * face_first]; heightfield heights are data_count values; a
+// compound body's data_count sub shapes are 16-double records from
+// data[data_first]: shape, size[3], offset[3], quaternion (i, j, k, w),
+// data_first, data_count, face_first, face_count, unused.
 void orc_couple_bodies(void* w, OrcBody* bodies, uint32_t nb, const double* data, const uint32_t* faces, double dt) {
   std::vector<World::Body> bs(nb);
   for (uint32_t k = 0; k < nb; ++k) {
@@ -981,14 +1027,18 @@ void orc_couple_bodies(void* w, OrcBody* bodies, uint32_t nb, const double* data
     for (int a = 0; a < 4; ++a) b.rot[a] = o.rot[a];
     b.vel = {o.vel[0], o.vel[1], o.vel[2]};
     b.inv_mass = o.inv_mass;
-    if (o.shape == 3) {
-      for (uint32_t v = 0; v < o.data_count; ++v) {
-        const double* d = data + o.data_first + 3 * v;
-        b.verts.push_back({d[0], d[1], d[2]});
+    shape_data(b, o.data_first, o.data_count, o.face_first, o.face_count, data, faces);
+    if (o.shape == 5) {
+      for (uint32_t q = 0; q < o.data_count; ++q) {
+        const double* r = data + o.data_first + 16 * (size_t)q;
+        World::Body sub;
+        sub.shape = (int)r[0];
+        for (int a = 0; a < 3; ++a) sub.size[a] = r[1 + a];
+        sub.pos = {r[4], r[5], r[6]};
+        for (int a = 0; a < 4; ++a) sub.rot[a] = r[7 + a];
+        shape_data(sub, (uint32_t)r[11], (uint32_t)r[12], (uint32_t)r[13], (uint32_t)r[14], data, faces);
+        b.subs.push_back(sub);
       }
-      b.faces.assign(faces + 3 * (size_t)o.face_first, faces + 3 * ((size_t)o.face_first + o.face_count));
-    } else if (o.shape == 4) {
-      b.heights.assign(data + o.data_first, data + o.data_first + o.data_count);
     }
   }
   static_cast<World*>(w)->couple_bodies(bs, dt);

@@ -44,7 +44,8 @@ FIELD_COMPONENTS = {FIELD_POS: 3, FIELD_VEL: 3, FIELD_ACC: 3, FIELD_BODY_ACC: 3,
 
 class PhyTuneTrial(C.Structure):
     _fields_ = [("ctas_per_sm", C.c_int32), ("queue", C.c_int32), ("sort_block", C.c_int32),
-                ("reserved", C.c_int32), ("ms_per_step", C.c_double)]
+                ("comp_tile", C.c_int32), ("ms_per_step", C.c_double), ("samples", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class PhyCoupleBody(C.Structure):
@@ -55,7 +56,7 @@ class PhyCoupleBody(C.Structure):
                 ("inv_mass", C.c_double)]
 
 
-SHAPES = {"sphere": 0, "capsule": 1, "box": 2, "convex": 3, "heightfield": 4}
+SHAPES = {"sphere": 0, "capsule": 1, "box": 2, "convex": 3, "heightfield": 4, "compound": 5}
 
 
 class PhySphParams(C.Structure):
@@ -138,6 +139,8 @@ SIGNATURES = {
     "phy_fluid_set_coupling": (C.c_int32, [H, C.c_uint32, DP]),
     "phy_fluid_set_stream": (C.c_int32, [H, C.c_void_p]),
     "phy_fluid_synchronize": (C.c_int32, [H]),
+    "phy_fluid_pin_host": (C.c_int32, [C.c_void_p, C.c_uint64]),
+    "phy_fluid_unpin_host": (C.c_int32, [C.c_void_p]),
     "phy_fluid_set_counting": (C.c_int32, [H, C.c_uint32, C.c_int32]),
     "phy_fluid_step_counters": (C.c_int32, [H, C.c_uint32, C.POINTER(C.c_uint64)]),
     "phy_fluid_set_timing": (C.c_int32, [H, C.c_uint32, C.c_int32]),
@@ -153,6 +156,8 @@ SIGNATURES = {
     "phy_fluid_step_backward": (C.c_int32, [H, C.c_uint32, DP, DP, DP, DP, DP]),
     "phy_fluid_autotune": (C.c_int32, [H, C.c_uint32, C.c_double, C.c_uint32, C.POINTER(PhyTuneTrial),
                                        C.c_uint32, C.POINTER(C.c_uint32)]),
+    "phy_fluid_autotune_horizon": (C.c_int32, [H, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32,
+                                               C.POINTER(PhyTuneTrial), C.c_uint32, C.POINTER(C.c_uint32)]),
     "phy_fluid_density_noalloc": (C.c_int32, [C.POINTER(PhySphParams), C.c_uint64, C.c_void_p, C.c_void_p,
                                               C.c_void_p, C.c_void_p, C.c_void_p]),
     "phy_fluid_last_error": (C.c_char_p, []),

@@ -49,6 +49,33 @@ __device__ __forceinline__ uint32_t candidate(const CoupleArgs& a, const uint32_
   return a.perm[s_beg[u] + (flat - s_pre[u])];
 }
 
+// The point's force from its ordered sums (world.rs:712-736), written to
+// q[7..9]; r = the reaction -f dt and the sum of the masses (the reference's
+// second pass sums them in the same order).
+__device__ __forceinline__ void point_force(const StepConsts& c, const CoupleArgs& a, double* q, double sx,
+                                            double sy, double sz, double sw, double* r) {
+  double vfx = 0.0, vfy = 0.0, vfz = 0.0;
+  if (sw > 0.0) {
+    vfx = sx / sw;
+    vfy = sy / sw;
+    vfz = sz / sw;
+  }
+  const double pm = q[6];
+  const double vol = a.soft_density > 0.0 ? pm / a.soft_density : 0.0;
+  const double rv = c.rest * vol;
+  const double dm = a.drag * pm;
+  const double fx = -c.g[0] * rv + (vfx - q[3]) * dm;
+  const double fy = -c.g[1] * rv + (vfy - q[4]) * dm;
+  const double fz = -c.g[2] * rv + (vfz - q[5]) * dm;
+  q[7] = fx;
+  q[8] = fy;
+  q[9] = fz;
+  r[0] = -fx * a.dt;
+  r[1] = -fy * a.dt;
+  r[2] = -fz * a.dt;
+  r[3] = sw;
+}
+
 __global__ void __launch_bounds__(kCT) k_couple_points(StepConsts c, CoupleArgs a) {
   __shared__ uint32_t s_beg[27];
   __shared__ uint32_t s_pre[28];
@@ -115,28 +142,7 @@ __global__ void __launch_bounds__(kCT) k_couple_points(StepConsts c, CoupleArgs 
         }
       __syncthreads();
     }
-    if (t == 0) {
-      double vfx = 0.0, vfy = 0.0, vfz = 0.0;
-      if (sw > 0.0) {
-        vfx = sx / sw;
-        vfy = sy / sw;
-        vfz = sz / sw;
-      }
-      const double pm = q[6];
-      const double vol = a.soft_density > 0.0 ? pm / a.soft_density : 0.0;
-      const double rv = c.rest * vol;
-      const double dm = a.drag * pm;
-      const double fx = -c.g[0] * rv + (vfx - q[3]) * dm;
-      const double fy = -c.g[1] * rv + (vfy - q[4]) * dm;
-      const double fz = -c.g[2] * rv + (vfz - q[5]) * dm;
-      q[7] = fx;
-      q[8] = fy;
-      q[9] = fz;
-      s_r[0] = -fx * a.dt;
-      s_r[1] = -fy * a.dt;
-      s_r[2] = -fz * a.dt;
-      s_r[3] = sw;  // sum of the masses in visit order, as the reference's second pass
-    }
+    if (t == 0) point_force(c, a, q, sx, sy, sz, sw, s_r);
     __syncthreads();
     const double msum = s_r[3];
     if (msum > 0.0)
@@ -150,6 +156,164 @@ __global__ void __launch_bounds__(kCT) k_couple_points(StepConsts c, CoupleArgs 
     __syncthreads();
   }
 }
+
+// Pipelined form of the same walk.  Only velocities change from one point to
+// the next, so while thread 0 runs point k's ordered sums, warps 1..7 build
+// point k+1's cell table and its candidates' particle indices and masses
+// (double-buffered in shared memory).  Point k's velocities are gathered once
+// after point k-1's reaction; the reaction reuses them (v_j + share, the same
+// f64 operations), so a point costs one gather, the ordered sums and one
+// scatter.  Points with more than kPB candidates take the chunked walk above.
+constexpr int kPB = 2048;  // candidates prefetched per point
+
+struct PointTable {
+  uint32_t beg[27];
+  uint32_t pre[28];
+  int in;
+};
+
+// Cell table of point k (one warp).
+__device__ __forceinline__ void point_table(const StepConsts& c, const CoupleArgs& a, int k, PointTable& T) {
+  const int lane = threadIdx.x & 31;
+  const double* q = a.pts + 10 * (size_t)k;
+  const double x = q[0], y = q[1], z = q[2];
+  // world.rs:704-711 (a NaN coordinate passes, as there).
+  const bool in = !(x < c.lo[0] || x > c.hi[0] || y < c.lo[1] || y > c.hi[1] || z < c.lo[2] || z > c.hi[2]);
+  if (lane == 0) T.in = in ? 1 : 0;
+  if (in) {
+    const long long kx = key_axis(x, c.inv_cell), ky = key_axis(y, c.inv_cell), kz = key_axis(z, c.inv_cell);
+    uint32_t beg = 0, cnt = 0;
+    if (lane < 27) {
+      const int lin = cell_linear(c, kx + lane / 9 - 1, ky + (lane / 3) % 3 - 1, kz + lane % 3 - 1);
+      if (lin >= 0) {
+        beg = a.cell_start[lin];
+        cnt = a.cell_start[lin + 1] - beg;
+      }
+    }
+    uint32_t incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane < 27) {
+      T.beg[lane] = beg;
+      T.pre[lane] = incl - cnt;
+    }
+    if (lane == 26) T.pre[27] = incl;
+  }
+  __syncwarp();
+}
+
+// Warps 1..7: the table of point k and, when it fits, its candidates'
+// indices and masses.
+__device__ __forceinline__ void prefetch_point(const StepConsts& c, const CoupleArgs& a, int k, PointTable& T,
+                                               uint32_t* idx, double* m) {
+  if ((threadIdx.x >> 5) == 1) point_table(c, a, k, T);
+  asm volatile("bar.sync 1, %0;" ::"r"(kCT - 32));
+  if (!T.in) return;
+  const uint32_t total = T.pre[27];
+  if (total > (uint32_t)kPB) return;
+  for (uint32_t e = threadIdx.x - 32; e < total; e += kCT - 32) {
+    const uint32_t i = candidate(a, T.beg, T.pre, e);
+    idx[e] = i;
+    m[e] = a.mass[i];
+  }
+}
+
+__global__ void __launch_bounds__(kCT) k_couple_points_piped(StepConsts c, CoupleArgs a) {
+  __shared__ PointTable s_tab[2];
+  __shared__ double s_r[4];  // reaction xyz, sum of masses
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* s_m = reinterpret_cast<double*>(smem);         // [2][kPB] masses
+  double* s_v = s_m + 2 * kPB;                           // [3][kPB] velocities
+  uint32_t* s_idx = reinterpret_cast<uint32_t*>(s_v + 3 * kPB);  // [2][kPB] particle indices
+  const int t = threadIdx.x, warp = t >> 5;
+  if (warp >= 1 && a.np > 0) prefetch_point(c, a, 0, s_tab[0], s_idx, s_m);
+  __syncthreads();
+  for (int k = 0; k < a.np; ++k) {
+    const int cur = k & 1, nxt = cur ^ 1;
+    const PointTable& T = s_tab[cur];
+    uint32_t* idx = s_idx + cur * kPB;
+    double* m = s_m + cur * kPB;
+    double* q = a.pts + 10 * (size_t)k;
+    const bool more = k + 1 < a.np;
+    const uint32_t total = T.in ? T.pre[27] : 0u;
+    if (!T.in || total > (uint32_t)kPB) {
+      if (T.in) {
+        // Chunked walk: candidates staged kPB at a time (m and s_v as staging).
+        double sx = 0.0, sy = 0.0, sz = 0.0, sw = 0.0;
+        for (uint32_t base = 0; base < total; base += kPB) {
+          const uint32_t cnt = min((uint32_t)kPB, total - base);
+          for (uint32_t e = t; e < cnt; e += kCT) {
+            const uint32_t i = candidate(a, T.beg, T.pre, base + e);
+            s_v[e] = a.vx[i];
+            s_v[kPB + e] = a.vy[i];
+            s_v[2 * kPB + e] = a.vz[i];
+            m[e] = a.mass[i];
+          }
+          __syncthreads();
+          if (t == 0)
+            for (uint32_t e = 0; e < cnt; ++e) {
+              const double w = m[e];
+              sx = sx + s_v[e] * w;
+              sy = sy + s_v[kPB + e] * w;
+              sz = sz + s_v[2 * kPB + e] * w;
+              sw = sw + w;
+            }
+          __syncthreads();
+        }
+        if (t == 0) point_force(c, a, q, sx, sy, sz, sw, s_r);
+        __syncthreads();
+        const double msum = s_r[3];
+        if (msum > 0.0)
+          for (uint32_t flat = t; flat < total; flat += kCT) {
+            const uint32_t i = candidate(a, T.beg, T.pre, flat);
+            const double frac = a.mass[i] / msum;
+            a.vx[i] = a.vx[i] + s_r[0] * frac;
+            a.vy[i] = a.vy[i] + s_r[1] * frac;
+            a.vz[i] = a.vz[i] + s_r[2] * frac;
+          }
+      }
+      __syncthreads();
+      if (warp >= 1 && more) prefetch_point(c, a, k + 1, s_tab[nxt], s_idx + nxt * kPB, s_m + nxt * kPB);
+      __syncthreads();
+      continue;
+    }
+    for (uint32_t e = t; e < total; e += kCT) {
+      const uint32_t i = idx[e];
+      s_v[e] = a.vx[i];
+      s_v[kPB + e] = a.vy[i];
+      s_v[2 * kPB + e] = a.vz[i];
+    }
+    __syncthreads();
+    if (t == 0) {
+      double sx = 0.0, sy = 0.0, sz = 0.0, sw = 0.0;
+      for (uint32_t e = 0; e < total; ++e) {
+        const double w = m[e];
+        sx = sx + s_v[e] * w;
+        sy = sy + s_v[kPB + e] * w;
+        sz = sz + s_v[2 * kPB + e] * w;
+        sw = sw + w;
+      }
+      point_force(c, a, q, sx, sy, sz, sw, s_r);
+    } else if (warp >= 1 && more) {
+      prefetch_point(c, a, k + 1, s_tab[nxt], s_idx + nxt * kPB, s_m + nxt * kPB);
+    }
+    __syncthreads();
+    const double msum = s_r[3];
+    if (msum > 0.0)
+      for (uint32_t e = t; e < total; e += kCT) {
+        const uint32_t i = idx[e];
+        const double frac = m[e] / msum;
+        a.vx[i] = s_v[e] + s_r[0] * frac;
+        a.vy[i] = s_v[kPB + e] + s_r[1] * frac;
+        a.vz[i] = s_v[2 * kPB + e] + s_r[2] * frac;
+      }
+    __syncthreads();
+  }
+}
+
+constexpr size_t kPipedSmem = (size_t)kPB * (2 * 8 + 3 * 8 + 2 * 4);
 
 // ---- couple_heat (world.rs:555-678) ------------------------------------------------
 //
@@ -401,7 +565,29 @@ __device__ __forceinline__ V3d body_pos(const PhyCoupleBody& b) { return v3(b.po
 __device__ __forceinline__ V3d to_local(const PhyCoupleBody& b, V3d p) { return qrot(b.rot, p - body_pos(b), true); }
 __device__ __forceinline__ V3d to_world(const PhyCoupleBody& b, V3d p) { return qrot(b.rot, p, false) + body_pos(b); }
 
-__device__ V3d support_local(const BodyArgs& a, const PhyCoupleBody& b, V3d dir) {  // shape.rs:198-256
+// A leaf shape (sphere, capsule, box, convex, heightfield): a body's own, or
+// one sub shape of a compound body.
+struct ShapeRef {
+  int shape;
+  double size[3];
+  uint32_t data_first, data_count, face_first, face_count;
+};
+
+__device__ __forceinline__ ShapeRef shape_of(const PhyCoupleBody& b) {
+  return {b.shape, {b.size[0], b.size[1], b.size[2]}, b.data_first, b.data_count, b.face_first, b.face_count};
+}
+
+// Sub shape q of compound body b (a 16-double record in the data array:
+// shape, size, offset, quaternion, then its own data ranges).
+__device__ __forceinline__ ShapeRef sub_shape(const BodyArgs& a, const PhyCoupleBody& b, uint32_t q, V3d& off,
+                                              double rot[4]) {
+  const double* r = a.data + b.data_first + 16 * (size_t)q;
+  off = v3(r[4], r[5], r[6]);
+  for (int k = 0; k < 4; ++k) rot[k] = r[7 + k];
+  return {(int)r[0], {r[1], r[2], r[3]}, (uint32_t)r[11], (uint32_t)r[12], (uint32_t)r[13], (uint32_t)r[14]};
+}
+
+__device__ V3d support_leaf(const BodyArgs& a, const ShapeRef& b, V3d dir) {  // shape.rs:198-236
   switch (b.shape) {
     case PHY_SHAPE_SPHERE:
       return vnormalize(dir) * b.size[0];
@@ -432,7 +618,30 @@ __device__ V3d support_local(const BodyArgs& a, const PhyCoupleBody& b, V3d dir)
   }
 }
 
-__device__ bool contains_local(const BodyArgs& a, const PhyCoupleBody& b, V3d p) {  // shape.rs:287-325
+// Shape::Compound: the sub shape farthest along dir, in body coordinates;
+// the search starts from the first sub shape's offset at dot 0
+// (shape.rs:238-254).
+__device__ V3d support_local(const BodyArgs& a, const PhyCoupleBody& b, V3d dir) {
+  if (b.shape != PHY_SHAPE_COMPOUND) return support_leaf(a, shape_of(b), dir);
+  V3d best = v3(0, 0, 0);
+  double best_dot = 0.0;
+  for (uint32_t q = 0; q < b.data_count; ++q) {
+    V3d off;
+    double rot[4];
+    const ShapeRef sub = sub_shape(a, b, q, off, rot);
+    if (q == 0) best = off;
+    const V3d s = support_leaf(a, sub, qrot(rot, dir, true));
+    const V3d ws = off + qrot(rot, s, false);
+    const double d = vdot(ws, dir);
+    if (d > best_dot) {
+      best_dot = d;
+      best = ws;
+    }
+  }
+  return best;
+}
+
+__device__ bool contains_leaf(const BodyArgs& a, const ShapeRef& b, V3d p) {  // shape.rs:287-318
   switch (b.shape) {
     case PHY_SHAPE_SPHERE:
       return vnorm(p) <= b.size[0];
@@ -461,7 +670,20 @@ __device__ bool contains_local(const BodyArgs& a, const PhyCoupleBody& b, V3d p)
   }
 }
 
-__device__ double body_volume(const BodyArgs& a, const PhyCoupleBody& b) {  // world.rs:506-540
+// Shape::Compound: any sub shape contains p in its own coordinates
+// (shape.rs:319-322).
+__device__ bool contains_local(const BodyArgs& a, const PhyCoupleBody& b, V3d p) {
+  if (b.shape != PHY_SHAPE_COMPOUND) return contains_leaf(a, shape_of(b), p);
+  for (uint32_t q = 0; q < b.data_count; ++q) {
+    V3d off;
+    double rot[4];
+    const ShapeRef sub = sub_shape(a, b, q, off, rot);
+    if (contains_leaf(a, sub, qrot(rot, p - off, true))) return true;
+  }
+  return false;
+}
+
+__device__ double volume_leaf(const BodyArgs& a, const ShapeRef& b) {  // world.rs:506-530
   const double pi = 3.14159265358979323846;
   switch (b.shape) {
     case PHY_SHAPE_SPHERE:
@@ -481,6 +703,20 @@ __device__ double body_volume(const BodyArgs& a, const PhyCoupleBody& b) {  // w
       return 0.0;
   }
 }
+
+// Shape::Compound: the sub shapes' volumes folded from 0 in order
+// (world.rs:531-534).
+__device__ double body_volume(const BodyArgs& a, const PhyCoupleBody& b) {
+  if (b.shape != PHY_SHAPE_COMPOUND) return volume_leaf(a, shape_of(b));
+  double v = 0.0;
+  for (uint32_t q = 0; q < b.data_count; ++q) {
+    V3d off;
+    double rot[4];
+    v = v + volume_leaf(a, sub_shape(a, b, q, off, rot));
+  }
+  return v;
+}
+
 
 // world.rs:755-773
 __device__ void push_out(const BodyArgs& a, const PhyCoupleBody& b, V3d& pos, V3d& vel) {
@@ -720,7 +956,14 @@ void launch_couple_points(const StepConsts& c, DevBuffers& b, double* d_pts, int
   a.dt = dt;
   a.drag = drag;
   a.soft_density = soft_density;
-  k_couple_points<<<1, kCT, 0, s>>>(c, a);
+  static const bool smem_ok = [] {
+    return cudaFuncSetAttribute(k_couple_points_piped, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kPipedSmem) == cudaSuccess;
+  }();
+  if (smem_ok)
+    k_couple_points_piped<<<1, kCT, kPipedSmem, s>>>(c, a);
+  else
+    k_couple_points<<<1, kCT, 0, s>>>(c, a);
 }
 
 }  // namespace phy

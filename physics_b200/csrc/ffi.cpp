@@ -80,7 +80,6 @@ uintptr_t read_vec(PhyWorldHandle* w, T* buf, uintptr_t len, int field) {
   World* W = as_world(w);
   if (!W || !buf) return 0;
   uintptr_t written = 0;  // particles
-  std::vector<double> tmp;
   for (auto& s : W->subs) {
     size_t n = s->world->len();
     if (n == 0) continue;
@@ -91,9 +90,8 @@ uintptr_t read_vec(PhyWorldHandle* w, T* buf, uintptr_t len, int field) {
       // The f32 channel is cast on the device (lib.rs:595-653: an `as f32` of each value).
       s->world->get_vec_f32(field, buf + 3 * written, take);
     } else {
-      tmp.resize(3 * n);
-      s->world->get_field(field, tmp.data());
-      for (size_t i = 0; i < 3 * take; ++i) buf[3 * written + i] = (T)tmp[i];
+      // One device-to-host copy of the first `take` particles into the caller's buffer.
+      s->world->get_vec_f64(field, buf + 3 * written, take);
     }
     written += take;
     if (take < n) break;
@@ -381,6 +379,28 @@ int32_t phy_fluid_set_stream(PhyWorldHandle* w, void* cuda_stream) {
   });
 }
 
+int32_t phy_fluid_pin_host(void* ptr, uint64_t bytes) {
+  if (!ptr || bytes == 0) {
+    g_last_error = "phy_fluid_pin_host: null pointer or zero size";
+    return -1;
+  }
+  return guard<int32_t>(-1, [&] {
+    phy::pin_host(ptr, (size_t)bytes);
+    return 0;
+  });
+}
+
+int32_t phy_fluid_unpin_host(void* ptr) {
+  if (!ptr) {
+    g_last_error = "phy_fluid_unpin_host: null pointer";
+    return -1;
+  }
+  return guard<int32_t>(-1, [&] {
+    phy::unpin_host(ptr);
+    return 0;
+  });
+}
+
 int32_t phy_fluid_synchronize(PhyWorldHandle* w) {
   World* W = as_world(w);
   if (!W) return -1;
@@ -539,20 +559,28 @@ int32_t phy_fluid_step_backward(PhyWorldHandle* w, uint32_t sub, const double* g
   });
 }
 
-int32_t phy_fluid_autotune(PhyWorldHandle* w, uint32_t sub, double dt, uint32_t steps, PhyTuneTrial* out,
-                           uint32_t cap, uint32_t* n_out) {
+int32_t phy_fluid_autotune_horizon(PhyWorldHandle* w, uint32_t sub, double dt, uint32_t steps, uint32_t horizon,
+                                   PhyTuneTrial* out, uint32_t cap, uint32_t* n_out) {
   return guard<int32_t>(-1, [&] {
-    const std::vector<TuneTrial> trials = sub_of(w, sub).world->autotune(dt, (int)steps);
+    if (horizon > (1u << 30)) throw std::invalid_argument("autotune: horizon too large");
+    const std::vector<TuneTrial> trials = sub_of(w, sub).world->autotune(dt, (int)steps, (int)horizon);
     for (size_t k = 0; out && k < trials.size() && k < cap; ++k) {
       out[k].ctas_per_sm = trials[k].tuning.ctas_per_sm;
       out[k].queue = trials[k].tuning.queue;
       out[k].sort_block = trials[k].tuning.sort_block;
-      out[k].reserved = 0;
+      out[k].comp_tile = trials[k].comp_tile;
       out[k].ms_per_step = trials[k].ms_per_step;
+      out[k].samples = trials[k].samples;
+      out[k].reserved = 0;
     }
     if (n_out) *n_out = (uint32_t)trials.size();
     return 0;
   });
+}
+
+int32_t phy_fluid_autotune(PhyWorldHandle* w, uint32_t sub, double dt, uint32_t steps, PhyTuneTrial* out,
+                           uint32_t cap, uint32_t* n_out) {
+  return phy_fluid_autotune_horizon(w, sub, dt, steps, 0, out, cap, n_out);
 }
 
 const char* phy_fluid_last_error(void) { return g_last_error.c_str(); }

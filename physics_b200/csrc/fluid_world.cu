@@ -335,6 +335,7 @@ FluidWorld::FluidWorld(const SphParams& p, Precision prec) : params(p), prec_(pr
   stream_ = own_stream_;
   dalloc(b_.flags, 1);
   dalloc(b_.counters, 2);
+  dalloc(b_.order_count, 1);
   cuda_check(cudaMemsetAsync(b_.flags, 0, sizeof(uint32_t), stream_), "memset");
   cuda_check(cudaMemsetAsync(b_.counters, 0, 2 * sizeof(unsigned long long), stream_), "memset");
 }
@@ -390,7 +391,7 @@ void FluidWorld::free_all() {
   dfree(b_.boxes);
   dfree(b_.queue);
   dfree(b_.tile_crowd);
-  dfree(b_.dense_cells);
+  dfree(b_.dense_q0);
   dfree(b_.okey);
   dfree(b_.cell_of);
   dfree(b_.rank);
@@ -401,6 +402,7 @@ void FluidWorld::free_all() {
   dfree(b_.stage);
   dfree(b_.flags);
   dfree(b_.counters);
+  dfree(b_.order_count);
 }
 
 void FluidWorld::set_stream(cudaStream_t s) {
@@ -454,7 +456,7 @@ void FluidWorld::ensure_capacity(size_t n) {
   dfree(b_.tile_head);
   dfree(b_.tile_slot);
   dfree(b_.tile_crowd);
-  dfree(b_.dense_cells);
+  dfree(b_.dense_q0);
   dfree(b_.okey);
   dgrow(b_.cell_of, 0, cap, s);
   dgrow(b_.rank, 0, cap, s);
@@ -480,15 +482,17 @@ void FluidWorld::ensure_mode_buffers() {
     if (!b_.tile_slot) dalloc(b_.tile_slot, cap + 1);
     if (!b_.tile_crowd) dalloc(b_.tile_crowd, cap + 1);
     if (!b_.num_tiles) dalloc(b_.num_tiles, 1);
-    if (!b_.queue) dalloc(b_.queue, 3);
-    if (!b_.dense_cells) dalloc(b_.dense_cells, cap);
+    if (!b_.queue) dalloc(b_.queue, 5);
+    // Dense-cell tasks: at most one per 32 particles plus one per occupied cell.
+    if (!b_.dense_q0) dalloc(b_.dense_q0, cap + cap / 32 + 64);
     if (!b_.okey) dalloc(b_.okey, cap);
   }
   ++alloc_gen_;
 }
 
 void FluidWorld::set_comp_tile(int t) {
-  if (t != 0 && t != 4) throw std::invalid_argument("comp tile must be 0 (x-major runs) or 4");
+  if (t != 0 && t != 2 && t != 4)
+    throw std::invalid_argument("comp tile must be 0 (x-major runs), 2 or 4 (cells per tile edge)");
   if (t == 0 && !scenes_.empty()) throw std::invalid_argument("batched scenes need the tiled form (comp tile 4)");
   comp_tile_ = t;
   ensure_mode_buffers();
@@ -716,6 +720,9 @@ StepConsts FluidWorld::make_consts(double dt) const {
   c.n_visc_k = (int)params.visc_k.size();
   for (size_t k = 0; k < params.visc_k.size() && k < (size_t)kMaxMaterials; ++k) c.visc_k[k] = params.visc_k[k];
   for (size_t k = 0; k < params.visc_n.size() && k < (size_t)kMaxMaterials; ++k) c.visc_n[k] = params.visc_n[k];
+  c.shear_live = 0;
+  for (int k = 0; k < c.n_visc_k && k < kMaxMaterials; ++k)
+    if (!(c.visc_n[k] == 1.0)) c.shear_live = 1;  // NaN exponents keep it live too
   c.n = (int)n_;
   c.bx0 = bx0_[0];
   c.by0 = bx0_[1];
@@ -725,7 +732,7 @@ StepConsts FluidWorld::make_consts(double dt) const {
   c.ncz = nc_[2];
   c.ncells = ncells_;
   c.tile = tile_;
-  c.tile_log2 = tile_ == 4 ? 2 : 0;
+  c.tile_log2 = tile_ == 4 ? 2 : (tile_ == 2 ? 1 : 0);
   c.halo_cap = halo_cap_;
   c.boxes = tile_ ? b_.boxes : nullptr;
   c.n_scenes = scenes_.empty() ? 1 : (int)scenes_.size();
@@ -887,6 +894,24 @@ void FluidWorld::get_field(int field, double* out) {
   cuda_check(cudaMemcpyAsync(out, st, (size_t)nc * n_ * sizeof(double), cudaMemcpyDeviceToHost, stream_),
              "get_field copy");
   cuda_check(cudaStreamSynchronize(stream_), "get_field sync");
+}
+
+void FluidWorld::get_vec_f64(int field, double* out, size_t count) {
+  if (field != PHY_FIELD_POS && field != PHY_FIELD_VEL) throw std::invalid_argument("get_vec_f64: pos or vel only");
+  if (n_ == 0 || count == 0) return;
+  if (count > n_) count = n_;
+  const int n = (int)n_;
+  const ParticleConsts& pc = b_.pc[b_.cur];
+  double* st = b_.stage;
+  const int o = field == PHY_FIELD_POS ? 0 : 3;
+  k_get_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, b_.pv1[o], b_.pv1[o + 1], b_.pv1[o + 2], st);
+  cuda_check(cudaGetLastError(), "get_vec_f64 kernel");
+  // The stage is in insertion order, so the first `count` particles are its
+  // first 3 * count values: one copy straight into the caller's buffer (a DMA
+  // when the caller registered it with phy_fluid_pin_host).
+  cuda_check(cudaMemcpyAsync(out, st, 3 * count * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+             "get_vec_f64 copy");
+  cuda_check(cudaStreamSynchronize(stream_), "get_vec_f64 sync");
 }
 
 void FluidWorld::get_vec_f32(int field, float* out, size_t count) {
@@ -1178,9 +1203,10 @@ void FluidWorld::clear_scenes() {
 // step reads and the outputs it leaves: pv1, the current per-particle
 // constants, rho, p, acc, xsph and mu.  The saved copy is kept until
 // release_snapshot().
-void FluidWorld::snapshot(bool restore) {
+void FluidWorld::snapshot(bool restore, int slot) {
+  if (slot < 0 || slot >= kSnapSlots) throw std::logic_error("snapshot: slot out of range");
   const size_t n = n_;
-  if (restore) b_.cur = snap_cur_;
+  if (restore) b_.cur = snap_cur_[slot];
   ParticleConsts& pc = b_.pc[b_.cur];
   std::vector<std::pair<void*, size_t>> arrays;
   for (int k = 0; k < 6; ++k) arrays.push_back({b_.pv1[k], n * 8});
@@ -1205,83 +1231,140 @@ void FluidWorld::snapshot(bool restore) {
     total += (arrays[q].second + 255) / 256 * 256;
   }
   if (!restore) {
-    if (total > snap_bytes_) {
-      release_snapshot();
-      dalloc(snap_arena_, total / 8);
-      snap_bytes_ = total;
+    if (total > snap_bytes_[slot]) {
+      dfree(snap_arena_[slot]);
+      snap_bytes_[slot] = 0;
+      dalloc(snap_arena_[slot], total / 8);
+      snap_bytes_[slot] = total;
     }
     for (size_t q = 0; q < arrays.size(); ++q)
-      cuda_check(cudaMemcpyAsync(reinterpret_cast<char*>(snap_arena_) + off[q], arrays[q].first, arrays[q].second,
-                                 cudaMemcpyDeviceToDevice, stream_),
+      cuda_check(cudaMemcpyAsync(reinterpret_cast<char*>(snap_arena_[slot]) + off[q], arrays[q].first,
+                                 arrays[q].second, cudaMemcpyDeviceToDevice, stream_),
                  "snapshot");
-    snap_cur_ = b_.cur;
-    snap_count_ = arrays.size();
+    snap_cur_[slot] = b_.cur;
+    snap_count_[slot] = arrays.size();
   } else {
-    if (snap_count_ != arrays.size() || !snap_arena_) throw std::logic_error("snapshot: no saved state of this layout");
+    if (snap_count_[slot] != arrays.size() || !snap_arena_[slot])
+      throw std::logic_error("snapshot: no saved state of this layout");
     for (size_t q = 0; q < arrays.size(); ++q)
-      cuda_check(cudaMemcpyAsync(arrays[q].first, reinterpret_cast<char*>(snap_arena_) + off[q], arrays[q].second,
-                                 cudaMemcpyDeviceToDevice, stream_),
+      cuda_check(cudaMemcpyAsync(arrays[q].first, reinterpret_cast<char*>(snap_arena_[slot]) + off[q],
+                                 arrays[q].second, cudaMemcpyDeviceToDevice, stream_),
                  "restore");
   }
   cuda_check(cudaStreamSynchronize(stream_), "snapshot sync");
 }
 
 void FluidWorld::release_snapshot() {
-  dfree(snap_arena_);
-  snap_bytes_ = 0;
-  snap_count_ = 0;
+  for (int q = 0; q < kSnapSlots; ++q) {
+    dfree(snap_arena_[q]);
+    snap_bytes_[q] = 0;
+    snap_count_[q] = 0;
+  }
 }
 
-std::vector<TuneTrial> FluidWorld::autotune(double dt, int steps) {
+double FluidWorld::time_tuning(const LaunchTuning& t, int comp_tile, double dt, int steps, int nslots,
+                               cudaEvent_t e0, cudaEvent_t e1) {
+  double total = 0.0;
+  for (int slot = 0; slot < nslots; ++slot) {
+    snapshot(true, slot);
+    tuning_ = t;
+    if (comp_tile != comp_tile_) set_comp_tile(comp_tile);
+    step_n(dt, 1);  // warm-up (and graph capture when chunked)
+    if (graph_chunk_ > 0) step_n(dt, graph_chunk_);
+    cuda_check(cudaEventRecord(e0, stream_), "event");
+    step_n(dt, steps);
+    cuda_check(cudaEventRecord(e1, stream_), "event");
+    cuda_check(cudaEventSynchronize(e1), "event sync");
+    float ms = 0.f;
+    cuda_check(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+    total += (double)ms / steps;
+  }
+  return total / nslots;
+}
+
+// Candidates: sort block 128/256, static tile stride or work queue, 1..the
+// occupancy limit of CTAs per SM, and (tiled worlds) 4 or 2 cells per tile
+// edge.  With horizon > 0 the states the run will meet are sampled first:
+// the current state, and the states after horizon/2 and horizon steps of the
+// current configuration.  Every candidate runs `steps` steps from the first
+// sample; the kKeep fastest then also run from the other samples, and the
+// fastest mean over all samples wins (successive halving keeps the tuning
+// time near one pass over the candidates).  The world returns to its
+// starting state.
+std::vector<TuneTrial> FluidWorld::autotune(double dt, int steps, int horizon) {
   std::vector<TuneTrial> trials;
   if (n_ == 0 || steps <= 0) return trials;
   if (timing_) throw std::invalid_argument("autotune: phase timing is on");
-  std::vector<LaunchTuning> cands;
+  if (horizon < 0) throw std::invalid_argument("autotune: negative horizon");
   const bool tiled = prec_ == Precision::F32Comp && comp_tile_ > 0;
   const int max_per_sm = tiled ? tiled_max_ctas_per_sm() : 1;
-  for (int sort_block : {128, 256})
-    for (int queue = 0; queue <= (tiled ? 1 : 0); ++queue)
-      for (int per = 1; per <= max_per_sm; ++per) {
-        LaunchTuning t;
-        t.ctas_per_sm = tiled ? per : 0;
-        t.queue = queue;
-        t.sort_block = sort_block;
-        cands.push_back(t);
-      }
+  std::vector<std::pair<LaunchTuning, int>> cands;
+  const std::vector<int> tiles = tiled ? std::vector<int>{4, 2} : std::vector<int>{comp_tile_};
+  for (int tile : tiles)
+    for (int sort_block : {128, 256})
+      for (int queue = 0; queue <= (tiled ? 1 : 0); ++queue)
+        for (int per = 1; per <= max_per_sm; ++per) {
+          LaunchTuning t;
+          t.ctas_per_sm = tiled ? per : 0;
+          t.queue = queue;
+          t.sort_block = sort_block;
+          cands.push_back({t, tile});
+        }
   const LaunchTuning saved = tuning_;
-  snapshot(false);
+  const int saved_tile = comp_tile_;
+  snapshot(false, 0);
+  int nslots = 1;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cuda_check(cudaEventCreate(&e0), "event");
   cuda_check(cudaEventCreate(&e1), "event");
+  auto restore_start = [&]() {
+    tuning_ = saved;
+    if (comp_tile_ != saved_tile) set_comp_tile(saved_tile);
+    snapshot(true, 0);
+  };
   try {
-    for (const LaunchTuning& t : cands) {
-      tuning_ = t;
-      step_n(dt, 1);  // warm-up (and graph capture when chunked)
-      if (graph_chunk_ > 0) step_n(dt, graph_chunk_);
-      cuda_check(cudaEventRecord(e0, stream_), "event");
-      step_n(dt, steps);
-      cuda_check(cudaEventRecord(e1, stream_), "event");
-      cuda_check(cudaEventSynchronize(e1), "event sync");
-      float ms = 0.f;
-      cuda_check(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
-      trials.push_back({t, (double)ms / steps});
-      snapshot(true);  // every candidate starts from the same state
+    if (horizon > 0) {
+      step_n(dt, horizon / 2);
+      snapshot(false, 1);
+      step_n(dt, horizon - horizon / 2);
+      snapshot(false, 2);
+      nslots = 3;
     }
+    for (const auto& cand : cands)
+      trials.push_back({cand.first, cand.second, time_tuning(cand.first, cand.second, dt, steps, 1, e0, e1), 1});
+    if (nslots > 1) {
+      constexpr size_t kKeep = 6;
+      std::vector<size_t> order(trials.size());
+      for (size_t q = 0; q < order.size(); ++q) order[q] = q;
+      std::stable_sort(order.begin(), order.end(),
+                       [&](size_t x, size_t y) { return trials[x].ms_per_step < trials[y].ms_per_step; });
+      for (size_t r = 0; r < std::min(kKeep, order.size()); ++r) {
+        TuneTrial& tr = trials[order[r]];
+        tr.ms_per_step = time_tuning(tr.tuning, tr.comp_tile, dt, steps, nslots, e0, e1);
+        tr.samples = nslots;
+      }
+    }
+    restore_start();
   } catch (...) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    tuning_ = saved;
-    snapshot(true);
+    try {
+      restore_start();
+    } catch (...) {
+    }
     release_snapshot();
     throw;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   release_snapshot();
-  size_t best = 0;
-  for (size_t q = 1; q < trials.size(); ++q)
-    if (trials[q].ms_per_step < trials[best].ms_per_step) best = q;
+  // The fastest among the trials that ran on every sample.
+  size_t best = trials.size();
+  for (size_t q = 0; q < trials.size(); ++q)
+    if (trials[q].samples == nslots && (best == trials.size() || trials[q].ms_per_step < trials[best].ms_per_step))
+      best = q;
   tuning_ = trials[best].tuning;
+  if (trials[best].comp_tile != comp_tile_) set_comp_tile(trials[best].comp_tile);
   return trials;
 }
 
@@ -1450,20 +1533,41 @@ void FluidWorld::couple_bodies(PhyCoupleBody* bodies, uint32_t nb, const double*
   if (!scenes_.empty()) throw std::invalid_argument("couple_bodies: not available for batched scenes");
   if (tape_.on) throw std::invalid_argument("couple_bodies: the adjoint tape does not record coupling");
   if (nb > (1u << 20)) throw std::invalid_argument("couple_bodies: more than 2^20 bodies");
+  // A leaf shape's data ranges (convex vertices and faces, heightfield heights).
+  auto check_leaf = [&](int shape, uint64_t data_first, uint64_t data_count, uint64_t face_first,
+                        uint64_t face_count) {
+    if (shape < PHY_SHAPE_SPHERE || shape > PHY_SHAPE_HEIGHTFIELD)
+      throw std::invalid_argument("couple_bodies: unsupported shape (compound shapes cannot nest)");
+    if (shape == PHY_SHAPE_CONVEX) {
+      if (data_count == 0 || !data || data_first + 3ull * data_count > n_data)
+        throw std::invalid_argument("couple_bodies: convex vertices out of range");
+      if ((face_count && !faces) || 3ull * (face_first + face_count) > n_faces)
+        throw std::invalid_argument("couple_bodies: convex faces out of range");
+      for (uint64_t f = 3ull * face_first; f < 3ull * (face_first + face_count); ++f)
+        if (faces[f] >= data_count) throw std::invalid_argument("couple_bodies: face index out of range");
+    } else if (shape == PHY_SHAPE_HEIGHTFIELD) {
+      if ((data_count && !data) || data_first + data_count > n_data)
+        throw std::invalid_argument("couple_bodies: heights out of range");
+    }
+  };
   for (uint32_t k = 0; k < nb; ++k) {
     const PhyCoupleBody& b = bodies[k];
-    if (b.shape < PHY_SHAPE_SPHERE || b.shape > PHY_SHAPE_HEIGHTFIELD)
-      throw std::invalid_argument("couple_bodies: unsupported shape");
-    if (b.shape == PHY_SHAPE_CONVEX) {
-      if (b.data_count == 0 || !data || (uint64_t)b.data_first + 3ull * b.data_count > n_data)
-        throw std::invalid_argument("couple_bodies: convex vertices out of range");
-      if ((b.face_count && !faces) || 3ull * ((uint64_t)b.face_first + b.face_count) > n_faces)
-        throw std::invalid_argument("couple_bodies: convex faces out of range");
-      for (uint64_t f = 3ull * b.face_first; f < 3ull * ((uint64_t)b.face_first + b.face_count); ++f)
-        if (faces[f] >= b.data_count) throw std::invalid_argument("couple_bodies: face index out of range");
-    } else if (b.shape == PHY_SHAPE_HEIGHTFIELD) {
-      if ((b.data_count && !data) || (uint64_t)b.data_first + b.data_count > n_data)
-        throw std::invalid_argument("couple_bodies: heights out of range");
+    if (b.shape != PHY_SHAPE_COMPOUND) {
+      check_leaf(b.shape, b.data_first, b.data_count, b.face_first, b.face_count);
+      continue;
+    }
+    // Shape::Compound: at least one sub shape (support_local reads the
+    // first, shape.rs:240), each a 16-double record of a leaf shape.
+    if (b.data_count == 0 || !data || (uint64_t)b.data_first + 16ull * b.data_count > n_data)
+      throw std::invalid_argument("couple_bodies: compound sub shapes out of range");
+    for (uint32_t q = 0; q < b.data_count; ++q) {
+      const double* r = data + b.data_first + 16ull * q;
+      for (int f = 11; f < 15; ++f)
+        if (!(r[f] >= 0.0 && r[f] < 4294967296.0 && r[f] == std::floor(r[f])))
+          throw std::invalid_argument("couple_bodies: compound sub shape with an invalid data range");
+      if (!(r[0] >= 0.0 && r[0] <= 4.0 && r[0] == std::floor(r[0])))
+        throw std::invalid_argument("couple_bodies: unsupported shape (compound shapes cannot nest)");
+      check_leaf((int)r[0], (uint64_t)r[11], (uint64_t)r[12], (uint64_t)r[13], (uint64_t)r[14]);
     }
   }
   ensure_cells();
@@ -1760,10 +1864,16 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
     snapshot(true);
   } catch (...) {
     cleanup();
-    if (snap_count_) snapshot(true);
+    if (snap_count_[0]) snapshot(true);
     throw;
   }
   cleanup();
 }
+
+void pin_host(void* ptr, size_t bytes) {
+  cuda_check(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault), "cudaHostRegister");
+}
+
+void unpin_host(void* ptr) { cuda_check(cudaHostUnregister(ptr), "cudaHostUnregister"); }
 
 }  // namespace phy

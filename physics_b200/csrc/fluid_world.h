@@ -51,7 +51,9 @@ void cuda_check(cudaError_t e, const char* what);
 // One configuration of the launch knobs and its measured step time.
 struct TuneTrial {
   LaunchTuning tuning;
-  double ms_per_step;
+  int comp_tile;       // cells per tile edge of the trial (0: not a tiled world)
+  double ms_per_step;  // mean over the sampled states the trial ran on
+  int samples;         // sampled states it ran on
 };
 
 class FluidWorld {
@@ -99,7 +101,7 @@ class FluidWorld {
   // fastest is kept.  Returns the trials in order.
   void set_launch_tuning(const LaunchTuning& t) { tuning_ = t; }
   LaunchTuning launch_tuning() const { return tuning_; }
-  std::vector<TuneTrial> autotune(double dt, int steps);
+  std::vector<TuneTrial> autotune(double dt, int steps, int horizon = 0);
 
   // Adjoint of the f64 plain step (world.rs:183-397).  tape_begin makes the
   // current state checkpoint 0 and records every following step's dt, with a
@@ -121,6 +123,9 @@ class FluidWorld {
   // Position or velocity as f32 (an exact `as f32` cast of each f64 value,
   // made on the device so half the bytes cross to the host): the first
   // `count` particles in insertion order, xyz interleaved.
+  // The first `count` particles' xyz (pos or vel) in insertion order, copied
+  // straight into `out` (no host bounce).
+  void get_vec_f64(int field, double* out, size_t count);
   void get_vec_f32(int field, float* out, size_t count);
   void set_field(int field, const double* in);
 
@@ -200,8 +205,12 @@ class FluidWorld {
   void enqueue_step(const StepConsts& c, const PassEvents& pe, const cudaEvent_t* ev);
   void run_graph(double dt, int k);
   void drop_graphs();
-  void snapshot(bool restore);
+  void snapshot(bool restore, int slot = 0);
   void release_snapshot();
+  // Mean ms per step of `steps` steps from each saved slot 0..nslots-1 under
+  // tuning t (warm-up and graph capture first).
+  double time_tuning(const LaunchTuning& t, int comp_tile, double dt, int steps, int nslots, cudaEvent_t e0,
+                     cudaEvent_t e1);
 
   Precision prec_;
   double h0_;
@@ -274,11 +283,13 @@ class FluidWorld {
   std::vector<uint32_t*> adj_slot_u_;
   std::vector<size_t> adj_slot_ucount_;
   bool recomputing_ = false;
-  // Saved state (autotuner, reverse sweep): one arena reused while large enough.
-  double* snap_arena_ = nullptr;
-  size_t snap_bytes_ = 0;
-  size_t snap_count_ = 0;
-  int snap_cur_ = 0;
+  // Saved states (autotuner, reverse sweep): per slot one arena reused while
+  // large enough.
+  static constexpr int kSnapSlots = 3;
+  double* snap_arena_[kSnapSlots] = {};
+  size_t snap_bytes_[kSnapSlots] = {};
+  size_t snap_count_[kSnapSlots] = {};
+  int snap_cur_[kSnapSlots] = {};
 };
 
 // FluidSubsystem<T> (subsystem.rs:26-55): the world plus coupling coefficients.
@@ -299,5 +310,9 @@ class World {
   int step_checked(double dt);     // world.rs:282-293
   size_t fluid_count() const;
 };
+
+// cudaHostRegister / cudaHostUnregister of a caller's buffer (throws on error).
+void pin_host(void* ptr, size_t bytes);
+void unpin_host(void* ptr);
 
 }  // namespace phy

@@ -13,6 +13,8 @@
 // 256-thread blocks and grid-stride loops sized to a multiple of the SM count.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "sph_buffers.h"
 
 namespace phy {
@@ -200,15 +202,27 @@ __global__ void __launch_bounds__(kThreads) k_scatter(int n, const uint32_t* __r
   tmp[cell_start[cell_of[i]] + rank[i]] = (uint32_t)i;
 }
 
-// Final slot of every particle: its rank by insertion index among the
-// particles of its cell.  The overflow cell keeps arrival order (its
-// particles never interact).
+// Cells up to kOrderSmall particles are ordered by k_order (each particle
+// counts the smaller keys of its cell); cells up to kOrderLarge by a bitonic
+// sort in shared memory (k_order_large); larger cells fall back to counting.
+constexpr uint32_t kOrderSmall = 64;
+constexpr uint32_t kOrderLarge = 4096;
+constexpr int kOrderThreads = 512;
+
+// Final slot of every particle: its rank by insertion index (or by in-cell
+// order key) among the particles of its cell.  The overflow cell keeps
+// arrival order (its particles never interact).  Cells of kOrderSmall <
+// count <= kOrderLarge particles are left to k_order_large: the thread of
+// their first slot appends them to `large` (a list in any order; each cell's
+// result does not depend on it).
 __global__ void __launch_bounds__(kThreads) k_order(int n, int ncells, const uint32_t* __restrict__ cell_of,
                                                     const uint32_t* __restrict__ cell_start,
                                                     const uint32_t* __restrict__ tmp,
                                                     const uint32_t* __restrict__ id,
                                                     const unsigned long long* __restrict__ okey,
-                                                    uint32_t* __restrict__ perm) {
+                                                    uint32_t* __restrict__ perm,
+                                                    uint32_t* __restrict__ large,
+                                                    uint32_t* __restrict__ large_count) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   uint32_t i = tmp[s];
@@ -218,6 +232,10 @@ __global__ void __launch_bounds__(kThreads) k_order(int n, int ncells, const uin
     return;
   }
   uint32_t cs = cell_start[cell], ce = cell_start[cell + 1];
+  if (ce - cs > kOrderSmall && ce - cs <= kOrderLarge) {
+    if ((uint32_t)s == cs) large[atomicAdd(large_count, 1u)] = cell;
+    return;
+  }
   uint32_t r = 0;
   if (okey) {
     const unsigned long long mine = okey[i];
@@ -227,6 +245,67 @@ __global__ void __launch_bounds__(kThreads) k_order(int n, int ncells, const uin
     for (uint32_t k = cs; k < ce; ++k) r += id[tmp[k]] < mine ? 1u : 0u;
   }
   perm[cs + r] = i;
+}
+
+// Order key of particle i: the in-cell order key (tiled form) or the
+// insertion index.
+__device__ __forceinline__ unsigned long long order_key(const unsigned long long* okey, const uint32_t* id,
+                                                        uint32_t i) {
+  return okey ? okey[i] : (unsigned long long)id[i];
+}
+
+// The cells k_order left: one CTA per cell (persistent grid over the
+// device-side list) sorts the cell's (key, particle) pairs in shared memory
+// with a bitonic network padded to a power of two (keys are unique: they end
+// in the insertion index), then writes them to their final slots.
+__global__ void __launch_bounds__(kOrderThreads) k_order_large(const uint32_t* __restrict__ cell_start,
+                                                              const uint32_t* __restrict__ tmp,
+                                                              const uint32_t* __restrict__ id,
+                                                              const unsigned long long* __restrict__ okey,
+                                                              const uint32_t* __restrict__ large,
+                                                              const uint32_t* __restrict__ large_count,
+                                                              uint32_t* __restrict__ perm) {
+  __shared__ unsigned long long s_key[kOrderLarge];
+  __shared__ uint32_t s_val[kOrderLarge];
+  const uint32_t nl = *large_count;
+  for (uint32_t w = blockIdx.x; w < nl; w += gridDim.x) {
+    const uint32_t cell = large[w];
+    const uint32_t cs = cell_start[cell], cnt = cell_start[cell + 1] - cs;
+    uint32_t m = 1;
+    while (m < cnt) m <<= 1;
+    __syncthreads();  // the previous cell's pairs are written out
+    for (uint32_t k = threadIdx.x; k < m; k += kOrderThreads) {
+      if (k < cnt) {
+        const uint32_t i = tmp[cs + k];
+        s_key[k] = order_key(okey, id, i);
+        s_val[k] = i;
+      } else {
+        s_key[k] = ~0ull;  // padding sorts last
+        s_val[k] = 0;
+      }
+    }
+    __syncthreads();
+    for (uint32_t size = 2; size <= m; size <<= 1) {
+      for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+        for (uint32_t k = threadIdx.x; k < m / 2; k += kOrderThreads) {
+          // Element pair (lo, lo + stride) of compare step k.
+          const uint32_t lo = 2 * k - (k & (stride - 1));
+          const uint32_t hi = lo + stride;
+          const bool up = (lo & size) == 0;
+          const unsigned long long a = s_key[lo], b = s_key[hi];
+          if ((a > b) == up) {
+            s_key[lo] = b;
+            s_key[hi] = a;
+            const uint32_t t = s_val[lo];
+            s_val[lo] = s_val[hi];
+            s_val[hi] = t;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (uint32_t k = threadIdx.x; k < cnt; k += kOrderThreads) perm[cs + k] = s_val[k];
+  }
 }
 
 struct GatherArgs {
@@ -268,9 +347,11 @@ __global__ void __launch_bounds__(kThreads) k_gather(int n, const uint32_t* __re
                             (float)(z - (double)kz * g.h0), (float)g.dst.mass[s]);
     g.cvel[s] = make_float4((float)g.dst_pv[3][s], (float)g.dst_pv[4][s], (float)g.dst_pv[5][s], 0.0f);
     if (s == 0 && g.queue) {
-      g.queue[0] = 0;  // density and force work queues
+      g.queue[0] = 0;  // density and force tile queues
       g.queue[1] = 0;
-      g.queue[2] = 0;  // dense-cell count
+      g.queue[2] = 0;  // dense-cell task count
+      g.queue[3] = 0;  // dense-cell tasks taken by the density and force passes
+      g.queue[4] = 0;
     }
   }
 }
@@ -366,6 +447,18 @@ __global__ void k_u32_from_f64(const double* src, uint32_t* dst, int n) {
 
 }  // namespace
 
+// Persistent grid of k_order_large: its resident CTAs on every SM.
+static int order_large_blocks() {
+  static const int blocks = [] {
+    int dev = 0, sms = 1, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_order_large, kOrderThreads, 0);
+    return std::max(sms, 1) * std::max(per, 1);
+  }();
+  return blocks;
+}
+
 // Cells scanned per step: the box plus the overflow cell, rounded up to whole
 // scan tiles (the padding stays zero, so the prefix at index ncells+1 is n).
 static int scan_length(int ncells) { return ((ncells + 2 + kScanTile - 1) / kScanTile) * kScanTile; }
@@ -389,7 +482,12 @@ static void build_cells(const StepConsts& c, DevBuffers& b, cudaStream_t s, int 
   k_scan_top<<<1, 1024, 0, s>>>(b.block_sums, nb);
   k_scan_apply<<<nb, kThreads, 0, s>>>(b.cell_start, b.block_sums);
   k_scatter<<<grid_for(n, bs), bs, 0, s>>>(n, b.cell_of, b.rank, b.cell_start, b.tmp);
-  k_order<<<grid_for(n, bs), bs, 0, s>>>(n, c.ncells, b.cell_of, b.cell_start, b.tmp, src.id, okey, b.perm);
+  // `rank` is free after the scatter: it holds the list of large cells.
+  cudaMemsetAsync(b.order_count, 0, sizeof(uint32_t), s);
+  k_order<<<grid_for(n, bs), bs, 0, s>>>(n, c.ncells, b.cell_of, b.cell_start, b.tmp, src.id, okey, b.perm,
+                                         b.rank, b.order_count);
+  k_order_large<<<order_large_blocks(), kOrderThreads, 0, s>>>(b.cell_start, b.tmp, src.id, okey, b.rank,
+                                                               b.order_count, b.perm);
 }
 
 void launch_cell_index(const StepConsts& c, DevBuffers& b, uint32_t* flags, cudaStream_t s) {

@@ -265,11 +265,16 @@ extern "C" int32_t phy_fluid_density_noalloc(const PhySphParams* params, uint64_
     long long cells = 1;
     int nc[3];
     for (int a = 0; a < 3; ++a) {
-      const long long d = bb[3 + a] - bb[a] + 3;  // one empty cell of padding on each side
-      if (d <= 0 || d > kMaxCells || (cells *= d) > kMaxCells)
+      // Every particle has a key (non-finite coordinates map to 0), so
+      // min <= max and the span is exact in unsigned 64-bit arithmetic even
+      // when the keys sit near opposite ends of the int64 range.
+      const unsigned long long span = (unsigned long long)bb[3 + a] - (unsigned long long)bb[a];
+      // The padding cell below the box must have an int64 key too.
+      if (bb[3 + a] < bb[a] || bb[a] == LLONG_MIN || bb[3 + a] == LLONG_MAX || span > (unsigned long long)kMaxCells ||
+          (cells *= (long long)span + 3) > kMaxCells)  // one empty cell of padding on each side
         throw std::invalid_argument("phy_fluid_density_noalloc: the particles span more than " +
                                     std::to_string(kMaxCells) + " grid cells (padded bounding box)");
-      nc[a] = (int)d;
+      nc[a] = (int)span + 3;
     }
     c.bx0 = bb[0] - 1;
     c.by0 = bb[1] - 1;

@@ -60,12 +60,13 @@ struct DevBuffers {
   uint8_t* tile_crowd = nullptr;  // 1: tile above kDenseMean per occupied cell
   uint32_t* num_tiles = nullptr;
   // Scene boxes of the tiled linearisation (one entry for a single world),
-  // the work-queue counters of the persistent passes (density, force) and the
-  // dense-cell count, and the dense-cell list (cells of tiles too dense to
-  // stage).
+  // the work counters of the persistent passes ([0] density tiles, [1] force
+  // tiles, [2] dense-cell task count, [3] density tasks taken, [4] force tasks
+  // taken), and the dense-cell tasks (first slot of up to 32 particles of one
+  // cell of a tile too dense to stage).
   SceneBox* boxes = nullptr;
   uint32_t* queue = nullptr;
-  uint32_t* dense_cells = nullptr;
+  uint32_t* dense_q0 = nullptr;
   // Sort scratch.
   uint32_t* cell_of = nullptr;
   uint32_t* rank = nullptr;
@@ -80,6 +81,7 @@ struct DevBuffers {
   // Insertion-order staging for uploads and downloads (f64 and u32 views).
   double* stage = nullptr;   // 8 * capacity doubles
   uint32_t* flags = nullptr; // error bits, device
+  uint32_t* order_count = nullptr;  // sort: cells of more than kOrderSmall particles (device count)
   unsigned long long* counters = nullptr;  // candidates, pairs (device)
   // Optional outputs of the f64 plain force pass for the adjoint's tape: the
   // raw viscous force and the strain-rate proxy of every sorted slot.

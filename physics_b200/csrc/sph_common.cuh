@@ -62,6 +62,11 @@ struct StepConsts {
   int n_visc_k;
   int n;
   double visc_k[kMaxMaterials], visc_n[kMaxMaterials];
+  // 0 when visc_n[m] == 1 for every reachable material m < n_visc_k: then
+  // mu = visc_k[m] * max(shear, shear_min)^0 = visc_k[m] exactly
+  // (world.rs:319-327) and the shear sum is never observed, so the force
+  // passes skip it (the same bits either way).
+  int shear_live;
   // Grid box: key of cell 0 and dimensions (cells per axis).
   long long bx0, by0, bz0;
   int ncx, ncy, ncz;

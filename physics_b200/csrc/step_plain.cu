@@ -148,7 +148,9 @@ struct PlainAcc {
 };
 
 // One neighbour of compute_forces' loop body (world.rs:291-316), in the
-// reference's expression order.
+// reference's expression order.  kShear = false leaves out the shear sum
+// (StepConsts::shear_live: every reachable visc_n is 1, so mu never reads it).
+template <bool kShear>
 __device__ __forceinline__ void plain_pair(const StepConsts& c, const PlainArgs& a, int j, double xi, double yi,
                                            double zi, double vxi, double vyi, double vzi, double m_i,
                                            double pr2_i, PlainAcc& q) {
@@ -185,13 +187,16 @@ __device__ __forceinline__ void plain_pair(const StepConsts& c, const PlainArgs&
   q.xsy = __dadd_rn(q.xsy, __dmul_rn(dvy, xw));
   q.xsz = __dadd_rn(q.xsz, __dmul_rn(dvz, xw));
   // shear += |v_j - v_i| / (r + 1e-4) * (m_j / rho_j)   (314-315)
-  const double dvn = __dsqrt_rn(norm2(dvx, dvy, dvz));
-  q.shear = __dadd_rn(q.shear, __dmul_rn(__ddiv_rn(dvn, __dadd_rn(r, 1e-4)), mr_j));
+  if (kShear) {
+    const double dvn = __dsqrt_rn(norm2(dvx, dvy, dvz));
+    q.shear = __dadd_rn(q.shear, __dmul_rn(__ddiv_rn(dvn, __dadd_rn(r, 1e-4)), mr_j));
+  }
 }
 
 // compute_forces (world.rs:252-347) fused with integrate (352-363) and
 // enforce_bounds (366-397).  The neighbours come from the density pass's list
 // (same visit order); a particle whose list overflowed rescans its 27 cells.
+template <bool kShear>
 __global__ void __launch_bounds__(kThreads) k_force_plain(StepConsts c, PlainArgs a) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.n) return;
@@ -203,7 +208,7 @@ __global__ void __launch_bounds__(kThreads) k_force_plain(StepConsts c, PlainArg
   if (cnt <= (uint32_t)kMaxNeighbors) {
     const uint32_t* lst = a.nbr + i;
     for (uint32_t k = 0; k < cnt; ++k)
-      plain_pair(c, a, (int)lst[(size_t)k * a.stride], xi, yi, zi, vxi, vyi, vzi, m_i, pr2_i, q);
+      plain_pair<kShear>(c, a, (int)lst[(size_t)k * a.stride], xi, yi, zi, vxi, vyi, vzi, m_i, pr2_i, q);
   } else {
     const long long kx = key_axis(xi, c.inv_cell);
     const long long ky = key_axis(yi, c.inv_cell);
@@ -214,7 +219,7 @@ __global__ void __launch_bounds__(kThreads) k_force_plain(StepConsts c, PlainArg
         const int c0 = base + (di * c.ncy + dj) * c.ncz;
         const int s = (int)a.cell_start[c0], e = (int)a.cell_start[c0 + 3];
         for (int j = s; j < e; ++j)
-          if (j != i) plain_pair(c, a, j, xi, yi, zi, vxi, vyi, vzi, m_i, pr2_i, q);
+          if (j != i) plain_pair<kShear>(c, a, j, xi, yi, zi, vxi, vyi, vzi, m_i, pr2_i, q);
       }
     }
   }
@@ -329,7 +334,10 @@ void launch_plain_passes(const StepConsts& c, DevBuffers& b, cudaStream_t s, con
   else
     k_density_plain<false><<<grid, kThreads, 0, s>>>(c, a);
   if (ev.after_density) cudaEventRecord(ev.after_density, s);
-  k_force_plain<<<grid, kThreads, 0, s>>>(c, a);
+  if (c.shear_live)
+    k_force_plain<true><<<grid, kThreads, 0, s>>>(c, a);
+  else
+    k_force_plain<false><<<grid, kThreads, 0, s>>>(c, a);
 }
 
 }  // namespace phy

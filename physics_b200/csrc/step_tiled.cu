@@ -1,11 +1,12 @@
 // FP32-compensated SPH passes over staged cell tiles.
 //
-// The sort orders cells in 4x4x4 tiles (tiled_index), so the particles of a
-// tile are one contiguous slot range.  A persistent grid walks the list of
-// occupied tiles; for each tile a CTA stages the particles of the tile's
-// 6x6x6-cell halo into shared memory once (about 3.4 stagings per particle
-// per pass instead of ~219 per-candidate gathers through L1/L2) and every
-// query particle of the tile reads its 27 neighbour cells from there.
+// The sort orders cells in TB x TB x TB tiles (tiled_index; TB = 4 by
+// default, or 2), so the particles of a tile are one contiguous slot range.
+// A persistent grid walks the list of occupied tiles; for each tile a CTA
+// stages the particles of the tile's (TB+2)^3-cell halo into shared memory
+// once (about 3.4 stagings per particle per pass at TB = 4, 8 at TB = 2,
+// instead of ~219 per-candidate gathers through L1/L2) and every query
+// particle of the tile reads its 27 neighbour cells from there.
 //
 // Arithmetic is the compensated form of step_comp.cu: f32 pair math on
 // tile-relative coordinates (cell offset + cell-local f32 coordinate, so the
@@ -31,13 +32,20 @@ namespace phy {
 
 namespace {
 
-constexpr int kTB = 4;                          // tile edge (cells)
-constexpr int kTL = 2;                          // log2(kTB)
-constexpr int kH = kTB + 2;                     // halo edge (cells)
-constexpr int kNH = kH * kH * kH;               // halo cells
+// Tile shape: TB cells per tile edge (4 or 2, the cells-per-tile knob), its
+// log2, the halo edge and the halo's cell count.
+template <int TB>
+struct Tile {
+  static_assert(TB == 2 || TB == 4, "tile edge 2 or 4");
+  static constexpr int B = TB;
+  static constexpr int L = TB == 4 ? 2 : 1;
+  static constexpr int H = TB + 2;
+  static constexpr int NH = H * H * H;
+};
+constexpr int kNHMax = Tile<4>::NH;             // halo table entries reserved in shared memory
 constexpr int kTT = 256;                        // threads per CTA
 constexpr int kHaloCap = 2000;                  // staged slots per tile (3 force CTAs fit an SM)
-static_assert(kNH <= kTT, "one halo cell per thread");
+static_assert(kNHMax <= kTT, "one halo cell per thread");
 static_assert(kHaloCap <= 65536, "16-bit slots");
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
@@ -77,10 +85,11 @@ struct TiledArgs {
   uint32_t* nbr_count;
   const uint16_t* __restrict__ scene;  // null: one scene
   uint32_t* queue;                      // null: static tile stride
-  // Cells of tiles too dense to stage (their halo does not fit even one
-  // x-slab), computed by the dense-cell kernels: list and device count.
-  uint32_t* dense_cells;
+  // Tasks of the dense-cell kernels (tiles too dense to stage): first slot of
+  // up to 32 consecutive particles of one cell, and the device task count.
+  uint32_t* dense_q0;
   uint32_t* dense_count;
+  uint32_t* dense_taken;  // [0]: tasks taken by the density pass, [1]: by the force pass
   int stride;
   uint32_t* flags;
   unsigned long long* counters;
@@ -151,13 +160,15 @@ struct TileGeom {
   uint32_t first, last;
 };
 
+template <int TB>
 __device__ __forceinline__ TileGeom tile_geom(const StepConsts& c, const TiledArgs& a, uint32_t k) {
+  using T = Tile<TB>;
   TileGeom g;
   g.first = a.tile_slot[k];
   g.last = a.tile_slot[k + 1];
   g.sc = a.scene ? (int)a.scene[g.first] : 0;
   const SceneBox& bx = c.boxes[g.sc];
-  const int t = (int)((a.sorted_cell[g.first] - (uint32_t)bx.cell_base) >> (3 * kTL));
+  const int t = (int)((a.sorted_cell[g.first] - (uint32_t)bx.cell_base) >> (3 * T::L));
   g.tz = t % bx.nt[2];
   g.ty = (t / bx.nt[2]) % bx.nt[1];
   g.tx = t / (bx.nt[2] * bx.nt[1]);
@@ -177,16 +188,18 @@ __device__ __forceinline__ uint32_t next_tile(uint32_t* queue, int pass, uint32_
 // Slot ranges of the tile's halo cells: s_src[h] / s_end[h] = global slot
 // range, s_off[h] = first staged slot; every cell's staged range is padded to
 // an even length (one far-away dummy particle), so all runs are pair-aligned.
-// s_off[kNH] = total staged slots.
+// s_off[T::NH] = total staged slots.
+template <int TB>
 __device__ __forceinline__ uint32_t halo_table(const StepConsts& c, const TiledArgs& a, const TileGeom& g,
                                                uint32_t* s_src, uint32_t* s_end, uint32_t* s_off, uint32_t* ws) {
+  using T = Tile<TB>;
   const int h = threadIdx.x;
   uint32_t cnt = 0, src = 0;
-  if (h < kNH) {
+  if (h < T::NH) {
     const SceneBox& bx = c.boxes[g.sc];
-    const int ax = g.tx * kTB - 1 + h / (kH * kH);
-    const int ay = g.ty * kTB - 1 + (h / kH) % kH;
-    const int az = g.tz * kTB - 1 + h % kH;
+    const int ax = g.tx * T::B - 1 + h / (T::H * T::H);
+    const int ay = g.ty * T::B - 1 + (h / T::H) % T::H;
+    const int az = g.tz * T::B - 1 + h % T::H;
     if (ax >= 0 && ay >= 0 && az >= 0 && ax < bx.nc[0] && ay < bx.nc[1] && az < bx.nc[2]) {
       const int lin = box_tiled_index(c, bx, ax, ay, az);
       src = a.cell_start[lin];
@@ -195,47 +208,52 @@ __device__ __forceinline__ uint32_t halo_table(const StepConsts& c, const TiledA
   }
   uint32_t total;
   const uint32_t off = block_scan((cnt + 1u) & ~1u, ws, total);
-  if (h < kNH) {
+  if (h < T::NH) {
     s_src[h] = src;
     s_end[h] = src + cnt;
     s_off[h] = off;
   }
-  if (h == 0) s_off[kNH] = total;
+  if (h == 0) s_off[T::NH] = total;
   __syncthreads();
   return total;
 }
 
 // Tile-relative f32 position of a particle staged from halo cell h.
+template <int TB>
 __device__ __forceinline__ float4 tile_rel(const StepConsts& c, float4 q, int h) {
-  const float ox = (float)(h / (kH * kH) - 1) * c.h0f;
-  const float oy = (float)((h / kH) % kH - 1) * c.h0f;
-  const float oz = (float)(h % kH - 1) * c.h0f;
+  using T = Tile<TB>;
+  const float ox = (float)(h / (T::H * T::H) - 1) * c.h0f;
+  const float oy = (float)((h / T::H) % T::H - 1) * c.h0f;
+  const float oz = (float)(h % T::H - 1) * c.h0f;
   return make_float4(ox + q.x, oy + q.y, oz + q.z, q.w);
 }
 
 // Halo cell of a particle of the tile itself.
+template <int TB>
 __device__ __forceinline__ int own_halo_cell(uint32_t cell) {
-  const int u = (int)(cell & ((1u << (3 * kTL)) - 1u));
-  const int ux = u >> (2 * kTL), uy = (u >> kTL) & (kTB - 1), uz = u & (kTB - 1);
-  return ((ux + 1) * kH + (uy + 1)) * kH + (uz + 1);
+  using T = Tile<TB>;
+  const int u = (int)(cell & ((1u << (3 * T::L)) - 1u));
+  const int ux = u >> (2 * T::L), uy = (u >> T::L) & (T::B - 1), uz = u & (T::B - 1);
+  return ((ux + 1) * T::H + (uy + 1)) * T::H + (uz + 1);
 }
 
 // Warp-cooperative staging: warp w copies halo z-runs w, w+8, ... (6 cells
 // with fixed hx, hy; their staged slots are contiguous), lanes taking
 // consecutive slots so global reads coalesce.  `emit(slot, h, src)` stores
 // one particle read from global slot `src` of halo cell h.
-template <class Emit, class Dummy>
+template <int TB, class Emit, class Dummy>
 __device__ __forceinline__ void stage_halo(const uint32_t* s_src, const uint32_t* s_end, const uint32_t* s_off,
                                            int run_lo, int run_hi, uint32_t base, Emit emit, Dummy dummy) {
+  using T = Tile<TB>;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int run = run_lo + warp; run < run_hi; run += kTT / 32) {
-    const int h0 = run * kH;
-    const uint32_t b0 = s_off[h0], b6 = s_off[h0 + kH];
+    const int h0 = run * T::H;
+    const uint32_t b0 = s_off[h0], b6 = s_off[h0 + T::H];
 #pragma unroll 4
     for (uint32_t k = b0 + lane; k < b6; k += 32) {
       int hz = 0;
 #pragma unroll
-      for (int z = 1; z < kH; ++z) hz += k >= s_off[h0 + z] ? 1 : 0;
+      for (int z = 1; z < T::H; ++z) hz += k >= s_off[h0 + z] ? 1 : 0;
       const int h = h0 + hz;
       const uint32_t src = s_src[h] + (k - s_off[h]);
       if (src < s_end[h])
@@ -248,13 +266,15 @@ __device__ __forceinline__ void stage_halo(const uint32_t* s_src, const uint32_t
 
 // Slab decomposition of a tile whose whole halo does not fit the staging
 // buffer: the core is processed in x-slabs of `slab` cell layers, each with
-// the (slab+2) x 6 x 6-cell halo (a contiguous halo-index range).  Returns
-// the thickest slab (4, 2 or 1) whose halos all fit, or 0 (none fits).
+// the (slab+2) x H x H-cell halo (a contiguous halo-index range).  Returns
+// the thickest slab (TB, 2 or 1) whose halos all fit, or 0 (none fits).
+template <int TB>
 __device__ __forceinline__ int pick_slab(const uint32_t* s_off, uint32_t cap) {
-  constexpr int L = kH * kH;  // halo cells per x-layer
-  if (s_off[kNH] <= cap) return kTB;
-  if (s_off[4 * L] - s_off[0] <= cap && s_off[6 * L] - s_off[2 * L] <= cap) return 2;
-  for (int x0 = 0; x0 < kTB; ++x0)
+  using T = Tile<TB>;
+  constexpr int L = T::H * T::H;  // halo cells per x-layer
+  if (s_off[T::NH] <= cap) return T::B;
+  if (T::B == 4 && s_off[4 * L] - s_off[0] <= cap && s_off[6 * L] - s_off[2 * L] <= cap) return 2;
+  for (int x0 = 0; x0 < T::B; ++x0)
     if (s_off[(x0 + 3) * L] - s_off[x0 * L] > cap) return 0;
   return 1;
 }
@@ -347,34 +367,57 @@ struct ListWriter {
   }
 };
 
-// Appends the occupied cells of tile g to the dense-cell list (one atomic per
-// tile).  Uniform across the CTA; `s_base` is shared scratch.
-__device__ __forceinline__ void queue_dense_cells(const TiledArgs& a, const TileGeom& g, uint32_t* ws,
-                                                  uint32_t* s_base) {
-  constexpr int kCells = kTB * kTB * kTB;
-  const uint32_t first_cell = (a.sorted_cell[g.first] >> (3 * kTL)) << (3 * kTL);
+// Appends the dense-cell work of tile g to the task list (one atomic per
+// tile): every occupied cell of the tile contributes ceil(count / 32) tasks,
+// each the first sorted slot of up to 32 consecutive particles of that cell
+// (the cell is sorted_cell[slot]).  Uniform across the CTA; `s_pre` is
+// shared scratch of T::B^3 + 1 entries (the caller lends the halo table's
+// s_src, which the next tile rebuilds).
+template <int TB>
+__device__ __forceinline__ void queue_dense_tasks(const TiledArgs& a, const TileGeom& g, uint32_t* ws,
+                                                  uint32_t* s_pre, uint32_t* s_base) {
+  using T = Tile<TB>;
+  constexpr int kCells = T::B * T::B * T::B;
+  const uint32_t first_cell = (a.sorted_cell[g.first] >> (3 * T::L)) << (3 * T::L);
   const int t = threadIdx.x;
   const uint32_t cell = first_cell + (uint32_t)t;
-  const uint32_t occupied = (t < kCells && a.cell_start[cell + 1] > a.cell_start[cell]) ? 1u : 0u;
+  uint32_t q0 = 0, cnt = 0;
+  if (t < kCells) {
+    q0 = a.cell_start[cell];
+    cnt = a.cell_start[cell + 1] - q0;
+  }
   uint32_t total;
-  const uint32_t off = block_scan(occupied, ws, total);
-  if (t == 0) *s_base = atomicAdd(a.dense_count, total);
+  const uint32_t off = block_scan((cnt + 31u) >> 5, ws, total);
+  if (t < kCells) s_pre[t] = off;
+  if (t == 0) {
+    s_pre[kCells] = total;
+    *s_base = atomicAdd(a.dense_count, total);
+  }
   __syncthreads();
-  if (occupied) a.dense_cells[*s_base + off] = cell;
+  const uint32_t base = *s_base;
+  for (uint32_t k = (uint32_t)t; k < total; k += kTT) {
+    int lo = 0, hi = kCells - 1;  // last cell with s_pre <= k
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (s_pre[mid] <= k) lo = mid; else hi = mid - 1;
+    }
+    a.dense_q0[base + k] = a.cell_start[first_cell + (uint32_t)lo] + 32u * (k - s_pre[lo]);
+  }
   __syncthreads();
 }
 
 // kExact: the cutoff min(h, h0) equals the kernel radius h0 (the usual case).
 // Six CTAs per SM is the shared-memory limit (35 KB each); the register cap
 // that matches it (40) costs no spill.
-template <bool kCount, bool kExact>
+template <int TB, bool kCount, bool kExact>
 __global__ void __launch_bounds__(kTT, 6) k_density_tiled(StepConsts c, TiledArgs a) {
+  using T = Tile<TB>;
   extern __shared__ __align__(16) unsigned char smem[];
   float* s_pp = reinterpret_cast<float*>(smem);  // kHaloCap slots, pair-interleaved
   uint32_t* s_src = reinterpret_cast<uint32_t*>(smem + kHaloCap * sizeof(float4));
-  uint32_t* s_end = s_src + kNH;
-  uint32_t* s_off = s_end + kNH;
-  uint32_t* ws = s_off + kNH + 1;
+  uint32_t* s_end = s_src + T::NH;
+  uint32_t* s_off = s_end + T::NH;
+  uint32_t* ws = s_off + T::NH + 1;
   const float hc2 = fminf(c.h2f, c.h0sqf);
   const f2 HC2 = f2_pack(hc2, hc2), H0SQ = f2_pack(c.h0sqf, c.h0sqf);
   __shared__ uint32_t s_next;
@@ -382,25 +425,25 @@ __global__ void __launch_bounds__(kTT, 6) k_density_tiled(StepConsts c, TiledArg
   unsigned cand = 0, pairs = 0;
   for (uint32_t k = next_tile(a.queue, 0, blockIdx.x, &s_next); k < ntiles;
        k = next_tile(a.queue, 0, k + gridDim.x, &s_next)) {
-    const TileGeom g = tile_geom(c, a, k);
-    halo_table(c, a, g, s_src, s_end, s_off, ws);
-    const int slab = a.tile_crowd[k] ? 0 : pick_slab(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
+    const TileGeom g = tile_geom<TB>(c, a, k);
+    halo_table<TB>(c, a, g, s_src, s_end, s_off, ws);
+    const int slab = a.tile_crowd[k] ? 0 : pick_slab<TB>(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
     if (slab == 0) {
-      queue_dense_cells(a, g, ws, &s_next);
+      queue_dense_tasks<TB>(a, g, ws, s_src, &s_next);
       continue;  // uniform across the CTA
     }
-    for (int x0 = 0; x0 < kTB; x0 += slab) {
-    const uint32_t base = s_off[x0 * kH * kH];
-    stage_halo(
-        s_src, s_end, s_off, x0 * kH, (x0 + slab + 2) * kH, base,
-        [&](uint32_t slot, int h, uint32_t src) { put_pair_slot(s_pp, slot, tile_rel(c, a.cpos[src], h)); },
+    for (int x0 = 0; x0 < T::B; x0 += slab) {
+    const uint32_t base = s_off[x0 * T::H * T::H];
+    stage_halo<TB>(
+        s_src, s_end, s_off, x0 * T::H, (x0 + slab + 2) * T::H, base,
+        [&](uint32_t slot, int h, uint32_t src) { put_pair_slot(s_pp, slot, tile_rel<TB>(c, a.cpos[src], h)); },
         [&](uint32_t slot) { put_pair_slot(s_pp, slot, make_float4(kFar, kFar, kFar, 0.f)); });
     __syncthreads();
     const float4* s_pp4 = reinterpret_cast<const float4*>(s_pp);
-    const uint32_t qfirst = s_src[((x0 + 1) * kH + 1) * kH + 1];
-    const uint32_t qlast = s_end[((x0 + slab) * kH + kTB) * kH + kTB];
+    const uint32_t qfirst = s_src[((x0 + 1) * T::H + 1) * T::H + 1];
+    const uint32_t qlast = s_end[((x0 + slab) * T::H + T::B) * T::H + T::B];
     for (uint32_t qi = qfirst + threadIdx.x; qi < qlast; qi += kTT) {
-      const int hq = own_halo_cell(a.sorted_cell[qi]);
+      const int hq = own_halo_cell<TB>(a.sorted_cell[qi]);
       const uint32_t si = s_off[hq] - base + (qi - s_src[hq]);
       const float* own = s_pp + (si >> 1) * 8 + (si & 1);
       const f2 PX = f2_pack(own[0], own[0]), PY = f2_pack(own[2], own[2]), PZ = f2_pack(own[4], own[4]);
@@ -411,7 +454,7 @@ __global__ void __launch_bounds__(kTT, 6) k_density_tiled(StepConsts c, TiledArg
       for (int di = -1; di <= 1; ++di) {
 #pragma unroll
         for (int dj = -1; dj <= 1; ++dj) {
-          const int h0 = hq + di * kH * kH + dj * kH - 1;  // cells h0 .. h0+2 (dk = -1, 0, 1)
+          const int h0 = hq + di * T::H * T::H + dj * T::H - 1;  // cells h0 .. h0+2 (dk = -1, 0, 1)
           const uint32_t s0 = s_off[h0] - base, e0 = s_off[h0 + 3] - base;  // both even
           if (kCount) cand += (s_end[h0] - s_src[h0]) + (s_end[h0 + 1] - s_src[h0 + 1]) + (s_end[h0 + 2] - s_src[h0 + 2]);
           f2 NPART = f2_pack(0.f, 0.f);
@@ -562,7 +605,9 @@ __device__ __forceinline__ void fold(CompAcc& q, ForcePart& b) {
 
 // One listed neighbour (r < min(h, h0) by construction; r == 0, i.e. i
 // itself or a coincident particle, contributes nothing, as the reference
-// skips r <= 0).  Branchless.
+// skips r <= 0).  Branchless.  kShear = false leaves out the shear sum
+// (StepConsts::shear_live).
+template <bool kShear>
 __device__ __forceinline__ void pair_listed(const StepConsts& c, float4 pj, float4 vj, float mr_j, float4 pi,
                                             float4 vi, float lapm_i, ForcePart& b, CompAcc& q) {
   const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
@@ -590,14 +635,18 @@ __device__ __forceinline__ void pair_listed(const StepConsts& c, float4 pj, floa
   q.xsy = fmaf(dvy, xw, q.xsy);
   q.xsz = fmaf(dvz, xw, q.xsz);
   // strain-rate proxy: |dv| / (r + 1e-4) * m_j / rho_j
-  const float dv2 = dvx * dvx + dvy * dvy + dvz * dvz;
-  const float dvn = dv2 > 0.f ? dv2 * rsqrtf(dv2) : 0.f;
-  q.shear = fmaf(__fdividef(dvn, r + 1e-4f), mr, q.shear);
+  if (kShear) {
+    const float dv2 = dvx * dvx + dvy * dvy + dvz * dvz;
+    const float dvn = dv2 > 0.f ? dv2 * rsqrtf(dv2) : 0.f;
+    q.shear = fmaf(__fdividef(dvn, r + 1e-4f), mr, q.shear);
+  }
 }
 
 // Three CTAs per SM is the shared-memory limit (75 KB each), so registers up to
 // 65536 / (3 x 256) cost no occupancy.
+template <int TB, bool kShear>
 __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs a) {
+  using T = Tile<TB>;
   extern __shared__ __align__(16) unsigned char smem[];
   // Staged neighbour records as separate 16-byte arrays (a 32-byte record
   // stride would map every record onto 4 of the 8 bank quads).
@@ -605,24 +654,24 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
   float4* s_vel = s_pos + kHaloCap;
   float* s_mr = reinterpret_cast<float*>(s_vel + kHaloCap);
   uint32_t* s_src = reinterpret_cast<uint32_t*>(s_mr + kHaloCap);
-  uint32_t* s_end = s_src + kNH;
-  uint32_t* s_off = s_end + kNH;
-  uint32_t* ws = s_off + kNH + 1;
+  uint32_t* s_end = s_src + T::NH;
+  uint32_t* s_off = s_end + T::NH;
+  uint32_t* ws = s_off + T::NH + 1;
   const float hc2 = fminf(c.h2f, c.h0sqf);
   __shared__ uint32_t s_next;
   const uint32_t ntiles = *a.num_tiles;
   for (uint32_t k = next_tile(a.queue, 1, blockIdx.x, &s_next); k < ntiles;
        k = next_tile(a.queue, 1, k + gridDim.x, &s_next)) {
-    const TileGeom g = tile_geom(c, a, k);
-    halo_table(c, a, g, s_src, s_end, s_off, ws);
-    const int slab = a.tile_crowd[k] ? 0 : pick_slab(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
+    const TileGeom g = tile_geom<TB>(c, a, k);
+    halo_table<TB>(c, a, g, s_src, s_end, s_off, ws);
+    const int slab = a.tile_crowd[k] ? 0 : pick_slab<TB>(s_off, (uint32_t)min(c.halo_cap, kHaloCap));
     if (slab == 0) continue;  // the dense-cell pass computes this tile
-    for (int x0 = 0; x0 < kTB; x0 += slab) {
-    const uint32_t base = s_off[x0 * kH * kH];
-    stage_halo(
-        s_src, s_end, s_off, x0 * kH, (x0 + slab + 2) * kH, base,
+    for (int x0 = 0; x0 < T::B; x0 += slab) {
+    const uint32_t base = s_off[x0 * T::H * T::H];
+    stage_halo<TB>(
+        s_src, s_end, s_off, x0 * T::H, (x0 + slab + 2) * T::H, base,
         [&](uint32_t slot, int h, uint32_t src) {
-          s_pos[slot] = tile_rel(c, a.cpos[src], h);
+          s_pos[slot] = tile_rel<TB>(c, a.cpos[src], h);
           s_vel[slot] = a.cvel[src];
           s_mr[slot] = a.cmr[src];
         },
@@ -632,10 +681,10 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
           s_mr[slot] = 0.f;
         });
     __syncthreads();
-    const uint32_t qfirst = s_src[((x0 + 1) * kH + 1) * kH + 1];
-    const uint32_t qlast = s_end[((x0 + slab) * kH + kTB) * kH + kTB];
+    const uint32_t qfirst = s_src[((x0 + 1) * T::H + 1) * T::H + 1];
+    const uint32_t qlast = s_end[((x0 + slab) * T::H + T::B) * T::H + T::B];
     for (uint32_t qi = qfirst + threadIdx.x; qi < qlast; qi += kTT) {
-      const int hq = own_halo_cell(a.sorted_cell[qi]);
+      const int hq = own_halo_cell<TB>(a.sorted_cell[qi]);
       const uint32_t si = s_off[hq] - base + (qi - s_src[hq]);
       const float4 pi = s_pos[si];
       const float4 vi = s_vel[si];
@@ -656,7 +705,7 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
           for (int u = 0; u < 8; ++u) {
             if (e0 + u < cnt) {
               const uint32_t j = (w[u >> 1] >> (16 * (u & 1))) & 0xffffu;
-              pair_listed(c, s_pos[j], s_vel[j], s_mr[j], pi, vi, lapm_i, b, q);
+              pair_listed<kShear>(c, s_pos[j], s_vel[j], s_mr[j], pi, vi, lapm_i, b, q);
             }
             if (u == 3 || u == 7) fold(q, b);
           }
@@ -666,12 +715,12 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
         // List overflow: rescan the 27 staged cells with the cutoff test.
         for (int di = -1; di <= 1; ++di)
           for (int dj = -1; dj <= 1; ++dj) {
-            const int h0 = hq + di * kH * kH + dj * kH - 1;
+            const int h0 = hq + di * T::H * T::H + dj * T::H - 1;
             for (uint32_t j = s_off[h0] - base; j < s_off[h0 + 3] - base; ++j) {
               const float4 pj = s_pos[j];
               const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
               if (!(dx * dx + dy * dy + dz * dz < hc2)) continue;
-              pair_listed(c, pj, s_vel[j], s_mr[j], pi, vi, lapm_i, b, q);
+              pair_listed<kShear>(c, pj, s_vel[j], s_mr[j], pi, vi, lapm_i, b, q);
               fold(q, b);
             }
           }
@@ -690,274 +739,300 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
 
 // ---- Dense cells ---------------------------------------------------------------
 //
-// Tiles whose halo does not fit the staging buffer even in 1-layer slabs
-// (cells of tens to thousands of particles, as when the fluid has collapsed
-// onto the floor) are computed per occupied cell.  The CTA streams each of
-// the cell's 27 neighbour cells through shared memory in chunks; every staged
-// candidate serves all the cell's queries (broadcast reads).  Work is sized
-// to the cell: a cell of Q particles gets S = clamp(512 / Q, 1, 32) lanes per
-// query (a power of two, lanes of one warp), each taking every S-th
-// candidate, and the S partial sums are combined by a fixed shuffle tree;
-// each lane group holds two queries.  The force pass has no list for these
-// particles; it tests every candidate.
+// Tiles whose halo does not fit the staging buffer even in 1-layer slabs, or
+// whose occupied cells average more than kDenseMean particles (cells of tens
+// to thousands of particles, as when the fluid has collapsed onto the floor),
+// are computed by warps: a task is up to 32 consecutive particles of one cell
+// (one query per lane; the in-cell Morton order makes them a compact clump),
+// and the warp streams each of the 27 neighbour cells in chunks of 32
+// candidates (one per lane, coalesced), staged in the warp's own shared
+// memory.  A chunk is skipped whole when the bounding boxes of the warp's
+// queries and of the chunk's candidates are at least the cutoff apart, which
+// removes about half the candidates of a crowded neighbourhood.  Tasks come
+// from a device counter (one atomic per task), so no barrier joins warps.
 
-constexpr int kDT = 256;       // threads per dense CTA
-constexpr int kDQ = 2;         // queries per lane group (density)
-constexpr int kFQ = 1;         // queries per lane group (force: its accumulators are large)
-constexpr int kDChunk = 1024;  // candidates staged per chunk
+constexpr int kWT = 256;  // threads per dense-task CTA
+constexpr int kWarps = kWT / 32;
+
+// Order-preserving map of f32 bits to u32 (for warp min/max reductions) and
+// its inverse.  NaN maps outside [-inf, inf], which makes a box conservative.
+__device__ __forceinline__ uint32_t ord_f32(float x) {
+  const uint32_t b = __float_as_uint(x);
+  return b ^ ((uint32_t)((int32_t)b >> 31) | 0x80000000u);
+}
+__device__ __forceinline__ float unord_f32(uint32_t u) {
+  return __uint_as_float(u ^ (((u >> 31) - 1u) | 0x80000000u));
+}
+
+// Bounding box of the valid lanes' points (all lanes call it).
+struct Box3 {
+  float lo[3], hi[3];
+};
+__device__ __forceinline__ Box3 warp_box(float x, float y, float z, bool valid) {
+  const float v[3] = {x, y, z};
+  Box3 b;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const uint32_t u = ord_f32(v[k]);
+    b.lo[k] = unord_f32(__reduce_min_sync(0xffffffffu, valid ? u : 0xffffffffu));
+    b.hi[k] = unord_f32(__reduce_max_sync(0xffffffffu, valid ? u : 0u));
+  }
+  return b;
+}
+
+// True when every point of box c (offset by off) is at least sqrt(hc2) from
+// every point of box q.  The gaps use the operations of the pair distance
+// (f32 subtraction of offset coordinates, fma sum of squares), which round
+// monotonically, so a skipped chunk holds no pair with r^2 < hc2; a NaN
+// bound never skips.
+__device__ __forceinline__ bool boxes_apart(const Box3& q, const Box3& c, const float off[3], float hc2) {
+  float g[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float a = (c.lo[k] + off[k]) - q.hi[k];
+    const float b = q.lo[k] - (c.hi[k] + off[k]);
+    g[k] = fmaxf(fmaxf(a, b), 0.f);
+  }
+  const float d2 = fmaf(g[2], g[2], fmaf(g[1], g[1], g[0] * g[0]));
+  return d2 >= hc2 * 1.0001f;
+}
 
 struct CellGeom {
   int ax, ay, az;  // box coordinates
   int sc;
 };
 
+template <int TB>
 __device__ __forceinline__ CellGeom cell_geom(const StepConsts& c, const TiledArgs& a, uint32_t cell) {
+  using T = Tile<TB>;
   CellGeom g;
   g.sc = a.scene ? (int)a.scene[a.cell_start[cell]] : 0;
   const SceneBox& bx = c.boxes[g.sc];
   const uint32_t rel = cell - (uint32_t)bx.cell_base;
-  const int t = (int)(rel >> (3 * kTL));
-  const int u = (int)(rel & ((1u << (3 * kTL)) - 1u));
+  const int t = (int)(rel >> (3 * T::L));
+  const int u = (int)(rel & ((1u << (3 * T::L)) - 1u));
   const int tz = t % bx.nt[2], ty = (t / bx.nt[2]) % bx.nt[1], tx = t / (bx.nt[2] * bx.nt[1]);
-  g.ax = tx * kTB + (u >> (2 * kTL));
-  g.ay = ty * kTB + ((u >> kTL) & (kTB - 1));
-  g.az = tz * kTB + (u & (kTB - 1));
+  g.ax = tx * T::B + (u >> (2 * T::L));
+  g.ay = ty * T::B + ((u >> T::L) & (T::B - 1));
+  g.az = tz * T::B + (u & (T::B - 1));
   return g;
 }
 
-// The cell's 27 neighbour cells as one virtual candidate range: s_src[nb] is
-// neighbour nb's first slot, s_pre[nb] its first virtual index (s_pre[27] =
-// the total).  Uniform across the CTA; ends with a barrier.
-__device__ __forceinline__ void dense_neighbour_table(const StepConsts& c, const TiledArgs& a, const SceneBox& bx,
-                                                      const CellGeom& cg, uint32_t* s_src, uint32_t* s_pre) {
-  if (threadIdx.x < 32) {
-    const int nb = threadIdx.x;
-    uint32_t src = 0, cnt = 0;
-    if (nb < 27) {
-      const int lin = box_tiled_index(c, bx, cg.ax + nb / 9 - 1, cg.ay + (nb / 3) % 3 - 1, cg.az + nb % 3 - 1);
-      src = a.cell_start[lin];
-      cnt = a.cell_start[lin + 1] - src;
-    }
-    uint32_t x = cnt;
+// The warp's task: slots [q0, q0 + qn) of `cell`, its box geometry, and the
+// 27 neighbour ranges held by lanes 0..26 (empty when the neighbour cell's
+// box is out of reach of the queries' box).
+struct DenseTask {
+  uint32_t q0, qn;
+  CellGeom cg;
+  uint32_t nb_s, nb_e;  // this lane's neighbour range (lane < 27)
+};
+
+template <int TB>
+__device__ __forceinline__ bool next_task(const StepConsts& c, const TiledArgs& a, uint32_t* counter,
+                                          uint32_t ntasks, DenseTask& t) {
+  const int lane = threadIdx.x & 31;
+  uint32_t k = 0;
+  if (lane == 0) k = atomicAdd(counter, 1u);
+  k = __shfl_sync(0xffffffffu, k, 0);
+  if (k >= ntasks) return false;
+  t.q0 = a.dense_q0[k];
+  const uint32_t cell = a.sorted_cell[t.q0];
+  t.qn = min(32u, a.cell_start[cell + 1] - t.q0);
+  t.cg = cell_geom<TB>(c, a, cell);
+  return true;
+}
+
+// Neighbour ranges of the task (lane nb < 27 holds neighbour nb), with
+// whole cells out of reach of the query box emptied.
+__device__ __forceinline__ void task_neighbours(const StepConsts& c, const TiledArgs& a, DenseTask& t,
+                                                const Box3& qb, float hc2) {
+  const int nb = threadIdx.x & 31;
+  t.nb_s = t.nb_e = 0;
+  if (nb < 27) {
+    const SceneBox& bx = c.boxes[t.cg.sc];
+    const int dx = nb / 9 - 1, dy = (nb / 3) % 3 - 1, dz = nb % 3 - 1;
+    const int lin = box_tiled_index(c, bx, t.cg.ax + dx, t.cg.ay + dy, t.cg.az + dz);
+    const uint32_t s0 = a.cell_start[lin], e0 = a.cell_start[lin + 1];
+    // The neighbour cell's box in query-cell coordinates, widened by 1e-3 h0
+    // for cell-local coordinates rounded just outside [0, h0].
+    const float m = 1e-3f * c.h0f;
+    Box3 cb;
+    const float o[3] = {(float)dx * c.h0f, (float)dy * c.h0f, (float)dz * c.h0f};
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (nb >= o) x += y;
+    for (int k = 0; k < 3; ++k) {
+      cb.lo[k] = -m;
+      cb.hi[k] = c.h0f + m;
     }
-    if (nb < 27) {
-      s_src[nb] = src;
-      s_pre[nb] = x - cnt;
+    if (!boxes_apart(qb, cb, o, hc2)) {
+      t.nb_s = s0;
+      t.nb_e = e0;
     }
-    if (nb == 26) s_pre[27] = x;
-  }
-  __syncthreads();
-}
-
-// Neighbour (0..26) holding virtual candidate v: the last nb with s_pre[nb] <= v.
-__device__ __forceinline__ int dense_neighbour_of(const uint32_t* s_pre, uint32_t v) {
-  int lo = 0, hi = 26;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (s_pre[mid] <= v) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
-// Stages virtual candidates [cb, cb + m) of the cell's neighbourhood: slot j
-// gets the candidate's position relative to the query cell's origin (its
-// cell-local f32 coordinates plus the neighbour cell's offset).  `emit(j,
-// src, rel)` stores one candidate.
-template <class Emit>
-__device__ __forceinline__ void dense_stage(const StepConsts& c, const TiledArgs& a, const uint32_t* s_src,
-                                            const uint32_t* s_pre, uint32_t cb, uint32_t m, Emit emit) {
-  for (uint32_t j = threadIdx.x; j < m; j += kDT) {
-    const uint32_t v = cb + j;
-    const int nb = dense_neighbour_of(s_pre, v);
-    const uint32_t src = s_src[nb] + (v - s_pre[nb]);
-    const float4 q = a.cpos[src];
-    const float4 rel = make_float4(q.x + (float)(nb / 9 - 1) * c.h0f, q.y + (float)((nb / 3) % 3 - 1) * c.h0f,
-                                   q.z + (float)(nb % 3 - 1) * c.h0f, q.w);
-    emit(j, src, rel);
   }
 }
 
-// Lanes per query for a cell of q particles when each lane group holds
-// `per_group` queries (a power of two, 1..32).
-__device__ __forceinline__ int dense_split(uint32_t q, int per_group) {
-  int sp = 1;
-  while (sp < 32 && (uint32_t)(2 * sp) * q <= (uint32_t)(kDT * per_group)) sp <<= 1;
-  return sp;
+__device__ __forceinline__ void neighbour_offset(const StepConsts& c, int nb, float off[3]) {
+  off[0] = (float)(nb / 9 - 1) * c.h0f;
+  off[1] = (float)((nb / 3) % 3 - 1) * c.h0f;
+  off[2] = (float)(nb % 3 - 1) * c.h0f;
 }
 
-// Sum over the `sp` lanes of a group (sp a power of two dividing 32); every
-// lane of the group receives the total.  All 32 lanes must call it.
-__device__ __forceinline__ float group_sum(float v, int sp) {
-  for (int o = 1; o < sp; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-template <bool kCount>
-// (At least 4 resident CTAs leave 64 registers a thread, enough to hold the
-// two queries without spilling.)
-__global__ void __launch_bounds__(kDT, 4) k_density_dense(StepConsts c, TiledArgs a) {
-  __shared__ float4 s_c[kDChunk];
-  __shared__ uint32_t s_src[27], s_pre[28];
-  const uint32_t ncells = *a.dense_count;
+// Density of the dense-cell particles: per query the compensated sum of
+// m_j poly6(r) over the 27 cells (world.rs:219-238), candidates in pairs on
+// f32x2 arithmetic (the filter of the tiled pass without the list).
+template <int TB, bool kCount, bool kExact>
+__global__ void __launch_bounds__(kWT, 5) k_density_dense(StepConsts c, TiledArgs a) {
+  __shared__ __align__(16) float s_pp[kWarps][32 * 4];  // 32 candidates, pair-interleaved
+  const int lane = threadIdx.x & 31;
+  float* sp = s_pp[threadIdx.x >> 5];
+  const float4* sp4 = reinterpret_cast<const float4*>(sp);
+  const uint32_t ntasks = *a.dense_count;
   const float hc2 = fminf(c.h2f, c.h0sqf);
+  const f2 HC2 = f2_pack(hc2, hc2), H0SQ = f2_pack(c.h0sqf, c.h0sqf);
   unsigned cand = 0, pairs = 0;
-  for (uint32_t w = blockIdx.x; w < ncells; w += gridDim.x) {
-    const uint32_t cell = a.dense_cells[w];
-    const CellGeom cg = cell_geom(c, a, cell);
-    const SceneBox& bx = c.boxes[cg.sc];
-    const uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
-    const int sp = dense_split(q1 - q0, kDQ);     // uniform across the CTA
-    const int groups = kDT / sp;
-    const int grp = threadIdx.x / sp, sub = threadIdx.x % sp;
-    __syncthreads();  // the previous cell's tables are no longer read
-    dense_neighbour_table(c, a, bx, cg, s_src, s_pre);
-    const uint32_t total = s_pre[27];
-    for (uint32_t qb = q0; qb < q1; qb += (uint32_t)(groups * kDQ)) {
-      float4 qp[kDQ];
-      float s[kDQ], comp[kDQ];
-      unsigned nvalid = 0;
-#pragma unroll
-      for (int k = 0; k < kDQ; ++k) {
-        const uint32_t qi = qb + (uint32_t)(grp + k * groups);
-        qp[k] = qi < q1 ? a.cpos[qi] : make_float4(kFar, kFar, kFar, 0.f);
-        nvalid += qi < q1 ? 1u : 0u;
-        s[k] = 0.f;
-        comp[k] = 0.f;
-      }
-      for (uint32_t cb = 0; cb < total; cb += kDChunk) {
-        const uint32_t m = min(total - cb, (uint32_t)kDChunk);
-        __syncthreads();  // the previous chunk is consumed
-        dense_stage(c, a, s_src, s_pre, cb, m, [&](uint32_t j, uint32_t, float4 rel) { s_c[j] = rel; });
-        __syncthreads();
-        if (kCount && sub == 0) cand += m * nvalid;
-        // This lane's candidates: sub, sub + sp, ...; partial sums of up to
-        // 32 of them folded by Kahan.
-        for (uint32_t j0 = (uint32_t)sub; j0 < m; j0 += 32u * (uint32_t)sp) {
-          const uint32_t j1 = min(j0 + 32u * (uint32_t)sp, m);
-          float part[kDQ];
-#pragma unroll
-          for (int k = 0; k < kDQ; ++k) part[k] = 0.f;
-          for (uint32_t j = j0; j < j1; j += (uint32_t)sp) {
-            const float4 v = s_c[j];
-#pragma unroll
-            for (int k = 0; k < kDQ; ++k) {
-              const float dx = v.x - qp[k].x, dy = v.y - qp[k].y, dz = v.z - qp[k].z;
-              const float r2 = dx * dx + dy * dy + dz * dz;
-              const bool in = r2 < hc2;
-              const float t = in ? c.h0sqf - r2 : 0.f;
-              part[k] = fmaf(t * t, t * v.w, part[k]);
-              if (kCount) pairs += in ? 1u : 0u;
-            }
+  DenseTask t;
+  while (next_task<TB>(c, a, a.dense_taken, ntasks, t)) {
+    const bool qv = (uint32_t)lane < t.qn;
+    const uint32_t qi = t.q0 + (uint32_t)lane;
+    const float4 q = qv ? a.cpos[qi] : make_float4(kFar, kFar, kFar, 0.f);
+    const Box3 qb = warp_box(q.x, q.y, q.z, qv);
+    task_neighbours(c, a, t, qb, hc2);
+    const f2 PX = f2_pack(q.x, q.x), PY = f2_pack(q.y, q.y), PZ = f2_pack(q.z, q.z);
+    float s = 0.f, comp = 0.f;
+    for (int nb = 0; nb < 27; ++nb) {
+      const uint32_t s0 = __shfl_sync(0xffffffffu, t.nb_s, nb), e0 = __shfl_sync(0xffffffffu, t.nb_e, nb);
+      if (s0 >= e0) continue;
+      float off[3];
+      neighbour_offset(c, nb, off);
+      for (uint32_t cb = s0; cb < e0; cb += 32) {
+        const uint32_t j = cb + (uint32_t)lane;
+        const bool cv = j < e0;
+        float4 p = cv ? a.cpos[j] : make_float4(kFar, kFar, kFar, 0.f);
+        const Box3 bb = warp_box(p.x, p.y, p.z, cv);
+        if (boxes_apart(qb, bb, off, hc2)) continue;  // uniform
+        p.x += off[0];
+        p.y += off[1];
+        p.z += off[2];
+        put_pair_slot(sp, (uint32_t)lane, p);
+        __syncwarp();
+        const uint32_t m = min(32u, e0 - cb);
+        if (kCount && qv) cand += m;
+        f2 NPART = f2_pack(0.f, 0.f);
+#pragma unroll 4
+        for (uint32_t k = 0; k < 32u; k += 2) {
+          if (k >= m) break;  // uniform; slot m of an odd m holds a far dummy
+          const float4 A = sp4[k];      // x0 x1 y0 y1
+          const float4 B = sp4[k + 1];  // z0 z1 m0 m1
+          const f2 DX = f2_sub(f2_pack(A.x, A.y), PX);
+          const f2 DY = f2_sub(f2_pack(A.z, A.w), PY);
+          const f2 DZ = f2_sub(f2_pack(B.x, B.y), PZ);
+          const f2 R2 = f2_fma(DZ, DZ, f2_fma(DY, DY, f2_mul(DX, DX)));
+          float d0, d1, n0, n1;
+          f2_unpack(f2_sub(R2, HC2), d0, d1);
+          if (kExact) {
+            n0 = fminf(d0, 0.f);
+            n1 = fminf(d1, 0.f);
+          } else {
+            float e0_, e1_;
+            f2_unpack(f2_sub(R2, H0SQ), e0_, e1_);
+            n0 = d0 < 0.f ? e0_ : 0.f;
+            n1 = d1 < 0.f ? e1_ : 0.f;
           }
-#pragma unroll
-          for (int k = 0; k < kDQ; ++k) kahan_add(s[k], comp[k], c.poly6_cf * part[k]);
+          if (kCount) pairs += (qv && d0 < 0.f ? 1u : 0u) + (qv && d1 < 0.f && k + 1 < m ? 1u : 0u);
+          const f2 N = f2_pack(n0, n1);
+          NPART = f2_fma(f2_mul(N, N), f2_mul(N, f2_pack(B.z, B.w)), NPART);
         }
+        float p0, p1;
+        f2_unpack(NPART, p0, p1);
+        kahan_add(s, comp, c.poly6_cf * -(p0 + p1));
+        __syncwarp();  // the chunk is consumed before the next one is staged
       }
-#pragma unroll
-      for (int k = 0; k < kDQ; ++k) {
-        const float st = group_sum(s[k], sp), ct = group_sum(comp[k], sp);
-        const uint32_t qi = qb + (uint32_t)(grp + k * groups);
-        if (sub == 0 && qi < q1) {
-          write_density(c, a, (int)qi, (double)st - (double)ct);
-          a.nbr_count[qi] = kNoList;
-        }
-      }
+    }
+    if (qv) {
+      write_density(c, a, (int)qi, (double)s - (double)comp);
+      a.nbr_count[qi] = kNoList;
     }
   }
   if (kCount) {
-    // Placeholder queries (kFar) never pair and count no candidates.
     const unsigned wc = __reduce_add_sync(0xffffffffu, cand);
     const unsigned wp = __reduce_add_sync(0xffffffffu, pairs);
-    if ((threadIdx.x & 31) == 0) {
+    if (lane == 0) {
       atomicAdd(&a.counters[0], (unsigned long long)wc);
       atomicAdd(&a.counters[1], (unsigned long long)wp);
     }
   }
 }
 
-// (Four resident CTAs, the limit of its shared memory, leave 64 registers a
-// thread, which its single query fits without spilling.)
-__global__ void __launch_bounds__(kDT, 4) k_force_dense(StepConsts c, TiledArgs a) {
-  __shared__ float4 s_pos[kDChunk];
-  __shared__ float4 s_vel[kDChunk];
-  __shared__ float s_mr[kDChunk];
-  __shared__ uint32_t s_src[27], s_pre[28];
-  const uint32_t ncells = *a.dense_count;
+// Forces, integration and bounds of the dense-cell particles: per chunk each
+// lane builds the mask of its in-range candidates (branch-free), then walks
+// its own mask through the pair terms of the tiled pass.
+template <int TB, bool kShear>
+__global__ void __launch_bounds__(kWT, 3) k_force_dense(StepConsts c, TiledArgs a) {
+  __shared__ float4 s_pos[kWarps][32];
+  __shared__ float4 s_vel[kWarps][32];
+  __shared__ float s_mr[kWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t ntasks = *a.dense_count;
   const float hc2 = fminf(c.h2f, c.h0sqf);
-  for (uint32_t w = blockIdx.x; w < ncells; w += gridDim.x) {
-    const uint32_t cell = a.dense_cells[w];
-    const CellGeom cg = cell_geom(c, a, cell);
-    const SceneBox& bx = c.boxes[cg.sc];
-    const uint32_t q0 = a.cell_start[cell], q1 = a.cell_start[cell + 1];
-    const int sp = dense_split(q1 - q0, kFQ);
-    const int groups = kDT / sp;
-    const int grp = threadIdx.x / sp, sub = threadIdx.x % sp;
-    __syncthreads();  // the previous cell's tables are no longer read
-    dense_neighbour_table(c, a, bx, cg, s_src, s_pre);
-    const uint32_t total = s_pre[27];
-    for (uint32_t qb = q0; qb < q1; qb += (uint32_t)(groups * kFQ)) {
-      float4 qp[kFQ], qv[kFQ];
-      CompAcc acc[kFQ];
-      ForcePart part[kFQ];
-#pragma unroll
-      for (int k = 0; k < kFQ; ++k) {
-        const uint32_t qi = qb + (uint32_t)(grp + k * groups);
-        qp[k] = qi < q1 ? a.cpos[qi] : make_float4(kFar, kFar, kFar, 0.f);
-        qv[k] = qi < q1 ? a.cvel[qi] : make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-      for (uint32_t cb = 0; cb < total; cb += kDChunk) {
-        const uint32_t m = min(total - cb, (uint32_t)kDChunk);
-        __syncthreads();
-        dense_stage(c, a, s_src, s_pre, cb, m, [&](uint32_t j, uint32_t src, float4 rel) {
-          s_pos[j] = rel;
-          s_vel[j] = a.cvel[src];
-          s_mr[j] = a.cmr[src];
-        });
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < kFQ; ++k) {
-          const float lapm = qp[k].w * c.lap_cf;
-          uint32_t since = 0;
-          for (uint32_t j = (uint32_t)sub; j < m; j += (uint32_t)sp) {
-            const float4 pj = s_pos[j];
-            const float dx = pj.x - qp[k].x, dy = pj.y - qp[k].y, dz = pj.z - qp[k].z;
-            if (!(dx * dx + dy * dy + dz * dz < hc2)) continue;
-            pair_listed(c, pj, s_vel[j], s_mr[j], qp[k], qv[k], lapm, part[k], acc[k]);
-            if (++since == 4) {
-              fold(acc[k], part[k]);
-              since = 0;
-            }
-          }
-          fold(acc[k], part[k]);
+  DenseTask t;
+  while (next_task<TB>(c, a, a.dense_taken + 1, ntasks, t)) {
+    const bool qv = (uint32_t)lane < t.qn;
+    const uint32_t qi = t.q0 + (uint32_t)lane;
+    const float4 qp = qv ? a.cpos[qi] : make_float4(kFar, kFar, kFar, 0.f);
+    const float4 qvel = qv ? a.cvel[qi] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const Box3 qb = warp_box(qp.x, qp.y, qp.z, qv);
+    task_neighbours(c, a, t, qb, hc2);
+    const float lapm = qp.w * c.lap_cf;
+    CompAcc acc;
+    ForcePart part;
+    uint32_t since = 0;
+    for (int nb = 0; nb < 27; ++nb) {
+      const uint32_t s0 = __shfl_sync(0xffffffffu, t.nb_s, nb), e0 = __shfl_sync(0xffffffffu, t.nb_e, nb);
+      if (s0 >= e0) continue;
+      float off[3];
+      neighbour_offset(c, nb, off);
+      for (uint32_t cb = s0; cb < e0; cb += 32) {
+        const uint32_t j = cb + (uint32_t)lane;
+        const bool cv = j < e0;
+        float4 p = cv ? a.cpos[j] : make_float4(kFar, kFar, kFar, 0.f);
+        const Box3 bb = warp_box(p.x, p.y, p.z, cv);
+        if (boxes_apart(qb, bb, off, hc2)) continue;  // uniform
+        p.x += off[0];
+        p.y += off[1];
+        p.z += off[2];
+        s_pos[w][lane] = p;
+        s_vel[w][lane] = cv ? a.cvel[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        s_mr[w][lane] = cv ? a.cmr[j] : 0.f;
+        __syncwarp();
+        const uint32_t m = min(32u, e0 - cb);
+        uint32_t mask = 0;
+#pragma unroll 8
+        for (uint32_t k = 0; k < 32u; ++k) {
+          if (k >= m) break;  // uniform
+          const float4 pj = s_pos[w][k];
+          const float dx = pj.x - qp.x, dy = pj.y - qp.y, dz = pj.z - qp.z;
+          const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+          mask |= (r2 < hc2 ? 1u : 0u) << k;
         }
-      }
-#pragma unroll
-      for (int k = 0; k < kFQ; ++k) {
-        // Combine the group's partial sums (compensations applied per lane).
-        CompAcc t;
-        t.fpx = group_sum(acc[k].fpx - acc[k].cpx, sp);
-        t.fpy = group_sum(acc[k].fpy - acc[k].cpy, sp);
-        t.fpz = group_sum(acc[k].fpz - acc[k].cpz, sp);
-        t.fvx = group_sum(acc[k].fvx - acc[k].cvx, sp);
-        t.fvy = group_sum(acc[k].fvy - acc[k].cvy, sp);
-        t.fvz = group_sum(acc[k].fvz - acc[k].cvz, sp);
-        t.xsx = group_sum(acc[k].xsx, sp);
-        t.xsy = group_sum(acc[k].xsy, sp);
-        t.xsz = group_sum(acc[k].xsz, sp);
-        t.shear = group_sum(acc[k].shear, sp);
-        const uint32_t qi = qb + (uint32_t)(grp + k * groups);
-        if (sub == 0 && qi < q1) finish_particle(c, a, (int)qi, t, bx);
+        if (!qv) mask = 0;
+        while (mask) {
+          const int k = __ffs(mask) - 1;
+          mask &= mask - 1;
+          pair_listed<kShear>(c, s_pos[w][k], s_vel[w][k], s_mr[w][k], qp, qvel, lapm, part, acc);
+          if (++since == 4) {
+            fold(acc, part);
+            since = 0;
+          }
+        }
+        __syncwarp();  // the chunk is consumed before the next one is staged
       }
     }
+    fold(acc, part);
+    if (qv) finish_particle(c, a, (int)qi, acc, c.boxes[t.cg.sc]);
   }
 }
 
-constexpr size_t kDensitySmem = kHaloCap * sizeof(float4) + (3 * kNH + 1 + 32) * 4;
-constexpr size_t kForceSmem = kHaloCap * (2 * sizeof(float4) + sizeof(float)) + (3 * kNH + 1 + 32) * 4;
+constexpr size_t kDensitySmem = kHaloCap * sizeof(float4) + (3 * kNHMax + 1 + 32) * 4;
+constexpr size_t kForceSmem = kHaloCap * (2 * sizeof(float4) + sizeof(float)) + (3 * kNHMax + 1 + 32) * 4;
 
 // Resident CTAs per SM of the persistent passes (occupancy limits, computed
 // once; the shared-memory opt-in is set on the same first call).
@@ -965,22 +1040,30 @@ struct Occupancy {
   int sms = 1, density = 1, force = 1, dense_density = 1, dense_force = 1;
 };
 
+template <int TB>
+void set_smem_limits() {
+  for (auto f : {k_density_tiled<TB, false, true>, k_density_tiled<TB, true, true>, k_density_tiled<TB, false, false>,
+                 k_density_tiled<TB, true, false>})
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDensitySmem);
+  for (auto f : {k_force_tiled<TB, false>, k_force_tiled<TB, true>})
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kForceSmem);
+}
+
 const Occupancy& occupancy() {
   static const Occupancy o = [] {
     Occupancy r;
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&r.sms, cudaDevAttrMultiProcessorCount, dev);
-    for (auto f : {k_density_tiled<false, true>, k_density_tiled<true, true>, k_density_tiled<false, false>,
-                   k_density_tiled<true, false>})
-      cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDensitySmem);
-    cudaFuncSetAttribute(k_force_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kForceSmem);
+    set_smem_limits<4>();
+    set_smem_limits<2>();
+    // Both tile edges use the same shared memory and registers per CTA.
     int bd = 0, bf = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bd, k_density_tiled<false, true>, kTT, kDensitySmem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force_tiled, kTT, kForceSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bd, k_density_tiled<4, false, true>, kTT, kDensitySmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_force_tiled<4, true>, kTT, kForceSmem);
     int dd = 0, df = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dd, k_density_dense<false>, kDT, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&df, k_force_dense, kDT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dd, k_density_dense<4, false, true>, kWT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&df, k_force_dense<4, true>, kWT, 0);
     r.dense_density = std::max(dd, 1);
     r.dense_force = std::max(df, 1);
     r.sms = std::max(r.sms, 1);
@@ -989,6 +1072,27 @@ const Occupancy& occupancy() {
     return r;
   }();
   return o;
+}
+
+// The four passes of a tiled step (staged and dense-cell density, staged and
+// dense-cell force) for tile edge TB.
+template <int TB>
+void launch_passes(const StepConsts& c, const TiledArgs& a, cudaStream_t s, const PassEvents& ev, bool exact,
+                   int density_blocks, int force_blocks, int dense_d_blocks, int dense_f_blocks) {
+  auto density = a.counters ? (exact ? k_density_tiled<TB, true, true> : k_density_tiled<TB, true, false>)
+                            : (exact ? k_density_tiled<TB, false, true> : k_density_tiled<TB, false, false>);
+  density<<<density_blocks, kTT, kDensitySmem, s>>>(c, a);
+  auto dense = a.counters ? (exact ? k_density_dense<TB, true, true> : k_density_dense<TB, true, false>)
+                          : (exact ? k_density_dense<TB, false, true> : k_density_dense<TB, false, false>);
+  dense<<<dense_d_blocks, kWT, 0, s>>>(c, a);
+  if (ev.after_density) cudaEventRecord(ev.after_density, s);
+  if (c.shear_live) {
+    k_force_tiled<TB, true><<<force_blocks, kTT, kForceSmem, s>>>(c, a);
+    k_force_dense<TB, true><<<dense_f_blocks, kWT, 0, s>>>(c, a);
+  } else {
+    k_force_tiled<TB, false><<<force_blocks, kTT, kForceSmem, s>>>(c, a);
+    k_force_dense<TB, false><<<dense_f_blocks, kWT, 0, s>>>(c, a);
+  }
 }
 
 }  // namespace
@@ -1034,7 +1138,8 @@ void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const
   a.scene = pc.scene;
   a.queue = t.queue ? b.queue : nullptr;
   a.dense_count = b.queue + 2;
-  a.dense_cells = b.dense_cells;
+  a.dense_taken = b.queue + 3;
+  a.dense_q0 = b.dense_q0;
   a.stride = b.capacity;
   a.flags = b.flags;
   a.counters = b.counters;
@@ -1049,16 +1154,10 @@ void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const
   if (ev.after_prep) cudaEventRecord(ev.after_prep, s);
   const int dense_d_blocks = o.sms * o.dense_density, dense_f_blocks = o.sms * o.dense_force;
   const bool exact = std::min(c.h2f, c.h0sqf) == c.h0sqf;
-  auto density = a.counters ? (exact ? k_density_tiled<true, true> : k_density_tiled<true, false>)
-                            : (exact ? k_density_tiled<false, true> : k_density_tiled<false, false>);
-  density<<<density_blocks, kTT, kDensitySmem, s>>>(c, a);
-  if (a.counters)
-    k_density_dense<true><<<dense_d_blocks, kDT, 0, s>>>(c, a);
+  if (c.tile == 2)
+    launch_passes<2>(c, a, s, ev, exact, density_blocks, force_blocks, dense_d_blocks, dense_f_blocks);
   else
-    k_density_dense<false><<<dense_d_blocks, kDT, 0, s>>>(c, a);
-  if (ev.after_density) cudaEventRecord(ev.after_density, s);
-  k_force_tiled<<<force_blocks, kTT, kForceSmem, s>>>(c, a);
-  k_force_dense<<<dense_f_blocks, kDT, 0, s>>>(c, a);
+    launch_passes<4>(c, a, s, ev, exact, density_blocks, force_blocks, dense_d_blocks, dense_f_blocks);
 }
 
 }  // namespace phy

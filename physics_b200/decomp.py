@@ -14,7 +14,7 @@ results are dropped.  Ownership is recomputed from the new positions before ever
 
 `SlabStepper` runs the slabs in one process (each slab's world may live on its own device);
 `RankSlabStepper` gives each rank of a torch.distributed group one slab and exchanges the
-halo and the migrating particles with point-to-point messages (gloo or NCCL).  A world is
+halo and the migrating particles as typed records in grouped point-to-point messages.  A world is
 made by a factory returning an adapter with add(pos, vel, mass, material), step(dt) and
 read() -> {field: array in insertion order}; `DeviceWorld` adapts FluidWorld.
 """
@@ -133,7 +133,14 @@ class RankSlabStepper:
     """One slab per rank of the default torch.distributed group.  Each rank keeps the
     particles it owns (with their insertion indices); before a step the ranks agree on the
     slab edges from the gathered key counts, then every rank sends each other rank the
-    particles that rank owns or needs as halo."""
+    particles that rank owns or needs as halo.
+
+    Every message is a typed tensor of fixed layout (no pickles): per particle an int64
+    record (insertion index, cell key x) and an f64 record (pos, vel, mass, material).
+    Counts travel first through all_gather; the records then move in one grouped
+    batch_isend_irecv, so no rank's send waits behind another rank's receive (a plain
+    isend/irecv sequence can deadlock under NCCL once messages exceed its buffers).  With
+    NCCL the buffers live on the rank's current device; with gloo on the host."""
 
     def __init__(self, make_world, h0: float, ids, pos, mass, vel=None, material=None):
         import torch.distributed as dist
@@ -151,10 +158,28 @@ class RankSlabStepper:
         for f in FIELDS[2:]:
             self.state[f] = np.zeros((n, 3) if f in ("acc", "xsph") else n)
 
-    def _gather(self, obj):
-        out = [None] * self.size
-        self.dist.all_gather_object(out, obj)
-        return out
+    def _device(self):
+        import torch
+        if self.dist.get_backend() == "nccl":
+            return torch.device("cuda", torch.cuda.current_device())
+        return torch.device("cpu")
+
+    def _allgather_rows(self, arr: np.ndarray) -> list:
+        """all_gather of a 2-D array whose row count differs by rank (same dtype and
+        width everywhere): the counts first, then the rows padded to the largest count."""
+        import torch
+        dev = self._device()
+        t = torch.from_numpy(np.ascontiguousarray(arr)).to(dev)
+        cnt = torch.tensor([t.shape[0]], dtype=torch.int64, device=dev)
+        cnts = [torch.zeros_like(cnt) for _ in range(self.size)]
+        self.dist.all_gather(cnts, cnt)
+        cnts = [int(c.item()) for c in cnts]
+        width = t.shape[1]
+        pad = torch.zeros((max(cnts), width), dtype=t.dtype, device=dev)
+        pad[: t.shape[0]] = t
+        outs = [torch.empty_like(pad) for _ in range(self.size)]
+        self.dist.all_gather(outs, pad)
+        return [o[:c].cpu().numpy() for o, c in zip(outs, cnts)]
 
     def step(self, dt: float, n: int = 1):
         for _ in range(n):
@@ -162,24 +187,26 @@ class RankSlabStepper:
             k = key_x(s["pos"], self.h0)
             # Slab edges from all ranks' distinct keys and counts (one entry per cell column;
             # every rank computes the same edges).
-            parts = self._gather(np.unique(k, return_counts=True))
-            uniq, inv = np.unique(np.concatenate([u for u, _ in parts]), return_inverse=True)
+            u, c = np.unique(k, return_counts=True)
+            parts = self._allgather_rows(np.stack([u, c.astype(np.int64)], axis=1))
+            allk = np.concatenate([q[:, 0] for q in parts])
+            uniq, inv = np.unique(allk, return_inverse=True)
             counts = np.zeros(len(uniq), np.int64)
-            np.add.at(counts, inv, np.concatenate([c for _, c in parts]))
+            np.add.at(counts, inv, np.concatenate([q[:, 1] for q in parts]))
             e = slab_edges_from_counts(uniq, counts, self.size)
             # Outgoing: for each rank, the particles it owns or needs as halo.
             packets = []
             for r in range(self.size):
                 sel = slab_mask(k, e[r], e[r + 1], HALO)
-                packets.append({"ids": self.ids[sel], "key": k[sel],
-                                **{f: s[f][sel] for f in ("pos", "vel", "mass", "material")}})
+                packets.append(_pack(self.ids[sel], k[sel], s, sel))
             inbox = self._exchange(packets)
-            ids = np.concatenate([p["ids"] for p in inbox])
+            ids = np.concatenate([p[0][:, 0] for p in inbox])
+            keys = np.concatenate([p[0][:, 1] for p in inbox])
+            rec = np.concatenate([p[1] for p in inbox])
             order = np.argsort(ids, kind="stable")  # ascending insertion index
-            merged = {f: np.concatenate([p[f] for p in inbox])[order]
-                      for f in ("pos", "vel", "mass", "material", "key")}
-            ids = ids[order]
-            own = slab_mask(merged["key"], e[self.rank], e[self.rank + 1])
+            ids, keys, rec = ids[order], keys[order], rec[order]
+            merged = _unpack(rec)
+            own = slab_mask(keys, e[self.rank], e[self.rank + 1])
             if own.any():
                 res = _step_slab(self.make_world, merged, np.arange(len(ids)), own, dt)
             else:
@@ -188,38 +215,74 @@ class RankSlabStepper:
             self.state = {"mass": merged["mass"][own], "material": merged["material"][own], **res}
 
     def _exchange(self, packets):
-        """packets[r] goes to rank r; returns the packets received from every rank in rank
-        order (this rank's own packet included).  Point to point: a length message, then
-        the pickled packet, to and from every other rank."""
-        import pickle
-
+        """packets[r] = (int64 [m, 2], f64 [m, 8]) goes to rank r; returns the packets
+        received from every rank in rank order (this rank's own packet included)."""
         import torch
-        dev = torch.device("cuda", torch.cuda.current_device()) if self.dist.get_backend() == "nccl" else "cpu"
-        blobs = [torch.frombuffer(bytearray(pickle.dumps(p)), dtype=torch.uint8).to(dev) for p in packets]
-        lens_out = {r: torch.tensor([blobs[r].numel()], dtype=torch.int64, device=dev) for r in range(self.size)}
-        lens_in = {r: torch.zeros(1, dtype=torch.int64, device=dev) for r in range(self.size)}
-        reqs = []
+        dev = self._device()
+        # Every rank learns every (sender, receiver) count.
+        mine = torch.tensor([p[0].shape[0] for p in packets], dtype=torch.int64, device=dev)
+        table = [torch.zeros_like(mine) for _ in range(self.size)]
+        self.dist.all_gather(table, mine)
+        incoming = [int(table[r][self.rank].item()) for r in range(self.size)]
+        ops, recv = [], {}
         for r in range(self.size):
-            if r != self.rank:
-                reqs.append(self.dist.isend(lens_out[r], r))
-                reqs.append(self.dist.irecv(lens_in[r], r))
-        for q in reqs:
-            q.wait()
-        bufs = {r: torch.empty(int(lens_in[r].item()), dtype=torch.uint8, device=dev) for r in range(self.size)
-                if r != self.rank}
-        reqs = []
+            if r == self.rank:
+                continue
+            if packets[r][0].shape[0]:
+                for a in packets[r]:
+                    ops.append(self.dist.P2POp(self.dist.isend, torch.from_numpy(np.ascontiguousarray(a)).to(dev), r))
+            if incoming[r]:
+                recv[r] = (torch.empty((incoming[r], 2), dtype=torch.int64, device=dev),
+                           torch.empty((incoming[r], _REC), dtype=torch.float64, device=dev))
+                for t in recv[r]:
+                    ops.append(self.dist.P2POp(self.dist.irecv, t, r))
+        if ops:
+            for q in self.dist.batch_isend_irecv(ops):
+                q.wait()
+        out = []
         for r in range(self.size):
-            if r != self.rank:
-                reqs.append(self.dist.isend(blobs[r], r))
-                reqs.append(self.dist.irecv(bufs[r], r))
-        for q in reqs:
-            q.wait()
-        return [packets[r] if r == self.rank else pickle.loads(bufs[r].cpu().numpy().tobytes())
-                for r in range(self.size)]
+            if r == self.rank:
+                out.append(packets[r])
+            elif r in recv:
+                out.append((recv[r][0].cpu().numpy(), recv[r][1].cpu().numpy()))
+            else:
+                out.append((np.zeros((0, 2), np.int64), np.zeros((0, _REC))))
+        return out
 
     def gather_state(self):
         """The whole state in insertion order (on every rank)."""
-        parts = self._gather((self.ids, self.state))
-        ids = np.concatenate([p[0] for p in parts])
+        s = self.state
+        n = len(self.ids)
+        cols = [self.ids.astype(np.float64)[:, None]]
+        for f in FIELDS:
+            cols.append(np.asarray(s[f], np.float64).reshape(n, -1))
+        cols += [np.asarray(s["mass"], np.float64)[:, None], np.asarray(s["material"], np.float64)[:, None]]
+        parts = self._allgather_rows(np.concatenate(cols, axis=1))
+        allrows = np.concatenate(parts)
+        ids = allrows[:, 0].astype(np.int64)
         order = np.argsort(ids, kind="stable")
-        return ids[order], {f: np.concatenate([p[1][f] for p in parts])[order] for f in parts[0][1]}
+        allrows = allrows[order]
+        out, c = {}, 1
+        for f in FIELDS:
+            w = 3 if f in ("pos", "vel", "acc", "xsph") else 1
+            out[f] = allrows[:, c:c + w] if w == 3 else allrows[:, c].copy()
+            c += w
+        out["mass"] = allrows[:, c].copy()
+        out["material"] = allrows[:, c + 1].astype(np.uint32)
+        return ids[order], out
+
+
+_REC = 8  # f64 record: pos 3, vel 3, mass, material (a u32, exact in f64)
+
+
+def _pack(ids, keys, s, sel):
+    """The fixed-layout records of the particles `sel` of state s."""
+    head = np.stack([ids, keys], axis=1).astype(np.int64)
+    rec = np.concatenate([s["pos"][sel], s["vel"][sel], s["mass"][sel][:, None],
+                          s["material"][sel].astype(np.float64)[:, None]], axis=1)
+    return head, np.ascontiguousarray(rec, np.float64)
+
+
+def _unpack(rec):
+    return {"pos": rec[:, 0:3].copy(), "vel": rec[:, 3:6].copy(), "mass": rec[:, 6].copy(),
+            "material": rec[:, 7].astype(np.uint32)}

@@ -26,6 +26,39 @@ def _precision(p) -> int:
     return _PREC[p]
 
 
+def _pack_shape_data(b: dict, data: list, faces: list) -> tuple:
+    """Appends the shape data of body or sub-shape dict `b` to the shared data / faces
+    lists (PhyCoupleBody layout, include/phy_fluid.h) and returns (data_first,
+    data_count, face_first, face_count): convex vertices and index faces, heightfield
+    heights, or a compound's 16-double sub-shape records (shape, size[3], offset[3],
+    quaternion i j k w, data_first, data_count, face_first, face_count, 0)."""
+    kind = b["shape"]
+    if kind == "convex":
+        d0, f0 = len(data), len(faces) // 3
+        data.extend(np.asarray(b["verts"], np.float64).reshape(-1).tolist())
+        faces.extend(np.asarray(b["faces"], np.uint32).reshape(-1).tolist())
+        return d0, len(b["verts"]), f0, len(b["faces"])
+    if kind == "heightfield":
+        d0 = len(data)
+        data.extend(float(h) for h in b["heights"])
+        return d0, len(b["heights"]), 0, 0
+    if kind == "compound":
+        subs = b["subs"]
+        d0 = len(data)
+        data.extend([0.0] * (16 * len(subs)))
+        for q, sub in enumerate(subs):
+            if sub["shape"] == "compound":
+                raise ValueError("nested compound shapes are not supported")
+            size = list(sub.get("size", ())) + [0.0] * 3
+            rec = [float(L.SHAPES[sub["shape"]])] + [float(v) for v in size[:3]]
+            rec += [float(v) for v in sub.get("offset", (0.0, 0.0, 0.0))]
+            rec += [float(v) for v in sub.get("rot", (0.0, 0.0, 0.0, 1.0))]
+            rec += [float(v) for v in _pack_shape_data(sub, data, faces)] + [0.0]
+            data[d0 + 16 * q: d0 + 16 * (q + 1)] = rec
+        return d0, len(subs), 0, 0
+    return 0, 0, 0, 0
+
+
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(L.DP)
 
@@ -333,17 +366,20 @@ class FluidWorld:
             out[name] = int(v.value)
         return out
 
-    def autotune(self, dt: float, steps: int = 10) -> list:
-        """The library's autotuner (phy_fluid_autotune): every launch-knob combination timed over
-        `steps` steps from the same state, the state restored, the fastest kept.  Returns the
-        trials as dicts in the order run."""
+    def autotune(self, dt: float, steps: int = 10, horizon: int = 0) -> list:
+        """The library's autotuner (phy_fluid_autotune_horizon): every knob combination (launch
+        knobs and, for tiled worlds, 4 or 2 cells per tile edge) timed over `steps` steps from
+        the same state; with horizon > 0 the fastest also from the states horizon/2 and
+        horizon steps ahead, ranked by the mean.  The state is restored and the fastest kept.
+        Returns the trials as dicts in the order run."""
         cap = 256
         out = (L.PhyTuneTrial * cap)()
         n = C.c_uint32()
-        L.check(self._lib.phy_fluid_autotune(self._h, self._sub, dt, steps, out, cap, C.byref(n)),
-                "phy_fluid_autotune")
+        L.check(self._lib.phy_fluid_autotune_horizon(self._h, self._sub, dt, steps, horizon, out, cap, C.byref(n)),
+                "phy_fluid_autotune_horizon")
         return [{"ctas_per_sm": t.ctas_per_sm, "queue": t.queue, "sort_block": t.sort_block,
-                 "ms_per_step": t.ms_per_step} for t in out[:min(n.value, cap)]]
+                 "comp_tile": t.comp_tile, "ms_per_step": t.ms_per_step, "samples": t.samples}
+                for t in out[:min(n.value, cap)]]
 
     # ---- adjoint (f64 plain form) ----------------------------------------------------
     def tape_begin(self, checkpoint_every: int = 10) -> None:
@@ -437,11 +473,12 @@ class FluidWorld:
 
     def couple_bodies(self, bodies, dt: float, friction: float = 0.0) -> np.ndarray:
         """FluidWorld::couple_bodies on the device over body dicts: `shape` (sphere, capsule,
-        box, convex, heightfield), `size` (sphere (r,), capsule (half_height, r), box half
-        extents, heightfield (nx, nz, cell)), `pos`, `rot` (unit quaternion i, j, k, w; default
-        identity), `vel`, `inv_mass` (0 = static), and `verts` + `faces` (convex) or `heights`
-        (heightfield).  Returns the bodies' updated velocities (n, 3); the fluid particles
-        inside a body are pushed out."""
+        box, convex, heightfield, compound), `size` (sphere (r,), capsule (half_height, r), box
+        half extents, heightfield (nx, nz, cell)), `pos`, `rot` (unit quaternion i, j, k, w;
+        default identity), `vel`, `inv_mass` (0 = static), `verts` + `faces` (convex),
+        `heights` (heightfield), or `subs` (compound: a list of shape dicts with their own
+        `offset` and `rot` relative to the body; no nested compounds).  Returns the bodies'
+        updated velocities (n, 3); the fluid particles inside a body are pushed out."""
         arr = (L.PhyCoupleBody * max(len(bodies), 1))()
         data, faces = [], []
         for k, b in enumerate(bodies):
@@ -454,14 +491,7 @@ class FluidWorld:
             for a, q in enumerate(b.get("rot", (0.0, 0.0, 0.0, 1.0))):
                 o.rot[a] = q
             o.inv_mass = b.get("inv_mass", 0.0)
-            if b["shape"] == "convex":
-                o.data_first, o.data_count = len(data), len(b["verts"])
-                data.extend(np.asarray(b["verts"], np.float64).reshape(-1).tolist())
-                o.face_first, o.face_count = len(faces) // 3, len(b["faces"])
-                faces.extend(np.asarray(b["faces"], np.uint32).reshape(-1).tolist())
-            elif b["shape"] == "heightfield":
-                o.data_first, o.data_count = len(data), len(b["heights"])
-                data.extend(list(b["heights"]))
+            o.data_first, o.data_count, o.face_first, o.face_count = _pack_shape_data(b, data, faces)
         d = np.array(data + [0.0], np.float64)
         f = np.array(faces + [0], np.uint32)
         L.check(self._lib.phy_fluid_couple_bodies(self._h, self._sub, C.cast(arr, C.c_void_p), len(bodies), _dp(d),

@@ -66,6 +66,9 @@ def test_null_pointer_is_safe():
                                      one.ctypes.data_as(L.DP), 0.01, 0.0, 0.0, 0.0) == -1
     assert lib.phy_fluid_couple_heat(None, 0, None, None, 1.0, None, None, 0.01, 0.0, 0.0, 0.0) == -1
     assert lib.phy_fluid_couple_bodies(None, 0, None, 1, None, 0, None, 0, 0.01, 0.0) == -1
+    assert lib.phy_fluid_pin_host(None, 64) == -1
+    assert lib.phy_fluid_pin_host(one.ctypes.data, 0) == -1
+    assert lib.phy_fluid_unpin_host(None) == -1
     assert lib.phy_fluid_last_error()  # a message was recorded
 
 

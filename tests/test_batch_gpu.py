@@ -36,8 +36,9 @@ def _batch_world(gpu, batch, **tuning):
     return w
 
 
-def _alone(gpu, b, steps):
+def _alone(gpu, b, steps, tile=4):
     w = gpu.FluidWorld(_params(b.bounds_min, b.bounds_max), "comp")
+    w.set_tuning(comp_tile=tile)
     w.add_particles(b.pos, np.full(b.n, scenes.lattice_mass(scenes.SPACING)))
     w.step(DT, steps)
     return {f: getattr(w, f) for f in FIELDS}
@@ -60,13 +61,14 @@ def _split(state, batch):
     return out
 
 
-def test_batch_scenes_bit_identical_to_alone(gpu):
+@pytest.mark.parametrize("tile", [4, 2])
+def test_batch_scenes_bit_identical_to_alone(gpu, tile):
     batch = scenes.batch_scenes(6, 300, 3000)
-    w = _batch_world(gpu, batch)
+    w = _batch_world(gpu, batch, comp_tile=tile)
     assert w.scene_count == 6
     w.step(DT, 12)
     for k, (b, got) in enumerate(zip(batch, _split(_state(w), batch))):
-        _assert_same(got, _alone(gpu, b, 12), f"scene {k}")
+        _assert_same(got, _alone(gpu, b, 12, tile), f"scene {k}")
 
 
 def test_batch_graph_and_launch_knobs_change_no_bit(gpu):
@@ -112,20 +114,30 @@ def test_batched_scene_vs_oracle_teacher_forced(gpu, oracle_mod):
         o += b.n
 
 
-def test_autotune_restores_state_and_keeps_fastest(gpu):
+@pytest.mark.parametrize("horizon", [0, 6])
+def test_autotune_restores_state_and_keeps_fastest(gpu, horizon):
+    """The autotuner over the launch knobs and 4 or 2 cells per tile edge, from the current
+    state (horizon 0) or also from the states 3 and 6 steps ahead (its six fastest
+    candidates): the world returns to its state, keeps the fastest candidate among those
+    timed on every sample, and steps on exactly like a world that never tuned (with the
+    chosen tile edge, the one knob that changes the summation order)."""
     batch = scenes.batch_scenes(4, 1000, 5000, seed=3)
     w = _batch_world(gpu, batch, graph_chunk=2)
     w.step(DT, 3)
     before = _state(w)
-    trials = w.autotune(DT, 4)
-    assert len(trials) >= 4
+    trials = w.autotune(DT, 4, horizon=horizon)
+    assert len(trials) >= 8 and {t["comp_tile"] for t in trials} == {2, 4}
     _assert_same(_state(w), before, "state after autotune")
-    best = min(trials, key=lambda t: t["ms_per_step"])
+    full = 3 if horizon else 1
+    finalists = [t for t in trials if t["samples"] == full]
+    assert len(finalists) == (6 if horizon else len(trials))
+    best = min(finalists, key=lambda t: t["ms_per_step"])
     tun = w.tuning()
-    assert (tun["ctas_per_sm"], tun["queue"], tun["sort_block"]) == (best["ctas_per_sm"], best["queue"],
-                                                                     best["sort_block"])
+    assert (tun["ctas_per_sm"], tun["queue"], tun["sort_block"], tun["comp_tile"]) == (
+        best["ctas_per_sm"], best["queue"], best["sort_block"], best["comp_tile"])
     # Stepping on from the restored state matches a world that never tuned.
     ref = _batch_world(gpu, batch, graph_chunk=2)
+    ref.set_tuning(comp_tile=tun["comp_tile"])
     ref.step(DT, 3)
     w.step(DT, 4)
     ref.step(DT, 4)

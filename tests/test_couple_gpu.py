@@ -76,11 +76,14 @@ def test_couple_points_on_tiled_compensated_world(gpu, oracle_mod):
     assert np.isfinite(w.pos).all()
 
 
-def test_couple_points_dense_neighbourhood(gpu, oracle_mod):
-    """Points whose 27 cells hold more than the 1024 candidates staged at a time."""
+@pytest.mark.parametrize("spacing,least", [(0.04, 1024), (0.03, 2048)])
+def test_couple_points_dense_neighbourhood(gpu, oracle_mod, spacing, least):
+    """Points whose 27 cells hold more than 1024 candidates, and (spacing 0.03) more than
+    the 2048 the pipelined walk prefetches, which take the chunked walk; the other points
+    of the same call stay on the pipelined one."""
     O = oracle_mod
-    w, ow, _ = _pair(gpu, O, lo=-0.3, hi=0.3, spacing=0.04, steps=2)
-    assert len(ow.neighbors_of_point([0.0, 0.0, 0.0])) > 1024
+    w, ow, _ = _pair(gpu, O, lo=-0.3, hi=0.3, spacing=spacing, steps=2)
+    assert len(ow.neighbors_of_point([0.0, 0.0, 0.0])) > least
     pts, vel, mass, prior = _points(n_random=10, seed=7)
     _check(O, w, ow, pts, vel, mass, prior)
 
@@ -296,9 +299,66 @@ def test_couple_bodies_rejects_invalid_input(gpu):
     with pytest.raises(gpu.PhyError):
         w.couple_bodies([bad_face], DT)
     arr = (L.PhyCoupleBody * 1)()
-    arr[0].shape = 5  # compound: not supported
+    arr[0].shape = 5  # compound without sub shapes
     d = np.zeros(1)
     f = np.zeros(1, np.uint32)
     assert L.load().phy_fluid_couple_bodies(w._h, 0, C.cast(arr, C.c_void_p), 1, d.ctypes.data_as(L.DP), 0,
                                             f.ctypes.data_as(C.POINTER(C.c_uint32)), 0, DT, 0.0) == -1
+    arr[0].shape = 6  # no such shape
+    assert L.load().phy_fluid_couple_bodies(w._h, 0, C.cast(arr, C.c_void_p), 1, d.ctypes.data_as(L.DP), 0,
+                                            f.ctypes.data_as(C.POINTER(C.c_uint32)), 0, DT, 0.0) == -1
+    # A compound whose sub shape is itself a compound (nesting is not supported).
+    rec = np.zeros(17)
+    rec[0], rec[10], rec[12] = 5.0, 1.0, 1.0
+    arr[0].shape, arr[0].data_first, arr[0].data_count = 5, 0, 1
+    assert L.load().phy_fluid_couple_bodies(w._h, 0, C.cast(arr, C.c_void_p), 1, rec.ctypes.data_as(L.DP), 16,
+                                            f.ctypes.data_as(C.POINTER(C.c_uint32)), 0, DT, 0.0) == -1
+    assert "nest" in L.last_error()
+    with pytest.raises(ValueError):
+        w.couple_bodies([{"shape": "compound", "pos": (0, 0, 0), "subs": [{"shape": "compound", "subs": []}]}], DT)
     w.couple_bodies([], DT)  # no bodies: no-op
+
+
+def _compounds(shift=0.0):
+    """Compound bodies (Shape::Compound, shape.rs:176-192): sub shapes with their own
+    offsets and rotations, one static, two dynamic, one holding a convex and a heightfield
+    sub shape (their data ranges follow the sub-shape records)."""
+    return [
+        {"shape": "compound", "pos": (0.1 + shift, 0.05, 0.0), "rot": _quat((0, 1, 1), 0.5), "vel": (0.1, -0.3, 0.0),
+         "inv_mass": 1.5,
+         "subs": [{"shape": "sphere", "size": (0.15,), "offset": (0.2, 0.0, 0.0)},
+                  {"shape": "box", "size": (0.1, 0.2, 0.08), "offset": (-0.15, 0.05, 0.0), "rot": _quat((1, 0, 0), 0.9)},
+                  {"shape": "capsule", "size": (0.12, 0.06), "offset": (0.0, -0.2, 0.1), "rot": _quat((0, 0, 1), 1.3)}]},
+        {"shape": "compound", "pos": (-0.3, -0.25, 0.2), "inv_mass": 0.0,
+         "subs": [{"shape": "box", "size": (0.2, 0.05, 0.2)}, {"shape": "sphere", "size": (0.1,), "offset": (0, 0.1, 0)}]},
+        {"shape": "compound", "pos": (0.25, 0.25, 0.25), "rot": _quat((1, -1, 0), 0.4), "inv_mass": 3.0,
+         "subs": [{"shape": "convex", **TETRA, "offset": (0.05, 0.0, 0.0), "rot": _quat((0, 1, 0), 0.3)},
+                  {"shape": "heightfield", "size": (2, 2, 0.3), "heights": [0.1, 0.2, -0.1, 0.05],
+                   "offset": (0.0, -0.1, 0.0)}]},
+    ]
+
+
+def test_couple_bodies_compound_bitwise(gpu, oracle_mod):
+    """Compound bodies: containment in any sub shape, push-out to the farthest sub-shape
+    support point, buoyancy of the summed sub-shape volumes, bit for bit against the
+    oracle, then 25 coupled steps with caller-integrated bodies."""
+    O = oracle_mod
+    w, ow, p = _pair(gpu, O)
+    x0 = w.pos.copy()
+    bodies = _compounds()
+    vg = _bodies_check(O, w, ow, bodies)
+    assert np.count_nonzero(np.any(w.pos != x0, axis=1)) > 20, "particles were pushed out"
+    assert not np.array_equal(vg[0], [0.1, -0.3, 0.0])
+    g = np.array(p.gravity)
+    for b, vb in zip(bodies, vg):
+        b["vel"] = tuple(vb)
+    for _ in range(25):
+        for b in bodies:
+            if b["inv_mass"] > 0:
+                b["vel"] = tuple(np.asarray(b.get("vel", (0.0, 0.0, 0.0))) + g * DT)
+                b["pos"] = tuple(np.asarray(b["pos"]) + np.asarray(b["vel"]) * DT)
+        w.step(DT)
+        ow.step(DT)
+        v = _bodies_check(O, w, ow, bodies + _bodies())
+        for b, vb in zip(bodies, v):
+            b["vel"] = tuple(vb)

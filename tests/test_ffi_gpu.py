@@ -139,6 +139,45 @@ def test_world_multiple_fluid_subsystems(gpu):
     assert sub.drag == 2.5 and sub.friction == 0.1
 
 
+def test_readback_into_pinned_buffer_and_across_subsystems(gpu):
+    """phy_world_get_fluid_positions/velocities copy straight into the caller's buffer
+    (lib.rs:399-460): the same bits whether the buffer is pageable or registered with
+    phy_fluid_pin_host, and truncation at len/3 particles that stops inside the second
+    subsystem keeps the first subsystem whole and the second's leading particles."""
+    lib = L.load()
+    p = gpu.SphParams.defaults()
+    world = gpu.World()
+    a = world.add_fluid(p)
+    b = world.add_fluid(p, "comp")
+    a.world.fill_box((-1, -1, -1), (0, 0, 0), 0.1, 0.05)
+    b.world.fill_box((1, 1, 1), (2, 2, 2), 0.1, 0.05)
+    for _ in range(3):
+        world.step(0.005)
+    na, nb = a.world.len(), b.world.len()
+    ref_pos = np.concatenate([a.world.pos, b.world.pos]).reshape(-1)
+    ref_vel = np.concatenate([a.world.vel, b.world.vel]).reshape(-1)
+    h = world.handle
+    pinned = np.empty(3 * (na + nb), np.float64)
+    assert lib.phy_fluid_pin_host(pinned.ctypes.data, pinned.nbytes) == 0, L.last_error()
+    try:
+        for fn, ref in ((lib.phy_world_get_fluid_positions, ref_pos), (lib.phy_world_get_fluid_velocities, ref_vel)):
+            pinned[:] = np.nan
+            assert fn(h, dp(pinned), pinned.size) == na + nb
+            assert_bits_equal(pinned, ref, "pinned readback")
+            k = na + 7
+            short = np.full(3 * k + 1, -1.0)
+            assert fn(h, dp(short), short.size) == k
+            assert_bits_equal(short[: 3 * k], ref[: 3 * k], "truncated across subsystems")
+            assert short[-1] == -1.0  # nothing written past len/3 particles
+            pinned[:] = np.nan
+            assert fn(h, dp(pinned), 3 * k) == k
+            assert_bits_equal(pinned[: 3 * k], ref[: 3 * k], "truncated pinned readback")
+            assert np.isnan(pinned[3 * k:]).all()
+    finally:
+        assert lib.phy_fluid_unpin_host(pinned.ctypes.data) == 0, L.last_error()
+    assert lib.phy_fluid_unpin_host(pinned.ctypes.data) == -1  # no longer registered
+
+
 def test_diagnostics_match_oracle(gpu, oracle_mod):
     O = oracle_mod
     p = gpu.SphParams.defaults()

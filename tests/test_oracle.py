@@ -316,3 +316,12 @@ def test_splitmix_matches_sequential_definition():
         z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
         ref.append(z ^ (z >> 31))
     assert scenes.splitmix64(12345, 0, 8).tolist() == ref
+
+
+def test_oracle_defaults_restatement_matches_library(oracle_mod):
+    """The oracle's own SphParams::defaults() (params.rs:55-85), used where the product
+    library must stay unloaded, equals the library's phy_sph_params_defaults field by field."""
+    a, b = oracle_mod.RefParams.defaults(), SphParams.defaults()
+    for name in ("rest_density", "stiffness", "viscosity", "visc_k", "visc_n", "shear_min", "mass", "h",
+                 "gravity", "bounds_min", "bounds_max", "boundary_damp", "xsph_eps"):
+        assert list(np.ravel(getattr(a, name))) == list(np.ravel(getattr(b, name))), name

@@ -245,3 +245,39 @@ def test_rotated_static_box_pushes_out(oracle_mod):
     x = w.get(O.F_POS)
     np.testing.assert_allclose(x[0], [0.2, 1.0, 0.2], atol=1e-15)
     assert_bits_equal(x[1], np.array([0.8, 0.0, 0.0]), "outside the turned box")
+
+
+def test_compound_body_known_answers(oracle_mod):
+    """Shape::Compound (phy-rigid shape.rs:176-192) in couple_bodies: two spheres of radius
+    0.3 at body offsets (-0.5, 0, 0) and (0.5, 0, 0).  A particle inside the +x sphere is
+    pushed to the farthest sub-shape support point along its direction from the body
+    origin, (0.8, 0, 0) (shape.rs:238-254); a particle between the spheres is inside
+    neither and stays; the body's buoyancy uses the summed sub-shape volume
+    (world.rs:531-534)."""
+    O = oracle_mod
+    p = ref_test_params(gravity=(0.0, -9.81, 0.0))
+    w = O.OracleWorld(p)
+    w.add_particles(np.array([[0.5, 0.0, 0.0], [0.0, 0.0, 0.0]]), 0.02)
+    r = 0.3
+    body = {"shape": "compound", "pos": (0.0, 0.0, 0.0), "inv_mass": 0.5,
+            "subs": [{"shape": "sphere", "size": (r,), "offset": (-0.5, 0.0, 0.0)},
+                     {"shape": "sphere", "size": (r,), "offset": (0.5, 0.0, 0.0)}]}
+    vb = w.couple_bodies([body], DT)[0]
+    x = w.get(O.F_POS)
+    assert_bits_equal(x[0], np.array([0.8, 0.0, 0.0]), "pushed to the +x sphere's support point")
+    assert_bits_equal(x[1], np.array([0.0, 0.0, 0.0]), "outside both sub shapes")
+    vol = 0.0
+    for _ in range(2):
+        vol = vol + 4.0 / 3.0 * np.pi * r * r * r
+    buoy = -np.array(p.gravity) * (p.rest_density * vol)
+    assert_bits_equal(vb, np.zeros(3) + (buoy * DT) * 0.5, "buoyancy of the summed volume (no contact at rest)")
+    # Rotated sub shape: a box rotated 90 degrees about z inside the body swaps its x/y extents.
+    w2 = O.OracleWorld(p)
+    w2.add_particles(np.array([[0.0, 0.25, 0.0], [0.25, 0.0, 0.0]]), 0.02)
+    q = (0.0, 0.0, np.sin(np.pi / 4), np.cos(np.pi / 4))
+    box = {"shape": "compound", "pos": (0.0, 0.0, 0.0), "inv_mass": 0.0,
+           "subs": [{"shape": "box", "size": (0.1, 0.3, 0.1), "rot": q}]}
+    w2.couple_bodies([box], DT)
+    x2 = w2.get(O.F_POS)
+    assert not np.array_equal(x2[1], [0.25, 0.0, 0.0]), "inside the rotated box: pushed out"
+    assert_bits_equal(x2[0], np.array([0.0, 0.25, 0.0]), "outside the rotated box: untouched")

@@ -112,11 +112,11 @@ def test_comp_free_running_stays_close(gpu, oracle_mod):
     assert dpos < 1e-3 and drho < 1e-2
 
 
-@pytest.mark.parametrize("tile,halo_cap", [(4, None), (0, None), (4, 0), (4, 300)])
+@pytest.mark.parametrize("tile,halo_cap", [(4, None), (2, None), (0, None), (4, 0), (2, 0), (4, 300), (2, 150)])
 def test_kernel_routes_agree(gpu, oracle_mod, tile, halo_cap):
-    """Each route of the compensated form (staged 4x4x4 tiles, x-major runs, tiles forced
-    through the global-memory path, a mix of staged and unstaged tiles) meets the density
-    gate on a developed state and keeps particles in bounds."""
+    """Each route of the compensated form (staged 4x4x4 and 2x2x2 tiles, x-major runs, tiles
+    forced through the dense-cell kernels, a mix of staged, slab-staged and dense tiles)
+    meets the density gate on a developed state and keeps particles in bounds."""
     O = oracle_mod
     sc = scenes.dam_break(14, 20, 14, box=3.2, dt=0.005, steps=0)
     p = _params(sc)
@@ -135,7 +135,7 @@ def test_kernel_routes_agree(gpu, oracle_mod, tile, halo_cap):
     assert np.isfinite(w.pos).all() and (w.pos >= 0).all() and (w.pos <= 3.2).all()
 
 
-@pytest.mark.parametrize("tile", [4, 0])
+@pytest.mark.parametrize("tile", [4, 2, 0])
 def test_comp_live_h_change(gpu, oracle_mod, tile):
     """A live params.h below the construction h (the cutoff trims the kernel support) and
     above it (the cutoff stays the kernel radius): the compensated routes meet the density
@@ -186,8 +186,9 @@ def test_tiled_sparse_and_out_of_bounds_particles(gpu, oracle_mod):
     assert np.isfinite(w.pos[fin]).all()
 
 
-@pytest.mark.parametrize("spacing,halo_cap", [(0.08, None), (0.08, 2500), (0.068, None)])
-def test_compressed_regimes(gpu, oracle_mod, spacing, halo_cap):
+@pytest.mark.parametrize("spacing,halo_cap,tile", [(0.08, None, 4), (0.08, 2500, 4), (0.068, None, 4),
+                                                   (0.08, None, 2), (0.068, None, 2)])
+def test_compressed_regimes(gpu, oracle_mod, spacing, halo_cap, tile):
     """Compressed fluid, as at the bottom of a tall column: ~16 particles per cell
     (spacing 0.08) makes a tile's halo too large to stage whole, so the tile is processed
     in x-slabs of 1 or 2 cell layers; at spacing 0.068 lists exceed their capacity and the
@@ -203,14 +204,14 @@ def test_compressed_regimes(gpu, oracle_mod, spacing, halo_cap):
     ow = O.OracleWorld(p, threads=O.max_threads())
     ow.add_particles(pos, 0.9, vel=vel)
     w = gpu.FluidWorld(p, "comp")
-    w.set_tuning(halo_cap=halo_cap)
+    w.set_tuning(halo_cap=halo_cap, comp_tile=tile)
     w.add_particles(pos, 0.9, vel=vel)
     w.set_counting(True)
     ow.step(0.001)
     w.step(0.001)
     e = errors(w, O, ow, p)
     cnt = w.step_counters()
-    print("compressed", spacing, halo_cap, e, cnt["pairs"] / len(pos))
+    print("compressed", spacing, halo_cap, tile, e, cnt["pairs"] / len(pos))
     assert e["rho_rel"] <= RHO_TOL and e["acc_rel_to_max"] <= 1e-3, e
 
 
@@ -243,3 +244,66 @@ def test_dense_cells(gpu, oracle_mod, per_cell):
     assert e["rho_rel"] <= RHO_TOL and e["acc_rel_to_max"] <= 1e-3, e
     # |p| errors scale with rho, which reaches many times rest density here.
     assert e["p_norm"] <= 1e-5 * max(1.0, float(np.max(ow.get(O.F_RHO))) / p.rest_density), e
+
+
+def _sheet_scene(per_cell, seed):
+    """A floor sheet of 4 x 4 cells with `per_cell` particles each plus a dense blob."""
+    rng = np.random.default_rng(seed)
+    ncell = 4 * 4
+    sheet = np.stack([rng.uniform(0.4, 1.2, ncell * per_cell), np.zeros(ncell * per_cell),
+                      rng.uniform(0.4, 1.2, ncell * per_cell)], -1)
+    blob = rng.uniform(0.6, 1.0, (4 * per_cell, 3))
+    pos = np.concatenate([sheet, blob])
+    return pos, rng.normal(0, 0.1, pos.shape)
+
+
+@pytest.mark.parametrize("per_cell,h,visc_n", [(400, 0.17, 1.0), (90, 0.2, 0.7), (400, 0.2, 1.3)])
+def test_dense_cells_live_h_and_shear(gpu, oracle_mod, per_cell, h, visc_n):
+    """The dense-cell kernels with a live params.h below the construction h (the cutoff
+    trims the kernel support: the general filter) and with a power-law material
+    (visc_n != 1: the shear sum sets mu_eff, world.rs:319-327), teacher-forced against
+    the oracle: the density gate, acceleration and mu_eff."""
+    O = oracle_mod
+    p = ref_test_params(gravity=(0.0, -9.81, 0.0))
+    p.bounds_min, p.bounds_max = (0.0, 0.0, 0.0), (1.6, 1.6, 1.6)
+    p.visc_n = [visc_n]
+    pos, vel = _sheet_scene(per_cell, per_cell + 7)
+    ow = O.OracleWorld(p, threads=O.max_threads())
+    ow.add_particles(pos, 0.02, vel=vel)
+    w = gpu.FluidWorld(p, "comp")
+    w.add_particles(pos, 0.02, vel=vel)
+    p2 = ref_test_params(gravity=(0.0, -9.81, 0.0))
+    p2.bounds_min, p2.bounds_max, p2.visc_n, p2.h = p.bounds_min, p.bounds_max, [visc_n], h
+    ow.set_params(p2)
+    w.params = p2
+    ow.step(0.001)
+    w.step(0.001)
+    e = errors(w, O, ow, p2)
+    mu_o = ow.get(O.F_MU_EFF)
+    e["mu_rel"] = float(np.max(np.abs(w.mu_eff - mu_o) / np.abs(mu_o)))
+    print("dense live h / shear", per_cell, h, visc_n, e)
+    assert e["rho_rel"] <= RHO_TOL and e["acc_rel_to_max"] <= 1e-3, e
+    assert e["p_norm"] <= 1e-5 * max(1.0, float(np.max(ow.get(O.F_RHO))) / p.rest_density), e
+    assert e["mu_rel"] <= (1e-4 if visc_n != 1.0 else 0.0), e
+
+
+@pytest.mark.parametrize("visc_n", [0.7, 1.3])
+def test_tiled_shear_thinning_and_thickening(gpu, oracle_mod, visc_n):
+    """A power-law material on the staged tiles (the shear sum is live): mu_eff and the
+    acceleration against the oracle, teacher-forced from a developed state."""
+    O = oracle_mod
+    sc = scenes.dam_break(16, 24, 16, box=3.2, dt=0.005, steps=0)
+    p = _params(sc)
+    p.visc_n = [visc_n]
+    ow = O.OracleWorld(p, threads=O.max_threads())
+    ow.add_particles(sc.pos, sc.mass)
+    ow.step(0.005, 40)
+    w = gpu.FluidWorld(p, "comp")
+    w.add_particles(ow.get(O.F_POS), ow.get(O.F_MASS), vel=ow.get(O.F_VEL))
+    ow.step(0.005)
+    w.step(0.005)
+    e = errors(w, O, ow, p)
+    mu_o = ow.get(O.F_MU_EFF)
+    e["mu_rel"] = float(np.max(np.abs(w.mu_eff - mu_o) / np.abs(mu_o)))
+    print("tiled shear", visc_n, e)
+    assert e["rho_rel"] <= RHO_TOL and e["acc_rel_to_max"] <= 1e-3 and e["mu_rel"] <= 1e-4, e

@@ -56,3 +56,51 @@ def test_4m_comp_density_vs_plain_and_determinism(gpu):
     again.step(sc.dt)
     assert_bits_equal(again.pos, plain.pos, "4M plain run-to-run")
     assert plain.len() == sc.n and np.isfinite(plain.pos).all()
+
+
+def test_plain_1m_500_steps_free_running(gpu, oracle_mod):
+    """The f64 plain-form configuration: 1,024,000 particles (80x160x80 at spacing h/2,
+    bounds [0, 32]^3), dt 0.005, 500 free-running steps, through the column's collapse
+    onto the floor (world.rs:183-397).
+    * run to run: a second world repeats every bit of the checkpoints and the end state;
+    * against the oracle, free-running: the first 10 steps bit for bit;
+    * against the oracle, teacher-forced along the whole run: from the GPU state at
+      steps 100, 250, 400 and 499 (the last in the collapsed regime) one oracle step
+      equals the GPU's next state bit for bit.  Every step being bit-exact is what
+      makes the free-running trajectory bit-exact; stepping the oracle itself through
+      all 500 collapsing steps takes tens of CPU minutes, so the steps are sampled."""
+    O = oracle_mod
+    sc = scenes.config("plain_1m")
+    p = _params(sc)
+    probes = (100, 250, 400, 499)
+    keep = set(probes) | {p_ + 1 for p_ in probes} | {10, sc.steps}
+
+    def run():
+        w = gpu.FluidWorld(p)
+        w.add_particles(sc.pos, sc.mass)
+        states, done = {}, 0
+        for s in sorted(keep):
+            w.step(sc.dt, s - done)
+            done = s
+            states[s] = (w.pos, w.vel)
+        return states
+
+    first = run()
+    second = run()
+    for s in sorted(keep):
+        assert_bits_equal(second[s][0], first[s][0], f"run-to-run pos @{s}")
+        assert_bits_equal(second[s][1], first[s][1], f"run-to-run vel @{s}")
+    assert np.isfinite(first[sc.steps][0]).all()
+
+    ow = O.OracleWorld(p, threads=O.max_threads())
+    ow.add_particles(sc.pos, sc.mass)
+    ow.step(sc.dt, 10)
+    assert_bits_equal(first[10][0], ow.get(O.F_POS), "free-running pos @10")
+    assert_bits_equal(first[10][1], ow.get(O.F_VEL), "free-running vel @10")
+    mass = np.full(sc.n, sc.mass)
+    for s in probes:
+        tw = O.OracleWorld(p, threads=O.max_threads())
+        tw.add_particles(first[s][0], mass, vel=first[s][1])
+        tw.step(sc.dt)
+        assert_bits_equal(first[s + 1][0], tw.get(O.F_POS), f"teacher-forced pos @{s}->{s + 1}")
+        assert_bits_equal(first[s + 1][1], tw.get(O.F_VEL), f"teacher-forced vel @{s}->{s + 1}")
