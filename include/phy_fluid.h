@@ -111,6 +111,23 @@ int32_t phy_fluid_get_field(PhyWorldHandle *w, uint32_t sub, int32_t field, doub
 int32_t phy_fluid_set_field(PhyWorldHandle *w, uint32_t sub, int32_t field, const double *in,
                             uint64_t len);
 
+/* Device-memory forms for callers whose particle data already lives on the
+ * GPU (a multi-GPU decomposition moving slabs between devices, an engine
+ * feeding its own buffers), so no host copy is made:
+ *   phy_fluid_set_particles_device replaces the whole particle set of `sub`
+ *   (the counterpart of assigning the reference's public `particles` Vec,
+ *   world.rs:21-30) from device arrays: pos and vel 3n doubles xyz
+ *   interleaved, mass n doubles, material n u32; vel and material may be
+ *   NULL (zeros).  Every other particle field starts at zero, as
+ *   Particle::new (particle.rs:50-63).  The positions may widen the grid box.
+ *   phy_fluid_get_field_device writes one field in insertion order to a
+ *   device buffer of at least len(sub) * components doubles.
+ * Both return after the world's stream has finished; 0 or -1 (batched
+ * scenes, an active adjoint tape, null arguments). */
+int32_t phy_fluid_set_particles_device(PhyWorldHandle *w, uint32_t sub, uint64_t n, const double *pos,
+                                       const double *vel, const double *mass, const uint32_t *material);
+int32_t phy_fluid_get_field_device(PhyWorldHandle *w, uint32_t sub, int32_t field, double *out, uint64_t len);
+
 /* The public `params` field: live read and write. */
 int32_t phy_fluid_get_params(PhyWorldHandle *w, uint32_t sub, PhySphParams *out);
 int32_t phy_fluid_set_params(PhyWorldHandle *w, uint32_t sub, const PhySphParams *in);

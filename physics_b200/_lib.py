@@ -139,6 +139,9 @@ SIGNATURES = {
     "phy_fluid_set_coupling": (C.c_int32, [H, C.c_uint32, DP]),
     "phy_fluid_set_stream": (C.c_int32, [H, C.c_void_p]),
     "phy_fluid_synchronize": (C.c_int32, [H]),
+    "phy_fluid_set_particles_device": (C.c_int32, [H, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                   C.c_void_p]),
+    "phy_fluid_get_field_device": (C.c_int32, [H, C.c_uint32, C.c_int32, C.c_void_p, C.c_uint64]),
     "phy_fluid_pin_host": (C.c_int32, [C.c_void_p, C.c_uint64]),
     "phy_fluid_unpin_host": (C.c_int32, [C.c_void_p]),
     "phy_fluid_set_counting": (C.c_int32, [H, C.c_uint32, C.c_int32]),

@@ -271,6 +271,26 @@ int32_t phy_fluid_get_field(PhyWorldHandle* w, uint32_t sub, int32_t field, doub
   });
 }
 
+int32_t phy_fluid_set_particles_device(PhyWorldHandle* w, uint32_t sub, uint64_t n, const double* pos,
+                                       const double* vel, const double* mass, const uint32_t* material) {
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->set_particles_device((size_t)n, pos, vel, mass, material);
+    return 0;
+  });
+}
+
+int32_t phy_fluid_get_field_device(PhyWorldHandle* w, uint32_t sub, int32_t field, double* out, uint64_t len) {
+  if (!out) return -1;
+  return guard<int32_t>(-1, [&] {
+    FluidWorld& fw = *sub_of(w, sub).world;
+    int nc = FluidWorld::components(field);
+    if (nc == 0) throw std::invalid_argument("unknown field");
+    if (len < (uint64_t)nc * fw.len()) throw std::invalid_argument("output buffer too small");
+    fw.get_field_device(field, out);
+    return 0;
+  });
+}
+
 int32_t phy_fluid_set_field(PhyWorldHandle* w, uint32_t sub, int32_t field, const double* in, uint64_t len) {
   if (!in) return -1;
   return guard<int32_t>(-1, [&] {

@@ -829,6 +829,65 @@ void FluidWorld::add_particles(size_t m, const double* pos, const double* vel, c
   cuda_check(cudaStreamSynchronize(stream_), "append sync");
 }
 
+// Device-side twin of k_append for set_particles_device: material as u32.
+__global__ void k_load_dev(int m, const double* __restrict__ pos, const double* __restrict__ vel,
+                           const double* __restrict__ mass, const uint32_t* __restrict__ material, double* px,
+                           double* py, double* pz, double* vx, double* vy, double* vz, double* ms, uint32_t* mat,
+                           uint32_t* id) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  px[k] = pos[3 * (size_t)k];
+  py[k] = pos[3 * (size_t)k + 1];
+  pz[k] = pos[3 * (size_t)k + 2];
+  vx[k] = vel ? vel[3 * (size_t)k] : 0.0;
+  vy[k] = vel ? vel[3 * (size_t)k + 1] : 0.0;
+  vz[k] = vel ? vel[3 * (size_t)k + 2] : 0.0;
+  ms[k] = mass[k];
+  mat[k] = material ? material[k] : 0u;
+  id[k] = (uint32_t)k;
+}
+
+void FluidWorld::set_particles_device(size_t m, const double* pos, const double* vel, const double* mass,
+                                      const uint32_t* material) {
+  if (m > 0 && (!pos || !mass)) throw std::invalid_argument("set_particles_device: pos and mass are required");
+  if (!scenes_.empty()) throw std::invalid_argument("set_particles_device: the world holds batched scenes");
+  if (tape_.on) throw std::invalid_argument("set_particles_device: the adjoint tape is recording");
+  if (m > (size_t)INT32_MAX) throw std::invalid_argument("set_particles_device: too many particles");
+  n_ = 0;
+  if (m == 0) return;
+  ensure_capacity(m);
+  // The positions, read from the caller's device buffer, may widen the grid box.
+  cuda_check(cudaMemcpyAsync(b_.stage, pos, 3 * m * sizeof(double), cudaMemcpyDeviceToDevice, stream_),
+             "set_particles_device positions");
+  grow_box_with_device_positions(m, b_.stage);
+  ParticleConsts& pc = b_.pc[b_.cur];
+  k_load_dev<<<grid_for(m), kThreads, 0, stream_>>>((int)m, pos, vel, mass, material, b_.pv1[0], b_.pv1[1],
+                                                    b_.pv1[2], b_.pv1[3], b_.pv1[4], b_.pv1[5], pc.mass, pc.mat,
+                                                    pc.id);
+  // Particle::new: acc, rho, p, mu_eff, xsph, body_acc start at zero (particle.rs:50-63).
+  const size_t bytes = m * sizeof(double);
+  cuda_check(cudaMemsetAsync(b_.rho, 0, bytes, stream_), "memset");
+  cuda_check(cudaMemsetAsync(b_.p, 0, bytes, stream_), "memset");
+  cuda_check(cudaMemsetAsync(b_.mu, 0, bytes, stream_), "memset");
+  for (int k = 0; k < 3; ++k) {
+    cuda_check(cudaMemsetAsync(b_.acc[k], 0, bytes, stream_), "memset");
+    cuda_check(cudaMemsetAsync(b_.xsph[k], 0, bytes, stream_), "memset");
+    if (b_.has_ba) cuda_check(cudaMemsetAsync(pc.ba[k], 0, bytes, stream_), "memset");
+  }
+  cuda_check(cudaGetLastError(), "set_particles_device kernel");
+  n_ = m;
+  cuda_check(cudaStreamSynchronize(stream_), "set_particles_device sync");
+}
+
+void FluidWorld::get_field_device(int field, double* out) {
+  if (components(field) == 0) throw std::invalid_argument("get_field_device: unknown field");
+  if (n_ == 0) return;
+  if (!out) throw std::invalid_argument("get_field_device: null output");
+  stage_field(field, out);
+  cuda_check(cudaGetLastError(), "get_field_device kernel");
+  cuda_check(cudaStreamSynchronize(stream_), "get_field_device sync");
+}
+
 int FluidWorld::components(int field) {
   switch (field) {
     case PHY_FIELD_POS:
@@ -848,13 +907,11 @@ int FluidWorld::components(int field) {
   }
 }
 
-void FluidWorld::get_field(int field, double* out) {
-  int nc = components(field);
-  if (nc == 0) throw std::invalid_argument("get_field: unknown field");
-  if (n_ == 0) return;
+// Field `field` of every particle in insertion order into device memory `st`
+// (3n or n doubles), on the world's stream.
+void FluidWorld::stage_field(int field, double* st) {
   const int n = (int)n_;
   const ParticleConsts& pc = b_.pc[b_.cur];
-  double* st = b_.stage;
   switch (field) {
     case PHY_FIELD_POS:
       k_get_vec_by_id<<<grid_for(n_), kThreads, 0, stream_>>>(n, pc.id, b_.pv1[0], b_.pv1[1], b_.pv1[2], st);
@@ -890,6 +947,14 @@ void FluidWorld::get_field(int field, double* out) {
       launch_unsort_u32(b_, n, pc.mat, st, stream_);
       break;
   }
+}
+
+void FluidWorld::get_field(int field, double* out) {
+  int nc = components(field);
+  if (nc == 0) throw std::invalid_argument("get_field: unknown field");
+  if (n_ == 0) return;
+  double* st = b_.stage;
+  stage_field(field, st);
   cuda_check(cudaGetLastError(), "get_field kernel");
   cuda_check(cudaMemcpyAsync(out, st, (size_t)nc * n_ * sizeof(double), cudaMemcpyDeviceToHost, stream_),
              "get_field copy");

@@ -120,6 +120,13 @@ class FluidWorld {
   // Insertion-order field access (particle.rs:17-46).
   static int components(int field);
   void get_field(int field, double* out);
+  // Device-memory forms (no host copy): replace the whole particle set from
+  // device arrays (pos/vel 3m interleaved, mass m, material m u32; vel and
+  // material may be null), and read a field in insertion order into a
+  // device buffer.
+  void set_particles_device(size_t m, const double* pos, const double* vel, const double* mass,
+                            const uint32_t* material);
+  void get_field_device(int field, double* out);
   // Position or velocity as f32 (an exact `as f32` cast of each f64 value,
   // made on the device so half the bytes cross to the host): the first
   // `count` particles in insertion order, xyz interleaved.
@@ -205,6 +212,7 @@ class FluidWorld {
   void enqueue_step(const StepConsts& c, const PassEvents& pe, const cudaEvent_t* ev);
   void run_graph(double dt, int k);
   void drop_graphs();
+  void stage_field(int field, double* st);
   void snapshot(bool restore, int slot = 0);
   void release_snapshot();
   // Mean ms per step of `steps` steps from each saved slot 0..nslots-1 under

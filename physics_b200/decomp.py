@@ -286,3 +286,219 @@ def _pack(ids, keys, s, sel):
 def _unpack(rec):
     return {"pos": rec[:, 0:3].copy(), "vel": rec[:, 3:6].copy(), "mass": rec[:, 6].copy(),
             "material": rec[:, 7].astype(np.uint32)}
+
+
+# ---- Device-resident form -------------------------------------------------------------
+#
+# The state stays in torch tensors on the slab's device (the rank's GPU under NCCL,
+# the host under gloo), each slab keeps one persistent world that is reloaded in
+# place every step (FluidWorld.set_particles_device: no host copy, no allocation
+# while the slab's size fits), and the halo and migrant records travel between
+# ranks as typed device tensors in grouped point-to-point messages.  The ownership
+# and ordering rules are those above, so the owned results are again the whole
+# world's bits.
+
+def key_x_t(pos, h0: float):
+    """key_x on a torch tensor of positions (same f64 operations: x * (1/h0), floor,
+    0 outside the int64 range or for non-finite values)."""
+    import torch
+    f = torch.floor(pos[:, 0] * (1.0 / h0))
+    ok = torch.isfinite(f) & (f > -9.223372036854775808e18) & (f < 9.223372036854775808e18)
+    return torch.where(ok, f, torch.zeros_like(f)).to(torch.int64)
+
+
+def slab_mask_t(keys, lo: int, hi: int, halo: int = 0):
+    return (keys >= max(lo - halo, I64_MIN)) & (keys < min(hi + halo, I64_MAX))
+
+
+class ResidentDeviceWorld:
+    """A persistent device FluidWorld reloaded in place each step from device tensors."""
+
+    def __init__(self, params, precision: str = "f64"):
+        from . import _lib as L
+        from .fluid import FluidWorld
+        self.w = FluidWorld(params, precision)
+        self.ids = {"pos": L.FIELD_POS, "vel": L.FIELD_VEL, "rho": L.FIELD_RHO, "p": L.FIELD_P, "acc": L.FIELD_ACC,
+                    "mu_eff": L.FIELD_MU_EFF, "xsph": L.FIELD_XSPH}
+
+    def load(self, pos, vel, mass, material):
+        import torch
+        self.w.set_particles_device(pos.contiguous(), mass.contiguous(), vel=vel.contiguous(),
+                                    material=material.to(torch.int32).contiguous())
+
+    def step(self, dt: float):
+        self.w.step(dt)
+
+    def read(self) -> dict:
+        import torch
+        n = len(self.w)
+        out = {}
+        for f, fid in self.ids.items():
+            t = torch.empty((n, 3) if f in ("pos", "vel", "acc", "xsph") else (n,), dtype=torch.float64,
+                            device=torch.device("cuda", torch.cuda.current_device()))
+            if n:
+                self.w.get_device(fid, t)
+            out[f] = t
+        return out
+
+
+def _state_t(pos, vel, mass, material, device):
+    import torch
+    n = pos.shape[0]
+    st = {
+        "pos": torch.as_tensor(pos, dtype=torch.float64, device=device).reshape(n, 3).contiguous(),
+        "vel": (torch.zeros((n, 3), dtype=torch.float64, device=device) if vel is None
+                else torch.as_tensor(vel, dtype=torch.float64, device=device).reshape(n, 3).contiguous()),
+        "mass": torch.as_tensor(np.broadcast_to(np.asarray(mass, np.float64), (n,)).copy(), device=device),
+        "material": (torch.zeros(n, dtype=torch.int64, device=device) if material is None
+                     else torch.as_tensor(np.asarray(material, np.int64), device=device)),
+    }
+    for f in FIELDS[2:]:
+        st[f] = torch.zeros((n, 3) if f in ("acc", "xsph") else (n,), dtype=torch.float64, device=device)
+    return st
+
+
+class ResidentSlabs:
+    """All slabs in one process on one device, each with its persistent world; the state
+    is kept in insertion order in device tensors."""
+
+    def __init__(self, make_world, h0: float, nslabs: int, pos, mass, vel=None, material=None, device="cuda"):
+        self.h0, self.nslabs = h0, nslabs
+        self.state = _state_t(np.asarray(pos, np.float64), vel, mass, material, device)
+        self.worlds = [make_world() for _ in range(nslabs)]
+        self.edges = None
+
+    def step(self, dt: float, n: int = 1):
+        import torch
+        for _ in range(n):
+            s = self.state
+            k = key_x_t(s["pos"], self.h0)
+            uniq, counts = torch.unique(k, return_counts=True)
+            self.edges = e = slab_edges_from_counts(uniq.cpu().numpy(), counts.cpu().numpy(), self.nslabs)
+            new = {f: s[f].clone() for f in FIELDS}
+            for r in range(self.nslabs):
+                own = slab_mask_t(k, e[r], e[r + 1])
+                if not bool(own.any()):
+                    continue
+                local = torch.nonzero(slab_mask_t(k, e[r], e[r + 1], HALO)).squeeze(1)  # ascending index
+                w = self.worlds[r]
+                w.load(s["pos"][local], s["vel"][local], s["mass"][local], s["material"][local])
+                w.step(dt)
+                res = w.read()
+                keep = own[local]
+                ids = local[keep]
+                for f in FIELDS:
+                    new[f][ids] = res[f][keep]
+            s.update(new)
+
+
+class ResidentSlabStepper:
+    """One slab per rank of the default torch.distributed group, state resident on the
+    rank's device (CUDA under NCCL, the host under gloo) with one persistent world.  Each
+    step: the ranks agree on slab edges from all-gathered (key, count) rows; every rank
+    sends each other rank the particles that rank owns or needs as halo as two typed
+    records (int64 [insertion index, key], f64 [pos, vel, mass, material]) in one grouped
+    batch_isend_irecv; the received rows are ordered by insertion index, loaded into the
+    slab's world, stepped, and the owned rows kept."""
+
+    def __init__(self, make_world, h0: float, ids, pos, mass, vel=None, material=None):
+        import torch
+        import torch.distributed as dist
+        self.dist = dist
+        self.rank, self.size = dist.get_rank(), dist.get_world_size()
+        self.dev = (torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl"
+                    else torch.device("cpu"))
+        self.h0 = h0
+        self.ids = torch.as_tensor(np.asarray(ids, np.int64), device=self.dev)
+        self.state = _state_t(np.asarray(pos, np.float64), vel, mass, material, self.dev)
+        self.world = make_world()
+
+    def _allgather_rows(self, t) -> list:
+        import torch
+        cnt = torch.tensor([t.shape[0]], dtype=torch.int64, device=self.dev)
+        cnts = [torch.zeros_like(cnt) for _ in range(self.size)]
+        self.dist.all_gather(cnts, cnt)
+        cnts = [int(c.item()) for c in cnts]
+        pad = torch.zeros((max(cnts), t.shape[1]), dtype=t.dtype, device=self.dev)
+        pad[: t.shape[0]] = t
+        outs = [torch.empty_like(pad) for _ in range(self.size)]
+        self.dist.all_gather(outs, pad)
+        return [o[:c] for o, c in zip(outs, cnts)]
+
+    def step(self, dt: float, n: int = 1):
+        import torch
+        for _ in range(n):
+            s = self.state
+            k = key_x_t(s["pos"], self.h0)
+            u, c = torch.unique(k, return_counts=True)
+            rows = torch.cat(self._allgather_rows(torch.stack([u, c.to(torch.int64)], dim=1)))
+            uniq, inv = torch.unique(rows[:, 0], return_inverse=True)
+            counts = torch.zeros(uniq.shape[0], dtype=torch.int64, device=self.dev).index_add_(0, inv, rows[:, 1])
+            e = slab_edges_from_counts(uniq.cpu().numpy(), counts.cpu().numpy(), self.size)
+            rec = torch.cat([s["pos"], s["vel"], s["mass"][:, None], s["material"].to(torch.float64)[:, None]], 1)
+            head = torch.stack([self.ids, k], dim=1)
+            packets = []
+            for r in range(self.size):
+                sel = slab_mask_t(k, e[r], e[r + 1], HALO)
+                packets.append((head[sel].contiguous(), rec[sel].contiguous()))
+            inbox = self._exchange(packets)
+            head_in = torch.cat([p[0] for p in inbox])
+            rec_in = torch.cat([p[1] for p in inbox])
+            order = torch.sort(head_in[:, 0], stable=True).indices  # ascending insertion index
+            head_in, rec_in = head_in[order], rec_in[order]
+            own = slab_mask_t(head_in[:, 1], e[self.rank], e[self.rank + 1])
+            res = None
+            if bool(own.any()):
+                self.world.load(rec_in[:, 0:3], rec_in[:, 3:6], rec_in[:, 6], rec_in[:, 7].to(torch.int64))
+                self.world.step(dt)
+                res = self.world.read()
+            self.ids = head_in[own, 0].contiguous()
+            self.state = {"mass": rec_in[own, 6].contiguous(), "material": rec_in[own, 7].to(torch.int64)}
+            for f in FIELDS:
+                shape = (0, 3) if f in ("pos", "vel", "acc", "xsph") else (0,)
+                self.state[f] = (res[f][own].to(self.dev).contiguous() if res is not None
+                                 else torch.zeros(shape, dtype=torch.float64, device=self.dev))
+
+    def _exchange(self, packets):
+        import torch
+        mine = torch.tensor([p[0].shape[0] for p in packets], dtype=torch.int64, device=self.dev)
+        table = [torch.zeros_like(mine) for _ in range(self.size)]
+        self.dist.all_gather(table, mine)
+        incoming = [int(table[r][self.rank].item()) for r in range(self.size)]
+        ops, recv = [], {}
+        for r in range(self.size):
+            if r == self.rank:
+                continue
+            if packets[r][0].shape[0]:
+                ops += [self.dist.P2POp(self.dist.isend, packets[r][0], r),
+                        self.dist.P2POp(self.dist.isend, packets[r][1], r)]
+            if incoming[r]:
+                recv[r] = (torch.empty((incoming[r], 2), dtype=torch.int64, device=self.dev),
+                           torch.empty((incoming[r], _REC), dtype=torch.float64, device=self.dev))
+                ops += [self.dist.P2POp(self.dist.irecv, t, r) for t in recv[r]]
+        if ops:
+            for q in self.dist.batch_isend_irecv(ops):
+                q.wait()
+        empty = (torch.zeros((0, 2), dtype=torch.int64, device=self.dev),
+                 torch.zeros((0, _REC), dtype=torch.float64, device=self.dev))
+        return [packets[r] if r == self.rank else recv.get(r, empty) for r in range(self.size)]
+
+    def gather_state(self):
+        """The whole state in insertion order, as numpy arrays (on every rank)."""
+        import torch
+        n = self.ids.shape[0]
+        cols = [self.ids.to(torch.float64)[:, None]]
+        for f in FIELDS:
+            cols.append(self.state[f].reshape(n, -1).to(torch.float64))
+        cols += [self.state["mass"][:, None], self.state["material"].to(torch.float64)[:, None]]
+        allrows = torch.cat(self._allgather_rows(torch.cat(cols, 1))).cpu().numpy()
+        order = np.argsort(allrows[:, 0].astype(np.int64), kind="stable")
+        allrows = allrows[order]
+        out, col = {}, 1
+        for f in FIELDS:
+            w = 3 if f in ("pos", "vel", "acc", "xsph") else 1
+            out[f] = allrows[:, col:col + w] if w == 3 else allrows[:, col].copy()
+            col += w
+        out["mass"] = allrows[:, col].copy()
+        out["material"] = allrows[:, col + 1].astype(np.uint32)
+        return allrows[:, 0].astype(np.int64), out

@@ -306,6 +306,26 @@ class FluidWorld:
         L.check(self._lib.phy_fluid_get_field(self._h, self._sub, fld, _dp(out), out.size), "phy_fluid_get_field")
         return out.reshape(n, nc) if nc == 3 else out
 
+    def set_particles_device(self, pos, mass, vel=None, material=None) -> None:
+        """Replaces the particle set with device tensors (phy_fluid_set_particles_device):
+        pos / vel (n, 3) float64, mass (n,) float64, material (n,) int32/uint32, all
+        contiguous on this world's device; no host copy."""
+        n = int(mass.shape[0])
+        for t, want in ((pos, 3 * n), (vel, 3 * n), (mass, n), (material, n)):
+            if t is not None and (not t.is_cuda or not t.is_contiguous() or t.numel() != want):
+                raise ValueError("set_particles_device: contiguous CUDA tensors of matching sizes")
+        ptr = (lambda t: C.c_void_p(t.data_ptr()) if t is not None else None)
+        L.check(self._lib.phy_fluid_set_particles_device(self._h, self._sub, n, ptr(pos), ptr(vel), ptr(mass),
+                                                         ptr(material)), "phy_fluid_set_particles_device")
+
+    def get_device(self, fld: int, out) -> None:
+        """Writes field `fld` in insertion order into the contiguous float64 CUDA tensor
+        `out` (phy_fluid_get_field_device); no host copy."""
+        if not out.is_cuda or not out.is_contiguous():
+            raise ValueError("get_device: a contiguous CUDA tensor")
+        L.check(self._lib.phy_fluid_get_field_device(self._h, self._sub, fld, C.c_void_p(out.data_ptr()),
+                                                     out.numel()), "phy_fluid_get_field_device")
+
     def set(self, fld: int, values) -> None:
         a = np.ascontiguousarray(values, np.float64).reshape(-1)
         L.check(self._lib.phy_fluid_set_field(self._h, self._sub, fld, _dp(a), a.size), "phy_fluid_set_field")

@@ -157,3 +157,81 @@ def test_device_slabs_equal_the_whole_device_world(gpu):
     ref = _whole(make, sc, vel, mat, 10)
     for f in decomp.FIELDS:
         assert_bits_equal(st.state[f], ref[f], f"{f}, device slabs")
+
+
+class OracleResidentWorld:
+    """The oracle behind the resident steppers' tensor interface (host tensors)."""
+
+    def __init__(self, O, params):
+        self.O, self.params = O, params
+
+    def load(self, pos, vel, mass, material):
+        self.w = self.O.OracleWorld(self.params)
+        if mass.shape[0]:
+            self.w.add_particles(pos.numpy(), mass.numpy(), vel=vel.numpy(), material=material.numpy())
+
+    def step(self, dt):
+        self.w.step(dt)
+
+    def read(self):
+        import torch
+        return {k: torch.from_numpy(np.ascontiguousarray(v)) for k, v in OracleSlabWorld.read(self).items()}
+
+
+def _resident_rank_main(rank, world_size, port, q):
+    import torch.distributed as dist
+    from oracle import oracle as O
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world_size)
+    try:
+        O.build()
+        sc, p, vel, mat = _scene()
+        mine = np.flatnonzero(np.arange(sc.n) % world_size == rank)
+        st = decomp.ResidentSlabStepper(lambda: OracleResidentWorld(O, p), p.h, mine, sc.pos[mine], sc.mass,
+                                        vel=vel[mine], material=mat[mine])
+        st.step(DT, 15)
+        ids, state = st.gather_state()
+        q.put((rank, int(st.ids.shape[0]), ids, state if rank == 0 else None))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world_size", [2, 3])
+def test_resident_ranks_equal_the_whole_world(oracle_mod, world_size):
+    """The device-resident form's exchange (typed records, grouped point-to-point,
+    persistent slab worlds reloaded in place) on gloo ranks over host tensors: the whole
+    world's bits."""
+    import multiprocessing as mp
+    O = oracle_mod
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_resident_rank_main, args=(r, world_size, port, q)) for r in range(world_size)]
+    for pr in procs:
+        pr.start()
+    out = sorted([q.get(timeout=300) for _ in procs], key=lambda t: t[0])
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    sc, p, vel, mat = _scene()
+    assert all(o[1] > 0 for o in out) and sum(o[1] for o in out) == sc.n
+    ids, state = out[0][2], out[0][3]
+    assert np.array_equal(ids, np.arange(sc.n))
+    ref = _whole(lambda: OracleSlabWorld(O, p), sc, vel, mat, 15)
+    for f in decomp.FIELDS:
+        assert_bits_equal(state[f], ref[f], f"{f}, {world_size} resident ranks")
+
+
+@pytest.mark.gpu
+def test_resident_device_slabs_equal_the_whole_device_world(gpu):
+    """Persistent device worlds, one per slab, reloaded in place from device tensors each
+    step (phy_fluid_set_particles_device / phy_fluid_get_field_device; the state never
+    leaves the GPU): the whole device world's bits, particles migrating between slabs."""
+    sc, p, vel, mat = _scene()
+    st = decomp.ResidentSlabs(lambda: decomp.ResidentDeviceWorld(p, "f64"), p.h, 3, sc.pos, sc.mass, vel=vel,
+                              material=mat)
+    st.step(DT, 12)
+    ref = _whole(lambda: decomp.DeviceWorld(p, "f64"), sc, vel, mat, 12)
+    for f in decomp.FIELDS:
+        assert_bits_equal(st.state[f].cpu().numpy(), ref[f], f"{f}, resident device slabs")
