@@ -159,16 +159,20 @@ __global__ void __launch_bounds__(kCT) k_couple_points(StepConsts c, CoupleArgs 
 
 // Pipelined form of the same walk.  Only velocities change from one point to
 // the next, so while thread 0 runs point k's ordered sums, warps 1..7 build
-// point k+1's cell table and its candidates' particle indices and masses
-// (double-buffered in shared memory).  Point k's velocities are gathered once
-// after point k-1's reaction; the reaction reuses them (v_j + share, the same
-// f64 operations), so a point costs one gather, the ordered sums and one
-// scatter.  Points with more than kPB candidates take the chunked walk above.
-constexpr int kPB = 2048;  // candidates prefetched per point
+// point k+1's cell table, its candidates' particle indices, masses and
+// velocities and the products v_j m_j (double-buffered in shared memory).
+// Point k's reaction can change only the velocities of particles in point
+// k's own 27 cells, so after it those of point k+1's cells that are also
+// point k's are gathered again (points far apart share none).  The ordered
+// sums then read ready products (sx + v m with the product formed once, the
+// same f64 operations), and the reaction reuses the gathered velocities
+// (v_j + share).  Points with more than kPB candidates take a chunked walk.
+constexpr int kPB = 1024;  // candidates prefetched per point
 
 struct PointTable {
   uint32_t beg[27];
   uint32_t pre[28];
+  uint32_t again;  // bit u: cell u is also a cell of the previous point (gather again after its reaction)
   int in;
 };
 
@@ -204,19 +208,60 @@ __device__ __forceinline__ void point_table(const StepConsts& c, const CoupleArg
   __syncwarp();
 }
 
+// Staged candidate data of one point: particle index, mass, velocity, and
+// the products (v m) in the order the ordered sums read them.
+struct PointBuf {
+  uint32_t* idx;  // [kPB]
+  double* m;      // [kPB]
+  double* v;      // [3][kPB]
+  double2* pw;    // [2 kPB]: (v_x m, v_y m), (v_z m, m) per candidate
+};
+
+// Buffer q (0 or 1) of the pipelined kernel's dynamic shared memory.
+__device__ __forceinline__ PointBuf point_buf(unsigned char* smem, int q) {
+  double2* pw = reinterpret_cast<double2*>(smem);             // [2][2 kPB]
+  double* v = reinterpret_cast<double*>(pw + 4 * kPB);         // [2][3][kPB]
+  double* m = v + 6 * kPB;                                     // [2][kPB]
+  uint32_t* idx = reinterpret_cast<uint32_t*>(m + 2 * kPB);    // [2][kPB]
+  return {idx + q * kPB, m + q * kPB, v + 3 * q * kPB, pw + 2 * q * kPB};
+}
+
+__device__ __forceinline__ void gather_candidate(const CoupleArgs& a, const PointBuf& B, uint32_t e) {
+  const uint32_t i = B.idx[e];
+  const double m = B.m[e];
+  const double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i];
+  B.v[e] = vx;
+  B.v[kPB + e] = vy;
+  B.v[2 * kPB + e] = vz;
+  B.pw[2 * e] = make_double2(vx * m, vy * m);
+  B.pw[2 * e + 1] = make_double2(vz * m, m);
+}
+
 // Warps 1..7: the table of point k and, when it fits, its candidates'
-// indices and masses.
+// indices, masses, velocities and products.  `prev` is the table of point
+// k-1 when its reaction has not run yet (its cells are flagged in `again`),
+// else null.
 __device__ __forceinline__ void prefetch_point(const StepConsts& c, const CoupleArgs& a, int k, PointTable& T,
-                                               uint32_t* idx, double* m) {
-  if ((threadIdx.x >> 5) == 1) point_table(c, a, k, T);
+                                               const PointTable* prev, const PointBuf& B) {
+  if ((threadIdx.x >> 5) == 1) {
+    point_table(c, a, k, T);
+    const int lane = threadIdx.x & 31;
+    bool shared = false;
+    if (T.in && prev && prev->in && lane < 27 && T.pre[lane + 1] > T.pre[lane])
+      for (int u = 0; u < 27; ++u)
+        shared = shared || (prev->pre[u + 1] > prev->pre[u] && prev->beg[u] == T.beg[lane]);
+    const uint32_t bits = __ballot_sync(0xffffffffu, shared);
+    if (lane == 0) T.again = bits;
+  }
   asm volatile("bar.sync 1, %0;" ::"r"(kCT - 32));
   if (!T.in) return;
   const uint32_t total = T.pre[27];
   if (total > (uint32_t)kPB) return;
   for (uint32_t e = threadIdx.x - 32; e < total; e += kCT - 32) {
     const uint32_t i = candidate(a, T.beg, T.pre, e);
-    idx[e] = i;
-    m[e] = a.mass[i];
+    B.idx[e] = i;
+    B.m[e] = a.mass[i];
+    gather_candidate(a, B, e);
   }
 }
 
@@ -224,40 +269,36 @@ __global__ void __launch_bounds__(kCT) k_couple_points_piped(StepConsts c, Coupl
   __shared__ PointTable s_tab[2];
   __shared__ double s_r[4];  // reaction xyz, sum of masses
   extern __shared__ __align__(16) unsigned char smem[];
-  double* s_m = reinterpret_cast<double*>(smem);         // [2][kPB] masses
-  double* s_v = s_m + 2 * kPB;                           // [3][kPB] velocities
-  uint32_t* s_idx = reinterpret_cast<uint32_t*>(s_v + 3 * kPB);  // [2][kPB] particle indices
   const int t = threadIdx.x, warp = t >> 5;
-  if (warp >= 1 && a.np > 0) prefetch_point(c, a, 0, s_tab[0], s_idx, s_m);
+  if (warp >= 1 && a.np > 0) prefetch_point(c, a, 0, s_tab[0], nullptr, point_buf(smem, 0));
   __syncthreads();
   for (int k = 0; k < a.np; ++k) {
     const int cur = k & 1, nxt = cur ^ 1;
     const PointTable& T = s_tab[cur];
-    uint32_t* idx = s_idx + cur * kPB;
-    double* m = s_m + cur * kPB;
+    const PointBuf B = point_buf(smem, cur);
     double* q = a.pts + 10 * (size_t)k;
     const bool more = k + 1 < a.np;
     const uint32_t total = T.in ? T.pre[27] : 0u;
     if (!T.in || total > (uint32_t)kPB) {
       if (T.in) {
-        // Chunked walk: candidates staged kPB at a time (m and s_v as staging).
+        // Chunked walk: candidates staged kPB at a time in this point's buffer.
         double sx = 0.0, sy = 0.0, sz = 0.0, sw = 0.0;
         for (uint32_t base = 0; base < total; base += kPB) {
           const uint32_t cnt = min((uint32_t)kPB, total - base);
           for (uint32_t e = t; e < cnt; e += kCT) {
             const uint32_t i = candidate(a, T.beg, T.pre, base + e);
-            s_v[e] = a.vx[i];
-            s_v[kPB + e] = a.vy[i];
-            s_v[2 * kPB + e] = a.vz[i];
-            m[e] = a.mass[i];
+            B.v[e] = a.vx[i];
+            B.v[kPB + e] = a.vy[i];
+            B.v[2 * kPB + e] = a.vz[i];
+            B.m[e] = a.mass[i];
           }
           __syncthreads();
           if (t == 0)
             for (uint32_t e = 0; e < cnt; ++e) {
-              const double w = m[e];
-              sx = sx + s_v[e] * w;
-              sy = sy + s_v[kPB + e] * w;
-              sz = sz + s_v[2 * kPB + e] * w;
+              const double w = B.m[e];
+              sx = sx + B.v[e] * w;
+              sy = sy + B.v[kPB + e] * w;
+              sz = sz + B.v[2 * kPB + e] * w;
               sw = sw + w;
             }
           __syncthreads();
@@ -275,45 +316,49 @@ __global__ void __launch_bounds__(kCT) k_couple_points_piped(StepConsts c, Coupl
           }
       }
       __syncthreads();
-      if (warp >= 1 && more) prefetch_point(c, a, k + 1, s_tab[nxt], s_idx + nxt * kPB, s_m + nxt * kPB);
+      // Point k's velocities are final: the next point needs no second gather.
+      if (warp >= 1 && more) prefetch_point(c, a, k + 1, s_tab[nxt], nullptr, point_buf(smem, nxt));
       __syncthreads();
       continue;
     }
-    for (uint32_t e = t; e < total; e += kCT) {
-      const uint32_t i = idx[e];
-      s_v[e] = a.vx[i];
-      s_v[kPB + e] = a.vy[i];
-      s_v[2 * kPB + e] = a.vz[i];
-    }
-    __syncthreads();
     if (t == 0) {
       double sx = 0.0, sy = 0.0, sz = 0.0, sw = 0.0;
       for (uint32_t e = 0; e < total; ++e) {
-        const double w = m[e];
-        sx = sx + s_v[e] * w;
-        sy = sy + s_v[kPB + e] * w;
-        sz = sz + s_v[2 * kPB + e] * w;
-        sw = sw + w;
+        const double2 p = B.pw[2 * e], r = B.pw[2 * e + 1];
+        sx = sx + p.x;
+        sy = sy + p.y;
+        sz = sz + r.x;
+        sw = sw + r.y;
       }
       point_force(c, a, q, sx, sy, sz, sw, s_r);
     } else if (warp >= 1 && more) {
-      prefetch_point(c, a, k + 1, s_tab[nxt], s_idx + nxt * kPB, s_m + nxt * kPB);
+      prefetch_point(c, a, k + 1, s_tab[nxt], &T, point_buf(smem, nxt));
     }
     __syncthreads();
     const double msum = s_r[3];
     if (msum > 0.0)
       for (uint32_t e = t; e < total; e += kCT) {
-        const uint32_t i = idx[e];
-        const double frac = m[e] / msum;
-        a.vx[i] = s_v[e] + s_r[0] * frac;
-        a.vy[i] = s_v[kPB + e] + s_r[1] * frac;
-        a.vz[i] = s_v[2 * kPB + e] + s_r[2] * frac;
+        const uint32_t i = B.idx[e];
+        const double frac = B.m[e] / msum;
+        a.vx[i] = B.v[e] + s_r[0] * frac;
+        a.vy[i] = B.v[kPB + e] + s_r[1] * frac;
+        a.vz[i] = B.v[2 * kPB + e] + s_r[2] * frac;
       }
     __syncthreads();
+    // The next point's candidates in cells this point shares took its
+    // reaction: gather them again.
+    if (more && s_tab[nxt].in && s_tab[nxt].pre[27] <= (uint32_t)kPB && s_tab[nxt].again) {
+      const PointTable& N = s_tab[nxt];
+      const PointBuf NB = point_buf(smem, nxt);
+      for (int u = 0; u < 27; ++u)
+        if (N.again >> u & 1u)
+          for (uint32_t e = N.pre[u] + t; e < N.pre[u + 1]; e += kCT) gather_candidate(a, NB, e);
+      __syncthreads();
+    }
   }
 }
 
-constexpr size_t kPipedSmem = (size_t)kPB * (2 * 8 + 3 * 8 + 2 * 4);
+constexpr size_t kPipedSmem = (size_t)kPB * (4 * 16 + 2 * 3 * 8 + 2 * 8 + 2 * 4);
 
 // ---- couple_heat (world.rs:555-678) ------------------------------------------------
 //

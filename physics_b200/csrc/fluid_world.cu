@@ -260,7 +260,11 @@ void dgrow(T*& p, size_t keep, size_t cap, cudaStream_t s) {
 }  // namespace
 
 void cuda_check(cudaError_t e, const char* what) {
-  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+  if (e == cudaSuccess) return;
+  // The error goes to the caller; a non-sticky API error must not stay in the
+  // runtime's last-error slot and fail the next, unrelated call's check.
+  (void)cudaGetLastError();
+  throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
 // ---- SphParams -------------------------------------------------------------

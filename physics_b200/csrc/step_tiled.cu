@@ -499,7 +499,7 @@ __global__ void __launch_bounds__(kTT, 6) k_density_tiled(StepConsts c, TiledArg
 struct CompAcc {
   float fpx = 0.f, fpy = 0.f, fpz = 0.f, cpx = 0.f, cpy = 0.f, cpz = 0.f;
   float fvx = 0.f, fvy = 0.f, fvz = 0.f, cvx = 0.f, cvy = 0.f, cvz = 0.f;
-  float xsx = 0.f, xsy = 0.f, xsz = 0.f, shear = 0.f;
+  float xsx = 0.f, xsy = 0.f, xsz = 0.f, shear = 0.f, csh = 0.f;
 };
 
 // mu_eff, acc, integrate and bounds in f64 (world.rs:319-397).
@@ -531,7 +531,7 @@ __device__ __forceinline__ void finish_particle(const StepConsts& c, const Tiled
   double kc, nn;
   material_coeffs(c, midx, kc, nn);
   const double ex = nn - 1.0;
-  const double sh = (double)q.shear;
+  const double sh = (double)q.shear - (double)q.csh;
   const double sreg = sh > c.shear_min ? sh : c.shear_min;
   const double mu = kc * (ex == 0.0 ? 1.0 : pow(sreg, ex));
   double ax = 0.0, ay = 0.0, az = 0.0;
@@ -587,12 +587,14 @@ __device__ __forceinline__ void finish_particle(const StepConsts& c, const Tiled
   finish_particle(c, a, i, q, bx, load_own(a, i));
 }
 
-// Batch partial sums of the pressure and raw viscous forces; folded into the
-// Kahan-compensated totals every four pairs.
+// Batch partial sums of the pressure and raw viscous forces (and of the
+// shear sum, when it is live); folded into the Kahan-compensated totals every
+// four pairs.
 struct ForcePart {
-  float fx = 0.f, fy = 0.f, fz = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+  float fx = 0.f, fy = 0.f, fz = 0.f, vx = 0.f, vy = 0.f, vz = 0.f, sh = 0.f;
 };
 
+template <bool kShear>
 __device__ __forceinline__ void fold(CompAcc& q, ForcePart& b) {
   kahan_add(q.fpx, q.cpx, b.fx);
   kahan_add(q.fpy, q.cpy, b.fy);
@@ -600,6 +602,7 @@ __device__ __forceinline__ void fold(CompAcc& q, ForcePart& b) {
   kahan_add(q.fvx, q.cvx, b.vx);
   kahan_add(q.fvy, q.cvy, b.vy);
   kahan_add(q.fvz, q.cvz, b.vz);
+  if (kShear) kahan_add(q.shear, q.csh, b.sh);
   b = ForcePart();
 }
 
@@ -638,7 +641,7 @@ __device__ __forceinline__ void pair_listed(const StepConsts& c, float4 pj, floa
   if (kShear) {
     const float dv2 = dvx * dvx + dvy * dvy + dvz * dvz;
     const float dvn = dv2 > 0.f ? dv2 * rsqrtf(dv2) : 0.f;
-    q.shear = fmaf(__fdividef(dvn, r + 1e-4f), mr, q.shear);
+    b.sh = fmaf(__fdividef(dvn, r + 1e-4f), mr, b.sh);
   }
 }
 
@@ -707,7 +710,7 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
               const uint32_t j = (w[u >> 1] >> (16 * (u & 1))) & 0xffffu;
               pair_listed<kShear>(c, s_pos[j], s_vel[j], s_mr[j], pi, vi, lapm_i, b, q);
             }
-            if (u == 3 || u == 7) fold(q, b);
+            if (u == 3 || u == 7) fold<kShear>(q, b);
           }
           cur = nxt;
         }
@@ -721,7 +724,7 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
               const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
               if (!(dx * dx + dy * dy + dz * dz < hc2)) continue;
               pair_listed<kShear>(c, pj, s_vel[j], s_mr[j], pi, vi, lapm_i, b, q);
-              fold(q, b);
+              fold<kShear>(q, b);
             }
           }
       }
@@ -1019,14 +1022,14 @@ __global__ void __launch_bounds__(kWT, 3) k_force_dense(StepConsts c, TiledArgs 
           mask &= mask - 1;
           pair_listed<kShear>(c, s_pos[w][k], s_vel[w][k], s_mr[w][k], qp, qvel, lapm, part, acc);
           if (++since == 4) {
-            fold(acc, part);
+            fold<kShear>(acc, part);
             since = 0;
           }
         }
         __syncwarp();  // the chunk is consumed before the next one is staged
       }
     }
-    fold(acc, part);
+    fold<kShear>(acc, part);
     if (qv) finish_particle(c, a, (int)qi, acc, c.boxes[t.cg.sc]);
   }
 }

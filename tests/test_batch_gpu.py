@@ -135,10 +135,11 @@ def test_autotune_restores_state_and_keeps_fastest(gpu, horizon):
     tun = w.tuning()
     assert (tun["ctas_per_sm"], tun["queue"], tun["sort_block"], tun["comp_tile"]) == (
         best["ctas_per_sm"], best["queue"], best["sort_block"], best["comp_tile"])
-    # Stepping on from the restored state matches a world that never tuned.
+    # Stepping on from the restored state matches a world that never tuned (its first
+    # three steps at the default tile edge, like the tuned world's).
     ref = _batch_world(gpu, batch, graph_chunk=2)
-    ref.set_tuning(comp_tile=tun["comp_tile"])
     ref.step(DT, 3)
+    ref.set_tuning(comp_tile=tun["comp_tile"])
     w.step(DT, 4)
     ref.step(DT, 4)
     _assert_same(_state(w), _state(ref), "after tuning")
