@@ -258,7 +258,9 @@ int32_t phy_fluid_phase_times(PhyWorldHandle *w, uint32_t sub, double *out5, int
  *                         FP32-compensated passes (cells per tile edge);
  *   PHY_TUNE_HALO_CAP     staged particles per tile halo before a tile is
  *                         computed from global memory (default: the kernels'
- *                         capacity).
+ *                         capacity);
+ *   PHY_TUNE_DENSE_MEAN   mean particles per occupied cell above which a
+ *                         tile goes to the dense-cell passes (default 32).
  * Launch knobs (results never depend on them):
  *   PHY_TUNE_CTAS_PER_SM  resident CTAs per SM of the tiled passes'
  *                         persistent grids (0 = occupancy limit, default);
@@ -276,7 +278,8 @@ enum {
   PHY_TUNE_CTAS_PER_SM = 2,
   PHY_TUNE_QUEUE = 3,
   PHY_TUNE_SORT_BLOCK = 4,
-  PHY_TUNE_GRAPH_CHUNK = 5
+  PHY_TUNE_GRAPH_CHUNK = 5,
+  PHY_TUNE_DENSE_MEAN = 6
 };
 int32_t phy_fluid_set_tuning(PhyWorldHandle *w, uint32_t sub, int32_t param, int64_t value);
 int32_t phy_fluid_get_tuning(PhyWorldHandle *w, uint32_t sub, int32_t param, int64_t *out);

@@ -22,8 +22,10 @@ TUNE_CTAS_PER_SM = 2
 TUNE_QUEUE = 3
 TUNE_SORT_BLOCK = 4
 TUNE_GRAPH_CHUNK = 5
+TUNE_DENSE_MEAN = 6
 TUNE_PARAMS = {"comp_tile": TUNE_COMP_TILE, "halo_cap": TUNE_HALO_CAP, "ctas_per_sm": TUNE_CTAS_PER_SM,
-               "queue": TUNE_QUEUE, "sort_block": TUNE_SORT_BLOCK, "graph_chunk": TUNE_GRAPH_CHUNK}
+               "queue": TUNE_QUEUE, "sort_block": TUNE_SORT_BLOCK, "graph_chunk": TUNE_GRAPH_CHUNK,
+               "dense_mean": TUNE_DENSE_MEAN}
 
 NOALLOC_MAX_PARTICLES = 65536
 NOALLOC_MAX_CELLS = 262144

@@ -493,6 +493,9 @@ int32_t phy_fluid_set_tuning(PhyWorldHandle* w, uint32_t sub, int32_t param, int
       case PHY_TUNE_GRAPH_CHUNK:
         fw.set_graph_chunk(in_range(0, 1 << 20));
         break;
+      case PHY_TUNE_DENSE_MEAN:
+        fw.set_dense_mean(in_range(1, 1 << 20));
+        break;
       default:
         throw std::invalid_argument("unknown tuning parameter");
     }
@@ -512,6 +515,7 @@ int32_t phy_fluid_get_tuning(PhyWorldHandle* w, uint32_t sub, int32_t param, int
       case PHY_TUNE_QUEUE: *out = t.queue; break;
       case PHY_TUNE_SORT_BLOCK: *out = t.sort_block; break;
       case PHY_TUNE_GRAPH_CHUNK: *out = fw.graph_chunk(); break;
+      case PHY_TUNE_DENSE_MEAN: *out = fw.dense_mean(); break;
       default: throw std::invalid_argument("unknown tuning parameter");
     }
     return 0;

@@ -738,6 +738,7 @@ StepConsts FluidWorld::make_consts(double dt) const {
   c.tile = tile_;
   c.tile_log2 = tile_ == 4 ? 2 : (tile_ == 2 ? 1 : 0);
   c.halo_cap = halo_cap_;
+  c.dense_mean = dense_mean_;
   c.boxes = tile_ ? b_.boxes : nullptr;
   c.n_scenes = scenes_.empty() ? 1 : (int)scenes_.size();
   if (tile_) {

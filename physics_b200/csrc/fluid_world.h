@@ -191,6 +191,8 @@ class FluidWorld {
   // smaller values route more tiles through the global-memory path.
   void set_halo_cap(int v) { halo_cap_ = v < 0 ? 0 : v; }
   int halo_cap() const { return halo_cap_; }
+  void set_dense_mean(int v) { dense_mean_ = v < 1 ? 1 : v; }
+  int dense_mean() const { return dense_mean_; }
 
   // Device state access for in-library consumers (sorted order).
   DevBuffers& buffers() { return b_; }
@@ -235,6 +237,7 @@ class FluidWorld {
   bool counting_ = false;
   int comp_tile_ = 4;
   int halo_cap_ = 1 << 30;
+  int dense_mean_ = (int)kDenseMean;
   int tile_ = 0;  // linearisation of the current box (0 = x-major)
   bool timing_ = false;
   // One set of 5 events per timed step, recycled after phase_times reads them.

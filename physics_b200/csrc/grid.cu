@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(kThreads) k_tile_emit(int n, int ncells, const
                                                        const uint32_t* __restrict__ cell_start,
                                                        uint32_t* __restrict__ tile_slot,
                                                        uint8_t* __restrict__ tile_crowd, int tile_log2,
-                                                       uint32_t* __restrict__ num_tiles) {
+                                                       int dense_mean, uint32_t* __restrict__ num_tiles) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) {
     if (s == n) {
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(kThreads) k_tile_emit(int n, int ncells, const
     uint32_t occ = 0;
     for (uint32_t u = 0; u < ncell; ++u) occ += cell_start[c0 + u + 1] > cell_start[c0 + u] ? 1u : 0u;
     const uint32_t np = cell_start[c0 + ncell] - cell_start[c0];
-    tile_crowd[k] = np > kDenseMean * occ ? 1 : 0;
+    tile_crowd[k] = np > (uint32_t)dense_mean * occ ? 1 : 0;
   }
 }
 
@@ -528,7 +528,8 @@ void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s, int block) 
     k_scan_top<<<1, 1024, 0, s>>>(b.block_sums, hb);
     k_scan_apply<<<hb, kThreads, 0, s>>>(b.tile_head, b.block_sums);
     k_tile_emit<<<grid_for(n + 1, bs), bs, 0, s>>>(n, c.ncells, b.sorted_cell, b.tile_head, b.cell_start,
-                                                   b.tile_slot, b.tile_crowd, c.tile_log2, b.num_tiles);
+                                                   b.tile_slot, b.tile_crowd, c.tile_log2, c.dense_mean,
+                                                   b.num_tiles);
   }
 }
 

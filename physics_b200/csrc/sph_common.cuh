@@ -28,10 +28,11 @@ constexpr int kCodeBits = 5;
 // and written out coalesced; further entries go straight to global memory.
 constexpr int kStagedNeighbors = 40;
 
-// Tiled form: a tile whose occupied cells hold more than this many particles
-// on average goes to the dense-cell passes even when its halo could be
-// staged; from about this density on, neighbour lists overflow and a staged
-// tile would rescan its cells for every query.
+// Tiled form: by default a tile whose occupied cells hold more than this many
+// particles on average goes to the dense-cell passes even when its halo could
+// be staged (StepConsts::dense_mean, a tuning knob); from about this density
+// on, neighbour lists overflow and a staged tile would rescan its cells for
+// every query.
 constexpr uint32_t kDenseMean = 32;
 
 // Error bits written by device code into the per-world flag word.
@@ -81,6 +82,9 @@ struct StepConsts {
   // Tiles whose halo holds more particles than this are computed from
   // global memory instead of shared memory (<= the kernels' capacity).
   int halo_cap;
+  // Tiles whose occupied cells average more particles than this go to the
+  // dense-cell passes.
+  int dense_mean;
   // Tiled form: device table of the scene boxes (one entry for a single
   // world).  A particle's scene is its entry in ParticleConsts::scene (all 0
   // when that array is absent); ncells counts the cells of all boxes.

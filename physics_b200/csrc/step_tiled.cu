@@ -966,16 +966,24 @@ __global__ void __launch_bounds__(kWT, 5) k_density_dense(StepConsts c, TiledArg
 }
 
 // Forces, integration and bounds of the dense-cell particles: per chunk each
-// lane builds the mask of its in-range candidates (branch-free), then walks
-// its own mask through the pair terms of the tiled pass.
+// lane builds the mask of its in-range candidates (branch-free, candidates in
+// pairs on f32x2 arithmetic), then the warp walks the masks in lockstep for
+// as many rounds as the fullest mask has bits, each lane taking its own next
+// candidate through the pair terms of the tiled pass.  The partial sums are
+// folded into the compensated totals every 8 rounds and at the end of the
+// chunk, uniformly across the warp.
 template <int TB, bool kShear>
 __global__ void __launch_bounds__(kWT, 3) k_force_dense(StepConsts c, TiledArgs a) {
   __shared__ float4 s_pos[kWarps][32];
   __shared__ float4 s_vel[kWarps][32];
   __shared__ float s_mr[kWarps][32];
+  __shared__ __align__(16) float s_pp[kWarps][32 * 4];  // the chunk's positions, pair-interleaved
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  float* sp = s_pp[w];
+  const float4* sp4 = reinterpret_cast<const float4*>(sp);
   const uint32_t ntasks = *a.dense_count;
   const float hc2 = fminf(c.h2f, c.h0sqf);
+  const f2 HC2 = f2_pack(hc2, hc2);
   DenseTask t;
   while (next_task<TB>(c, a, a.dense_taken + 1, ntasks, t)) {
     const bool qv = (uint32_t)lane < t.qn;
@@ -985,9 +993,9 @@ __global__ void __launch_bounds__(kWT, 3) k_force_dense(StepConsts c, TiledArgs 
     const Box3 qb = warp_box(qp.x, qp.y, qp.z, qv);
     task_neighbours(c, a, t, qb, hc2);
     const float lapm = qp.w * c.lap_cf;
+    const f2 PX = f2_pack(qp.x, qp.x), PY = f2_pack(qp.y, qp.y), PZ = f2_pack(qp.z, qp.z);
     CompAcc acc;
     ForcePart part;
-    uint32_t since = 0;
     for (int nb = 0; nb < 27; ++nb) {
       const uint32_t s0 = __shfl_sync(0xffffffffu, t.nb_s, nb), e0 = __shfl_sync(0xffffffffu, t.nb_e, nb);
       if (s0 >= e0) continue;
@@ -1003,33 +1011,41 @@ __global__ void __launch_bounds__(kWT, 3) k_force_dense(StepConsts c, TiledArgs 
         p.y += off[1];
         p.z += off[2];
         s_pos[w][lane] = p;
+        put_pair_slot(sp, (uint32_t)lane, p);
         s_vel[w][lane] = cv ? a.cvel[j] : make_float4(0.f, 0.f, 0.f, 0.f);
         s_mr[w][lane] = cv ? a.cmr[j] : 0.f;
         __syncwarp();
-        const uint32_t m = min(32u, e0 - cb);
+        // In-range bits (r^2 < hc2; the sign of r^2 - hc2, which is never -0),
+        // shifted in so that the chunk's first candidate ends in the highest
+        // bit; slots past the chunk hold far dummies (bit 0).
         uint32_t mask = 0;
-#pragma unroll 8
-        for (uint32_t k = 0; k < 32u; ++k) {
-          if (k >= m) break;  // uniform
-          const float4 pj = s_pos[w][k];
-          const float dx = pj.x - qp.x, dy = pj.y - qp.y, dz = pj.z - qp.z;
-          const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-          mask |= (r2 < hc2 ? 1u : 0u) << k;
+#pragma unroll
+        for (uint32_t k = 0; k < 32u; k += 2) {
+          const float4 A = sp4[k];      // x0 x1 y0 y1
+          const float4 B = sp4[k + 1];  // z0 z1 m0 m1
+          const f2 DX = f2_sub(f2_pack(A.x, A.y), PX);
+          const f2 DY = f2_sub(f2_pack(A.z, A.w), PY);
+          const f2 DZ = f2_sub(f2_pack(B.x, B.y), PZ);
+          const f2 R2 = f2_fma(DZ, DZ, f2_fma(DY, DY, f2_mul(DX, DX)));
+          float d0, d1;
+          f2_unpack(f2_sub(R2, HC2), d0, d1);
+          mask = __funnelshift_l(__float_as_uint(d0), mask, 1);
+          mask = __funnelshift_l(__float_as_uint(d1), mask, 1);
         }
-        if (!qv) mask = 0;
-        while (mask) {
-          const int k = __ffs(mask) - 1;
-          mask &= mask - 1;
-          pair_listed<kShear>(c, s_pos[w][k], s_vel[w][k], s_mr[w][k], qp, qvel, lapm, part, acc);
-          if (++since == 4) {
-            fold<kShear>(acc, part);
-            since = 0;
+        mask = qv ? __brev(mask) : 0u;  // bit k = candidate k
+        const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(mask));
+        for (int r = 0; r < rounds; ++r) {
+          if (mask) {
+            const int k = __ffs(mask) - 1;
+            mask &= mask - 1;
+            pair_listed<kShear>(c, s_pos[w][k], s_vel[w][k], s_mr[w][k], qp, qvel, lapm, part, acc);
           }
+          if ((r & 7) == 7) fold<kShear>(acc, part);
         }
+        if (rounds & 7) fold<kShear>(acc, part);
         __syncwarp();  // the chunk is consumed before the next one is staged
       }
     }
-    fold<kShear>(acc, part);
     if (qv) finish_particle(c, a, (int)qi, acc, c.boxes[t.cg.sc]);
   }
 }
