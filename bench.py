@@ -276,14 +276,14 @@ def run_adjoint(pb, scenes, stream, directions: int) -> dict:
     n = pos.shape[0]
     mass = scenes.lattice_mass(scenes.SPACING)
 
-    def world(v, stiffness=None, visc=None):
+    def world(v, stiffness=None, visc=None, form="f64"):
         p = pb.SphParams.defaults()
         p.bounds_min, p.bounds_max = (0.0, 0.0, 0.0), (ADJ_BOX, ADJ_BOX, ADJ_BOX)
         if stiffness is not None:
             p.stiffness = stiffness
         if visc is not None:
             p.visc_k = [visc]
-        w = pb.FluidWorld(p, "f64")
+        w = pb.FluidWorld(p, form)
         w.set_stream(stream.cuda_stream)
         w.add_particles(pos, mass, vel=v)
         return w
@@ -333,6 +333,35 @@ def run_adjoint(pb, scenes, stream, directions: int) -> dict:
     fd_visc = (run_loss(v0, visc=3.5 + eps) - run_loss(v0, visc=3.5 - eps)) / (2 * eps)
     hk = 250.0 * eps
     fd_stiff = (run_loss(v0, stiffness=250.0 + hk) - run_loss(v0, stiffness=250.0 - hk)) / (2 * hk)
+
+    # The same on the FP32-compensated world (its adjoint differentiates the step along
+    # the compensated trajectory through f64 records of each state).
+    cw = world(v0, form="comp")
+    cw.step(ADJ_DT, 10)
+    cw = world(v0, form="comp")
+    cfwd_ms, _ = timed(lambda: cw.step(ADJ_DT, ADJ_STEPS))
+    cw = world(v0, form="comp")
+    cw.tape_begin(ADJ_EVERY)
+    cw.step(ADJ_DT, ADJ_STEPS)
+    cxT = cw.pos
+    cgx = 2.0 * (cxT - target) / n
+    cw.step_backward(cgx, None)
+    cbwd_ms, cg = timed(lambda: cw.step_backward(cgx, None))
+    del cw
+
+    def run_closs(v):
+        q = world(v, form="comp")
+        q.step(ADJ_DT, ADJ_STEPS)
+        return loss(q.pos)
+
+    cerrs = []
+    for _ in range(min(directions, 8)):
+        d = rng.normal(size=v0.shape)
+        d /= np.linalg.norm(d)
+        fd = (run_closs(v0 + eps * d) - run_closs(v0 - eps * d)) / (2 * eps)
+        cerrs.append(abs(float(np.sum(cg["vel"] * d)) - fd) / abs(fd))
+    comp = {"forward_ms": cfwd_ms, "backward_ms": cbwd_ms, "backward_over_forward": cbwd_ms / cfwd_ms,
+            "fd_directions": len(cerrs), "fd_max_rel_err": max(cerrs), "fd_median_rel_err": float(np.median(cerrs))}
     return {
         "workload": f"dam_break_{ADJ_DIMS[0]}x{ADJ_DIMS[1]}x{ADJ_DIMS[2]}: {n} particles, {ADJ_STEPS} steps at "
                     f"dt={ADJ_DT}, checkpoint every {ADJ_EVERY}; loss = mean |x_T - target|^2",
@@ -352,6 +381,7 @@ def run_adjoint(pb, scenes, stream, directions: int) -> dict:
         "grad_stiffness": g["stiffness"],
         "fd_stiffness_rel_err": abs(g["stiffness"] - fd_stiff) / abs(fd_stiff),
         "fd_stiffness_step": hk,
+        "comp": comp,
     }
 
 

@@ -332,7 +332,8 @@ int32_t phy_fluid_autotune(PhyWorldHandle *w, uint32_t sub, double dt, uint32_t 
 int32_t phy_fluid_autotune_horizon(PhyWorldHandle *w, uint32_t sub, double dt, uint32_t steps, uint32_t horizon,
                                    PhyTuneTrial *out, uint32_t cap, uint32_t *n_out);
 
-/* Adjoint of the f64 plain step (PHY_PRECISION_F64_PLAIN worlds only).
+/* Adjoint of the SPH step, f64 plain worlds and FP32-compensated worlds on
+ * the tiled passes (the default; the x-major route is rejected).
  * phy_fluid_tape_begin makes the current state checkpoint 0 and records every
  * following phy_fluid_step of `sub` (its dt), saving a state checkpoint every
  * `checkpoint_every` steps; parameters must stay unchanged and body
@@ -343,10 +344,13 @@ int32_t phy_fluid_autotune_horizon(PhyWorldHandle *w, uint32_t sub, double dt, u
  * interleaved; NULL = zero) it writes dL/dpos_0, dL/dvel_0 (3n each) and
  * grad_params2 = {dL/d stiffness, dL/d visc_k[0]} (any output may be NULL).
  * Neighbour sets and branches (walls, max(0, .), shear_min) are held as the
- * forward took them.  The world is left in its recorded end state and the
- * tape is kept for further sweeps until phy_fluid_tape_clear or the next
- * phy_fluid_tape_begin.  The reference has no adjoint; these calls replace
- * nothing in phy_ffi.h. */
+ * forward took them.  A compensated world is differentiated along its own
+ * trajectory: each re-run step first takes an f64 plain recording step from
+ * the compensated state, so the sweep is the exact adjoint of the step map at
+ * the states the compensated forward visited.  The world is left in its
+ * recorded end state and the tape is kept for further sweeps until
+ * phy_fluid_tape_clear or the next phy_fluid_tape_begin.  The reference has
+ * no adjoint; these calls replace nothing in phy_ffi.h. */
 int32_t phy_fluid_tape_begin(PhyWorldHandle *w, uint32_t sub, uint32_t checkpoint_every);
 int32_t phy_fluid_tape_clear(PhyWorldHandle *w, uint32_t sub);
 uint32_t phy_fluid_tape_steps(PhyWorldHandle *w, uint32_t sub);

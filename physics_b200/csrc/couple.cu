@@ -20,6 +20,9 @@
 // updates are disjoint).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "sph_buffers.h"
 
 namespace phy {
@@ -158,147 +161,209 @@ __global__ void __launch_bounds__(kCT) k_couple_points(StepConsts c, CoupleArgs 
 }
 
 // Pipelined form of the same walk.  Only velocities change from one point to
-// the next, so while thread 0 runs point k's ordered sums, warps 1..7 build
-// point k+1's cell table, its candidates' particle indices, masses and
-// velocities and the products v_j m_j (double-buffered in shared memory).
-// Point k's reaction can change only the velocities of particles in point
-// k's own 27 cells, so after it those of point k+1's cells that are also
-// point k's are gathered again (points far apart share none).  The ordered
-// sums then read ready products (sx + v m with the product formed once, the
-// same f64 operations), and the reaction reuses the gathered velocities
-// (v_j + share).  Points with more than kPB candidates take a chunked walk.
-constexpr int kPB = 1024;  // candidates prefetched per point
+// the next, so everything else is prepared in parallel first: one warp per
+// point finds its 27 cell ranges (k_point_tables), and, after a prefix sum of
+// the candidate counts, writes its candidates' particle indices and masses
+// in visit order (k_point_candidates).  The ordered walk (one CTA) then reads
+// those lists two points ahead: while thread 0 runs point k's ordered f64
+// sums, warps 1..7 gather point k+1's velocities and the products v_j m_j
+// into shared memory and load point k+2's list.  Point k's reaction can
+// change only the velocities of particles in point k's own cells, so after
+// it the candidates of point k+1 in cells that point k shares are gathered
+// again (points far apart share none).  The ordered sums read ready products
+// (sx + v m with the product formed once: the same f64 operations), and the
+// reaction reuses the gathered velocities (v_j + share).  Points with more
+// than kPB candidates take a chunked walk through their cells.
+constexpr int kPB = 1024;   // candidates a point may have for the pipelined walk
+constexpr int kTabU = 56;   // u32 per point table: in, total, beg[27], cnt[27]
 
 struct PointTable {
   uint32_t beg[27];
+  uint32_t cnt[27];
   uint32_t pre[28];
-  uint32_t again;  // bit u: cell u is also a cell of the previous point (gather again after its reaction)
+  uint32_t again;  // bit u: cell u is also a cell of the previous point
   int in;
+  __device__ bool fits() const { return in && pre[27] <= (uint32_t)kPB; }
 };
 
-// Cell table of point k (one warp).
-__device__ __forceinline__ void point_table(const StepConsts& c, const CoupleArgs& a, int k, PointTable& T) {
-  const int lane = threadIdx.x & 31;
-  const double* q = a.pts + 10 * (size_t)k;
+// One warp per point: in-bounds flag, candidate count and cell ranges.
+__global__ void __launch_bounds__(256) k_point_tables(StepConsts c, CoupleArgs a, int p0, int nb, uint32_t* tab,
+                                                      uint32_t* totals) {
+  const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (w >= nb) return;
+  const double* q = a.pts + 10 * (size_t)(p0 + w);
   const double x = q[0], y = q[1], z = q[2];
   // world.rs:704-711 (a NaN coordinate passes, as there).
   const bool in = !(x < c.lo[0] || x > c.hi[0] || y < c.lo[1] || y > c.hi[1] || z < c.lo[2] || z > c.hi[2]);
-  if (lane == 0) T.in = in ? 1 : 0;
-  if (in) {
+  uint32_t beg = 0, cnt = 0;
+  if (in && lane < 27) {
     const long long kx = key_axis(x, c.inv_cell), ky = key_axis(y, c.inv_cell), kz = key_axis(z, c.inv_cell);
-    uint32_t beg = 0, cnt = 0;
-    if (lane < 27) {
-      const int lin = cell_linear(c, kx + lane / 9 - 1, ky + (lane / 3) % 3 - 1, kz + lane % 3 - 1);
-      if (lin >= 0) {
-        beg = a.cell_start[lin];
-        cnt = a.cell_start[lin + 1] - beg;
-      }
+    const int lin = cell_linear(c, kx + lane / 9 - 1, ky + (lane / 3) % 3 - 1, kz + lane % 3 - 1);
+    if (lin >= 0) {
+      beg = a.cell_start[lin];
+      cnt = a.cell_start[lin + 1] - beg;
     }
-    uint32_t incl = cnt;
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += v;
-    }
-    if (lane < 27) {
-      T.beg[lane] = beg;
-      T.pre[lane] = incl - cnt;
-    }
-    if (lane == 26) T.pre[27] = incl;
   }
-  __syncwarp();
+  const uint32_t total = __reduce_add_sync(0xffffffffu, cnt);
+  uint32_t* t = tab + (size_t)w * kTabU;
+  if (lane < 27) {
+    t[2 + lane] = beg;
+    t[29 + lane] = cnt;
+  }
+  if (lane == 0) {
+    t[0] = in ? 1u : 0u;
+    t[1] = total;
+    totals[w] = in && total <= (uint32_t)kPB ? total : 0u;
+  }
 }
 
-// Staged candidate data of one point: particle index, mass, velocity, and
-// the products (v m) in the order the ordered sums read them.
+// One warp per point: the candidates of a point that fits, in visit order
+// (cell after cell, ascending slot: ascending insertion index), from off[w].
+__global__ void __launch_bounds__(256) k_point_candidates(CoupleArgs a, int nb, const uint32_t* tab,
+                                                          const uint32_t* off, uint32_t* idx, double* m) {
+  const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (w >= nb) return;
+  const uint32_t* t = tab + (size_t)w * kTabU;
+  if (!t[0] || t[1] > (uint32_t)kPB) return;
+  uint32_t o = off[w];
+  for (int u = 0; u < 27; ++u) {
+    const uint32_t beg = t[2 + u], cnt = t[29 + u];
+    for (uint32_t e = lane; e < cnt; e += 32) {
+      const uint32_t i = a.perm[beg + e];
+      idx[o + e] = i;
+      m[o + e] = a.mass[i];
+    }
+    o += cnt;
+  }
+}
+
+struct PointLists {
+  const uint32_t* tab;
+  const uint32_t* off;
+  const uint32_t* idx;
+  const double* m;
+};
+
+// Staged data of one point: particle indices and masses (three buffers),
+// velocities and products (two buffers).
 struct PointBuf {
   uint32_t* idx;  // [kPB]
   double* m;      // [kPB]
-  double* v;      // [3][kPB]
-  double2* pw;    // [2 kPB]: (v_x m, v_y m), (v_z m, m) per candidate
+};
+struct VelBuf {
+  double* v;    // [3][kPB]
+  double2* pw;  // [2 kPB]: (v_x m, v_y m), (v_z m, m) per candidate
 };
 
-// Buffer q (0 or 1) of the pipelined kernel's dynamic shared memory.
 __device__ __forceinline__ PointBuf point_buf(unsigned char* smem, int q) {
-  double2* pw = reinterpret_cast<double2*>(smem);             // [2][2 kPB]
-  double* v = reinterpret_cast<double*>(pw + 4 * kPB);         // [2][3][kPB]
-  double* m = v + 6 * kPB;                                     // [2][kPB]
-  uint32_t* idx = reinterpret_cast<uint32_t*>(m + 2 * kPB);    // [2][kPB]
-  return {idx + q * kPB, m + q * kPB, v + 3 * q * kPB, pw + 2 * q * kPB};
+  double* m = reinterpret_cast<double*>(smem);                     // [3][kPB]
+  uint32_t* idx = reinterpret_cast<uint32_t*>(m + 3 * kPB);        // [3][kPB]
+  return {idx + q * kPB, m + q * kPB};
+}
+__device__ __forceinline__ VelBuf vel_buf(unsigned char* smem, int q) {
+  double* v = reinterpret_cast<double*>(smem) + 3 * kPB + 3 * kPB / 2;  // after m and idx (16-byte aligned)
+  double2* pw = reinterpret_cast<double2*>(v + 6 * kPB);               // [2][2 kPB]
+  return {v + 3 * q * kPB, pw + 2 * q * kPB};
 }
 
-__device__ __forceinline__ void gather_candidate(const CoupleArgs& a, const PointBuf& B, uint32_t e) {
+// Threads t0.. (stride nt): table and list of point j into slot q.
+__device__ __forceinline__ void load_point(const PointLists& L, int j, PointTable& T, const PointBuf& B, int t0,
+                                           int nt) {
+  const uint32_t* t = L.tab + (size_t)j * kTabU;
+  const int t1 = (int)threadIdx.x - t0;
+  if (t1 == 0) {
+    T.in = (int)t[0];
+    uint32_t p = 0;
+    for (int u = 0; u < 27; ++u) {
+      T.beg[u] = t[2 + u];
+      T.cnt[u] = t[29 + u];
+      T.pre[u] = p;
+      p += T.cnt[u];
+    }
+    T.pre[27] = p;
+  }
+  if (t[0] && t[1] <= (uint32_t)kPB) {
+    const uint32_t o = L.off[j], total = t[1];
+    for (uint32_t e = (uint32_t)t1; e < total; e += (uint32_t)nt) {
+      B.idx[e] = L.idx[o + e];
+      B.m[e] = L.m[o + e];
+    }
+  }
+}
+
+__device__ __forceinline__ void gather_candidate(const CoupleArgs& a, const PointBuf& B, const VelBuf& V,
+                                                 uint32_t e) {
   const uint32_t i = B.idx[e];
   const double m = B.m[e];
   const double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i];
-  B.v[e] = vx;
-  B.v[kPB + e] = vy;
-  B.v[2 * kPB + e] = vz;
-  B.pw[2 * e] = make_double2(vx * m, vy * m);
-  B.pw[2 * e + 1] = make_double2(vz * m, m);
+  V.v[e] = vx;
+  V.v[kPB + e] = vy;
+  V.v[2 * kPB + e] = vz;
+  V.pw[2 * e] = make_double2(vx * m, vy * m);
+  V.pw[2 * e + 1] = make_double2(vz * m, m);
 }
 
-// Warps 1..7: the table of point k and, when it fits, its candidates'
-// indices, masses, velocities and products.  `prev` is the table of point
-// k-1 when its reaction has not run yet (its cells are flagged in `again`),
-// else null.
-__device__ __forceinline__ void prefetch_point(const StepConsts& c, const CoupleArgs& a, int k, PointTable& T,
-                                               const PointTable* prev, const PointBuf& B) {
+// Warps 1..7: velocities of point j (its list already staged) and, when
+// `prev` (the previous point, reaction not yet applied) is given, the cells
+// the two share.
+__device__ __forceinline__ void gather_point(const CoupleArgs& a, PointTable& T, const PointTable* prev,
+                                             const PointBuf& B, const VelBuf& V) {
   if ((threadIdx.x >> 5) == 1) {
-    point_table(c, a, k, T);
     const int lane = threadIdx.x & 31;
     bool shared = false;
-    if (T.in && prev && prev->in && lane < 27 && T.pre[lane + 1] > T.pre[lane])
-      for (int u = 0; u < 27; ++u)
-        shared = shared || (prev->pre[u + 1] > prev->pre[u] && prev->beg[u] == T.beg[lane]);
+    if (prev && prev->in && lane < 27 && T.cnt[lane] > 0)
+      for (int u = 0; u < 27; ++u) shared = shared || (prev->cnt[u] > 0 && prev->beg[u] == T.beg[lane]);
     const uint32_t bits = __ballot_sync(0xffffffffu, shared);
     if (lane == 0) T.again = bits;
   }
-  asm volatile("bar.sync 1, %0;" ::"r"(kCT - 32));
-  if (!T.in) return;
-  const uint32_t total = T.pre[27];
-  if (total > (uint32_t)kPB) return;
-  for (uint32_t e = threadIdx.x - 32; e < total; e += kCT - 32) {
-    const uint32_t i = candidate(a, T.beg, T.pre, e);
-    B.idx[e] = i;
-    B.m[e] = a.mass[i];
-    gather_candidate(a, B, e);
-  }
+  for (uint32_t e = threadIdx.x - 32; e < T.pre[27]; e += kCT - 32) gather_candidate(a, B, V, e);
 }
 
-__global__ void __launch_bounds__(kCT) k_couple_points_piped(StepConsts c, CoupleArgs a) {
-  __shared__ PointTable s_tab[2];
+__global__ void __launch_bounds__(kCT) k_couple_points_piped(StepConsts c, CoupleArgs a, int p0, int nb,
+                                                             PointLists L) {
+  __shared__ PointTable s_tab[3];
   __shared__ double s_r[4];  // reaction xyz, sum of masses
   extern __shared__ __align__(16) unsigned char smem[];
   const int t = threadIdx.x, warp = t >> 5;
-  if (warp >= 1 && a.np > 0) prefetch_point(c, a, 0, s_tab[0], nullptr, point_buf(smem, 0));
+  // Prologue: lists of points 0 and 1, velocities of point 0.
+  if (nb > 0) load_point(L, 0, s_tab[0], point_buf(smem, 0), 0, kCT);
+  if (nb > 1) load_point(L, 1, s_tab[1], point_buf(smem, 1), 0, kCT);
   __syncthreads();
-  for (int k = 0; k < a.np; ++k) {
-    const int cur = k & 1, nxt = cur ^ 1;
-    const PointTable& T = s_tab[cur];
-    const PointBuf B = point_buf(smem, cur);
-    double* q = a.pts + 10 * (size_t)k;
-    const bool more = k + 1 < a.np;
+  if (nb > 0 && s_tab[0].fits()) {
+    if (t == 32) s_tab[0].again = 0;
+    if (warp >= 1)
+      for (uint32_t e = t - 32; e < s_tab[0].pre[27]; e += kCT - 32)
+        gather_candidate(a, point_buf(smem, 0), vel_buf(smem, 0), e);
+  }
+  __syncthreads();
+  for (int j = 0; j < nb; ++j) {
+    const int r3 = j % 3, n3 = (j + 1) % 3, f3 = (j + 2) % 3, r2 = j & 1, n2 = r2 ^ 1;
+    const PointTable& T = s_tab[r3];
+    const PointBuf B = point_buf(smem, r3);
+    const VelBuf V = vel_buf(smem, r2);
+    double* q = a.pts + 10 * (size_t)(p0 + j);
+    const bool has1 = j + 1 < nb, has2 = j + 2 < nb;
     const uint32_t total = T.in ? T.pre[27] : 0u;
-    if (!T.in || total > (uint32_t)kPB) {
+    if (!T.fits()) {
       if (T.in) {
-        // Chunked walk: candidates staged kPB at a time in this point's buffer.
+        // Chunked walk through the cells: candidates staged kPB at a time.
         double sx = 0.0, sy = 0.0, sz = 0.0, sw = 0.0;
         for (uint32_t base = 0; base < total; base += kPB) {
           const uint32_t cnt = min((uint32_t)kPB, total - base);
           for (uint32_t e = t; e < cnt; e += kCT) {
             const uint32_t i = candidate(a, T.beg, T.pre, base + e);
-            B.v[e] = a.vx[i];
-            B.v[kPB + e] = a.vy[i];
-            B.v[2 * kPB + e] = a.vz[i];
+            V.v[e] = a.vx[i];
+            V.v[kPB + e] = a.vy[i];
+            V.v[2 * kPB + e] = a.vz[i];
             B.m[e] = a.mass[i];
           }
           __syncthreads();
           if (t == 0)
             for (uint32_t e = 0; e < cnt; ++e) {
               const double w = B.m[e];
-              sx = sx + B.v[e] * w;
-              sy = sy + B.v[kPB + e] * w;
-              sz = sz + B.v[2 * kPB + e] * w;
+              sx = sx + V.v[e] * w;
+              sy = sy + V.v[kPB + e] * w;
+              sz = sz + V.v[2 * kPB + e] * w;
               sw = sw + w;
             }
           __syncthreads();
@@ -316,23 +381,27 @@ __global__ void __launch_bounds__(kCT) k_couple_points_piped(StepConsts c, Coupl
           }
       }
       __syncthreads();
-      // Point k's velocities are final: the next point needs no second gather.
-      if (warp >= 1 && more) prefetch_point(c, a, k + 1, s_tab[nxt], nullptr, point_buf(smem, nxt));
+      // Point j's reaction is applied: point j+1's velocities are final.
+      if (warp >= 1) {
+        if (has1 && s_tab[n3].fits()) gather_point(a, s_tab[n3], nullptr, point_buf(smem, n3), vel_buf(smem, n2));
+        if (has2) load_point(L, j + 2, s_tab[f3], point_buf(smem, f3), 32, kCT - 32);
+      }
       __syncthreads();
       continue;
     }
     if (t == 0) {
       double sx = 0.0, sy = 0.0, sz = 0.0, sw = 0.0;
       for (uint32_t e = 0; e < total; ++e) {
-        const double2 p = B.pw[2 * e], r = B.pw[2 * e + 1];
+        const double2 p = V.pw[2 * e], r = V.pw[2 * e + 1];
         sx = sx + p.x;
         sy = sy + p.y;
         sz = sz + r.x;
         sw = sw + r.y;
       }
       point_force(c, a, q, sx, sy, sz, sw, s_r);
-    } else if (warp >= 1 && more) {
-      prefetch_point(c, a, k + 1, s_tab[nxt], &T, point_buf(smem, nxt));
+    } else if (warp >= 1) {
+      if (has1 && s_tab[n3].fits()) gather_point(a, s_tab[n3], &T, point_buf(smem, n3), vel_buf(smem, n2));
+      if (has2) load_point(L, j + 2, s_tab[f3], point_buf(smem, f3), 32, kCT - 32);
     }
     __syncthreads();
     const double msum = s_r[3];
@@ -340,25 +409,26 @@ __global__ void __launch_bounds__(kCT) k_couple_points_piped(StepConsts c, Coupl
       for (uint32_t e = t; e < total; e += kCT) {
         const uint32_t i = B.idx[e];
         const double frac = B.m[e] / msum;
-        a.vx[i] = B.v[e] + s_r[0] * frac;
-        a.vy[i] = B.v[kPB + e] + s_r[1] * frac;
-        a.vz[i] = B.v[2 * kPB + e] + s_r[2] * frac;
+        a.vx[i] = V.v[e] + s_r[0] * frac;
+        a.vy[i] = V.v[kPB + e] + s_r[1] * frac;
+        a.vz[i] = V.v[2 * kPB + e] + s_r[2] * frac;
       }
     __syncthreads();
     // The next point's candidates in cells this point shares took its
     // reaction: gather them again.
-    if (more && s_tab[nxt].in && s_tab[nxt].pre[27] <= (uint32_t)kPB && s_tab[nxt].again) {
-      const PointTable& N = s_tab[nxt];
-      const PointBuf NB = point_buf(smem, nxt);
+    if (has1 && s_tab[n3].fits() && s_tab[n3].again) {
+      const PointTable& N = s_tab[n3];
+      const PointBuf NB = point_buf(smem, n3);
+      const VelBuf NV = vel_buf(smem, n2);
       for (int u = 0; u < 27; ++u)
         if (N.again >> u & 1u)
-          for (uint32_t e = N.pre[u] + t; e < N.pre[u + 1]; e += kCT) gather_candidate(a, NB, e);
+          for (uint32_t e = N.pre[u] + t; e < N.pre[u + 1]; e += kCT) gather_candidate(a, NB, NV, e);
       __syncthreads();
     }
   }
 }
 
-constexpr size_t kPipedSmem = (size_t)kPB * (4 * 16 + 2 * 3 * 8 + 2 * 8 + 2 * 4);
+constexpr size_t kPipedSmem = (size_t)kPB * (3 * 8 + 3 * 4 + 2 * 3 * 8 + 2 * 2 * 16);
 
 // ---- couple_heat (world.rs:555-678) ------------------------------------------------
 //
@@ -987,8 +1057,35 @@ void launch_couple_heat(const StepConsts& c, DevBuffers& b, const HeatGrid& g, u
   k_heat_deposit<<<blocks, kCT, 0, s>>>(kin, iin, val, n, none, src);
 }
 
+namespace {
+
+// Grows a device array to hold `count` elements (contents dropped).
+template <class T>
+void scratch_grow(T*& p, size_t& cap, size_t count, cudaStream_t s) {
+  if (count <= cap && p) return;
+  if (p) {
+    cuda_check(cudaStreamSynchronize(s), "couple scratch sync");
+    cudaFree(p);
+    p = nullptr;
+  }
+  cap = std::max<size_t>(count, 1);
+  cuda_check(cudaMalloc((void**)&p, cap * sizeof(T)), "cudaMalloc");
+}
+
+}  // namespace
+
+void CouplePointsScratch::release() {
+  for (uint32_t** p : {&tab, &totals, &off, &idx}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  if (m) cudaFree(m);
+  m = nullptr;
+  cap_tab = cap_totals = cap_off = cap_idx = cap_m = 0;
+}
+
 void launch_couple_points(const StepConsts& c, DevBuffers& b, double* d_pts, int np, double dt, double drag,
-                          double soft_density, cudaStream_t s) {
+                          double soft_density, cudaStream_t s, CouplePointsScratch& sc) {
   CoupleArgs a;
   a.cell_start = b.cell_start;
   a.perm = b.perm;
@@ -1005,10 +1102,46 @@ void launch_couple_points(const StepConsts& c, DevBuffers& b, double* d_pts, int
     return cudaFuncSetAttribute(k_couple_points_piped, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)kPipedSmem) == cudaSuccess;
   }();
-  if (smem_ok)
-    k_couple_points_piped<<<1, kCT, kPipedSmem, s>>>(c, a);
-  else
+  if (!smem_ok) {
     k_couple_points<<<1, kCT, 0, s>>>(c, a);
+    return;
+  }
+  // Points run in batches (one ordered walk per batch, in order on the
+  // stream), which bounds the candidate lists.
+  constexpr int kBatch = 65536;
+  std::vector<uint32_t> totals, off;
+  for (int p0 = 0; p0 < np; p0 += kBatch) {
+    const int nb = std::min(kBatch, np - p0);
+    CoupleArgs ab = a;
+    ab.pts = d_pts + 10 * (size_t)p0;
+    scratch_grow(sc.tab, sc.cap_tab, (size_t)nb * kTabU, s);
+    scratch_grow(sc.totals, sc.cap_totals, (size_t)nb, s);
+    const int warps_per_block = 256 / 32, blocks = (nb + warps_per_block - 1) / warps_per_block;
+    k_point_tables<<<blocks, 256, 0, s>>>(c, ab, 0, nb, sc.tab, sc.totals);
+    cuda_check(cudaGetLastError(), "point tables");
+    totals.resize(nb);
+    cuda_check(cudaMemcpyAsync(totals.data(), sc.totals, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
+               "point totals");
+    cuda_check(cudaStreamSynchronize(s), "point totals sync");
+    off.resize(nb + 1);
+    uint64_t sum = 0;
+    for (int k = 0; k < nb; ++k) {
+      off[k] = (uint32_t)sum;
+      sum += totals[k];
+    }
+    off[nb] = (uint32_t)sum;  // at most kBatch * kPB candidates: fits 32 bits
+    scratch_grow(sc.off, sc.cap_off, (size_t)nb + 1, s);
+    scratch_grow(sc.idx, sc.cap_idx, (size_t)sum, s);
+    scratch_grow(sc.m, sc.cap_m, (size_t)sum, s);
+    cuda_check(cudaMemcpyAsync(sc.off, off.data(), (nb + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s),
+               "point offsets");
+    k_point_candidates<<<blocks, 256, 0, s>>>(ab, nb, sc.tab, sc.off, sc.idx, sc.m);
+    PointLists L{sc.tab, sc.off, sc.idx, sc.m};
+    k_couple_points_piped<<<1, kCT, kPipedSmem, s>>>(c, ab, 0, nb, L);
+    cuda_check(cudaGetLastError(), "couple points");
+    // The offsets' host copy must outlive the upload.
+    cuda_check(cudaStreamSynchronize(s), "couple points sync");
+  }
 }
 
 }  // namespace phy

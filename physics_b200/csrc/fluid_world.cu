@@ -350,6 +350,7 @@ FluidWorld::~FluidWorld() {
   free_all();
   dfree(d_bbox_);
   dfree(d_couple_);
+  couple_scratch_.release();
   dfree(d_heat_);
   dfree(d_bodies_);
   dfree(d_pbase_);
@@ -1534,7 +1535,7 @@ void FluidWorld::couple_points(size_t np, const double* pos, const double* vel, 
   const size_t bytes = h.size() * sizeof(double);
   cuda_check(cudaMemcpyAsync(d_couple_, h.data(), bytes, cudaMemcpyHostToDevice, stream_), "couple upload");
   launch_cell_index(c, b_, reinterpret_cast<uint32_t*>(d_couple_ + 10 * np), stream_);
-  launch_couple_points(c, b_, d_couple_, (int)np, dt, drag, soft_density, stream_);
+  launch_couple_points(c, b_, d_couple_, (int)np, dt, drag, soft_density, stream_, couple_scratch_);
   cuda_check(cudaGetLastError(), "couple launch");
   cuda_check(cudaMemcpyAsync(h.data(), d_couple_, bytes, cudaMemcpyDeviceToHost, stream_), "couple download");
   cuda_check(cudaStreamSynchronize(stream_), "couple sync");
@@ -1733,7 +1734,8 @@ void FluidWorld::tape_clear() {
 }
 
 void FluidWorld::tape_begin(int every) {
-  if (prec_ != Precision::F64Plain) throw std::invalid_argument("tape_begin: the adjoint is of the f64 plain form");
+  if (prec_ == Precision::F32Comp && comp_tile_ == 0)
+    throw std::invalid_argument("tape_begin: the compensated form's adjoint needs the tiled passes");
   if (!scenes_.empty()) throw std::invalid_argument("tape_begin: batched scenes are not recorded");
   if (b_.has_ba) throw std::invalid_argument("tape_begin: body accelerations are not recorded");
   if (every < 1) throw std::invalid_argument("tape_begin: checkpoint interval must be >= 1");
@@ -1832,10 +1834,17 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
     adj_slot_u_.resize(nslots, nullptr);
     adj_slot_ucount_.resize(nslots, 0);
   }
+  // A compensated world is differentiated along its own trajectory: each
+  // re-run step first takes an f64 plain recording step from the same state
+  // (the records of the exact step map at that state), then returns to the
+  // state and takes the compensated step to the next one.
+  const Precision form = prec_;
+  const bool comp = form == Precision::F32Comp;
   auto cleanup = [&]() {
     for (int k = 0; k < 3; ++k) b_.tape_fv[k] = nullptr;
     b_.tape_shear = nullptr;
     recomputing_ = false;
+    prec_ = form;
   };
   try {
     snapshot(false);  // the world returns to x_T, v_T afterwards
@@ -1866,6 +1875,11 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
       for (int t = t0; t < t1; ++t) {
         TapeSlot& sl = slots[t - t0];
         const int si = t - t0;
+        if (comp) {
+          snapshot(false, 1);  // the compensated state of step t
+          prec_ = Precision::F64Plain;
+          ensure_mode_buffers();  // f64 neighbour lists, kept for later sweeps
+        }
         const StepConsts c = step_impl(tape_.dts[t]);
         const size_t ncs = (size_t)c.ncells + 2;
         const size_t ucount = (3 + (size_t)kMaxNeighbors) * n + ncs;
@@ -1912,6 +1926,12 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
         cuda_check(cudaMemcpyAsync(const_cast<uint32_t*>(v.cell_start), b_.cell_start, ncs * 4,
                                    cudaMemcpyDeviceToDevice, s),
                    "tape copy");
+        if (comp) {
+          // The records are copied (stream order) before the state returns.
+          prec_ = Precision::F32Comp;
+          snapshot(true, 1);
+          step_impl(tape_.dts[t]);
+        }
       }
       for (int t = t1 - 1; t >= t0; --t) launch_adjoint_step(slots[t - t0].c, slots[t - t0].view(n), w, s);
       cuda_check(cudaGetLastError(), "adjoint step");

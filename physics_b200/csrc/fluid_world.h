@@ -249,6 +249,7 @@ class FluidWorld {
   long long* d_bbox_ = nullptr;  // 7 values: min xyz, max xyz, non-finite flag
   // Point records of couple_points (10 doubles each) plus one word of flags.
   double* d_couple_ = nullptr;
+  CouplePointsScratch couple_scratch_;
   size_t couple_cap_ = 0;
   // Scratch arena of couple_heat (grid, sources, sort keys).
   unsigned char* d_heat_ = nullptr;

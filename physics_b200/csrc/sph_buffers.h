@@ -100,8 +100,23 @@ void launch_cell_index(const StepConsts& c, DevBuffers& b, uint32_t* flags, cuda
 // couple.cu: FluidWorld::couple_points over np points (10 doubles each on the
 // device: pos xyz, vel xyz, mass, force xyz) after launch_cell_index; updates
 // the fluid velocities in pv1 and the forces of the points inside the bounds.
+// Throws CudaError with `what` and the CUDA message unless e is cudaSuccess
+// (fluid_world.cu).
+void cuda_check(cudaError_t e, const char* what);
+
+// Scratch of couple_points (owned by the world, grown on demand): per-point
+// cell tables, candidate counts and offsets, candidate indices and masses.
+struct CouplePointsScratch {
+  uint32_t* tab = nullptr;
+  uint32_t* totals = nullptr;
+  uint32_t* off = nullptr;
+  uint32_t* idx = nullptr;
+  double* m = nullptr;
+  size_t cap_tab = 0, cap_totals = 0, cap_off = 0, cap_idx = 0, cap_m = 0;
+  void release();
+};
 void launch_couple_points(const StepConsts& c, DevBuffers& b, double* d_pts, int np, double dt, double drag,
-                          double soft_density, cudaStream_t s);
+                          double soft_density, cudaStream_t s, CouplePointsScratch& scratch);
 
 // couple.cu: FluidWorld::couple_heat against a heat grid of nx*ny*nz cells
 // (x fastest), origin and cell size.  The scratch arena (size from

@@ -113,6 +113,11 @@ __device__ __forceinline__ f2 f2_sub(f2 a, f2 b) {
   asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
   return r;
 }
+__device__ __forceinline__ f2 f2_add(f2 a, f2 b) {
+  f2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
 __device__ __forceinline__ f2 f2_mul(f2 a, f2 b) {
   f2 r;
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
@@ -645,6 +650,98 @@ __device__ __forceinline__ void pair_listed(const StepConsts& c, float4 pj, floa
   }
 }
 
+// Two listed neighbours of one query at once on packed f32x2 arithmetic
+// (the terms of pair_listed without the shear sum).  A candidate given with
+// mass 0 and m/rho 0 adds exactly nothing, which pads a lane's odd last pair.
+struct QueryPack {
+  f2 px, py, pz, pw, vx, vy, vz, vw, lapm, h0, h0sq, spk, p6;
+};
+struct ForcePart2 {
+  f2 fx, fy, fz, vx, vy, vz, xx, xy, xz;
+};
+
+__device__ __forceinline__ QueryPack query_pack(const StepConsts& c, float4 pi, float4 vi, float lapm) {
+  QueryPack q;
+  q.px = f2_pack(pi.x, pi.x);
+  q.py = f2_pack(pi.y, pi.y);
+  q.pz = f2_pack(pi.z, pi.z);
+  q.pw = f2_pack(pi.w, pi.w);
+  q.vx = f2_pack(vi.x, vi.x);
+  q.vy = f2_pack(vi.y, vi.y);
+  q.vz = f2_pack(vi.z, vi.z);
+  q.vw = f2_pack(vi.w, vi.w);
+  q.lapm = f2_pack(lapm, lapm);
+  q.h0 = f2_pack(c.h0f, c.h0f);
+  q.h0sq = f2_pack(c.h0sqf, c.h0sqf);
+  q.spk = f2_pack(c.spiky_cf, c.spiky_cf);
+  q.p6 = f2_pack(c.poly6_cf, c.poly6_cf);
+  return q;
+}
+
+__device__ __forceinline__ void zero(ForcePart2& b) {
+  const f2 z = f2_pack(0.f, 0.f);
+  b.fx = b.fy = b.fz = b.vx = b.vy = b.vz = b.xx = b.xy = b.xz = z;
+}
+
+__device__ __forceinline__ void pair2_listed(const QueryPack& Q, float4 pa, float4 va, float mra, float4 pb,
+                                             float4 vb, float mrb, ForcePart2& b) {
+  const f2 DX = f2_sub(f2_pack(pa.x, pb.x), Q.px);
+  const f2 DY = f2_sub(f2_pack(pa.y, pb.y), Q.py);
+  const f2 DZ = f2_sub(f2_pack(pa.z, pb.z), Q.pz);
+  const f2 R2 = f2_fma(DZ, DZ, f2_fma(DY, DY, f2_mul(DX, DX)));
+  float r2a, r2b;
+  f2_unpack(R2, r2a, r2b);
+  const bool posa = r2a > 0.f, posb = r2b > 0.f;
+  const f2 INV = f2_pack(posa ? rsqrtf(r2a) : 0.f, posb ? rsqrtf(r2b) : 0.f);
+  const f2 MR = f2_pack(posa ? mra : 0.f, posb ? mrb : 0.f);
+  const f2 HR = f2_sub(Q.h0, f2_mul(R2, INV));
+  // (d/r) * m_i m_j (p_i/rho_i^2 + p_j/rho_j^2) * spiky(r)
+  const f2 FP = f2_mul(f2_mul(f2_mul(f2_mul(Q.pw, f2_pack(pa.w, pb.w)), f2_add(Q.vw, f2_pack(va.w, vb.w))),
+                              f2_mul(Q.spk, HR)),
+                       f2_mul(HR, INV));
+  b.fx = f2_fma(DX, FP, b.fx);
+  b.fy = f2_fma(DY, FP, b.fy);
+  b.fz = f2_fma(DZ, FP, b.fz);
+  // dv * (m_i m_j / rho_j * lap(r))
+  const f2 DVX = f2_sub(f2_pack(va.x, vb.x), Q.vx);
+  const f2 DVY = f2_sub(f2_pack(va.y, vb.y), Q.vy);
+  const f2 DVZ = f2_sub(f2_pack(va.z, vb.z), Q.vz);
+  const f2 VF = f2_mul(f2_mul(Q.lapm, MR), HR);
+  b.vx = f2_fma(DVX, VF, b.vx);
+  b.vy = f2_fma(DVY, VF, b.vy);
+  b.vz = f2_fma(DVZ, VF, b.vz);
+  // XSPH: dv * (m_j / rho_j * poly6(r))
+  const f2 T = f2_sub(Q.h0sq, R2);
+  const f2 XW = f2_mul(f2_mul(MR, Q.p6), f2_mul(f2_mul(T, T), T));
+  b.xx = f2_fma(DVX, XW, b.xx);
+  b.xy = f2_fma(DVY, XW, b.xy);
+  b.xz = f2_fma(DVZ, XW, b.xz);
+}
+
+// Folds both halves of the packed partial sums into the compensated totals.
+__device__ __forceinline__ void fold2(CompAcc& q, ForcePart2& b) {
+  float lo, hi;
+  f2_unpack(b.fx, lo, hi);
+  kahan_add(q.fpx, q.cpx, lo + hi);
+  f2_unpack(b.fy, lo, hi);
+  kahan_add(q.fpy, q.cpy, lo + hi);
+  f2_unpack(b.fz, lo, hi);
+  kahan_add(q.fpz, q.cpz, lo + hi);
+  f2_unpack(b.vx, lo, hi);
+  kahan_add(q.fvx, q.cvx, lo + hi);
+  f2_unpack(b.vy, lo, hi);
+  kahan_add(q.fvy, q.cvy, lo + hi);
+  f2_unpack(b.vz, lo, hi);
+  kahan_add(q.fvz, q.cvz, lo + hi);
+  f2_unpack(b.xx, lo, hi);
+  q.xsx += lo + hi;
+  f2_unpack(b.xy, lo, hi);
+  q.xsy += lo + hi;
+  f2_unpack(b.xz, lo, hi);
+  q.xsz += lo + hi;
+  zero(b);
+}
+
 // Three CTAs per SM is the shared-memory limit (75 KB each), so registers up to
 // 65536 / (3 x 256) cost no occupancy.
 template <int TB, bool kShear>
@@ -973,7 +1070,7 @@ __global__ void __launch_bounds__(kWT, 5) k_density_dense(StepConsts c, TiledArg
 // folded into the compensated totals every 8 rounds and at the end of the
 // chunk, uniformly across the warp.
 template <int TB, bool kShear>
-__global__ void __launch_bounds__(kWT, 3) k_force_dense(StepConsts c, TiledArgs a) {
+__global__ void __launch_bounds__(kWT, 2) k_force_dense(StepConsts c, TiledArgs a) {
   __shared__ float4 s_pos[kWarps][32];
   __shared__ float4 s_vel[kWarps][32];
   __shared__ float s_mr[kWarps][32];
@@ -993,9 +1090,11 @@ __global__ void __launch_bounds__(kWT, 3) k_force_dense(StepConsts c, TiledArgs 
     const Box3 qb = warp_box(qp.x, qp.y, qp.z, qv);
     task_neighbours(c, a, t, qb, hc2);
     const float lapm = qp.w * c.lap_cf;
-    const f2 PX = f2_pack(qp.x, qp.x), PY = f2_pack(qp.y, qp.y), PZ = f2_pack(qp.z, qp.z);
+    const QueryPack Q = query_pack(c, qp, qvel, lapm);
     CompAcc acc;
     ForcePart part;
+    ForcePart2 part2;
+    zero(part2);
     for (int nb = 0; nb < 27; ++nb) {
       const uint32_t s0 = __shfl_sync(0xffffffffu, t.nb_s, nb), e0 = __shfl_sync(0xffffffffu, t.nb_e, nb);
       if (s0 >= e0) continue;
@@ -1023,9 +1122,9 @@ __global__ void __launch_bounds__(kWT, 3) k_force_dense(StepConsts c, TiledArgs 
         for (uint32_t k = 0; k < 32u; k += 2) {
           const float4 A = sp4[k];      // x0 x1 y0 y1
           const float4 B = sp4[k + 1];  // z0 z1 m0 m1
-          const f2 DX = f2_sub(f2_pack(A.x, A.y), PX);
-          const f2 DY = f2_sub(f2_pack(A.z, A.w), PY);
-          const f2 DZ = f2_sub(f2_pack(B.x, B.y), PZ);
+          const f2 DX = f2_sub(f2_pack(A.x, A.y), Q.px);
+          const f2 DY = f2_sub(f2_pack(A.z, A.w), Q.py);
+          const f2 DZ = f2_sub(f2_pack(B.x, B.y), Q.pz);
           const f2 R2 = f2_fma(DZ, DZ, f2_fma(DY, DY, f2_mul(DX, DX)));
           float d0, d1;
           f2_unpack(f2_sub(R2, HC2), d0, d1);
@@ -1033,16 +1132,37 @@ __global__ void __launch_bounds__(kWT, 3) k_force_dense(StepConsts c, TiledArgs 
           mask = __funnelshift_l(__float_as_uint(d1), mask, 1);
         }
         mask = qv ? __brev(mask) : 0u;  // bit k = candidate k
-        const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(mask));
-        for (int r = 0; r < rounds; ++r) {
-          if (mask) {
-            const int k = __ffs(mask) - 1;
+        if (!kShear) {
+          // Two candidates per round; a lane out of candidates pads with a
+          // weightless copy of slot 0.
+          const int rounds = (int)(__reduce_max_sync(0xffffffffu, (unsigned)__popc(mask)) + 1) >> 1;
+          for (int r = 0; r < rounds; ++r) {
+            const bool ha = mask != 0;
+            const int ka = ha ? __ffs(mask) - 1 : 0;
             mask &= mask - 1;
-            pair_listed<kShear>(c, s_pos[w][k], s_vel[w][k], s_mr[w][k], qp, qvel, lapm, part, acc);
+            const bool hb = mask != 0;
+            const int kb = hb ? __ffs(mask) - 1 : 0;
+            mask &= mask - 1;
+            float4 pa = s_pos[w][ka], pb = s_pos[w][kb];
+            pa.w = ha ? pa.w : 0.f;
+            pb.w = hb ? pb.w : 0.f;
+            pair2_listed(Q, pa, s_vel[w][ka], ha ? s_mr[w][ka] : 0.f, pb, s_vel[w][kb], hb ? s_mr[w][kb] : 0.f,
+                         part2);
+            if ((r & 7) == 7) fold2(acc, part2);
           }
-          if ((r & 7) == 7) fold<kShear>(acc, part);
+          if (rounds & 7) fold2(acc, part2);
+        } else {
+          const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(mask));
+          for (int r = 0; r < rounds; ++r) {
+            if (mask) {
+              const int k = __ffs(mask) - 1;
+              mask &= mask - 1;
+              pair_listed<kShear>(c, s_pos[w][k], s_vel[w][k], s_mr[w][k], qp, qvel, lapm, part, acc);
+            }
+            if ((r & 7) == 7) fold<kShear>(acc, part);
+          }
+          if (rounds & 7) fold<kShear>(acc, part);
         }
-        if (rounds & 7) fold<kShear>(acc, part);
         __syncwarp();  // the chunk is consumed before the next one is staged
       }
     }
