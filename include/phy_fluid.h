@@ -243,6 +243,11 @@ int32_t phy_fluid_set_counting(PhyWorldHandle *w, uint32_t sub, int32_t on);
  * pairs with r < h, particles, grid cells}.  Used for roofline accounting. */
 int32_t phy_fluid_step_counters(PhyWorldHandle *w, uint32_t sub, uint64_t *out4);
 
+/* The dense-cell mask buffer of `sub` (PHY_TUNE_DENSE_MASKS), after waiting
+ * for its stream: out2 = {entries allocated, entries the dense-cell tasks of
+ * the last step reserved}.  An entry is one chunk of 32 candidates (33 u32). */
+int32_t phy_fluid_dense_mask_info(PhyWorldHandle *w, uint32_t sub, uint64_t *out2);
+
 /* Per-phase device timing of `sub` with CUDA events on its stream.  While on,
  * every step records five events without waiting for them (steps are then
  * not captured into CUDA graphs); phy_fluid_phase_times waits for the last
@@ -270,7 +275,11 @@ int32_t phy_fluid_phase_times(PhyWorldHandle *w, uint32_t sub, double *out5, int
  *   PHY_TUNE_GRAPH_CHUNK  0 = launch every step (default); k > 0 = capture
  *                         runs of k steps of phy_fluid_step into a CUDA graph
  *                         once and replay it (re-captured when parameters,
- *                         dt, the particle set or a buffer change).
+ *                         dt, the particle set or a buffer change);
+ *   PHY_TUNE_DENSE_MASKS  1 = the dense-cell force pass walks the in-range
+ *                         masks the density pass kept (default; the buffer
+ *                         grows with the tasks' demand, within half the free
+ *                         device memory), 0 = it filters the candidates again.
  * phy_fluid_get_tuning reads the same parameters. */
 enum {
   PHY_TUNE_COMP_TILE = 0,
@@ -279,7 +288,8 @@ enum {
   PHY_TUNE_QUEUE = 3,
   PHY_TUNE_SORT_BLOCK = 4,
   PHY_TUNE_GRAPH_CHUNK = 5,
-  PHY_TUNE_DENSE_MEAN = 6
+  PHY_TUNE_DENSE_MEAN = 6,
+  PHY_TUNE_DENSE_MASKS = 7
 };
 int32_t phy_fluid_set_tuning(PhyWorldHandle *w, uint32_t sub, int32_t param, int64_t value);
 int32_t phy_fluid_get_tuning(PhyWorldHandle *w, uint32_t sub, int32_t param, int64_t *out);

@@ -23,9 +23,10 @@ TUNE_QUEUE = 3
 TUNE_SORT_BLOCK = 4
 TUNE_GRAPH_CHUNK = 5
 TUNE_DENSE_MEAN = 6
+TUNE_DENSE_MASKS = 7
 TUNE_PARAMS = {"comp_tile": TUNE_COMP_TILE, "halo_cap": TUNE_HALO_CAP, "ctas_per_sm": TUNE_CTAS_PER_SM,
                "queue": TUNE_QUEUE, "sort_block": TUNE_SORT_BLOCK, "graph_chunk": TUNE_GRAPH_CHUNK,
-               "dense_mean": TUNE_DENSE_MEAN}
+               "dense_mean": TUNE_DENSE_MEAN, "dense_masks": TUNE_DENSE_MASKS}
 
 NOALLOC_MAX_PARTICLES = 65536
 NOALLOC_MAX_CELLS = 262144
@@ -148,6 +149,7 @@ SIGNATURES = {
     "phy_fluid_unpin_host": (C.c_int32, [C.c_void_p]),
     "phy_fluid_set_counting": (C.c_int32, [H, C.c_uint32, C.c_int32]),
     "phy_fluid_step_counters": (C.c_int32, [H, C.c_uint32, C.POINTER(C.c_uint64)]),
+    "phy_fluid_dense_mask_info": (C.c_int32, [H, C.c_uint32, C.POINTER(C.c_uint64)]),
     "phy_fluid_set_timing": (C.c_int32, [H, C.c_uint32, C.c_int32]),
     "phy_fluid_phase_times": (C.c_int32, [H, C.c_uint32, DP, C.c_int32]),
     "phy_fluid_set_tuning": (C.c_int32, [H, C.c_uint32, C.c_int32, C.c_int64]),

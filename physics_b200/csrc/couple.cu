@@ -166,8 +166,8 @@ __global__ void __launch_bounds__(kCT) k_couple_points(StepConsts c, CoupleArgs 
 // the candidate counts, writes its candidates' particle indices and masses
 // in visit order (k_point_candidates).  The ordered walk (one CTA) then reads
 // those lists two points ahead: while thread 0 runs point k's ordered f64
-// sums, warps 1..7 gather point k+1's velocities and the products v_j m_j
-// into shared memory and load point k+2's list.  Point k's reaction can
+// sums, warps 1..4 gather point k+1's velocities and the products v_j m_j
+// into shared memory while warps 5..7 load point k+2's table and list.  Point k's reaction can
 // change only the velocities of particles in point k's own cells, so after
 // it the candidates of point k+1 in cells that point k shares are gathered
 // again (points far apart share none).  The ordered sums read ready products
@@ -266,29 +266,49 @@ __device__ __forceinline__ VelBuf vel_buf(unsigned char* smem, int q) {
   return {v + 3 * q * kPB, pw + 2 * q * kPB};
 }
 
-// Threads t0.. (stride nt): table and list of point j into slot q.
-__device__ __forceinline__ void load_point(const PointLists& L, int j, PointTable& T, const PointBuf& B, int t0,
-                                           int nt) {
+// One warp: the cell table of point j (a word per lane, prefix sums by a
+// warp scan).
+__device__ __forceinline__ void load_table(const PointLists& L, int j, PointTable& T) {
+  const int lane = threadIdx.x & 31;
   const uint32_t* t = L.tab + (size_t)j * kTabU;
-  const int t1 = (int)threadIdx.x - t0;
-  if (t1 == 0) {
-    T.in = (int)t[0];
-    uint32_t p = 0;
-    for (int u = 0; u < 27; ++u) {
-      T.beg[u] = t[2 + u];
-      T.cnt[u] = t[29 + u];
-      T.pre[u] = p;
-      p += T.cnt[u];
-    }
-    T.pre[27] = p;
+  const uint32_t beg = lane < 27 ? t[2 + lane] : 0u, cnt = lane < 27 ? t[29 + lane] : 0u;
+  uint32_t incl = cnt;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
   }
+  if (lane < 27) {
+    T.beg[lane] = beg;
+    T.cnt[lane] = cnt;
+    T.pre[lane] = incl - cnt;
+  }
+  if (lane == 26) T.pre[27] = incl;
+  if (lane == 0) T.in = (int)t[0];
+}
+
+// Threads t0.. (stride nt): the candidate list of point j (when it fits) into
+// buffer B; independent of the table in shared memory.
+__device__ __forceinline__ void load_list(const PointLists& L, int j, const PointBuf& B, int t0, int nt) {
+  const uint32_t* t = L.tab + (size_t)j * kTabU;
   if (t[0] && t[1] <= (uint32_t)kPB) {
     const uint32_t o = L.off[j], total = t[1];
-    for (uint32_t e = (uint32_t)t1; e < total; e += (uint32_t)nt) {
+    for (uint32_t e = (uint32_t)((int)threadIdx.x - t0); e < total; e += (uint32_t)nt) {
       B.idx[e] = L.idx[o + e];
       B.m[e] = L.m[o + e];
     }
   }
+}
+
+// Table and list of point j by all threads (the prologue).
+__device__ __forceinline__ void load_point(const PointLists& L, int j, PointTable& T, const PointBuf& B) {
+  if ((threadIdx.x >> 5) == 0) load_table(L, j, T);
+  load_list(L, j, B, 0, kCT);
+}
+
+// Warps 5..7 during the walk: table and list of point j.
+__device__ __forceinline__ void load_ahead(const PointLists& L, int j, PointTable& T, const PointBuf& B) {
+  if ((threadIdx.x >> 5) == 5) load_table(L, j, T);
+  load_list(L, j, B, 5 * 32, kCT - 5 * 32);
 }
 
 __device__ __forceinline__ void gather_candidate(const CoupleArgs& a, const PointBuf& B, const VelBuf& V,
@@ -303,9 +323,10 @@ __device__ __forceinline__ void gather_candidate(const CoupleArgs& a, const Poin
   V.pw[2 * e + 1] = make_double2(vz * m, m);
 }
 
-// Warps 1..7: velocities of point j (its list already staged) and, when
+// Warps 1..4: velocities of point j (its list already staged) and, when
 // `prev` (the previous point, reaction not yet applied) is given, the cells
 // the two share.
+constexpr int kGatherThreads = 4 * 32;
 __device__ __forceinline__ void gather_point(const CoupleArgs& a, PointTable& T, const PointTable* prev,
                                              const PointBuf& B, const VelBuf& V) {
   if ((threadIdx.x >> 5) == 1) {
@@ -316,7 +337,7 @@ __device__ __forceinline__ void gather_point(const CoupleArgs& a, PointTable& T,
     const uint32_t bits = __ballot_sync(0xffffffffu, shared);
     if (lane == 0) T.again = bits;
   }
-  for (uint32_t e = threadIdx.x - 32; e < T.pre[27]; e += kCT - 32) gather_candidate(a, B, V, e);
+  for (uint32_t e = threadIdx.x - 32; e < T.pre[27]; e += kGatherThreads) gather_candidate(a, B, V, e);
 }
 
 __global__ void __launch_bounds__(kCT) k_couple_points_piped(StepConsts c, CoupleArgs a, int p0, int nb,
@@ -326,8 +347,8 @@ __global__ void __launch_bounds__(kCT) k_couple_points_piped(StepConsts c, Coupl
   extern __shared__ __align__(16) unsigned char smem[];
   const int t = threadIdx.x, warp = t >> 5;
   // Prologue: lists of points 0 and 1, velocities of point 0.
-  if (nb > 0) load_point(L, 0, s_tab[0], point_buf(smem, 0), 0, kCT);
-  if (nb > 1) load_point(L, 1, s_tab[1], point_buf(smem, 1), 0, kCT);
+  if (nb > 0) load_point(L, 0, s_tab[0], point_buf(smem, 0));
+  if (nb > 1) load_point(L, 1, s_tab[1], point_buf(smem, 1));
   __syncthreads();
   if (nb > 0 && s_tab[0].fits()) {
     if (t == 32) s_tab[0].again = 0;
@@ -359,6 +380,7 @@ __global__ void __launch_bounds__(kCT) k_couple_points_piped(StepConsts c, Coupl
           }
           __syncthreads();
           if (t == 0)
+#pragma unroll 8
             for (uint32_t e = 0; e < cnt; ++e) {
               const double w = B.m[e];
               sx = sx + V.v[e] * w;
@@ -382,16 +404,35 @@ __global__ void __launch_bounds__(kCT) k_couple_points_piped(StepConsts c, Coupl
       }
       __syncthreads();
       // Point j's reaction is applied: point j+1's velocities are final.
-      if (warp >= 1) {
+      if (warp >= 1 && warp <= 4) {
         if (has1 && s_tab[n3].fits()) gather_point(a, s_tab[n3], nullptr, point_buf(smem, n3), vel_buf(smem, n2));
-        if (has2) load_point(L, j + 2, s_tab[f3], point_buf(smem, f3), 32, kCT - 32);
+      } else if (warp >= 5 && has2) {
+        load_ahead(L, j + 2, s_tab[f3], point_buf(smem, f3));
       }
       __syncthreads();
       continue;
     }
     if (t == 0) {
+      // Eight candidates' products are loaded before they are added, so the
+      // loads overlap while the four sums still add in candidate order.
       double sx = 0.0, sy = 0.0, sz = 0.0, sw = 0.0;
-      for (uint32_t e = 0; e < total; ++e) {
+      uint32_t e = 0;
+      for (; e + 8 <= total; e += 8) {
+        double2 P[8], R[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          P[u] = V.pw[2 * (e + u)];
+          R[u] = V.pw[2 * (e + u) + 1];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          sx = sx + P[u].x;
+          sy = sy + P[u].y;
+          sz = sz + R[u].x;
+          sw = sw + R[u].y;
+        }
+      }
+      for (; e < total; ++e) {
         const double2 p = V.pw[2 * e], r = V.pw[2 * e + 1];
         sx = sx + p.x;
         sy = sy + p.y;
@@ -399,9 +440,10 @@ __global__ void __launch_bounds__(kCT) k_couple_points_piped(StepConsts c, Coupl
         sw = sw + r.y;
       }
       point_force(c, a, q, sx, sy, sz, sw, s_r);
-    } else if (warp >= 1) {
+    } else if (warp >= 1 && warp <= 4) {
       if (has1 && s_tab[n3].fits()) gather_point(a, s_tab[n3], &T, point_buf(smem, n3), vel_buf(smem, n2));
-      if (has2) load_point(L, j + 2, s_tab[f3], point_buf(smem, f3), 32, kCT - 32);
+    } else if (warp >= 5 && has2) {
+      load_ahead(L, j + 2, s_tab[f3], point_buf(smem, f3));
     }
     __syncthreads();
     const double msum = s_r[3];

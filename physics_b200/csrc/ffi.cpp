@@ -441,6 +441,14 @@ int32_t phy_fluid_step_counters(PhyWorldHandle* w, uint32_t sub, uint64_t* out4)
   });
 }
 
+int32_t phy_fluid_dense_mask_info(PhyWorldHandle* w, uint32_t sub, uint64_t* out2) {
+  if (!out2) return -1;
+  return guard<int32_t>(-1, [&] {
+    sub_of(w, sub).world->dense_mask_info(out2);
+    return 0;
+  });
+}
+
 int32_t phy_fluid_set_counting(PhyWorldHandle* w, uint32_t sub, int32_t on) {
   return guard<int32_t>(-1, [&] {
     sub_of(w, sub).world->set_counting(on != 0);
@@ -496,6 +504,10 @@ int32_t phy_fluid_set_tuning(PhyWorldHandle* w, uint32_t sub, int32_t param, int
       case PHY_TUNE_DENSE_MEAN:
         fw.set_dense_mean(in_range(1, 1 << 20));
         break;
+      case PHY_TUNE_DENSE_MASKS:
+        t.dense_masks = in_range(0, 1);
+        fw.set_launch_tuning(t);
+        break;
       default:
         throw std::invalid_argument("unknown tuning parameter");
     }
@@ -516,6 +528,7 @@ int32_t phy_fluid_get_tuning(PhyWorldHandle* w, uint32_t sub, int32_t param, int
       case PHY_TUNE_SORT_BLOCK: *out = t.sort_block; break;
       case PHY_TUNE_GRAPH_CHUNK: *out = fw.graph_chunk(); break;
       case PHY_TUNE_DENSE_MEAN: *out = fw.dense_mean(); break;
+      case PHY_TUNE_DENSE_MASKS: *out = t.dense_masks; break;
       default: throw std::invalid_argument("unknown tuning parameter");
     }
     return 0;

@@ -224,6 +224,86 @@ __global__ void k_tape_copy(int n, TapeCopy t) {
   for (uint32_t k = 0; k < m; ++k) t.nbr_dst[(size_t)k * n + s] = t.nbr[(size_t)k * t.nbr_stride + s];
 }
 
+// Several device arrays copied in one launch (blockIdx.y = array): 16-byte
+// words where both ends are 16-byte aligned, 8-byte words where they are
+// 8-byte aligned, bytes for the rest.
+struct ArrayCopy {
+  static constexpr int kMax = 24;
+  const unsigned char* src[kMax];
+  unsigned char* dst[kMax];
+  size_t bytes[kMax];
+};
+
+__global__ void k_copy_arrays(ArrayCopy a) {
+  const int q = blockIdx.y;
+  const unsigned char* s = a.src[q];
+  unsigned char* d = a.dst[q];
+  const size_t bytes = a.bytes[q];
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uintptr_t align = reinterpret_cast<uintptr_t>(s) | reinterpret_cast<uintptr_t>(d);
+  size_t done = 0;
+  if ((align & 15) == 0) {
+    const size_t words = bytes / 16;
+    for (size_t k = i; k < words; k += stride)
+      reinterpret_cast<uint4*>(d)[k] = reinterpret_cast<const uint4*>(s)[k];
+    done = words * 16;
+  } else if ((align & 7) == 0) {
+    const size_t words = bytes / 8;
+    for (size_t k = i; k < words; k += stride)
+      reinterpret_cast<unsigned long long*>(d)[k] = reinterpret_cast<const unsigned long long*>(s)[k];
+    done = words * 8;
+  }
+  for (size_t k = done + i; k < bytes; k += stride) d[k] = s[k];
+}
+
+// The compensated step's outputs by insertion index (9 doubles each: rho, p,
+// mu, acc xyz, xsph xyz), for the records of the compensated adjoint.
+__global__ void k_comp_outputs_by_id(int n, const uint32_t* __restrict__ id, const double* __restrict__ rho,
+                                     const double* __restrict__ p, const double* __restrict__ mu,
+                                     const double* __restrict__ ax, const double* __restrict__ ay,
+                                     const double* __restrict__ az, const double* __restrict__ xx,
+                                     const double* __restrict__ xy, const double* __restrict__ xz,
+                                     double* __restrict__ out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  double* o = out + 9 * (size_t)id[s];
+  o[0] = rho[s];
+  o[1] = p[s];
+  o[2] = mu[s];
+  o[3] = ax[s];
+  o[4] = ay[s];
+  o[5] = az[s];
+  o[6] = xx[s];
+  o[7] = xy[s];
+  o[8] = xz[s];
+}
+
+// Overwrites a tape slot's density, pressure and force records (in the f64
+// recording step's order) with the compensated step's values of the same
+// particles, so the reverse sweep takes the compensated forward's branches
+// (max(0, rho - rho0), walls) and values; p/rho^2 and m/rho follow from them
+// with the f64 density pass's operations.
+__global__ void k_tape_override(int n, const uint32_t* __restrict__ id, const double* __restrict__ mass,
+                                const double* __restrict__ comp, double* rho, double* p, double* pr2, double* mr,
+                                double* mu, double* ax, double* ay, double* az, double* xx, double* xy, double* xz) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const double* o = comp + 9 * (size_t)id[s];
+  const double r = o[0], pr = o[1];
+  rho[s] = r;
+  p[s] = pr;
+  pr2[s] = __ddiv_rn(pr, __dmul_rn(r, r));
+  mr[s] = __ddiv_rn(mass[s], r);
+  mu[s] = o[2];
+  ax[s] = o[3];
+  ay[s] = o[4];
+  az[s] = o[5];
+  xx[s] = o[6];
+  xy[s] = o[7];
+  xz[s] = o[8];
+}
+
 // num-traits ToPrimitive::to_i64 on f64 with None -> 0 (grid.rs:25-33).
 long long key_axis_host(double x, double inv) {
   double f = std::floor(x * inv);
@@ -397,6 +477,15 @@ void FluidWorld::free_all() {
   dfree(b_.queue);
   dfree(b_.tile_crowd);
   dfree(b_.dense_q0);
+  dfree(b_.task_mbase);
+  dfree(b_.task_mcount);
+  dfree(b_.mask_hdr);
+  dfree(b_.mask_bits);
+  dfree(b_.mask_ctl);
+  b_.mask_cap = 0;
+  mask_tried_ = 0;
+  if (b_.mask_demand) cudaFreeHost(b_.mask_demand);
+  b_.mask_demand = nullptr;
   dfree(b_.okey);
   dfree(b_.cell_of);
   dfree(b_.rank);
@@ -462,6 +551,8 @@ void FluidWorld::ensure_capacity(size_t n) {
   dfree(b_.tile_slot);
   dfree(b_.tile_crowd);
   dfree(b_.dense_q0);
+  dfree(b_.task_mbase);
+  dfree(b_.task_mcount);
   dfree(b_.okey);
   dgrow(b_.cell_of, 0, cap, s);
   dgrow(b_.rank, 0, cap, s);
@@ -490,6 +581,13 @@ void FluidWorld::ensure_mode_buffers() {
     if (!b_.queue) dalloc(b_.queue, 5);
     // Dense-cell tasks: at most one per 32 particles plus one per occupied cell.
     if (!b_.dense_q0) dalloc(b_.dense_q0, cap + cap / 32 + 64);
+    if (!b_.task_mbase) dalloc(b_.task_mbase, cap + cap / 32 + 64);
+    if (!b_.task_mcount) dalloc(b_.task_mcount, cap + cap / 32 + 64);
+    if (!b_.mask_ctl) dalloc(b_.mask_ctl, 1);
+    if (!b_.mask_demand) {
+      cuda_check(cudaMallocHost((void**)&b_.mask_demand, sizeof(unsigned long long)), "cudaMallocHost");
+      *b_.mask_demand = 0;
+    }
     if (!b_.okey) dalloc(b_.okey, cap);
   }
   ++alloc_gen_;
@@ -803,7 +901,8 @@ void FluidWorld::add_particles(size_t m, const double* pos, const double* vel, c
                                const uint32_t* material) {
   if (m == 0) return;
   if (!pos || !mass) throw std::invalid_argument("add_particles: pos and mass are required");
-  if (!scenes_.empty()) throw std::invalid_argument("add_particles: the world holds batched scenes (clear_scenes first)");
+  if (!scenes_.empty())
+    throw std::invalid_argument("add_particles: the world holds batched scenes (clear_scenes first)");
   ensure_capacity(n_ + m);
   // Staging layout: pos 3m | vel 3m | mass m | material m (as doubles).
   std::vector<double> st(8 * m, 0.0);
@@ -1068,7 +1167,40 @@ StepConsts FluidWorld::prepare_step(double dt) {
   if (!scenes_.empty() && !(prec_ == Precision::F32Comp && comp_tile_ > 0))
     throw std::invalid_argument("step: batched scenes need the tiled compensated form");
   ensure_cells();
+  if (prec_ == Precision::F32Comp && comp_tile_ > 0) ensure_masks();
   return make_consts(dt);
+}
+
+// Grows the dense-cell mask buffer to the entries the tasks of a recent step
+// reserved (the pinned copy lags by the steps still in flight), within half
+// the free device memory; tasks that find no room filter again in the force
+// pass, so the size never changes a result.  A failed allocation leaves the
+// buffer empty and is not retried below the demand that failed.
+void FluidWorld::ensure_masks() {
+  if (!tuning_.dense_masks || !b_.mask_ctl || !b_.mask_demand) return;
+  const unsigned long long want = *reinterpret_cast<volatile unsigned long long*>(b_.mask_demand);
+  if (want <= b_.mask_cap || want <= mask_tried_) return;
+  mask_tried_ = want;
+  constexpr unsigned long long kEntryBytes = 33 * sizeof(uint32_t);
+  cuda_check(cudaStreamSynchronize(stream_), "mask buffer sync");
+  size_t free_b = 0, total_b = 0;
+  cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+  const unsigned long long limit =
+      std::min<unsigned long long>((free_b / 2 + b_.mask_cap * kEntryBytes) / kEntryBytes, 0xfffffffeull);
+  const unsigned long long cap = std::min(want + want / 2 + 1024, limit);
+  if (cap <= b_.mask_cap) return;
+  dfree(b_.mask_hdr);
+  dfree(b_.mask_bits);
+  b_.mask_cap = 0;
+  ++alloc_gen_;
+  if (cudaMalloc((void**)&b_.mask_hdr, cap * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc((void**)&b_.mask_bits, cap * 32 * sizeof(uint32_t)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    dfree(b_.mask_hdr);
+    dfree(b_.mask_bits);
+    return;
+  }
+  b_.mask_cap = cap;
 }
 
 // The device work of one step on the world's stream.
@@ -1146,7 +1278,8 @@ void FluidWorld::run_graph(double dt, int k) {
   std::vector<unsigned char> key(sizeof(StepConsts) + 64, 0);
   std::memcpy(key.data(), &c, sizeof(StepConsts));
   long long extra[8] = {k, (long long)alloc_gen_, b_.cur, counting_ ? 1 : 0, b_.has_ba ? 1 : 0,
-                        tuning_.ctas_per_sm + 1000ll * tuning_.queue, tuning_.sort_block,
+                        tuning_.ctas_per_sm + 1000ll * tuning_.queue + 10000ll * tuning_.dense_masks,
+                        tuning_.sort_block,
                         (long long)(uintptr_t)stream_};
   std::memcpy(key.data() + sizeof(StepConsts), extra, sizeof(extra));
   const int cur0 = b_.cur;
@@ -1274,7 +1407,7 @@ void FluidWorld::clear_scenes() {
 // step reads and the outputs it leaves: pv1, the current per-particle
 // constants, rho, p, acc, xsph and mu.  The saved copy is kept until
 // release_snapshot().
-void FluidWorld::snapshot(bool restore, int slot) {
+void FluidWorld::snapshot(bool restore, int slot, bool sync) {
   if (slot < 0 || slot >= kSnapSlots) throw std::logic_error("snapshot: slot out of range");
   const size_t n = n_;
   if (restore) b_.cur = snap_cur_[slot];
@@ -1301,6 +1434,7 @@ void FluidWorld::snapshot(bool restore, int slot) {
     off[q] = total;
     total += (arrays[q].second + 255) / 256 * 256;
   }
+  if (arrays.size() > (size_t)ArrayCopy::kMax) throw std::logic_error("snapshot: too many arrays");
   if (!restore) {
     if (total > snap_bytes_[slot]) {
       dfree(snap_arena_[slot]);
@@ -1308,21 +1442,27 @@ void FluidWorld::snapshot(bool restore, int slot) {
       dalloc(snap_arena_[slot], total / 8);
       snap_bytes_[slot] = total;
     }
-    for (size_t q = 0; q < arrays.size(); ++q)
-      cuda_check(cudaMemcpyAsync(reinterpret_cast<char*>(snap_arena_[slot]) + off[q], arrays[q].first,
-                                 arrays[q].second, cudaMemcpyDeviceToDevice, stream_),
-                 "snapshot");
     snap_cur_[slot] = b_.cur;
     snap_count_[slot] = arrays.size();
-  } else {
-    if (snap_count_[slot] != arrays.size() || !snap_arena_[slot])
-      throw std::logic_error("snapshot: no saved state of this layout");
-    for (size_t q = 0; q < arrays.size(); ++q)
-      cuda_check(cudaMemcpyAsync(arrays[q].first, reinterpret_cast<char*>(snap_arena_[slot]) + off[q],
-                                 arrays[q].second, cudaMemcpyDeviceToDevice, stream_),
-                 "restore");
+  } else if (snap_count_[slot] != arrays.size() || !snap_arena_[slot]) {
+    throw std::logic_error("snapshot: no saved state of this layout");
   }
-  cuda_check(cudaStreamSynchronize(stream_), "snapshot sync");
+  ArrayCopy ac{};
+  size_t widest = 0;
+  for (size_t q = 0; q < arrays.size(); ++q) {
+    unsigned char* saved = reinterpret_cast<unsigned char*>(snap_arena_[slot]) + off[q];
+    unsigned char* live = static_cast<unsigned char*>(arrays[q].first);
+    ac.src[q] = restore ? saved : live;
+    ac.dst[q] = restore ? live : saved;
+    ac.bytes[q] = arrays[q].second;
+    widest = std::max(widest, arrays[q].second);
+  }
+  if (widest > 0) {
+    const size_t blocks = std::min<size_t>((widest / 16 + kThreads - 1) / kThreads + 1, 1184);
+    k_copy_arrays<<<dim3((unsigned)blocks, (unsigned)arrays.size()), kThreads, 0, stream_>>>(ac);
+    cuda_check(cudaGetLastError(), restore ? "restore" : "snapshot");
+  }
+  if (sync) cuda_check(cudaStreamSynchronize(stream_), "snapshot sync");
 }
 
 void FluidWorld::release_snapshot() {
@@ -1470,6 +1610,12 @@ uint32_t FluidWorld::last_step_flags() {
   cuda_check(cudaMemcpyAsync(&f, b_.flags, sizeof(f), cudaMemcpyDeviceToHost, stream_), "flags");
   cuda_check(cudaStreamSynchronize(stream_), "flags sync");
   return f;
+}
+
+void FluidWorld::dense_mask_info(uint64_t* out2) {
+  cuda_check(cudaStreamSynchronize(stream_), "mask info sync");
+  out2[0] = b_.mask_cap;
+  out2[1] = b_.mask_demand ? *reinterpret_cast<volatile unsigned long long*>(b_.mask_demand) : 0;
 }
 
 void FluidWorld::last_step_counters(uint64_t* out2) {
@@ -1725,6 +1871,8 @@ void FluidWorld::tape_clear() {
   tape_.on = false;
   tape_.n = 0;
   dfree(adj_work_);
+  dfree(comp_rec_);
+  comp_rec_cap_ = 0;
   for (auto& p : adj_slot_f_) dfree(p);
   for (auto& p : adj_slot_u_) dfree(p);
   adj_slot_f_.clear();
@@ -1837,9 +1985,19 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
   // A compensated world is differentiated along its own trajectory: each
   // re-run step first takes an f64 plain recording step from the same state
   // (the records of the exact step map at that state), then returns to the
-  // state and takes the compensated step to the next one.
+  // state and takes the compensated step to the next one, whose density,
+  // pressure, viscosity, acceleration and XSPH outputs replace the recorded
+  // f64 values.
   const Precision form = prec_;
   const bool comp = form == Precision::F32Comp;
+  double* comp_rec = nullptr;  // compensated outputs by insertion index, 9 per particle
+  if (comp) {
+    if (comp_rec_cap_ < 9 * n) {
+      dalloc(comp_rec_, 9 * n);
+      comp_rec_cap_ = 9 * n;
+    }
+    comp_rec = comp_rec_;
+  }
   auto cleanup = [&]() {
     for (int k = 0; k < 3; ++k) b_.tape_fv[k] = nullptr;
     b_.tape_shear = nullptr;
@@ -1876,7 +2034,9 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
         TapeSlot& sl = slots[t - t0];
         const int si = t - t0;
         if (comp) {
-          snapshot(false, 1);  // the compensated state of step t
+          // The f64 recording step from state t first; state t is kept in
+          // slot 1 for the compensated step that follows it.
+          snapshot(false, 1, false);
           prec_ = Precision::F64Plain;
           ensure_mode_buffers();  // f64 neighbour lists, kept for later sweeps
         }
@@ -1927,10 +2087,21 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
                                    cudaMemcpyDeviceToDevice, s),
                    "tape copy");
         if (comp) {
-          // The records are copied (stream order) before the state returns.
+          // Back to state t for the compensated step to state t+1; its
+          // outputs (by insertion index) replace the recorded f64 ones.
+          snapshot(true, 1, false);
           prec_ = Precision::F32Comp;
-          snapshot(true, 1);
           step_impl(tape_.dts[t]);
+          const ParticleConsts& cq = b_.pc[b_.cur];
+          k_comp_outputs_by_id<<<grid_for(n), kThreads, 0, s>>>((int)n, cq.id, b_.rho, b_.p, b_.mu, b_.acc[0],
+                                                                b_.acc[1], b_.acc[2], b_.xsph[0], b_.xsph[1],
+                                                                b_.xsph[2], comp_rec);
+          k_tape_override<<<grid_for(n), kThreads, 0, s>>>(
+              (int)n, v.id, v.mass, comp_rec, const_cast<double*>(v.rho), const_cast<double*>(v.p),
+              const_cast<double*>(v.pr2), const_cast<double*>(v.mr), const_cast<double*>(v.mu),
+              const_cast<double*>(v.acc[0]), const_cast<double*>(v.acc[1]), const_cast<double*>(v.acc[2]),
+              const_cast<double*>(v.xsph[0]), const_cast<double*>(v.xsph[1]), const_cast<double*>(v.xsph[2]));
+          cuda_check(cudaGetLastError(), "tape override");
         }
       }
       for (int t = t1 - 1; t >= t0; --t) launch_adjoint_step(slots[t - t0].c, slots[t - t0].view(n), w, s);

@@ -145,6 +145,9 @@ class FluidWorld {
   // by set_counting(true) and costs one atomic per warp.
   void set_counting(bool on) { counting_ = on; }
   void last_step_counters(uint64_t* out2);
+  // Dense-cell mask buffer: entries allocated, entries the last step's tasks
+  // reserved (waits for the stream).
+  void dense_mask_info(uint64_t* out2);
   int grid_cells() const { return ncells_; }
 
   // FluidWorld::couple_points (world.rs:691-752) on the device, bit-exact:
@@ -201,6 +204,7 @@ class FluidWorld {
  private:
   void ensure_capacity(size_t n);
   void ensure_mode_buffers();
+  void ensure_masks();
   void ensure_cells();
   void grow_box_with_bounds();
   void grow_box_with_positions(size_t n, const double* pos3);
@@ -215,7 +219,9 @@ class FluidWorld {
   void run_graph(double dt, int k);
   void drop_graphs();
   void stage_field(int field, double* st);
-  void snapshot(bool restore, int slot = 0);
+  // Saves (or restores) the per-particle state in slot `slot` with one copy
+  // launch on the world's stream; `sync` waits for it.
+  void snapshot(bool restore, int slot = 0, bool sync = true);
   void release_snapshot();
   // Mean ms per step of `steps` steps from each saved slot 0..nslots-1 under
   // tuning t (warm-up and graph capture first).
@@ -291,12 +297,15 @@ class FluidWorld {
   } tape_;
   // Reverse-sweep buffers kept between sweeps (freed by tape_clear).
   double* adj_work_ = nullptr;
+  double* comp_rec_ = nullptr;  // compensated adjoint: the compensated step's outputs by insertion index
+  size_t comp_rec_cap_ = 0;
   std::vector<double*> adj_slot_f_;
   std::vector<uint32_t*> adj_slot_u_;
   std::vector<size_t> adj_slot_ucount_;
   bool recomputing_ = false;
   // Saved states (autotuner, reverse sweep): per slot one arena reused while
   // large enough.
+  unsigned long long mask_tried_ = 0;  // the last mask demand the buffer was grown for
   static constexpr int kSnapSlots = 3;
   double* snap_arena_[kSnapSlots] = {};
   size_t snap_bytes_[kSnapSlots] = {};

@@ -67,6 +67,19 @@ struct DevBuffers {
   SceneBox* boxes = nullptr;
   uint32_t* queue = nullptr;
   uint32_t* dense_q0 = nullptr;
+  // In-range masks of the dense-cell density pass, read back by the force
+  // pass of the same step instead of filtering again: per task its first
+  // entry (kNoMasks: none stored) and entry count; per entry the chunk's
+  // first sorted slot << 5 | neighbour cell, and 32 lane masks.  mask_ctl
+  // counts the entries the tasks reserved (their upper bounds, stored or
+  // not), so the host can grow mask_cap; mask_demand is its pinned host copy.
+  uint32_t* task_mbase = nullptr;
+  uint32_t* task_mcount = nullptr;
+  uint32_t* mask_hdr = nullptr;
+  uint32_t* mask_bits = nullptr;
+  unsigned long long mask_cap = 0;  // entries
+  unsigned long long* mask_ctl = nullptr;
+  unsigned long long* mask_demand = nullptr;
   // Sort scratch.
   uint32_t* cell_of = nullptr;
   uint32_t* rank = nullptr;
@@ -183,6 +196,7 @@ struct LaunchTuning {
   int ctas_per_sm = 0;
   int queue = 0;
   int sort_block = 256;
+  int dense_masks = 1;  // 1: the dense-cell force pass walks the density pass's masks
 };
 
 // step_tiled.cu: the FP32-compensated passes over staged 4x4x4-cell tiles.

@@ -90,6 +90,13 @@ struct TiledArgs {
   uint32_t* dense_q0;
   uint32_t* dense_count;
   uint32_t* dense_taken;  // [0]: tasks taken by the density pass, [1]: by the force pass
+  // The density pass's in-range masks for the force pass (null: none kept).
+  uint32_t* task_mbase;
+  uint32_t* task_mcount;
+  uint32_t* mask_hdr;
+  uint32_t* mask_bits;
+  unsigned long long* mask_ctl;
+  unsigned long long mask_cap;
   int stride;
   uint32_t* flags;
   unsigned long long* counters;
@@ -461,7 +468,8 @@ __global__ void __launch_bounds__(kTT, 6) k_density_tiled(StepConsts c, TiledArg
         for (int dj = -1; dj <= 1; ++dj) {
           const int h0 = hq + di * T::H * T::H + dj * T::H - 1;  // cells h0 .. h0+2 (dk = -1, 0, 1)
           const uint32_t s0 = s_off[h0] - base, e0 = s_off[h0 + 3] - base;  // both even
-          if (kCount) cand += (s_end[h0] - s_src[h0]) + (s_end[h0 + 1] - s_src[h0 + 1]) + (s_end[h0 + 2] - s_src[h0 + 2]);
+          if (kCount)
+            cand += (s_end[h0] - s_src[h0]) + (s_end[h0 + 1] - s_src[h0 + 1]) + (s_end[h0 + 2] - s_src[h0 + 2]);
           f2 NPART = f2_pack(0.f, 0.f);
           for (uint32_t cb = s0; cb < e0; cb += 32) {
             const uint32_t ce = min(cb + 32u, e0);
@@ -850,9 +858,17 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
 // queries and of the chunk's candidates are at least the cutoff apart, which
 // removes about half the candidates of a crowded neighbourhood.  Tasks come
 // from a device counter (one atomic per task), so no barrier joins warps.
+//
+// The density pass also keeps every chunk's 32 lane masks of in-range
+// candidates (chunks where some lane has one), in a buffer each task reserves
+// at its start for its upper bound of chunks.  The force pass of the same
+// step, at the same positions, walks the kept masks in the same order instead
+// of filtering again, which gives the same pairs in the same order; a task
+// whose reservation did not fit filters as before.
 
 constexpr int kWT = 256;  // threads per dense-task CTA
 constexpr int kWarps = kWT / 32;
+constexpr uint32_t kNoMasks = 0xffffffffu;
 
 // Order-preserving map of f32 bits to u32 (for warp min/max reductions) and
 // its inverse.  NaN maps outside [-inf, inf], which makes a box conservative.
@@ -922,6 +938,7 @@ __device__ __forceinline__ CellGeom cell_geom(const StepConsts& c, const TiledAr
 // 27 neighbour ranges held by lanes 0..26 (empty when the neighbour cell's
 // box is out of reach of the queries' box).
 struct DenseTask {
+  uint32_t k;  // task index
   uint32_t q0, qn;
   CellGeom cg;
   uint32_t nb_s, nb_e;  // this lane's neighbour range (lane < 27)
@@ -935,6 +952,7 @@ __device__ __forceinline__ bool next_task(const StepConsts& c, const TiledArgs& 
   if (lane == 0) k = atomicAdd(counter, 1u);
   k = __shfl_sync(0xffffffffu, k, 0);
   if (k >= ntasks) return false;
+  t.k = k;
   t.q0 = a.dense_q0[k];
   const uint32_t cell = a.sorted_cell[t.q0];
   t.qn = min(32u, a.cell_start[cell + 1] - t.q0);
@@ -980,7 +998,7 @@ __device__ __forceinline__ void neighbour_offset(const StepConsts& c, int nb, fl
 // m_j poly6(r) over the 27 cells (world.rs:219-238), candidates in pairs on
 // f32x2 arithmetic (the filter of the tiled pass without the list).
 template <int TB, bool kCount, bool kExact>
-__global__ void __launch_bounds__(kWT, 5) k_density_dense(StepConsts c, TiledArgs a) {
+__global__ void __launch_bounds__(kWT, 4) k_density_dense(StepConsts c, TiledArgs a) {
   __shared__ __align__(16) float s_pp[kWarps][32 * 4];  // 32 candidates, pair-interleaved
   const int lane = threadIdx.x & 31;
   float* sp = s_pp[threadIdx.x >> 5];
@@ -997,6 +1015,16 @@ __global__ void __launch_bounds__(kWT, 5) k_density_dense(StepConsts c, TiledArg
     const Box3 qb = warp_box(q.x, q.y, q.z, qv);
     task_neighbours(c, a, t, qb, hc2);
     const f2 PX = f2_pack(q.x, q.x), PY = f2_pack(q.y, q.y), PZ = f2_pack(q.z, q.z);
+    // Mask entries: reserve the task's upper bound (one entry per chunk of
+    // every neighbour cell in reach).
+    uint32_t mbase = kNoMasks, mcount = 0;
+    if (a.mask_ctl) {
+      const uint32_t bound = __reduce_add_sync(0xffffffffu, (t.nb_e - t.nb_s + 31u) >> 5);
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(a.mask_ctl, (unsigned long long)bound);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base + bound <= a.mask_cap) mbase = (uint32_t)base;
+    }
     float s = 0.f, comp = 0.f;
     for (int nb = 0; nb < 27; ++nb) {
       const uint32_t s0 = __shfl_sync(0xffffffffu, t.nb_s, nb), e0 = __shfl_sync(0xffffffffu, t.nb_e, nb);
@@ -1017,6 +1045,9 @@ __global__ void __launch_bounds__(kWT, 5) k_density_dense(StepConsts c, TiledArg
         const uint32_t m = min(32u, e0 - cb);
         if (kCount && qv) cand += m;
         f2 NPART = f2_pack(0.f, 0.f);
+        // In-range bits as the force pass forms them (the sign of r^2 - hc2),
+        // the chunk's first candidate shifted in first.
+        uint32_t mask = 0;
 #pragma unroll 4
         for (uint32_t k = 0; k < 32u; k += 2) {
           if (k >= m) break;  // uniform; slot m of an odd m holds a far dummy
@@ -1038,18 +1069,34 @@ __global__ void __launch_bounds__(kWT, 5) k_density_dense(StepConsts c, TiledArg
             n1 = d1 < 0.f ? e1_ : 0.f;
           }
           if (kCount) pairs += (qv && d0 < 0.f ? 1u : 0u) + (qv && d1 < 0.f && k + 1 < m ? 1u : 0u);
+          mask = __funnelshift_l(__float_as_uint(d0), mask, 1);
+          mask = __funnelshift_l(__float_as_uint(d1), mask, 1);
           const f2 N = f2_pack(n0, n1);
           NPART = f2_fma(f2_mul(N, N), f2_mul(N, f2_pack(B.z, B.w)), NPART);
         }
         float p0, p1;
         f2_unpack(NPART, p0, p1);
         kahan_add(s, comp, c.poly6_cf * -(p0 + p1));
+        if (mbase != kNoMasks) {
+          // 2 ceil(m / 2) bits were shifted in (at least 2); bit k = candidate k.
+          const uint32_t used = (m + 1u) & ~1u;
+          const uint32_t bits = qv ? __brev(used < 32u ? mask << (32u - used) : mask) : 0u;
+          if (__any_sync(0xffffffffu, bits != 0u)) {
+            a.mask_bits[(size_t)(mbase + mcount) * 32u + (uint32_t)lane] = bits;
+            if (lane == 0) a.mask_hdr[mbase + mcount] = (cb << 5) | (uint32_t)nb;
+            ++mcount;
+          }
+        }
         __syncwarp();  // the chunk is consumed before the next one is staged
       }
     }
     if (qv) {
       write_density(c, a, (int)qi, (double)s - (double)comp);
       a.nbr_count[qi] = kNoList;
+    }
+    if (a.mask_ctl && lane == 0) {
+      a.task_mbase[t.k] = mbase;
+      a.task_mcount[t.k] = mcount;
     }
   }
   if (kCount) {
@@ -1063,12 +1110,12 @@ __global__ void __launch_bounds__(kWT, 5) k_density_dense(StepConsts c, TiledArg
 }
 
 // Forces, integration and bounds of the dense-cell particles: per chunk each
-// lane builds the mask of its in-range candidates (branch-free, candidates in
-// pairs on f32x2 arithmetic), then the warp walks the masks in lockstep for
-// as many rounds as the fullest mask has bits, each lane taking its own next
-// candidate through the pair terms of the tiled pass.  The partial sums are
-// folded into the compensated totals every 8 rounds and at the end of the
-// chunk, uniformly across the warp.
+// lane has the mask of its in-range candidates (kept by the density pass, or
+// built here branch-free, candidates in pairs on f32x2 arithmetic), then the
+// warp walks the masks in lockstep for as many rounds as the fullest mask has
+// bits, each lane taking its own next candidate through the pair terms of the
+// tiled pass.  The partial sums are folded into the compensated totals every
+// 8 rounds and at the end of the chunk, uniformly across the warp.
 template <int TB, bool kShear>
 __global__ void __launch_bounds__(kWT, 2) k_force_dense(StepConsts c, TiledArgs a) {
   __shared__ float4 s_pos[kWarps][32];
@@ -1087,83 +1134,122 @@ __global__ void __launch_bounds__(kWT, 2) k_force_dense(StepConsts c, TiledArgs 
     const uint32_t qi = t.q0 + (uint32_t)lane;
     const float4 qp = qv ? a.cpos[qi] : make_float4(kFar, kFar, kFar, 0.f);
     const float4 qvel = qv ? a.cvel[qi] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const Box3 qb = warp_box(qp.x, qp.y, qp.z, qv);
-    task_neighbours(c, a, t, qb, hc2);
     const float lapm = qp.w * c.lap_cf;
     const QueryPack Q = query_pack(c, qp, qvel, lapm);
     CompAcc acc;
     ForcePart part;
     ForcePart2 part2;
     zero(part2);
-    for (int nb = 0; nb < 27; ++nb) {
-      const uint32_t s0 = __shfl_sync(0xffffffffu, t.nb_s, nb), e0 = __shfl_sync(0xffffffffu, t.nb_e, nb);
-      if (s0 >= e0) continue;
-      float off[3];
-      neighbour_offset(c, nb, off);
-      for (uint32_t cb = s0; cb < e0; cb += 32) {
-        const uint32_t j = cb + (uint32_t)lane;
-        const bool cv = j < e0;
+    // The walk of one staged chunk given this lane's in-range bits (bit k =
+    // candidate k; zero for a lane without a query).
+    auto walk = [&](uint32_t mask) {
+      if (!kShear) {
+        // Two candidates per round; a lane out of candidates pads with a
+        // weightless copy of slot 0.
+        const int rounds = (int)(__reduce_max_sync(0xffffffffu, (unsigned)__popc(mask)) + 1) >> 1;
+        for (int r = 0; r < rounds; ++r) {
+          const bool ha = mask != 0;
+          const int ka = ha ? __ffs(mask) - 1 : 0;
+          mask &= mask - 1;
+          const bool hb = mask != 0;
+          const int kb = hb ? __ffs(mask) - 1 : 0;
+          mask &= mask - 1;
+          float4 pa = s_pos[w][ka], pb = s_pos[w][kb];
+          pa.w = ha ? pa.w : 0.f;
+          pb.w = hb ? pb.w : 0.f;
+          pair2_listed(Q, pa, s_vel[w][ka], ha ? s_mr[w][ka] : 0.f, pb, s_vel[w][kb], hb ? s_mr[w][kb] : 0.f,
+                       part2);
+          if ((r & 7) == 7) fold2(acc, part2);
+        }
+        if (rounds & 7) fold2(acc, part2);
+      } else {
+        const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(mask));
+        for (int r = 0; r < rounds; ++r) {
+          if (mask) {
+            const int k = __ffs(mask) - 1;
+            mask &= mask - 1;
+            pair_listed<kShear>(c, s_pos[w][k], s_vel[w][k], s_mr[w][k], qp, qvel, lapm, part, acc);
+          }
+          if ((r & 7) == 7) fold<kShear>(acc, part);
+        }
+        if (rounds & 7) fold<kShear>(acc, part);
+      }
+    };
+    const uint32_t mbase = a.task_mbase ? a.task_mbase[t.k] : kNoMasks;
+    if (mbase != kNoMasks) {
+      // The density pass's chunks, in its order; the next entry's header and
+      // mask are loaded while the current chunk is walked.
+      const uint32_t mcount = a.task_mcount[t.k];
+      uint32_t hdr = 0, bits = 0;
+      if (mcount) {
+        hdr = a.mask_hdr[mbase];
+        bits = a.mask_bits[(size_t)mbase * 32u + (uint32_t)lane];
+      }
+      for (uint32_t e = 0; e < mcount; ++e) {
+        const uint32_t h = hdr, mask = bits;
+        if (e + 1 < mcount) {
+          hdr = a.mask_hdr[mbase + e + 1];
+          bits = a.mask_bits[(size_t)(mbase + e + 1) * 32u + (uint32_t)lane];
+        }
+        // Only candidates some lane has in range are loaded; the other slots
+        // hold far dummies (never walked, finite for the padding).
+        const bool cv = ((__reduce_or_sync(0xffffffffu, mask) >> lane) & 1u) != 0u;
+        const uint32_t j = (h >> 5) + (uint32_t)lane;
+        float off[3];
+        neighbour_offset(c, (int)(h & 31u), off);
         float4 p = cv ? a.cpos[j] : make_float4(kFar, kFar, kFar, 0.f);
-        const Box3 bb = warp_box(p.x, p.y, p.z, cv);
-        if (boxes_apart(qb, bb, off, hc2)) continue;  // uniform
         p.x += off[0];
         p.y += off[1];
         p.z += off[2];
         s_pos[w][lane] = p;
-        put_pair_slot(sp, (uint32_t)lane, p);
         s_vel[w][lane] = cv ? a.cvel[j] : make_float4(0.f, 0.f, 0.f, 0.f);
         s_mr[w][lane] = cv ? a.cmr[j] : 0.f;
         __syncwarp();
-        // In-range bits (r^2 < hc2; the sign of r^2 - hc2, which is never -0),
-        // shifted in so that the chunk's first candidate ends in the highest
-        // bit; slots past the chunk hold far dummies (bit 0).
-        uint32_t mask = 0;
-#pragma unroll
-        for (uint32_t k = 0; k < 32u; k += 2) {
-          const float4 A = sp4[k];      // x0 x1 y0 y1
-          const float4 B = sp4[k + 1];  // z0 z1 m0 m1
-          const f2 DX = f2_sub(f2_pack(A.x, A.y), Q.px);
-          const f2 DY = f2_sub(f2_pack(A.z, A.w), Q.py);
-          const f2 DZ = f2_sub(f2_pack(B.x, B.y), Q.pz);
-          const f2 R2 = f2_fma(DZ, DZ, f2_fma(DY, DY, f2_mul(DX, DX)));
-          float d0, d1;
-          f2_unpack(f2_sub(R2, HC2), d0, d1);
-          mask = __funnelshift_l(__float_as_uint(d0), mask, 1);
-          mask = __funnelshift_l(__float_as_uint(d1), mask, 1);
-        }
-        mask = qv ? __brev(mask) : 0u;  // bit k = candidate k
-        if (!kShear) {
-          // Two candidates per round; a lane out of candidates pads with a
-          // weightless copy of slot 0.
-          const int rounds = (int)(__reduce_max_sync(0xffffffffu, (unsigned)__popc(mask)) + 1) >> 1;
-          for (int r = 0; r < rounds; ++r) {
-            const bool ha = mask != 0;
-            const int ka = ha ? __ffs(mask) - 1 : 0;
-            mask &= mask - 1;
-            const bool hb = mask != 0;
-            const int kb = hb ? __ffs(mask) - 1 : 0;
-            mask &= mask - 1;
-            float4 pa = s_pos[w][ka], pb = s_pos[w][kb];
-            pa.w = ha ? pa.w : 0.f;
-            pb.w = hb ? pb.w : 0.f;
-            pair2_listed(Q, pa, s_vel[w][ka], ha ? s_mr[w][ka] : 0.f, pb, s_vel[w][kb], hb ? s_mr[w][kb] : 0.f,
-                         part2);
-            if ((r & 7) == 7) fold2(acc, part2);
-          }
-          if (rounds & 7) fold2(acc, part2);
-        } else {
-          const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(mask));
-          for (int r = 0; r < rounds; ++r) {
-            if (mask) {
-              const int k = __ffs(mask) - 1;
-              mask &= mask - 1;
-              pair_listed<kShear>(c, s_pos[w][k], s_vel[w][k], s_mr[w][k], qp, qvel, lapm, part, acc);
-            }
-            if ((r & 7) == 7) fold<kShear>(acc, part);
-          }
-          if (rounds & 7) fold<kShear>(acc, part);
-        }
+        walk(mask);
         __syncwarp();  // the chunk is consumed before the next one is staged
+      }
+    } else {
+      const Box3 qb = warp_box(qp.x, qp.y, qp.z, qv);
+      task_neighbours(c, a, t, qb, hc2);
+      for (int nb = 0; nb < 27; ++nb) {
+        const uint32_t s0 = __shfl_sync(0xffffffffu, t.nb_s, nb), e0 = __shfl_sync(0xffffffffu, t.nb_e, nb);
+        if (s0 >= e0) continue;
+        float off[3];
+        neighbour_offset(c, nb, off);
+        for (uint32_t cb = s0; cb < e0; cb += 32) {
+          const uint32_t j = cb + (uint32_t)lane;
+          const bool cv = j < e0;
+          float4 p = cv ? a.cpos[j] : make_float4(kFar, kFar, kFar, 0.f);
+          const Box3 bb = warp_box(p.x, p.y, p.z, cv);
+          if (boxes_apart(qb, bb, off, hc2)) continue;  // uniform
+          p.x += off[0];
+          p.y += off[1];
+          p.z += off[2];
+          s_pos[w][lane] = p;
+          put_pair_slot(sp, (uint32_t)lane, p);
+          s_vel[w][lane] = cv ? a.cvel[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+          s_mr[w][lane] = cv ? a.cmr[j] : 0.f;
+          __syncwarp();
+          // In-range bits (r^2 < hc2; the sign of r^2 - hc2, which is never
+          // -0), shifted in so that the chunk's first candidate ends in the
+          // highest bit; slots past the chunk hold far dummies (bit 0).
+          uint32_t mask = 0;
+#pragma unroll
+          for (uint32_t k = 0; k < 32u; k += 2) {
+            const float4 A = sp4[k];      // x0 x1 y0 y1
+            const float4 B = sp4[k + 1];  // z0 z1 m0 m1
+            const f2 DX = f2_sub(f2_pack(A.x, A.y), Q.px);
+            const f2 DY = f2_sub(f2_pack(A.z, A.w), Q.py);
+            const f2 DZ = f2_sub(f2_pack(B.x, B.y), Q.pz);
+            const f2 R2 = f2_fma(DZ, DZ, f2_fma(DY, DY, f2_mul(DX, DX)));
+            float d0, d1;
+            f2_unpack(f2_sub(R2, HC2), d0, d1);
+            mask = __funnelshift_l(__float_as_uint(d0), mask, 1);
+            mask = __funnelshift_l(__float_as_uint(d1), mask, 1);
+          }
+          walk(qv ? __brev(mask) : 0u);
+          __syncwarp();  // the chunk is consumed before the next one is staged
+        }
       }
     }
     if (qv) finish_particle(c, a, (int)qi, acc, c.boxes[t.cg.sc]);
@@ -1279,6 +1365,13 @@ void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const
   a.dense_count = b.queue + 2;
   a.dense_taken = b.queue + 3;
   a.dense_q0 = b.dense_q0;
+  const bool masks = t.dense_masks && b.mask_ctl != nullptr;
+  a.task_mbase = masks ? b.task_mbase : nullptr;
+  a.task_mcount = b.task_mcount;
+  a.mask_hdr = b.mask_hdr;
+  a.mask_bits = b.mask_bits;
+  a.mask_ctl = masks ? b.mask_ctl : nullptr;
+  a.mask_cap = b.mask_cap;
   a.stride = b.capacity;
   a.flags = b.flags;
   a.counters = b.counters;
@@ -1293,10 +1386,14 @@ void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const
   if (ev.after_prep) cudaEventRecord(ev.after_prep, s);
   const int dense_d_blocks = o.sms * o.dense_density, dense_f_blocks = o.sms * o.dense_force;
   const bool exact = std::min(c.h2f, c.h0sqf) == c.h0sqf;
+  if (masks) cudaMemsetAsync(b.mask_ctl, 0, sizeof(unsigned long long), s);
   if (c.tile == 2)
     launch_passes<2>(c, a, s, ev, exact, density_blocks, force_blocks, dense_d_blocks, dense_f_blocks);
   else
     launch_passes<4>(c, a, s, ev, exact, density_blocks, force_blocks, dense_d_blocks, dense_f_blocks);
+  // The entries this step's tasks asked for, for the host's next sizing.
+  if (masks && b.mask_demand)
+    cudaMemcpyAsync(b.mask_demand, b.mask_ctl, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
 }
 
 }  // namespace phy

@@ -365,10 +365,18 @@ class FluidWorld:
         L.check(self._lib.phy_fluid_step_counters(self._h, self._sub, out), "phy_fluid_step_counters")
         return {"candidates": out[0], "pairs": out[1], "particles": out[2], "cells": out[3]}
 
+    def dense_mask_info(self) -> dict:
+        """The dense-cell mask buffer (phy_fluid_dense_mask_info): entries allocated and the
+        entries the last step's dense-cell tasks reserved."""
+        out = (C.c_uint64 * 2)()
+        L.check(self._lib.phy_fluid_dense_mask_info(self._h, self._sub, out), "phy_fluid_dense_mask_info")
+        return {"capacity": out[0], "demand": out[1]}
+
     def set_tuning(self, **knobs: int) -> None:
         """Kernel configuration (phy_fluid_set_tuning): comp_tile, halo_cap, ctas_per_sm, queue,
-        sort_block, graph_chunk.  Results of the f64 form never change; the launch knobs
-        (ctas_per_sm, queue, sort_block, graph_chunk) change no result of either form."""
+        sort_block, graph_chunk, dense_mean, dense_masks.  Results of the f64 form never
+        change; the launch knobs (ctas_per_sm, queue, sort_block, graph_chunk, dense_masks)
+        change no result of either form."""
         for name, value in knobs.items():
             if name not in L.TUNE_PARAMS:
                 raise ValueError(f"unknown tuning parameter {name!r}")

@@ -327,10 +327,13 @@ def _compounds(shift=0.0):
         {"shape": "compound", "pos": (0.1 + shift, 0.05, 0.0), "rot": _quat((0, 1, 1), 0.5), "vel": (0.1, -0.3, 0.0),
          "inv_mass": 1.5,
          "subs": [{"shape": "sphere", "size": (0.15,), "offset": (0.2, 0.0, 0.0)},
-                  {"shape": "box", "size": (0.1, 0.2, 0.08), "offset": (-0.15, 0.05, 0.0), "rot": _quat((1, 0, 0), 0.9)},
-                  {"shape": "capsule", "size": (0.12, 0.06), "offset": (0.0, -0.2, 0.1), "rot": _quat((0, 0, 1), 1.3)}]},
+                  {"shape": "box", "size": (0.1, 0.2, 0.08), "offset": (-0.15, 0.05, 0.0),
+                   "rot": _quat((1, 0, 0), 0.9)},
+                  {"shape": "capsule", "size": (0.12, 0.06), "offset": (0.0, -0.2, 0.1),
+                   "rot": _quat((0, 0, 1), 1.3)}]},
         {"shape": "compound", "pos": (-0.3, -0.25, 0.2), "inv_mass": 0.0,
-         "subs": [{"shape": "box", "size": (0.2, 0.05, 0.2)}, {"shape": "sphere", "size": (0.1,), "offset": (0, 0.1, 0)}]},
+         "subs": [{"shape": "box", "size": (0.2, 0.05, 0.2)},
+                  {"shape": "sphere", "size": (0.1,), "offset": (0, 0.1, 0)}]},
         {"shape": "compound", "pos": (0.25, 0.25, 0.25), "rot": _quat((1, -1, 0), 0.4), "inv_mass": 3.0,
          "subs": [{"shape": "convex", **TETRA, "offset": (0.05, 0.0, 0.0), "rot": _quat((0, 1, 0), 0.3)},
                   {"shape": "heightfield", "size": (2, 2, 0.3), "heights": [0.1, 0.2, -0.1, 0.05],

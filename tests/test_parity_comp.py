@@ -310,3 +310,29 @@ def test_tiled_shear_thinning_and_thickening(gpu, oracle_mod, visc_n):
     e["mu_rel"] = float(np.max(np.abs(w.mu_eff - mu_o) / np.abs(mu_o)))
     print("tiled shear", visc_n, e)
     assert e["rho_rel"] <= RHO_TOL and e["acc_rel_to_max"] <= 1e-3 and e["mu_rel"] <= 1e-4, e
+
+
+@pytest.mark.parametrize("tile,visc_n", [(4, 1.0), (2, 1.0), (4, 0.7)])
+def test_dense_masks_change_no_bit(gpu, tile, visc_n):
+    """The dense-cell force pass walking the in-range masks the density pass kept gives the
+    bits of the force pass that filters the candidates again, over several steps (the first
+    step sizes the mask buffer; the host read after each step makes the next one see it)."""
+    p = ref_test_params(gravity=(0.0, -9.81, 0.0))
+    p.bounds_min, p.bounds_max = (0.0, 0.0, 0.0), (1.6, 1.6, 1.6)
+    p.visc_n = [visc_n]
+    pos, vel = _sheet_scene(400, 21)
+    worlds = []
+    for masks in (1, 0):
+        w = gpu.FluidWorld(p, "comp")
+        w.set_tuning(comp_tile=tile, dense_masks=masks)
+        w.add_particles(pos, 0.02, vel=vel)
+        for _ in range(4):
+            w.step(0.001)
+            w.pos  # a host read between steps
+        worlds.append(w)
+    info = worlds[0].dense_mask_info()
+    print("dense masks", tile, visc_n, info)
+    assert info["demand"] > 0 and info["capacity"] >= info["demand"], info
+    assert worlds[1].dense_mask_info()["capacity"] == 0
+    for name in ("pos", "vel", "rho", "p", "acc", "mu_eff"):
+        assert_bits_equal(getattr(worlds[0], name), getattr(worlds[1], name), name)
