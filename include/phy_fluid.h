@@ -244,9 +244,11 @@ int32_t phy_fluid_set_counting(PhyWorldHandle *w, uint32_t sub, int32_t on);
 int32_t phy_fluid_step_counters(PhyWorldHandle *w, uint32_t sub, uint64_t *out4);
 
 /* The dense-cell mask buffer of `sub` (PHY_TUNE_DENSE_MASKS), after waiting
- * for its stream: out2 = {entries allocated, entries the dense-cell tasks of
- * the last step reserved}.  An entry is one chunk of 32 candidates (33 u32). */
-int32_t phy_fluid_dense_mask_info(PhyWorldHandle *w, uint32_t sub, uint64_t *out2);
+ * for its stream: out3 = {entries allocated, entries the dense-cell tasks of
+ * the last step reserved, 1 when the last step's force pass found a task's
+ * kept masks outside the buffer (it filtered that task again) else 0}.  An
+ * entry is one chunk of 32 candidates (33 u32). */
+int32_t phy_fluid_dense_mask_info(PhyWorldHandle *w, uint32_t sub, uint64_t *out3);
 
 /* Per-phase device timing of `sub` with CUDA events on its stream.  While on,
  * every step records five events without waiting for them (steps are then
@@ -278,8 +280,9 @@ int32_t phy_fluid_phase_times(PhyWorldHandle *w, uint32_t sub, double *out5, int
  *                         dt, the particle set or a buffer change);
  *   PHY_TUNE_DENSE_MASKS  1 = the dense-cell force pass walks the in-range
  *                         masks the density pass kept (default; the buffer
- *                         grows with the tasks' demand, within half the free
- *                         device memory), 0 = it filters the candidates again.
+ *                         grows with the tasks' demand, within a quarter of
+ *                         the free device memory and 16 GiB), 0 = it filters
+ *                         the candidates again.
  * phy_fluid_get_tuning reads the same parameters. */
 enum {
   PHY_TUNE_COMP_TILE = 0,

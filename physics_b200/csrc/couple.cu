@@ -14,10 +14,12 @@
 //   * a point outside the bounds is skipped and its force left unwritten.
 //
 // One CTA walks the points in order.  Per point, its candidates are staged
-// through shared memory by all threads and summed in visit order by one
-// thread (the reference's sequential sums); the reaction is then applied by
-// all threads in parallel (every fluid particle lies in one cell, so the
-// updates are disjoint).
+// through shared memory and summed in visit order by one thread (the
+// reference's sequential sums); the reaction is then applied in parallel
+// (every fluid particle lies in one cell, so the updates are disjoint).
+// Consecutive points whose neighbourhoods are pairwise disjoint run at once,
+// one warp each (k_couple_points_grouped); k_couple_points is the one-point-
+// at-a-time form, used when the grouped walk's shared memory is unavailable.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -160,50 +162,65 @@ __global__ void __launch_bounds__(kCT) k_couple_points(StepConsts c, CoupleArgs 
   }
 }
 
-// Pipelined form of the same walk.  Only velocities change from one point to
+// Grouped form of the same walk.  Only velocities change from one point to
 // the next, so everything else is prepared in parallel first: one warp per
-// point finds its 27 cell ranges (k_point_tables), and, after a prefix sum of
-// the candidate counts, writes its candidates' particle indices and masses
-// in visit order (k_point_candidates).  The ordered walk (one CTA) then reads
-// those lists two points ahead: while thread 0 runs point k's ordered f64
-// sums, warps 1..4 gather point k+1's velocities and the products v_j m_j
-// into shared memory while warps 5..7 load point k+2's table and list.  Point k's reaction can
-// change only the velocities of particles in point k's own cells, so after
-// it the candidates of point k+1 in cells that point k shares are gathered
-// again (points far apart share none).  The ordered sums read ready products
-// (sx + v m with the product formed once: the same f64 operations), and the
-// reaction reuses the gathered velocities (v_j + share).  Points with more
-// than kPB candidates take a chunked walk through their cells.
-constexpr int kPB = 1024;   // candidates a point may have for the pipelined walk
-constexpr int kTabU = 56;   // u32 per point table: in, total, beg[27], cnt[27]
+// point finds its 27 cell ranges and whether its neighbourhood overlaps those
+// of the kGW - 1 points before it (k_point_tables), and, after a prefix sum
+// of the candidate counts, writes its candidates' particle indices and masses
+// in visit order (k_point_candidates).  Two points whose centre cells are
+// more than 2 apart on some axis have disjoint 27-cell neighbourhoods, so
+// they read and write disjoint particles: a run of consecutive points that
+// are pairwise disjoint (a group) gives the same velocities and forces
+// whether its points run one after another or at once.  The walk (one CTA)
+// takes the groups in order and runs a group's points at once, one warp
+// each: the lanes stage the candidates' products v_j m_j in the warp's
+// shared buffer (the same f64 products), lane 0 adds them in visit order
+// (the reference's sequential sums), and the lanes apply the reaction to the
+// candidates they hold (v_j + share, with the velocities they gathered).
+// Points with more than kPB candidates have no list and read their
+// candidates through their cell table.
+constexpr int kGW = 8;          // warps of the walk: points per group at most
+constexpr int kPer = 16;        // candidates a lane holds per chunk
+constexpr int kWB = 32 * kPer;  // candidates per chunk of a warp
+constexpr int kPB = 4096;       // candidates a point may have for a list
+constexpr int kTabU = 56;       // u32 per point table: in, total, beg[27], cnt[27]
 
-struct PointTable {
-  uint32_t beg[27];
-  uint32_t cnt[27];
-  uint32_t pre[28];
-  uint32_t again;  // bit u: cell u is also a cell of the previous point
-  int in;
-  __device__ bool fits() const { return in && pre[27] <= (uint32_t)kPB; }
-};
+// world.rs:704-711 (a NaN coordinate passes, as there).
+__device__ __forceinline__ bool point_in(const StepConsts& c, const double* q) {
+  const double x = q[0], y = q[1], z = q[2];
+  return !(x < c.lo[0] || x > c.hi[0] || y < c.lo[1] || y > c.hi[1] || z < c.lo[2] || z > c.hi[2]);
+}
 
-// One warp per point: in-bounds flag, candidate count and cell ranges.
-__global__ void __launch_bounds__(256) k_point_tables(StepConsts c, CoupleArgs a, int p0, int nb, uint32_t* tab,
-                                                      uint32_t* totals) {
+// One warp per point w of the batch: in-bounds flag, candidate count and
+// cell ranges, and conf[w]: bit m (1 <= m < kGW) when the neighbourhood of
+// point w overlaps that of point w - m (both in bounds, centre cells at most
+// 2 apart on every axis).
+__global__ void __launch_bounds__(256) k_point_tables(StepConsts c, CoupleArgs a, int nb, uint32_t* tab,
+                                                      uint32_t* totals, uint8_t* conf) {
   const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (w >= nb) return;
-  const double* q = a.pts + 10 * (size_t)(p0 + w);
-  const double x = q[0], y = q[1], z = q[2];
-  // world.rs:704-711 (a NaN coordinate passes, as there).
-  const bool in = !(x < c.lo[0] || x > c.hi[0] || y < c.lo[1] || y > c.hi[1] || z < c.lo[2] || z > c.hi[2]);
+  const double* q = a.pts + 10 * (size_t)w;
+  const bool in = point_in(c, q);
+  const long long kx = key_axis(q[0], c.inv_cell), ky = key_axis(q[1], c.inv_cell),
+                  kz = key_axis(q[2], c.inv_cell);
   uint32_t beg = 0, cnt = 0;
   if (in && lane < 27) {
-    const long long kx = key_axis(x, c.inv_cell), ky = key_axis(y, c.inv_cell), kz = key_axis(z, c.inv_cell);
     const int lin = cell_linear(c, kx + lane / 9 - 1, ky + (lane / 3) % 3 - 1, kz + lane % 3 - 1);
     if (lin >= 0) {
       beg = a.cell_start[lin];
       cnt = a.cell_start[lin + 1] - beg;
     }
   }
+  bool overlap = false;
+  if (in && lane >= 1 && lane < kGW && w - lane >= 0) {
+    const double* p = a.pts + 10 * (size_t)(w - lane);
+    if (point_in(c, p)) {
+      const long long dx = key_axis(p[0], c.inv_cell) - kx, dy = key_axis(p[1], c.inv_cell) - ky,
+                      dz = key_axis(p[2], c.inv_cell) - kz;
+      overlap = dx >= -2 && dx <= 2 && dy >= -2 && dy <= 2 && dz >= -2 && dz <= 2;
+    }
+  }
+  const uint32_t bits = __ballot_sync(0xffffffffu, overlap);
   const uint32_t total = __reduce_add_sync(0xffffffffu, cnt);
   uint32_t* t = tab + (size_t)w * kTabU;
   if (lane < 27) {
@@ -214,11 +231,13 @@ __global__ void __launch_bounds__(256) k_point_tables(StepConsts c, CoupleArgs a
     t[0] = in ? 1u : 0u;
     t[1] = total;
     totals[w] = in && total <= (uint32_t)kPB ? total : 0u;
+    conf[w] = (uint8_t)bits;
   }
 }
 
-// One warp per point: the candidates of a point that fits, in visit order
-// (cell after cell, ascending slot: ascending insertion index), from off[w].
+// One warp per point: the candidates of a point that has a list, in visit
+// order (cell after cell, ascending slot: ascending insertion index), from
+// off[w].
 __global__ void __launch_bounds__(256) k_point_candidates(CoupleArgs a, int nb, const uint32_t* tab,
                                                           const uint32_t* off, uint32_t* idx, double* m) {
   const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
@@ -242,187 +261,71 @@ struct PointLists {
   const uint32_t* off;
   const uint32_t* idx;
   const double* m;
+  const uint8_t* conf;
 };
 
-// Staged data of one point: particle indices and masses (three buffers),
-// velocities and products (two buffers).
-struct PointBuf {
-  uint32_t* idx;  // [kPB]
-  double* m;      // [kPB]
-};
-struct VelBuf {
-  double* v;    // [3][kPB]
-  double2* pw;  // [2 kPB]: (v_x m, v_y m), (v_z m, m) per candidate
+// Cell table of a point without a list (its warp's copy).
+struct WarpTable {
+  uint32_t beg[27];
+  uint32_t pre[28];
 };
 
-__device__ __forceinline__ PointBuf point_buf(unsigned char* smem, int q) {
-  double* m = reinterpret_cast<double*>(smem);                     // [3][kPB]
-  uint32_t* idx = reinterpret_cast<uint32_t*>(m + 3 * kPB);        // [3][kPB]
-  return {idx + q * kPB, m + q * kPB};
-}
-__device__ __forceinline__ VelBuf vel_buf(unsigned char* smem, int q) {
-  double* v = reinterpret_cast<double*>(smem) + 3 * kPB + 3 * kPB / 2;  // after m and idx (16-byte aligned)
-  double2* pw = reinterpret_cast<double2*>(v + 6 * kPB);               // [2][2 kPB]
-  return {v + 3 * q * kPB, pw + 2 * q * kPB};
-}
-
-// One warp: the cell table of point j (a word per lane, prefix sums by a
-// warp scan).
-__device__ __forceinline__ void load_table(const PointLists& L, int j, PointTable& T) {
+// One warp: all of point j's work in the walk.  `pw` is the warp's buffer of
+// 2 kWB products, `r` its reaction and mass sum.
+__device__ __forceinline__ void walk_point(const StepConsts& c, const CoupleArgs& a, const PointLists& L, int j,
+                                           double2* pw, WarpTable& T, double* r) {
   const int lane = threadIdx.x & 31;
   const uint32_t* t = L.tab + (size_t)j * kTabU;
-  const uint32_t beg = lane < 27 ? t[2 + lane] : 0u, cnt = lane < 27 ? t[29 + lane] : 0u;
-  uint32_t incl = cnt;
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
-  }
-  if (lane < 27) {
-    T.beg[lane] = beg;
-    T.cnt[lane] = cnt;
-    T.pre[lane] = incl - cnt;
-  }
-  if (lane == 26) T.pre[27] = incl;
-  if (lane == 0) T.in = (int)t[0];
-}
-
-// Threads t0.. (stride nt): the candidate list of point j (when it fits) into
-// buffer B; independent of the table in shared memory.
-__device__ __forceinline__ void load_list(const PointLists& L, int j, const PointBuf& B, int t0, int nt) {
-  const uint32_t* t = L.tab + (size_t)j * kTabU;
-  if (t[0] && t[1] <= (uint32_t)kPB) {
-    const uint32_t o = L.off[j], total = t[1];
-    for (uint32_t e = (uint32_t)((int)threadIdx.x - t0); e < total; e += (uint32_t)nt) {
-      B.idx[e] = L.idx[o + e];
-      B.m[e] = L.m[o + e];
+  if (!t[0]) return;  // outside the bounds: skipped, force left unwritten
+  const uint32_t total = t[1];
+  const bool listed = total <= (uint32_t)kPB;
+  const uint32_t o = listed ? L.off[j] : 0u;
+  if (!listed) {
+    const uint32_t beg = lane < 27 ? t[2 + lane] : 0u, cnt = lane < 27 ? t[29 + lane] : 0u;
+    uint32_t incl = cnt;
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += v;
     }
-  }
-}
-
-// Table and list of point j by all threads (the prologue).
-__device__ __forceinline__ void load_point(const PointLists& L, int j, PointTable& T, const PointBuf& B) {
-  if ((threadIdx.x >> 5) == 0) load_table(L, j, T);
-  load_list(L, j, B, 0, kCT);
-}
-
-// Warps 5..7 during the walk: table and list of point j.
-__device__ __forceinline__ void load_ahead(const PointLists& L, int j, PointTable& T, const PointBuf& B) {
-  if ((threadIdx.x >> 5) == 5) load_table(L, j, T);
-  load_list(L, j, B, 5 * 32, kCT - 5 * 32);
-}
-
-__device__ __forceinline__ void gather_candidate(const CoupleArgs& a, const PointBuf& B, const VelBuf& V,
-                                                 uint32_t e) {
-  const uint32_t i = B.idx[e];
-  const double m = B.m[e];
-  const double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i];
-  V.v[e] = vx;
-  V.v[kPB + e] = vy;
-  V.v[2 * kPB + e] = vz;
-  V.pw[2 * e] = make_double2(vx * m, vy * m);
-  V.pw[2 * e + 1] = make_double2(vz * m, m);
-}
-
-// Warps 1..4: velocities of point j (its list already staged) and, when
-// `prev` (the previous point, reaction not yet applied) is given, the cells
-// the two share.
-constexpr int kGatherThreads = 4 * 32;
-__device__ __forceinline__ void gather_point(const CoupleArgs& a, PointTable& T, const PointTable* prev,
-                                             const PointBuf& B, const VelBuf& V) {
-  if ((threadIdx.x >> 5) == 1) {
-    const int lane = threadIdx.x & 31;
-    bool shared = false;
-    if (prev && prev->in && lane < 27 && T.cnt[lane] > 0)
-      for (int u = 0; u < 27; ++u) shared = shared || (prev->cnt[u] > 0 && prev->beg[u] == T.beg[lane]);
-    const uint32_t bits = __ballot_sync(0xffffffffu, shared);
-    if (lane == 0) T.again = bits;
-  }
-  for (uint32_t e = threadIdx.x - 32; e < T.pre[27]; e += kGatherThreads) gather_candidate(a, B, V, e);
-}
-
-__global__ void __launch_bounds__(kCT) k_couple_points_piped(StepConsts c, CoupleArgs a, int p0, int nb,
-                                                             PointLists L) {
-  __shared__ PointTable s_tab[3];
-  __shared__ double s_r[4];  // reaction xyz, sum of masses
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int t = threadIdx.x, warp = t >> 5;
-  // Prologue: lists of points 0 and 1, velocities of point 0.
-  if (nb > 0) load_point(L, 0, s_tab[0], point_buf(smem, 0));
-  if (nb > 1) load_point(L, 1, s_tab[1], point_buf(smem, 1));
-  __syncthreads();
-  if (nb > 0 && s_tab[0].fits()) {
-    if (t == 32) s_tab[0].again = 0;
-    if (warp >= 1)
-      for (uint32_t e = t - 32; e < s_tab[0].pre[27]; e += kCT - 32)
-        gather_candidate(a, point_buf(smem, 0), vel_buf(smem, 0), e);
-  }
-  __syncthreads();
-  for (int j = 0; j < nb; ++j) {
-    const int r3 = j % 3, n3 = (j + 1) % 3, f3 = (j + 2) % 3, r2 = j & 1, n2 = r2 ^ 1;
-    const PointTable& T = s_tab[r3];
-    const PointBuf B = point_buf(smem, r3);
-    const VelBuf V = vel_buf(smem, r2);
-    double* q = a.pts + 10 * (size_t)(p0 + j);
-    const bool has1 = j + 1 < nb, has2 = j + 2 < nb;
-    const uint32_t total = T.in ? T.pre[27] : 0u;
-    if (!T.fits()) {
-      if (T.in) {
-        // Chunked walk through the cells: candidates staged kPB at a time.
-        double sx = 0.0, sy = 0.0, sz = 0.0, sw = 0.0;
-        for (uint32_t base = 0; base < total; base += kPB) {
-          const uint32_t cnt = min((uint32_t)kPB, total - base);
-          for (uint32_t e = t; e < cnt; e += kCT) {
-            const uint32_t i = candidate(a, T.beg, T.pre, base + e);
-            V.v[e] = a.vx[i];
-            V.v[kPB + e] = a.vy[i];
-            V.v[2 * kPB + e] = a.vz[i];
-            B.m[e] = a.mass[i];
-          }
-          __syncthreads();
-          if (t == 0)
-#pragma unroll 8
-            for (uint32_t e = 0; e < cnt; ++e) {
-              const double w = B.m[e];
-              sx = sx + V.v[e] * w;
-              sy = sy + V.v[kPB + e] * w;
-              sz = sz + V.v[2 * kPB + e] * w;
-              sw = sw + w;
-            }
-          __syncthreads();
-        }
-        if (t == 0) point_force(c, a, q, sx, sy, sz, sw, s_r);
-        __syncthreads();
-        const double msum = s_r[3];
-        if (msum > 0.0)
-          for (uint32_t flat = t; flat < total; flat += kCT) {
-            const uint32_t i = candidate(a, T.beg, T.pre, flat);
-            const double frac = a.mass[i] / msum;
-            a.vx[i] = a.vx[i] + s_r[0] * frac;
-            a.vy[i] = a.vy[i] + s_r[1] * frac;
-            a.vz[i] = a.vz[i] + s_r[2] * frac;
-          }
-      }
-      __syncthreads();
-      // Point j's reaction is applied: point j+1's velocities are final.
-      if (warp >= 1 && warp <= 4) {
-        if (has1 && s_tab[n3].fits()) gather_point(a, s_tab[n3], nullptr, point_buf(smem, n3), vel_buf(smem, n2));
-      } else if (warp >= 5 && has2) {
-        load_ahead(L, j + 2, s_tab[f3], point_buf(smem, f3));
-      }
-      __syncthreads();
-      continue;
+    if (lane < 27) {
+      T.beg[lane] = beg;
+      T.pre[lane] = incl - cnt;
     }
-    if (t == 0) {
+    if (lane == 26) T.pre[27] = incl;
+    __syncwarp();
+  }
+  double sx = 0.0, sy = 0.0, sz = 0.0, sw = 0.0;  // lane 0's sums
+  uint32_t ci[kPer];
+  double cm[kPer], cx[kPer], cy[kPer], cz[kPer];
+  for (uint32_t base = 0; base < total; base += kWB) {
+    const uint32_t cnt = min((uint32_t)kWB, total - base);
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const uint32_t e = (uint32_t)lane + 32u * k;
+      if (e < cnt) {
+        const uint32_t i = listed ? L.idx[o + base + e] : candidate(a, T.beg, T.pre, base + e);
+        const double m = listed ? L.m[o + base + e] : a.mass[i];
+        const double vx = a.vx[i], vy = a.vy[i], vz = a.vz[i];
+        pw[2 * e] = make_double2(vx * m, vy * m);
+        pw[2 * e + 1] = make_double2(vz * m, m);
+        ci[k] = i;
+        cm[k] = m;
+        cx[k] = vx;
+        cy[k] = vy;
+        cz[k] = vz;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
       // Eight candidates' products are loaded before they are added, so the
       // loads overlap while the four sums still add in candidate order.
-      double sx = 0.0, sy = 0.0, sz = 0.0, sw = 0.0;
       uint32_t e = 0;
-      for (; e + 8 <= total; e += 8) {
+      for (; e + 8 <= cnt; e += 8) {
         double2 P[8], R[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-          P[u] = V.pw[2 * (e + u)];
-          R[u] = V.pw[2 * (e + u) + 1];
+          P[u] = pw[2 * (e + u)];
+          R[u] = pw[2 * (e + u) + 1];
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
@@ -432,45 +335,75 @@ __global__ void __launch_bounds__(kCT) k_couple_points_piped(StepConsts c, Coupl
           sw = sw + R[u].y;
         }
       }
-      for (; e < total; ++e) {
-        const double2 p = V.pw[2 * e], r = V.pw[2 * e + 1];
-        sx = sx + p.x;
-        sy = sy + p.y;
-        sz = sz + r.x;
-        sw = sw + r.y;
+      for (; e < cnt; ++e) {
+        const double2 P = pw[2 * e], R = pw[2 * e + 1];
+        sx = sx + P.x;
+        sy = sy + P.y;
+        sz = sz + R.x;
+        sw = sw + R.y;
       }
-      point_force(c, a, q, sx, sy, sz, sw, s_r);
-    } else if (warp >= 1 && warp <= 4) {
-      if (has1 && s_tab[n3].fits()) gather_point(a, s_tab[n3], &T, point_buf(smem, n3), vel_buf(smem, n2));
-    } else if (warp >= 5 && has2) {
-      load_ahead(L, j + 2, s_tab[f3], point_buf(smem, f3));
     }
-    __syncthreads();
-    const double msum = s_r[3];
-    if (msum > 0.0)
-      for (uint32_t e = t; e < total; e += kCT) {
-        const uint32_t i = B.idx[e];
-        const double frac = B.m[e] / msum;
-        a.vx[i] = V.v[e] + s_r[0] * frac;
-        a.vy[i] = V.v[kPB + e] + s_r[1] * frac;
-        a.vz[i] = V.v[2 * kPB + e] + s_r[2] * frac;
+    __syncwarp();  // the chunk is summed before the next one is staged
+  }
+  if (lane == 0) point_force(c, a, a.pts + 10 * (size_t)j, sx, sy, sz, sw, r);
+  __syncwarp();
+  const double msum = r[3];
+  if (!(msum > 0.0)) return;
+  const double rx = r[0], ry = r[1], rz = r[2];
+  if (total <= (uint32_t)kWB) {
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const uint32_t e = (uint32_t)lane + 32u * k;
+      if (e < total) {
+        const double frac = cm[k] / msum;
+        a.vx[ci[k]] = cx[k] + rx * frac;
+        a.vy[ci[k]] = cy[k] + ry * frac;
+        a.vz[ci[k]] = cz[k] + rz * frac;
       }
-    __syncthreads();
-    // The next point's candidates in cells this point shares took its
-    // reaction: gather them again.
-    if (has1 && s_tab[n3].fits() && s_tab[n3].again) {
-      const PointTable& N = s_tab[n3];
-      const PointBuf NB = point_buf(smem, n3);
-      const VelBuf NV = vel_buf(smem, n2);
-      for (int u = 0; u < 27; ++u)
-        if (N.again >> u & 1u)
-          for (uint32_t e = N.pre[u] + t; e < N.pre[u + 1]; e += kCT) gather_candidate(a, NB, NV, e);
-      __syncthreads();
+    }
+  } else {
+    for (uint32_t e = lane; e < total; e += 32) {
+      const uint32_t i = listed ? L.idx[o + e] : candidate(a, T.beg, T.pre, e);
+      const double frac = (listed ? L.m[o + e] : a.mass[i]) / msum;
+      a.vx[i] = a.vx[i] + rx * frac;
+      a.vy[i] = a.vy[i] + ry * frac;
+      a.vz[i] = a.vz[i] + rz * frac;
     }
   }
 }
 
-constexpr size_t kPipedSmem = (size_t)kPB * (3 * 8 + 3 * 4 + 2 * 3 * 8 + 2 * 2 * 16);
+// The walk over the nb points of a batch: group after group, a group being
+// the longest run (at most kGW) of points after its first whose
+// neighbourhoods overlap none of the run's earlier points.
+__global__ void __launch_bounds__(kGW * 32, 1) k_couple_points_grouped(StepConsts c, CoupleArgs a, int nb,
+                                                                       PointLists L) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double2* s_pw = reinterpret_cast<double2*>(smem);                    // [kGW][2 kWB]
+  uint8_t* s_conf = reinterpret_cast<uint8_t*>(s_pw + 2 * kWB * kGW);  // [nb]
+  __shared__ WarpTable s_tab[kGW];
+  __shared__ double s_r[kGW][4];
+  __shared__ int s_group;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int k = threadIdx.x; k < nb; k += kGW * 32) s_conf[k] = L.conf[k];
+  __syncthreads();
+  for (int j = 0; j < nb;) {
+    if (warp == 0) {
+      // Lane l < kGW stops the group before point j + l when that point
+      // overlaps one of j .. j + l - 1 (conf bits 1..l) or is past the batch.
+      bool stop = false;
+      if (lane >= 1 && lane < kGW) stop = j + lane >= nb || (s_conf[j + lane] & ((2u << lane) - 1u)) != 0u;
+      const uint32_t b = __ballot_sync(0xffffffffu, stop) | (1u << kGW);
+      if (lane == 0) s_group = __ffs((int)(b >> 1));
+    }
+    __syncthreads();
+    const int g = s_group;
+    if (warp < g) walk_point(c, a, L, j + warp, s_pw + (size_t)warp * 2 * kWB, s_tab[warp], s_r[warp]);
+    __syncthreads();  // the group's reactions are applied before the next group gathers
+    j += g;
+  }
+}
+
+constexpr size_t kGroupedSmemFixed = (size_t)kGW * 2 * kWB * sizeof(double2);
 
 // ---- couple_heat (world.rs:555-678) ------------------------------------------------
 //
@@ -1123,7 +1056,9 @@ void CouplePointsScratch::release() {
   }
   if (m) cudaFree(m);
   m = nullptr;
-  cap_tab = cap_totals = cap_off = cap_idx = cap_m = 0;
+  if (conf) cudaFree(conf);
+  conf = nullptr;
+  cap_tab = cap_totals = cap_off = cap_idx = cap_m = cap_conf = 0;
 }
 
 void launch_couple_points(const StepConsts& c, DevBuffers& b, double* d_pts, int np, double dt, double drag,
@@ -1140,17 +1075,17 @@ void launch_couple_points(const StepConsts& c, DevBuffers& b, double* d_pts, int
   a.dt = dt;
   a.drag = drag;
   a.soft_density = soft_density;
+  // Points run in batches (one ordered walk per batch, in order on the
+  // stream), which bounds the candidate lists and the walk's shared memory.
+  constexpr int kBatch = 16384;
   static const bool smem_ok = [] {
-    return cudaFuncSetAttribute(k_couple_points_piped, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kPipedSmem) == cudaSuccess;
+    return cudaFuncSetAttribute(k_couple_points_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(kGroupedSmemFixed + kBatch)) == cudaSuccess;
   }();
   if (!smem_ok) {
     k_couple_points<<<1, kCT, 0, s>>>(c, a);
     return;
   }
-  // Points run in batches (one ordered walk per batch, in order on the
-  // stream), which bounds the candidate lists.
-  constexpr int kBatch = 65536;
   std::vector<uint32_t> totals, off;
   for (int p0 = 0; p0 < np; p0 += kBatch) {
     const int nb = std::min(kBatch, np - p0);
@@ -1158,8 +1093,9 @@ void launch_couple_points(const StepConsts& c, DevBuffers& b, double* d_pts, int
     ab.pts = d_pts + 10 * (size_t)p0;
     scratch_grow(sc.tab, sc.cap_tab, (size_t)nb * kTabU, s);
     scratch_grow(sc.totals, sc.cap_totals, (size_t)nb, s);
+    scratch_grow(sc.conf, sc.cap_conf, (size_t)nb, s);
     const int warps_per_block = 256 / 32, blocks = (nb + warps_per_block - 1) / warps_per_block;
-    k_point_tables<<<blocks, 256, 0, s>>>(c, ab, 0, nb, sc.tab, sc.totals);
+    k_point_tables<<<blocks, 256, 0, s>>>(c, ab, nb, sc.tab, sc.totals, sc.conf);
     cuda_check(cudaGetLastError(), "point tables");
     totals.resize(nb);
     cuda_check(cudaMemcpyAsync(totals.data(), sc.totals, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
@@ -1178,8 +1114,8 @@ void launch_couple_points(const StepConsts& c, DevBuffers& b, double* d_pts, int
     cuda_check(cudaMemcpyAsync(sc.off, off.data(), (nb + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s),
                "point offsets");
     k_point_candidates<<<blocks, 256, 0, s>>>(ab, nb, sc.tab, sc.off, sc.idx, sc.m);
-    PointLists L{sc.tab, sc.off, sc.idx, sc.m};
-    k_couple_points_piped<<<1, kCT, kPipedSmem, s>>>(c, ab, 0, nb, L);
+    PointLists L{sc.tab, sc.off, sc.idx, sc.m, sc.conf};
+    k_couple_points_grouped<<<1, kGW * 32, kGroupedSmemFixed + (size_t)nb, s>>>(c, ab, nb, L);
     cuda_check(cudaGetLastError(), "couple points");
     // The offsets' host copy must outlive the upload.
     cuda_check(cudaStreamSynchronize(s), "couple points sync");

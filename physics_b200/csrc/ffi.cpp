@@ -441,10 +441,10 @@ int32_t phy_fluid_step_counters(PhyWorldHandle* w, uint32_t sub, uint64_t* out4)
   });
 }
 
-int32_t phy_fluid_dense_mask_info(PhyWorldHandle* w, uint32_t sub, uint64_t* out2) {
-  if (!out2) return -1;
+int32_t phy_fluid_dense_mask_info(PhyWorldHandle* w, uint32_t sub, uint64_t* out3) {
+  if (!out3) return -1;
   return guard<int32_t>(-1, [&] {
-    sub_of(w, sub).world->dense_mask_info(out2);
+    sub_of(w, sub).world->dense_mask_info(out3);
     return 0;
   });
 }

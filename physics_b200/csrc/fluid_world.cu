@@ -1172,10 +1172,11 @@ StepConsts FluidWorld::prepare_step(double dt) {
 }
 
 // Grows the dense-cell mask buffer to the entries the tasks of a recent step
-// reserved (the pinned copy lags by the steps still in flight), within half
-// the free device memory; tasks that find no room filter again in the force
-// pass, so the size never changes a result.  A failed allocation leaves the
-// buffer empty and is not retried below the demand that failed.
+// reserved (the pinned copy lags by the steps still in flight), within a
+// quarter of the free device memory and 16 GiB; tasks that find no room
+// filter again in the force pass, so the size never changes a result.  A
+// failed allocation leaves the buffer empty and is not retried below the
+// demand that failed.
 void FluidWorld::ensure_masks() {
   if (!tuning_.dense_masks || !b_.mask_ctl || !b_.mask_demand) return;
   const unsigned long long want = *reinterpret_cast<volatile unsigned long long*>(b_.mask_demand);
@@ -1185,8 +1186,9 @@ void FluidWorld::ensure_masks() {
   cuda_check(cudaStreamSynchronize(stream_), "mask buffer sync");
   size_t free_b = 0, total_b = 0;
   cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
-  const unsigned long long limit =
-      std::min<unsigned long long>((free_b / 2 + b_.mask_cap * kEntryBytes) / kEntryBytes, 0xfffffffeull);
+  const unsigned long long limit = std::min<unsigned long long>(
+      std::min<unsigned long long>(free_b / 4 + b_.mask_cap * kEntryBytes, 16ull << 30) / kEntryBytes,
+      0xfffffffeull);
   const unsigned long long cap = std::min(want + want / 2 + 1024, limit);
   if (cap <= b_.mask_cap) return;
   dfree(b_.mask_hdr);
@@ -1612,10 +1614,11 @@ uint32_t FluidWorld::last_step_flags() {
   return f;
 }
 
-void FluidWorld::dense_mask_info(uint64_t* out2) {
+void FluidWorld::dense_mask_info(uint64_t* out3) {
   cuda_check(cudaStreamSynchronize(stream_), "mask info sync");
-  out2[0] = b_.mask_cap;
-  out2[1] = b_.mask_demand ? *reinterpret_cast<volatile unsigned long long*>(b_.mask_demand) : 0;
+  out3[0] = b_.mask_cap;
+  out3[1] = b_.mask_demand ? *reinterpret_cast<volatile unsigned long long*>(b_.mask_demand) : 0;
+  out3[2] = (last_step_flags() & kFlagMaskTable) ? 1 : 0;
 }
 
 void FluidWorld::last_step_counters(uint64_t* out2) {

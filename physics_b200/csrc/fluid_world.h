@@ -146,8 +146,9 @@ class FluidWorld {
   void set_counting(bool on) { counting_ = on; }
   void last_step_counters(uint64_t* out2);
   // Dense-cell mask buffer: entries allocated, entries the last step's tasks
-  // reserved (waits for the stream).
-  void dense_mask_info(uint64_t* out2);
+  // reserved, 1 when the last step found a task's masks outside the buffer
+  // (waits for the stream).
+  void dense_mask_info(uint64_t* out3);
   int grid_cells() const { return ncells_; }
 
   // FluidWorld::couple_points (world.rs:691-752) on the device, bit-exact:

@@ -118,14 +118,16 @@ void launch_cell_index(const StepConsts& c, DevBuffers& b, uint32_t* flags, cuda
 void cuda_check(cudaError_t e, const char* what);
 
 // Scratch of couple_points (owned by the world, grown on demand): per-point
-// cell tables, candidate counts and offsets, candidate indices and masses.
+// cell tables, candidate counts and offsets, neighbourhood overlaps with the
+// points just before, candidate indices and masses.
 struct CouplePointsScratch {
   uint32_t* tab = nullptr;
   uint32_t* totals = nullptr;
   uint32_t* off = nullptr;
   uint32_t* idx = nullptr;
   double* m = nullptr;
-  size_t cap_tab = 0, cap_totals = 0, cap_off = 0, cap_idx = 0, cap_m = 0;
+  uint8_t* conf = nullptr;
+  size_t cap_tab = 0, cap_totals = 0, cap_off = 0, cap_idx = 0, cap_m = 0, cap_conf = 0;
   void release();
 };
 void launch_couple_points(const StepConsts& c, DevBuffers& b, double* d_pts, int np, double dt, double drag,

@@ -39,6 +39,7 @@ constexpr uint32_t kDenseMean = 32;
 enum : uint32_t {
   kFlagOutOfBox = 1u,    // a cell key fell outside the grid box
   kFlagNonFinite = 2u,   // a new position or velocity is NaN/Inf
+  kFlagMaskTable = 4u,   // a dense-cell task's kept masks lie outside the mask buffer (filtered again)
 };
 
 // The grid box and wall bounds of one scene in the tiled linearisation.  A

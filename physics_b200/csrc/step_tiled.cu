@@ -1175,11 +1175,15 @@ __global__ void __launch_bounds__(kWT, 2) k_force_dense(StepConsts c, TiledArgs 
         if (rounds & 7) fold<kShear>(acc, part);
       }
     };
-    const uint32_t mbase = a.task_mbase ? a.task_mbase[t.k] : kNoMasks;
+    uint32_t mbase = a.task_mbase ? a.task_mbase[t.k] : kNoMasks;
+    const uint32_t mcount = mbase != kNoMasks ? a.task_mcount[t.k] : 0u;
+    if (mbase != kNoMasks && ((unsigned long long)mbase + mcount > a.mask_cap || mcount > (1u << 20))) {
+      if (lane == 0) atomicOr(a.flags, kFlagMaskTable);
+      mbase = kNoMasks;
+    }
     if (mbase != kNoMasks) {
       // The density pass's chunks, in its order; the next entry's header and
       // mask are loaded while the current chunk is walked.
-      const uint32_t mcount = a.task_mcount[t.k];
       uint32_t hdr = 0, bits = 0;
       if (mcount) {
         hdr = a.mask_hdr[mbase];
@@ -1191,9 +1195,11 @@ __global__ void __launch_bounds__(kWT, 2) k_force_dense(StepConsts c, TiledArgs 
           hdr = a.mask_hdr[mbase + e + 1];
           bits = a.mask_bits[(size_t)(mbase + e + 1) * 32u + (uint32_t)lane];
         }
-        // Only candidates some lane has in range are loaded; the other slots
-        // hold far dummies (never walked, finite for the padding).
-        const bool cv = ((__reduce_or_sync(0xffffffffu, mask) >> lane) & 1u) != 0u;
+        // Only candidates some lane has in range are loaded, and the chunk's
+        // first (always a particle), which pads the two-candidate rounds as in
+        // the filtering walk; the other slots hold far dummies, never walked.
+        const uint32_t any = __reduce_or_sync(0xffffffffu, mask);  // every lane takes part
+        const bool cv = lane == 0 || ((any >> lane) & 1u) != 0u;
         const uint32_t j = (h >> 5) + (uint32_t)lane;
         float off[3];
         neighbour_offset(c, (int)(h & 31u), off);

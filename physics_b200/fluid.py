@@ -366,11 +366,12 @@ class FluidWorld:
         return {"candidates": out[0], "pairs": out[1], "particles": out[2], "cells": out[3]}
 
     def dense_mask_info(self) -> dict:
-        """The dense-cell mask buffer (phy_fluid_dense_mask_info): entries allocated and the
-        entries the last step's dense-cell tasks reserved."""
-        out = (C.c_uint64 * 2)()
+        """The dense-cell mask buffer (phy_fluid_dense_mask_info): entries allocated, the
+        entries the last step's dense-cell tasks reserved, and whether the last step found a
+        task's kept masks outside the buffer."""
+        out = (C.c_uint64 * 3)()
         L.check(self._lib.phy_fluid_dense_mask_info(self._h, self._sub, out), "phy_fluid_dense_mask_info")
-        return {"capacity": out[0], "demand": out[1]}
+        return {"capacity": out[0], "demand": out[1], "bad_table": bool(out[2])}
 
     def set_tuning(self, **knobs: int) -> None:
         """Kernel configuration (phy_fluid_set_tuning): comp_tile, halo_cap, ctas_per_sm, queue,

@@ -204,10 +204,14 @@ def test_gradient_64k_form_vs_oracle_jvp(gpu, oracle_mod):
 #
 # step_backward on a compensated world differentiates the step map along the
 # compensated trajectory: every re-run step first takes an f64 plain recording step
-# from the compensated state, so the reverse sweep is the exact adjoint at the states
-# the compensated forward visited.  Its gradient then differs from the f64 trajectory's
-# by the compensated form's own error (about 1e-6 relative per step) and matches
-# central differences of the compensated forward.
+# from the compensated state, then the compensated step, whose outputs replace the
+# recorded ones, so the reverse sweep is the adjoint of the exact step map at the states
+# the compensated forward visited.  Its gradient differs from the f64 trajectory's by
+# the compensated form's own error (about 1e-6 relative per step).  Central differences
+# of the compensated forward itself carry its f32 rounding: at eps = 1e-4 they scatter
+# by about 1e-3 relative around any smooth gradient (the f64 adjoint's and the
+# compensated adjoint's alike), so they are taken at eps = 1e-2 on the small problem,
+# and the 64k form is checked against central differences of the smooth f64 map.
 
 def test_comp_adjoint_vs_oracle_jvp_and_interval(gpu, oracle_mod):
     O = oracle_mod
@@ -233,7 +237,7 @@ def test_comp_adjoint_vs_oracle_jvp_and_interval(gpu, oracle_mod):
 
 def test_comp_adjoint_central_differences_and_state(gpu):
     sc, v0, target = _problem()
-    steps, eps = 24, 1e-4
+    steps = 24
     w, _, g = _adjoint(gpu, sc, v0, target, steps, every=6, form="comp")
     ref = _gpu_world(gpu, sc, v0, "comp")
     ref.step(DT, steps)
@@ -242,25 +246,37 @@ def test_comp_adjoint_central_differences_and_state(gpu):
     errs = []
     for _ in range(4):
         d = _unit(rng, v0.shape)
-        fd = (_loss(gpu, sc, v0 + eps * d, target, steps, "comp") -
-              _loss(gpu, sc, v0 - eps * d, target, steps, "comp")) / (2 * eps)
-        errs.append(abs(float(np.sum(g["vel"] * d)) - fd) / abs(fd))
-    print("comp adjoint vs central differences", errs)
-    assert max(errs) <= 1e-4, errs
+        for form, eps in (("comp", 1e-2), ("f64", 1e-4)):
+            fd = (_loss(gpu, sc, v0 + eps * d, target, steps, form) -
+                  _loss(gpu, sc, v0 - eps * d, target, steps, form)) / (2 * eps)
+            errs.append((form, abs(float(np.sum(g["vel"] * d)) - fd) / abs(fd)))
+    print("comp adjoint vs central differences (compensated eps 1e-2, f64 eps 1e-4)", errs)
+    assert max(e for _, e in errs) <= 1e-4, errs
 
 
 def test_comp_gradient_64k_form(gpu):
-    """The differentiation form on the compensated world: adjoint vs central
-    differences of the compensated forward on 4 directions."""
+    """The differentiation form on the compensated world (64k particles, 100 steps): the
+    compensated adjoint against central differences of the f64 map on 4 directions and
+    against the f64 adjoint; central differences of the compensated forward are no
+    closer to the f64 adjoint than to the compensated one (their scatter is the
+    forward's rounding, not the adjoint's)."""
     sc, v0, target = _problem((32, 64, 32), 12.8, seed=64)
     steps, eps = 100, 1e-4
     _, L, g = _adjoint(gpu, sc, v0, target, steps, every=10, form="comp")
+    _, _, gf = _adjoint(gpu, sc, v0, target, steps, every=10)
+    rel = float(np.linalg.norm(g["vel"] - gf["vel"]) / np.linalg.norm(gf["vel"]))
     rng = np.random.default_rng(3)
-    errs = []
+    errs, spread = [], []
     for _ in range(4):
         d = _unit(rng, v0.shape)
-        fd = (_loss(gpu, sc, v0 + eps * d, target, steps, "comp") -
-              _loss(gpu, sc, v0 - eps * d, target, steps, "comp")) / (2 * eps)
+        fd = (_loss(gpu, sc, v0 + eps * d, target, steps) - _loss(gpu, sc, v0 - eps * d, target, steps)) / (2 * eps)
         errs.append(abs(float(np.sum(g["vel"] * d)) - fd) / abs(fd))
-    print("comp 64k relative errors vs central differences", errs)
+        fc = (_loss(gpu, sc, v0 + 1e-2 * d, target, steps, "comp") -
+              _loss(gpu, sc, v0 - 1e-2 * d, target, steps, "comp")) / 2e-2
+        spread.append((abs(float(np.sum(g["vel"] * d)) - fc), abs(float(np.sum(gf["vel"] * d)) - fc), abs(fc)))
+    print("comp 64k: vs f64 central differences", errs, "vs f64 adjoint", rel,
+          "compensated central differences (|comp adj - fd|, |f64 adj - fd|, |fd|)", spread)
     assert max(errs) <= 1e-4, errs
+    assert rel <= 1e-5, rel
+    for dc, df, f in spread:
+        assert dc <= df + 1e-4 * f, spread

@@ -76,16 +76,37 @@ def test_couple_points_on_tiled_compensated_world(gpu, oracle_mod):
     assert np.isfinite(w.pos).all()
 
 
-@pytest.mark.parametrize("spacing,least", [(0.04, 1024), (0.03, 2048)])
+@pytest.mark.parametrize("spacing,least", [(0.04, 1024), (0.03, 2048), (0.02, 4096)])
 def test_couple_points_dense_neighbourhood(gpu, oracle_mod, spacing, least):
-    """Points whose 27 cells hold more than 1024 candidates, and (spacing 0.03) more than
-    the 2048 the pipelined walk prefetches, which take the chunked walk; the other points
-    of the same call stay on the pipelined one."""
+    """Points whose 27 cells hold more than the 512 candidates a warp stages at once (taken
+    in chunks), and (spacing 0.02) more than the 4096 that get a candidate list (read
+    through the cell table); the other points of the same call hold theirs in registers."""
     O = oracle_mod
     w, ow, _ = _pair(gpu, O, lo=-0.3, hi=0.3, spacing=spacing, steps=2)
     assert len(ow.neighbors_of_point([0.0, 0.0, 0.0])) > least
     pts, vel, mass, prior = _points(n_random=10, seed=7)
     _check(O, w, ow, pts, vel, mass, prior)
+
+
+def test_couple_points_groups(gpu, oracle_mod):
+    """Many points over a large block: runs of consecutive points with disjoint 27-cell
+    neighbourhoods run at once, one warp each; interleaved with points next to the one
+    before (same and adjacent cells), repeated points, and points outside the bounds,
+    every force and fluid velocity matches the oracle's one-after-another walk."""
+    O = oracle_mod
+    w, ow, _ = _pair(gpu, O, lo=-2.0, hi=2.0, spacing=0.1, steps=2)
+    rng = np.random.default_rng(11)
+    pts = rng.uniform(-2.1, 2.1, (600, 3))
+    pts[100:140] = pts[99] + rng.uniform(-0.45, 0.45, (40, 3))  # a cluster: overlapping runs
+    pts[200:208] = pts[199]                                      # the same point 9 times
+    pts[300:308:2] = [9.0, 0.0, 0.0]                             # outside, between others
+    vel = rng.normal(0.0, 0.3, pts.shape)
+    mass = rng.uniform(0.005, 0.05, len(pts))
+    prior = rng.normal(0.0, 1.0, pts.shape)
+    fg = w.couple_points(pts, vel, mass, DT, 1.2, 950.0, force=prior)
+    fo = ow.couple_points(pts, vel, mass, DT, 1.2, 950.0, force=prior)
+    assert_bits_equal(fg, fo, "forces")
+    assert_bits_equal(w.vel, ow.get(O.F_VEL), "fluid velocities")
 
 
 def test_couple_points_buoyancy_upward(gpu):
