@@ -471,6 +471,10 @@ void FluidWorld::free_all() {
   dfree(b_.nbr16);
   dfree(b_.sorted_cell);
   dfree(b_.tile_head);
+  dfree(b_.tile_index);
+  b_.tile_scan_entries = 0;
+  dfree(b_.tile_of);
+  dfree(b_.large_cells);
   dfree(b_.tile_slot);
   dfree(b_.num_tiles);
   dfree(b_.boxes);
@@ -547,7 +551,8 @@ void FluidWorld::ensure_capacity(size_t n) {
   dfree(b_.nbr);
   dfree(b_.nbr16);
   dfree(b_.sorted_cell);
-  dfree(b_.tile_head);
+  dfree(b_.tile_of);
+  dfree(b_.large_cells);
   dfree(b_.tile_slot);
   dfree(b_.tile_crowd);
   dfree(b_.dense_q0);
@@ -574,7 +579,8 @@ void FluidWorld::ensure_mode_buffers() {
   if (tiled) {
     if (!b_.nbr16) dalloc(b_.nbr16, (size_t)kMaxNeighbors * cap);
     if (!b_.sorted_cell) dalloc(b_.sorted_cell, cap);
-    if (!b_.tile_head) dalloc(b_.tile_head, tile_head_length((int)cap));
+    if (!b_.tile_of) dalloc(b_.tile_of, cap + 1);
+    if (!b_.large_cells) dalloc(b_.large_cells, cap / 64 + 64);  // cells of more than 64 particles
     if (!b_.tile_slot) dalloc(b_.tile_slot, cap + 1);
     if (!b_.tile_crowd) dalloc(b_.tile_crowd, cap + 1);
     if (!b_.num_tiles) dalloc(b_.num_tiles, 1);
@@ -780,10 +786,17 @@ void FluidWorld::ensure_cells() {
     b_.cell_capacity = cap;
     ++alloc_gen_;
   }
-  // The scan's tile sums serve the cell scan and the tile-head scan (n + 1
-  // entries) alike.
-  const int sums = (int)std::max(scan_block_sums_needed(b_.cell_capacity),
-                                 tile_head_length(std::max(b_.capacity, 1)) / 4096);
+  // The tiled sort's tile counts and occupied-tile index.
+  if (tile_ && tile_scan_length(b_.cell_capacity) > b_.tile_scan_entries) {
+    const size_t len = tile_scan_length(b_.cell_capacity);
+    cuda_check(cudaStreamSynchronize(stream_), "tile scan sync");
+    dalloc(b_.tile_head, len);
+    dalloc(b_.tile_index, len);
+    b_.tile_scan_entries = len;
+    ++alloc_gen_;
+  }
+  // The scan's tile sums serve the cell scan and the tile scans alike.
+  const int sums = (int)scan_block_sums_needed(b_.cell_capacity);
   if (sums > b_.block_sums_capacity) {
     cuda_check(cudaStreamSynchronize(stream_), "sums sync");
     dalloc(b_.block_sums, (size_t)sums);

@@ -48,10 +48,13 @@ __device__ __forceinline__ uint32_t quantise_local(double x, long long k, double
   return t >= 1023.0 ? 1023u : (uint32_t)t;
 }
 
-// Cell of every particle plus its arrival rank inside the cell.  Lanes of a
-// warp that share a cell (the common case: the previous order is already
-// sorted by cell) are aggregated into one atomic.
-__global__ void __launch_bounds__(kThreads) k_cell_hist(StepConsts c, const double* __restrict__ px,
+// Cell of every particle plus its arrival rank inside its bucket: the cell
+// (bucket_shift 0), or the tile of 2^bucket_shift consecutive cells (the
+// overflow cell's bucket follows the last tile's).  Lanes of a warp that
+// share a bucket (the common case: the previous order is already sorted by
+// cell) are aggregated into one atomic.
+__global__ void __launch_bounds__(kThreads) k_cell_hist(StepConsts c, int bucket_shift,
+                                                        const double* __restrict__ px,
                                                         const double* __restrict__ py,
                                                         const double* __restrict__ pz,
                                                         uint32_t* __restrict__ cell_of,
@@ -96,11 +99,12 @@ __global__ void __launch_bounds__(kThreads) k_cell_hist(StepConsts c, const doub
   }
   unsigned mask = __ballot_sync(0xffffffffu, active);
   if (!active) return;
-  unsigned peers = __match_any_sync(mask, cell);
+  const uint32_t bucket = cell >> bucket_shift;
+  unsigned peers = __match_any_sync(mask, bucket);
   int lane = threadIdx.x & 31;
   int leader = __ffs(peers) - 1;
   uint32_t base = 0;
-  if (lane == leader) base = atomicAdd(&count[cell], (uint32_t)__popc(peers));
+  if (lane == leader) base = atomicAdd(&count[bucket], (uint32_t)__popc(peers));
   base = __shfl_sync(peers, base, leader);
   rank[i] = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
 }
@@ -193,13 +197,15 @@ __global__ void __launch_bounds__(kThreads) k_scan_apply(uint32_t* __restrict__ 
     t[q] = make_uint4(a[4 * q] + off, a[4 * q + 1] + off, a[4 * q + 2] + off, a[4 * q + 3] + off);
 }
 
-__global__ void __launch_bounds__(kThreads) k_scatter(int n, const uint32_t* __restrict__ cell_of,
+// Every particle to its bucket's range (start = the scanned bucket counts),
+// in arrival order inside the bucket.
+__global__ void __launch_bounds__(kThreads) k_scatter(int n, int bucket_shift, const uint32_t* __restrict__ cell_of,
                                                       const uint32_t* __restrict__ rank,
-                                                      const uint32_t* __restrict__ cell_start,
+                                                      const uint32_t* __restrict__ start,
                                                       uint32_t* __restrict__ tmp) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  tmp[cell_start[cell_of[i]] + rank[i]] = (uint32_t)i;
+  tmp[start[cell_of[i] >> bucket_shift] + rank[i]] = (uint32_t)i;
 }
 
 // Cells up to kOrderSmall particles are ordered by k_order (each particle
@@ -308,6 +314,190 @@ __global__ void __launch_bounds__(kOrderThreads) k_order_large(const uint32_t* _
   }
 }
 
+// ---- Tiled sort: counts per tile, cells per occupied tile ------------------
+//
+// The tiled linearisation numbers a tile's cells consecutively, so the sort
+// counts particles per tile (a histogram a 64th of the cell box, or an 8th
+// with 2x2x2 tiles), scans the tile counts and the occupied-tile flags, and
+// orders each occupied tile's particles in one CTA with shared counters.
+// Only occupied tiles get cell starts: a reader of a cell in an empty tile
+// finds the tile empty in the scanned tile counts (its start equals the next
+// tile's start).
+
+// flag[t] = 1 for tiles t < ntiles that hold particles (tstart: the scanned
+// tile counts), 0 up to len.
+__global__ void __launch_bounds__(kThreads) k_tile_occupied(int ntiles, int len, const uint32_t* __restrict__ tstart,
+                                                            uint32_t* __restrict__ flag) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= len) return;
+  flag[t] = (t < ntiles && tstart[t + 1] > tstart[t]) ? 1u : 0u;
+}
+
+// Per tile (one thread each): an occupied tile is recorded under its list
+// index (tindex: the scanned occupied flags).  The thread past the last tile
+// writes the overflow cell's range and the end of the tile list.
+__global__ void __launch_bounds__(kThreads) k_tile_list(int n, int ncells, int ntiles,
+                                                        const uint32_t* __restrict__ tstart,
+                                                        const uint32_t* __restrict__ tindex,
+                                                        uint32_t* __restrict__ cell_start,
+                                                        uint32_t* __restrict__ tile_of,
+                                                        uint32_t* __restrict__ tile_slot,
+                                                        uint32_t* __restrict__ num_tiles) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > ntiles) return;
+  if (t == ntiles) {
+    const uint32_t of = tstart[ntiles], count = tindex[ntiles];
+    cell_start[ncells] = of;
+    cell_start[ncells + 1] = (uint32_t)n;
+    *num_tiles = count;
+    tile_slot[count] = of;  // the end of the last tile
+    return;
+  }
+  if (tstart[t + 1] > tstart[t]) tile_of[tindex[t]] = (uint32_t)t;
+}
+
+// One CTA per occupied tile (persistent over the tile list).  The tile's
+// particles (`tmp`, grouped by tile) are counted per cell in shared memory;
+// the cells' starts are written, with the start of the next tile's first
+// cell (the end of this tile's last), and the tile's list entry with the flag
+// that routes a tile whose occupied cells average more than dense_mean
+// particles to the dense-cell passes.  Then every particle goes to its final
+// slot in `perm`: its rank among its cell's particles by in-cell order key
+// (the keys are unique).  A tile of at most kTileOrder particles whose cells
+// hold at most kOrderSmall each counts the smaller keys in shared memory;
+// other tiles scatter their particles by cell into `out` and count in global
+// memory, except in cells of kOrderSmall < count <= kOrderLarge particles,
+// which go to `large` for k_order_large (the thread of the cell's first slot
+// appends it).  Particles of the overflow cell keep their slots.
+constexpr int kTileCache = 4;                         // particles per thread held in registers
+constexpr int kTileOrder = kTileCache * kThreads;     // 1024
+template <int kCells>
+__global__ void __launch_bounds__(kThreads) k_tile_cells(int n, int ncells, const uint32_t* __restrict__ tstart,
+                                                         const uint32_t* __restrict__ tile_of,
+                                                         const uint32_t* __restrict__ num_tiles,
+                                                         const uint32_t* __restrict__ tmp,
+                                                         const uint32_t* __restrict__ cell_of,
+                                                         const unsigned long long* __restrict__ okey,
+                                                         uint32_t* __restrict__ rank, uint32_t* __restrict__ perm,
+                                                         uint32_t* __restrict__ out, uint32_t* __restrict__ cell_start,
+                                                         uint32_t* __restrict__ tile_slot,
+                                                         uint8_t* __restrict__ tile_crowd, int dense_mean,
+                                                         uint32_t* __restrict__ large,
+                                                         uint32_t* __restrict__ large_count) {
+  static_assert(kCells == 8 || kCells == 64, "tile of 2x2x2 or 4x4x4 cells");
+  __shared__ uint32_t s_cnt[kCells];
+  __shared__ uint32_t s_off[kCells + 1];
+  __shared__ unsigned long long s_key[kTileOrder];
+  __shared__ int s_small;  // every cell of the tile holds at most kOrderSmall particles
+  const uint32_t count = *num_tiles;
+  const int lane = threadIdx.x & 31;
+  for (uint32_t k = blockIdx.x; k < count; k += gridDim.x) {
+    const uint32_t t = tile_of[k];
+    const uint32_t ts = tstart[t], te = tstart[t + 1];
+    const uint32_t cell0 = t * (uint32_t)kCells;
+    const bool cached = te - ts <= (uint32_t)kTileOrder;  // uniform
+    for (int l = threadIdx.x; l < kCells; l += blockDim.x) s_cnt[l] = 0;
+    __syncthreads();
+    uint32_t ci[kTileCache], cl[kTileCache], cr[kTileCache];
+    if (cached) {
+#pragma unroll
+      for (int j = 0; j < kTileCache; ++j) {
+        const uint32_t e = ts + threadIdx.x + (uint32_t)(j * kThreads);
+        ci[j] = cl[j] = cr[j] = 0;
+        if (e < te) {
+          ci[j] = tmp[e];
+          cl[j] = cell_of[ci[j]] - cell0;
+          cr[j] = atomicAdd(&s_cnt[cl[j]], 1u);
+        }
+      }
+    } else {
+      for (uint32_t e = ts + threadIdx.x; e < te; e += blockDim.x) {
+        const uint32_t i = tmp[e];
+        rank[i] = atomicAdd(&s_cnt[cell_of[i] - cell0], 1u);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      // Lane l holds cells l and l + 32: two warp scans.
+      const uint32_t a0 = lane < kCells ? s_cnt[lane] : 0u;
+      const uint32_t a1 = kCells > 32 ? s_cnt[(lane + 32) & (kCells - 1)] : 0u;
+      uint32_t x0 = a0, x1 = a1;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y0 = __shfl_up_sync(0xffffffffu, x0, o), y1 = __shfl_up_sync(0xffffffffu, x1, o);
+        if (lane >= o) {
+          x0 += y0;
+          x1 += y1;
+        }
+      }
+      const uint32_t total0 = __shfl_sync(0xffffffffu, x0, 31);
+      const uint32_t occ = __popc(__ballot_sync(0xffffffffu, a0 > 0u)) + __popc(__ballot_sync(0xffffffffu, a1 > 0u));
+      const bool big = __any_sync(0xffffffffu, a0 > kOrderSmall || a1 > kOrderSmall);
+      if (lane < kCells) {
+        s_off[lane] = x0 - a0;
+        cell_start[cell0 + lane] = ts + x0 - a0;
+      }
+      if (kCells > 32) {
+        s_off[lane + 32] = total0 + x1 - a1;
+        cell_start[cell0 + lane + 32] = ts + total0 + x1 - a1;
+      }
+      if (lane == 0) {
+        s_off[kCells] = te - ts;
+        cell_start[cell0 + kCells] = te;  // the next tile's first cell starts here too
+        tile_slot[k] = ts;
+        tile_crowd[k] = te - ts > (uint32_t)dense_mean * occ ? 1 : 0;
+        s_small = big ? 0 : 1;
+      }
+    }
+    __syncthreads();
+    if (cached && s_small) {
+#pragma unroll
+      for (int j = 0; j < kTileCache; ++j)
+        if (ts + threadIdx.x + (uint32_t)(j * kThreads) < te) s_key[s_off[cl[j]] + cr[j]] = okey[ci[j]];
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < kTileCache; ++j)
+        if (ts + threadIdx.x + (uint32_t)(j * kThreads) < te) {
+          const uint32_t c0 = s_off[cl[j]], c1 = s_off[cl[j] + 1];
+          const unsigned long long mine = s_key[c0 + cr[j]];
+          uint32_t r = 0;
+          for (uint32_t q = c0; q < c1; ++q) r += s_key[q] < mine ? 1u : 0u;
+          perm[ts + c0 + r] = ci[j];
+        }
+    } else {
+      if (cached) {
+#pragma unroll
+        for (int j = 0; j < kTileCache; ++j)
+          if (ts + threadIdx.x + (uint32_t)(j * kThreads) < te) out[ts + s_off[cl[j]] + cr[j]] = ci[j];
+      } else {
+        for (uint32_t e = ts + threadIdx.x; e < te; e += blockDim.x) {
+          const uint32_t i = tmp[e];
+          out[ts + s_off[cell_of[i] - cell0] + rank[i]] = i;
+        }
+      }
+      __syncthreads();  // the by-cell order is complete
+      for (uint32_t e = ts + threadIdx.x; e < te; e += blockDim.x) {
+        const uint32_t i = out[e];
+        const uint32_t l = cell_of[i] - cell0;
+        const uint32_t c0 = ts + s_off[l], c1 = ts + s_off[l + 1];
+        if (c1 - c0 > kOrderSmall && c1 - c0 <= kOrderLarge) {
+          if (e == c0) large[atomicAdd(large_count, 1u)] = cell0 + l;
+          continue;
+        }
+        const unsigned long long mine = okey[i];
+        uint32_t r = 0;
+        for (uint32_t q = c0; q < c1; ++q) r += okey[out[q]] < mine ? 1u : 0u;
+        perm[c0 + r] = i;
+      }
+    }
+    __syncthreads();  // the counters and keys are free for the next tile
+  }
+  const uint32_t of = cell_start[ncells];
+  for (uint32_t e = of + blockIdx.x * blockDim.x + threadIdx.x; e < (uint32_t)n; e += gridDim.x * blockDim.x) {
+    out[e] = tmp[e];
+    perm[e] = tmp[e];
+  }
+}
+
 struct GatherArgs {
   const double* src_pv[6];
   double* dst_pv[6];
@@ -353,56 +543,6 @@ __global__ void __launch_bounds__(kThreads) k_gather(int n, const uint32_t* __re
       g.queue[3] = 0;  // dense-cell tasks taken by the density and force passes
       g.queue[4] = 0;
     }
-  }
-}
-
-// Tile list of a tiled sort: head[s] = 1 where slot s starts a new tile
-// (slots of the overflow cell excluded); head[n] = 0.
-__global__ void __launch_bounds__(kThreads) k_tile_heads(int n, int ncells, int tile_log2,
-                                                        const uint32_t* __restrict__ sorted_cell,
-                                                        uint32_t* __restrict__ head) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s > n) return;
-  uint32_t h = 0;
-  if (s < n) {
-    const uint32_t c = sorted_cell[s];
-    if ((int)c != ncells) {
-      const uint32_t t = c >> (3 * tile_log2);
-      h = (s == 0 || (sorted_cell[s - 1] >> (3 * tile_log2)) != t) ? 1u : 0u;
-    }
-  }
-  head[s] = h;
-}
-
-// After the exclusive scan of head: tile_slot[k] = first slot of tile k;
-// tile_slot[count] = first overflow slot (end of the last tile);
-// *num_tiles = count.
-__global__ void __launch_bounds__(kThreads) k_tile_emit(int n, int ncells, const uint32_t* __restrict__ sorted_cell,
-                                                       const uint32_t* __restrict__ scanned,
-                                                       const uint32_t* __restrict__ cell_start,
-                                                       uint32_t* __restrict__ tile_slot,
-                                                       uint8_t* __restrict__ tile_crowd, int tile_log2,
-                                                       int dense_mean, uint32_t* __restrict__ num_tiles) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) {
-    if (s == n) {
-      const uint32_t count = scanned[n];
-      *num_tiles = count;
-      tile_slot[count] = cell_start[ncells];
-    }
-    return;
-  }
-  if (scanned[s + 1] != scanned[s]) {
-    const uint32_t k = scanned[s];
-    tile_slot[k] = (uint32_t)s;
-    // Occupied cells of the tile and its particle count (its cells are
-    // consecutive): marks tiles too crowded for the staged passes.
-    const uint32_t c0 = (sorted_cell[s] >> (3 * tile_log2)) << (3 * tile_log2);
-    const uint32_t ncell = 1u << (3 * tile_log2);
-    uint32_t occ = 0;
-    for (uint32_t u = 0; u < ncell; ++u) occ += cell_start[c0 + u + 1] > cell_start[c0 + u] ? 1u : 0u;
-    const uint32_t np = cell_start[c0 + ncell] - cell_start[c0];
-    tile_crowd[k] = np > (uint32_t)dense_mean * occ ? 1 : 0;
   }
 }
 
@@ -459,33 +599,76 @@ static int order_large_blocks() {
   return blocks;
 }
 
-// Cells scanned per step: the box plus the overflow cell, rounded up to whole
-// scan tiles (the padding stays zero, so the prefix at index ncells+1 is n).
-static int scan_length(int ncells) { return ((ncells + 2 + kScanTile - 1) / kScanTile) * kScanTile; }
+// Persistent grid of k_tile_cells: its resident CTAs on every SM.
+static int tile_cells_blocks() {
+  static const int blocks = [] {
+    int dev = 0, sms = 1, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_tile_cells<64>, kThreads, 0);
+    return std::max(sms, 1) * std::max(per, 1);
+  }();
+  return blocks;
+}
+
+// Entries scanned per step: the buckets (cells, or tiles) plus the overflow
+// bucket, rounded up to whole scan tiles (the padding stays zero, so the
+// prefix at index buckets+1 is n).
+static int scan_length(int buckets) { return ((buckets + 2 + kScanTile - 1) / kScanTile) * kScanTile; }
 
 size_t scan_block_sums_needed(int ncells) { return (size_t)scan_length(ncells) / kScanTile; }
-size_t tile_head_length(int n) { return (size_t)((n + 1 + kScanTile - 1) / kScanTile) * kScanTile; }
+size_t tile_scan_length(int ncells) { return (size_t)scan_length(ncells / 8); }
 
 // Cells of the current positions (pv1): cell_start over the box and perm[s]
 // = the particle (index into the current arrays) at sorted slot s, ordered
 // by (cell, okey) when okey is given, else by (cell, insertion index).
+// In-place exclusive scan of len (a whole number of scan tiles) entries.
+static void scan_in_place(uint32_t* v, int len, uint32_t* block_sums, cudaStream_t s) {
+  const int nb = len / kScanTile;
+  k_scan_reduce<<<nb, kThreads, 0, s>>>(v, block_sums);
+  k_scan_top<<<1, 1024, 0, s>>>(block_sums, nb);
+  k_scan_apply<<<nb, kThreads, 0, s>>>(v, block_sums);
+}
+
 static void build_cells(const StepConsts& c, DevBuffers& b, cudaStream_t s, int bs, unsigned long long* okey,
                         uint32_t* flags) {
   const int n = c.n;
-  const int len = scan_length(c.ncells);
-  const int nb = len / kScanTile;
   const ParticleConsts& src = b.pc[b.cur];
-  cudaMemsetAsync(b.cell_start, 0, (size_t)len * sizeof(uint32_t), s);
-  k_cell_hist<<<grid_for(n, bs), bs, 0, s>>>(c, b.pv1[0], b.pv1[1], b.pv1[2], b.cell_of, b.rank,
-                                               b.cell_start, flags, src.scene, src.id, okey);
-  k_scan_reduce<<<nb, kThreads, 0, s>>>(b.cell_start, b.block_sums);
-  k_scan_top<<<1, 1024, 0, s>>>(b.block_sums, nb);
-  k_scan_apply<<<nb, kThreads, 0, s>>>(b.cell_start, b.block_sums);
-  k_scatter<<<grid_for(n, bs), bs, 0, s>>>(n, b.cell_of, b.rank, b.cell_start, b.tmp);
-  // `rank` is free after the scatter: it holds the list of large cells.
   cudaMemsetAsync(b.order_count, 0, sizeof(uint32_t), s);
-  k_order<<<grid_for(n, bs), bs, 0, s>>>(n, c.ncells, b.cell_of, b.cell_start, b.tmp, src.id, okey, b.perm,
-                                         b.rank, b.order_count);
+  if (c.tile) {
+    // Tiled: counts per tile, then cells and in-cell order per occupied tile
+    // (the tile-count array is tile_head, the occupied-tile index
+    // tile_index; the by-cell list of the tiles ordered in global memory goes
+    // to sorted_cell, which the gather rewrites).
+    const int shift = 3 * c.tile_log2;
+    const int ntiles = c.ncells >> shift;
+    const int tlen = scan_length(ntiles);
+    cudaMemsetAsync(b.tile_head, 0, (size_t)tlen * sizeof(uint32_t), s);
+    k_cell_hist<<<grid_for(n, bs), bs, 0, s>>>(c, shift, b.pv1[0], b.pv1[1], b.pv1[2], b.cell_of, b.rank,
+                                                 b.tile_head, flags, src.scene, src.id, okey);
+    scan_in_place(b.tile_head, tlen, b.block_sums, s);
+    k_scatter<<<grid_for(n, bs), bs, 0, s>>>(n, shift, b.cell_of, b.rank, b.tile_head, b.tmp);
+    k_tile_occupied<<<grid_for(tlen), kThreads, 0, s>>>(ntiles, tlen, b.tile_head, b.tile_index);
+    scan_in_place(b.tile_index, tlen, b.block_sums, s);
+    k_tile_list<<<grid_for(ntiles + 1), kThreads, 0, s>>>(n, c.ncells, ntiles, b.tile_head, b.tile_index,
+                                                          b.cell_start, b.tile_of, b.tile_slot, b.num_tiles);
+    auto cells = c.tile == 4 ? k_tile_cells<64> : k_tile_cells<8>;
+    cells<<<tile_cells_blocks(), kThreads, 0, s>>>(n, c.ncells, b.tile_head, b.tile_of, b.num_tiles, b.tmp, b.cell_of,
+                                                  okey, b.rank, b.perm, b.sorted_cell, b.cell_start, b.tile_slot,
+                                                  b.tile_crowd, c.dense_mean, b.large_cells, b.order_count);
+    k_order_large<<<order_large_blocks(), kOrderThreads, 0, s>>>(b.cell_start, b.sorted_cell, src.id, okey,
+                                                                 b.large_cells, b.order_count, b.perm);
+    return;
+  }
+  const int len = scan_length(c.ncells);
+  cudaMemsetAsync(b.cell_start, 0, (size_t)len * sizeof(uint32_t), s);
+  k_cell_hist<<<grid_for(n, bs), bs, 0, s>>>(c, 0, b.pv1[0], b.pv1[1], b.pv1[2], b.cell_of, b.rank, b.cell_start,
+                                               flags, src.scene, src.id, okey);
+  scan_in_place(b.cell_start, len, b.block_sums, s);
+  k_scatter<<<grid_for(n, bs), bs, 0, s>>>(n, 0, b.cell_of, b.rank, b.cell_start, b.tmp);
+  // `rank` is free after the scatter: it holds the list of large cells.
+  k_order<<<grid_for(n, bs), bs, 0, s>>>(n, c.ncells, b.cell_of, b.cell_start, b.tmp, src.id, okey, b.perm, b.rank,
+                                         b.order_count);
   k_order_large<<<order_large_blocks(), kOrderThreads, 0, s>>>(b.cell_start, b.tmp, src.id, okey, b.rank,
                                                                b.order_count, b.perm);
 }
@@ -518,19 +701,6 @@ void launch_sort(const StepConsts& c, DevBuffers& b, cudaStream_t s, int block) 
   g.h0 = c.h0;
   k_gather<<<grid_for(n, bs), bs, 0, s>>>(n, b.perm, g);
   b.cur ^= 1;
-  if (c.tile) {
-    // head flags in `rank` (free after the scatter), scanned in place.
-    const int hlen = ((n + 1 + kScanTile - 1) / kScanTile) * kScanTile;
-    cudaMemsetAsync(b.tile_head, 0, (size_t)hlen * sizeof(uint32_t), s);
-    k_tile_heads<<<grid_for(n + 1, bs), bs, 0, s>>>(n, c.ncells, c.tile_log2, b.sorted_cell, b.tile_head);
-    const int hb = hlen / kScanTile;
-    k_scan_reduce<<<hb, kThreads, 0, s>>>(b.tile_head, b.block_sums);
-    k_scan_top<<<1, 1024, 0, s>>>(b.block_sums, hb);
-    k_scan_apply<<<hb, kThreads, 0, s>>>(b.tile_head, b.block_sums);
-    k_tile_emit<<<grid_for(n + 1, bs), bs, 0, s>>>(n, c.ncells, b.sorted_cell, b.tile_head, b.cell_start,
-                                                   b.tile_slot, b.tile_crowd, c.tile_log2, c.dense_mean,
-                                                   b.num_tiles);
-  }
 }
 
 void launch_unsort_f64(const DevBuffers& b, int n, const double* src_sorted, double* dst_orig,

@@ -52,11 +52,19 @@ struct DevBuffers {
   // tile's halo), row-major: the kMaxNeighbors entries of sorted slot i at
   // nbr16[i * kMaxNeighbors ..].
   uint16_t* nbr16 = nullptr;
-  // Tiled sort: cell of each sorted slot, tile heads (scan scratch), first
-  // slot of every occupied tile (+ end), and the device-side tile count.
+  // Tiled sort: cell of each sorted slot (before the gather: the particles
+  // grouped by cell), particles per tile scanned to tile starts (tile_head)
+  // and occupied tiles scanned to list indices (tile_index), both over the
+  // cell box's tiles plus the overflow bucket (tile_scan_entries); the tile of
+  // every list entry, the first slot of every occupied tile (+ end), and the
+  // device-side tile count.
   uint32_t* sorted_cell = nullptr;
   uint32_t* tile_head = nullptr;
+  uint32_t* tile_index = nullptr;
+  size_t tile_scan_entries = 0;
+  uint32_t* tile_of = nullptr;
   uint32_t* tile_slot = nullptr;
+  uint32_t* large_cells = nullptr;  // cells of more than kOrderSmall particles (capacity / 64 + 64)
   uint8_t* tile_crowd = nullptr;  // 1: tile above kDenseMean per occupied cell
   uint32_t* num_tiles = nullptr;
   // Scene boxes of the tiled linearisation (one entry for a single world),
@@ -188,7 +196,9 @@ void launch_plain_passes(const StepConsts& c, DevBuffers& b, cudaStream_t s, con
 void launch_comp_passes(const StepConsts& c, DevBuffers& b, cudaStream_t s, const PassEvents& ev);
 
 size_t scan_block_sums_needed(int count);
-size_t tile_head_length(int n);
+// Entries of the tiled sort's tile scans for a box of ncells cells (tiles of 8
+// cells or more, plus the overflow bucket, in whole scan tiles).
+size_t tile_scan_length(int ncells);
 
 // Launch knobs (results do not depend on them): resident CTAs per SM of the
 // tiled passes' persistent grids (0 = the occupancy limit), their tile

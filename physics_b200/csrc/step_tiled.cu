@@ -64,7 +64,11 @@ struct TiledArgs {
   const double* __restrict__ vz;
   const double* __restrict__ mass;
   const uint32_t* __restrict__ mat;
+  // Cell starts of the occupied tiles' cells (and of the cell after each
+  // occupied tile); a tile's particles start at tile_start[tile] and a tile
+  // is empty when tile_start[tile + 1] equals it.
   const uint32_t* __restrict__ cell_start;
+  const uint32_t* __restrict__ tile_start;
   const uint32_t* __restrict__ sorted_cell;
   const uint32_t* __restrict__ tile_slot;
   const uint8_t* __restrict__ tile_crowd;  // 1: route the tile to the dense-cell passes
@@ -197,6 +201,19 @@ __device__ __forceinline__ uint32_t next_tile(uint32_t* queue, int pass, uint32_
   return *s_next;
 }
 
+// Slot range [s, e) of cell `lin` of the tiled box: empty when the cell's
+// tile holds no particles (an empty tile's cell starts are not written).
+template <int TB>
+__device__ __forceinline__ void cell_range(const TiledArgs& a, uint32_t lin, uint32_t& s, uint32_t& e) {
+  const uint32_t t = lin >> (3 * Tile<TB>::L);
+  if (a.tile_start[t + 1] == a.tile_start[t]) {
+    s = e = 0;
+    return;
+  }
+  s = a.cell_start[lin];
+  e = a.cell_start[lin + 1];
+}
+
 // Slot ranges of the tile's halo cells: s_src[h] / s_end[h] = global slot
 // range, s_off[h] = first staged slot; every cell's staged range is padded to
 // an even length (one far-away dummy particle), so all runs are pair-aligned.
@@ -213,9 +230,9 @@ __device__ __forceinline__ uint32_t halo_table(const StepConsts& c, const TiledA
     const int ay = g.ty * T::B - 1 + (h / T::H) % T::H;
     const int az = g.tz * T::B - 1 + h % T::H;
     if (ax >= 0 && ay >= 0 && az >= 0 && ax < bx.nc[0] && ay < bx.nc[1] && az < bx.nc[2]) {
-      const int lin = box_tiled_index(c, bx, ax, ay, az);
-      src = a.cell_start[lin];
-      cnt = a.cell_start[lin + 1] - src;
+      uint32_t end;
+      cell_range<TB>(a, (uint32_t)box_tiled_index(c, bx, ax, ay, az), src, end);
+      cnt = end - src;
     }
   }
   uint32_t total;
@@ -962,6 +979,7 @@ __device__ __forceinline__ bool next_task(const StepConsts& c, const TiledArgs& 
 
 // Neighbour ranges of the task (lane nb < 27 holds neighbour nb), with
 // whole cells out of reach of the query box emptied.
+template <int TB>
 __device__ __forceinline__ void task_neighbours(const StepConsts& c, const TiledArgs& a, DenseTask& t,
                                                 const Box3& qb, float hc2) {
   const int nb = threadIdx.x & 31;
@@ -970,7 +988,8 @@ __device__ __forceinline__ void task_neighbours(const StepConsts& c, const Tiled
     const SceneBox& bx = c.boxes[t.cg.sc];
     const int dx = nb / 9 - 1, dy = (nb / 3) % 3 - 1, dz = nb % 3 - 1;
     const int lin = box_tiled_index(c, bx, t.cg.ax + dx, t.cg.ay + dy, t.cg.az + dz);
-    const uint32_t s0 = a.cell_start[lin], e0 = a.cell_start[lin + 1];
+    uint32_t s0, e0;
+    cell_range<TB>(a, (uint32_t)lin, s0, e0);
     // The neighbour cell's box in query-cell coordinates, widened by 1e-3 h0
     // for cell-local coordinates rounded just outside [0, h0].
     const float m = 1e-3f * c.h0f;
@@ -1013,7 +1032,7 @@ __global__ void __launch_bounds__(kWT, 4) k_density_dense(StepConsts c, TiledArg
     const uint32_t qi = t.q0 + (uint32_t)lane;
     const float4 q = qv ? a.cpos[qi] : make_float4(kFar, kFar, kFar, 0.f);
     const Box3 qb = warp_box(q.x, q.y, q.z, qv);
-    task_neighbours(c, a, t, qb, hc2);
+    task_neighbours<TB>(c, a, t, qb, hc2);
     const f2 PX = f2_pack(q.x, q.x), PY = f2_pack(q.y, q.y), PZ = f2_pack(q.z, q.z);
     // Mask entries: reserve the task's upper bound (one entry per chunk of
     // every neighbour cell in reach).
@@ -1216,7 +1235,7 @@ __global__ void __launch_bounds__(kWT, 2) k_force_dense(StepConsts c, TiledArgs 
       }
     } else {
       const Box3 qb = warp_box(qp.x, qp.y, qp.z, qv);
-      task_neighbours(c, a, t, qb, hc2);
+      task_neighbours<TB>(c, a, t, qb, hc2);
       for (int nb = 0; nb < 27; ++nb) {
         const uint32_t s0 = __shfl_sync(0xffffffffu, t.nb_s, nb), e0 = __shfl_sync(0xffffffffu, t.nb_e, nb);
         if (s0 >= e0) continue;
@@ -1346,6 +1365,7 @@ void launch_comp_tiled(const StepConsts& c, DevBuffers& b, cudaStream_t s, const
   a.mass = pc.mass;
   a.mat = pc.mat;
   a.cell_start = b.cell_start;
+  a.tile_start = b.tile_head;
   a.sorted_cell = b.sorted_cell;
   a.tile_slot = b.tile_slot;
   a.tile_crowd = b.tile_crowd;
