@@ -186,6 +186,42 @@ def test_tiled_sparse_and_out_of_bounds_particles(gpu, oracle_mod):
     assert np.isfinite(w.pos[fin]).all()
 
 
+@pytest.mark.parametrize("tile", [4, 2])
+def test_sort_extreme_tiles(gpu, oracle_mod, tile):
+    """The per-tile sort's paths side by side: a cell of 5,000 particles (ordered by
+    counting, above the bitonic limit), cells of ~100 (the bitonic CTA), tiles of ~1,600
+    particles in cells of ~25 (too many to order in shared memory), ordinary tiles, and
+    tiles left empty between them; the density gate against the oracle and the same bits
+    on a second run."""
+    O = oracle_mod
+    p = ref_test_params(gravity=(0.0, 0.0, 0.0))
+    p.bounds_min, p.bounds_max = (-3.0, -3.0, -3.0), (3.0, 3.0, 3.0)
+    rng = np.random.default_rng(tile)
+    h = p.h
+    big = rng.uniform(0.0, h, (5000, 3)) + np.array([-2.0, -2.0, -2.0])           # one cell
+    mid = rng.uniform(0.0, 2 * h, (800, 3)) + np.array([1.6, -2.0, -2.0])          # 8 cells of ~100
+    wide = rng.uniform(0.0, 8 * h, (12800, 3)) + np.array([-2.0, 0.4, 0.4])        # cells of ~25
+    rest = rng.uniform(-0.6, 0.6, (600, 3))
+    pos = np.concatenate([big, mid, wide, rest])
+    vel = rng.normal(0.0, 0.05, pos.shape)
+    ow = O.OracleWorld(p, threads=O.max_threads())
+    ow.add_particles(pos, 0.02, vel=vel)
+    ow.step(0.0005)
+    outs = []
+    for _ in range(2):
+        w = gpu.FluidWorld(p, "comp")
+        w.set_tuning(comp_tile=tile)
+        w.add_particles(pos, 0.02, vel=vel)
+        w.step(0.0005)
+        outs.append((w.rho.copy(), w.pos.copy()))
+    ro = ow.get(O.F_RHO)
+    err = float(np.max(np.abs(outs[0][0] - ro) / ro))
+    print("extreme tiles", tile, err)
+    assert err <= RHO_TOL, err
+    assert_bits_equal(outs[0][0], outs[1][0], "density run-to-run")
+    assert_bits_equal(outs[0][1], outs[1][1], "positions run-to-run")
+
+
 @pytest.mark.parametrize("spacing,halo_cap,tile", [(0.08, None, 4), (0.08, 2500, 4), (0.068, None, 4),
                                                    (0.08, None, 2), (0.068, None, 2)])
 def test_compressed_regimes(gpu, oracle_mod, spacing, halo_cap, tile):
