@@ -261,9 +261,12 @@ __device__ __forceinline__ unsigned long long order_key(const unsigned long long
 }
 
 // The cells k_order left: one CTA per cell (persistent grid over the
-// device-side list) sorts the cell's (key, particle) pairs in shared memory
-// with a bitonic network padded to a power of two (keys are unique: they end
-// in the insertion index), then writes them to their final slots.
+// device-side list) stages the cell's (key, particle) pairs in shared memory
+// (keys are unique: they end in the insertion index).  A cell of at most
+// kRankCount particles ranks each pair by counting the smaller keys (no
+// barrier between steps); a larger one is sorted with a bitonic network
+// padded to a power of two.  Either way each particle goes to its final slot.
+constexpr uint32_t kRankCount = 256;
 __global__ void __launch_bounds__(kOrderThreads) k_order_large(const uint32_t* __restrict__ cell_start,
                                                               const uint32_t* __restrict__ tmp,
                                                               const uint32_t* __restrict__ id,
@@ -291,6 +294,15 @@ __global__ void __launch_bounds__(kOrderThreads) k_order_large(const uint32_t* _
       }
     }
     __syncthreads();
+    if (cnt <= kRankCount) {
+      for (uint32_t k = threadIdx.x; k < cnt; k += kOrderThreads) {
+        const unsigned long long mine = s_key[k];
+        uint32_t r = 0;
+        for (uint32_t q = 0; q < cnt; ++q) r += s_key[q] < mine ? 1u : 0u;
+        perm[cs + r] = s_val[k];
+      }
+      continue;  // uniform; the next cell's staging waits at the loop's first barrier
+    }
     for (uint32_t size = 2; size <= m; size <<= 1) {
       for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
         for (uint32_t k = threadIdx.x; k < m / 2; k += kOrderThreads) {
@@ -411,9 +423,20 @@ __global__ void __launch_bounds__(kThreads) k_tile_cells(int n, int ncells, cons
         }
       }
     } else {
-      for (uint32_t e = ts + threadIdx.x; e < te; e += blockDim.x) {
-        const uint32_t i = tmp[e];
-        rank[i] = atomicAdd(&s_cnt[cell_of[i] - cell0], 1u);
+      // A crowded tile: kTileCache particles per thread per round, their
+      // loads issued before their counters are taken.
+      for (uint32_t e0 = ts + threadIdx.x; e0 < te; e0 += (uint32_t)(kTileCache * kThreads)) {
+        uint32_t ii[kTileCache], ll[kTileCache];
+#pragma unroll
+        for (int j = 0; j < kTileCache; ++j) {
+          const uint32_t e = e0 + (uint32_t)(j * kThreads);
+          ii[j] = e < te ? tmp[e] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < kTileCache; ++j) ll[j] = e0 + (uint32_t)(j * kThreads) < te ? cell_of[ii[j]] - cell0 : 0u;
+#pragma unroll
+        for (int j = 0; j < kTileCache; ++j)
+          if (e0 + (uint32_t)(j * kThreads) < te) rank[ii[j]] = atomicAdd(&s_cnt[ll[j]], 1u);
       }
     }
     __syncthreads();
@@ -469,9 +492,22 @@ __global__ void __launch_bounds__(kThreads) k_tile_cells(int n, int ncells, cons
         for (int j = 0; j < kTileCache; ++j)
           if (ts + threadIdx.x + (uint32_t)(j * kThreads) < te) out[ts + s_off[cl[j]] + cr[j]] = ci[j];
       } else {
-        for (uint32_t e = ts + threadIdx.x; e < te; e += blockDim.x) {
-          const uint32_t i = tmp[e];
-          out[ts + s_off[cell_of[i] - cell0] + rank[i]] = i;
+        for (uint32_t e0 = ts + threadIdx.x; e0 < te; e0 += (uint32_t)(kTileCache * kThreads)) {
+          uint32_t ii[kTileCache], ll[kTileCache], rr[kTileCache];
+#pragma unroll
+          for (int j = 0; j < kTileCache; ++j) {
+            const uint32_t e = e0 + (uint32_t)(j * kThreads);
+            ii[j] = e < te ? tmp[e] : 0u;
+          }
+#pragma unroll
+          for (int j = 0; j < kTileCache; ++j) {
+            const bool v = e0 + (uint32_t)(j * kThreads) < te;
+            ll[j] = v ? cell_of[ii[j]] - cell0 : 0u;
+            rr[j] = v ? rank[ii[j]] : 0u;
+          }
+#pragma unroll
+          for (int j = 0; j < kTileCache; ++j)
+            if (e0 + (uint32_t)(j * kThreads) < te) out[ts + s_off[ll[j]] + rr[j]] = ii[j];
         }
       }
       __syncthreads();  // the by-cell order is complete
