@@ -1137,9 +1137,11 @@ __global__ void __launch_bounds__(kWT, 4) k_density_dense(StepConsts c, TiledArg
 // 8 rounds and at the end of the chunk, uniformly across the warp.
 template <int TB, bool kShear>
 __global__ void __launch_bounds__(kWT, 2) k_force_dense(StepConsts c, TiledArgs a) {
-  __shared__ float4 s_pos[kWarps][32];
-  __shared__ float4 s_vel[kWarps][32];
-  __shared__ float s_mr[kWarps][32];
+  // The chunk's 32 candidates, and in slot 32 a weightless copy of its first
+  // (mass and m/rho 0) that pads the two-candidate rounds.
+  __shared__ float4 s_pos[kWarps][33];
+  __shared__ float4 s_vel[kWarps][33];
+  __shared__ float s_mr[kWarps][33];
   __shared__ __align__(16) float s_pp[kWarps][32 * 4];  // the chunk's positions, pair-interleaved
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   float* sp = s_pp[w];
@@ -1159,24 +1161,31 @@ __global__ void __launch_bounds__(kWT, 2) k_force_dense(StepConsts c, TiledArgs 
     ForcePart part;
     ForcePart2 part2;
     zero(part2);
+    // Stages this lane's candidate (offset position p, velocity, m/rho) in
+    // its slot; lane 0 also fills the padding slot 32.
+    auto stage = [&](float4 p, float4 v, float mr) {
+      s_pos[w][lane] = p;
+      s_vel[w][lane] = v;
+      s_mr[w][lane] = mr;
+      if (lane == 0) {
+        s_pos[w][32] = make_float4(p.x, p.y, p.z, 0.f);
+        s_vel[w][32] = v;
+        s_mr[w][32] = 0.f;
+      }
+    };
     // The walk of one staged chunk given this lane's in-range bits (bit k =
     // candidate k; zero for a lane without a query).
     auto walk = [&](uint32_t mask) {
       if (!kShear) {
-        // Two candidates per round; a lane out of candidates pads with a
-        // weightless copy of slot 0.
+        // Two candidates per round; a lane out of candidates takes the
+        // weightless padding slot.
         const int rounds = (int)(__reduce_max_sync(0xffffffffu, (unsigned)__popc(mask)) + 1) >> 1;
         for (int r = 0; r < rounds; ++r) {
-          const bool ha = mask != 0;
-          const int ka = ha ? __ffs(mask) - 1 : 0;
+          const int ka = mask != 0 ? __ffs(mask) - 1 : 32;
           mask &= mask - 1;
-          const bool hb = mask != 0;
-          const int kb = hb ? __ffs(mask) - 1 : 0;
+          const int kb = mask != 0 ? __ffs(mask) - 1 : 32;
           mask &= mask - 1;
-          float4 pa = s_pos[w][ka], pb = s_pos[w][kb];
-          pa.w = ha ? pa.w : 0.f;
-          pb.w = hb ? pb.w : 0.f;
-          pair2_listed(Q, pa, s_vel[w][ka], ha ? s_mr[w][ka] : 0.f, pb, s_vel[w][kb], hb ? s_mr[w][kb] : 0.f,
+          pair2_listed(Q, s_pos[w][ka], s_vel[w][ka], s_mr[w][ka], s_pos[w][kb], s_vel[w][kb], s_mr[w][kb],
                        part2);
           if ((r & 7) == 7) fold2(acc, part2);
         }
@@ -1226,9 +1235,7 @@ __global__ void __launch_bounds__(kWT, 2) k_force_dense(StepConsts c, TiledArgs 
         p.x += off[0];
         p.y += off[1];
         p.z += off[2];
-        s_pos[w][lane] = p;
-        s_vel[w][lane] = cv ? a.cvel[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-        s_mr[w][lane] = cv ? a.cmr[j] : 0.f;
+        stage(p, cv ? a.cvel[j] : make_float4(0.f, 0.f, 0.f, 0.f), cv ? a.cmr[j] : 0.f);
         __syncwarp();
         walk(mask);
         __syncwarp();  // the chunk is consumed before the next one is staged
@@ -1250,10 +1257,8 @@ __global__ void __launch_bounds__(kWT, 2) k_force_dense(StepConsts c, TiledArgs 
           p.x += off[0];
           p.y += off[1];
           p.z += off[2];
-          s_pos[w][lane] = p;
+          stage(p, cv ? a.cvel[j] : make_float4(0.f, 0.f, 0.f, 0.f), cv ? a.cmr[j] : 0.f);
           put_pair_slot(sp, (uint32_t)lane, p);
-          s_vel[w][lane] = cv ? a.cvel[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-          s_mr[w][lane] = cv ? a.cmr[j] : 0.f;
           __syncwarp();
           // In-range bits (r^2 < hc2; the sign of r^2 - hc2, which is never
           // -0), shifted in so that the chunk's first candidate ends in the
