@@ -822,84 +822,165 @@ __device__ void push_out(const BodyArgs& a, const PhyCoupleBody& b, V3d& pos, V3
 
 // Flags the particles inside any body: their insertion index and slot are
 // appended (in no particular order) to key / val, the count to *count.
+// mask[s] = the bit of the one body that holds slot s (bodies 0..31); a
+// particle inside two or more bodies sets *multi.
 __global__ void __launch_bounds__(kCT) k_body_flags(BodyArgs a, int n, const double* px, const double* py,
                                                      const double* pz, const uint32_t* id, uint32_t* key,
-                                                     uint32_t* val, uint32_t* count) {
+                                                     uint32_t* val, uint32_t* count, uint32_t* mask,
+                                                     uint32_t* multi) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const V3d p = v3(px[s], py[s], pz[s]);
-  bool inside = false;
-  for (int bi = 0; bi < a.nb && !inside; ++bi) inside = contains_local(a, a.bodies[bi], to_local(a.bodies[bi], p));
-  if (!inside) return;
+  int hits = 0, first = 0;
+  for (int bi = 0; bi < a.nb; ++bi)
+    if (contains_local(a, a.bodies[bi], to_local(a.bodies[bi], p))) {
+      if (hits == 0) first = bi;
+      ++hits;
+    }
+  if (hits == 0) return;
+  if (hits > 1) atomicOr(multi, 1u);
+  mask[s] = first < 32 ? 1u << first : 0u;
   const uint32_t k = atomicAdd(count, 1u);
   key[k] = id[s];
   val[k] = (uint32_t)s;
 }
 
+// One particle's contact with one body that holds it (the body of the
+// reference's inner loop, world.rs:452-481): a static body pushes the particle
+// out; a dynamic body takes the normal impulse of an approaching particle,
+// counts its displaced volume and pushes it out (push_out's velocity replaces
+// the particle's, as there).
+__device__ __forceinline__ void body_contact(const BodyArgs& a, PhyCoupleBody& body, int bi, V3d p_world,
+                                             double m_p, double particle_vol, V3d& pos, V3d& vel, V3d& v_p) {
+  constexpr double restitution = 0.0;
+  const V3d local = to_local(body, p_world);
+  const V3d n = vnorm(local) > 1e-9 ? vnormalize(local) : v3(0.0, 1.0, 0.0);
+  if (body.inv_mass <= 0.0) {
+    push_out(a, body, pos, vel);
+    v_p = vel;
+    return;
+  }
+  const double v_rel_n = vdot(v_p - v3(body.vel[0], body.vel[1], body.vel[2]), n);
+  if (v_rel_n < 0.0) {
+    const double inv_sum = (1.0 / m_p) + body.inv_mass;
+    const double j_mag = -(1.0 + restitution) * v_rel_n / inv_sum;
+    const V3d j = n * j_mag;
+    v_p = v_p + j / m_p;
+    body.vel[0] = body.vel[0] + -j.x * body.inv_mass;  // apply_impulse(-j) (shape.rs:461-463)
+    body.vel[1] = body.vel[1] + -j.y * body.inv_mass;
+    body.vel[2] = body.vel[2] + -j.z * body.inv_mass;
+  }
+  a.displaced[bi] = a.displaced[bi] + particle_vol;
+  push_out(a, body, pos, vel);
+  v_p = vel;
+}
+
 // The reference's loops over the flagged particles (insertion order) and the
-// bodies, then the buoyancy impulses.  One thread.
-__global__ void k_body_contacts(StepConsts c, BodyArgs a, const uint32_t* slots, int m, const double* mass,
-                                double* px, double* py, double* pz, double* vx, double* vy, double* vz, double dt,
-                                double particle_vol) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+// bodies, then the buoyancy impulses (one CTA of kCT threads).  A body's
+// velocity changes particle after particle, so the loops are ordered; but
+// when every flagged particle lies in exactly one body (of at most 32), the
+// bodies share no particle and each body's own sequence runs on its own
+// thread: the warps first list each body's particles in insertion order (into
+// `lists`), then thread b walks body b's.  Otherwise one thread runs the loops
+// as written.  Both give the same bits.
+__global__ void __launch_bounds__(kCT) k_body_contacts(StepConsts c, BodyArgs a, const uint32_t* slots, int m,
+                                                        const double* mass, double* px, double* py, double* pz,
+                                                        double* vx, double* vy, double* vz, double dt,
+                                                        double particle_vol, const uint32_t* mask,
+                                                        const uint32_t* multi, uint32_t* lists) {
+  __shared__ uint32_t s_cnt[32];
+  __shared__ uint32_t s_off[33];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const double rho_f = c.rest;
-  const double restitution = 0.0;
-  for (int bi = 0; bi < a.nb; ++bi) a.displaced[bi] = 0.0;
-  for (int k = 0; k < m; ++k) {
-    const uint32_t s = slots[k];
-    const V3d p_world = v3(px[s], py[s], pz[s]);
-    V3d pos = p_world;
-    V3d vel = v3(vx[s], vy[s], vz[s]);
-    V3d v_p = vel;
-    const double m_p = mass[s];
+  if (t == 0)
+    for (int bi = 0; bi < a.nb; ++bi) a.displaced[bi] = 0.0;
+  __syncthreads();
+  const bool by_body = a.nb <= 32 && *multi == 0u;  // uniform
+  if (!by_body) {
+    if (t == 0)
+      for (int k = 0; k < m; ++k) {
+        const uint32_t s = slots[k];
+        const V3d p_world = v3(px[s], py[s], pz[s]);
+        V3d pos = p_world;
+        V3d vel = v3(vx[s], vy[s], vz[s]);
+        V3d v_p = vel;
+        const double m_p = mass[s];
+        for (int bi = 0; bi < a.nb; ++bi) {
+          PhyCoupleBody& body = a.bodies[bi];
+          if (!contains_local(a, body, to_local(body, p_world))) continue;
+          body_contact(a, body, bi, p_world, m_p, particle_vol, pos, vel, v_p);
+        }
+        px[s] = pos.x;
+        py[s] = pos.y;
+        pz[s] = pos.z;
+        vx[s] = v_p.x;
+        vy[s] = v_p.y;
+        vz[s] = v_p.z;
+      }
+  } else {
+    const int nw = blockDim.x >> 5;
+    for (int bb = warp; bb < a.nb; bb += nw) {
+      uint32_t cnt = 0;
+      for (int k0 = 0; k0 < m; k0 += 32) {
+        const int k = k0 + lane;
+        cnt += __popc(__ballot_sync(0xffffffffu, k < m && mask[slots[k]] == (1u << bb)));
+      }
+      if (lane == 0) s_cnt[bb] = cnt;
+    }
+    __syncthreads();
+    if (t == 0) {
+      s_off[0] = 0;
+      for (int bi = 0; bi < a.nb; ++bi) s_off[bi + 1] = s_off[bi] + s_cnt[bi];
+    }
+    __syncthreads();
+    for (int bb = warp; bb < a.nb; bb += nw) {
+      uint32_t o = s_off[bb];
+      for (int k0 = 0; k0 < m; k0 += 32) {
+        const int k = k0 + lane;
+        const bool hit = k < m && mask[slots[k]] == (1u << bb);
+        const uint32_t bal = __ballot_sync(0xffffffffu, hit);
+        if (hit) lists[o + __popc(bal & ((1u << lane) - 1u))] = slots[k];
+        o += __popc(bal);
+      }
+    }
+    __syncthreads();
+    if (t < a.nb) {
+      PhyCoupleBody& body = a.bodies[t];
+      for (uint32_t e = s_off[t]; e < s_off[t + 1]; ++e) {
+        const uint32_t s = lists[e];
+        const V3d p_world = v3(px[s], py[s], pz[s]);
+        V3d pos = p_world;
+        V3d vel = v3(vx[s], vy[s], vz[s]);
+        V3d v_p = vel;
+        body_contact(a, body, t, p_world, mass[s], particle_vol, pos, vel, v_p);
+        px[s] = pos.x;
+        py[s] = pos.y;
+        pz[s] = pos.z;
+        vx[s] = v_p.x;
+        vy[s] = v_p.y;
+        vz[s] = v_p.z;
+      }
+    }
+  }
+  __syncthreads();
+  if (t == 0)
     for (int bi = 0; bi < a.nb; ++bi) {
       PhyCoupleBody& body = a.bodies[bi];
-      const V3d local = to_local(body, p_world);
-      if (!contains_local(a, body, local)) continue;
-      const V3d n = vnorm(local) > 1e-9 ? vnormalize(local) : v3(0.0, 1.0, 0.0);
-      if (body.inv_mass <= 0.0) {
-        push_out(a, body, pos, vel);
-        v_p = vel;
-        continue;
-      }
-      const double v_rel_n = vdot(v_p - v3(body.vel[0], body.vel[1], body.vel[2]), n);
-      if (v_rel_n < 0.0) {
-        const double inv_sum = (1.0 / m_p) + body.inv_mass;
-        const double j_mag = -(1.0 + restitution) * v_rel_n / inv_sum;
-        const V3d j = n * j_mag;
-        v_p = v_p + j / m_p;
-        body.vel[0] = body.vel[0] + -j.x * body.inv_mass;  // apply_impulse(-j) (shape.rs:461-463)
-        body.vel[1] = body.vel[1] + -j.y * body.inv_mass;
-        body.vel[2] = body.vel[2] + -j.z * body.inv_mass;
-      }
-      a.displaced[bi] = a.displaced[bi] + particle_vol;
-      push_out(a, body, pos, vel);
-      v_p = vel;
+      if (body.inv_mass <= 0.0) continue;
+      const double vol_b = body_volume(a, body);
+      const double v_sub = a.displaced[bi] > 0.0 ? vol_b : 0.0;
+      const double rv = rho_f * v_sub;
+      body.vel[0] = body.vel[0] + -c.g[0] * rv * dt * body.inv_mass;
+      body.vel[1] = body.vel[1] + -c.g[1] * rv * dt * body.inv_mass;
+      body.vel[2] = body.vel[2] + -c.g[2] * rv * dt * body.inv_mass;
     }
-    px[s] = pos.x;
-    py[s] = pos.y;
-    pz[s] = pos.z;
-    vx[s] = v_p.x;
-    vy[s] = v_p.y;
-    vz[s] = v_p.z;
-  }
-  for (int bi = 0; bi < a.nb; ++bi) {
-    PhyCoupleBody& body = a.bodies[bi];
-    if (body.inv_mass <= 0.0) continue;
-    const double vol_b = body_volume(a, body);
-    const double v_sub = a.displaced[bi] > 0.0 ? vol_b : 0.0;
-    const double rv = rho_f * v_sub;
-    body.vel[0] = body.vel[0] + -c.g[0] * rv * dt * body.inv_mass;
-    body.vel[1] = body.vel[1] + -c.g[1] * rv * dt * body.inv_mass;
-    body.vel[2] = body.vel[2] + -c.g[2] * rv * dt * body.inv_mass;
-  }
 }
 
 }  // namespace
 
 size_t couple_bodies_scratch_bytes(int n, int nb, uint64_t n_data, uint64_t n_faces) {
   return (size_t)nb * sizeof(PhyCoupleBody) + 8 * (size_t)nb + 8 * (size_t)n_data + 4 * (size_t)n_faces +
-         16 * (size_t)n + 1024 * (size_t)((n + kRTile - 1) / kRTile) + 512;
+         20 * (size_t)n + 1024 * (size_t)((n + kRTile - 1) / kRTile) + 512;
 }
 
 int launch_couple_bodies(const StepConsts& c, DevBuffers& b, const CoupleBodiesLaunch& l, cudaStream_t s) {
@@ -917,8 +998,10 @@ int launch_couple_bodies(const StepConsts& c, DevBuffers& b, const CoupleBodiesL
   uint32_t* key1 = key0 + n;
   uint32_t* val0 = key1 + n;
   uint32_t* val1 = val0 + n;
-  uint32_t* hist = val1 + n;
+  uint32_t* mask = val1 + n;  // by slot: the bit of the one body holding it
+  uint32_t* hist = mask + n;
   uint32_t* count = hist + 256 * nbk;
+  uint32_t* multi = count + 1;
   if (l.n_data && cudaMemcpyAsync(data, l.data, l.n_data * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
     return -1;
   if (l.n_faces &&
@@ -931,9 +1014,9 @@ int launch_couple_bodies(const StepConsts& c, DevBuffers& b, const CoupleBodiesL
   a.faces = faces;
   a.displaced = displaced;
   const ParticleConsts& pc = b.pc[b.cur];
-  cudaMemsetAsync(count, 0, sizeof(uint32_t), s);
+  cudaMemsetAsync(count, 0, 2 * sizeof(uint32_t), s);  // count and multi
   const int blocks = (n + kCT - 1) / kCT;
-  k_body_flags<<<blocks, kCT, 0, s>>>(a, n, b.pv1[0], b.pv1[1], b.pv1[2], pc.id, key0, val0, count);
+  k_body_flags<<<blocks, kCT, 0, s>>>(a, n, b.pv1[0], b.pv1[1], b.pv1[2], pc.id, key0, val0, count, mask, multi);
   uint32_t m = 0;
   if (cudaMemcpyAsync(&m, count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
@@ -955,8 +1038,9 @@ int launch_couple_bodies(const StepConsts& c, DevBuffers& b, const CoupleBodiesL
       vout = t;
     }
   }
-  k_body_contacts<<<1, 32, 0, s>>>(c, a, vin, (int)m, pc.mass, b.pv1[0], b.pv1[1], b.pv1[2], b.pv1[3], b.pv1[4],
-                                    b.pv1[5], c.dt, l.particle_vol);
+  // kout is free after the sort: it takes the per-body lists.
+  k_body_contacts<<<1, kCT, 0, s>>>(c, a, vin, (int)m, pc.mass, b.pv1[0], b.pv1[1], b.pv1[2], b.pv1[3], b.pv1[4],
+                                     b.pv1[5], c.dt, l.particle_vol, mask, multi, kout);
   if (cudaGetLastError() != cudaSuccess ||
       cudaMemcpyAsync(l.bodies, bodies, (size_t)l.nb * sizeof(PhyCoupleBody), cudaMemcpyDeviceToHost, s) !=
           cudaSuccess ||

@@ -259,6 +259,35 @@ def test_couple_bodies_f64_bitwise_and_next_steps(gpu, oracle_mod):
     assert_bits_equal(w.vel, ow.get(O.F_VEL), "velocities after coupling and 5 steps")
 
 
+@pytest.mark.parametrize("layout", ["disjoint", "overlapping", "many"])
+def test_couple_bodies_per_body_and_ordered_loops(gpu, oracle_mod, layout):
+    """Disjoint bodies (every flagged particle in one body: each body's sequence on its own
+    thread), two overlapping spheres and a particle in both (the ordered loops as
+    written), and 40 bodies (more than the per-body path takes): bit for bit against the
+    oracle's loops, body velocities included."""
+    O = oracle_mod
+    w, ow, _ = _pair(gpu, O, lo=-0.6, hi=0.6, spacing=0.06, steps=1)
+    rng = np.random.default_rng({"disjoint": 1, "overlapping": 2, "many": 3}[layout])
+    if layout == "disjoint":
+        centres = [(x, y, z) for x in (-0.3, 0.3) for y in (-0.3, 0.3) for z in (-0.3, 0.3)]
+        bodies = [{"shape": "sphere", "size": (0.12,), "pos": c, "vel": tuple(rng.normal(0, 0.3, 3)),
+                   "inv_mass": float(rng.uniform(0.5, 5.0))} for c in centres]
+        bodies[3] = {"shape": "box", "size": (0.1, 0.08, 0.12), "pos": centres[3], "rot": _quat((1, 1, 0), 0.5),
+                     "inv_mass": 0.0}
+    elif layout == "overlapping":
+        bodies = [{"shape": "sphere", "size": (0.2,), "pos": (0.0, 0.0, 0.0), "vel": (0.0, -0.3, 0.0),
+                   "inv_mass": 2.0},
+                  {"shape": "sphere", "size": (0.2,), "pos": (0.15, 0.05, 0.0), "vel": (0.2, 0.0, 0.0),
+                   "inv_mass": 3.0},
+                  {"shape": "sphere", "size": (0.1,), "pos": (-0.4, 0.4, 0.4), "inv_mass": 1.0}]
+    else:
+        bodies = [{"shape": "sphere", "size": (0.05,), "pos": tuple(rng.uniform(-0.55, 0.55, 3)),
+                   "vel": tuple(rng.normal(0, 0.2, 3)), "inv_mass": float(rng.uniform(0.5, 5.0))}
+                  for _ in range(40)]
+    vg = _bodies_check(O, w, ow, bodies)
+    assert np.isfinite(vg).all()
+
+
 def test_couple_bodies_repeated_with_moving_bodies(gpu, oracle_mod):
     """Bodies integrated by the caller between steps (sph/tests.rs:160-169 style): the
     coupled trajectory stays bit-identical."""
