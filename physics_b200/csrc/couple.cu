@@ -508,7 +508,7 @@ __global__ void __launch_bounds__(kCT) k_heat_particles(StepConsts c, HeatArgs h
 // counts digit d in block b, and its exclusive scan (digit-major) is the
 // first output slot of block b's keys of digit d.
 constexpr int kRT = 256;
-constexpr int kRRounds = 8;
+constexpr int kRRounds = 32;
 constexpr int kRTile = kRT * kRRounds;
 
 __global__ void __launch_bounds__(kRT) k_radix_hist(const uint32_t* key, int n, int shift, uint32_t* hist,
