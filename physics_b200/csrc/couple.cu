@@ -179,8 +179,8 @@ __global__ void __launch_bounds__(kCT) k_couple_points(StepConsts c, CoupleArgs 
 // candidates they hold (v_j + share, with the velocities they gathered).
 // Points with more than kPB candidates have no list and read their
 // candidates through their cell table.
-constexpr int kGW = 8;          // warps of the walk: points per group at most
-constexpr int kPer = 16;        // candidates a lane holds per chunk
+constexpr int kGW = 16;         // warps of the walk: points per group at most
+constexpr int kPer = 8;         // candidates a lane holds per chunk
 constexpr int kWB = 32 * kPer;  // candidates per chunk of a warp
 constexpr int kPB = 4096;       // candidates a point may have for a list
 constexpr int kTabU = 56;       // u32 per point table: in, total, beg[27], cnt[27]
@@ -196,7 +196,7 @@ __device__ __forceinline__ bool point_in(const StepConsts& c, const double* q) {
 // point w overlaps that of point w - m (both in bounds, centre cells at most
 // 2 apart on every axis).
 __global__ void __launch_bounds__(256) k_point_tables(StepConsts c, CoupleArgs a, int nb, uint32_t* tab,
-                                                      uint32_t* totals, uint8_t* conf) {
+                                                      uint32_t* totals, uint16_t* conf) {
   const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (w >= nb) return;
   const double* q = a.pts + 10 * (size_t)w;
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(256) k_point_tables(StepConsts c, CoupleArgs a
     t[0] = in ? 1u : 0u;
     t[1] = total;
     totals[w] = in && total <= (uint32_t)kPB ? total : 0u;
-    conf[w] = (uint8_t)bits;
+    conf[w] = (uint16_t)bits;
   }
 }
 
@@ -261,7 +261,7 @@ struct PointLists {
   const uint32_t* off;
   const uint32_t* idx;
   const double* m;
-  const uint8_t* conf;
+  const uint16_t* conf;
 };
 
 // Cell table of a point without a list (its warp's copy).
@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(kGW * 32, 1) k_couple_points_grouped(StepConst
                                                                        PointLists L) {
   extern __shared__ __align__(16) unsigned char smem[];
   double2* s_pw = reinterpret_cast<double2*>(smem);                    // [kGW][2 kWB]
-  uint8_t* s_conf = reinterpret_cast<uint8_t*>(s_pw + 2 * kWB * kGW);  // [nb]
+  uint16_t* s_conf = reinterpret_cast<uint16_t*>(s_pw + 2 * kWB * kGW);  // [nb]
   __shared__ WarpTable s_tab[kGW];
   __shared__ double s_r[kGW][4];
   __shared__ int s_group;
@@ -1164,7 +1164,7 @@ void launch_couple_points(const StepConsts& c, DevBuffers& b, double* d_pts, int
   constexpr int kBatch = 16384;
   static const bool smem_ok = [] {
     return cudaFuncSetAttribute(k_couple_points_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(kGroupedSmemFixed + kBatch)) == cudaSuccess;
+                                (int)(kGroupedSmemFixed + kBatch * sizeof(uint16_t))) == cudaSuccess;
   }();
   if (!smem_ok) {
     k_couple_points<<<1, kCT, 0, s>>>(c, a);
@@ -1199,7 +1199,7 @@ void launch_couple_points(const StepConsts& c, DevBuffers& b, double* d_pts, int
                "point offsets");
     k_point_candidates<<<blocks, 256, 0, s>>>(ab, nb, sc.tab, sc.off, sc.idx, sc.m);
     PointLists L{sc.tab, sc.off, sc.idx, sc.m, sc.conf};
-    k_couple_points_grouped<<<1, kGW * 32, kGroupedSmemFixed + (size_t)nb, s>>>(c, ab, nb, L);
+    k_couple_points_grouped<<<1, kGW * 32, kGroupedSmemFixed + (size_t)nb * sizeof(uint16_t), s>>>(c, ab, nb, L);
     cuda_check(cudaGetLastError(), "couple points");
     // The offsets' host copy must outlive the upload.
     cuda_check(cudaStreamSynchronize(s), "couple points sync");

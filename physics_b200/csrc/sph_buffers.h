@@ -134,7 +134,7 @@ struct CouplePointsScratch {
   uint32_t* off = nullptr;
   uint32_t* idx = nullptr;
   double* m = nullptr;
-  uint8_t* conf = nullptr;
+  uint16_t* conf = nullptr;
   size_t cap_tab = 0, cap_totals = 0, cap_off = 0, cap_idx = 0, cap_m = 0, cap_conf = 0;
   void release();
 };
