@@ -209,6 +209,7 @@ struct TapeCopy {
   const uint32_t* nbr;      // column-major, stride nbr_stride
   uint32_t* nbr_dst;        // column-major, stride n
   int nbr_stride;
+  uint32_t* slot_of;        // nullable: insertion index -> recorded slot
 };
 
 __global__ void k_tape_copy(int n, TapeCopy t) {
@@ -217,7 +218,9 @@ __global__ void k_tape_copy(int n, TapeCopy t) {
 #pragma unroll
   for (int k = 0; k < 22; ++k) t.dst[k][s] = t.src[k][s];
   t.udst[0][s] = t.usrc[0][s];
-  t.udst[1][s] = t.usrc[1][s];
+  const uint32_t id = t.usrc[1][s];
+  t.udst[1][s] = id;
+  if (t.slot_of) t.slot_of[id] = (uint32_t)s;
   const uint32_t cnt = t.usrc[2][s];
   t.udst[2][s] = cnt;
   const uint32_t m = cnt < (uint32_t)kMaxNeighbors ? cnt : (uint32_t)kMaxNeighbors;
@@ -257,51 +260,41 @@ __global__ void k_copy_arrays(ArrayCopy a) {
   for (size_t k = done + i; k < bytes; k += stride) d[k] = s[k];
 }
 
-// The compensated step's outputs by insertion index (9 doubles each: rho, p,
-// mu, acc xyz, xsph xyz), for the records of the compensated adjoint.
-__global__ void k_comp_outputs_by_id(int n, const uint32_t* __restrict__ id, const double* __restrict__ rho,
-                                     const double* __restrict__ p, const double* __restrict__ mu,
-                                     const double* __restrict__ ax, const double* __restrict__ ay,
-                                     const double* __restrict__ az, const double* __restrict__ xx,
-                                     const double* __restrict__ xy, const double* __restrict__ xz,
-                                     double* __restrict__ out) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  double* o = out + 9 * (size_t)id[s];
-  o[0] = rho[s];
-  o[1] = p[s];
-  o[2] = mu[s];
-  o[3] = ax[s];
-  o[4] = ay[s];
-  o[5] = az[s];
-  o[6] = xx[s];
-  o[7] = xy[s];
-  o[8] = xz[s];
-}
+// The compensated step's outputs (its sorted order, slot q) written over the
+// recorded f64 ones (the recorded slot of the same particle, from slot_of):
+// density, pressure, p/rho^2 and m/rho from them, mu, acceleration, XSPH.
+struct CompOverride {
+  const uint32_t* id;  // compensated order: insertion index
+  const double* mass;
+  const double* rho;
+  const double* p;
+  const double* mu;
+  const double* acc[3];
+  const double* xsph[3];
+  const uint32_t* slot_of;
+  double* t_rho;
+  double* t_p;
+  double* t_pr2;
+  double* t_mr;
+  double* t_mu;
+  double* t_acc[3];
+  double* t_xsph[3];
+};
 
-// Overwrites a tape slot's density, pressure and force records (in the f64
-// recording step's order) with the compensated step's values of the same
-// particles, so the reverse sweep takes the compensated forward's branches
-// (max(0, rho - rho0), walls) and values; p/rho^2 and m/rho follow from them
-// with the f64 density pass's operations.
-__global__ void k_tape_override(int n, const uint32_t* __restrict__ id, const double* __restrict__ mass,
-                                const double* __restrict__ comp, double* rho, double* p, double* pr2, double* mr,
-                                double* mu, double* ax, double* ay, double* az, double* xx, double* xy, double* xz) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const double* o = comp + 9 * (size_t)id[s];
-  const double r = o[0], pr = o[1];
-  rho[s] = r;
-  p[s] = pr;
-  pr2[s] = __ddiv_rn(pr, __dmul_rn(r, r));
-  mr[s] = __ddiv_rn(mass[s], r);
-  mu[s] = o[2];
-  ax[s] = o[3];
-  ay[s] = o[4];
-  az[s] = o[5];
-  xx[s] = o[6];
-  xy[s] = o[7];
-  xz[s] = o[8];
+__global__ void k_comp_override(int n, CompOverride o) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const uint32_t s = o.slot_of[o.id[q]];
+  const double r = o.rho[q], pr = o.p[q];
+  o.t_rho[s] = r;
+  o.t_p[s] = pr;
+  o.t_pr2[s] = __ddiv_rn(pr, __dmul_rn(r, r));
+  o.t_mr[s] = __ddiv_rn(o.mass[q], r);
+  o.t_mu[s] = o.mu[q];
+  for (int k = 0; k < 3; ++k) {
+    o.t_acc[k][s] = o.acc[k][q];
+    o.t_xsph[k][s] = o.xsph[k][q];
+  }
 }
 
 // num-traits ToPrimitive::to_i64 on f64 with None -> 0 (grid.rs:25-33).
@@ -2006,13 +1999,13 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
   // f64 values.
   const Precision form = prec_;
   const bool comp = form == Precision::F32Comp;
-  double* comp_rec = nullptr;  // compensated outputs by insertion index, 9 per particle
+  uint32_t* slot_of = nullptr;  // compensated: insertion index -> recorded slot of the step being re-run
   if (comp) {
-    if (comp_rec_cap_ < 9 * n) {
-      dalloc(comp_rec_, 9 * n);
-      comp_rec_cap_ = 9 * n;
+    if (comp_rec_cap_ < n) {
+      dalloc(comp_rec_, n);
+      comp_rec_cap_ = n;
     }
-    comp_rec = comp_rec_;
+    slot_of = comp_rec_;
   }
   auto cleanup = [&]() {
     for (int k = 0; k < 3; ++k) b_.tape_fv[k] = nullptr;
@@ -2050,9 +2043,7 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
         TapeSlot& sl = slots[t - t0];
         const int si = t - t0;
         if (comp) {
-          // The f64 recording step from state t first; state t is kept in
-          // slot 1 for the compensated step that follows it.
-          snapshot(false, 1, false);
+          // The f64 recording step from state t first.
           prec_ = Precision::F64Plain;
           ensure_mode_buffers();  // f64 neighbour lists, kept for later sweeps
         }
@@ -2098,25 +2089,47 @@ void FluidWorld::step_backward(const double* gx, const double* gv, double* gx0, 
         tc.nbr = b_.nbr;
         tc.nbr_dst = const_cast<uint32_t*>(v.nbr);
         tc.nbr_stride = b_.capacity;
+        tc.slot_of = slot_of;
         k_tape_copy<<<grid_for(n), kThreads, 0, s>>>((int)n, tc);
         cuda_check(cudaMemcpyAsync(const_cast<uint32_t*>(v.cell_start), b_.cell_start, ncs * 4,
                                    cudaMemcpyDeviceToDevice, s),
                    "tape copy");
         if (comp) {
-          // Back to state t for the compensated step to state t+1; its
-          // outputs (by insertion index) replace the recorded f64 ones.
-          snapshot(true, 1, false);
+          // Back to state t for the compensated step to state t+1: the
+          // recording step left state t, sorted, in pv0 with the constants of
+          // that order current, and a step's result does not depend on the
+          // order of its input.  Its outputs replace the recorded f64 ones
+          // (matched through the particles' insertion indices).
+          ArrayCopy back{};
+          for (int k = 0; k < 6; ++k) {
+            back.src[k] = reinterpret_cast<const unsigned char*>(b_.pv0[k]);
+            back.dst[k] = reinterpret_cast<unsigned char*>(b_.pv1[k]);
+            back.bytes[k] = n * sizeof(double);
+          }
+          const size_t blocks = std::min<size_t>((n * sizeof(double) / 16 + kThreads - 1) / kThreads + 1, 1184);
+          k_copy_arrays<<<dim3((unsigned)blocks, 6), kThreads, 0, s>>>(back);
           prec_ = Precision::F32Comp;
           step_impl(tape_.dts[t]);
           const ParticleConsts& cq = b_.pc[b_.cur];
-          k_comp_outputs_by_id<<<grid_for(n), kThreads, 0, s>>>((int)n, cq.id, b_.rho, b_.p, b_.mu, b_.acc[0],
-                                                                b_.acc[1], b_.acc[2], b_.xsph[0], b_.xsph[1],
-                                                                b_.xsph[2], comp_rec);
-          k_tape_override<<<grid_for(n), kThreads, 0, s>>>(
-              (int)n, v.id, v.mass, comp_rec, const_cast<double*>(v.rho), const_cast<double*>(v.p),
-              const_cast<double*>(v.pr2), const_cast<double*>(v.mr), const_cast<double*>(v.mu),
-              const_cast<double*>(v.acc[0]), const_cast<double*>(v.acc[1]), const_cast<double*>(v.acc[2]),
-              const_cast<double*>(v.xsph[0]), const_cast<double*>(v.xsph[1]), const_cast<double*>(v.xsph[2]));
+          CompOverride co;
+          co.id = cq.id;
+          co.mass = cq.mass;
+          co.rho = b_.rho;
+          co.p = b_.p;
+          co.mu = b_.mu;
+          co.slot_of = slot_of;
+          co.t_rho = const_cast<double*>(v.rho);
+          co.t_p = const_cast<double*>(v.p);
+          co.t_pr2 = const_cast<double*>(v.pr2);
+          co.t_mr = const_cast<double*>(v.mr);
+          co.t_mu = const_cast<double*>(v.mu);
+          for (int a = 0; a < 3; ++a) {
+            co.acc[a] = b_.acc[a];
+            co.xsph[a] = b_.xsph[a];
+            co.t_acc[a] = const_cast<double*>(v.acc[a]);
+            co.t_xsph[a] = const_cast<double*>(v.xsph[a]);
+          }
+          k_comp_override<<<grid_for(n), kThreads, 0, s>>>((int)n, co);
           cuda_check(cudaGetLastError(), "tape override");
         }
       }

@@ -298,7 +298,7 @@ class FluidWorld {
   } tape_;
   // Reverse-sweep buffers kept between sweeps (freed by tape_clear).
   double* adj_work_ = nullptr;
-  double* comp_rec_ = nullptr;  // compensated adjoint: the compensated step's outputs by insertion index
+  uint32_t* comp_rec_ = nullptr;  // compensated adjoint: insertion index -> recorded slot
   size_t comp_rec_cap_ = 0;
   std::vector<double*> adj_slot_f_;
   std::vector<uint32_t*> adj_slot_u_;
