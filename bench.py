@@ -472,6 +472,8 @@ def run_ours(args):
         w.set_stream(stream.cuda_stream)
         mass = w.lattice_mass(0.1)
         w.add_particles(p, mass, vel=v)
+        if args.graph_chunk > 0:
+            w.set_tuning(graph_chunk=args.graph_chunk)
         return w
 
     def timed(w, steps, warmup, sample_clocks=False, phase=False):
@@ -532,17 +534,20 @@ def run_ours(args):
         errors = {"workload": f"teacher-forced: one f32c step and one f64 plain step from the state of the "
                               f"{args.full_steps}-step trajectory at each listed step",
                   "reference": "f64 plain step (bit-identical to the f64 oracle)", "at_step": {}}
-        done, ms_full = 0, 0.0
+        done, ms_full, segments, seg_clocks = 0, 0.0, [], []
         for s_probe in probes + [args.full_steps]:
             seg = s_probe - done
             if seg > 0:
-                ms_seg, _, _ = timed(traj, seg, 0)
+                ms_seg, clk, _ = timed(traj, seg, 0, sample_clocks=rank == 0)
                 ms_full += ms_seg
+                segments.append({"steps": [done, s_probe], "ms_per_step": ms_seg / seg,
+                                 "sm_mhz": clk["sm_mhz"] if clk else None,
+                                 "reasons": clk["reasons"] if clk else None})
                 done = s_probe
             if s_probe < args.full_steps and rank == 0:
                 errors["at_step"][str(s_probe)] = probe_errors(pb, new_world, traj, n, params)
         full = {"steps": args.full_steps, "value": world_size * n * args.full_steps / (ms_full / 1e3),
-                "ms_per_step": ms_full / args.full_steps}
+                "ms_per_step": ms_full / args.full_steps, "segments": segments}
         traj.set_timing(True)
         traj.phase_times(reset=True)
         traj.step(DT, 20)
@@ -553,6 +558,7 @@ def run_ours(args):
         traj.step(DT)
         full["pairs_per_particle_at_end"] = traj.step_counters()["pairs"] / n
         traj.set_counting(False)
+        full["dense_masks_at_end"] = traj.dense_mask_info()
         del traj
         if rank == 0:
             at = errors["at_step"].values()
@@ -834,6 +840,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--graph-chunk", type=int, default=0,
+                    help="steps per captured CUDA graph of the single-scene worlds (0: launch every step)")
     ap.add_argument("--batch-scenes", type=int, default=256, help="scenes of the batched form (0: skip)")
     ap.add_argument("--adjoint-directions", type=int, default=32,
                     help="finite-difference directions of the adjoint check (0: skip the adjoint)")

@@ -1177,25 +1177,32 @@ StepConsts FluidWorld::prepare_step(double dt) {
   return make_consts(dt);
 }
 
-// Grows the dense-cell mask buffer to the entries the tasks of a recent step
-// reserved (the pinned copy lags by the steps still in flight), within a
-// quarter of the free device memory and 16 GiB; tasks that find no room
+// Grows the dense-cell mask buffer ahead of the entries the dense-cell tasks
+// reserve.  The host reads the demand of a recent step from its pinned copy,
+// which lags by the steps still in flight (hundreds when a caller enqueues a
+// long run), and a collapsing fluid's demand keeps rising meanwhile; so once
+// the demand passes three quarters of the buffer it is re-read after a wait
+// and the buffer grows to three times it, and at least to 12 entries per
+// particle (a fluid collapsed to a thousand particles per cell reserves about
+// 8) and 2^20 entries, within a quarter of the free device memory and 16 GiB.  Tasks that find no room
 // filter again in the force pass, so the size never changes a result.  A
 // failed allocation leaves the buffer empty and is not retried below the
 // demand that failed.
 void FluidWorld::ensure_masks() {
   if (!tuning_.dense_masks || !b_.mask_ctl || !b_.mask_demand) return;
-  const unsigned long long want = *reinterpret_cast<volatile unsigned long long*>(b_.mask_demand);
-  if (want <= b_.mask_cap || want <= mask_tried_) return;
-  mask_tried_ = want;
+  const volatile unsigned long long* demand = b_.mask_demand;
+  const unsigned long long seen = *demand;
+  if (seen == 0 || 4 * seen <= 3 * b_.mask_cap || seen <= mask_tried_) return;
+  mask_tried_ = seen;
   constexpr unsigned long long kEntryBytes = 33 * sizeof(uint32_t);
   cuda_check(cudaStreamSynchronize(stream_), "mask buffer sync");
+  const unsigned long long want = std::max(seen, (unsigned long long)*demand);  // current after the wait
   size_t free_b = 0, total_b = 0;
   cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
   const unsigned long long limit = std::min<unsigned long long>(
       std::min<unsigned long long>(free_b / 4 + b_.mask_cap * kEntryBytes, 16ull << 30) / kEntryBytes,
       0xfffffffeull);
-  const unsigned long long cap = std::min(want + want / 2 + 1024, limit);
+  const unsigned long long cap = std::min(std::max({3 * want, 12ull * n_, 1ull << 20}), limit);
   if (cap <= b_.mask_cap) return;
   dfree(b_.mask_hdr);
   dfree(b_.mask_bits);
