@@ -60,12 +60,12 @@ FORCE_BYTES = {"f64": 188, "comp": 200}
 # 4M launch is larger than an ncu capture should be); at constant density the
 # traffic grows with the particle count, so a full launch is scaled by it.
 FORCE_TRAFFIC_PER_PARTICLE = (238.714880e6 + 79.238912e6) / 1024000
-# Kernels one compensated step launches: the sort (tile histogram, 3-kernel
-# scan of the tile counts, scatter by tile, occupied flags, 3-kernel scan of
-# the flags, tile list, per-tile cells and order, order of large cells,
+# Kernels one compensated step launches: the sort (tile histogram, the sums
+# of the tile counts and occupied tiles per scan tile, their scan with the
+# tile list, scatter by tile, per-tile cells and order, order of large cells,
 # gather) and the passes (tiled and dense-cell density, tiled and dense-cell
 # force).
-LAUNCHES_PER_STEP = 13 + 4
+LAUNCHES_PER_STEP = 7 + 4
 # Whole-step compulsory state traffic (f64 pos, vel, mass in; pos, vel, rho, p out):
 # the algorithmic bytes of one particle-step.
 STEP_BYTES = 120

@@ -464,7 +464,6 @@ void FluidWorld::free_all() {
   dfree(b_.nbr16);
   dfree(b_.sorted_cell);
   dfree(b_.tile_head);
-  dfree(b_.tile_index);
   b_.tile_scan_entries = 0;
   dfree(b_.tile_of);
   dfree(b_.large_cells);
@@ -779,17 +778,16 @@ void FluidWorld::ensure_cells() {
     b_.cell_capacity = cap;
     ++alloc_gen_;
   }
-  // The tiled sort's tile counts and occupied-tile index.
+  // The tiled sort's tile counts.
   if (tile_ && tile_scan_length(b_.cell_capacity) > b_.tile_scan_entries) {
     const size_t len = tile_scan_length(b_.cell_capacity);
     cuda_check(cudaStreamSynchronize(stream_), "tile scan sync");
     dalloc(b_.tile_head, len);
-    dalloc(b_.tile_index, len);
     b_.tile_scan_entries = len;
     ++alloc_gen_;
   }
-  // The scan's tile sums serve the cell scan and the tile scans alike.
-  const int sums = (int)scan_block_sums_needed(b_.cell_capacity);
+  // The scan's tile sums serve the cell scan and the tile scan alike.
+  const int sums = (int)std::max(scan_block_sums_needed(b_.cell_capacity), tile_scan_sums_needed(b_.cell_capacity));
   if (sums > b_.block_sums_capacity) {
     cuda_check(cudaStreamSynchronize(stream_), "sums sync");
     dalloc(b_.block_sums, (size_t)sums);

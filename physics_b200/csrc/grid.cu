@@ -336,36 +336,101 @@ __global__ void __launch_bounds__(kOrderThreads) k_order_large(const uint32_t* _
 // finds the tile empty in the scanned tile counts (its start equals the next
 // tile's start).
 
-// flag[t] = 1 for tiles t < ntiles that hold particles (tstart: the scanned
-// tile counts), 0 up to len.
-__global__ void __launch_bounds__(kThreads) k_tile_occupied(int ntiles, int len, const uint32_t* __restrict__ tstart,
-                                                            uint32_t* __restrict__ flag) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= len) return;
-  flag[t] = (t < ntiles && tstart[t + 1] > tstart[t]) ? 1u : 0u;
+// Per scan tile of the tile counts (kScanTile entries, kScanItems per
+// thread): the sum of the counts and the number of occupied tiles (index
+// below ntiles, count above zero).
+__global__ void __launch_bounds__(kThreads) k_tile_reduce(uint32_t ntiles, const uint32_t* __restrict__ cnt,
+                                                          uint2* __restrict__ sums) {
+  const uint32_t e0 = blockIdx.x * (uint32_t)kScanTile + threadIdx.x * (uint32_t)kScanItems;
+  const uint4* t = reinterpret_cast<const uint4*>(cnt + e0);
+  uint32_t s = 0, o = 0;
+#pragma unroll
+  for (int q = 0; q < kScanItems / 4; ++q) {
+    const uint4 a = t[q];
+    const uint32_t e = e0 + 4u * (uint32_t)q;
+    s += a.x + a.y + a.z + a.w;
+    o += (a.x != 0u && e < ntiles) + (a.y != 0u && e + 1 < ntiles) + (a.z != 0u && e + 2 < ntiles) +
+         (a.w != 0u && e + 3 < ntiles);
+  }
+  for (int d = 16; d > 0; d >>= 1) {
+    s += __shfl_xor_sync(0xffffffffu, s, d);
+    o += __shfl_xor_sync(0xffffffffu, o, d);
+  }
+  __shared__ uint2 ws[kThreads / 32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = make_uint2(s, o);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint2 tot = make_uint2(0u, 0u);
+    for (int w = 0; w < kThreads / 32; ++w) {
+      tot.x += ws[w].x;
+      tot.y += ws[w].y;
+    }
+    sums[blockIdx.x] = tot;
+  }
 }
 
-// Per tile (one thread each): an occupied tile is recorded under its list
-// index (tindex: the scanned occupied flags).  The thread past the last tile
-// writes the overflow cell's range and the end of the tile list.
-__global__ void __launch_bounds__(kThreads) k_tile_list(int n, int ncells, int ntiles,
-                                                        const uint32_t* __restrict__ tstart,
-                                                        const uint32_t* __restrict__ tindex,
+// Exclusive scans of the tile counts (in place: the tile starts) and of the
+// occupied flags, which place every occupied tile in the tile list (tile_of,
+// ascending tile index); each block first adds up the sums of the scan tiles
+// before its own.  The thread holding entry ntiles (the overflow bucket)
+// writes the overflow cell's range, the number of occupied tiles and the end
+// of the last tile.
+__global__ void __launch_bounds__(kThreads) k_tile_scan(int n, int ncells, uint32_t ntiles, uint32_t* __restrict__ cnt,
+                                                        const uint2* __restrict__ sums,
                                                         uint32_t* __restrict__ cell_start,
                                                         uint32_t* __restrict__ tile_of,
                                                         uint32_t* __restrict__ tile_slot,
                                                         uint32_t* __restrict__ num_tiles) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t > ntiles) return;
-  if (t == ntiles) {
-    const uint32_t of = tstart[ntiles], count = tindex[ntiles];
+  uint32_t ps = 0, po = 0, total = 0;
+  for (uint32_t k = threadIdx.x; k < blockIdx.x; k += blockDim.x) {
+    const uint2 v = sums[k];
+    ps += v.x;
+    po += v.y;
+  }
+  (void)block_exclusive_scan(ps, total);
+  const uint32_t carry_s = total;
+  (void)block_exclusive_scan(po, total);
+  const uint32_t carry_o = total;
+  const uint32_t e0 = blockIdx.x * (uint32_t)kScanTile + threadIdx.x * (uint32_t)kScanItems;
+  uint4* t = reinterpret_cast<uint4*>(cnt + e0);
+  uint32_t a[kScanItems];
+#pragma unroll
+  for (int q = 0; q < kScanItems / 4; ++q) {
+    const uint4 u = t[q];
+    a[4 * q] = u.x;
+    a[4 * q + 1] = u.y;
+    a[4 * q + 2] = u.z;
+    a[4 * q + 3] = u.w;
+  }
+  uint32_t s = 0, o = 0, occ = 0;
+#pragma unroll
+  for (int q = 0; q < kScanItems; ++q) {
+    const uint32_t x = a[q];
+    const bool f = x != 0u && e0 + (uint32_t)q < ntiles;
+    occ |= (uint32_t)f << q;
+    o += f;
+    a[q] = s;
+    s += x;
+  }
+  const uint32_t off_s = block_exclusive_scan(s, total) + carry_s;
+  const uint32_t off_o = block_exclusive_scan(o, total) + carry_o;
+#pragma unroll
+  for (int q = 0; q < kScanItems / 4; ++q)
+    t[q] = make_uint4(a[4 * q] + off_s, a[4 * q + 1] + off_s, a[4 * q + 2] + off_s, a[4 * q + 3] + off_s);
+  uint32_t li = off_o;
+  for (uint32_t bits = occ; bits != 0u; bits &= bits - 1u) tile_of[li++] = e0 + (uint32_t)(__ffs(bits) - 1);
+  if (ntiles >= e0 && ntiles < e0 + (uint32_t)kScanItems) {
+    const uint32_t q = ntiles - e0;
+    uint32_t of = off_s;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j)
+      if ((uint32_t)j == q) of = a[j] + off_s;
+    const uint32_t count = off_o + (uint32_t)__popc(occ);  // no flags at or past ntiles
     cell_start[ncells] = of;
     cell_start[ncells + 1] = (uint32_t)n;
     *num_tiles = count;
     tile_slot[count] = of;  // the end of the last tile
-    return;
   }
-  if (tstart[t + 1] > tstart[t]) tile_of[tindex[t]] = (uint32_t)t;
 }
 
 // One CTA per occupied tile (persistent over the tile list).  The tile's
@@ -654,6 +719,7 @@ static int scan_length(int buckets) { return ((buckets + 2 + kScanTile - 1) / kS
 
 size_t scan_block_sums_needed(int ncells) { return (size_t)scan_length(ncells) / kScanTile; }
 size_t tile_scan_length(int ncells) { return (size_t)scan_length(ncells / 8); }
+size_t tile_scan_sums_needed(int ncells) { return 2 * tile_scan_length(ncells) / kScanTile; }
 
 // Cells of the current positions (pv1): cell_start over the box and perm[s]
 // = the particle (index into the current arrays) at sorted slot s, ordered
@@ -672,22 +738,21 @@ static void build_cells(const StepConsts& c, DevBuffers& b, cudaStream_t s, int 
   const ParticleConsts& src = b.pc[b.cur];
   cudaMemsetAsync(b.order_count, 0, sizeof(uint32_t), s);
   if (c.tile) {
-    // Tiled: counts per tile, then cells and in-cell order per occupied tile
-    // (the tile-count array is tile_head, the occupied-tile index
-    // tile_index; the by-cell list of the tiles ordered in global memory goes
+    // Tiled: counts per tile, their scan with the occupied-tile list, then
+    // cells and in-cell order per occupied tile (the tile-count array is
+    // tile_head; the by-cell list of the tiles ordered in global memory goes
     // to sorted_cell, which the gather rewrites).
     const int shift = 3 * c.tile_log2;
     const int ntiles = c.ncells >> shift;
     const int tlen = scan_length(ntiles);
+    uint2* sums = reinterpret_cast<uint2*>(b.block_sums);  // 2 x tlen / kScanTile entries
     cudaMemsetAsync(b.tile_head, 0, (size_t)tlen * sizeof(uint32_t), s);
     k_cell_hist<<<grid_for(n, bs), bs, 0, s>>>(c, shift, b.pv1[0], b.pv1[1], b.pv1[2], b.cell_of, b.rank,
                                                  b.tile_head, flags, src.scene, src.id, okey);
-    scan_in_place(b.tile_head, tlen, b.block_sums, s);
+    k_tile_reduce<<<tlen / kScanTile, kThreads, 0, s>>>((uint32_t)ntiles, b.tile_head, sums);
+    k_tile_scan<<<tlen / kScanTile, kThreads, 0, s>>>(n, c.ncells, (uint32_t)ntiles, b.tile_head, sums,
+                                                      b.cell_start, b.tile_of, b.tile_slot, b.num_tiles);
     k_scatter<<<grid_for(n, bs), bs, 0, s>>>(n, shift, b.cell_of, b.rank, b.tile_head, b.tmp);
-    k_tile_occupied<<<grid_for(tlen), kThreads, 0, s>>>(ntiles, tlen, b.tile_head, b.tile_index);
-    scan_in_place(b.tile_index, tlen, b.block_sums, s);
-    k_tile_list<<<grid_for(ntiles + 1), kThreads, 0, s>>>(n, c.ncells, ntiles, b.tile_head, b.tile_index,
-                                                          b.cell_start, b.tile_of, b.tile_slot, b.num_tiles);
     auto cells = c.tile == 4 ? k_tile_cells<64> : k_tile_cells<8>;
     cells<<<tile_cells_blocks(), kThreads, 0, s>>>(n, c.ncells, b.tile_head, b.tile_of, b.num_tiles, b.tmp, b.cell_of,
                                                   okey, b.rank, b.perm, b.sorted_cell, b.cell_start, b.tile_slot,

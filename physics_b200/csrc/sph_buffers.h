@@ -54,13 +54,11 @@ struct DevBuffers {
   uint16_t* nbr16 = nullptr;
   // Tiled sort: cell of each sorted slot (before the gather: the particles
   // grouped by cell), particles per tile scanned to tile starts (tile_head)
-  // and occupied tiles scanned to list indices (tile_index), both over the
-  // cell box's tiles plus the overflow bucket (tile_scan_entries); the tile of
-  // every list entry, the first slot of every occupied tile (+ end), and the
-  // device-side tile count.
+  // over the cell box's tiles plus the overflow bucket (tile_scan_entries);
+  // the tile of every list entry, the first slot of every occupied tile
+  // (+ end), and the device-side tile count.
   uint32_t* sorted_cell = nullptr;
   uint32_t* tile_head = nullptr;
-  uint32_t* tile_index = nullptr;
   size_t tile_scan_entries = 0;
   uint32_t* tile_of = nullptr;
   uint32_t* tile_slot = nullptr;
@@ -199,6 +197,8 @@ size_t scan_block_sums_needed(int count);
 // Entries of the tiled sort's tile scans for a box of ncells cells (tiles of 8
 // cells or more, plus the overflow bucket, in whole scan tiles).
 size_t tile_scan_length(int ncells);
+// Scan-tile sums the tile scan needs (two per scan tile) for a box of ncells.
+size_t tile_scan_sums_needed(int ncells);
 
 // Launch knobs (results do not depend on them): resident CTAs per SM of the
 // tiled passes' persistent grids (0 = the occupancy limit), their tile
