@@ -1134,7 +1134,8 @@ __global__ void __launch_bounds__(kWT, 4) k_density_dense(StepConsts c, TiledArg
 // warp walks the masks in lockstep for as many rounds as the fullest mask has
 // bits, each lane taking its own next candidate through the pair terms of the
 // tiled pass.  The partial sums are folded into the compensated totals every
-// 8 rounds and at the end of the chunk, uniformly across the warp.
+// 16 rounds (every 8 with the shear sum, one candidate per round) and at the
+// end of the chunk, uniformly across the warp.
 template <int TB, bool kShear>
 __global__ void __launch_bounds__(kWT, 2) k_force_dense(StepConsts c, TiledArgs a) {
   // The chunk's 32 candidates, and in slot 32 a weightless copy of its first
@@ -1187,9 +1188,9 @@ __global__ void __launch_bounds__(kWT, 2) k_force_dense(StepConsts c, TiledArgs 
           mask &= mask - 1;
           pair2_listed(Q, s_pos[w][ka], s_vel[w][ka], s_mr[w][ka], s_pos[w][kb], s_vel[w][kb], s_mr[w][kb],
                        part2);
-          if ((r & 7) == 7) fold2(acc, part2);
+          if ((r & 15) == 15) fold2(acc, part2);
         }
-        if (rounds & 7) fold2(acc, part2);
+        if (rounds & 15) fold2(acc, part2);
       } else {
         const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(mask));
         for (int r = 0; r < rounds; ++r) {
