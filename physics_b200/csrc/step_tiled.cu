@@ -619,19 +619,20 @@ __device__ __forceinline__ void finish_particle(const StepConsts& c, const Tiled
 
 // Batch partial sums of the pressure and raw viscous forces (and of the
 // shear sum, when it is live); folded into the Kahan-compensated totals every
-// four pairs.
+// eight pairs, scaled by the query's common factors (sp = m_i * spiky
+// coefficient, sv = m_i * laplacian coefficient).
 struct ForcePart {
   float fx = 0.f, fy = 0.f, fz = 0.f, vx = 0.f, vy = 0.f, vz = 0.f, sh = 0.f;
 };
 
 template <bool kShear>
-__device__ __forceinline__ void fold(CompAcc& q, ForcePart& b) {
-  kahan_add(q.fpx, q.cpx, b.fx);
-  kahan_add(q.fpy, q.cpy, b.fy);
-  kahan_add(q.fpz, q.cpz, b.fz);
-  kahan_add(q.fvx, q.cvx, b.vx);
-  kahan_add(q.fvy, q.cvy, b.vy);
-  kahan_add(q.fvz, q.cvz, b.vz);
+__device__ __forceinline__ void fold(CompAcc& q, ForcePart& b, float sp, float sv) {
+  kahan_add(q.fpx, q.cpx, sp * b.fx);
+  kahan_add(q.fpy, q.cpy, sp * b.fy);
+  kahan_add(q.fpz, q.cpz, sp * b.fz);
+  kahan_add(q.fvx, q.cvx, sv * b.vx);
+  kahan_add(q.fvy, q.cvy, sv * b.vy);
+  kahan_add(q.fvz, q.cvz, sv * b.vz);
   if (kShear) kahan_add(q.shear, q.csh, b.sh);
   b = ForcePart();
 }
@@ -650,14 +651,16 @@ __device__ __forceinline__ void pair_listed(const StepConsts& c, float4 pj, floa
   const float mr = pos ? mr_j : 0.f;
   const float r = r2 * inv_r;
   const float hr = c.h0f - r;
-  // (d/r) * m_i m_j (p_i/rho_i^2 + p_j/rho_j^2) * spiky(r)
-  const float fp = (pi.w * pj.w) * (vi.w + vj.w) * (c.spiky_cf * hr) * (hr * inv_r);
+  // (d/r) * m_j (p_i/rho_i^2 + p_j/rho_j^2) (h - r)^2; times m_i and the
+  // spiky coefficient at the fold
+  const float fp = (pj.w * (vi.w + vj.w)) * (hr * (hr * inv_r));
   b.fx = fmaf(dx, fp, b.fx);
   b.fy = fmaf(dy, fp, b.fy);
   b.fz = fmaf(dz, fp, b.fz);
-  // dv * (m_i m_j / rho_j * lap(r))
+  // dv * m_j / rho_j (h - r); times m_i and the laplacian coefficient at the
+  // fold
   const float dvx = vj.x - vi.x, dvy = vj.y - vi.y, dvz = vj.z - vi.z;
-  const float vf = lapm_i * mr * hr;
+  const float vf = mr * hr;
   b.vx = fmaf(dvx, vf, b.vx);
   b.vy = fmaf(dvy, vf, b.vy);
   b.vz = fmaf(dvz, vf, b.vz);
@@ -832,7 +835,7 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
               const uint32_t j = (w[u >> 1] >> (16 * (u & 1))) & 0xffffu;
               pair_listed<kShear>(c, s_pos[j], s_vel[j], s_mr[j], pi, vi, lapm_i, b, q);
             }
-            if (u == 3 || u == 7) fold<kShear>(q, b);
+            if (u == 7) fold<kShear>(q, b, pi.w * c.spiky_cf, lapm_i);
           }
           cur = nxt;
         }
@@ -846,7 +849,7 @@ __global__ void __launch_bounds__(kTT, 3) k_force_tiled(StepConsts c, TiledArgs 
               const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
               if (!(dx * dx + dy * dy + dz * dz < hc2)) continue;
               pair_listed<kShear>(c, pj, s_vel[j], s_mr[j], pi, vi, lapm_i, b, q);
-              fold<kShear>(q, b);
+              fold<kShear>(q, b, pi.w * c.spiky_cf, lapm_i);
             }
           }
       }
@@ -1199,9 +1202,9 @@ __global__ void __launch_bounds__(kWT, 2) k_force_dense(StepConsts c, TiledArgs 
             mask &= mask - 1;
             pair_listed<kShear>(c, s_pos[w][k], s_vel[w][k], s_mr[w][k], qp, qvel, lapm, part, acc);
           }
-          if ((r & 7) == 7) fold<kShear>(acc, part);
+          if ((r & 7) == 7) fold<kShear>(acc, part, qp.w * c.spiky_cf, lapm);
         }
-        if (rounds & 7) fold<kShear>(acc, part);
+        if (rounds & 7) fold<kShear>(acc, part, qp.w * c.spiky_cf, lapm);
       }
     };
     uint32_t mbase = a.task_mbase ? a.task_mbase[t.k] : kNoMasks;
