@@ -59,7 +59,7 @@ FORCE_BYTES = {"f64": 188, "comp": 200}
 # dram__bytes_write.sum from an ncu capture of the 80x160x80 dam break (the
 # 4M launch is larger than an ncu capture should be); at constant density the
 # traffic grows with the particle count, so a full launch is scaled by it.
-FORCE_TRAFFIC_PER_PARTICLE = (238.714880e6 + 79.238912e6) / 1024000
+FORCE_TRAFFIC_PER_PARTICLE = (239.449344e6 + 80.680448e6) / 1024000
 # Kernels one compensated step launches: the sort (tile histogram, the sums
 # of the tile counts and occupied tiles per scan tile, their scan with the
 # tile list, scatter by tile, per-tile cells and order, order of large cells,
