@@ -129,6 +129,47 @@ def test_kat_two_particle_force(oracle_mod):
     assert np.all(acc[:, 1:] == 0.0)
 
 
+def test_kat_integrate_and_bounds_by_hand(oracle_mod):
+    """integrate (world.rs:352-363) and enforce_bounds (world.rs:366-397) evaluated by hand in
+    the reference's operation order on isolated particles (more than h apart: no pair term,
+    so acc = xsph = 0): a = (acc + g) + body_acc; v += a dt; v += xsph eps; x += v dt;
+    body_acc cleared; a coordinate past a wall is set to the wall and that velocity
+    component becomes -v * damp.  Two steps, so the second sees body_acc cleared."""
+    O = oracle_mod
+    p = SphParams.defaults()
+    p.bounds_min, p.bounds_max = (0.0, 0.0, 0.0), (1.0, 1.0, 1.0)
+    g, damp, eps, dt = (0.0, -9.81, 0.0), 0.4, 0.5, 0.01
+    pos = [[0.005, 0.5, 0.99], [0.5, 0.002, 0.5], [0.8, 0.8, 0.2]]
+    vel = [[-1.0, 0.5, 2.0], [0.25, -0.5, 0.125], [0.1, 0.2, 0.3]]
+    body = [[0.25, 1.5, -0.75], [0.0, 0.0, 0.0], [0.0, 0.0, 0.0]]
+    w = world(O, p)
+    w.add_particles(pos, 2.0, vel=vel)
+    w.set(O.F_BODY_ACC, np.array(body))
+    x = [list(r) for r in pos]
+    v = [list(r) for r in vel]
+    for step in range(2):
+        w.step(dt)
+        for i in range(3):
+            for k in range(3):
+                a = (0.0 + g[k]) + (body[i][k] if step == 0 else 0.0)
+                v[i][k] = v[i][k] + a * dt
+                v[i][k] = v[i][k] + 0.0 * eps
+                x[i][k] = x[i][k] + v[i][k] * dt
+                if x[i][k] < 0.0:
+                    x[i][k], v[i][k] = 0.0, -v[i][k] * damp
+                elif x[i][k] > 1.0:
+                    x[i][k], v[i][k] = 1.0, -v[i][k] * damp
+        assert np.all(w.get(O.F_ACC) == 0.0) and np.all(w.get(O.F_XSPH) == 0.0)
+        assert np.all(w.get(O.F_BODY_ACC) == 0.0)
+        assert_bits_equal(w.get(O.F_POS), np.array(x), f"positions after step {step + 1}")
+        assert_bits_equal(w.get(O.F_VEL), np.array(v), f"velocities after step {step + 1}")
+        if step == 0:
+            # The first step meets the walls: x of particle 0 and y of particle 1 low, z of
+            # particle 0 high; the second moves them back inside.
+            assert x[0][0] == 0.0 and x[1][1] == 0.0 and x[0][2] == 1.0
+            assert v[0][0] > 0.0 and v[1][1] > 0.0 and v[0][2] < 0.0
+
+
 def test_kat_interior_lattice_density(oracle_mod):
     """An interior particle of an unjittered lattice has rho = rest density (world.rs:146-169)."""
     O = oracle_mod
