@@ -129,6 +129,46 @@ def test_kat_two_particle_force(oracle_mod):
     assert np.all(acc[:, 1:] == 0.0)
 
 
+def test_kat_two_particle_xsph_and_power_law_viscosity(oracle_mod):
+    """Two compressed particles at r < h with a shear-thinning material (visc_n = 0.5), by hand from
+    compute_forces (world.rs:252-347): XSPH sum (v_j - v_i) m_j/rho_j W_poly6(r), the
+    strain-rate proxy |v_j - v_i| / (r + 1e-4) m_j/rho_j, mu_eff = k max(shear,
+    shear_min)^(n - 1), the equation of state, and the acceleration with its pressure term and
+    its viscous term scaled by mu_eff."""
+    O = oracle_mod
+    p = ref_test_params(gravity=(0.0, 0.0, 0.0), visc_k=[3.5], visc_n=[0.5])
+    w = world(O, p)
+    w.add_particles([[0.0, 0.0, 0.0], [0.05, 0.0, 0.0]], 4.0, vel=[[0.0, 0.0, 0.0], [1.0, 0.0, 0.0]])
+    w.step(1e-3)
+    h, r, m = 0.2, 0.05, 4.0
+    c6 = 315.0 / (64.0 * math.pi * h ** 9)
+    wr = c6 * (h * h - r * r) ** 3
+    rho = m * c6 * (h * h) ** 3 + m * wr
+    np.testing.assert_allclose(w.get(O.F_RHO), rho, rtol=1e-14)
+    prs = 250.0 * (rho - 1000.0) if rho > 1000.0 else 0.0
+    assert prs > 0.0  # the pair is compressed: the pressure term is live
+    np.testing.assert_allclose(w.get(O.F_P), [prs, prs], rtol=1e-12)
+    xs = m / rho * wr  # dv = +1 on particle 0, -1 on particle 1
+    xsph = w.get(O.F_XSPH)
+    np.testing.assert_allclose(xsph[0], [xs, 0.0, 0.0], rtol=1e-13)
+    np.testing.assert_allclose(xsph[1], [-xs, 0.0, 0.0], rtol=1e-13)
+    shear = 1.0 / (r + 1e-4) * (m / rho)
+    mu = 3.5 * max(shear, 0.01) ** (0.5 - 1.0)
+    np.testing.assert_allclose(w.get(O.F_MU_EFF), [mu, mu], rtol=1e-13)
+    spiky = -45.0 / (math.pi * h ** 6) * (h - r) ** 2
+    lap = 45.0 / (math.pi * h ** 6) * (h - r)
+    acc0 = (m * m * (2 * prs / rho ** 2) * spiky + (m * m / rho * lap) * mu) / rho
+    acc = w.get(O.F_ACC)
+    np.testing.assert_allclose(acc[:, 0], [acc0, -acc0], rtol=1e-12)
+    assert np.all(acc[:, 1:] == 0.0)
+    # With visc_n = 1 the same pair gives mu_eff = visc_k exactly (sph/tests.rs:406-427).
+    p1 = ref_test_params(gravity=(0.0, 0.0, 0.0))
+    w1 = world(O, p1)
+    w1.add_particles([[0.0, 0.0, 0.0], [0.05, 0.0, 0.0]], 2.0, vel=[[0.0, 0.0, 0.0], [1.0, 0.0, 0.0]])
+    w1.step(1e-3)
+    assert np.all(w1.get(O.F_MU_EFF) == 3.5)
+
+
 def test_kat_integrate_and_bounds_by_hand(oracle_mod):
     """integrate (world.rs:352-363) and enforce_bounds (world.rs:366-397) evaluated by hand in
     the reference's operation order on isolated particles (more than h apart: no pair term,
