@@ -169,6 +169,27 @@ def test_kat_two_particle_xsph_and_power_law_viscosity(oracle_mod):
     assert np.all(w1.get(O.F_MU_EFF) == 3.5)
 
 
+def test_kat_diagnostics_in_insertion_order(oracle_mod):
+    """FluidSubsystem::total_momentum and kinetic_energy (subsystem.rs:149-163) by hand:
+    p += v * m and e += (|v|^2 * m) / (1 + 1) over the particles in insertion order, with
+    nalgebra's norm_squared as (x^2 + y^2) + z^2; bit for bit."""
+    O = oracle_mod
+    rng = np.random.default_rng(11)
+    n = 257
+    pos = rng.uniform(-2.5, 2.5, (n, 3))
+    vel = rng.normal(0.0, 3.0, (n, 3))
+    mass = rng.uniform(0.5, 2.0, n)
+    w = world(O, ref_test_params())
+    w.add_particles(pos, mass, vel=vel)
+    px = py = pz = e = 0.0
+    for i in range(n):
+        vx, vy, vz = (float(c) for c in vel[i])
+        m = float(mass[i])
+        px, py, pz = px + vx * m, py + vy * m, pz + vz * m
+        e = e + ((vx * vx + vy * vy) + vz * vz) * m / (1.0 + 1.0)
+    assert_bits_equal(w.diagnostics(), np.array([px, py, pz, e]), "momentum and kinetic energy")
+
+
 def test_kat_integrate_and_bounds_by_hand(oracle_mod):
     """integrate (world.rs:352-363) and enforce_bounds (world.rs:366-397) evaluated by hand in
     the reference's operation order on isolated particles (more than h apart: no pair term,
