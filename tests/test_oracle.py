@@ -190,6 +190,99 @@ def test_kat_diagnostics_in_insertion_order(oracle_mod):
     assert_bits_equal(w.diagnostics(), np.array([px, py, pz, e]), "momentum and kinetic energy")
 
 
+def _hand_step_one_cell(pos, vel, mass, dt, h=0.2, rest=1000.0, stiff=250.0, visc=3.5, shear_min=0.01,
+                        g=(0.0, -9.81, 0.0), xsph_eps=0.5):
+    """One FluidWorld<f64>::step of particles that all lie in one grid cell, so that every
+    particle's neighbours are visited in insertion order, written directly from
+    kernels.rs:21-66 (coefficients, poly6, spiky gradient, viscosity laplacian) and
+    world.rs:204-363 in their operation order; norm() is sqrt((x^2 + y^2) + z^2), the
+    3-vector case of nalgebra's dot product.  Material 0 with visc_n = 1, no walls met."""
+    pi = math.pi
+    h2 = h * h
+    h3 = h2 * h
+    h6 = h3 * h3
+    h9 = h6 * h3
+    c_poly6 = 315.0 / (64.0 * pi * h9)
+    c_spiky = -45.0 / (pi * h6)
+    c_lap = 45.0 / (pi * h6)
+
+    def poly6(r):
+        if r >= h:
+            return 0.0
+        d = h2 - r * r
+        return c_poly6 * d * d * d
+
+    def norm(a):
+        return math.sqrt((a[0] * a[0] + a[1] * a[1]) + a[2] * a[2])
+
+    def sub(a, b):
+        return [a[0] - b[0], a[1] - b[1], a[2] - b[2]]
+
+    n = len(pos)
+    rho, prs = [], []
+    for i in range(n):
+        acc_rho = 0.0
+        for j in range(n):
+            r = norm(sub(pos[i], pos[j]))
+            if r < h:
+                acc_rho += mass[j] * poly6(r)
+        rho.append(acc_rho)
+        over = acc_rho - rest
+        prs.append(stiff * over if over > 0.0 else 0.0)
+    acc, xsph, mu = [], [], []
+    for i in range(n):
+        fp, fv, xs, shear = [0.0] * 3, [0.0] * 3, [0.0] * 3, 0.0
+        for j in range(n):
+            if j == i:
+                continue
+            d = sub(pos[j], pos[i])
+            r = norm(d)
+            if r >= h or r <= 0.0:
+                continue
+            grad = c_spiky * (h - r) * (h - r)
+            coef = mass[i] * mass[j] * (prs[i] / (rho[i] * rho[i]) + prs[j] / (rho[j] * rho[j]))
+            dv = sub(vel[j], vel[i])
+            lap = c_lap * (h - r)
+            wv = mass[i] * mass[j] / rho[j] * lap
+            wx = mass[j] / rho[j] * poly6(r)
+            for k in range(3):
+                fp[k] += d[k] / r * (coef * grad)
+                fv[k] += dv[k] * wv
+                xs[k] += dv[k] * wx
+            shear += norm(dv) / (r + 1e-4) * (mass[j] / rho[j])
+        m_eff = visc * (shear if shear > shear_min else shear_min) ** (1.0 - 1.0)
+        acc.append([(fp[k] + fv[k] * m_eff) / rho[i] if rho[i] > 0.0 else 0.0 for k in range(3)])
+        xsph.append(xs)
+        mu.append(m_eff)
+    x, v = [list(r) for r in pos], [list(r) for r in vel]
+    for i in range(n):
+        for k in range(3):
+            v[i][k] = v[i][k] + ((acc[i][k] + g[k]) + 0.0) * dt
+            v[i][k] = v[i][k] + xsph[i][k] * xsph_eps
+            x[i][k] = x[i][k] + v[i][k] * dt
+    return rho, prs, acc, xsph, mu, x, v
+
+
+def test_kat_one_cell_step_by_hand(oracle_mod):
+    """A whole step of four compressed, moving particles in one grid cell, evaluated by hand
+    from the reference's kernels and passes (_hand_step_one_cell), equals the oracle bit for
+    bit in every output: density, pressure, acceleration, XSPH, mu_eff, position, velocity."""
+    O = oracle_mod
+    pos = [[0.03, 0.04, 0.05], [0.09, 0.06, 0.08], [0.12, 0.15, 0.07], [0.05, 0.13, 0.16]]
+    vel = [[0.5, -0.25, 0.0], [-0.75, 0.125, 0.5], [0.0, 1.0, -0.5], [0.25, 0.0, 0.375]]
+    mass = [3.0, 3.5, 2.75, 4.0]
+    dt = 0.002
+    w = world(O, ref_test_params())
+    w.add_particles(pos, np.array(mass), vel=vel)
+    w.step(dt)
+    rho, prs, acc, xsph, mu, x, v = _hand_step_one_cell(pos, vel, mass, dt)
+    assert all(p > 0.0 for p in prs)  # every particle compressed: the pressure terms are live
+    for name, field, want in (("rho", O.F_RHO, rho), ("p", O.F_P, prs), ("acc", O.F_ACC, acc),
+                              ("xsph", O.F_XSPH, xsph), ("mu_eff", O.F_MU_EFF, mu), ("pos", O.F_POS, x),
+                              ("vel", O.F_VEL, v)):
+        assert_bits_equal(w.get(field), np.array(want), name)
+
+
 def test_kat_integrate_and_bounds_by_hand(oracle_mod):
     """integrate (world.rs:352-363) and enforce_bounds (world.rs:366-397) evaluated by hand in
     the reference's operation order on isolated particles (more than h apart: no pair term,
