@@ -190,13 +190,14 @@ def test_kat_diagnostics_in_insertion_order(oracle_mod):
     assert_bits_equal(w.diagnostics(), np.array([px, py, pz, e]), "momentum and kinetic energy")
 
 
-def _hand_step_one_cell(pos, vel, mass, dt, h=0.2, rest=1000.0, stiff=250.0, visc=3.5, shear_min=0.01,
-                        g=(0.0, -9.81, 0.0), xsph_eps=0.5):
-    """One FluidWorld<f64>::step of particles that all lie in one grid cell, so that every
-    particle's neighbours are visited in insertion order, written directly from
-    kernels.rs:21-66 (coefficients, poly6, spiky gradient, viscosity laplacian) and
-    world.rs:204-363 in their operation order; norm() is sqrt((x^2 + y^2) + z^2), the
-    3-vector case of nalgebra's dot product.  Material 0 with visc_n = 1, no walls met."""
+def _hand_step(pos, vel, mass, dt, h=0.2, rest=1000.0, stiff=250.0, visc=3.5, shear_min=0.01,
+               g=(0.0, -9.81, 0.0), xsph_eps=0.5):
+    """One FluidWorld<f64>::step written directly from grid.rs:25-56 (cell keys
+    floor(x * (1/h)), cells listing their particles in insertion order, the 3x3x3 cells
+    visited x-outer, z-inner), kernels.rs:21-66 (coefficients, poly6, spiky gradient,
+    viscosity laplacian) and world.rs:204-363, each in its operation order; norm() is
+    sqrt((x^2 + y^2) + z^2), the 3-vector case of nalgebra's dot product.  Material 0 with
+    visc_n = 1, no walls met."""
     pi = math.pi
     h2 = h * h
     h3 = h2 * h
@@ -219,10 +220,26 @@ def _hand_step_one_cell(pos, vel, mass, dt, h=0.2, rest=1000.0, stiff=250.0, vis
         return [a[0] - b[0], a[1] - b[1], a[2] - b[2]]
 
     n = len(pos)
+    inv = 1.0 / h
+
+    def key(p):
+        return tuple(math.floor(c * inv) for c in p)
+
+    cells = {}
+    for i in range(n):
+        cells.setdefault(key(pos[i]), []).append(i)
+
+    def neighbours(i):
+        ci, cj, ck = key(pos[i])
+        for di in (-1, 0, 1):
+            for dj in (-1, 0, 1):
+                for dk in (-1, 0, 1):
+                    yield from cells.get((ci + di, cj + dj, ck + dk), [])
+
     rho, prs = [], []
     for i in range(n):
         acc_rho = 0.0
-        for j in range(n):
+        for j in neighbours(i):
             r = norm(sub(pos[i], pos[j]))
             if r < h:
                 acc_rho += mass[j] * poly6(r)
@@ -232,7 +249,7 @@ def _hand_step_one_cell(pos, vel, mass, dt, h=0.2, rest=1000.0, stiff=250.0, vis
     acc, xsph, mu = [], [], []
     for i in range(n):
         fp, fv, xs, shear = [0.0] * 3, [0.0] * 3, [0.0] * 3, 0.0
-        for j in range(n):
+        for j in neighbours(i):
             if j == i:
                 continue
             d = sub(pos[j], pos[i])
@@ -265,7 +282,7 @@ def _hand_step_one_cell(pos, vel, mass, dt, h=0.2, rest=1000.0, stiff=250.0, vis
 
 def test_kat_one_cell_step_by_hand(oracle_mod):
     """A whole step of four compressed, moving particles in one grid cell, evaluated by hand
-    from the reference's kernels and passes (_hand_step_one_cell), equals the oracle bit for
+    from the reference's kernels and passes (_hand_step), equals the oracle bit for
     bit in every output: density, pressure, acceleration, XSPH, mu_eff, position, velocity."""
     O = oracle_mod
     pos = [[0.03, 0.04, 0.05], [0.09, 0.06, 0.08], [0.12, 0.15, 0.07], [0.05, 0.13, 0.16]]
@@ -275,12 +292,34 @@ def test_kat_one_cell_step_by_hand(oracle_mod):
     w = world(O, ref_test_params())
     w.add_particles(pos, np.array(mass), vel=vel)
     w.step(dt)
-    rho, prs, acc, xsph, mu, x, v = _hand_step_one_cell(pos, vel, mass, dt)
+    rho, prs, acc, xsph, mu, x, v = _hand_step(pos, vel, mass, dt)
     assert all(p > 0.0 for p in prs)  # every particle compressed: the pressure terms are live
-    for name, field, want in (("rho", O.F_RHO, rho), ("p", O.F_P, prs), ("acc", O.F_ACC, acc),
-                              ("xsph", O.F_XSPH, xsph), ("mu_eff", O.F_MU_EFF, mu), ("pos", O.F_POS, x),
-                              ("vel", O.F_VEL, v)):
-        assert_bits_equal(w.get(field), np.array(want), name)
+    _assert_step_outputs(O, w, (rho, prs, acc, xsph, mu, x, v))
+
+
+def _assert_step_outputs(O, w, want):
+    for name, field, values in zip(("rho", "p", "acc", "xsph", "mu_eff", "pos", "vel"),
+                                   (O.F_RHO, O.F_P, O.F_ACC, O.F_XSPH, O.F_MU_EFF, O.F_POS, O.F_VEL), want):
+        assert_bits_equal(w.get(field), np.array(values), name)
+
+
+def test_kat_multi_cell_step_by_hand(oracle_mod):
+    """The same hand evaluation over 80 random particles spread over a 5x5x5 block of grid
+    cells, negative coordinates included (floor keys): the 27-cell visit order decides every
+    sum's order, so bit equality pins the oracle's neighbour order as well as its arithmetic."""
+    O = oracle_mod
+    rng = np.random.default_rng(5)
+    pos = rng.uniform(-0.35, 0.45, (80, 3))
+    vel = rng.normal(0.0, 0.5, (80, 3))
+    mass = rng.uniform(3.0, 6.0, 80)
+    dt = 0.001
+    w = world(O, ref_test_params())
+    w.add_particles(pos, mass, vel=vel)
+    w.step(dt)
+    want = _hand_step(pos.tolist(), vel.tolist(), mass.tolist(), dt)
+    assert sum(p > 0.0 for p in want[1]) > 40  # most particles are compressed
+    assert len({tuple(np.floor(q / 0.2).astype(int)) for q in pos}) >= 27
+    _assert_step_outputs(O, w, want)
 
 
 def test_kat_integrate_and_bounds_by_hand(oracle_mod):
