@@ -322,6 +322,62 @@ def test_kat_multi_cell_step_by_hand(oracle_mod):
     _assert_step_outputs(O, w, want)
 
 
+def _hand_lattice_mass(s, h=0.2, rest=1000.0):
+    """FluidWorld::lattice_mass (world.rs:148-169) restated: rest / sum of poly6 over the
+    lattice points of spacing s within h, shells -n..n with n = ceil(h / s) + 1, visited
+    i-outer, l-inner, r = s * sqrt(i^2 + j^2 + l^2)."""
+    h2 = h * h
+    h9 = (h2 * h) * (h2 * h) * (h2 * h)
+    c6 = 315.0 / (64.0 * math.pi * h9)
+    n_shell = math.ceil(h / s) + 1
+    total = 0.0
+    for i in range(-n_shell, n_shell + 1):
+        for j in range(-n_shell, n_shell + 1):
+            for l in range(-n_shell, n_shell + 1):
+                r = s * math.sqrt(float(i * i + j * j + l * l))
+                if r < h:
+                    d = h2 - r * r
+                    total += c6 * d * d * d
+    return rest / total
+
+
+def _hand_fill_box(mn, mx, spacing, margin):
+    """FluidWorld::fill_box (world.rs:124-144) restated: the lattice from min + margin to
+    max - margin by repeated addition of the spacing, x-outer, z-inner."""
+    lo = [c + margin for c in mn]
+    hi = [c - margin for c in mx]
+    out = []
+    x = lo[0]
+    while x <= hi[0]:
+        y = lo[1]
+        while y <= hi[1]:
+            z = lo[2]
+            while z <= hi[2]:
+                out.append([x, y, z])
+                z += spacing
+            y += spacing
+        x += spacing
+    return out
+
+
+@pytest.mark.parametrize("mn,mx,spacing,margin", [((-1, 1, -1), (1, 3, 1), 0.3, 0.1),
+                                                  ((0.0, 0.0, 0.0), (1.0, 0.7, 0.45), 0.1, 0.05),
+                                                  ((-0.4, -0.2, 0.1), (0.3, 0.35, 0.9), 0.07, 0.0)])
+def test_kat_fill_box_and_lattice_mass_by_hand(oracle_mod, mn, mx, spacing, margin):
+    """fill_box's positions (accumulated coordinates, so the last point of a row can fall
+    short of or land on hi) and lattice_mass, restated from world.rs:124-169, equal the
+    oracle's bit for bit."""
+    O = oracle_mod
+    w = world(O)
+    w.fill_box(mn, mx, spacing, margin)
+    want = _hand_fill_box([float(c) for c in mn], [float(c) for c in mx], spacing, margin)
+    assert len(w) == len(want) > 0
+    assert_bits_equal(w.get(O.F_POS), np.array(want), "fill_box positions")
+    m = _hand_lattice_mass(spacing)
+    assert_bits_equal(w.get(O.F_MASS), np.full(len(want), m), "lattice mass")
+    assert w.lattice_mass(spacing) == m
+
+
 def test_kat_integrate_and_bounds_by_hand(oracle_mod):
     """integrate (world.rs:352-363) and enforce_bounds (world.rs:366-397) evaluated by hand in
     the reference's operation order on isolated particles (more than h apart: no pair term,
