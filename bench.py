@@ -135,6 +135,27 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# Algorithmic flops of one particle-step: the candidate test (~8 flops: three
+# differences, a sum of squares, a compare) in each of the two passes, the
+# density term (~12) and the force terms (~60: distance, pressure, viscosity,
+# XSPH, strain rate) per in-range pair, with candidates and pairs counted on the
+# device (phy_fluid_step_counters).
+FLOPS_PER_CANDIDATE_PASS = 8
+FLOPS_PER_PAIR = 12 + 60
+
+
+def flop_rate(counters: dict, n: int, step_ms: float) -> dict:
+    """The flop side of the step's roofline: algorithmic flops per particle-step from the
+    device counters of one counted step, and the rate they imply at step_ms per step.  No
+    FP32 CUDA-core peak is measured on this hardware, so no fraction is formed."""
+    c = counters["candidates"] / n if n else 0.0
+    p = counters["pairs"] / n if n else 0.0
+    per = 2 * FLOPS_PER_CANDIDATE_PASS * c + FLOPS_PER_PAIR * p
+    return {"flops_per_particle_step": per, "candidates_per_particle": c, "pairs_per_particle": p,
+            "achieved_tflops": per * n / (step_ms / 1e3) / 1e12 if step_ms > 0 else None,
+            "peak": None, "unit": "TFLOP/s"}
+
+
 def bench_config(dims, n: int, world_size: int) -> dict:
     """The workload both arms run (the precision of each arm is its line's dtype)."""
     return {"workload": f"dam_break_{dims[0]}x{dims[1]}x{dims[2]}: {n} particles, spacing 0.1 = h/2, "
@@ -641,6 +662,7 @@ def run_ours(args):
             "full_trajectory": {"steps": full["steps"], "ms_per_step": full["ms_per_step"],
                                 "value": full["value"]} if full else None,
             "pairs_per_particle": cnt["pairs"] / n,
+            "flops": flop_rate(cnt, n, step_ms),
             "roofline": {
                 "bound": "issue",
                 "axis": "hbm",

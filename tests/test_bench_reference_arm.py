@@ -1,8 +1,8 @@
-"""bench.py's reference arm on CPU: it times the oracle (the CPU restatement of the
-reference's rayon step) through the same command line as the product's arm, prints the
-contract's JSON line with "impl": "reference", and never loads the product library
-(libphysph.so) into its process, so the measured baseline contains none of this
-library's code."""
+"""bench.py's host side on CPU.  The reference arm times the oracle (the CPU restatement
+of the reference's rayon step) through the same command line as the product's arm,
+prints the contract's JSON line with "impl": "reference", and never loads the product
+library (libphysph.so) into its process, so the measured baseline contains none of this
+library's code.  The flop side of the roofline follows from the device counters."""
 import json
 import subprocess
 import sys
@@ -41,3 +41,14 @@ def test_reference_arm_prints_its_line_without_the_product_library():
     libs = json.loads(mapped[0][len("MAPPED "):])
     assert any(p.endswith("liboracle.so") for p in libs), libs
     assert not any("libphysph" in p for p in libs), libs
+
+
+def test_flop_rate_from_counters():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    n = 1000
+    r = bench.flop_rate({"candidates": 219 * n, "pairs": 30 * n, "particles": n, "cells": 0}, n, 2.0)
+    assert r["candidates_per_particle"] == 219.0 and r["pairs_per_particle"] == 30.0
+    assert r["flops_per_particle_step"] == 2 * 8 * 219 + 72 * 30
+    assert abs(r["achieved_tflops"] - r["flops_per_particle_step"] * n / 2e-3 / 1e12) < 1e-15
+    assert r["peak"] is None
