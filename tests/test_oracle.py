@@ -594,6 +594,26 @@ def test_scene_generator_sizes():
     assert u.min() >= 0.0 and u.max() < 1.0
 
 
+def test_batched_form_scenes_follow_their_configuration():
+    """The batched form's 256 scenes: counts log-uniform in [2k, 200k] (rounded per axis, so
+    within a few percent of the range), fill fraction U[0.2, 0.5] (rounding likewise), every
+    particle inside its scene's box, about half the scenes below the geometric mean, and the
+    same 12,067,610 particles on every call."""
+    b = scenes.batch_scenes(256)
+    n = np.array([x.n for x in b])
+    assert int(n.sum()) == 12067610
+    assert n.min() >= 0.95 * 2000 and n.max() <= 1.05 * 200000
+    box = np.array([x.bounds_max for x in b])
+    fill = n * scenes.SPACING ** 3 / box.prod(axis=1)
+    assert fill.min() >= 0.19 and fill.max() <= 0.53
+    for x in b:
+        assert x.bounds_min == (0.0, 0.0, 0.0)
+        assert (x.pos >= 0.0).all() and (x.pos <= np.array(x.bounds_max)).all()
+    assert 0.4 <= float((n < np.sqrt(2000 * 200000)).mean()) <= 0.6
+    again = scenes.batch_scenes(256)
+    assert all(np.array_equal(x.pos, y.pos) and x.bounds_max == y.bounds_max for x, y in zip(b, again))
+
+
 def test_splitmix_matches_sequential_definition():
     """Vectorised SplitMix64 equals the sequential Rng::next_u64 (replay.rs:40-46)."""
     mask = (1 << 64) - 1
