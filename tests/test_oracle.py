@@ -594,6 +594,26 @@ def test_scene_generator_sizes():
     assert u.min() >= 0.0 and u.max() < 1.0
 
 
+def test_dam_break_jitter_follows_its_recipe():
+    """The scale configurations' lattice: points at ((i + 0.5) s, (j + 0.5) s, (k + 0.5) s),
+    x-outer, each coordinate moved by U(-0.05 s, 0.05 s) from SplitMix64 draws in order
+    (x, y, z per point), and the same block restated by the independent generator of the
+    golden fixtures (tests/golden/gen_golden.py) bit for bit."""
+    import importlib.util
+    from pathlib import Path
+    pos = scenes.dam_break_positions(6, 6, 6)
+    s = scenes.SPACING
+    i, j, k = np.meshgrid(np.arange(6), np.arange(6), np.arange(6), indexing="ij")
+    base = np.stack([(i + 0.5) * s, (j + 0.5) * s, (k + 0.5) * s], axis=-1).reshape(-1, 3)
+    assert np.abs(pos - base).max() <= 0.05 * s
+    assert np.abs(pos - base).max() > 0.04 * s  # the jitter is there
+    spec = importlib.util.spec_from_file_location(
+        "gen_golden_for_jitter", Path(__file__).resolve().parent / "golden" / "gen_golden.py")
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    assert_bits_equal(pos, np.array(gen.jittered_block(6, 6, 6)), "jittered block")
+
+
 def test_batched_form_scenes_follow_their_configuration():
     """The batched form's 256 scenes: counts log-uniform in [2k, 200k] (rounded per axis, so
     within a few percent of the range), fill fraction U[0.2, 0.5] (rounding likewise), every
